@@ -1,0 +1,354 @@
+"""Benchmark of the matrix-free heat operator on the config-2 workload.
+
+Workload (synthetic, seeded): unit cube, 64^3 hexahedra with interior vertices
+displaced by U[-0.1h, 0.1h] (PCG64 seed 2), FE_Q(4) (16,974,593 DoFs), heat
+operator M/dt + div(k(T) grad) with k(T) = k0 (1 + 1e-3 T), k0 = 1, rho c_p = 1,
+dt = 1e-3, T ~ U[300, 3000] (seed 3), Dirichlet T = 0 on all faces.
+
+A step is one FP64 operator apply (vmult) with all data resident in HBM; value =
+DoFs x steps / time (whole job: N GPUs run independent replicas).  After the
+timed steps the same operator is solved with CG + Chebyshev(5)/Jacobi to a
+relative residual of 1e-10 in the plain FP64 form and in the FP32-inner /
+FP64-defect-correction form (solves/s, iterations, error against the FP64
+solution, p50/p99 latency over repeated solves).
+
+`--impl reference` times the CPU restatement of the reference's operator
+(the reference itself needs deal.II/Trilinos/p4est/MPI, which this image does
+not have) on a bounded sample of the same workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "mat-free DoFs/s & solves/s, FP32+FP64-refined vs FP64 at 1e-10; p50/p99 latency"
+NC, DEGREE = (64, 64, 64), 4
+DT, K0, K_ALPHA = 1e-3, 1.0, 1e-3
+
+# dram__bytes_read.sum + dram__bytes_write.sum per apply of the FP64 cell kernel
+# (8 colour launches), from the ncu capture summarised in
+# profiles/heat_apply_q4_kT_fp64.md; None until a capture exists.
+MEASURED_TRAFFIC_BYTES = None
+
+
+def algorithmic_bytes(n_dofs, n_cells, degree, real_bytes):
+    """src + dst + T (one read/write each) + the metric stream (JxW and the 6
+    entries of JxW J^-1 J^-T per quadrature point)."""
+    nq = (degree + 1) ** 3
+    return real_bytes * (3 * n_dofs) + real_bytes * 7 * nq * n_cells
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = os.path.join("/tmp", f"mpdg_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem():
+    import meltpooldg_b200 as M
+    V = M.box_vertices(NC, perturb=0.1, seed=2)
+    mask = M.boundary_mask(NC, DEGREE)
+    mesh = M.Mesh(V, NC, DEGREE, mask)
+    T = np.random.Generator(np.random.PCG64(3)).uniform(300.0, 3000.0, mesh.n_dofs)
+    return M, V, mask, mesh, T
+
+
+def cpu_reference_rate(V, T, mask, n_dofs, target_seconds=10.0, cell_fraction=None):
+    """Oracle apply over a contiguous block of cells; returns (DoFs/s, sample text, threads)."""
+    from oracle import oracle as O
+    om = O.Mesh(3, DEGREE, NC, V)
+    op = O.Operator(O.HEAT, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA, temperature=T, dirichlet=mask)
+    src = np.random.Generator(np.random.PCG64(0)).uniform(-1.0, 1.0, n_dofs)
+    n_cells = int(np.prod(NC))
+    # calibrate on a small block, then time a block of ~target_seconds
+    c = 256
+    t0 = time.perf_counter()
+    O.vmult_cells(om, op, src, 0, c)
+    dt = time.perf_counter() - t0
+    if cell_fraction is None:
+        c = int(min(n_cells, max(256, c * target_seconds / max(dt, 1e-6))))
+    else:
+        c = max(1, int(n_cells * cell_fraction))
+    t0 = time.perf_counter()
+    O.vmult_cells(om, op, src, 0, c)
+    dt = time.perf_counter() - t0
+    rate = n_dofs * (c / n_cells) / dt
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return rate, f"{c} of {n_cells} cells of one apply ({dt:.2f} s)", threads, dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    M = None
+    import meltpooldg_b200  # noqa: F401  (only to share the mesh helpers)
+    from meltpooldg_b200 import box_vertices, boundary_mask
+    V = box_vertices(NC, perturb=0.1, seed=2)
+    mask = boundary_mask(NC, DEGREE)
+    n_dofs = int(np.prod([n * DEGREE + 1 for n in NC]))
+    T = np.random.Generator(np.random.PCG64(3)).uniform(300.0, 3000.0, n_dofs)
+    # each step: a fixed sample of cells sized to ~4 s
+    _, _, _, _ = cpu_reference_rate(V, T, mask, n_dofs, target_seconds=0.5)
+    rate0, sample, threads, dt0 = cpu_reference_rate(V, T, mask, n_dofs, target_seconds=4.0)
+    frac = float(sample.split(" of ")[0]) / np.prod(NC)
+    for _ in range(args.warmup):
+        cpu_reference_rate(V, T, mask, n_dofs, cell_fraction=frac)
+    times = []
+    for _ in range(args.steps):
+        r, _, _, dt = cpu_reference_rate(V, T, mask, n_dofs, cell_fraction=frac)
+        times.append(dt)
+    tot = sum(times)
+    value = n_dofs * frac * args.steps / tot
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "DoFs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "heat operator apply, Q4, 64^3 perturbed hex cells, k(T)=k0(1+1e-3T)",
+                   "n_dofs": n_dofs, "cells": int(np.prod(NC)), "degree": DEGREE,
+                   "sample": f"{frac:.5f} of the cells per step"},
+        "cpu_baseline": {"value": value, "unit": "DoFs/s", "cores": threads, "kind": "port",
+                         "sample": f"{frac * np.prod(NC):.0f} cells of one apply per step"},
+        "e2e": {"value": value, "unit": "DoFs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "CPU restatement of the reference's operator (oracle/); the reference needs "
+                "deal.II + Trilinos + p4est + MPI, absent from this image",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    M, V, mask, mesh, T = build_problem()
+    N = mesh.n_dofs
+    op = M.HeatDiffuseOperator(mesh, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA,
+                               precisions=("fp64", "fp32"))
+    Td = torch.tensor(T, device="cuda")
+    op.set_temperature(Td)
+    rng = np.random.Generator(np.random.PCG64(0))
+    src = torch.tensor(rng.uniform(-1.0, 1.0, N), device="cuda")
+    dst = torch.empty_like(src)
+    src32, dst32 = src.float(), torch.empty(N, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        op.vmult(dst, src)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = M.kernel_launches()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            op.vmult(dst, src)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = M.kernel_launches() - launches0
+    barrier()
+    t = e0.elapsed_time(e1) / 1e3
+    t_max = t
+    if world > 1:
+        tt = torch.tensor([t], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt)
+    value = N * args.steps * world / t_max
+    apply_s = t / args.steps
+
+    # FP32 apply
+    for _ in range(3):
+        op.vmult(dst32, src32)
+    e0.record(stream)
+    for _ in range(args.steps):
+        op.vmult(dst32, src32)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    apply32_s = e0.elapsed_time(e1) / 1e3 / args.steps
+
+    # end to end through the host-buffer C-ABI call (pinned host buffers)
+    hsrc = torch.empty(N, dtype=torch.float64).pin_memory()
+    hdst = torch.empty(N, dtype=torch.float64).pin_memory()
+    hsrc.copy_(src.cpu())
+    hs, hd = hsrc.numpy(), hdst.numpy()
+    op.vmult_host(hd, hs)
+    e2e_steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        op.vmult_host(hd, hs)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+
+    peak, peak_kind = load_peaks()
+    E = int(np.prod(NC))
+    b64 = algorithmic_bytes(N, E, DEGREE, 8)
+    b32 = algorithmic_bytes(N, E, DEGREE, 4)
+    roof = {"bound": "hbm", "achieved": b64 / apply_s / 1e9, "peak": peak, "unit": "GB/s",
+            "frac": b64 / apply_s / 1e9 / peak,
+            "traffic": MEASURED_TRAFFIC_BYTES,
+            "algorithmic_bytes": b64, "kernel": "cell_kernel<4,double,GENERAL,LINEAR,kT> x 8 colours",
+            "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+            "fp32": {"achieved": b32 / apply32_s / 1e9, "frac": b32 / apply32_s / 1e9 / peak,
+                     "algorithmic_bytes": b32}}
+
+    # solves: CG + Chebyshev(5)/Jacobi to 1e-10, FP64 and FP32-inner/FP64-refined
+    solves = None
+    if not args.no_solve:
+        xs = torch.tensor(np.random.Generator(np.random.PCG64(5)).uniform(-1, 1, N), device="cuda")
+        xs[torch.tensor(mask.astype(bool), device="cuda")] = 0.0
+        b = torch.empty_like(xs)
+        op.vmult(b, xs)
+        solves = {}
+        ref_x = None
+        for form, mixed in (("fp64", False), ("fp32_refined", True)):
+            data = M.LinearSolverData(solver_type="CG", preconditioner_type="Chebyshev",
+                                      rel_tolerance=1e-10, abs_tolerance=1e-20, mixed_precision=mixed)
+            lat = []
+            rep = None
+            for r in range(args.solve_reps):
+                x = torch.zeros_like(xs)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                M.LinearSolver.solve(op, x, b, data)
+                torch.cuda.synchronize()
+                lat.append(time.perf_counter() - t0)
+                rep = dict(M.LinearSolver.last_report)
+            if ref_x is None:
+                ref_x = x.clone()
+            err = float((x - ref_x).abs().max() / ref_x.abs().max())
+            lat.sort()
+            solves[form] = {
+                "solves_per_s": world / statistics.median(lat),
+                "p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                "iterations": rep["iterations"], "outer_iterations": rep["outer_iterations"],
+                "operator_applies": rep["operator_applies"],
+                "relative_residual": rep["final_residual"] / rep["initial_residual"],
+                "max_rel_error_vs_fp64_solution": err,
+                "max_rel_error_vs_exact": float((x - xs).abs().max() / xs.abs().max()),
+            }
+        solves["speedup_fp32_refined_vs_fp64"] = (solves["fp32_refined"]["solves_per_s"] /
+                                                  solves["fp64"]["solves_per_s"])
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        rate, sample, threads, _ = cpu_reference_rate(V, T, mask, N, target_seconds=args.cpu_seconds)
+        cpu = {"value": rate, "unit": "DoFs/s", "cores": threads, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "DoFs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "heat operator apply, Q4, 64^3 perturbed hex cells, k(T)=k0(1+1e-3T)",
+                       "n_dofs": N, "cells": E, "degree": DEGREE, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (metric stream 1.8 GB per apply)"},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": N / e2e_s, "unit": "DoFs/s", "h2d_bytes_per_step": 8 * N,
+                    "d2h_bytes_per_step": 8 * N, "call": "mpdg_vmult_host (pinned host buffers)"},
+            "fp32_apply": {"value": N / apply32_s, "unit": "DoFs/s"},
+            "solves": solves,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--solve-reps", type=int, default=3)
+    ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,183 @@
+/*
+ * mpdg.h -- C ABI of the B200 matrix-free heat / advection-diffusion operator
+ * library (libmpdg.so, CUDA sm_100a).
+ *
+ * Every entry point returns an int status (MPDG_OK = 0, negative = error) and
+ * never throws.  Vectors passed to the apply/solve calls are DEVICE pointers
+ * (unless the name says _host), laid out in the library's lexicographic DoF
+ * numbering (x fastest):
+ *     g = (Z * NY + Y) * NX + X,   X = ix * degree + i  in [0, nc[0] * degree]
+ * Constrained (Dirichlet) DoFs are read as zero by the operator apply and are
+ * never written by it, as in MeltPoolDG's MatrixFree cell loops.
+ *
+ * Each entry point names the MeltPoolDG interface it replaces.  Calls on one
+ * operator must be serialised by the caller; they are queued on the
+ * operator's stream (set with mpdg_op_set_stream, default: the legacy stream).
+ */
+#ifndef MPDG_H
+#define MPDG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int mpdg_status;
+enum {
+  MPDG_OK = 0,
+  MPDG_ERR_ARG = -1,            /* invalid argument */
+  MPDG_ERR_CUDA = -2,           /* CUDA runtime error (see mpdg_last_error) */
+  MPDG_ERR_ALLOC = -3,          /* device allocation failed */
+  MPDG_ERR_NOT_CONVERGED = -4,  /* iteration limit reached (SolverControl::NoConvergence) */
+  MPDG_ERR_BREAKDOWN = -5,      /* CG breakdown: p.Ap <= 0 or rz <= 0 */
+  MPDG_ERR_NAN = -6,            /* non-finite residual */
+  MPDG_ERR_UNSUPPORTED = -7,    /* configuration not implemented on the device */
+  MPDG_ERR_BUDGET = -8,         /* request exceeds the memory budget (serving) */
+  MPDG_ERR_SIZE = -9            /* problem larger than a fixed capacity */
+};
+
+enum { MPDG_OP_HEAT = 0, MPDG_OP_ADVDIFF = 1 };
+enum { MPDG_FP64 = 0, MPDG_FP32 = 1 };
+enum {
+  MPDG_VEL_NONE = 0,
+  MPDG_VEL_ROTATION = 1, /* u = s (z, 0, -x): advection_diffusion_vortex.hpp:93-115 (dim 3) */
+  MPDG_VEL_VORTEX = 2,   /* u = (sin pi x cos pi y, -cos pi x sin pi y, 0) */
+  MPDG_VEL_CONST = 3     /* u = vel_param */
+};
+enum { MPDG_GEOM_AUTO = 0, MPDG_GEOM_GENERAL = 1 };
+enum { MPDG_SOLVER_CG = 0, MPDG_SOLVER_GMRES = 1 };
+enum { MPDG_PREC_IDENTITY = 0, MPDG_PREC_JACOBI = 1, MPDG_PREC_CHEBYSHEV = 2 };
+enum { MPDG_FIELD_TEMPERATURE = 0 };
+
+typedef struct mpdg_mesh mpdg_mesh;
+typedef struct mpdg_op mpdg_op;
+
+/* Structured hexahedral mesh of nc[0] x nc[1] x nc[2] trilinear cells carrying
+ * FE_Q(degree) on Gauss-Lobatto points with QGauss(degree+1) quadrature
+ * (source/utilities/fe_util.cpp:18-57). */
+typedef struct {
+  int dim;                         /* must be 3 */
+  int degree;                      /* 1..4 */
+  int nc[3];
+  const double *vertices;          /* host, (nc0+1)(nc1+1)(nc2+1) x 3, x fastest */
+  const uint8_t *dirichlet_mask;   /* host, n_dofs entries (1 = constrained) or NULL */
+  int geometry;                    /* MPDG_GEOM_AUTO: uniform boxes skip the metric stream */
+} mpdg_mesh_desc;
+
+/* Operator parameters (names follow MeltPoolDG's HeatData / AdvectionDiffusionData). */
+typedef struct {
+  int kind;                 /* MPDG_OP_HEAT or MPDG_OP_ADVDIFF */
+  double dt;                /* time increment (OperatorBase::reset_time_increment) */
+  /* heat: v = rho_cp/dt u + rho_cp vel.grad u, g = k(T) grad u, k(T) = k0 (1 + k_alpha T) */
+  double rho_cp, k0, k_alpha;
+  int full_tangent;         /* add dk/dT grad(T) u to the flux (non-symmetric tangent) */
+  /* advection-diffusion: v = u/dt + theta vel.grad u, g = theta D grad u */
+  double theta, diffusivity;
+  int vel_kind;
+  double vel_param[3];
+  int precision_mask;       /* bit MPDG_FP64 / bit MPDG_FP32: forms to prepare (0 = FP64) */
+} mpdg_op_desc;
+
+typedef struct {
+  int solver;               /* MPDG_SOLVER_CG or MPDG_SOLVER_GMRES (right preconditioned) */
+  int preconditioner;       /* MPDG_PREC_* */
+  int max_iterations;       /* LinearSolverData::max_iterations */
+  double rel_tolerance;     /* LinearSolverData::rel_tolerance */
+  double abs_tolerance;     /* LinearSolverData::abs_tolerance */
+  int gmres_restart;        /* Krylov basis size, default 30 */
+  int chebyshev_degree;     /* residual polynomial degree (degree-1 applies), default 5 */
+  int lanczos_steps;        /* eigenvalue estimate steps, default 10 */
+  double chebyshev_range;   /* lambda_min = lambda_max / range, default 30 */
+  double chebyshev_safety;  /* lambda_max scaled by this, default 1.2 */
+  int mixed_precision;      /* 1: FP32 inner CG + FP64 defect correction */
+  double inner_tolerance;   /* relative reduction of each inner FP32 solve, default 1e-4 */
+  int max_outer;            /* defect-correction steps, default 20 */
+} mpdg_solver_desc;
+
+typedef struct {
+  int status;               /* MPDG_OK or an error code */
+  int iterations;           /* Krylov iterations (sum of inner ones when mixed) */
+  int outer_iterations;     /* defect-correction steps (mixed) */
+  int operator_applies;     /* all operator applies, any precision */
+  double initial_residual;  /* |b - A x0|_2 */
+  double final_residual;    /* |b - A x|_2 in FP64 */
+  double lambda_max;        /* Chebyshev estimate (0 if unused) */
+  double seconds;           /* wall time of the solve */
+} mpdg_solve_report;
+
+/* ------------------------------------------------------------------ general */
+const char *mpdg_last_error(void);
+int mpdg_version(void);
+
+/* ------------------------------------------------------------------ meshes */
+/* replaces ScratchData::build / MatrixFree::reinit: source/core/scratch_data.cpp:191-268 */
+mpdg_status mpdg_mesh_create(const mpdg_mesh_desc *desc, mpdg_mesh **mesh);
+mpdg_status mpdg_mesh_destroy(mpdg_mesh *mesh);
+/* n_dofs of the mesh (ScratchData::get_dof_handler(idx).n_dofs()) */
+mpdg_status mpdg_mesh_n_dofs(const mpdg_mesh *mesh, int64_t *n_dofs);
+/* device bytes held by the mesh (geometry stream, masks) */
+mpdg_status mpdg_mesh_device_bytes(const mpdg_mesh *mesh, int64_t *bytes);
+
+/* ---------------------------------------------------------------- operators */
+/* replaces the constructors of HeatDiffuseMultiPhaseOperator
+ * (include/meltpooldg/heat/heat_diffuse_operator.hpp:110) and
+ * AdvectionDiffusionOperator (source/level_set/advection_diffusion_operator.cpp:17-41) */
+mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **op);
+mpdg_status mpdg_op_destroy(mpdg_op *op);
+/* OperatorBase::reset_time_increment, include/meltpooldg/core/operator_base.hpp:41-46 */
+mpdg_status mpdg_op_reset_time_increment(mpdg_op *op, double dt);
+/* OperatorBase::reset_dof_index, operator_base.hpp:31-35: use_dirichlet = 0 selects
+ * the constraint set without Dirichlet rows (used for the lifting of
+ * include/meltpooldg/linear_algebra/utilities_matrixfree.hpp:39-101) */
+mpdg_status mpdg_op_use_dirichlet(mpdg_op *op, int use_dirichlet);
+/* state vectors the operator reads (temperature for k(T) and the Newton residual);
+ * device pointer, FP64, n_dofs; an FP32 copy is made for the FP32 form */
+mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *device_values);
+mpdg_status mpdg_op_set_stream(mpdg_op *op, void *cuda_stream);
+
+/* OperatorMatrixFree::vmult, operator_base.hpp:239-243
+ * (heat: source/heat/heat_diffuse_operator.cpp:179-197;
+ *  advection-diffusion: source/level_set/advection_diffusion_operator.cpp:238-272) */
+mpdg_status mpdg_vmult(mpdg_op *op, double *dst, const double *src);
+/* the same operator applied in FP32 (operator data and vectors in FP32) */
+mpdg_status mpdg_vmult_f32(mpdg_op *op, float *dst, const float *src);
+/* host-buffer form: copies src to the device, applies, copies dst back */
+mpdg_status mpdg_vmult_host(mpdg_op *op, double *dst_host, const double *src_host);
+
+/* OperatorMatrixFree::compute_inverse_diagonal_from_matrixfree, operator_base.hpp:268-272
+ * (heat: heat_diffuse_operator.cpp:271-284, threshold 1e-10;
+ *  advection-diffusion: advection_diffusion_operator.cpp:401-446, threshold 1e-14 max(1,|d|inf)) */
+mpdg_status mpdg_compute_inverse_diagonal(mpdg_op *op, double *inv_diag);
+/* the diagonal itself (before inversion; constrained entries 1) */
+mpdg_status mpdg_compute_diagonal(mpdg_op *op, double *diag);
+
+/* OperatorMatrixFree::create_rhs, operator_base.hpp:208-212: dst += rhs contribution.
+ * heat (heat_diffuse_operator.cpp:783-806): src = T_old, the operator's temperature
+ *   field is T, heat_source may be NULL; Dirichlet DoFs are not written.
+ * advection-diffusion (advection_diffusion_operator.cpp:276-358): src = phi_old,
+ *   heat_source must be NULL; written to all DoFs unless Dirichlet rows are selected. */
+mpdg_status mpdg_create_rhs(mpdg_op *op, double *dst, const double *src, const double *heat_source);
+
+/* LinearSolver::solve, include/meltpooldg/linear_algebra/linear_solver.hpp:26-134,
+ * with the Jacobi preconditioner of preconditioner_jacobi.hpp:29-88 (or the
+ * Chebyshev smoother on top of it).  x holds the initial guess on entry. */
+mpdg_status mpdg_solve(mpdg_op *op, const mpdg_solver_desc *desc, double *x, const double *b,
+                       mpdg_solve_report *report);
+/* host-buffer form of mpdg_solve (x_host in/out, b_host in) */
+mpdg_status mpdg_solve_host(mpdg_op *op, const mpdg_solver_desc *desc, double *x_host,
+                            const double *b_host, mpdg_solve_report *report);
+void mpdg_solver_desc_default(mpdg_solver_desc *desc);
+
+/* integrated L2 norm of a DoF vector (VectorTools::compute_norm,
+ * source/utilities/vector_tools.cpp:170-201), FP64 */
+mpdg_status mpdg_l2_norm(mpdg_op *op, const double *u, double *norm);
+
+/* number of kernels this library launched since load (its own kernels only) */
+int64_t mpdg_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,127 @@
+"""ctypes binding of libmpdg.so (the C ABI declared in include/mpdg.h).
+
+The library is loaded from this package directory.  A missing or unloadable
+library raises at import of the operator classes: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpdg.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "mpdg.h")
+
+# status codes (mirror include/mpdg.h)
+OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_NAN, ERR_UNSUPPORTED, \
+    ERR_BUDGET, ERR_SIZE = 0, -1, -2, -3, -4, -5, -6, -7, -8, -9
+OP_HEAT, OP_ADVDIFF = 0, 1
+FP64, FP32 = 0, 1
+VEL_NONE, VEL_ROTATION, VEL_VORTEX, VEL_CONST = 0, 1, 2, 3
+GEOM_AUTO, GEOM_GENERAL = 0, 1
+SOLVER_CG, SOLVER_GMRES = 0, 1
+PREC_IDENTITY, PREC_JACOBI, PREC_CHEBYSHEV = 0, 1, 2
+FIELD_TEMPERATURE = 0
+
+_STATUS_NAMES = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_ALLOC", -4: "ERR_NOT_CONVERGED",
+                 -5: "ERR_BREAKDOWN", -6: "ERR_NAN", -7: "ERR_UNSUPPORTED", -8: "ERR_BUDGET",
+                 -9: "ERR_SIZE"}
+
+
+class MpdgError(RuntimeError):
+    def __init__(self, status, where, msg):
+        super().__init__(f"{where}: {_STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class NoConvergence(MpdgError):
+    """Counterpart of dealii::SolverControl::NoConvergence (linear_solver.hpp:124-129)."""
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("dim", C.c_int), ("degree", C.c_int), ("nc", C.c_int * 3),
+                ("vertices", C.POINTER(C.c_double)), ("dirichlet_mask", C.POINTER(C.c_uint8)),
+                ("geometry", C.c_int)]
+
+
+class OpDesc(C.Structure):
+    _fields_ = [("kind", C.c_int), ("dt", C.c_double), ("rho_cp", C.c_double), ("k0", C.c_double),
+                ("k_alpha", C.c_double), ("full_tangent", C.c_int), ("theta", C.c_double),
+                ("diffusivity", C.c_double), ("vel_kind", C.c_int), ("vel_param", C.c_double * 3),
+                ("precision_mask", C.c_int)]
+
+
+class SolverDesc(C.Structure):
+    _fields_ = [("solver", C.c_int), ("preconditioner", C.c_int), ("max_iterations", C.c_int),
+                ("rel_tolerance", C.c_double), ("abs_tolerance", C.c_double),
+                ("gmres_restart", C.c_int), ("chebyshev_degree", C.c_int),
+                ("lanczos_steps", C.c_int), ("chebyshev_range", C.c_double),
+                ("chebyshev_safety", C.c_double), ("mixed_precision", C.c_int),
+                ("inner_tolerance", C.c_double), ("max_outer", C.c_int)]
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("outer_iterations", C.c_int),
+                ("operator_applies", C.c_int), ("initial_residual", C.c_double),
+                ("final_residual", C.c_double), ("lambda_max", C.c_double), ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def header_symbols():
+    """Function names declared in include/mpdg.h."""
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(mpdg_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib():
+    """The loaded library; raises if it is absent (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libmpdg.so is not built ({LIB_PATH}); run __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, fp = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_float)
+    L.mpdg_last_error.restype = C.c_char_p
+    L.mpdg_kernel_launches.restype = C.c_int64
+    L.mpdg_mesh_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(vp)]
+    L.mpdg_mesh_destroy.argtypes = [vp]
+    L.mpdg_mesh_n_dofs.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.mpdg_mesh_device_bytes.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.mpdg_op_create.argtypes = [vp, C.POINTER(OpDesc), C.POINTER(vp)]
+    L.mpdg_op_destroy.argtypes = [vp]
+    L.mpdg_op_reset_time_increment.argtypes = [vp, C.c_double]
+    L.mpdg_op_use_dirichlet.argtypes = [vp, C.c_int]
+    L.mpdg_op_set_field.argtypes = [vp, C.c_int, vp]
+    L.mpdg_op_set_stream.argtypes = [vp, vp]
+    L.mpdg_vmult.argtypes = [vp, vp, vp]
+    L.mpdg_vmult_f32.argtypes = [vp, vp, vp]
+    L.mpdg_vmult_host.argtypes = [vp, dp, dp]
+    L.mpdg_compute_inverse_diagonal.argtypes = [vp, vp]
+    L.mpdg_compute_diagonal.argtypes = [vp, vp]
+    L.mpdg_create_rhs.argtypes = [vp, vp, vp, vp]
+    L.mpdg_solve.argtypes = [vp, C.POINTER(SolverDesc), vp, vp, C.POINTER(SolveReport)]
+    L.mpdg_solve_host.argtypes = [vp, C.POINTER(SolverDesc), dp, dp, C.POINTER(SolveReport)]
+    L.mpdg_solver_desc_default.argtypes = [C.POINTER(SolverDesc)]
+    L.mpdg_solver_desc_default.restype = None
+    L.mpdg_l2_norm.argtypes = [vp, vp, dp]
+    _lib = L
+    return L
+
+
+def check(status, where):
+    if status != OK:
+        msg = lib().mpdg_last_error().decode(errors="replace")
+        cls = NoConvergence if status == ERR_NOT_CONVERGED else MpdgError
+        raise cls(status, where, msg)
+    return status
+
+
+def kernel_launches():
+    return int(lib().mpdg_kernel_launches())

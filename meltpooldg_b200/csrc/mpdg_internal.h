@@ -1,0 +1,111 @@
+// Internal declarations of libmpdg (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mpdg.h"
+
+namespace mpdg {
+
+constexpr int kMaxDegree = 4;
+constexpr int kMaxN = kMaxDegree + 1;
+
+// thrown inside the library, converted to a status code at the C boundary
+struct Error {
+  int status;
+  std::string msg;
+};
+
+void set_last_error(const std::string &msg);
+void count_launch(int n = 1);
+
+#define MPDG_CUDA(call)                                                               \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      throw ::mpdg::Error{MPDG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+#define MPDG_LAUNCHED()                                      \
+  do {                                                       \
+    cudaError_t e_ = cudaGetLastError();                     \
+    if (e_ != cudaSuccess)                                   \
+      throw ::mpdg::Error{MPDG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)}; \
+    ::mpdg::count_launch();                                  \
+  } while (0)
+
+// Cells are processed in 8 parity colours (ix%2, iy%2, iz%2): two cells of one
+// colour never share a DoF, so a colour's cells add into dst without atomics.
+struct Colour {
+  int par[3];
+  int cn[3];     // cells per direction in this colour
+  long count;    // cells in this colour
+  long first;    // index of its first cell in colour-major order
+};
+
+struct Mesh {
+  int degree = 1, n = 2;
+  int nc[3] = {1, 1, 1};
+  long NX = 0, NY = 0, NZ = 0, N = 0, n_cells = 0;
+  bool uniform = false;
+  double h[3] = {0, 0, 0}, origin[3] = {0, 0, 0};
+  Colour colour[8];
+  std::vector<double> vertices;        // host copy
+  double *d_vert = nullptr;            // device vertices
+  double *d_metric64 = nullptr;        // general geometry: [colour-major cell][7][n^3]
+  float *d_metric32 = nullptr;
+  uint8_t *d_dmask = nullptr;          // Dirichlet mask per DoF (nullptr: none)
+  uint8_t *d_cell_flags = nullptr;     // per colour-major cell: bit0 touches a constrained DoF
+  bool has_dirichlet = false;
+  size_t device_bytes = 0;
+  bool metric32_ready = false;
+};
+
+struct Workspace;  // solver vectors (solvers.cu)
+
+struct Op {
+  Mesh *mesh = nullptr;
+  mpdg_op_desc d{};
+  bool use_dirichlet = true;
+  cudaStream_t stream = nullptr;
+  const double *T64 = nullptr;         // caller-owned temperature (device)
+  float *T32 = nullptr;                // FP32 copy of T
+  double *d_velb64 = nullptr;          // general geometry + velocity: [cell][3][n^3]
+  float *d_velb32 = nullptr;
+  float *d_trig32 = nullptr;           // uniform vortex velocity: sin/cos tables
+  double *d_trig64 = nullptr;
+  Workspace *ws = nullptr;
+  size_t device_bytes = 0;
+};
+
+// ---- operator kernels (operator_kernels.cu)
+void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_general);
+void ensure_metric32(Mesh &m, cudaStream_t s);
+void build_op_device_data(Op &op);
+void ensure_T32(Op &op);
+
+template <typename Real>
+void launch_apply(Op &op, Real *dst, const Real *src);
+void launch_rhs(Op &op, double *dst, const double *src, const double *heat_source);
+void launch_diagonal(Op &op, double *diag);
+void launch_invert_diagonal(Op &op, double *diag);
+double l2_norm_integrated(Op &op, const double *u);
+
+// ---- vector kernels (vector_kernels.cu)
+template <typename Real>
+struct Reducer;  // deterministic two-pass reductions into FP64
+
+double dot(const double *a, const double *b, long n, cudaStream_t s);
+double dot_f(const float *a, const float *b, long n, cudaStream_t s);
+double norm2(const double *a, long n, cudaStream_t s);
+double linf(const double *a, long n, cudaStream_t s);
+
+// ---- solvers (solvers.cu)
+int solve(Op &op, const mpdg_solver_desc &desc, double *x, const double *b, mpdg_solve_report &rep);
+void free_workspace(Op &op);
+
+}  // namespace mpdg

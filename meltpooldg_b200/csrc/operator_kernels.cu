@@ -1,0 +1,1260 @@
+// Matrix-free cell kernels of the heat and advection-diffusion operators (sm_100a).
+//
+// One cell is handled by n*n threads (n = degree + 1): thread (i, j) keeps the
+// DoF column (i, j, 0..n-1) in registers.  Contractions along z run in
+// registers, along x and y through a per-cell shared-memory tile.  Values at
+// the Gauss points come from the 1D interpolation matrix S (Gauss-Lobatto basis
+// at the Gauss points); gradients from the collocation derivative matrix Dc on
+// the Gauss points, which is exact for the interpolated polynomial.  The
+// quadrature-point kernels restate
+//   heat:    source/heat/heat_diffuse_operator.cpp:1029-1078 (tangent),
+//            :479-505 (residual), with the k(T) = k0 (1 + a T) law;
+//   advdiff: source/level_set/advection_diffusion_operator.cpp:471-493 (tangent),
+//            :318-353 (rhs).
+// Cells of one parity colour share no DoF; a launch per colour adds the cell
+// results into dst with plain loads and stores (atomic-free, deterministic).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "mpdg_internal.h"
+
+namespace mpdg {
+
+// ------------------------------------------------------------------ 1D tables
+
+template <typename Real>
+struct Tables {
+  Real S[kMaxN * kMaxN];   // S[q*n+i]  = phi_i(x_q): Gauss-Lobatto basis at Gauss points
+  Real D[kMaxN * kMaxN];   // D[q*n+i]  = phi_i'(x_q)
+  Real Dc[kMaxN * kMaxN];  // Dc[q*n+r] = l_r'(x_q): collocation derivative on Gauss points
+  Real w[kMaxN];           // Gauss weights on [0,1]
+  Real x[kMaxN];           // Gauss points on [0,1]
+};
+
+__constant__ Tables<double> c_tab64[kMaxDegree + 1];
+__constant__ Tables<float> c_tab32[kMaxDegree + 1];
+
+template <typename Real>
+__device__ __forceinline__ const Tables<Real> &tab(int p);
+template <>
+__device__ __forceinline__ const Tables<double> &tab<double>(int p) { return c_tab64[p]; }
+template <>
+__device__ __forceinline__ const Tables<float> &tab<float>(int p) { return c_tab32[p]; }
+
+namespace {
+
+void legendre(int n, double x, double &p, double &dp)
+{
+  double p0 = 1.0, p1 = x;
+  if (n == 0) { p = 1.0; dp = 0.0; return; }
+  for (int k = 2; k <= n; ++k) {
+    const double pk = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+    p0 = p1;
+    p1 = pk;
+  }
+  p = p1;
+  dp = n * (x * p1 - p0) / (x * x - 1.0);
+}
+
+// Gauss-Legendre points/weights on [0,1], ascending
+void gauss(int n, double *x, double *w)
+{
+  for (int i = 0; i < n; ++i) {
+    double z = std::cos(M_PI * (i + 0.75) / (n + 0.5)), p, dp;
+    for (int it = 0; it < 100; ++it) {
+      legendre(n, z, p, dp);
+      const double dz = p / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    legendre(n, z, p, dp);
+    x[n - 1 - i] = 0.5 * (1.0 + z);
+    w[n - 1 - i] = 1.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+// Gauss-Lobatto nodes on [0,1]: endpoints and roots of P'_{n-1}
+void lobatto(int n, double *x)
+{
+  const int m = n - 1;
+  x[0] = 0.0;
+  x[n - 1] = 1.0;
+  for (int i = 1; i < n - 1; ++i) {
+    double z = -std::cos(M_PI * i / m), p, dp;
+    for (int it = 0; it < 100; ++it) {
+      legendre(m, z, p, dp);
+      const double ddp = (2.0 * z * dp - m * (m + 1.0) * p) / (1.0 - z * z);
+      const double dz = dp / ddp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    x[i] = 0.5 * (1.0 + z);
+  }
+}
+
+// value and derivative at t of the Lagrange polynomial through nodes z, index i
+void lagrange(int n, const double *z, int i, double t, double &v, double &d)
+{
+  v = 1.0;
+  d = 0.0;
+  for (int j = 0; j < n; ++j)
+    if (j != i) v *= (t - z[j]) / (z[i] - z[j]);
+  for (int k = 0; k < n; ++k) {
+    if (k == i) continue;
+    double s = 1.0 / (z[i] - z[k]);
+    for (int j = 0; j < n; ++j)
+      if (j != i && j != k) s *= (t - z[j]) / (z[i] - z[j]);
+    d += s;
+  }
+}
+
+bool g_tables_ready = false;
+
+void upload_tables()
+{
+  if (g_tables_ready) return;
+  Tables<double> t64[kMaxDegree + 1];
+  Tables<float> t32[kMaxDegree + 1];
+  std::memset(t64, 0, sizeof(t64));
+  std::memset(t32, 0, sizeof(t32));
+  for (int p = 1; p <= kMaxDegree; ++p) {
+    const int n = p + 1;
+    double xq[kMaxN], wq[kMaxN], zl[kMaxN];
+    gauss(n, xq, wq);
+    lobatto(n, zl);
+    for (int q = 0; q < n; ++q) {
+      t64[p].w[q] = wq[q];
+      t64[p].x[q] = xq[q];
+      for (int i = 0; i < n; ++i) {
+        double v, d;
+        lagrange(n, zl, i, xq[q], v, d);
+        t64[p].S[q * n + i] = v;
+        t64[p].D[q * n + i] = d;
+        lagrange(n, xq, i, xq[q], v, d);
+        t64[p].Dc[q * n + i] = d;
+      }
+    }
+    for (int k = 0; k < kMaxN * kMaxN; ++k) {
+      t32[p].S[k] = (float)t64[p].S[k];
+      t32[p].D[k] = (float)t64[p].D[k];
+      t32[p].Dc[k] = (float)t64[p].Dc[k];
+    }
+    for (int k = 0; k < kMaxN; ++k) {
+      t32[p].w[k] = (float)t64[p].w[k];
+      t32[p].x[k] = (float)t64[p].x[k];
+    }
+  }
+  MPDG_CUDA(cudaMemcpyToSymbol(c_tab64, t64, sizeof(t64)));
+  MPDG_CUDA(cudaMemcpyToSymbol(c_tab32, t32, sizeof(t32)));
+  g_tables_ready = true;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ kernel params
+
+enum { MODE_LINEAR = 0, MODE_HEAT_RESIDUAL = 1 };
+enum { GEOM_UNIFORM = 0, GEOM_GENERAL = 1 };
+
+template <typename Real>
+struct KP {
+  const Real *src;        // LINEAR: operand (or phi_old for the advdiff rhs); RESIDUAL: T_old
+  Real *dst;
+  const Real *T;          // k(T) field (LINEAR) / current T (RESIDUAL)
+  const Real *q_src;      // RESIDUAL: nodal heat source (may be null)
+  const Real *metric;     // GENERAL: [cell][7][n^3] = JxW, G00 G01 G02 G11 G12 G22
+  const Real *velb;       // GENERAL + velocity: [cell][3][n^3] = JxW J^-1 u
+  const Real *trig;       // UNIFORM vortex: sin(pi x), cos(pi x), sin(pi y), cos(pi y)
+  const uint8_t *dmask;
+  const uint8_t *cell_flags;
+  long NX, NY;
+  int trig_stride;
+  int par[3], cn[3];
+  long ccount, cfirst;
+  Real h[3], origin[3];
+  Real c_mass, c_vel, c_diff, k_alpha;
+  int vel_kind;
+  Real vel_param[3];
+  int masked_read, masked_write, full_tangent;
+};
+
+template <int n>
+struct Cfg {
+  static constexpr int cpb = (n == 2) ? 32 : (n == 3) ? 14 : (n == 4) ? 8 : 5;
+};
+
+// ---------------------------------------------------- contraction helpers
+// tile layout: t[k*n*n + j*n + i]
+
+template <int n, typename Real, bool TR>
+__device__ __forceinline__ void cz(const Real *M, const Real (&in)[n], Real (&out)[n])
+{
+#pragma unroll
+  for (int q = 0; q < n; ++q) {
+    Real s = 0;
+#pragma unroll
+    for (int k = 0; k < n; ++k) s += (TR ? M[k * n + q] : M[q * n + k]) * in[k];
+    out[q] = s;
+  }
+}
+
+template <int n, typename Real, bool TR>
+__device__ __forceinline__ void cx(const Real *M, const Real *t, int i, int j, Real (&out)[n])
+{
+#pragma unroll
+  for (int k = 0; k < n; ++k) {
+    Real s = 0;
+#pragma unroll
+    for (int r = 0; r < n; ++r) s += (TR ? M[r * n + i] : M[i * n + r]) * t[k * n * n + j * n + r];
+    out[k] = s;
+  }
+}
+
+template <int n, typename Real, bool TR>
+__device__ __forceinline__ void cy(const Real *M, const Real *t, int i, int j, Real (&out)[n])
+{
+#pragma unroll
+  for (int k = 0; k < n; ++k) {
+    Real s = 0;
+#pragma unroll
+    for (int r = 0; r < n; ++r) s += (TR ? M[r * n + j] : M[j * n + r]) * t[k * n * n + r * n + i];
+    out[k] = s;
+  }
+}
+
+template <int n, typename Real>
+__device__ __forceinline__ void put(Real *t, int i, int j, const Real (&v)[n])
+{
+#pragma unroll
+  for (int k = 0; k < n; ++k) t[k * n * n + j * n + i] = v[k];
+}
+
+// nodal column -> values at the Gauss points (thread (i,j) ends with qp (i,j,*))
+template <int n, typename Real>
+__device__ __forceinline__ void to_qp(const Real *S, Real *t, int i, int j, const Real (&u)[n],
+                                      Real (&v)[n])
+{
+  Real a[n];
+  cz<n, Real, false>(S, u, a);
+  put<n>(t, i, j, a);
+  __syncthreads();
+  cy<n, Real, false>(S, t, i, j, v);
+  __syncthreads();
+  put<n>(t, i, j, v);
+  __syncthreads();
+  cx<n, Real, false>(S, t, i, j, a);
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < n; ++k) v[k] = a[k];
+}
+
+// values at the Gauss points -> reference gradients (collocation)
+template <int n, typename Real>
+__device__ __forceinline__ void grad_qp(const Real *Dc, Real *t, int i, int j, const Real (&v)[n],
+                                        Real (&gx)[n], Real (&gy)[n], Real (&gz)[n])
+{
+  put<n>(t, i, j, v);
+  __syncthreads();
+  cx<n, Real, false>(Dc, t, i, j, gx);
+  cy<n, Real, false>(Dc, t, i, j, gy);
+  cz<n, Real, false>(Dc, v, gz);
+  __syncthreads();
+}
+
+// test with (value, reference gradient) and return the nodal column
+template <int n, typename Real>
+__device__ __forceinline__ void from_qp(const Real *S, const Real *Dc, Real *t0, Real *t1, int i,
+                                        int j, const Real (&val)[n], const Real (&fx)[n],
+                                        const Real (&fy)[n], const Real (&fz)[n], Real (&out)[n])
+{
+  Real a[n], b[n];
+  put<n>(t0, i, j, fx);
+  put<n>(t1, i, j, fy);
+  __syncthreads();
+  cx<n, Real, true>(Dc, t0, i, j, a);
+  cy<n, Real, true>(Dc, t1, i, j, b);
+  cz<n, Real, true>(Dc, fz, out);
+#pragma unroll
+  for (int k = 0; k < n; ++k) a[k] += b[k] + out[k] + val[k];
+  __syncthreads();
+  put<n>(t0, i, j, a);
+  __syncthreads();
+  cx<n, Real, true>(S, t0, i, j, b);
+  __syncthreads();
+  put<n>(t0, i, j, b);
+  __syncthreads();
+  cy<n, Real, true>(S, t0, i, j, a);
+  cz<n, Real, true>(S, a, out);
+}
+
+template <typename Real, int n>
+__device__ __forceinline__ void uniform_velocity(const KP<Real> &p, const Tables<Real> &T, int ix,
+                                                 int iy, int iz, int i, int j, int k, Real u[3])
+{
+  if (p.vel_kind == MPDG_VEL_VORTEX) {
+    const Real sx = p.trig[ix * n + i], cxv = p.trig[p.trig_stride + ix * n + i];
+    const Real sy = p.trig[2 * p.trig_stride + iy * n + j],
+               cyv = p.trig[3 * p.trig_stride + iy * n + j];
+    u[0] = sx * cyv;
+    u[1] = -cxv * sy;
+    u[2] = 0;
+  } else if (p.vel_kind == MPDG_VEL_ROTATION) {
+    const Real x = p.origin[0] + (ix + T.x[i]) * p.h[0];
+    const Real z = p.origin[2] + (iz + T.x[k]) * p.h[2];
+    u[0] = p.vel_param[0] * z;
+    u[1] = 0;
+    u[2] = -p.vel_param[0] * x;
+  } else {
+    u[0] = p.vel_param[0];
+    u[1] = p.vel_param[1];
+    u[2] = p.vel_param[2];
+  }
+}
+
+// ------------------------------------------------------------ the cell kernel
+
+template <int P, typename Real, int GEOM, int MODE, bool KT>
+__global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
+{
+  constexpr int n = P + 1, n2 = n * n, n3 = n2 * n, CPB = Cfg<n>::cpb;
+  __shared__ Real sm[CPB][2][n3];
+  __shared__ Real sS[n2], sDc[n2];
+  const Tables<Real> &T = tab<Real>(P);
+  const int tid = threadIdx.x, slot = threadIdx.y;
+  const int i = tid % n, j = tid / n;
+  // 1D tables in shared memory: rows are indexed by the thread's i/j, which
+  // the constant cache would serialise
+  if (slot == 0) {
+    sS[tid] = T.S[tid];
+    sDc[tid] = T.Dc[tid];
+  }
+  __syncthreads();
+  const long cidx = (long)blockIdx.x * CPB + slot;
+  const bool active = cidx < p.ccount;
+  int ix = 0, iy = 0, iz = 0;
+  if (active) {
+    const long a = cidx % p.cn[0], b = (cidx / p.cn[0]) % p.cn[1], c = cidx / ((long)p.cn[0] * p.cn[1]);
+    ix = 2 * (int)a + p.par[0];
+    iy = 2 * (int)b + p.par[1];
+    iz = 2 * (int)c + p.par[2];
+  }
+  const long cell = p.cfirst + cidx;
+  const long zs = p.NX * p.NY;
+  const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
+  const bool bflag = active && p.cell_flags && (p.cell_flags[cell] & 1);
+  Real *t0 = sm[slot][0], *t1 = sm[slot][1];
+
+  Real u[n], uq[n], gx[n], gy[n], gz[n];
+#pragma unroll
+  for (int k = 0; k < n; ++k) {
+    Real v = 0;
+    if (active) {
+      v = p.src[g0 + k * zs];
+      if (MODE == MODE_LINEAR && p.masked_read && bflag && p.dmask[g0 + k * zs]) v = 0;
+    }
+    u[k] = v;
+  }
+
+  // temperature field at the Gauss points (k(T) law, Newton residual)
+  Real Tq[n], Tgx[n], Tgy[n], Tgz[n];
+  const bool needT = KT || MODE == MODE_HEAT_RESIDUAL;
+  if (needT) {
+    Real tl[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) tl[k] = active ? p.T[g0 + k * zs] : Real(0);
+    to_qp<n>(sS, t1, i, j, tl, Tq);
+    if (MODE == MODE_HEAT_RESIDUAL || p.full_tangent) grad_qp<n>(sDc, t1, i, j, Tq, Tgx, Tgy, Tgz);
+  }
+  Real oq[n], hq[n];
+  if (MODE == MODE_HEAT_RESIDUAL) {
+    // u holds T_old here; the residual is evaluated at T
+    to_qp<n>(sS, t0, i, j, u, oq);
+    Real ql[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) ql[k] = (active && p.q_src) ? p.q_src[g0 + k * zs] : Real(0);
+    to_qp<n>(sS, t0, i, j, ql, hq);
+#pragma unroll
+    for (int k = 0; k < n; ++k) {
+      uq[k] = Tq[k];
+      gx[k] = Tgx[k];
+      gy[k] = Tgy[k];
+      gz[k] = Tgz[k];
+    }
+  } else {
+    to_qp<n>(sS, t0, i, j, u, uq);
+    grad_qp<n>(sDc, t0, i, j, uq, gx, gy, gz);
+  }
+
+  // quadrature-point kernel
+  Real val[n], fx[n], fy[n], fz[n];
+#pragma unroll
+  for (int k = 0; k < n; ++k) {
+    Real JxW, G00, G01, G02, G11, G12, G22, b0 = 0, b1 = 0, b2 = 0;
+    if (GEOM == GEOM_GENERAL) {
+      const Real *m = p.metric + (cell * 7) * n3 + k * n2 + j * n + i;
+      if (active) {
+        JxW = m[0];
+        G00 = m[n3];
+        G01 = m[2 * n3];
+        G02 = m[3 * n3];
+        G11 = m[4 * n3];
+        G12 = m[5 * n3];
+        G22 = m[6 * n3];
+        if (p.vel_kind != MPDG_VEL_NONE) {
+          const Real *vb = p.velb + (cell * 3) * n3 + k * n2 + j * n + i;
+          b0 = vb[0];
+          b1 = vb[n3];
+          b2 = vb[2 * n3];
+        }
+      } else {
+        JxW = G00 = G11 = G22 = 1;
+        G01 = G02 = G12 = 0;
+      }
+    } else {
+      JxW = p.h[0] * p.h[1] * p.h[2] * T.w[i] * T.w[j] * T.w[k];
+      G00 = JxW / (p.h[0] * p.h[0]);
+      G11 = JxW / (p.h[1] * p.h[1]);
+      G22 = JxW / (p.h[2] * p.h[2]);
+      G01 = G02 = G12 = 0;
+      if (p.vel_kind != MPDG_VEL_NONE) {
+        Real uv[3];
+        uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, k, uv);
+        b0 = JxW * uv[0] / p.h[0];
+        b1 = JxW * uv[1] / p.h[1];
+        b2 = JxW * uv[2] / p.h[2];
+      }
+    }
+    Real kq = p.c_diff;
+    if (needT) kq = p.c_diff * (Real(1) + p.k_alpha * Tq[k]);
+    const Real adv = b0 * gx[k] + b1 * gy[k] + b2 * gz[k];
+    Real f0, f1, f2;
+    if (GEOM == GEOM_GENERAL) {
+      f0 = G00 * gx[k] + G01 * gy[k] + G02 * gz[k];
+      f1 = G01 * gx[k] + G11 * gy[k] + G12 * gz[k];
+      f2 = G02 * gx[k] + G12 * gy[k] + G22 * gz[k];
+    } else {
+      f0 = G00 * gx[k];
+      f1 = G11 * gy[k];
+      f2 = G22 * gz[k];
+    }
+    if (MODE == MODE_HEAT_RESIDUAL) {
+      // -( rho_cp/dt (T - T_old) - q + rho_cp vel.grad T ) N - k(T) grad T . grad N
+      val[k] = -(p.c_mass * JxW * (uq[k] - oq[k]) - JxW * hq[k] + p.c_vel * adv);
+      fx[k] = -kq * f0;
+      fy[k] = -kq * f1;
+      fz[k] = -kq * f2;
+    } else {
+      val[k] = p.c_mass * JxW * uq[k] + p.c_vel * adv;
+      fx[k] = kq * f0;
+      fy[k] = kq * f1;
+      fz[k] = kq * f2;
+      if (KT && p.full_tangent) {
+        // dk/dT grad T du, tested with grad N: G (reference grad T) scaled by u
+        const Real dk = p.c_diff * p.k_alpha * uq[k];
+        if (GEOM == GEOM_GENERAL) {
+          fx[k] += dk * (G00 * Tgx[k] + G01 * Tgy[k] + G02 * Tgz[k]);
+          fy[k] += dk * (G01 * Tgx[k] + G11 * Tgy[k] + G12 * Tgz[k]);
+          fz[k] += dk * (G02 * Tgx[k] + G12 * Tgy[k] + G22 * Tgz[k]);
+        } else {
+          fx[k] += dk * G00 * Tgx[k];
+          fy[k] += dk * G11 * Tgy[k];
+          fz[k] += dk * G22 * Tgz[k];
+        }
+      }
+    }
+  }
+
+  Real out[n];
+  from_qp<n>(sS, sDc, t0, t1, i, j, val, fx, fy, fz, out);
+
+  if (active) {
+#pragma unroll
+    for (int k = 0; k < n; ++k) {
+      const long g = g0 + k * zs;
+      if (p.masked_write && bflag && p.dmask[g]) continue;
+      p.dst[g] += out[k];
+    }
+  }
+}
+
+// --------------------------------------------------------- diagonal kernel
+// diag_i = sum_q F_t(q) A_x[qx][ix] A_y[qy][iy] A_z[qz][iz] over the terms t of
+// the element matrix diagonal (mass, the six G components, the three velocity
+// components), each a product of squared/mixed 1D tables: the same entries
+// MatrixFreeTools::compute_diagonal extracts by unit-vector sweeps.
+
+template <int n, typename Real>
+__device__ __forceinline__ void diag_term(Real *t, int i, int j, const Real (&F)[n],
+                                          const Real *Ax, const Real *Ay, const Real *Az,
+                                          Real (&acc)[n])
+{
+  Real a[n], b[n];
+  cz<n, Real, true>(Az, F, a);
+  put<n>(t, i, j, a);
+  __syncthreads();
+  cy<n, Real, true>(Ay, t, i, j, b);
+  __syncthreads();
+  put<n>(t, i, j, b);
+  __syncthreads();
+  cx<n, Real, true>(Ax, t, i, j, a);
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < n; ++k) acc[k] += a[k];
+}
+
+template <int P, int GEOM, bool KT>
+__global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
+{
+  using Real = double;
+  constexpr int n = P + 1, n2 = n * n, n3 = n2 * n, CPB = Cfg<n>::cpb;
+  __shared__ Real sm[CPB][n3];
+  __shared__ Real tb[5][n2];  // S^2, D^2, S*D, S, Dc
+  const Tables<Real> &T = tab<Real>(P);
+  const int tid = threadIdx.x, slot = threadIdx.y;
+  const int lin = slot * blockDim.x + tid;
+  if (lin < n2) {
+    const Real s = T.S[lin], d = T.D[lin];
+    tb[0][lin] = s * s;
+    tb[1][lin] = d * d;
+    tb[2][lin] = s * d;
+    tb[3][lin] = s;
+    tb[4][lin] = T.Dc[lin];
+  }
+  __syncthreads();
+  const Real *SS = tb[0], *DD = tb[1], *SD = tb[2];
+  const int i = tid % n, j = tid / n;
+  const long cidx = (long)blockIdx.x * CPB + slot;
+  const bool active = cidx < p.ccount;
+  int ix = 0, iy = 0, iz = 0;
+  if (active) {
+    const long a = cidx % p.cn[0], b = (cidx / p.cn[0]) % p.cn[1], c = cidx / ((long)p.cn[0] * p.cn[1]);
+    ix = 2 * (int)a + p.par[0];
+    iy = 2 * (int)b + p.par[1];
+    iz = 2 * (int)c + p.par[2];
+  }
+  const long cell = p.cfirst + cidx;
+  const long zs = p.NX * p.NY;
+  const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
+  const bool bflag = active && p.cell_flags && (p.cell_flags[cell] & 1);
+  Real *t = sm[slot];
+
+  Real Tq[n], Tgx[n], Tgy[n], Tgz[n];
+  if (KT) {
+    Real tl[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) tl[k] = active ? p.T[g0 + k * zs] : Real(0);
+    to_qp<n>(tb[3], t, i, j, tl, Tq);
+    if (p.full_tangent) grad_qp<n>(tb[4], t, i, j, Tq, Tgx, Tgy, Tgz);
+  }
+  Real Fm[n], F00[n], F11[n], F22[n], F01[n], F02[n], F12[n], Fb0[n], Fb1[n], Fb2[n];
+#pragma unroll
+  for (int k = 0; k < n; ++k) {
+    Real JxW, G00, G01, G02, G11, G12, G22, b0 = 0, b1 = 0, b2 = 0;
+    if (GEOM == GEOM_GENERAL) {
+      const Real *m = p.metric + (cell * 7) * n3 + k * n2 + j * n + i;
+      JxW = active ? m[0] : 0;
+      G00 = active ? m[n3] : 0;
+      G01 = active ? m[2 * n3] : 0;
+      G02 = active ? m[3 * n3] : 0;
+      G11 = active ? m[4 * n3] : 0;
+      G12 = active ? m[5 * n3] : 0;
+      G22 = active ? m[6 * n3] : 0;
+      if (p.vel_kind != MPDG_VEL_NONE && active) {
+        const Real *vb = p.velb + (cell * 3) * n3 + k * n2 + j * n + i;
+        b0 = vb[0];
+        b1 = vb[n3];
+        b2 = vb[2 * n3];
+      }
+    } else {
+      JxW = p.h[0] * p.h[1] * p.h[2] * T.w[i] * T.w[j] * T.w[k];
+      G00 = JxW / (p.h[0] * p.h[0]);
+      G11 = JxW / (p.h[1] * p.h[1]);
+      G22 = JxW / (p.h[2] * p.h[2]);
+      G01 = G02 = G12 = 0;
+      if (p.vel_kind != MPDG_VEL_NONE) {
+        Real uv[3];
+        uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, k, uv);
+        b0 = JxW * uv[0] / p.h[0];
+        b1 = JxW * uv[1] / p.h[1];
+        b2 = JxW * uv[2] / p.h[2];
+      }
+    }
+    Real kq = p.c_diff;
+    if (KT) kq = p.c_diff * (Real(1) + p.k_alpha * Tq[k]);
+    Fm[k] = p.c_mass * JxW;
+    F00[k] = kq * G00;
+    F11[k] = kq * G11;
+    F22[k] = kq * G22;
+    F01[k] = 2 * kq * G01;
+    F02[k] = 2 * kq * G02;
+    F12[k] = 2 * kq * G12;
+    // velocity term phi_i (b . grad phi_i), plus the full-tangent term
+    // grad phi_i . (dk G gradT) phi_i, which has the same table structure
+    Real e0 = p.c_vel * b0, e1 = p.c_vel * b1, e2 = p.c_vel * b2;
+    if (KT && p.full_tangent) {
+      const Real dk = p.c_diff * p.k_alpha;
+      e0 += dk * (G00 * Tgx[k] + G01 * Tgy[k] + G02 * Tgz[k]);
+      e1 += dk * (G01 * Tgx[k] + G11 * Tgy[k] + G12 * Tgz[k]);
+      e2 += dk * (G02 * Tgx[k] + G12 * Tgy[k] + G22 * Tgz[k]);
+    }
+    Fb0[k] = e0;
+    Fb1[k] = e1;
+    Fb2[k] = e2;
+  }
+  Real acc[n];
+#pragma unroll
+  for (int k = 0; k < n; ++k) acc[k] = 0;
+  diag_term<n>(t, i, j, Fm, SS, SS, SS, acc);
+  diag_term<n>(t, i, j, F00, DD, SS, SS, acc);
+  diag_term<n>(t, i, j, F11, SS, DD, SS, acc);
+  diag_term<n>(t, i, j, F22, SS, SS, DD, acc);
+  diag_term<n>(t, i, j, Fb0, SD, SS, SS, acc);
+  diag_term<n>(t, i, j, Fb1, SS, SD, SS, acc);
+  diag_term<n>(t, i, j, Fb2, SS, SS, SD, acc);
+  if (GEOM == GEOM_GENERAL) {
+    diag_term<n>(t, i, j, F01, SD, SD, SS, acc);
+    diag_term<n>(t, i, j, F02, SD, SS, SD, acc);
+    diag_term<n>(t, i, j, F12, SS, SD, SD, acc);
+  }
+  if (active) {
+#pragma unroll
+    for (int k = 0; k < n; ++k) {
+      const long g = g0 + k * zs;
+      if (p.masked_write && bflag && p.dmask[g]) continue;
+      p.dst[g] += acc[k];
+    }
+  }
+}
+
+// ------------------------------------------------------ geometry kernels
+
+// per (cell, qp): JxW and G = JxW J^-1 J^-T of the trilinear map, colour-major
+__global__ void metric_kernel(const double *vert, int nc0, int nc1, int nc2, int P,
+                              const Colour *colours, double *metric, float *metric32,
+                              const double *xq_all, const double *wq_all)
+{
+  const int n = P + 1, n3 = n * n * n;
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long n_cells = (long)nc0 * nc1 * nc2;
+  if (gid >= n_cells * n3) return;
+  const long cell = gid / n3;
+  const int q = (int)(gid % n3);
+  int c = 0;
+  while (c < 7 && cell >= colours[c + 1].first) ++c;
+  const Colour &C = colours[c];
+  const long cidx = cell - C.first;
+  const int ix = 2 * (int)(cidx % C.cn[0]) + C.par[0];
+  const int iy = 2 * (int)((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
+  const int iz = 2 * (int)(cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
+  const int qi = q % n, qj = (q / n) % n, qk = q / (n * n);
+  const double xi[3] = {xq_all[qi], xq_all[qj], xq_all[qk]};
+  const double w = wq_all[qi] * wq_all[qj] * wq_all[qk];
+  double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int v = 0; v < 8; ++v) {
+    const int bx = v & 1, by = (v >> 1) & 1, bz = (v >> 2) & 1;
+    const long vid = ((long)(iz + bz) * (nc1 + 1) + (iy + by)) * (nc0 + 1) + (ix + bx);
+    const double f[3] = {bx ? xi[0] : 1 - xi[0], by ? xi[1] : 1 - xi[1], bz ? xi[2] : 1 - xi[2]};
+    const double df[3] = {bx ? 1.0 : -1.0, by ? 1.0 : -1.0, bz ? 1.0 : -1.0};
+    const double dB[3] = {df[0] * f[1] * f[2], f[0] * df[1] * f[2], f[0] * f[1] * df[2]};
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) J[a][b] += vert[vid * 3 + a] * dB[b];
+  }
+  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                     J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  const double id = 1.0 / det;
+  double Ji[3][3];
+  Ji[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) * id;
+  Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+  Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+  Ji[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) * id;
+  Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+  Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+  Ji[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) * id;
+  Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+  Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  const double JxW = det * w;
+  double G[6];
+  const int ab[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  for (int e = 0; e < 6; ++e) {
+    double s = 0;
+    for (int c2 = 0; c2 < 3; ++c2) s += Ji[ab[e][0]][c2] * Ji[ab[e][1]][c2];
+    G[e] = JxW * s;
+  }
+  double *m = metric + cell * 7 * n3 + q;
+  m[0] = JxW;
+  for (int e = 0; e < 6; ++e) m[(e + 1) * n3] = G[e];
+  if (metric32) {
+    float *m32 = metric32 + cell * 7 * n3 + q;
+    m32[0] = (float)JxW;
+    for (int e = 0; e < 6; ++e) m32[(e + 1) * n3] = (float)G[e];
+  }
+}
+
+// per (cell, qp): b = JxW J^-1 u(x_q) for a prescribed velocity on a general mesh
+__global__ void velb_kernel(const double *vert, int nc0, int nc1, int nc2, int P,
+                            const Colour *colours, int vel_kind, double s0, double s1, double s2,
+                            double *velb, float *velb32, const double *xq_all,
+                            const double *wq_all)
+{
+  const int n = P + 1, n3 = n * n * n;
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long n_cells = (long)nc0 * nc1 * nc2;
+  if (gid >= n_cells * n3) return;
+  const long cell = gid / n3;
+  const int q = (int)(gid % n3);
+  int c = 0;
+  while (c < 7 && cell >= colours[c + 1].first) ++c;
+  const Colour &C = colours[c];
+  const long cidx = cell - C.first;
+  const int ix = 2 * (int)(cidx % C.cn[0]) + C.par[0];
+  const int iy = 2 * (int)((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
+  const int iz = 2 * (int)(cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
+  const int qi = q % n, qj = (q / n) % n, qk = q / (n * n);
+  const double xi[3] = {xq_all[qi], xq_all[qj], xq_all[qk]};
+  const double w = wq_all[qi] * wq_all[qj] * wq_all[qk];
+  double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, x[3] = {0, 0, 0};
+  for (int v = 0; v < 8; ++v) {
+    const int bx = v & 1, by = (v >> 1) & 1, bz = (v >> 2) & 1;
+    const long vid = ((long)(iz + bz) * (nc1 + 1) + (iy + by)) * (nc0 + 1) + (ix + bx);
+    const double f[3] = {bx ? xi[0] : 1 - xi[0], by ? xi[1] : 1 - xi[1], bz ? xi[2] : 1 - xi[2]};
+    const double df[3] = {bx ? 1.0 : -1.0, by ? 1.0 : -1.0, bz ? 1.0 : -1.0};
+    const double dB[3] = {df[0] * f[1] * f[2], f[0] * df[1] * f[2], f[0] * f[1] * df[2]};
+    const double B = f[0] * f[1] * f[2];
+    for (int a = 0; a < 3; ++a) {
+      x[a] += vert[vid * 3 + a] * B;
+      for (int b = 0; b < 3; ++b) J[a][b] += vert[vid * 3 + a] * dB[b];
+    }
+  }
+  double u[3] = {0, 0, 0};
+  if (vel_kind == MPDG_VEL_VORTEX) {
+    u[0] = sin(M_PI * x[0]) * cos(M_PI * x[1]);
+    u[1] = -cos(M_PI * x[0]) * sin(M_PI * x[1]);
+  } else if (vel_kind == MPDG_VEL_ROTATION) {
+    u[0] = s0 * x[2];
+    u[2] = -s0 * x[0];
+  } else {
+    u[0] = s0;
+    u[1] = s1;
+    u[2] = s2;
+  }
+  // JxW J^-1 = w adj(J)
+  double A[3][3];
+  A[0][0] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  A[0][1] = J[0][2] * J[2][1] - J[0][1] * J[2][2];
+  A[0][2] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+  A[1][0] = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  A[1][1] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+  A[1][2] = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+  A[2][0] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  A[2][1] = J[0][1] * J[2][0] - J[0][0] * J[2][1];
+  A[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+  for (int a = 0; a < 3; ++a) {
+    const double b = w * (A[a][0] * u[0] + A[a][1] * u[1] + A[a][2] * u[2]);
+    velb[cell * 3 * n3 + a * n3 + q] = b;
+    if (velb32) velb32[cell * 3 * n3 + a * n3 + q] = (float)b;
+  }
+}
+
+__global__ void cast_kernel(const double *a, float *b, long n)
+{
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+// inverse diagonal with the reference's thresholds; constrained entries -> 1
+__global__ void invert_kernel(double *d, long n, const uint8_t *mask, double thr)
+{
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (mask && mask[i]) {
+    d[i] = 1.0;
+    return;
+  }
+  const double v = d[i];
+  d[i] = (fabs(v) > thr) ? 1.0 / v : 1.0;
+}
+
+__global__ void set_masked_kernel(double *d, long n, const uint8_t *mask, double value)
+{
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && mask[i]) d[i] = value;
+}
+
+// ------------------------------------------------------------- host side
+
+namespace {
+
+void colour_layout(Mesh &m)
+{
+  long first = 0;
+  for (int c = 0; c < 8; ++c) {
+    Colour &C = m.colour[c];
+    C.par[0] = c & 1;
+    C.par[1] = (c >> 1) & 1;
+    C.par[2] = (c >> 2) & 1;
+    for (int d = 0; d < 3; ++d) C.cn[d] = (m.nc[d] - C.par[d] + 1) / 2;
+    C.count = (long)C.cn[0] * C.cn[1] * C.cn[2];
+    C.first = first;
+    first += C.count;
+  }
+}
+
+template <typename T>
+T *dev_alloc(size_t count, size_t &bytes)
+{
+  T *p = nullptr;
+  if (count == 0) return nullptr;
+  cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  if (e != cudaSuccess) throw Error{MPDG_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+  bytes += count * sizeof(T);
+  return p;
+}
+
+unsigned grid_for(long n, int block) { return (unsigned)((n + block - 1) / block); }
+
+}  // namespace
+
+void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_general)
+{
+  upload_tables();
+  colour_layout(m);
+  const int p = m.degree, n = p + 1, n3 = n * n * n;
+  // uniform axis-aligned box detection
+  const int nv0 = m.nc[0] + 1, nv1 = m.nc[1] + 1, nv2 = m.nc[2] + 1;
+  const double *V = m.vertices.data();
+  for (int d = 0; d < 3; ++d) {
+    m.origin[d] = V[d];
+    const long last = (d == 0) ? (nv0 - 1) : (d == 1) ? (long)(nv1 - 1) * nv0 : (long)(nv2 - 1) * nv0 * nv1;
+    m.h[d] = (V[last * 3 + d] - V[d]) / m.nc[d];
+  }
+  bool uniform = !force_general;
+  double scale = 0.0;
+  for (int d = 0; d < 3; ++d) scale = std::fmax(scale, std::fabs(m.h[d]) * m.nc[d]);
+  for (long v = 0; uniform && v < (long)nv0 * nv1 * nv2; ++v) {
+    const long c[3] = {v % nv0, (v / nv0) % nv1, v / ((long)nv0 * nv1)};
+    for (int d = 0; d < 3; ++d)
+      if (std::fabs(V[v * 3 + d] - (m.origin[d] + c[d] * m.h[d])) > 1e-14 * scale) {
+        uniform = false;
+        break;
+      }
+  }
+  m.uniform = uniform;
+
+  m.d_vert = dev_alloc<double>(m.vertices.size(), m.device_bytes);
+  MPDG_CUDA(cudaMemcpy(m.d_vert, V, m.vertices.size() * sizeof(double), cudaMemcpyHostToDevice));
+
+  if (!uniform) {
+    Colour *d_col = nullptr;
+    MPDG_CUDA(cudaMalloc(&d_col, sizeof(m.colour)));
+    MPDG_CUDA(cudaMemcpy(d_col, m.colour, sizeof(m.colour), cudaMemcpyHostToDevice));
+    double *d_xw = nullptr;
+    double xw[2 * kMaxN];
+    {
+      double xq[kMaxN], wq[kMaxN];
+      gauss(n, xq, wq);
+      for (int q = 0; q < n; ++q) {
+        xw[q] = xq[q];
+        xw[kMaxN + q] = wq[q];
+      }
+    }
+    MPDG_CUDA(cudaMalloc(&d_xw, sizeof(xw)));
+    MPDG_CUDA(cudaMemcpy(d_xw, xw, sizeof(xw), cudaMemcpyHostToDevice));
+    m.d_metric64 = dev_alloc<double>((size_t)m.n_cells * 7 * n3, m.device_bytes);
+    const long total = m.n_cells * n3;
+    metric_kernel<<<grid_for(total, 256), 256>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col,
+                                                 m.d_metric64, nullptr, d_xw, d_xw + kMaxN);
+    MPDG_LAUNCHED();
+    MPDG_CUDA(cudaDeviceSynchronize());
+    cudaFree(d_col);
+    cudaFree(d_xw);
+  }
+
+  // Dirichlet mask and per-cell flags
+  if (host_mask) {
+    std::vector<uint8_t> flags(m.n_cells, 0);
+    bool any = false;
+    for (int c = 0; c < 8; ++c) {
+      const Colour &C = m.colour[c];
+      for (long k = 0; k < C.count; ++k) {
+        const int ix = 2 * (int)(k % C.cn[0]) + C.par[0];
+        const int iy = 2 * (int)((k / C.cn[0]) % C.cn[1]) + C.par[1];
+        const int iz = 2 * (int)(k / ((long)C.cn[0] * C.cn[1])) + C.par[2];
+        uint8_t f = 0;
+        for (int kk = 0; kk <= p && !f; ++kk)
+          for (int jj = 0; jj <= p && !f; ++jj)
+            for (int ii = 0; ii <= p && !f; ++ii) {
+              const long g = ((long)(iz * p + kk) * m.NY + (iy * p + jj)) * m.NX + (ix * p + ii);
+              if (host_mask[g]) f = 1;
+            }
+        flags[C.first + k] = f;
+        any = any || f;
+      }
+    }
+    m.has_dirichlet = any;
+    if (any) {
+      m.d_dmask = dev_alloc<uint8_t>(m.N, m.device_bytes);
+      MPDG_CUDA(cudaMemcpy(m.d_dmask, host_mask, m.N, cudaMemcpyHostToDevice));
+      m.d_cell_flags = dev_alloc<uint8_t>(m.n_cells, m.device_bytes);
+      MPDG_CUDA(cudaMemcpy(m.d_cell_flags, flags.data(), m.n_cells, cudaMemcpyHostToDevice));
+    }
+  }
+}
+
+void ensure_metric32(Mesh &m, cudaStream_t s)
+{
+  if (m.uniform || m.metric32_ready) return;
+  const int n = m.degree + 1, n3 = n * n * n;
+  const long total = m.n_cells * 7 * n3;
+  m.d_metric32 = dev_alloc<float>(total, m.device_bytes);
+  cast_kernel<<<grid_for(total, 256), 256, 0, s>>>(m.d_metric64, m.d_metric32, total);
+  MPDG_LAUNCHED();
+  m.metric32_ready = true;
+}
+
+void build_op_device_data(Op &op)
+{
+  Mesh &m = *op.mesh;
+  const int p = m.degree, n = p + 1, n3 = n * n * n;
+  const bool want32 = (op.d.precision_mask & (1 << MPDG_FP32)) != 0;
+  if (want32) ensure_metric32(m, op.stream);
+  if (op.d.vel_kind == MPDG_VEL_NONE) return;
+  if (!m.uniform) {
+    Colour *d_col = nullptr;
+    MPDG_CUDA(cudaMalloc(&d_col, sizeof(m.colour)));
+    MPDG_CUDA(cudaMemcpy(d_col, m.colour, sizeof(m.colour), cudaMemcpyHostToDevice));
+    double xw[2 * kMaxN], xq[kMaxN], wq[kMaxN];
+    gauss(n, xq, wq);
+    for (int q = 0; q < n; ++q) {
+      xw[q] = xq[q];
+      xw[kMaxN + q] = wq[q];
+    }
+    double *d_xw = nullptr;
+    MPDG_CUDA(cudaMalloc(&d_xw, sizeof(xw)));
+    MPDG_CUDA(cudaMemcpy(d_xw, xw, sizeof(xw), cudaMemcpyHostToDevice));
+    const long total = m.n_cells * n3;
+    op.d_velb64 = dev_alloc<double>((size_t)m.n_cells * 3 * n3, op.device_bytes);
+    if (want32) op.d_velb32 = dev_alloc<float>((size_t)m.n_cells * 3 * n3, op.device_bytes);
+    velb_kernel<<<grid_for(total, 256), 256>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col,
+                                               op.d.vel_kind, op.d.vel_param[0], op.d.vel_param[1],
+                                               op.d.vel_param[2], op.d_velb64, op.d_velb32, d_xw,
+                                               d_xw + kMaxN);
+    MPDG_LAUNCHED();
+    MPDG_CUDA(cudaDeviceSynchronize());
+    cudaFree(d_col);
+    cudaFree(d_xw);
+  } else if (op.d.vel_kind == MPDG_VEL_VORTEX) {
+    // separable velocity: sin/cos of pi x at every Gauss point position per axis
+    double xq[kMaxN], wq[kMaxN];
+    gauss(n, xq, wq);
+    const int stride = std::max(m.nc[0], m.nc[1]) * n;
+    std::vector<double> t(4 * (size_t)stride, 0.0);
+    for (int c = 0; c < m.nc[0]; ++c)
+      for (int q = 0; q < n; ++q) {
+        const double x = m.origin[0] + (c + xq[q]) * m.h[0];
+        t[c * n + q] = std::sin(M_PI * x);
+        t[stride + c * n + q] = std::cos(M_PI * x);
+      }
+    for (int c = 0; c < m.nc[1]; ++c)
+      for (int q = 0; q < n; ++q) {
+        const double y = m.origin[1] + (c + xq[q]) * m.h[1];
+        t[2 * stride + c * n + q] = std::sin(M_PI * y);
+        t[3 * stride + c * n + q] = std::cos(M_PI * y);
+      }
+    op.d_trig64 = dev_alloc<double>(t.size(), op.device_bytes);
+    MPDG_CUDA(cudaMemcpy(op.d_trig64, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<float> t32(t.begin(), t.end());
+    op.d_trig32 = dev_alloc<float>(t.size(), op.device_bytes);
+    MPDG_CUDA(cudaMemcpy(op.d_trig32, t32.data(), t32.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+}
+
+void ensure_T32(Op &op)
+{
+  if (!op.T64) return;
+  const long N = op.mesh->N;
+  if (!op.T32) op.T32 = dev_alloc<float>(N, op.device_bytes);
+  cast_kernel<<<grid_for(N, 256), 256, 0, op.stream>>>(op.T64, op.T32, N);
+  MPDG_LAUNCHED();
+}
+
+namespace {
+
+template <typename Real>
+KP<Real> base_params(Op &op)
+{
+  Mesh &m = *op.mesh;
+  KP<Real> k{};
+  k.NX = m.NX;
+  k.NY = m.NY;
+  for (int d = 0; d < 3; ++d) {
+    k.h[d] = (Real)m.h[d];
+    k.origin[d] = (Real)m.origin[d];
+    k.vel_param[d] = (Real)op.d.vel_param[d];
+  }
+  k.vel_kind = op.d.vel_kind;
+  if constexpr (sizeof(Real) == 8) {
+    k.metric = m.d_metric64;
+    k.velb = op.d_velb64;
+    k.trig = op.d_trig64;
+    k.T = op.T64;
+  } else {
+    k.metric = m.d_metric32;
+    k.velb = op.d_velb32;
+    k.trig = op.d_trig32;
+    k.T = op.T32;
+  }
+  k.trig_stride = std::max(m.nc[0], m.nc[1]) * m.n;
+  k.dmask = m.d_dmask;
+  k.cell_flags = m.d_cell_flags;
+  const bool heat = op.d.kind == MPDG_OP_HEAT;
+  k.c_mass = (Real)(heat ? op.d.rho_cp / op.d.dt : 1.0 / op.d.dt);
+  k.c_vel = (Real)(heat ? op.d.rho_cp : op.d.theta);
+  k.c_diff = (Real)(heat ? op.d.k0 : op.d.theta * op.d.diffusivity);
+  k.k_alpha = (Real)(heat ? op.d.k_alpha : 0.0);
+  k.full_tangent = heat && op.d.full_tangent;
+  const bool mask = op.use_dirichlet && m.has_dirichlet;
+  k.masked_read = mask;
+  k.masked_write = mask;
+  return k;
+}
+
+template <typename Real>
+void colour_params(KP<Real> &k, const Colour &C)
+{
+  for (int d = 0; d < 3; ++d) {
+    k.par[d] = C.par[d];
+    k.cn[d] = C.cn[d];
+  }
+  k.ccount = C.count;
+  k.cfirst = C.first;
+}
+
+template <int P, typename Real, int MODE, bool KT>
+void run_cells(Op &op, KP<Real> k)
+{
+  Mesh &m = *op.mesh;
+  constexpr int n = P + 1, CPB = Cfg<n>::cpb;
+  const dim3 block(n * n, CPB);
+  for (int c = 0; c < 8; ++c) {
+    const Colour &C = m.colour[c];
+    if (C.count == 0) continue;
+    colour_params(k, C);
+    const unsigned grid = (unsigned)((C.count + CPB - 1) / CPB);
+    if (m.uniform)
+      cell_kernel<P, Real, GEOM_UNIFORM, MODE, KT><<<grid, block, 0, op.stream>>>(k);
+    else
+      cell_kernel<P, Real, GEOM_GENERAL, MODE, KT><<<grid, block, 0, op.stream>>>(k);
+    MPDG_LAUNCHED();
+  }
+}
+
+template <typename Real, int MODE, bool KT>
+void dispatch_degree(Op &op, const KP<Real> &k)
+{
+  switch (op.mesh->degree) {
+    case 1: run_cells<1, Real, MODE, KT>(op, k); break;
+    case 2: run_cells<2, Real, MODE, KT>(op, k); break;
+    case 3: run_cells<3, Real, MODE, KT>(op, k); break;
+    case 4: run_cells<4, Real, MODE, KT>(op, k); break;
+    default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+  }
+}
+
+bool uses_kT(const Op &op)
+{
+  return op.d.kind == MPDG_OP_HEAT && (op.d.k_alpha != 0.0 || op.d.full_tangent);
+}
+
+}  // namespace
+
+template <typename Real>
+void launch_apply(Op &op, Real *dst, const Real *src)
+{
+  Mesh &m = *op.mesh;
+  if (!m.uniform && sizeof(Real) == 4) ensure_metric32(m, op.stream);
+  KP<Real> k = base_params<Real>(op);
+  k.src = src;
+  k.dst = dst;
+  const bool kt = uses_kT(op);
+  if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
+  MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * m.N, op.stream));
+  if (kt) dispatch_degree<Real, MODE_LINEAR, true>(op, k);
+  else dispatch_degree<Real, MODE_LINEAR, false>(op, k);
+}
+
+template void launch_apply<double>(Op &, double *, const double *);
+template void launch_apply<float>(Op &, float *, const float *);
+
+void launch_rhs(Op &op, double *dst, const double *src, const double *heat_source)
+{
+  KP<double> k = base_params<double>(op);
+  k.src = src;
+  k.dst = dst;
+  k.masked_read = 0;  // read_dof_values_plain
+  if (op.d.kind == MPDG_OP_HEAT) {
+    if (!op.T64) throw Error{MPDG_ERR_ARG, "heat residual needs the temperature field"};
+    k.q_src = heat_source;
+    dispatch_degree<double, MODE_HEAT_RESIDUAL, false>(op, k);
+  } else {
+    if (heat_source) throw Error{MPDG_ERR_ARG, "advection-diffusion rhs takes no heat source"};
+    // phi_old/dt N - (1-theta) vel.grad phi_old N - (1-theta) D grad phi_old . grad N
+    k.c_mass = 1.0 / op.d.dt;
+    k.c_vel = -(1.0 - op.d.theta);
+    k.c_diff = -(1.0 - op.d.theta) * op.d.diffusivity;
+    k.k_alpha = 0.0;
+    k.full_tangent = 0;
+    dispatch_degree<double, MODE_LINEAR, false>(op, k);
+  }
+}
+
+namespace {
+template <int P, bool KT>
+void run_diag(Op &op, KP<double> k)
+{
+  Mesh &m = *op.mesh;
+  constexpr int n = P + 1, CPB = Cfg<n>::cpb;
+  const dim3 block(n * n, CPB);
+  for (int c = 0; c < 8; ++c) {
+    const Colour &C = m.colour[c];
+    if (C.count == 0) continue;
+    colour_params(k, C);
+    const unsigned grid = (unsigned)((C.count + CPB - 1) / CPB);
+    if (m.uniform) diag_kernel<P, GEOM_UNIFORM, KT><<<grid, block, 0, op.stream>>>(k);
+    else diag_kernel<P, GEOM_GENERAL, KT><<<grid, block, 0, op.stream>>>(k);
+    MPDG_LAUNCHED();
+  }
+}
+}  // namespace
+
+void launch_diagonal(Op &op, double *diag)
+{
+  Mesh &m = *op.mesh;
+  KP<double> k = base_params<double>(op);
+  k.dst = diag;
+  const bool kt = uses_kT(op);
+  if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
+  MPDG_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * m.N, op.stream));
+  switch (m.degree) {
+    case 1: kt ? run_diag<1, true>(op, k) : run_diag<1, false>(op, k); break;
+    case 2: kt ? run_diag<2, true>(op, k) : run_diag<2, false>(op, k); break;
+    case 3: kt ? run_diag<3, true>(op, k) : run_diag<3, false>(op, k); break;
+    case 4: kt ? run_diag<4, true>(op, k) : run_diag<4, false>(op, k); break;
+    default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+  }
+  if (op.use_dirichlet && m.has_dirichlet) {
+    set_masked_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, m.d_dmask, 1.0);
+    MPDG_LAUNCHED();
+  }
+}
+
+void launch_invert_diagonal(Op &op, double *diag)
+{
+  Mesh &m = *op.mesh;
+  double thr = 1e-10;  // heat_diffuse_operator.cpp:283
+  if (op.d.kind == MPDG_OP_ADVDIFF) {
+    // advection_diffusion_operator.cpp:436-439
+    thr = 1e-14 * std::fmax(1.0, linf(diag, m.N, op.stream));
+  }
+  const uint8_t *mask = (op.use_dirichlet && m.has_dirichlet) ? m.d_dmask : nullptr;
+  invert_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, mask, thr);
+  MPDG_LAUNCHED();
+}
+
+}  // namespace mpdg
+
+namespace mpdg {
+
+// per-cell integrated L2 norm squared (one thread per cell), summed per block
+template <int P>
+__global__ void l2_cells_kernel(const double *u, long NX, long NY, int nc0, int nc1, long n_cells,
+                                const Colour *colours, const double *metric, double hx, double hy,
+                                double hz, double *partial)
+{
+  constexpr int n = P + 1, n3 = n * n * n;
+  const Tables<double> &T = tab<double>(P);
+  double s = 0.0;
+  for (long cell = (long)blockIdx.x * blockDim.x + threadIdx.x; cell < n_cells;
+       cell += (long)gridDim.x * blockDim.x) {
+    int c = 0;
+    while (c < 7 && cell >= colours[c + 1].first) ++c;
+    const Colour &C = colours[c];
+    const long cidx = cell - C.first;
+    const int ix = 2 * (int)(cidx % C.cn[0]) + C.par[0];
+    const int iy = 2 * (int)((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
+    const int iz = 2 * (int)(cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
+    double a[n3], b[n3];
+    for (int k = 0; k < n; ++k)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+          a[(k * n + j) * n + i] = u[((long)(iz * P + k) * NY + (iy * P + j)) * NX + (ix * P + i)];
+    // x, y, z interpolation to the Gauss points
+    for (int k = 0; k < n; ++k)
+      for (int j = 0; j < n; ++j)
+        for (int q = 0; q < n; ++q) {
+          double t = 0;
+          for (int i = 0; i < n; ++i) t += T.S[q * n + i] * a[(k * n + j) * n + i];
+          b[(k * n + j) * n + q] = t;
+        }
+    for (int k = 0; k < n; ++k)
+      for (int q = 0; q < n; ++q)
+        for (int i = 0; i < n; ++i) {
+          double t = 0;
+          for (int j = 0; j < n; ++j) t += T.S[q * n + j] * b[(k * n + j) * n + i];
+          a[(k * n + q) * n + i] = t;
+        }
+    for (int q = 0; q < n; ++q)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+          double t = 0;
+          for (int k = 0; k < n; ++k) t += T.S[q * n + k] * a[(k * n + j) * n + i];
+          b[(q * n + j) * n + i] = t;
+        }
+    for (int q = 0; q < n3; ++q) {
+      const int qi = q % n, qj = (q / n) % n, qk = q / (n * n);
+      const double JxW = metric ? metric[cell * 7 * n3 + q] : hx * hy * hz * T.w[qi] * T.w[qj] * T.w[qk];
+      s += b[q] * b[q] * JxW;
+    }
+  }
+  __shared__ double ws[256];
+  ws[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) ws[threadIdx.x] += ws[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = ws[0];
+}
+
+double l2_norm_integrated(Op &op, const double *u)
+{
+  Mesh &m = *op.mesh;
+  const int blocks = 256;
+  Colour *d_col = nullptr;
+  double *partial = nullptr;
+  MPDG_CUDA(cudaMalloc(&d_col, sizeof(m.colour)));
+  MPDG_CUDA(cudaMemcpy(d_col, m.colour, sizeof(m.colour), cudaMemcpyHostToDevice));
+  MPDG_CUDA(cudaMalloc(&partial, sizeof(double) * blocks));
+  const double *met = m.uniform ? nullptr : m.d_metric64;
+  switch (m.degree) {
+    case 1: l2_cells_kernel<1><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, met, m.h[0], m.h[1], m.h[2], partial); break;
+    case 2: l2_cells_kernel<2><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, met, m.h[0], m.h[1], m.h[2], partial); break;
+    case 3: l2_cells_kernel<3><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, met, m.h[0], m.h[1], m.h[2], partial); break;
+    case 4: l2_cells_kernel<4><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, met, m.h[0], m.h[1], m.h[2], partial); break;
+    default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+  }
+  MPDG_LAUNCHED();
+  std::vector<double> h(blocks);
+  MPDG_CUDA(cudaMemcpyAsync(h.data(), partial, sizeof(double) * blocks, cudaMemcpyDeviceToHost, op.stream));
+  MPDG_CUDA(cudaStreamSynchronize(op.stream));
+  cudaFree(partial);
+  cudaFree(d_col);
+  double s = 0.0;
+  for (double v : h) s += v;
+  return std::sqrt(s);
+}
+
+}  // namespace mpdg

@@ -1,0 +1,484 @@
+// Krylov solvers on the device: preconditioned CG and right-preconditioned
+// restarted GMRES with deal.II ReductionControl semantics
+// (include/meltpooldg/linear_algebra/linear_solver.hpp:26-134: converged when
+// |r_k|_2 <= max(abs_tol, rel_tol |r_0|_2)), the Jacobi preconditioner of
+// include/meltpooldg/linear_algebra/preconditioner_jacobi.hpp:50-69, a Chebyshev
+// smoother over it, and the FP32-inner / FP64-defect-correction driver.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <random>
+#include <vector>
+
+#include "mpdg_internal.h"
+#include "vector_kernels.cuh"
+
+namespace mpdg {
+
+struct Workspace {
+  long N = 0;
+  // FP64 vectors
+  double *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr, *invd = nullptr, *cd = nullptr,
+         *ct = nullptr;
+  // FP32 vectors
+  float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *Ap32 = nullptr, *x32 = nullptr,
+        *invd32 = nullptr, *cd32 = nullptr, *ct32 = nullptr;
+  double *V = nullptr;  // GMRES basis
+  int V_cols = 0;
+  double *partial = nullptr;  // reduction partials: 64 groups of kRedBlocks
+  double *scal = nullptr;     // device scalars (kNScalars) + GMRES h (64)
+  double *host = nullptr;     // pinned host mirror
+  bool invd_valid = false;
+  size_t bytes = 0;
+};
+
+namespace {
+
+template <typename T>
+T *walloc(Workspace &w, size_t count)
+{
+  T *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  if (e != cudaSuccess) throw Error{MPDG_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+  w.bytes += count * sizeof(T);
+  return p;
+}
+
+Workspace &ws64(Op &op)
+{
+  if (!op.ws) op.ws = new Workspace();
+  Workspace &w = *op.ws;
+  const long N = op.mesh->N;
+  w.N = N;
+  if (!w.r) {
+    w.r = walloc<double>(w, N);
+    w.z = walloc<double>(w, N);
+    w.p = walloc<double>(w, N);
+    w.Ap = walloc<double>(w, N);
+    w.invd = walloc<double>(w, N);
+    w.cd = walloc<double>(w, N);
+    w.ct = walloc<double>(w, N);
+    w.partial = walloc<double>(w, 64L * kRedBlocks);
+    w.scal = walloc<double>(w, kNScalars + 64);
+    MPDG_CUDA(cudaMallocHost(&w.host, sizeof(double) * (kNScalars + 64)));
+  }
+  return w;
+}
+
+Workspace &ws32(Op &op)
+{
+  Workspace &w = ws64(op);
+  const long N = op.mesh->N;
+  if (!w.r32) {
+    w.r32 = walloc<float>(w, N);
+    w.z32 = walloc<float>(w, N);
+    w.p32 = walloc<float>(w, N);
+    w.Ap32 = walloc<float>(w, N);
+    w.x32 = walloc<float>(w, N);
+    w.invd32 = walloc<float>(w, N);
+    w.cd32 = walloc<float>(w, N);
+    w.ct32 = walloc<float>(w, N);
+  }
+  return w;
+}
+
+double fetch(Op &op, Workspace &w, const double *dev, int count = 1)
+{
+  MPDG_CUDA(cudaMemcpyAsync(w.host, dev, sizeof(double) * count, cudaMemcpyDeviceToHost, op.stream));
+  MPDG_CUDA(cudaStreamSynchronize(op.stream));
+  return w.host[0];
+}
+
+struct Prec {
+  int kind = MPDG_PREC_JACOBI;
+  int degree = 5;
+  double lmin = 0, lmax = 0;
+};
+
+template <typename R>
+struct V {
+  R *r, *z, *p, *Ap, *invd, *cd, *ct;
+};
+
+V<double> vecs(Workspace &w, double *) { return {w.r, w.z, w.p, w.Ap, w.invd, w.cd, w.ct}; }
+V<float> vecs(Workspace &w, float *) { return {w.r32, w.z32, w.p32, w.Ap32, w.invd32, w.cd32, w.ct32}; }
+
+template <typename R>
+void prec_apply(Op &op, const Prec &P, const V<R> &v, const R *r, R *z, int &applies)
+{
+  const long N = op.mesh->N;
+  if (P.kind == MPDG_PREC_IDENTITY) {
+    dev_copy<R>(N, r, z, op.stream);
+    return;
+  }
+  if (P.kind == MPDG_PREC_JACOBI) {
+    dev_mul<R>(N, v.invd, r, z, op.stream);
+    return;
+  }
+  // Chebyshev semi-iteration on D^-1 A over [lmin, lmax], zero start
+  const double theta = 0.5 * (P.lmax + P.lmin), delta = 0.5 * (P.lmax - P.lmin);
+  const double sigma = theta / delta;
+  double rho = 1.0 / sigma;
+  dev_cheb_start<R>(N, 1.0 / theta, v.invd, r, v.cd, z, op.stream);
+  for (int k = 1; k < P.degree; ++k) {
+    launch_apply<R>(op, v.ct, z);
+    ++applies;
+    const double rho_new = 1.0 / (2.0 * sigma - rho);
+    dev_cheb_step<R>(N, rho_new * rho, 2.0 * rho_new / delta, v.invd, r, v.ct, v.cd, z, op.stream);
+    rho = rho_new;
+  }
+}
+
+// preconditioned CG; returns MPDG_OK / error; deal.II SolverCG recurrence
+template <typename R>
+int pcg(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero, double rel_tol,
+        double abs_tol, int max_it, int &iters, double &res0, double &res, int &applies)
+{
+  const long N = op.mesh->N;
+  V<R> v = vecs(w, (R *)nullptr);
+  cudaStream_t s = op.stream;
+  double *sc = w.scal;
+  if (x_is_zero) {
+    dev_copy<R>(N, b, v.r, s);
+  } else {
+    launch_apply<R>(op, v.Ap, x);
+    ++applies;
+    dev_copy<R>(N, b, v.r, s);
+    dev_axpby<R>(N, -1.0, v.Ap, 1.0, v.r, s);
+  }
+  if (sizeof(R) == 8)
+    dev_dot((const double *)v.r, (const double *)v.r, N, w.partial, sc + kRR, s);
+  else
+    dev_dot_f((const float *)v.r, (const float *)v.r, N, w.partial, sc + kRR, s);
+  res0 = std::sqrt(fetch(op, w, sc + kRR));
+  res = res0;
+  iters = 0;
+  if (!std::isfinite(res0)) return MPDG_ERR_NAN;
+  const double tol = std::fmax(abs_tol, rel_tol * res0);
+  if (res0 <= tol) return MPDG_OK;
+  prec_apply<R>(op, P, v, v.r, v.z, applies);
+  auto dot_into = [&](const R *a, const R *bb, double *out) {
+    if (sizeof(R) == 8)
+      dev_dot((const double *)a, (const double *)bb, N, w.partial, out, s);
+    else
+      dev_dot_f((const float *)a, (const float *)bb, N, w.partial, out, s);
+  };
+  dot_into(v.r, v.z, sc + kRZ);
+  dev_copy<R>(N, v.z, v.p, s);
+  const bool fused_jacobi = P.kind == MPDG_PREC_JACOBI;
+  while (true) {
+    launch_apply<R>(op, v.Ap, v.p);
+    ++applies;
+    dot_into(v.p, v.Ap, sc + kPAP);
+    dev_cg_update<R, R>(N, sc, x, v.r, v.p, v.Ap, fused_jacobi ? v.invd : nullptr, v.z, w.partial, s);
+    ++iters;
+    res = std::sqrt(fetch(op, w, sc + kRR));
+    if (!std::isfinite(res)) return MPDG_ERR_NAN;
+    if (res <= tol) return MPDG_OK;
+    if (iters >= max_it) return MPDG_ERR_NOT_CONVERGED;
+    if (!fused_jacobi) {
+      prec_apply<R>(op, P, v, v.r, v.z, applies);
+      dot_into(v.r, v.z, sc + kRZNEW);
+    }
+    dev_cg_direction<R>(N, sc, v.p, v.z, s);
+  }
+}
+
+// right-preconditioned restarted GMRES (classical Gram-Schmidt applied twice)
+int gmres(Op &op, Workspace &w, const Prec &P, const double *b, double *x, double rel_tol,
+          double abs_tol, int max_it, int restart, int &iters, double &res0, double &res,
+          int &applies)
+{
+  const long N = op.mesh->N;
+  cudaStream_t s = op.stream;
+  V<double> v = vecs(w, (double *)nullptr);
+  const int m = std::max(1, std::min(restart, 60));
+  if (!w.V || w.V_cols < m + 1) {
+    if (w.V) cudaFree(w.V);
+    w.V = walloc<double>(w, (size_t)N * (m + 1));
+    w.V_cols = m + 1;
+  }
+  std::vector<double> H((m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), y(m), h(m + 1);
+  iters = 0;
+  double tol = -1.0;
+  int status = MPDG_ERR_NOT_CONVERGED;
+  while (true) {
+    launch_apply<double>(op, v.Ap, x);
+    ++applies;
+    dev_copy<double>(N, b, w.V, s);
+    dev_axpby<double>(N, -1.0, v.Ap, 1.0, w.V, s);
+    dev_dot(w.V, w.V, N, w.partial, w.scal + kRR, s);
+    const double beta = std::sqrt(fetch(op, w, w.scal + kRR));
+    if (tol < 0.0) {
+      res0 = beta;
+      tol = std::fmax(abs_tol, rel_tol * beta);
+    }
+    res = beta;
+    if (!std::isfinite(beta)) return MPDG_ERR_NAN;
+    if (beta <= tol) {
+      status = MPDG_OK;
+      break;
+    }
+    if (iters >= max_it) break;
+    dev_axpby<double>(N, 0.0, w.V, 1.0 / beta, w.V, s);
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int j = 0;
+    bool done = false;
+    for (; j < m && iters < max_it; ++j) {
+      double *vj = w.V + (long)j * N, *vn = w.V + (long)(j + 1) * N;
+      prec_apply<double>(op, P, v, vj, v.z, applies);
+      launch_apply<double>(op, vn, v.z);
+      ++applies;
+      // two passes of classical Gram-Schmidt
+      for (int k = 0; k <= j; ++k) h[k] = 0.0;
+      for (int pass = 0; pass < 2; ++pass) {
+        dev_mdot(w.V, N, j + 1, vn, w.partial, w.scal + kNScalars, s);
+        MPDG_CUDA(cudaMemcpyAsync(w.host, w.scal + kNScalars, sizeof(double) * (j + 1),
+                                  cudaMemcpyDeviceToHost, s));
+        MPDG_CUDA(cudaStreamSynchronize(s));
+        for (int k = 0; k <= j; ++k) h[k] += w.host[k];
+        dev_mgs_update(w.V, N, j + 1, w.scal + kNScalars, vn, s);
+      }
+      dev_dot(vn, vn, N, w.partial, w.scal + kRR, s);
+      const double hn = std::sqrt(fetch(op, w, w.scal + kRR));
+      dev_axpby<double>(N, 0.0, vn, hn > 0 ? 1.0 / hn : 0.0, vn, s);
+      for (int k = 0; k <= j; ++k) H[k * m + j] = h[k];
+      H[(j + 1) * m + j] = hn;
+      for (int k = 0; k < j; ++k) {
+        const double t = cs[k] * H[k * m + j] + sn[k] * H[(k + 1) * m + j];
+        H[(k + 1) * m + j] = -sn[k] * H[k * m + j] + cs[k] * H[(k + 1) * m + j];
+        H[k * m + j] = t;
+      }
+      const double a = H[j * m + j], c = H[(j + 1) * m + j], rr = std::sqrt(a * a + c * c);
+      cs[j] = a / rr;
+      sn[j] = c / rr;
+      H[j * m + j] = rr;
+      H[(j + 1) * m + j] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      ++iters;
+      res = std::fabs(g[j + 1]);
+      if (!std::isfinite(res)) return MPDG_ERR_NAN;
+      if (res <= tol) {
+        ++j;
+        done = true;
+        break;
+      }
+    }
+    for (int k = j - 1; k >= 0; --k) {
+      double t = g[k];
+      for (int l = k + 1; l < j; ++l) t -= H[k * m + l] * y[l];
+      y[k] = t / H[k * m + k];
+    }
+    MPDG_CUDA(cudaMemcpyAsync(w.scal + kNScalars, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, s));
+    dev_combine(w.V, N, j, w.scal + kNScalars, v.ct, s);
+    prec_apply<double>(op, P, v, v.ct, v.z, applies);
+    dev_axpby<double>(N, 1.0, v.z, 1.0, x, s);
+    MPDG_CUDA(cudaStreamSynchronize(s));  // y is read from pageable memory
+    if (done) {
+      status = MPDG_OK;
+      break;
+    }
+    if (iters >= max_it) break;
+  }
+  return status;
+}
+
+// largest eigenvalue of D^-1 A from CG-Lanczos on A x = start
+double lanczos_lmax(Op &op, Workspace &w, int steps, int &applies)
+{
+  const long N = op.mesh->N;
+  cudaStream_t s = op.stream;
+  std::vector<double> h(N);
+  std::mt19937_64 rng(4);
+  std::uniform_real_distribution<double> U(-1.0, 1.0);
+  for (long i = 0; i < N; ++i) h[i] = U(rng);
+  double *start = w.cd;
+  MPDG_CUDA(cudaMemcpyAsync(start, h.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  if (op.use_dirichlet && op.mesh->has_dirichlet) {
+    // constrained rows of A are zero: keep the start vector in the free space
+    std::vector<uint8_t> mk(N);
+    MPDG_CUDA(cudaMemcpyAsync(mk.data(), op.mesh->d_dmask, N, cudaMemcpyDeviceToHost, s));
+    MPDG_CUDA(cudaStreamSynchronize(s));
+    for (long i = 0; i < N; ++i)
+      if (mk[i]) h[i] = 0.0;
+    MPDG_CUDA(cudaMemcpyAsync(start, h.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  }
+  MPDG_CUDA(cudaStreamSynchronize(s));
+  double *r = w.r, *z = w.z, *p = w.p, *Ap = w.Ap, *sc = w.scal;
+  dev_copy<double>(N, start, r, s);
+  dev_mul<double>(N, w.invd, r, z, s);
+  dev_copy<double>(N, z, p, s);
+  dev_dot(r, z, N, w.partial, sc + kRZ, s);
+  std::vector<double> al, be;
+  double *xdummy = w.ct;
+  MPDG_CUDA(cudaMemsetAsync(xdummy, 0, sizeof(double) * N, s));
+  for (int k = 0; k < steps; ++k) {
+    launch_apply<double>(op, Ap, p);
+    ++applies;
+    dev_dot(p, Ap, N, w.partial, sc + kPAP, s);
+    dev_cg_update<double, double>(N, sc, xdummy, r, p, Ap, w.invd, z, w.partial, s);
+    MPDG_CUDA(cudaMemcpyAsync(w.host, sc, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+    MPDG_CUDA(cudaStreamSynchronize(s));
+    const double rz = w.host[kRZ], rz_new = w.host[kRZNEW], pap = w.host[kPAP];
+    if (!(pap > 0) || !(rz > 0)) break;
+    al.push_back(rz / pap);
+    be.push_back(rz_new / rz);
+    dev_cg_direction<double>(N, sc, p, z, s);
+    if (!(rz_new > 0)) break;
+  }
+  const int k = (int)al.size();
+  if (k == 0) return 1.0;
+  std::vector<double> dg(k), of(k, 0.0);
+  for (int j = 0; j < k; ++j) {
+    dg[j] = 1.0 / al[j] + (j > 0 ? be[j - 1] / al[j - 1] : 0.0);
+    of[j] = (j + 1 < k) ? std::sqrt(be[j]) / al[j] : 0.0;
+  }
+  double lo = 0.0, hi = 0.0;
+  for (int j = 0; j < k; ++j) hi = std::fmax(hi, dg[j] + std::fabs(of[j]) + (j > 0 ? std::fabs(of[j - 1]) : 0.0));
+  for (int it = 0; it < 200; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    int cnt = 0;
+    double q = 1.0;
+    for (int j = 0; j < k; ++j) {
+      q = dg[j] - mid - (j > 0 ? of[j - 1] * of[j - 1] / q : 0.0);
+      if (q == 0.0) q = -1e-300;
+      if (q < 0.0) ++cnt;
+    }
+    if (cnt >= k) hi = mid;
+    else lo = mid;
+  }
+  return hi;
+}
+
+__global__ void cast_down_kernel(const double *a, float *b, long n)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+}  // namespace
+
+int solve(Op &op, const mpdg_solver_desc &d, double *x, const double *b, mpdg_solve_report &rep)
+{
+  const auto t0 = std::chrono::steady_clock::now();
+  Workspace &w = ws64(op);
+  const long N = op.mesh->N;
+  cudaStream_t s = op.stream;
+  rep = mpdg_solve_report{};
+  int applies = 0;
+  Prec P;
+  P.kind = d.preconditioner;
+  P.degree = d.chebyshev_degree > 0 ? d.chebyshev_degree : 5;
+  if (P.kind != MPDG_PREC_IDENTITY) {
+    launch_diagonal(op, w.invd);
+    launch_invert_diagonal(op, w.invd);
+  }
+  if (P.kind == MPDG_PREC_CHEBYSHEV) {
+    const double lam = lanczos_lmax(op, w, d.lanczos_steps > 0 ? d.lanczos_steps : 10, applies);
+    const double range = d.chebyshev_range > 0 ? d.chebyshev_range : 30.0;
+    const double safety = d.chebyshev_safety > 0 ? d.chebyshev_safety : 1.2;
+    P.lmax = safety * lam;
+    P.lmin = lam / range;
+    rep.lambda_max = lam;
+  }
+  const double rel = d.rel_tolerance, abs_tol = d.abs_tolerance;
+  const int max_it = d.max_iterations > 0 ? d.max_iterations : 10000;
+  int status = MPDG_OK;
+  double res0 = 0, res = 0;
+  if (!d.mixed_precision) {
+    int it = 0;
+    if (d.solver == MPDG_SOLVER_CG)
+      status = pcg<double>(op, w, P, b, x, false, rel, abs_tol, max_it, it, res0, res, applies);
+    else
+      status = gmres(op, w, P, b, x, rel, abs_tol, max_it, d.gmres_restart > 0 ? d.gmres_restart : 30,
+                     it, res0, res, applies);
+    rep.iterations = it;
+  } else {
+    if (d.solver != MPDG_SOLVER_CG) throw Error{MPDG_ERR_UNSUPPORTED, "mixed precision uses CG"};
+    Workspace &w32 = ws32(op);
+    if (op.T64) ensure_T32(op);
+    cast_down_kernel<<<1184, 256, 0, s>>>(w.invd, w32.invd32, N);
+    MPDG_LAUNCHED();
+    // FP64 defect: r = b - A x
+    launch_apply<double>(op, w.Ap, x);
+    ++applies;
+    dev_copy<double>(N, b, w.r, s);
+    dev_axpby<double>(N, -1.0, w.Ap, 1.0, w.r, s);
+    dev_dot(w.r, w.r, N, w.partial, w.scal + kRR, s);
+    res0 = std::sqrt(fetch(op, w, w.scal + kRR));
+    res = res0;
+    const double tol = std::fmax(abs_tol, rel * res0);
+    const double inner = d.inner_tolerance > 0 ? d.inner_tolerance : 1e-4;
+    const int max_outer = d.max_outer > 0 ? d.max_outer : 20;
+    int outer = 0, total = 0;
+    status = std::isfinite(res0) ? MPDG_OK : MPDG_ERR_NAN;
+    while (status == MPDG_OK && res > tol) {
+      if (outer >= max_outer || total >= max_it) {
+        status = MPDG_ERR_NOT_CONVERGED;
+        break;
+      }
+      // unit-norm FP32 defect, FP32 correction, FP64 update
+      dev_scale_copy<float>(N, 1.0 / res, w.r, w32.z32, s);
+      MPDG_CUDA(cudaMemsetAsync(w32.x32, 0, sizeof(float) * N, s));
+      int it = 0;
+      double r0i = 0, ri = 0;
+      // the inner CG reads its rhs from z32 (copied into r32 by pcg)
+      int st = pcg<float>(op, w32, P, w32.z32, w32.x32, true, inner, 0.0,
+                          std::max(1, max_it - total), it, r0i, ri, applies);
+      total += it;
+      if (st == MPDG_ERR_NAN) {
+        status = st;
+        break;
+      }
+      dev_add_scaled<float>(N, res, w32.x32, x, s);
+      launch_apply<double>(op, w.Ap, x);
+      ++applies;
+      dev_copy<double>(N, b, w.r, s);
+      dev_axpby<double>(N, -1.0, w.Ap, 1.0, w.r, s);
+      dev_dot(w.r, w.r, N, w.partial, w.scal + kRR, s);
+      res = std::sqrt(fetch(op, w, w.scal + kRR));
+      ++outer;
+      if (!std::isfinite(res)) status = MPDG_ERR_NAN;
+    }
+    rep.iterations = total;
+    rep.outer_iterations = outer;
+  }
+  MPDG_CUDA(cudaStreamSynchronize(s));
+  rep.status = status;
+  rep.operator_applies = applies;
+  rep.initial_residual = res0;
+  rep.final_residual = res;
+  rep.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return status;
+}
+
+void free_workspace(Op &op)
+{
+  if (!op.ws) return;
+  Workspace &w = *op.ws;
+  for (void *p : {(void *)w.r, (void *)w.z, (void *)w.p, (void *)w.Ap, (void *)w.invd, (void *)w.cd,
+                  (void *)w.ct, (void *)w.r32, (void *)w.z32, (void *)w.p32, (void *)w.Ap32,
+                  (void *)w.x32, (void *)w.invd32, (void *)w.cd32, (void *)w.ct32, (void *)w.V,
+                  (void *)w.partial, (void *)w.scal})
+    if (p) cudaFree(p);
+  if (w.host) cudaFreeHost(w.host);
+  delete op.ws;
+  op.ws = nullptr;
+}
+
+double linf(const double *a, long n, cudaStream_t s)
+{
+  double *partial = nullptr, *out = nullptr, h = 0.0;
+  MPDG_CUDA(cudaMalloc(&partial, sizeof(double) * (kRedBlocks + 1)));
+  out = partial + kRedBlocks;
+  dev_linf(a, n, partial, out, s);
+  MPDG_CUDA(cudaMemcpyAsync(&h, out, sizeof(double), cudaMemcpyDeviceToHost, s));
+  MPDG_CUDA(cudaStreamSynchronize(s));
+  cudaFree(partial);
+  return h;
+}
+
+}  // namespace mpdg

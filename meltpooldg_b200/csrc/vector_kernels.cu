@@ -1,0 +1,405 @@
+// Vector kernels of the Krylov solvers: deterministic FP64 reductions (warp
+// shuffles, then a fixed-order block pass) and the fused CG / Chebyshev / GMRES
+// updates.  All reductions accumulate in FP64 whatever the vector precision.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "mpdg_internal.h"
+#include "vector_kernels.cuh"
+
+namespace mpdg {
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// block-wide sum of v (blockDim.x == kRedThreads); result valid in thread 0
+__device__ __forceinline__ double block_sum(double v)
+{
+  __shared__ double ws[kRedThreads / 32];
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (w == 0) {
+    s = (lane < kRedThreads / 32) ? ws[lane] : 0.0;
+    s = warp_sum(s);
+  }
+  __syncthreads();
+  return s;
+}
+
+template <typename A, typename B>
+__global__ void __launch_bounds__(kRedThreads) dot_partial_kernel(const A *a, const B *b, long n,
+                                                                  double *partial)
+{
+  double s = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    s += (double)a[i] * (double)b[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(kRedThreads) linf_partial_kernel(const double *a, long n, double *partial)
+{
+  __shared__ double ws[kRedThreads / 32];
+  double s = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    s = fmax(s, fabs(a[i]));
+  s = warp_max(s);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) ws[w] = s;
+  __syncthreads();
+  if (w == 0) {
+    s = (lane < kRedThreads / 32) ? ws[lane] : 0.0;
+    s = warp_max(s);
+    if (lane == 0) partial[blockIdx.x] = s;
+  }
+}
+
+// sums (or max-reduces) `count` groups of kRedBlocks partials into out[0..count)
+__global__ void __launch_bounds__(kRedThreads) finish_kernel(const double *partial, int count,
+                                                             double *out, int use_max)
+{
+  const int g = blockIdx.x;
+  if (g >= count) return;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < kRedBlocks; i += blockDim.x) {
+    const double v = partial[(long)g * kRedBlocks + i];
+    s = use_max ? fmax(s, v) : s + v;
+  }
+  if (use_max) {
+    __shared__ double ws[kRedThreads / 32];
+    s = warp_max(s);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) ws[w] = s;
+    __syncthreads();
+    if (w == 0) {
+      s = (lane < kRedThreads / 32) ? ws[lane] : 0.0;
+      s = warp_max(s);
+      if (lane == 0) out[g] = s;
+    }
+  } else {
+    s = block_sum(s);
+    if (threadIdx.x == 0) out[g] = s;
+  }
+}
+
+// multi-dot: partial[k][block] = V_k . w for k < m  (V rows of stride n)
+__global__ void __launch_bounds__(kRedThreads) mdot_partial_kernel(const double *V, long n, int m,
+                                                                   const double *w, double *partial)
+{
+  for (int k = 0; k < m; ++k) {
+    double s = 0.0;
+    const double *v = V + (long)k * n;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+      s += v[i] * w[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) partial[(long)k * kRedBlocks + blockIdx.x] = s;
+  }
+}
+
+// w -= sum_k h[k] V_k
+__global__ void mgs_update_kernel(const double *V, long n, int m, const double *h, double *w)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double s = w[i];
+    for (int k = 0; k < m; ++k) s -= h[k] * V[(long)k * n + i];
+    w[i] = s;
+  }
+}
+
+// x += sum_k y[k] V_k
+__global__ void combine_kernel(const double *V, long n, int m, const double *y, double *x)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < m; ++k) s += y[k] * V[(long)k * n + i];
+    x[i] = s;
+  }
+}
+
+template <typename R>
+__global__ void axpby_kernel(long n, double a, const R *x, double b, R *y)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    y[i] = (R)(a * (double)x[i] + b * (double)y[i]);
+}
+
+// y = b - y
+__global__ void residual_kernel(long n, const double *b, double *y)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    y[i] = b[i] - y[i];
+}
+
+template <typename R>
+__global__ void scale_copy_kernel(long n, double a, const double *x, R *y)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    y[i] = (R)(a * x[i]);
+}
+
+template <typename R>
+__global__ void add_scaled_kernel(long n, double a, const R *x, double *y)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    y[i] += a * (double)x[i];
+}
+
+template <typename R>
+__global__ void mul_kernel(long n, const R *d, const R *x, R *y)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    y[i] = d[i] * x[i];
+}
+
+// CG step part 1: alpha = s[RZ] / s[PAP]; x += alpha p; r -= alpha Ap;
+// with jacobi: z = invd r; partials of r.r (slot 0) and r.z (slot 1)
+template <typename R, typename RX>
+__global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long n, const double *s, RX *x,
+                                                                R *r, const R *p, const R *Ap,
+                                                                const R *invd, R *z,
+                                                                double *partial)
+{
+  const double alpha = s[kRZ] / s[kPAP];
+  double rr = 0.0, rz = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    x[i] = (RX)((double)x[i] + alpha * (double)p[i]);
+    const R ri = (R)((double)r[i] - alpha * (double)Ap[i]);
+    r[i] = ri;
+    rr += (double)ri * (double)ri;
+    if (invd) {
+      const R zi = invd[i] * ri;
+      z[i] = zi;
+      rz += (double)ri * (double)zi;
+    }
+  }
+  rr = block_sum(rr);
+  if (threadIdx.x == 0) partial[blockIdx.x] = rr;
+  if (invd) {
+    rz = block_sum(rz);
+    if (threadIdx.x == 0) partial[kRedBlocks + blockIdx.x] = rz;
+  }
+}
+
+// CG step part 2: beta = s[RZNEW] / s[RZ]; p = z + beta p; s[RZ] <- s[RZNEW] (block 0)
+template <typename R>
+__global__ void cg_direction_kernel(long n, double *s, R *p, const R *z)
+{
+  const double beta = s[kRZNEW] / s[kRZ];
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    p[i] = (R)((double)z[i] + beta * (double)p[i]);
+}
+
+__global__ void shift_scalar_kernel(double *s)
+{
+  s[kRZ] = s[kRZNEW];
+}
+
+// Chebyshev start: d = invd r / theta; z = d
+template <typename R>
+__global__ void cheb_start_kernel(long n, double inv_theta, const R *invd, const R *r, R *d, R *z)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const R v = (R)(inv_theta * (double)(invd[i] * r[i]));
+    d[i] = v;
+    z[i] = v;
+  }
+}
+
+// Chebyshev step: d = c1 d + c2 invd (r - t); z += d
+template <typename R>
+__global__ void cheb_step_kernel(long n, double c1, double c2, const R *invd, const R *r, const R *t,
+                                 R *d, R *z)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const R v = (R)(c1 * (double)d[i] + c2 * (double)(invd[i] * (r[i] - t[i])));
+    d[i] = v;
+    z[i] += v;
+  }
+}
+
+// ------------------------------------------------------------------ host side
+
+namespace {
+unsigned vgrid(long n)
+{
+  long g = (n + 255) / 256;
+  if (g > 148L * 16) g = 148L * 16;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+}  // namespace
+
+void dev_dot(const double *a, const double *b, long n, double *partial, double *out, cudaStream_t s)
+{
+  dot_partial_kernel<double, double><<<kRedBlocks, kRedThreads, 0, s>>>(a, b, n, partial);
+  MPDG_LAUNCHED();
+  finish_kernel<<<1, kRedThreads, 0, s>>>(partial, 1, out, 0);
+  MPDG_LAUNCHED();
+}
+
+void dev_dot_f(const float *a, const float *b, long n, double *partial, double *out, cudaStream_t s)
+{
+  dot_partial_kernel<float, float><<<kRedBlocks, kRedThreads, 0, s>>>(a, b, n, partial);
+  MPDG_LAUNCHED();
+  finish_kernel<<<1, kRedThreads, 0, s>>>(partial, 1, out, 0);
+  MPDG_LAUNCHED();
+}
+
+void dev_linf(const double *a, long n, double *partial, double *out, cudaStream_t s)
+{
+  linf_partial_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(a, n, partial);
+  MPDG_LAUNCHED();
+  finish_kernel<<<1, kRedThreads, 0, s>>>(partial, 1, out, 1);
+  MPDG_LAUNCHED();
+}
+
+void dev_mdot(const double *V, long n, int m, const double *w, double *partial, double *out,
+              cudaStream_t s)
+{
+  mdot_partial_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(V, n, m, w, partial);
+  MPDG_LAUNCHED();
+  finish_kernel<<<m, kRedThreads, 0, s>>>(partial, m, out, 0);
+  MPDG_LAUNCHED();
+}
+
+void dev_mgs_update(const double *V, long n, int m, const double *h, double *w, cudaStream_t s)
+{
+  mgs_update_kernel<<<vgrid(n), 256, 0, s>>>(V, n, m, h, w);
+  MPDG_LAUNCHED();
+}
+
+void dev_combine(const double *V, long n, int m, const double *y, double *x, cudaStream_t s)
+{
+  combine_kernel<<<vgrid(n), 256, 0, s>>>(V, n, m, y, x);
+  MPDG_LAUNCHED();
+}
+
+template <typename R>
+void dev_axpby(long n, double a, const R *x, double b, R *y, cudaStream_t s)
+{
+  axpby_kernel<R><<<vgrid(n), 256, 0, s>>>(n, a, x, b, y);
+  MPDG_LAUNCHED();
+}
+template void dev_axpby<double>(long, double, const double *, double, double *, cudaStream_t);
+template void dev_axpby<float>(long, double, const float *, double, float *, cudaStream_t);
+
+void dev_residual(long n, const double *b, double *y, cudaStream_t s)
+{
+  residual_kernel<<<vgrid(n), 256, 0, s>>>(n, b, y);
+  MPDG_LAUNCHED();
+}
+
+template <typename R>
+void dev_scale_copy(long n, double a, const double *x, R *y, cudaStream_t s)
+{
+  scale_copy_kernel<R><<<vgrid(n), 256, 0, s>>>(n, a, x, y);
+  MPDG_LAUNCHED();
+}
+template void dev_scale_copy<double>(long, double, const double *, double *, cudaStream_t);
+template void dev_scale_copy<float>(long, double, const double *, float *, cudaStream_t);
+
+template <typename R>
+void dev_add_scaled(long n, double a, const R *x, double *y, cudaStream_t s)
+{
+  add_scaled_kernel<R><<<vgrid(n), 256, 0, s>>>(n, a, x, y);
+  MPDG_LAUNCHED();
+}
+template void dev_add_scaled<double>(long, double, const double *, double *, cudaStream_t);
+template void dev_add_scaled<float>(long, double, const float *, double *, cudaStream_t);
+
+template <typename R>
+void dev_mul(long n, const R *d, const R *x, R *y, cudaStream_t s)
+{
+  mul_kernel<R><<<vgrid(n), 256, 0, s>>>(n, d, x, y);
+  MPDG_LAUNCHED();
+}
+template void dev_mul<double>(long, const double *, const double *, double *, cudaStream_t);
+template void dev_mul<float>(long, const float *, const float *, float *, cudaStream_t);
+
+template <typename R, typename RX>
+void dev_cg_update(long n, double *s, RX *x, R *r, const R *p, const R *Ap, const R *invd, R *z,
+                   double *partial, cudaStream_t st)
+{
+  cg_update_kernel<R, RX><<<kRedBlocks, kRedThreads, 0, st>>>(n, s, x, r, p, Ap, invd, z, partial);
+  MPDG_LAUNCHED();
+  // rr -> s[kRR]; rz -> s[kRZNEW]
+  finish_kernel<<<1, kRedThreads, 0, st>>>(partial, 1, s + kRR, 0);
+  MPDG_LAUNCHED();
+  if (invd) {
+    finish_kernel<<<1, kRedThreads, 0, st>>>(partial + kRedBlocks, 1, s + kRZNEW, 0);
+    MPDG_LAUNCHED();
+  }
+}
+template void dev_cg_update<double, double>(long, double *, double *, double *, const double *,
+                                            const double *, const double *, double *, double *,
+                                            cudaStream_t);
+template void dev_cg_update<float, float>(long, double *, float *, float *, const float *,
+                                          const float *, const float *, float *, double *,
+                                          cudaStream_t);
+
+template <typename R>
+void dev_cg_direction(long n, double *s, R *p, const R *z, cudaStream_t st)
+{
+  cg_direction_kernel<R><<<vgrid(n), 256, 0, st>>>(n, s, p, z);
+  MPDG_LAUNCHED();
+  shift_scalar_kernel<<<1, 1, 0, st>>>(s);
+  MPDG_LAUNCHED();
+}
+template void dev_cg_direction<double>(long, double *, double *, const double *, cudaStream_t);
+template void dev_cg_direction<float>(long, double *, float *, const float *, cudaStream_t);
+
+template <typename R>
+void dev_cheb_start(long n, double inv_theta, const R *invd, const R *r, R *d, R *z, cudaStream_t s)
+{
+  cheb_start_kernel<R><<<vgrid(n), 256, 0, s>>>(n, inv_theta, invd, r, d, z);
+  MPDG_LAUNCHED();
+}
+template void dev_cheb_start<double>(long, double, const double *, const double *, double *,
+                                     double *, cudaStream_t);
+template void dev_cheb_start<float>(long, double, const float *, const float *, float *, float *,
+                                    cudaStream_t);
+
+template <typename R>
+void dev_cheb_step(long n, double c1, double c2, const R *invd, const R *r, const R *t, R *d, R *z,
+                   cudaStream_t s)
+{
+  cheb_step_kernel<R><<<vgrid(n), 256, 0, s>>>(n, c1, c2, invd, r, t, d, z);
+  MPDG_LAUNCHED();
+}
+template void dev_cheb_step<double>(long, double, double, const double *, const double *,
+                                    const double *, double *, double *, cudaStream_t);
+template void dev_cheb_step<float>(long, double, double, const float *, const float *, const float *,
+                                   float *, float *, cudaStream_t);
+
+template <typename R>
+__global__ void copy_kernel(long n, const R *x, R *y)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    y[i] = x[i];
+}
+
+template <typename R>
+void dev_copy(long n, const R *x, R *y, cudaStream_t s)
+{
+  copy_kernel<R><<<vgrid(n), 256, 0, s>>>(n, x, y);
+  MPDG_LAUNCHED();
+}
+template void dev_copy<double>(long, const double *, double *, cudaStream_t);
+template void dev_copy<float>(long, const float *, float *, cudaStream_t);
+
+}  // namespace mpdg

@@ -1,0 +1,43 @@
+// Host launchers of the solver vector kernels (vector_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace mpdg {
+
+constexpr int kRedThreads = 256;  // threads per reduction block
+constexpr int kRedBlocks = 592;   // 4 blocks per SM on 148 SMs: fixed, so sums are deterministic
+
+// slots of the device scalar array used by the CG kernels
+enum { kRZ = 0, kRZNEW = 1, kPAP = 2, kRR = 3, kNScalars = 8 };
+
+void dev_dot(const double *a, const double *b, long n, double *partial, double *out, cudaStream_t s);
+void dev_dot_f(const float *a, const float *b, long n, double *partial, double *out, cudaStream_t s);
+void dev_linf(const double *a, long n, double *partial, double *out, cudaStream_t s);
+void dev_mdot(const double *V, long n, int m, const double *w, double *partial, double *out,
+              cudaStream_t s);
+void dev_mgs_update(const double *V, long n, int m, const double *h, double *w, cudaStream_t s);
+void dev_combine(const double *V, long n, int m, const double *y, double *x, cudaStream_t s);
+template <typename R>
+void dev_axpby(long n, double a, const R *x, double b, R *y, cudaStream_t s);
+void dev_residual(long n, const double *b, double *y, cudaStream_t s);
+template <typename R>
+void dev_scale_copy(long n, double a, const double *x, R *y, cudaStream_t s);
+template <typename R>
+void dev_add_scaled(long n, double a, const R *x, double *y, cudaStream_t s);
+template <typename R>
+void dev_mul(long n, const R *d, const R *x, R *y, cudaStream_t s);
+template <typename R, typename RX>
+void dev_cg_update(long n, double *s, RX *x, R *r, const R *p, const R *Ap, const R *invd, R *z,
+                   double *partial, cudaStream_t st);
+template <typename R>
+void dev_cg_direction(long n, double *s, R *p, const R *z, cudaStream_t st);
+template <typename R>
+void dev_cheb_start(long n, double inv_theta, const R *invd, const R *r, R *d, R *z, cudaStream_t s);
+template <typename R>
+void dev_cheb_step(long n, double c1, double c2, const R *invd, const R *r, const R *t, R *d, R *z,
+                   cudaStream_t s);
+template <typename R>
+void dev_copy(long n, const R *x, R *y, cudaStream_t s);
+
+}  // namespace mpdg

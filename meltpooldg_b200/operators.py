@@ -1,0 +1,301 @@
+"""Host-side mirror of MeltPoolDG's matrix-free operator interface over the
+C ABI of libmpdg.so.
+
+Class and method names follow the reference so that code written against
+OperatorMatrixFree (include/meltpooldg/core/operator_base.hpp:189-283) reads the
+same:
+
+    op = HeatDiffuseOperator(mesh, dt=..., rho_cp=..., k0=...)
+    op.vmult(dst, src)                                   # operator_base.hpp:239-243
+    op.compute_inverse_diagonal_from_matrixfree(diag)    # operator_base.hpp:268-272
+    op.create_rhs(dst, src)                              # operator_base.hpp:208-212
+    LinearSolver.solve(op, x, b, LinearSolverData(...))  # linear_solver.hpp:26-134
+
+Vectors are torch tensors on the CUDA device (float64, or float32 for the FP32
+form) in the library's lexicographic DoF numbering.  torch only provides device
+memory and streams; all arithmetic runs in the library's own kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi as A
+
+try:
+    import torch
+except ImportError:  # pragma: no cover - torch is part of the environment
+    torch = None
+
+
+def _dptr(t):
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("vectors must be contiguous CUDA tensors")
+    return C.c_void_p(t.data_ptr())
+
+
+class Mesh:
+    """Structured hexahedral mesh with FE_Q(degree) on Gauss-Lobatto points
+    (ScratchData + MatrixFree set-up, source/core/scratch_data.cpp:191-268)."""
+
+    def __init__(self, vertices, nc, degree, dirichlet_mask=None, geometry="auto"):
+        L = A.lib()
+        self.nc = tuple(int(v) for v in nc)
+        self.degree = int(degree)
+        self.vertices = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+        self.mask = None if dirichlet_mask is None else np.ascontiguousarray(dirichlet_mask, np.uint8)
+        d = A.MeshDesc(3, self.degree, (C.c_int * 3)(*self.nc),
+                       self.vertices.ctypes.data_as(C.POINTER(C.c_double)),
+                       None if self.mask is None else self.mask.ctypes.data_as(C.POINTER(C.c_uint8)),
+                       A.GEOM_GENERAL if geometry == "general" else A.GEOM_AUTO)
+        h = C.c_void_p()
+        A.check(L.mpdg_mesh_create(C.byref(d), C.byref(h)), "mpdg_mesh_create")
+        self._h = h
+        n = C.c_int64()
+        L.mpdg_mesh_n_dofs(h, C.byref(n))
+        self.n_dofs = int(n.value)
+        self.shape = tuple(self.nc[d_] * self.degree + 1 for d_ in range(3))
+
+    @classmethod
+    def box(cls, nc, degree, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), perturb=0.0, seed=None,
+            dirichlet="none", geometry="auto"):
+        V = box_vertices(nc, lo, hi, perturb, seed)
+        mask = None
+        if dirichlet == "all":
+            mask = boundary_mask(nc, degree)
+        elif dirichlet is not None and not isinstance(dirichlet, str):
+            mask = dirichlet
+        return cls(V, nc, degree, mask, geometry)
+
+    def device_bytes(self):
+        b = C.c_int64()
+        A.lib().mpdg_mesh_device_bytes(self._h, C.byref(b))
+        return int(b.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            A.lib().mpdg_mesh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def box_vertices(nc, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), perturb=0.0, seed=None):
+    """Vertices (x fastest) of an nc[0] x nc[1] x nc[2] box; interior vertices
+    displaced by U[-perturb h, perturb h] per coordinate (PCG64(seed))."""
+    axes = [np.linspace(lo[d], hi[d], nc[d] + 1) for d in range(3)]
+    Z, Y, X = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    V = np.stack([X.reshape(-1), Y.reshape(-1), Z.reshape(-1)], axis=1)
+    if perturb > 0.0:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        h = np.array([(hi[d] - lo[d]) / nc[d] for d in range(3)])
+        disp = rng.uniform(-1.0, 1.0, size=V.shape) * perturb * h
+        kz, ky, kx = np.meshgrid(np.arange(nc[2] + 1), np.arange(nc[1] + 1), np.arange(nc[0] + 1),
+                                 indexing="ij")
+        idx = np.stack([kx.reshape(-1), ky.reshape(-1), kz.reshape(-1)], axis=1)
+        interior = np.all((idx > 0) & (idx < np.array(nc)), axis=1)
+        V[interior] += disp[interior]
+    return np.ascontiguousarray(V)
+
+
+def boundary_mask(nc, degree, faces=None):
+    """uint8 mask of the DoFs on the selected box faces ((direction, side) pairs;
+    default all six)."""
+    shape = tuple(nc[d] * degree + 1 for d in range(3))
+    Z, Y, X = np.meshgrid(*[np.arange(s) for s in shape[::-1]], indexing="ij")
+    g = [X.reshape(-1), Y.reshape(-1), Z.reshape(-1)]
+    m = np.zeros(g[0].shape, dtype=bool)
+    for d, s in (faces if faces is not None else [(d, s) for d in range(3) for s in (0, 1)]):
+        m |= g[d] == (0 if s == 0 else shape[d] - 1)
+    return m.astype(np.uint8)
+
+
+class _MatrixFreeOperator:
+    """Common part of the two operators (OperatorBase + OperatorMatrixFree)."""
+
+    def __init__(self, mesh, desc, precisions):
+        mask = 0
+        for p in precisions:
+            mask |= 1 << (A.FP32 if p in ("fp32", "float32") else A.FP64)
+        desc.precision_mask = mask
+        h = C.c_void_p()
+        A.check(A.lib().mpdg_op_create(mesh._h, C.byref(desc), C.byref(h)), "mpdg_op_create")
+        self._h = h
+        self.mesh = mesh
+        self.n_dofs = mesh.n_dofs
+        self._desc = desc
+        self._fields = {}
+
+    # OperatorBase::reset_time_increment (operator_base.hpp:41-46)
+    def reset_time_increment(self, dt):
+        A.check(A.lib().mpdg_op_reset_time_increment(self._h, float(dt)), "reset_time_increment")
+
+    # OperatorBase::reset_dof_index (operator_base.hpp:31-35): with_dirichlet=False
+    # selects the constraint set without Dirichlet rows
+    def reset_dof_index(self, with_dirichlet=True):
+        A.check(A.lib().mpdg_op_use_dirichlet(self._h, int(bool(with_dirichlet))), "reset_dof_index")
+
+    def set_stream(self, stream):
+        A.lib().mpdg_op_set_stream(self._h, C.c_void_p(stream.cuda_stream if stream is not None else 0))
+
+    def vmult(self, dst, src):
+        if dst.dtype == torch.float32:
+            A.check(A.lib().mpdg_vmult_f32(self._h, _dptr(dst), _dptr(src)), "vmult_f32")
+        else:
+            A.check(A.lib().mpdg_vmult(self._h, _dptr(dst), _dptr(src)), "vmult")
+
+    def vmult_host(self, dst: np.ndarray, src: np.ndarray):
+        dp = C.POINTER(C.c_double)
+        A.check(A.lib().mpdg_vmult_host(self._h, dst.ctypes.data_as(dp), src.ctypes.data_as(dp)),
+                "vmult_host")
+
+    def compute_inverse_diagonal_from_matrixfree(self, diag):
+        A.check(A.lib().mpdg_compute_inverse_diagonal(self._h, _dptr(diag)), "compute_inverse_diagonal")
+
+    def compute_diagonal(self, diag):
+        A.check(A.lib().mpdg_compute_diagonal(self._h, _dptr(diag)), "compute_diagonal")
+
+    def l2_norm(self, u):
+        v = C.c_double()
+        A.check(A.lib().mpdg_l2_norm(self._h, _dptr(u), C.byref(v)), "l2_norm")
+        return v.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            A.lib().mpdg_op_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HeatDiffuseOperator(_MatrixFreeOperator):
+    """Tangent and residual of the heat equation
+    (HeatDiffuseMultiPhaseOperator, source/heat/heat_diffuse_operator.cpp):
+    v = rho_cp/dt u + rho_cp vel.grad u, g = k(T) grad u, k(T) = k0 (1 + k_alpha T).
+    `full_tangent` adds the Newton term dk/dT grad(T) u (non-symmetric)."""
+
+    def __init__(self, mesh, dt, rho_cp=1.0, k0=1.0, k_alpha=0.0, full_tangent=False,
+                 velocity=None, precisions=("fp64",)):
+        vk, vp = _velocity(velocity)
+        d = A.OpDesc(A.OP_HEAT, dt, rho_cp, k0, k_alpha, int(full_tangent), 0.0, 0.0, vk,
+                     (C.c_double * 3)(*vp), 0)
+        super().__init__(mesh, d, precisions)
+
+    def set_temperature(self, T):
+        """The temperature the operator linearises about (the `temperature`
+        vector the reference operator holds by reference)."""
+        self._fields["T"] = T
+        A.check(A.lib().mpdg_op_set_field(self._h, A.FIELD_TEMPERATURE, _dptr(T)), "set_field")
+
+    def create_rhs(self, dst, src, heat_source=None):
+        """dst += -R(T): Newton residual with T the operator's temperature and
+        src = T_old (heat_diffuse_operator.cpp:783-806)."""
+        A.check(A.lib().mpdg_create_rhs(self._h, _dptr(dst), _dptr(src), _dptr(heat_source)), "create_rhs")
+
+
+class AdvectionDiffusionOperator(_MatrixFreeOperator):
+    """theta-scheme advection-diffusion tangent
+    (source/level_set/advection_diffusion_operator.cpp): v = u/dt + theta vel.grad u,
+    g = theta D grad u."""
+
+    def __init__(self, mesh, dt, theta=0.5, diffusivity=0.0, velocity=None,
+                 precisions=("fp64",)):
+        vk, vp = _velocity(velocity)
+        d = A.OpDesc(A.OP_ADVDIFF, dt, 0.0, 0.0, 0.0, 0, theta, diffusivity, vk,
+                     (C.c_double * 3)(*vp), 0)
+        super().__init__(mesh, d, precisions)
+
+    def create_rhs(self, dst, src):
+        """dst += phi_old/dt N - (1-theta) vel.grad phi_old N - (1-theta) D grad phi_old.grad N
+        (advection_diffusion_operator.cpp:276-358)."""
+        A.check(A.lib().mpdg_create_rhs(self._h, _dptr(dst), _dptr(src), None), "create_rhs")
+
+
+def _velocity(v):
+    if v is None:
+        return A.VEL_NONE, (0.0, 0.0, 0.0)
+    if isinstance(v, str):
+        if v == "vortex":
+            return A.VEL_VORTEX, (0.0, 0.0, 0.0)
+        raise ValueError(v)
+    if isinstance(v, tuple) and v and v[0] == "rotation":
+        return A.VEL_ROTATION, (float(v[1]), 0.0, 0.0)
+    vals = tuple(float(x) for x in v)
+    return A.VEL_CONST, vals
+
+
+@dataclass
+class LinearSolverData:
+    """LinearSolverData (include/meltpooldg/linear_algebra/linear_solver_data.hpp:38-51)
+    plus the device-only Chebyshev and mixed-precision settings."""
+    solver_type: str = "GMRES"
+    preconditioner_type: str = "Diagonal"
+    max_iterations: int = 10000
+    rel_tolerance: float = 1e-12
+    abs_tolerance: float = 1e-20
+    gmres_restart: int = 30
+    chebyshev_degree: int = 5
+    lanczos_steps: int = 10
+    chebyshev_range: float = 30.0
+    chebyshev_safety: float = 1.2
+    mixed_precision: bool = False
+    inner_tolerance: float = 1e-4
+    max_outer: int = 20
+
+    def desc(self):
+        d = A.SolverDesc()
+        A.lib().mpdg_solver_desc_default(C.byref(d))
+        d.solver = A.SOLVER_CG if self.solver_type == "CG" else A.SOLVER_GMRES
+        d.preconditioner = {"Identity": A.PREC_IDENTITY, "Diagonal": A.PREC_JACOBI,
+                            "Chebyshev": A.PREC_CHEBYSHEV}[self.preconditioner_type]
+        d.max_iterations = self.max_iterations
+        d.rel_tolerance = self.rel_tolerance
+        d.abs_tolerance = self.abs_tolerance
+        d.gmres_restart = self.gmres_restart
+        d.chebyshev_degree = self.chebyshev_degree
+        d.lanczos_steps = self.lanczos_steps
+        d.chebyshev_range = self.chebyshev_range
+        d.chebyshev_safety = self.chebyshev_safety
+        d.mixed_precision = int(self.mixed_precision)
+        d.inner_tolerance = self.inner_tolerance
+        d.max_outer = self.max_outer
+        return d
+
+
+class LinearSolver:
+    """LinearSolver::solve (include/meltpooldg/linear_algebra/linear_solver.hpp:26-134):
+    returns the iteration count, raises NoConvergence when the limit is hit."""
+
+    last_report: dict = {}
+
+    @staticmethod
+    def solve(op, solution, rhs, data: LinearSolverData = None):
+        data = data or LinearSolverData()
+        rep = A.SolveReport()
+        st = A.lib().mpdg_solve(op._h, C.byref(data.desc()), _dptr(solution), _dptr(rhs), C.byref(rep))
+        LinearSolver.last_report = rep.as_dict()
+        A.check(st, "LinearSolver::solve")
+        return rep.iterations
+
+    @staticmethod
+    def solve_host(op, solution: np.ndarray, rhs: np.ndarray, data: LinearSolverData = None):
+        data = data or LinearSolverData()
+        rep = A.SolveReport()
+        dp = C.POINTER(C.c_double)
+        st = A.lib().mpdg_solve_host(op._h, C.byref(data.desc()), solution.ctypes.data_as(dp),
+                                     rhs.ctypes.data_as(dp), C.byref(rep))
+        LinearSolver.last_report = rep.as_dict()
+        A.check(st, "LinearSolver::solve_host")
+        return rep.iterations

@@ -1,0 +1,142 @@
+"""Replays of the reference's golden integration cases with the CPU oracle
+(TEST INFRASTRUCTURE ONLY).
+
+Each driver rebuilds a reference application case from its parameter file and
+case source and returns the quantity the reference prints per time step, so
+that the oracle can be pinned against the committed .output digits:
+
+* advection_diffusion_vortex (applications/mp-advec-diff/cases/advection_diffusion_vortex.hpp):
+  domain [-1,1]^dim refined `refinements` times, FE_Q(1); tanh level set
+  around a sphere of radius 0.25 (:33-73); rotating velocity s*(y,-x) with
+  s = 4 (:75-100, :291); inflow faces selected by face centre (:170-193) with
+  Dirichlet value -1 (:158); Crank-Nicolson (theta = 0.5), D = 0, dt = 0.01,
+  GMRES + Diagonal at rel. tol. 1e-12 (advection_diffusion_data.cpp:11-12,
+  linear_solver_data.hpp:38-51); the per-step solve follows
+  source/level_set/advection_diffusion_operation.cpp:227-367 with the
+  Dirichlet lifting of include/meltpooldg/linear_algebra/utilities_matrixfree.hpp:39-101;
+  printed value: the integrated L2 norm of the advected field (:331-342).
+* unidirectional_heat_transfer
+  (applications/mp-heat-transfer/cases/unidirectional_heat_transfer/unidirectional_heat_transfer.cpp):
+  [0,0.1]^2 refined 5 times, FE_Q(1), T0 = x (LinearTemp(0, 0.1), :27-47),
+  single-phase material, Newton-Raphson (source/linear_algebra/newton_raphson_solver.cpp:24-80)
+  with GMRES + Diagonal (heat_data.cpp:11-12); optional convective (Robin)
+  boundary on the right face (:217-221) with T0 = 1000 (:233-236); printed
+  value: integrated L2 norm of T after Newton convergence.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import oracle as O
+
+
+def vortex_inflow_mask(mesh: O.Mesh, lo=-1.0, hi=1.0):
+    """DoFs on faces whose centre satisfies the inflow rule of
+    advection_diffusion_vortex.hpp:170-193."""
+    dim, p = mesh.dim, mesh.degree
+    coords = mesh.vert
+    nc = mesh.nc
+    nv = [nc[d] + 1 for d in range(dim)]
+    gi = mesh.grid_index()
+    mask = np.zeros(mesh.n_dofs, dtype=bool)
+    half = 0.5 * (lo + hi)
+
+    def vid(c):
+        v = 0
+        for d in reversed(range(dim)):
+            v = v * nv[d] + c[d]
+        return v
+
+    for d in range(dim):
+        for s in (0, 1):
+            # enumerate boundary faces orthogonal to d on side s
+            tang = [t for t in range(dim) if t != d]
+            ranges = [range(nc[t]) for t in tang]
+            for cell_t in np.ndindex(*[len(r) for r in ranges]):
+                corners = []
+                for off in np.ndindex(*([2] * len(tang))):
+                    c = [0] * dim
+                    c[d] = 0 if s == 0 else nc[d]
+                    for a, t in enumerate(tang):
+                        c[t] = cell_t[a] + off[a]
+                    corners.append(coords[vid(c)])
+                centre = np.mean(corners, axis=0)
+                inflow = ((centre[0] == lo and centre[dim - 1] >= half)
+                          or (centre[0] == hi and centre[dim - 1] <= half)
+                          or (centre[dim - 1] == hi and centre[0] >= half)
+                          or (centre[dim - 1] == lo and centre[0] <= half))
+                if not inflow:
+                    continue
+                sel = gi[:, d] == (0 if s == 0 else mesh.shape[d] - 1)
+                for a, t in enumerate(tang):
+                    sel &= (gi[:, t] >= cell_t[a] * p) & (gi[:, t] <= (cell_t[a] + 1) * p)
+                mask |= sel
+    return mask.astype(np.uint8)
+
+
+def vortex_setup(dim, refinements, degree=1):
+    n = 2 ** refinements
+    mesh = O.Mesh.box(dim, degree, [n] * dim, lo=[-1.0] * dim, hi=[1.0] * dim)
+    h = 2.0 / n
+    eps = 0.5 * (h * np.sqrt(dim)) / np.sqrt(dim)  # 0.5 * minimal diameter / sqrt(dim)
+    centre = np.zeros(dim)
+    centre[dim - 1] = 0.5
+    x = mesh.dof_coordinates()
+    sd = 0.25 - np.linalg.norm(x - centre, axis=1)
+    phi0 = np.tanh(sd / (2.0 * eps))
+    mask = vortex_inflow_mask(mesh)
+    return mesh, phi0, mask
+
+
+def vortex_case(dim, refinements, n_steps=5, dt=0.01, velocity_scale=4.0, theta=0.5,
+                diffusivity=0.0, solver=None):
+    """Returns the per-step integrated L2 norms.  `solver(op, rhs, x0, inv)` can
+    replace the oracle GMRES (used to drive the GPU path through the same case)."""
+    mesh, phi, mask = vortex_setup(dim, refinements)
+    phi = phi.copy()
+    phi[mask == 1] = -1.0
+    op_nobc = O.Operator(O.ADVDIFF, dt, theta=theta, diffusivity=diffusivity,
+                         vel_kind=O.VEL_ROTATION, vel_param=(velocity_scale, 0.0, 0.0))
+    op = op_nobc.with_dirichlet(mask)
+    bc = np.where(mask == 1, -1.0, 0.0)
+    norms = []
+    for _ in range(n_steps):
+        temp = -O.vmult(mesh, op_nobc, bc)
+        O.rhs_advdiff(mesh, op_nobc, phi, dst=temp)
+        temp[mask == 1] = 0.0
+        inv = O.inverse_diagonal(mesh, op)
+        x, it, hist, ok = O.gmres(mesh, op, temp, x0=phi, inv_diag=inv, rel_tol=1e-12,
+                                  abs_tol=1e-20)
+        assert ok
+        x[mask == 1] = -1.0
+        norms.append(O.l2_norm(mesh, x))
+        phi = x
+    return norms
+
+
+def unidirectional_heat_case(n_steps=5, dt=1e-4, k=1.0, rho=1.0, cp=1.0, convection=0.0,
+                             t_inf=300.0, refinements=5):
+    """Returns the per-step integrated L2 norms of T after Newton convergence."""
+    n = 2 ** refinements
+    mesh = O.Mesh.box(2, 1, [n, n], lo=[0.0, 0.0], hi=[0.1, 0.1])
+    x = mesh.dof_coordinates()
+    T = np.full(mesh.n_dofs, 1000.0) if convection > 0.0 else x[:, 0].copy()
+    robin_faces = (1 << (2 * 0 + 1)) if convection > 0.0 else 0
+    norms = []
+    for _ in range(n_steps):
+        T_old = T.copy()
+        op = O.Operator(O.HEAT, dt, rho_cp=rho * cp, k0=k, temperature=T,
+                        robin_alpha=convection, robin_t_inf=t_inf, robin_faces=robin_faces)
+        inv = O.inverse_diagonal(mesh, op)
+        for _it in range(10):
+            op = op.with_temperature(T)
+            rhs = O.rhs_heat(mesh, op, T_old)
+            dx, _, _, ok = O.gmres(mesh, op, rhs, inv_diag=inv, rel_tol=1e-12, abs_tol=1e-20)
+            assert ok
+            if np.linalg.norm(rhs) < 5e-9 and np.linalg.norm(dx) < 1e-10:
+                break
+            T = T + dx
+        else:
+            raise RuntimeError("Newton did not converge")
+        norms.append(O.l2_norm(mesh, T))
+    return norms

@@ -1,0 +1,1106 @@
+/*
+ * mpdg_oracle.c -- FP64 CPU restatement of MeltPoolDG's matrix-free heat and
+ * advection-diffusion operators.  TEST INFRASTRUCTURE ONLY (the checker of the
+ * CUDA path; see mpdg_oracle.h for the reference call sites restated here).
+ *
+ * Two independent evaluation routes are provided:
+ *   orc_vmult        sum factorisation: nodal values -> (S,D) 1D contractions ->
+ *                    quadrature-point kernel -> transposed contractions
+ *                    (what deal.II's FEEvaluation::evaluate/integrate computes);
+ *   orc_vmult_brute  dense element matrices assembled from full tensor
+ *                    quadrature, like the reference's matrix-based path
+ *                    source/level_set/advection_diffusion_operator.cpp:78-206.
+ * Both follow the same operator definitions:
+ *   heat     v = rho_cp/dt u + rho_cp (vel . grad u),  g = k(T) grad u
+ *            (+ dk/dT grad T u with full_tangent)         heat_diffuse_operator.cpp:1029-1078
+ *            Robin face term alpha u v                    heat_diffuse_operator.cpp:1088-1129
+ *   advdiff  v = u/dt + theta (vel . grad u), g = theta D grad u
+ *                                                         advection_diffusion_operator.cpp:471-493
+ * Constrained (Dirichlet) DoFs are read as zero and never written, which is
+ * what MatrixFree::loop with read_dof_values/distribute_local_to_global does.
+ */
+#include "mpdg_oracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define MAXN 10
+#define MAXN3 (MAXN * MAXN * MAXN)
+
+/* ------------------------------------------------------------------ 1D rules */
+
+static void legendre_eval(int n, double x, double *p, double *dp)
+{
+  /* P_n and P_n' on [-1,1] by the three-term recurrence */
+  double p0 = 1.0, p1 = x;
+  if (n == 0) { *p = 1.0; *dp = 0.0; return; }
+  for (int k = 2; k <= n; ++k) {
+    double pk = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+    p0 = p1;
+    p1 = pk;
+  }
+  *p = p1;
+  *dp = (fabs(x) < 1.0) ? n * (x * p1 - p0) / (x * x - 1.0) : 0.5 * x * n * (n + 1.0);
+  if (fabs(x) >= 1.0) *dp = (x > 0 ? 1.0 : ((n % 2) ? 1.0 : -1.0)) * 0.5 * n * (n + 1.0);
+}
+
+void orc_gauss_legendre(int n, double *x, double *w)
+{
+  for (int i = 0; i < n; ++i) {
+    double z = cos(M_PI * (i + 0.75) / (n + 0.5)), p, dp;
+    for (int it = 0; it < 100; ++it) {
+      legendre_eval(n, z, &p, &dp);
+      double dz = p / dp;
+      z -= dz;
+      if (fabs(dz) < 1e-16) break;
+    }
+    legendre_eval(n, z, &p, &dp);
+    /* ascending order on [0,1] */
+    x[n - 1 - i] = 0.5 * (1.0 + z);
+    w[n - 1 - i] = 1.0 / ((1.0 - z * z) * dp * dp); /* = 2/((1-z^2)P'^2) / 2 */
+  }
+}
+
+void orc_gauss_lobatto(int n, double *x)
+{
+  /* endpoints plus the roots of P'_{n-1}; (1-z^2) P''_m = 2 z P'_m - m(m+1) P_m */
+  const int m = n - 1;
+  x[0] = 0.0;
+  x[n - 1] = 1.0;
+  for (int i = 1; i < n - 1; ++i) {
+    double z = -cos(M_PI * i / m), p, dp;
+    for (int it = 0; it < 100; ++it) {
+      legendre_eval(m, z, &p, &dp);
+      double ddp = (2.0 * z * dp - m * (m + 1.0) * p) / (1.0 - z * z);
+      double dz = dp / ddp;
+      z -= dz;
+      if (fabs(dz) < 1e-16) break;
+    }
+    x[i] = 0.5 * (1.0 + z);
+  }
+}
+
+void orc_shape_tables(int n, const double *xq, int nq, double *S, double *D)
+{
+  double z[MAXN];
+  orc_gauss_lobatto(n, z);
+  for (int q = 0; q < nq; ++q)
+    for (int i = 0; i < n; ++i) {
+      double v = 1.0, d = 0.0;
+      for (int j = 0; j < n; ++j)
+        if (j != i) v *= (xq[q] - z[j]) / (z[i] - z[j]);
+      for (int k = 0; k < n; ++k) {
+        if (k == i) continue;
+        double t = 1.0 / (z[i] - z[k]);
+        for (int j = 0; j < n; ++j)
+          if (j != i && j != k) t *= (xq[q] - z[j]) / (z[i] - z[j]);
+        d += t;
+      }
+      S[q * n + i] = v;
+      D[q * n + i] = d;
+    }
+}
+
+/* -------------------------------------------------------------- mesh helpers */
+
+typedef struct {
+  int dim, p, n;      /* n = p + 1 points per direction */
+  int nc[3];
+  long NX, NY, NZ, N;
+  long n_cells;
+  double xq[MAXN], wq[MAXN];
+  double S[MAXN * MAXN], D[MAXN * MAXN];
+} geo_t;
+
+static void geo_init(const orc_mesh *m, geo_t *g)
+{
+  g->dim = m->dim;
+  g->p = m->degree;
+  g->n = m->degree + 1;
+  g->nc[0] = m->nc[0];
+  g->nc[1] = m->nc[1];
+  g->nc[2] = (m->dim == 3) ? m->nc[2] : 1;
+  g->NX = (long)g->nc[0] * g->p + 1;
+  g->NY = (long)g->nc[1] * g->p + 1;
+  g->NZ = (m->dim == 3) ? (long)g->nc[2] * g->p + 1 : 1;
+  g->N = g->NX * g->NY * g->NZ;
+  g->n_cells = (long)g->nc[0] * g->nc[1] * g->nc[2];
+  orc_gauss_legendre(g->n, g->xq, g->wq);
+  orc_shape_tables(g->n, g->xq, g->n, g->S, g->D);
+}
+
+long orc_n_dofs(const orc_mesh *m)
+{
+  geo_t g;
+  geo_init(m, &g);
+  return g.N;
+}
+
+static long vert_index(const geo_t *g, int vx, int vy, int vz)
+{
+  return ((long)vz * (g->nc[1] + 1) + vy) * (g->nc[0] + 1) + vx;
+}
+
+/* vertices of cell (ix,iy,iz): vc[c][a], c = bx + 2 by + 4 bz */
+static void cell_vertices(const orc_mesh *m, const geo_t *g, int ix, int iy, int iz,
+                          double vc[8][3])
+{
+  const int nv = (g->dim == 3) ? 8 : 4;
+  for (int c = 0; c < nv; ++c) {
+    long v = vert_index(g, ix + (c & 1), iy + ((c >> 1) & 1), iz + ((c >> 2) & 1));
+    for (int a = 0; a < 3; ++a) vc[c][a] = (a < g->dim) ? m->vert[v * g->dim + a] : 0.0;
+  }
+}
+
+/* multilinear map at reference point xi: position x and Jacobian J[a][b] = dx_a/dxi_b */
+static void map_point(const geo_t *g, double vc[8][3], const double xi[3], double x[3],
+                      double J[3][3])
+{
+  const int dim = g->dim, nv = 1 << dim;
+  for (int a = 0; a < 3; ++a) {
+    x[a] = 0.0;
+    for (int b = 0; b < 3; ++b) J[a][b] = 0.0;
+  }
+  for (int c = 0; c < nv; ++c) {
+    double f[3], df[3];
+    for (int d = 0; d < dim; ++d) {
+      int bit = (c >> d) & 1;
+      f[d] = bit ? xi[d] : 1.0 - xi[d];
+      df[d] = bit ? 1.0 : -1.0;
+    }
+    double B = 1.0;
+    for (int d = 0; d < dim; ++d) B *= f[d];
+    for (int b = 0; b < dim; ++b) {
+      double dB = df[b];
+      for (int d = 0; d < dim; ++d)
+        if (d != b) dB *= f[d];
+      for (int a = 0; a < dim; ++a) J[a][b] += vc[c][a] * dB;
+    }
+    for (int a = 0; a < dim; ++a) x[a] += vc[c][a] * B;
+  }
+  if (dim == 2) J[2][2] = 1.0;
+}
+
+/* inverse and determinant of a 3x3 (2D embedded with J[2][2] = 1) */
+static double inverse3(double J[3][3], double Ji[3][3])
+{
+  double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+               J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+               J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  double id = 1.0 / det;
+  Ji[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) * id;
+  Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+  Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+  Ji[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) * id;
+  Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+  Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+  Ji[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) * id;
+  Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+  Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  return det;
+}
+
+static void cell_dofs(const geo_t *g, int ix, int iy, int iz, long *idx)
+{
+  const int n = g->n, nz = (g->dim == 3) ? n : 1;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i)
+        idx[(k * n + j) * n + i] =
+          ((long)(iz * g->p + k) * g->NY + (iy * g->p + j)) * g->NX + (ix * g->p + i);
+}
+
+void orc_dof_coordinates(const orc_mesh *m, double *xyz)
+{
+  geo_t g;
+  geo_init(m, &g);
+  double z[MAXN];
+  orc_gauss_lobatto(g.n, z);
+  const int nz = (g.dim == 3) ? g.n : 1;
+  for (int iz = 0; iz < g.nc[2]; ++iz)
+    for (int iy = 0; iy < g.nc[1]; ++iy)
+      for (int ix = 0; ix < g.nc[0]; ++ix) {
+        double vc[8][3];
+        long idx[MAXN3];
+        cell_vertices(m, &g, ix, iy, iz, vc);
+        cell_dofs(&g, ix, iy, iz, idx);
+        for (int k = 0; k < nz; ++k)
+          for (int j = 0; j < g.n; ++j)
+            for (int i = 0; i < g.n; ++i) {
+              double xi[3] = {z[i], z[j], (g.dim == 3) ? z[k] : 0.0}, x[3], J[3][3];
+              map_point(&g, vc, xi, x, J);
+              long gi = idx[(k * g.n + j) * g.n + i];
+              for (int a = 0; a < g.dim; ++a) xyz[gi * g.dim + a] = x[a];
+            }
+      }
+}
+
+/* ---------------------------------------------------------- velocity at a point */
+
+static void velocity_at(const orc_op *op, int dim, const double x[3], double u[3])
+{
+  u[0] = u[1] = u[2] = 0.0;
+  switch (op->vel_kind) {
+    case ORC_VEL_ROTATION: {
+      const double s = op->vel_param[0];
+      u[0] = s * x[dim - 1];
+      u[dim - 1] = -s * x[0];
+      break;
+    }
+    case ORC_VEL_VORTEX:
+      u[0] = sin(M_PI * x[0]) * cos(M_PI * x[1]);
+      u[1] = -cos(M_PI * x[0]) * sin(M_PI * x[1]);
+      break;
+    case ORC_VEL_CONST:
+      for (int d = 0; d < dim; ++d) u[d] = op->vel_param[d];
+      break;
+    default:
+      break;
+  }
+}
+
+/* ----------------------------------------------------- sum factorisation kernels */
+
+/* out = M (n x n, row = output point) applied along direction dir; transpose: M^T */
+static void contract(const geo_t *g, const double *M, int transpose, int dir, const double *in,
+                     double *out)
+{
+  const int n = g->n, nz = (g->dim == 3) ? n : 1;
+  const int ext[3] = {n, n, nz};
+  const int stride[3] = {1, n, n * n};
+  const int total = n * n * nz;
+  for (int t = 0; t < total; ++t) {
+    int c[3] = {t % n, (t / n) % n, t / (n * n)};
+    double s = 0.0;
+    int base = t - c[dir] * stride[dir];
+    for (int r = 0; r < ext[dir]; ++r) {
+      double a = transpose ? M[r * n + c[dir]] : M[c[dir] * n + r];
+      s += a * in[base + r * stride[dir]];
+    }
+    out[t] = s;
+  }
+}
+
+/* values and reference gradients at the quadrature points */
+static void evaluate(const geo_t *g, const double *u, double *val, double grad[3][MAXN3])
+{
+  double t1[MAXN3], t2[MAXN3];
+  const int dim = g->dim;
+  /* value: S along every direction */
+  if (val) {
+    contract(g, g->S, 0, 0, u, t1);
+    contract(g, g->S, 0, 1, t1, (dim == 3) ? t2 : val);
+    if (dim == 3) contract(g, g->S, 0, 2, t2, val);
+  }
+  if (grad)
+    for (int b = 0; b < dim; ++b) {
+      const double *M0 = (b == 0) ? g->D : g->S;
+      const double *M1 = (b == 1) ? g->D : g->S;
+      const double *M2 = (b == 2) ? g->D : g->S;
+      contract(g, M0, 0, 0, u, t1);
+      contract(g, M1, 0, 1, t1, (dim == 3) ? t2 : grad[b]);
+      if (dim == 3) contract(g, M2, 0, 2, t2, grad[b]);
+    }
+}
+
+/* out += S^T(val) + sum_b D_b^T(grad[b]) */
+static void integrate(const geo_t *g, const double *val, double grad[3][MAXN3], double *out)
+{
+  double t1[MAXN3], t2[MAXN3];
+  const int dim = g->dim, n = g->n, nz = (dim == 3) ? n : 1, total = n * n * nz;
+  for (int b = -1; b < dim; ++b) {
+    const double *src = (b < 0) ? val : grad[b];
+    if (!src) continue;
+    const double *M0 = (b == 0) ? g->D : g->S;
+    const double *M1 = (b == 1) ? g->D : g->S;
+    const double *M2 = (b == 2) ? g->D : g->S;
+    if (dim == 3) {
+      contract(g, M2, 1, 2, src, t1);
+      contract(g, M1, 1, 1, t1, t2);
+      contract(g, M0, 1, 0, t2, t1);
+    } else {
+      contract(g, M1, 1, 1, src, t2);
+      contract(g, M0, 1, 0, t2, t1);
+    }
+    for (int t = 0; t < total; ++t) out[t] += t1[t];
+  }
+}
+
+/* per-cell quadrature-point data shared by the tangent, the residual and the diagonal */
+typedef struct {
+  double JxW, Ji[3][3], x[3], vel[3];
+  double T, gradT[3]; /* physical */
+} qdata_t;
+
+static void cell_qdata(const orc_mesh *m, const orc_op *op, const geo_t *g, int ix, int iy,
+                       int iz, const long *idx, qdata_t *qd)
+{
+  const int n = g->n, dim = g->dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+  double vc[8][3];
+  cell_vertices(m, g, ix, iy, iz, vc);
+  /* temperature at the quadrature points (values and reference gradients) */
+  double Tl[MAXN3], Tv[MAXN3], Tg[3][MAXN3];
+  int haveT = op->temperature != NULL;
+  if (haveT) {
+    for (int t = 0; t < nqt; ++t) Tl[t] = op->temperature[idx[t]];
+    evaluate(g, Tl, Tv, Tg);
+  }
+  double Vv[3][MAXN3];
+  if (op->vel_kind == ORC_VEL_NODAL)
+    for (int d = 0; d < dim; ++d) {
+      double Vl[MAXN3];
+      for (int t = 0; t < nqt; ++t) Vl[t] = op->vel_nodal[(long)d * g->N + idx[t]];
+      evaluate(g, Vl, Vv[d], NULL);
+    }
+  for (int qz = 0; qz < nz; ++qz)
+    for (int qy = 0; qy < n; ++qy)
+      for (int qx = 0; qx < n; ++qx) {
+        int q = (qz * n + qy) * n + qx;
+        double xi[3] = {g->xq[qx], g->xq[qy], (dim == 3) ? g->xq[qz] : 0.0};
+        double w = g->wq[qx] * g->wq[qy] * ((dim == 3) ? g->wq[qz] : 1.0);
+        double J[3][3];
+        map_point(g, vc, xi, qd[q].x, J);
+        double det = inverse3(J, qd[q].Ji);
+        qd[q].JxW = det * w;
+        if (op->vel_kind == ORC_VEL_NODAL) {
+          for (int d = 0; d < 3; ++d) qd[q].vel[d] = (d < dim) ? Vv[d][q] : 0.0;
+        } else {
+          velocity_at(op, dim, qd[q].x, qd[q].vel);
+        }
+        qd[q].T = haveT ? Tv[q] : 0.0;
+        for (int a = 0; a < 3; ++a) {
+          double s = 0.0;
+          if (haveT)
+            for (int b = 0; b < dim; ++b) s += qd[q].Ji[b][a] * Tg[b][q];
+          qd[q].gradT[a] = (a < dim) ? s : 0.0;
+        }
+      }
+}
+
+/* quadrature-point kernel of the tangent: returns value coefficient v and the
+ * physical flux f for the trial value u and physical gradient gu */
+static void tangent_qp(const orc_op *op, int dim, const qdata_t *qd, double u, const double gu[3],
+                       double *v, double f[3])
+{
+  double vgu = 0.0;
+  for (int a = 0; a < dim; ++a) vgu += qd->vel[a] * gu[a];
+  if (op->kind == ORC_HEAT) {
+    const double k = op->k0 * (1.0 + op->k_alpha * qd->T);
+    const double dk = op->k0 * op->k_alpha;
+    *v = op->rho_cp / op->dt * u + op->rho_cp * vgu;
+    for (int a = 0; a < 3; ++a)
+      f[a] = k * gu[a] + (op->full_tangent ? dk * qd->gradT[a] * u : 0.0);
+  } else {
+    *v = u / op->dt + op->theta * vgu;
+    for (int a = 0; a < 3; ++a) f[a] = op->theta * op->diffusivity * gu[a];
+  }
+}
+
+static int cell_colour(int ix, int iy, int iz) { return (ix & 1) | ((iy & 1) << 1) | ((iz & 1) << 2); }
+
+/* one cell of the sum-factorised tangent; adds into dst (caller guarantees no race) */
+static void apply_cell(const orc_mesh *m, const orc_op *op, const geo_t *g, int ix, int iy,
+                       int iz, double *dst, const double *src)
+{
+  const int n = g->n, dim = g->dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+  long idx[MAXN3];
+  cell_dofs(g, ix, iy, iz, idx);
+  static __thread qdata_t qd[MAXN3];
+  cell_qdata(m, op, g, ix, iy, iz, idx, qd);
+  double ul[MAXN3], uv[MAXN3], ug[3][MAXN3], out[MAXN3];
+  for (int t = 0; t < nqt; ++t)
+    ul[t] = (op->dirichlet && op->dirichlet[idx[t]]) ? 0.0 : src[idx[t]];
+  evaluate(g, ul, uv, ug);
+  for (int q = 0; q < nqt; ++q) {
+    double gu[3] = {0, 0, 0}, v, f[3];
+    for (int a = 0; a < dim; ++a)
+      for (int b = 0; b < dim; ++b) gu[a] += qd[q].Ji[b][a] * ug[b][q];
+    tangent_qp(op, dim, &qd[q], uv[q], gu, &v, f);
+    uv[q] = v * qd[q].JxW;
+    for (int b = 0; b < dim; ++b) {
+      double s = 0.0;
+      for (int a = 0; a < dim; ++a) s += qd[q].Ji[b][a] * f[a];
+      ug[b][q] = s * qd[q].JxW;
+    }
+  }
+  memset(out, 0, sizeof(double) * nqt);
+  integrate(g, uv, ug, out);
+  for (int t = 0; t < nqt; ++t)
+    if (!(op->dirichlet && op->dirichlet[idx[t]])) dst[idx[t]] += out[t];
+}
+
+/* ------------------------------------------------------------ Robin faces (heat) */
+
+/* face f of a cell: direction d, side s; returns the n^(dim-1) local dof indices,
+ * face quadrature JxW and point coordinates; values of the face shape functions
+ * are products of 1D S tables (nodal on GL nodes, so the face trace uses the
+ * face's own dofs only). */
+static void robin_face_matrix_apply(const orc_mesh *m, const geo_t *g, int ix, int iy, int iz,
+                                    int d, int s, double alpha, const double *ul_cell,
+                                    double *out_cell, double *diag_cell)
+{
+  const int n = g->n, dim = g->dim;
+  double vc[8][3];
+  cell_vertices(m, g, ix, iy, iz, vc);
+  int t0 = (d == 0) ? 1 : 0;           /* tangential directions */
+  int t1 = (dim == 3) ? ((d == 2) ? 1 : 2) : -1;
+  const int nq1 = (dim == 3) ? n : 1;
+  for (int qb = 0; qb < nq1; ++qb)
+    for (int qa = 0; qa < n; ++qa) {
+      double xi[3] = {0, 0, 0};
+      xi[d] = s ? 1.0 : 0.0;
+      xi[t0] = g->xq[qa];
+      if (t1 >= 0) xi[t1] = g->xq[qb];
+      double x[3], J[3][3];
+      map_point(g, vc, xi, x, J);
+      double w = g->wq[qa] * ((t1 >= 0) ? g->wq[qb] : 1.0), ds;
+      if (dim == 2) {
+        ds = sqrt(J[0][t0] * J[0][t0] + J[1][t0] * J[1][t0]);
+      } else {
+        double a0[3] = {J[0][t0], J[1][t0], J[2][t0]}, a1[3] = {J[0][t1], J[1][t1], J[2][t1]};
+        double c[3] = {a0[1] * a1[2] - a0[2] * a1[1], a0[2] * a1[0] - a0[0] * a1[2],
+                       a0[0] * a1[1] - a0[1] * a1[0]};
+        ds = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+      }
+      const double JxW = ds * w;
+      /* face dofs: local index with coordinate d fixed to 0 or p */
+      double uq = 0.0;
+      const int nb = (dim == 3) ? n : 1;
+      for (int b = 0; b < nb; ++b)
+        for (int a = 0; a < n; ++a) {
+          int c[3] = {0, 0, 0};
+          c[d] = s ? n - 1 : 0;
+          c[t0] = a;
+          if (t1 >= 0) c[t1] = b;
+          int li = (c[2] * n + c[1]) * n + c[0];
+          double phi = g->S[qa * n + a] * ((t1 >= 0) ? g->S[qb * n + b] : 1.0);
+          if (ul_cell) uq += phi * ul_cell[li];
+          if (diag_cell) diag_cell[li] += alpha * phi * phi * JxW;
+        }
+      if (out_cell)
+        for (int b = 0; b < nb; ++b)
+          for (int a = 0; a < n; ++a) {
+            int c[3] = {0, 0, 0};
+            c[d] = s ? n - 1 : 0;
+            c[t0] = a;
+            if (t1 >= 0) c[t1] = b;
+            int li = (c[2] * n + c[1]) * n + c[0];
+            double phi = g->S[qa * n + a] * ((t1 >= 0) ? g->S[qb * n + b] : 1.0);
+            out_cell[li] += alpha * uq * phi * JxW;
+          }
+    }
+}
+
+static int cell_on_face(const geo_t *g, int ix, int iy, int iz, int d, int s)
+{
+  int c[3] = {ix, iy, iz};
+  return s ? (c[d] == g->nc[d] - 1) : (c[d] == 0);
+}
+
+static void apply_robin(const orc_mesh *m, const orc_op *op, const geo_t *g, double *dst,
+                        const double *src)
+{
+  if (op->kind != ORC_HEAT || !op->robin_faces || op->robin_alpha == 0.0) return;
+  const int n = g->n, dim = g->dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+  for (int iz = 0; iz < g->nc[2]; ++iz)
+    for (int iy = 0; iy < g->nc[1]; ++iy)
+      for (int ix = 0; ix < g->nc[0]; ++ix)
+        for (int d = 0; d < dim; ++d)
+          for (int s = 0; s < 2; ++s) {
+            if (!(op->robin_faces & (1 << (2 * d + s)))) continue;
+            if (!cell_on_face(g, ix, iy, iz, d, s)) continue;
+            long idx[MAXN3];
+            double ul[MAXN3], out[MAXN3];
+            cell_dofs(g, ix, iy, iz, idx);
+            for (int t = 0; t < nqt; ++t) {
+              ul[t] = (op->dirichlet && op->dirichlet[idx[t]]) ? 0.0 : src[idx[t]];
+              out[t] = 0.0;
+            }
+            robin_face_matrix_apply(m, g, ix, iy, iz, d, s, op->robin_alpha, ul, out, NULL);
+            for (int t = 0; t < nqt; ++t)
+              if (!(op->dirichlet && op->dirichlet[idx[t]])) dst[idx[t]] += out[t];
+          }
+}
+
+/* ------------------------------------------------------------------- vmult */
+
+void orc_vmult_cells(const orc_mesh *m, const orc_op *op, double *dst, const double *src,
+                     long cell_begin, long cell_end)
+{
+  geo_t g;
+  geo_init(m, &g);
+  const long nxy = (long)g.nc[0] * g.nc[1];
+  /* colour loop: cells of one parity colour share no DoF, so they may run in parallel */
+  for (int colour = 0; colour < 8; ++colour) {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long c = cell_begin; c < cell_end; ++c) {
+      int iz = (int)(c / nxy), iy = (int)((c / g.nc[0]) % g.nc[1]), ix = (int)(c % g.nc[0]);
+      if (cell_colour(ix, iy, iz) != colour) continue;
+      apply_cell(m, op, &g, ix, iy, iz, dst, src);
+    }
+  }
+}
+
+void orc_vmult(const orc_mesh *m, const orc_op *op, double *dst, const double *src)
+{
+  geo_t g;
+  geo_init(m, &g);
+  memset(dst, 0, sizeof(double) * g.N);
+  orc_vmult_cells(m, op, dst, src, 0, g.n_cells);
+  apply_robin(m, op, &g, dst, src);
+}
+
+/* ----------------------------------------------- brute-force element matrices */
+
+static void element_matrix(const orc_mesh *m, const orc_op *op, const geo_t *g, int ix, int iy,
+                           int iz, const long *idx, double *A /* nqt x nqt */)
+{
+  const int n = g->n, dim = g->dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+  double vc[8][3];
+  cell_vertices(m, g, ix, iy, iz, vc);
+  memset(A, 0, sizeof(double) * nqt * nqt);
+  static __thread double phi[MAXN3], gphi[MAXN3][3];
+  for (int qz = 0; qz < nz; ++qz)
+    for (int qy = 0; qy < n; ++qy)
+      for (int qx = 0; qx < n; ++qx) {
+        const int qq[3] = {qx, qy, qz};
+        double xi[3] = {g->xq[qx], g->xq[qy], (dim == 3) ? g->xq[qz] : 0.0};
+        double w = g->wq[qx] * g->wq[qy] * ((dim == 3) ? g->wq[qz] : 1.0);
+        qdata_t qd;
+        double J[3][3];
+        map_point(g, vc, xi, qd.x, J);
+        double det = inverse3(J, qd.Ji);
+        qd.JxW = det * w;
+        /* shape values and physical gradients by direct products */
+        for (int t = 0; t < nqt; ++t) {
+          int c[3] = {t % n, (t / n) % n, t / (n * n)};
+          double f[3], df[3];
+          for (int d = 0; d < 3; ++d) {
+            f[d] = (d < dim) ? g->S[qq[d] * n + c[d]] : 1.0;
+            df[d] = (d < dim) ? g->D[qq[d] * n + c[d]] : 0.0;
+          }
+          phi[t] = f[0] * f[1] * f[2];
+          double gr[3] = {df[0] * f[1] * f[2], f[0] * df[1] * f[2], f[0] * f[1] * df[2]};
+          for (int a = 0; a < 3; ++a) {
+            double s = 0.0;
+            for (int b = 0; b < dim; ++b) s += qd.Ji[b][a] * gr[b];
+            gphi[t][a] = (a < dim) ? s : 0.0;
+          }
+        }
+        /* fields at this point by direct summation */
+        qd.T = 0.0;
+        qd.gradT[0] = qd.gradT[1] = qd.gradT[2] = 0.0;
+        if (op->temperature)
+          for (int t = 0; t < nqt; ++t) {
+            double Tt = op->temperature[idx[t]];
+            qd.T += Tt * phi[t];
+            for (int a = 0; a < 3; ++a) qd.gradT[a] += Tt * gphi[t][a];
+          }
+        if (op->vel_kind == ORC_VEL_NODAL) {
+          for (int d = 0; d < 3; ++d) {
+            qd.vel[d] = 0.0;
+            if (d < dim)
+              for (int t = 0; t < nqt; ++t) qd.vel[d] += op->vel_nodal[(long)d * g->N + idx[t]] * phi[t];
+          }
+        } else {
+          velocity_at(op, dim, qd.x, qd.vel);
+        }
+        for (int j = 0; j < nqt; ++j) {
+          double v, fl[3];
+          tangent_qp(op, dim, &qd, phi[j], gphi[j], &v, fl);
+          for (int i = 0; i < nqt; ++i)
+            A[i * nqt + j] += (v * phi[i] + fl[0] * gphi[i][0] + fl[1] * gphi[i][1] +
+                               fl[2] * gphi[i][2]) * qd.JxW;
+        }
+      }
+}
+
+void orc_vmult_brute(const orc_mesh *m, const orc_op *op, double *dst, const double *src)
+{
+  geo_t g;
+  geo_init(m, &g);
+  const int n = g.n, nz = (g.dim == 3) ? n : 1, nqt = n * n * nz;
+  memset(dst, 0, sizeof(double) * g.N);
+  double *A = (double *)malloc(sizeof(double) * nqt * nqt);
+  for (int iz = 0; iz < g.nc[2]; ++iz)
+    for (int iy = 0; iy < g.nc[1]; ++iy)
+      for (int ix = 0; ix < g.nc[0]; ++ix) {
+        long idx[MAXN3];
+        cell_dofs(&g, ix, iy, iz, idx);
+        element_matrix(m, op, &g, ix, iy, iz, idx, A);
+        for (int i = 0; i < nqt; ++i) {
+          if (op->dirichlet && op->dirichlet[idx[i]]) continue;
+          double s = 0.0;
+          for (int j = 0; j < nqt; ++j)
+            if (!(op->dirichlet && op->dirichlet[idx[j]])) s += A[i * nqt + j] * src[idx[j]];
+          dst[idx[i]] += s;
+        }
+      }
+  free(A);
+  apply_robin(m, op, &g, dst, src);
+}
+
+/* ---------------------------------------------------------------- diagonal */
+
+void orc_diagonal(const orc_mesh *m, const orc_op *op, double *diag)
+{
+  geo_t g;
+  geo_init(m, &g);
+  const int n = g.n, dim = g.dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+  memset(diag, 0, sizeof(double) * g.N);
+  const long nxy = (long)g.nc[0] * g.nc[1];
+  for (int colour = 0; colour < 8; ++colour) {
+#pragma omp parallel
+    {
+      double *A = (double *)malloc(sizeof(double) * nqt * nqt);
+#pragma omp for schedule(dynamic, 16)
+      for (long c = 0; c < g.n_cells; ++c) {
+        int iz = (int)(c / nxy), iy = (int)((c / g.nc[0]) % g.nc[1]), ix = (int)(c % g.nc[0]);
+        if (cell_colour(ix, iy, iz) != colour) continue;
+        long idx[MAXN3];
+        cell_dofs(&g, ix, iy, iz, idx);
+        element_matrix(m, op, &g, ix, iy, iz, idx, A);
+        double dc[MAXN3];
+        for (int i = 0; i < nqt; ++i) dc[i] = A[i * nqt + i];
+        if (op->kind == ORC_HEAT && op->robin_faces && op->robin_alpha != 0.0)
+          for (int d = 0; d < dim; ++d)
+            for (int s = 0; s < 2; ++s)
+              if ((op->robin_faces & (1 << (2 * d + s))) && cell_on_face(&g, ix, iy, iz, d, s))
+                robin_face_matrix_apply(m, &g, ix, iy, iz, d, s, op->robin_alpha, NULL, NULL, dc);
+        for (int i = 0; i < nqt; ++i)
+          if (!(op->dirichlet && op->dirichlet[idx[i]])) diag[idx[i]] += dc[i];
+      }
+      free(A);
+    }
+  }
+  if (op->dirichlet)
+    for (long i = 0; i < g.N; ++i)
+      if (op->dirichlet[i]) diag[i] = 1.0;
+}
+
+/* inversion rules: heat_diffuse_operator.cpp:282-283 (|d| > 1e-10),
+ * advection_diffusion_operator.cpp:437-439 (|d| > 1e-14 max(1, |d|_inf)) */
+void orc_invert_diagonal(const orc_mesh *m, const orc_op *op, double *diag)
+{
+  const long N = orc_n_dofs(m);
+  double thr = 1e-10;
+  if (op->kind == ORC_ADVDIFF) {
+    double mx = 1.0;
+    for (long i = 0; i < N; ++i) mx = fmax(mx, fabs(diag[i]));
+    thr = 1e-14 * mx;
+  }
+  for (long i = 0; i < N; ++i) diag[i] = (fabs(diag[i]) > thr) ? 1.0 / diag[i] : 1.0;
+}
+
+/* -------------------------------------------------------------- residuals */
+
+void orc_rhs_heat(const orc_mesh *m, const orc_op *op, double *dst, const double *t_old,
+                  const double *heat_source, const unsigned char *scatter_mask)
+{
+  geo_t g;
+  geo_init(m, &g);
+  const int n = g.n, dim = g.dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+  const long nxy = (long)g.nc[0] * g.nc[1];
+  for (int colour = 0; colour < 8; ++colour) {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long c = 0; c < g.n_cells; ++c) {
+      int iz = (int)(c / nxy), iy = (int)((c / g.nc[0]) % g.nc[1]), ix = (int)(c % g.nc[0]);
+      if (cell_colour(ix, iy, iz) != colour) continue;
+      long idx[MAXN3];
+      cell_dofs(&g, ix, iy, iz, idx);
+      static __thread qdata_t qd[MAXN3];
+      cell_qdata(m, op, &g, ix, iy, iz, idx, qd);
+      double ol[MAXN3], ov[MAXN3], ql[MAXN3], qv[MAXN3], val[MAXN3], grd[3][MAXN3], out[MAXN3];
+      for (int t = 0; t < nqt; ++t) {
+        ol[t] = t_old[idx[t]];
+        ql[t] = heat_source ? heat_source[idx[t]] : 0.0;
+      }
+      evaluate(&g, ol, ov, NULL);
+      evaluate(&g, ql, qv, NULL);
+      for (int q = 0; q < nqt; ++q) {
+        const double k = op->k0 * (1.0 + op->k_alpha * qd[q].T);
+        double v = op->rho_cp / op->dt * (qd[q].T - ov[q]) - qv[q];
+        double vg = 0.0;
+        for (int a = 0; a < dim; ++a) vg += qd[q].gradT[a] * qd[q].vel[a];
+        v += op->rho_cp * vg;
+        val[q] = -v * qd[q].JxW;
+        for (int b = 0; b < dim; ++b) {
+          double s = 0.0;
+          for (int a = 0; a < dim; ++a) s += qd[q].Ji[b][a] * k * qd[q].gradT[a];
+          grd[b][q] = -s * qd[q].JxW;
+        }
+      }
+      memset(out, 0, sizeof(double) * nqt);
+      integrate(&g, val, grd, out);
+      for (int t = 0; t < nqt; ++t)
+        if (!(scatter_mask && scatter_mask[idx[t]])) dst[idx[t]] += out[t];
+    }
+  }
+  /* Robin faces: -alpha (T - T_inf) tested with N (heat_diffuse_operator.cpp:760-770) */
+  if (op->robin_faces && op->robin_alpha != 0.0) {
+    for (int iz = 0; iz < g.nc[2]; ++iz)
+      for (int iy = 0; iy < g.nc[1]; ++iy)
+        for (int ix = 0; ix < g.nc[0]; ++ix)
+          for (int d = 0; d < dim; ++d)
+            for (int s = 0; s < 2; ++s) {
+              if (!(op->robin_faces & (1 << (2 * d + s))) || !cell_on_face(&g, ix, iy, iz, d, s))
+                continue;
+              long idx[MAXN3];
+              double ul[MAXN3], out[MAXN3], one[MAXN3];
+              cell_dofs(&g, ix, iy, iz, idx);
+              for (int t = 0; t < nqt; ++t) {
+                ul[t] = -(op->temperature ? op->temperature[idx[t]] : 0.0);
+                one[t] = op->robin_t_inf;
+                out[t] = 0.0;
+              }
+              /* -alpha T + alpha T_inf (the constant is reproduced exactly by the nodal basis) */
+              for (int t = 0; t < nqt; ++t) ul[t] += one[t];
+              robin_face_matrix_apply(m, &g, ix, iy, iz, d, s, op->robin_alpha, ul, out, NULL);
+              for (int t = 0; t < nqt; ++t)
+                if (!(scatter_mask && scatter_mask[idx[t]])) dst[idx[t]] += out[t];
+            }
+  }
+}
+
+void orc_rhs_advdiff(const orc_mesh *m, const orc_op *op, double *dst, const double *phi_old,
+                     const unsigned char *scatter_mask)
+{
+  geo_t g;
+  geo_init(m, &g);
+  const int n = g.n, dim = g.dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+  const long nxy = (long)g.nc[0] * g.nc[1];
+  orc_op op2 = *op;
+  op2.temperature = NULL;
+  for (int colour = 0; colour < 8; ++colour) {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long c = 0; c < g.n_cells; ++c) {
+      int iz = (int)(c / nxy), iy = (int)((c / g.nc[0]) % g.nc[1]), ix = (int)(c % g.nc[0]);
+      if (cell_colour(ix, iy, iz) != colour) continue;
+      long idx[MAXN3];
+      cell_dofs(&g, ix, iy, iz, idx);
+      static __thread qdata_t qd[MAXN3];
+      cell_qdata(m, &op2, &g, ix, iy, iz, idx, qd);
+      double ul[MAXN3], uv[MAXN3], ug[3][MAXN3], out[MAXN3];
+      for (int t = 0; t < nqt; ++t) ul[t] = phi_old[idx[t]];
+      evaluate(&g, ul, uv, ug);
+      for (int q = 0; q < nqt; ++q) {
+        double gp[3] = {0, 0, 0}, vg = 0.0;
+        for (int a = 0; a < dim; ++a) {
+          for (int b = 0; b < dim; ++b) gp[a] += qd[q].Ji[b][a] * ug[b][q];
+          vg += qd[q].vel[a] * gp[a];
+        }
+        uv[q] = (uv[q] / op->dt - (1.0 - op->theta) * vg) * qd[q].JxW;
+        for (int b = 0; b < dim; ++b) {
+          double s = 0.0;
+          for (int a = 0; a < dim; ++a) s += qd[q].Ji[b][a] * gp[a];
+          ug[b][q] = -(1.0 - op->theta) * op->diffusivity * s * qd[q].JxW;
+        }
+      }
+      memset(out, 0, sizeof(double) * nqt);
+      integrate(&g, uv, ug, out);
+      for (int t = 0; t < nqt; ++t)
+        if (!(scatter_mask && scatter_mask[idx[t]])) dst[idx[t]] += out[t];
+    }
+  }
+}
+
+/* integrated L2 norm with QGauss(p+1): VectorTools::compute_norm,
+ * source/utilities/vector_tools.cpp:170-201 */
+/* per-cell integrated L2 norms (what VectorTools::integrate_difference writes
+ * into its Vector<float> of cell errors, before the float rounding) */
+void orc_l2_norm_cells(const orc_mesh *m, const double *u, double *cell_norms)
+{
+  geo_t g;
+  geo_init(m, &g);
+  const int n = g.n, dim = g.dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < g.n_cells; ++c) {
+    const long nxy = (long)g.nc[0] * g.nc[1];
+    int iz = (int)(c / nxy), iy = (int)((c / g.nc[0]) % g.nc[1]), ix = (int)(c % g.nc[0]);
+    long idx[MAXN3];
+    double ul[MAXN3], uv[MAXN3], vc[8][3];
+    cell_dofs(&g, ix, iy, iz, idx);
+    cell_vertices(m, &g, ix, iy, iz, vc);
+    for (int t = 0; t < nqt; ++t) ul[t] = u[idx[t]];
+    evaluate(&g, ul, uv, NULL);
+    double s = 0.0;
+    for (int qz = 0; qz < nz; ++qz)
+      for (int qy = 0; qy < n; ++qy)
+        for (int qx = 0; qx < n; ++qx) {
+          double xi[3] = {g.xq[qx], g.xq[qy], (dim == 3) ? g.xq[qz] : 0.0}, x[3], J[3][3], Ji[3][3];
+          map_point(&g, vc, xi, x, J);
+          double w = g.wq[qx] * g.wq[qy] * ((dim == 3) ? g.wq[qz] : 1.0);
+          double v = uv[(qz * n + qy) * n + qx];
+          s += v * v * inverse3(J, Ji) * w;
+        }
+    cell_norms[c] = sqrt(s);
+  }
+}
+
+double orc_l2_norm(const orc_mesh *m, const double *u)
+{
+  geo_t g;
+  geo_init(m, &g);
+  const int n = g.n, dim = g.dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+  double total = 0.0;
+#pragma omp parallel for reduction(+ : total) schedule(static)
+  for (long c = 0; c < g.n_cells; ++c) {
+    const long nxy = (long)g.nc[0] * g.nc[1];
+    int iz = (int)(c / nxy), iy = (int)((c / g.nc[0]) % g.nc[1]), ix = (int)(c % g.nc[0]);
+    long idx[MAXN3];
+    double ul[MAXN3], uv[MAXN3], vc[8][3];
+    cell_dofs(&g, ix, iy, iz, idx);
+    cell_vertices(m, &g, ix, iy, iz, vc);
+    for (int t = 0; t < nqt; ++t) ul[t] = u[idx[t]];
+    evaluate(&g, ul, uv, NULL);
+    double s = 0.0;
+    for (int qz = 0; qz < nz; ++qz)
+      for (int qy = 0; qy < n; ++qy)
+        for (int qx = 0; qx < n; ++qx) {
+          double xi[3] = {g.xq[qx], g.xq[qy], (dim == 3) ? g.xq[qz] : 0.0}, x[3], J[3][3], Ji[3][3];
+          map_point(&g, vc, xi, x, J);
+          double w = g.wq[qx] * g.wq[qy] * ((dim == 3) ? g.wq[qz] : 1.0);
+          double v = uv[(qz * n + qy) * n + qx];
+          s += v * v * inverse3(J, Ji) * w;
+        }
+    total += s;
+  }
+  return sqrt(total);
+}
+
+/* ------------------------------------------------------------- Krylov solvers */
+
+static double dotv(long N, const double *a, const double *b)
+{
+  double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+  for (long i = 0; i < N; ++i) s += a[i] * b[i];
+  return s;
+}
+
+/* Chebyshev semi-iteration on D^-1 A with zero start (residual polynomial of
+ * the given degree; degree-1 operator applies); degree 1 is a scaled Jacobi */
+void orc_prec_apply(const orc_mesh *m, const orc_op *op, const orc_prec *P, double *z,
+                    const double *r)
+{
+  const long N = orc_n_dofs(m);
+  if (!P || P->type == ORC_PREC_IDENTITY) {
+    memcpy(z, r, sizeof(double) * N);
+    return;
+  }
+  if (P->type == ORC_PREC_JACOBI) {
+    for (long i = 0; i < N; ++i) z[i] = P->inv_diag[i] * r[i];
+    return;
+  }
+  const double a = P->lambda_min, b = P->lambda_max;
+  const double theta = 0.5 * (b + a), delta = 0.5 * (b - a), sigma = theta / delta;
+  double rho = 1.0 / sigma;
+  double *d = (double *)malloc(sizeof(double) * N), *t = (double *)malloc(sizeof(double) * N);
+  for (long i = 0; i < N; ++i) {
+    d[i] = P->inv_diag[i] * r[i] / theta;
+    z[i] = d[i];
+  }
+  for (int k = 1; k < P->degree; ++k) {
+    orc_vmult(m, op, t, z);
+    double rho_new = 1.0 / (2.0 * sigma - rho);
+    for (long i = 0; i < N; ++i) {
+      d[i] = rho_new * rho * d[i] + 2.0 * rho_new / delta * P->inv_diag[i] * (r[i] - t[i]);
+      z[i] += d[i];
+    }
+    rho = rho_new;
+  }
+  free(d);
+  free(t);
+}
+
+/* preconditioned CG, deal.II SolverCG + ReductionControl semantics:
+ * converged when |r_k| <= max(abs_tol, rel_tol |r_0|), |.| the l2 norm of the
+ * unpreconditioned residual; *n_it = iterations performed */
+int orc_cg(const orc_mesh *m, const orc_op *op, const orc_prec *P, const double *b, double *x,
+           double rel_tol, double abs_tol, int max_it, int *n_it, double *res_hist)
+{
+  const long N = orc_n_dofs(m);
+  double *r = malloc(sizeof(double) * N), *z = malloc(sizeof(double) * N),
+         *p = malloc(sizeof(double) * N), *Ap = malloc(sizeof(double) * N);
+  orc_vmult(m, op, Ap, x);
+  for (long i = 0; i < N; ++i) r[i] = b[i] - Ap[i];
+  double res = sqrt(dotv(N, r, r));
+  const double tol = fmax(abs_tol, rel_tol * res);
+  if (res_hist) res_hist[0] = res;
+  int it = 0, status = 1;
+  if (res <= tol) status = 0;
+  double rz = 0.0;
+  if (status) {
+    orc_prec_apply(m, op, P, z, r);
+    memcpy(p, z, sizeof(double) * N);
+    rz = dotv(N, r, z);
+  }
+  while (status && it < max_it) {
+    orc_vmult(m, op, Ap, p);
+    const double alpha = rz / dotv(N, p, Ap);
+    for (long i = 0; i < N; ++i) {
+      x[i] += alpha * p[i];
+      r[i] -= alpha * Ap[i];
+    }
+    ++it;
+    res = sqrt(dotv(N, r, r));
+    if (res_hist) res_hist[it] = res;
+    if (res <= tol) {
+      status = 0;
+      break;
+    }
+    orc_prec_apply(m, op, P, z, r);
+    const double rz_new = dotv(N, r, z), beta = rz_new / rz;
+    rz = rz_new;
+    for (long i = 0; i < N; ++i) p[i] = z[i] + beta * p[i];
+  }
+  *n_it = it;
+  free(r);
+  free(z);
+  free(p);
+  free(Ap);
+  return status;
+}
+
+/* right-preconditioned restarted GMRES (modified Gram-Schmidt, Givens rotations);
+ * the monitored residual is that of the unpreconditioned system, as in
+ * deal.II SolverGMRES with right_preconditioning = true (linear_solver.hpp:112-119) */
+int orc_gmres(const orc_mesh *m, const orc_op *op, const orc_prec *P, const double *b, double *x,
+              double rel_tol, double abs_tol, int max_it, int restart, int *n_it,
+              double *res_hist)
+{
+  const long N = orc_n_dofs(m);
+  const int mk = restart;
+  double *V = malloc(sizeof(double) * N * (mk + 1));
+  double *w = malloc(sizeof(double) * N), *z = malloc(sizeof(double) * N);
+  double *H = calloc((size_t)(mk + 1) * mk, sizeof(double));
+  double *cs = malloc(sizeof(double) * mk), *sn = malloc(sizeof(double) * mk),
+         *gv = malloc(sizeof(double) * (mk + 1)), *y = malloc(sizeof(double) * mk);
+  int it = 0, status = 1;
+  double tol = -1.0;
+  for (;;) {
+    orc_vmult(m, op, w, x);
+    for (long i = 0; i < N; ++i) V[i] = b[i] - w[i];
+    double beta = sqrt(dotv(N, V, V));
+    if (tol < 0.0) {
+      tol = fmax(abs_tol, rel_tol * beta);
+      if (res_hist) res_hist[0] = beta;
+    }
+    if (beta <= tol) {
+      status = 0;
+      break;
+    }
+    if (it >= max_it) break;
+    for (long i = 0; i < N; ++i) V[i] /= beta;
+    for (int k = 0; k <= mk; ++k) gv[k] = 0.0;
+    gv[0] = beta;
+    int j = 0;
+    for (; j < mk && it < max_it; ++j) {
+      orc_prec_apply(m, op, P, z, V + (long)j * N);
+      orc_vmult(m, op, w, z);
+      for (int k = 0; k <= j; ++k) {
+        double h = dotv(N, w, V + (long)k * N);
+        H[k * mk + j] = h;
+        for (long i = 0; i < N; ++i) w[i] -= h * V[(long)k * N + i];
+      }
+      double hn = sqrt(dotv(N, w, w));
+      H[(j + 1) * mk + j] = hn;
+      for (long i = 0; i < N; ++i) V[(long)(j + 1) * N + i] = (hn > 0.0) ? w[i] / hn : 0.0;
+      for (int k = 0; k < j; ++k) {
+        double t = cs[k] * H[k * mk + j] + sn[k] * H[(k + 1) * mk + j];
+        H[(k + 1) * mk + j] = -sn[k] * H[k * mk + j] + cs[k] * H[(k + 1) * mk + j];
+        H[k * mk + j] = t;
+      }
+      double a = H[j * mk + j], c = H[(j + 1) * mk + j], r = sqrt(a * a + c * c);
+      cs[j] = a / r;
+      sn[j] = c / r;
+      H[j * mk + j] = r;
+      H[(j + 1) * mk + j] = 0.0;
+      gv[j + 1] = -sn[j] * gv[j];
+      gv[j] = cs[j] * gv[j];
+      ++it;
+      if (res_hist) res_hist[it] = fabs(gv[j + 1]);
+      if (fabs(gv[j + 1]) <= tol) {
+        ++j;
+        status = 0;
+        break;
+      }
+    }
+    /* x += M^-1 V y */
+    for (int k = j - 1; k >= 0; --k) {
+      double s = gv[k];
+      for (int l = k + 1; l < j; ++l) s -= H[k * mk + l] * y[l];
+      y[k] = s / H[k * mk + k];
+    }
+    for (long i = 0; i < N; ++i) w[i] = 0.0;
+    for (int k = 0; k < j; ++k)
+      for (long i = 0; i < N; ++i) w[i] += y[k] * V[(long)k * N + i];
+    orc_prec_apply(m, op, P, z, w);
+    for (long i = 0; i < N; ++i) x[i] += z[i];
+    if (status == 0 || it >= max_it) break;
+  }
+  *n_it = it;
+  free(V);
+  free(w);
+  free(z);
+  free(H);
+  free(cs);
+  free(sn);
+  free(gv);
+  free(y);
+  return status;
+}
+
+/* largest eigenvalue of D^-1 A from n_steps of CG-Lanczos (Jacobi-preconditioned
+ * CG on A x = start from x = 0); Sturm bisection on the tridiagonal matrix */
+double orc_estimate_lambda_max(const orc_mesh *m, const orc_op *op, const double *inv_diag,
+                               const double *start, int n_steps)
+{
+  const long N = orc_n_dofs(m);
+  double *r = malloc(sizeof(double) * N), *z = malloc(sizeof(double) * N),
+         *p = malloc(sizeof(double) * N), *Ap = malloc(sizeof(double) * N);
+  double al[64], be[64];
+  memcpy(r, start, sizeof(double) * N);
+  for (long i = 0; i < N; ++i) z[i] = inv_diag[i] * r[i];
+  memcpy(p, z, sizeof(double) * N);
+  double rz = dotv(N, r, z);
+  int k = 0;
+  for (; k < n_steps && k < 64; ++k) {
+    orc_vmult(m, op, Ap, p);
+    al[k] = rz / dotv(N, p, Ap);
+    for (long i = 0; i < N; ++i) r[i] -= al[k] * Ap[i];
+    for (long i = 0; i < N; ++i) z[i] = inv_diag[i] * r[i];
+    double rz_new = dotv(N, r, z);
+    be[k] = rz_new / rz;
+    rz = rz_new;
+    for (long i = 0; i < N; ++i) p[i] = z[i] + be[k] * p[i];
+  }
+  /* tridiagonal T: T_jj = 1/al_j + be_{j-1}/al_{j-1}, T_{j,j+1} = sqrt(be_j)/al_j */
+  double dg[64], of[64];
+  for (int j = 0; j < k; ++j) {
+    dg[j] = 1.0 / al[j] + ((j > 0) ? be[j - 1] / al[j - 1] : 0.0);
+    of[j] = (j + 1 < k) ? sqrt(be[j]) / al[j] : 0.0;
+  }
+  double lo = 0.0, hi = 0.0;
+  for (int j = 0; j < k; ++j)
+    hi = fmax(hi, dg[j] + fabs(of[j]) + ((j > 0) ? fabs(of[j - 1]) : 0.0));
+  for (int itb = 0; itb < 200; ++itb) {
+    double mid = 0.5 * (lo + hi);
+    int cnt = 0;
+    double q = 1.0;
+    for (int j = 0; j < k; ++j) {
+      q = dg[j] - mid - ((j > 0) ? of[j - 1] * of[j - 1] / q : 0.0);
+      if (q == 0.0) q = -1e-300;
+      if (q < 0.0) ++cnt;
+    }
+    if (cnt >= k) hi = mid; /* all eigenvalues below mid */
+    else lo = mid;
+  }
+  free(r);
+  free(z);
+  free(p);
+  free(Ap);
+  return hi;
+}

@@ -1,0 +1,113 @@
+/*
+ * mpdg_oracle.h -- CPU oracle for the matrix-free heat / advection-diffusion
+ * operators.  TEST INFRASTRUCTURE ONLY: the tests, the smoke check and the
+ * CPU-baseline leg of bench.py use it as the checker; no product code path
+ * links or calls it.
+ *
+ * It restates, in plain FP64 C, the arithmetic that MeltPoolDG performs
+ * through deal.II's MatrixFree/FEEvaluation on the operator path:
+ *   - heat tangent      source/heat/heat_diffuse_operator.cpp:179-197,955-1086
+ *   - heat Robin faces  source/heat/heat_diffuse_operator.cpp:1088-1129
+ *   - heat residual     source/heat/heat_diffuse_operator.cpp:393-529,726-806
+ *   - heat diagonal     source/heat/heat_diffuse_operator.cpp:271-284
+ *   - advdiff tangent   source/level_set/advection_diffusion_operator.cpp:238-272,450-495
+ *   - advdiff rhs       source/level_set/advection_diffusion_operator.cpp:276-358
+ *   - advdiff diagonal  source/level_set/advection_diffusion_operator.cpp:401-446
+ *   - discretisation    source/utilities/fe_util.cpp:18-57 (FE_Q(p) on Gauss-Lobatto
+ *                       support points, MappingQGeneric, QGauss(p+1))
+ *   - Krylov solvers    include/meltpooldg/linear_algebra/linear_solver.hpp:26-134
+ *                       (ReductionControl semantics)
+ *
+ * Meshes are structured boxes of nc[0] x nc[1] (x nc[2]) multilinear cells
+ * whose vertices are given explicitly (so they may be perturbed).  Global
+ * DoFs are numbered lexicographically, x fastest:
+ *   g = (Z * NY + Y) * NX + X,  X = ix*p + i in [0, nc[0]*p], ...
+ */
+#ifndef MPDG_ORACLE_H
+#define MPDG_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_HEAT = 0, ORC_ADVDIFF = 1 };
+
+enum {
+  ORC_VEL_NONE = 0,
+  ORC_VEL_ROTATION = 1, /* u = s * (x_{dim-1}, 0.., -x_0): advection_diffusion_vortex.hpp:93-115 */
+  ORC_VEL_VORTEX = 2,   /* u = (sin pi x cos pi y, -cos pi x sin pi y, 0) */
+  ORC_VEL_CONST = 3,    /* u = vel_param */
+  ORC_VEL_NODAL = 4     /* u interpolated from a dim x N nodal field (component-major) */
+};
+
+enum { ORC_PREC_IDENTITY = 0, ORC_PREC_JACOBI = 1, ORC_PREC_CHEBYSHEV = 2 };
+
+typedef struct {
+  int dim;             /* 2 or 3 */
+  int degree;          /* p >= 1 */
+  int nc[3];           /* cells per direction (nc[2] ignored for dim 2) */
+  const double *vert;  /* (nc0+1)(nc1+1)(nc2+1) x dim vertex coordinates, x fastest */
+} orc_mesh;
+
+typedef struct {
+  int kind;                  /* ORC_HEAT or ORC_ADVDIFF */
+  double dt;                 /* time increment */
+  /* heat */
+  double rho_cp;             /* volumetric heat capacity rho*c_p */
+  double k0, k_alpha;        /* conductivity law k(T) = k0 * (1 + k_alpha * T) */
+  int full_tangent;          /* add dk/dT * grad(T) * du to the flux (non-symmetric) */
+  const double *temperature; /* nodal T for k(T) and the residual; NULL means T = 0 */
+  double robin_alpha;        /* convection coefficient on Robin faces */
+  double robin_t_inf;        /* ambient temperature of the Robin condition (residual only) */
+  int robin_faces;           /* bit (2*d + side): box face with normal along d, side 0 = min */
+  /* advection-diffusion */
+  double theta, diffusivity;
+  /* velocity, both operators */
+  int vel_kind;
+  double vel_param[3];
+  const double *vel_nodal;
+  /* homogeneous Dirichlet mask: constrained DoFs are read as 0 and never written */
+  const unsigned char *dirichlet;
+} orc_op;
+
+typedef struct {
+  int type;                 /* ORC_PREC_* */
+  const double *inv_diag;   /* Jacobi / Chebyshev diagonal */
+  int degree;               /* Chebyshev: residual polynomial degree (degree-1 operator applies) */
+  double lambda_min, lambda_max;
+} orc_prec;
+
+long orc_n_dofs(const orc_mesh *m);
+void orc_gauss_legendre(int n, double *x, double *w);  /* on [0,1] */
+void orc_gauss_lobatto(int n, double *x);              /* on [0,1] */
+/* S[q*n+i] = phi_i(xq), D[q*n+i] = phi_i'(xq), phi on the n Gauss-Lobatto nodes */
+void orc_shape_tables(int n, const double *xq, int nq, double *S, double *D);
+void orc_dof_coordinates(const orc_mesh *m, double *xyz);   /* N x dim */
+
+void orc_vmult(const orc_mesh *m, const orc_op *op, double *dst, const double *src);
+void orc_vmult_brute(const orc_mesh *m, const orc_op *op, double *dst, const double *src);
+void orc_vmult_cells(const orc_mesh *m, const orc_op *op, double *dst, const double *src,
+                     long cell_begin, long cell_end);
+void orc_diagonal(const orc_mesh *m, const orc_op *op, double *diag);
+void orc_invert_diagonal(const orc_mesh *m, const orc_op *op, double *diag);
+void orc_rhs_heat(const orc_mesh *m, const orc_op *op, double *dst, const double *t_old,
+                  const double *heat_source, const unsigned char *scatter_mask);
+void orc_rhs_advdiff(const orc_mesh *m, const orc_op *op, double *dst, const double *phi_old,
+                     const unsigned char *scatter_mask);
+double orc_l2_norm(const orc_mesh *m, const double *u);
+void orc_l2_norm_cells(const orc_mesh *m, const double *u, double *cell_norms);
+
+int orc_cg(const orc_mesh *m, const orc_op *op, const orc_prec *P, const double *b, double *x,
+           double rel_tol, double abs_tol, int max_it, int *n_it, double *res_hist);
+int orc_gmres(const orc_mesh *m, const orc_op *op, const orc_prec *P, const double *b, double *x,
+              double rel_tol, double abs_tol, int max_it, int restart, int *n_it,
+              double *res_hist);
+double orc_estimate_lambda_max(const orc_mesh *m, const orc_op *op, const double *inv_diag,
+                               const double *start, int n_steps);
+void orc_prec_apply(const orc_mesh *m, const orc_op *op, const orc_prec *P, double *z,
+                    const double *r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,294 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, the smoke check and the CPU-baseline leg of bench.py import this
+module; it is the checker of the CUDA path, never part of it.  The C side
+(mpdg_oracle.c) restates MeltPoolDG's operator arithmetic; this file adds mesh
+and boundary-mask builders and thin wrappers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpdg_oracle.so")
+
+HEAT, ADVDIFF = 0, 1
+VEL_NONE, VEL_ROTATION, VEL_VORTEX, VEL_CONST, VEL_NODAL = 0, 1, 2, 3, 4
+PREC_IDENTITY, PREC_JACOBI, PREC_CHEBYSHEV = 0, 1, 2
+
+_dp = C.POINTER(C.c_double)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class _Mesh(C.Structure):
+    _fields_ = [("dim", C.c_int), ("degree", C.c_int), ("nc", C.c_int * 3), ("vert", _dp)]
+
+
+class _Op(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("dt", C.c_double),
+        ("rho_cp", C.c_double), ("k0", C.c_double), ("k_alpha", C.c_double),
+        ("full_tangent", C.c_int), ("temperature", _dp),
+        ("robin_alpha", C.c_double), ("robin_t_inf", C.c_double), ("robin_faces", C.c_int),
+        ("theta", C.c_double), ("diffusivity", C.c_double),
+        ("vel_kind", C.c_int), ("vel_param", C.c_double * 3), ("vel_nodal", _dp),
+        ("dirichlet", _u8p),
+    ]
+
+
+class _Prec(C.Structure):
+    _fields_ = [("type", C.c_int), ("inv_diag", _dp), ("degree", C.c_int),
+                ("lambda_min", C.c_double), ("lambda_max", C.c_double)]
+
+
+def build():
+    """Compile the oracle with its Makefile (gcc, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P_m, P_o, P_p = C.POINTER(_Mesh), C.POINTER(_Op), C.POINTER(_Prec)
+        L.orc_n_dofs.restype = C.c_long
+        L.orc_n_dofs.argtypes = [P_m]
+        for name in ("orc_vmult", "orc_vmult_brute"):
+            getattr(L, name).argtypes = [P_m, P_o, _dp, _dp]
+        L.orc_vmult_cells.argtypes = [P_m, P_o, _dp, _dp, C.c_long, C.c_long]
+        L.orc_diagonal.argtypes = [P_m, P_o, _dp]
+        L.orc_invert_diagonal.argtypes = [P_m, P_o, _dp]
+        L.orc_rhs_heat.argtypes = [P_m, P_o, _dp, _dp, _dp, _u8p]
+        L.orc_rhs_advdiff.argtypes = [P_m, P_o, _dp, _dp, _u8p]
+        L.orc_l2_norm.restype = C.c_double
+        L.orc_l2_norm.argtypes = [P_m, _dp]
+        L.orc_dof_coordinates.argtypes = [P_m, _dp]
+        L.orc_cg.argtypes = [P_m, P_o, P_p, _dp, _dp, C.c_double, C.c_double, C.c_int,
+                             C.POINTER(C.c_int), _dp]
+        L.orc_gmres.argtypes = [P_m, P_o, P_p, _dp, _dp, C.c_double, C.c_double, C.c_int,
+                                C.c_int, C.POINTER(C.c_int), _dp]
+        L.orc_estimate_lambda_max.restype = C.c_double
+        L.orc_estimate_lambda_max.argtypes = [P_m, P_o, _dp, _dp, C.c_int]
+        L.orc_prec_apply.argtypes = [P_m, P_o, P_p, _dp, _dp]
+        L.orc_gauss_legendre.argtypes = [C.c_int, _dp, _dp]
+        L.orc_gauss_lobatto.argtypes = [C.c_int, _dp]
+        _lib = L
+    return _lib
+
+
+def _ptr(a, t=_dp):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+# ----------------------------------------------------------------- meshes
+
+def box_vertices(dim, nc, lo, hi, perturb=0.0, seed=None):
+    """Vertices of a structured box mesh, x fastest; interior vertices moved by
+    U[-perturb*h, perturb*h] per coordinate when perturb > 0 (boundary fixed)."""
+    nc = list(nc)[:dim]
+    axes = [np.linspace(lo[d], hi[d], nc[d] + 1) for d in range(dim)]
+    grids = np.meshgrid(*axes[::-1], indexing="ij")[::-1]  # slowest axis first
+    V = np.stack([g.reshape(-1) for g in grids], axis=1).astype(np.float64)
+    if perturb > 0.0:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        h = np.array([(hi[d] - lo[d]) / nc[d] for d in range(dim)])
+        disp = rng.uniform(-1.0, 1.0, size=V.shape) * perturb * h
+        idx = np.stack(np.meshgrid(*[np.arange(n + 1) for n in nc[::-1]], indexing="ij")[::-1],
+                       axis=-1).reshape(-1, dim)
+        interior = np.all((idx > 0) & (idx < np.array(nc)), axis=1)
+        V[interior] += disp[interior]
+    return np.ascontiguousarray(V)
+
+
+class Mesh:
+    def __init__(self, dim, degree, nc, vertices):
+        self.dim, self.degree = dim, degree
+        self.nc = (list(nc) + [1, 1, 1])[:3]
+        if dim == 2:
+            self.nc[2] = 1
+        self.vert = np.ascontiguousarray(vertices, dtype=np.float64)
+        self._c = _Mesh(dim, degree, (C.c_int * 3)(*self.nc), _ptr(self.vert))
+        self.shape = tuple(self.nc[d] * degree + 1 for d in range(dim))  # (NX, NY[, NZ])
+        self.n_dofs = int(np.prod(self.shape))
+        self.n_cells = int(np.prod(self.nc[:dim]))
+
+    @classmethod
+    def box(cls, dim, degree, nc, lo=None, hi=None, perturb=0.0, seed=None):
+        lo = lo if lo is not None else [0.0] * dim
+        hi = hi if hi is not None else [1.0] * dim
+        return cls(dim, degree, nc, box_vertices(dim, nc, lo, hi, perturb, seed))
+
+    def dof_coordinates(self):
+        x = np.zeros((self.n_dofs, self.dim))
+        lib().orc_dof_coordinates(C.byref(self._c), _ptr(x))
+        return x
+
+    def grid_index(self):
+        """Integer grid coordinates (X, Y[, Z]) of each DoF."""
+        idx = np.indices(self.shape[::-1]).reshape(self.dim, -1)[::-1]
+        return idx.T
+
+    def boundary_face_mask(self, faces=None):
+        """uint8 mask of DoFs on the selected box faces (default: all faces);
+        faces = iterable of (direction, side)."""
+        gi = self.grid_index()
+        mask = np.zeros(self.n_dofs, dtype=bool)
+        if faces is None:
+            faces = [(d, s) for d in range(self.dim) for s in (0, 1)]
+        for d, s in faces:
+            mask |= gi[:, d] == (0 if s == 0 else self.shape[d] - 1)
+        return mask.astype(np.uint8)
+
+
+class Operator:
+    """Parameters of one heat or advection-diffusion operator (oracle side)."""
+
+    def __init__(self, kind, dt, rho_cp=1.0, k0=1.0, k_alpha=0.0, full_tangent=False,
+                 temperature=None, robin_alpha=0.0, robin_t_inf=0.0, robin_faces=0,
+                 theta=0.5, diffusivity=0.0, vel_kind=VEL_NONE, vel_param=(0.0, 0.0, 0.0),
+                 vel_nodal=None, dirichlet=None):
+        self.temperature = None if temperature is None else np.ascontiguousarray(temperature, np.float64)
+        self.vel_nodal = None if vel_nodal is None else np.ascontiguousarray(vel_nodal, np.float64)
+        self.dirichlet = None if dirichlet is None else np.ascontiguousarray(dirichlet, np.uint8)
+        self.kind, self.dt = kind, dt
+        self._c = _Op(kind, dt, rho_cp, k0, k_alpha, int(full_tangent), _ptr(self.temperature),
+                      robin_alpha, robin_t_inf, robin_faces, theta, diffusivity, vel_kind,
+                      (C.c_double * 3)(*vel_param), _ptr(self.vel_nodal),
+                      _ptr(self.dirichlet, _u8p))
+        self.params = dict(kind=kind, dt=dt, rho_cp=rho_cp, k0=k0, k_alpha=k_alpha,
+                           full_tangent=full_tangent, robin_alpha=robin_alpha,
+                           robin_t_inf=robin_t_inf, robin_faces=robin_faces, theta=theta,
+                           diffusivity=diffusivity, vel_kind=vel_kind, vel_param=vel_param)
+
+    def with_dirichlet(self, mask):
+        p = dict(self.params)
+        return Operator(**p, temperature=self.temperature, vel_nodal=self.vel_nodal, dirichlet=mask)
+
+    def with_temperature(self, T):
+        p = dict(self.params)
+        return Operator(**p, temperature=T, vel_nodal=self.vel_nodal, dirichlet=self.dirichlet)
+
+
+# ----------------------------------------------------------- operations
+
+def vmult(mesh, op, src, brute=False):
+    src = np.ascontiguousarray(src, np.float64)
+    dst = np.zeros(mesh.n_dofs)
+    f = lib().orc_vmult_brute if brute else lib().orc_vmult
+    f(C.byref(mesh._c), C.byref(op._c), _ptr(dst), _ptr(src))
+    return dst
+
+
+def vmult_cells(mesh, op, src, cell_begin, cell_end):
+    """Apply of a contiguous range of cells only (CPU-baseline sampling)."""
+    src = np.ascontiguousarray(src, np.float64)
+    dst = np.zeros(mesh.n_dofs)
+    lib().orc_vmult_cells(C.byref(mesh._c), C.byref(op._c), _ptr(dst), _ptr(src),
+                          int(cell_begin), int(cell_end))
+    return dst
+
+
+def diagonal(mesh, op):
+    d = np.zeros(mesh.n_dofs)
+    lib().orc_diagonal(C.byref(mesh._c), C.byref(op._c), _ptr(d))
+    return d
+
+
+def inverse_diagonal(mesh, op):
+    d = diagonal(mesh, op)
+    lib().orc_invert_diagonal(C.byref(mesh._c), C.byref(op._c), _ptr(d))
+    return d
+
+
+def rhs_heat(mesh, op, t_old, heat_source=None, scatter_mask=None, dst=None):
+    dst = np.zeros(mesh.n_dofs) if dst is None else dst
+    t_old = np.ascontiguousarray(t_old, np.float64)
+    hs = None if heat_source is None else np.ascontiguousarray(heat_source, np.float64)
+    sm = None if scatter_mask is None else np.ascontiguousarray(scatter_mask, np.uint8)
+    lib().orc_rhs_heat(C.byref(mesh._c), C.byref(op._c), _ptr(dst), _ptr(t_old), _ptr(hs),
+                       _ptr(sm, _u8p))
+    return dst
+
+
+def rhs_advdiff(mesh, op, phi_old, scatter_mask=None, dst=None):
+    dst = np.zeros(mesh.n_dofs) if dst is None else dst
+    phi_old = np.ascontiguousarray(phi_old, np.float64)
+    sm = None if scatter_mask is None else np.ascontiguousarray(scatter_mask, np.uint8)
+    lib().orc_rhs_advdiff(C.byref(mesh._c), C.byref(op._c), _ptr(dst), _ptr(phi_old),
+                          _ptr(sm, _u8p))
+    return dst
+
+
+def l2_norm(mesh, u):
+    u = np.ascontiguousarray(u, np.float64)
+    return lib().orc_l2_norm(C.byref(mesh._c), _ptr(u))
+
+
+def _prec(kind, inv_diag=None, degree=0, lmin=0.0, lmax=0.0):
+    return _Prec(kind, _ptr(inv_diag), degree, lmin, lmax)
+
+
+def cg(mesh, op, b, x0=None, inv_diag=None, rel_tol=1e-12, abs_tol=1e-20, max_it=10000,
+       chebyshev=None):
+    """Returns (x, iterations, residual history, converged)."""
+    x = np.zeros(mesh.n_dofs) if x0 is None else np.array(x0, dtype=np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    if chebyshev is not None:
+        P = _prec(PREC_CHEBYSHEV, inv_diag, chebyshev["degree"], chebyshev["lambda_min"],
+                  chebyshev["lambda_max"])
+    elif inv_diag is not None:
+        P = _prec(PREC_JACOBI, inv_diag)
+    else:
+        P = _prec(PREC_IDENTITY)
+    it = C.c_int(0)
+    hist = np.zeros(max_it + 1)
+    st = lib().orc_cg(C.byref(mesh._c), C.byref(op._c), C.byref(P), _ptr(b), _ptr(x), rel_tol,
+                      abs_tol, max_it, C.byref(it), _ptr(hist))
+    return x, it.value, hist[: it.value + 1], st == 0
+
+
+def gmres(mesh, op, b, x0=None, inv_diag=None, rel_tol=1e-12, abs_tol=1e-20, max_it=10000,
+          restart=30):
+    x = np.zeros(mesh.n_dofs) if x0 is None else np.array(x0, dtype=np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    P = _prec(PREC_JACOBI, inv_diag) if inv_diag is not None else _prec(PREC_IDENTITY)
+    it = C.c_int(0)
+    hist = np.zeros(max_it + 1)
+    st = lib().orc_gmres(C.byref(mesh._c), C.byref(op._c), C.byref(P), _ptr(b), _ptr(x), rel_tol,
+                         abs_tol, max_it, restart, C.byref(it), _ptr(hist))
+    return x, it.value, hist[: it.value + 1], st == 0
+
+
+def lambda_max(mesh, op, inv_diag, start, n_steps=10):
+    start = np.ascontiguousarray(start, np.float64)
+    return lib().orc_estimate_lambda_max(C.byref(mesh._c), C.byref(op._c), _ptr(inv_diag),
+                                         _ptr(start), n_steps)
+
+
+def chebyshev_apply(mesh, op, inv_diag, r, degree, lmin, lmax):
+    z = np.zeros(mesh.n_dofs)
+    r = np.ascontiguousarray(r, np.float64)
+    P = _prec(PREC_CHEBYSHEV, inv_diag, degree, lmin, lmax)
+    lib().orc_prec_apply(C.byref(mesh._c), C.byref(op._c), C.byref(P), _ptr(z), _ptr(r))
+    return z
+
+
+def gauss_legendre(n):
+    x, w = np.zeros(n), np.zeros(n)
+    lib().orc_gauss_legendre(n, _ptr(x), _ptr(w))
+    return x, w
+
+
+def gauss_lobatto(n):
+    x = np.zeros(n)
+    lib().orc_gauss_lobatto(n, _ptr(x))
+    return x
