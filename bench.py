@@ -71,8 +71,12 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                 stderr=subprocess.DEVNULL)
+            # wait for the first sample so the timed region is covered
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
@@ -143,9 +147,7 @@ def cpu_reference_rate(V, T, mask, n_dofs, target_seconds=10.0, cell_fraction=No
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    M = None
-    import meltpooldg_b200  # noqa: F401  (only to share the mesh helpers)
-    from meltpooldg_b200 import box_vertices, boundary_mask
+    from meltpooldg_b200.operators import box_vertices, boundary_mask
     V = box_vertices(NC, perturb=0.1, seed=2)
     mask = boundary_mask(NC, DEGREE)
     n_dofs = int(np.prod([n * DEGREE + 1 for n in NC]))
@@ -324,7 +326,7 @@ def run_ours(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--solve-reps", type=int, default=3)

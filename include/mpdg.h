@@ -136,6 +136,9 @@ mpdg_status mpdg_op_use_dirichlet(mpdg_op *op, int use_dirichlet);
  * device pointer, FP64, n_dofs; an FP32 copy is made for the FP32 form */
 mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *device_values);
 mpdg_status mpdg_op_set_stream(mpdg_op *op, void *cuda_stream);
+/* reads and clears the operator's device error word: nonzero when a bounded
+ * device-side wait (bulk-copy completion) expired; synchronises the stream */
+mpdg_status mpdg_op_device_error(mpdg_op *op, int *flag);
 
 /* OperatorMatrixFree::vmult, operator_base.hpp:239-243
  * (heat: source/heat/heat_diffuse_operator.cpp:179-197;

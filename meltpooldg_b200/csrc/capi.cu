@@ -139,7 +139,7 @@ mpdg_status mpdg_op_destroy(mpdg_op *op)
   if (!op) return MPDG_OK;
   Op &o = op->o;
   free_workspace(o);
-  for (void *p : {(void *)o.T32, (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32,
+  for (void *p : {(void *)o.d_err, (void *)o.T32, (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32,
                   (void *)o.d_trig64})
     if (p) cudaFree(p);
   delete op;
@@ -167,6 +167,17 @@ mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *values)
     if (field != MPDG_FIELD_TEMPERATURE) throw Error{MPDG_ERR_ARG, "unknown field"};
     op->o.T64 = values;
     if (values && (op->o.d.precision_mask & (1 << MPDG_FP32))) ensure_T32(op->o);
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_op_device_error(mpdg_op *op, int *flag)
+{
+  return guarded([&]() -> int {
+    if (!op || !flag) throw Error{MPDG_ERR_ARG, "null argument"};
+    MPDG_CUDA(cudaStreamSynchronize(op->o.stream));
+    MPDG_CUDA(cudaMemcpy(flag, op->o.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    MPDG_CUDA(cudaMemset(op->o.d_err, 0, sizeof(int)));
     return MPDG_OK;
   });
 }

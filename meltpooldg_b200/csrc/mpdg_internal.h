@@ -14,6 +14,12 @@ namespace mpdg {
 constexpr int kMaxDegree = 4;
 constexpr int kMaxN = kMaxDegree + 1;
 
+// Per-cell strides of the streamed geometry (7 metric values, 3 velocity
+// values per quadrature point), padded to 4 elements so that every cell block
+// starts on a 16-byte boundary in both precisions (bulk-copy requirement).
+__host__ __device__ constexpr int metric_stride(int n) { return ((7 * n * n * n + 3) / 4) * 4; }
+__host__ __device__ constexpr int velb_stride(int n) { return ((3 * n * n * n + 3) / 4) * 4; }
+
 // thrown inside the library, converted to a status code at the C boundary
 struct Error {
   int status;
@@ -79,6 +85,7 @@ struct Op {
   float *d_trig32 = nullptr;           // uniform vortex velocity: sin/cos tables
   double *d_trig64 = nullptr;
   Workspace *ws = nullptr;
+  int *d_err = nullptr;                // device error word (bounded waits that expired)
   size_t device_bytes = 0;
 };
 

@@ -171,6 +171,7 @@ struct KP {
   const uint8_t *dmask;
   const uint8_t *cell_flags;
   long NX, NY;
+  int nc[3];
   int trig_stride;
   int par[3], cn[3];
   long ccount, cfirst;
@@ -314,6 +315,8 @@ __device__ __forceinline__ void uniform_velocity(const KP<Real> &p, const Tables
   }
 }
 
+#include "apply_warp.cuh"
+
 // ------------------------------------------------------------ the cell kernel
 
 template <int P, typename Real, int GEOM, int MODE, bool KT>
@@ -394,7 +397,7 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
   for (int k = 0; k < n; ++k) {
     Real JxW, G00, G01, G02, G11, G12, G22, b0 = 0, b1 = 0, b2 = 0;
     if (GEOM == GEOM_GENERAL) {
-      const Real *m = p.metric + (cell * 7) * n3 + k * n2 + j * n + i;
+      const Real *m = p.metric + cell * metric_stride(n) + k * n2 + j * n + i;
       if (active) {
         JxW = m[0];
         G00 = m[n3];
@@ -404,7 +407,7 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
         G12 = m[5 * n3];
         G22 = m[6 * n3];
         if (p.vel_kind != MPDG_VEL_NONE) {
-          const Real *vb = p.velb + (cell * 3) * n3 + k * n2 + j * n + i;
+          const Real *vb = p.velb + cell * velb_stride(n) + k * n2 + j * n + i;
           b0 = vb[0];
           b1 = vb[n3];
           b2 = vb[2 * n3];
@@ -554,7 +557,7 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
   for (int k = 0; k < n; ++k) {
     Real JxW, G00, G01, G02, G11, G12, G22, b0 = 0, b1 = 0, b2 = 0;
     if (GEOM == GEOM_GENERAL) {
-      const Real *m = p.metric + (cell * 7) * n3 + k * n2 + j * n + i;
+      const Real *m = p.metric + cell * metric_stride(n) + k * n2 + j * n + i;
       JxW = active ? m[0] : 0;
       G00 = active ? m[n3] : 0;
       G01 = active ? m[2 * n3] : 0;
@@ -563,7 +566,7 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
       G12 = active ? m[5 * n3] : 0;
       G22 = active ? m[6 * n3] : 0;
       if (p.vel_kind != MPDG_VEL_NONE && active) {
-        const Real *vb = p.velb + (cell * 3) * n3 + k * n2 + j * n + i;
+        const Real *vb = p.velb + cell * velb_stride(n) + k * n2 + j * n + i;
         b0 = vb[0];
         b1 = vb[n3];
         b2 = vb[2 * n3];
@@ -684,11 +687,11 @@ __global__ void metric_kernel(const double *vert, int nc0, int nc1, int nc2, int
     for (int c2 = 0; c2 < 3; ++c2) s += Ji[ab[e][0]][c2] * Ji[ab[e][1]][c2];
     G[e] = JxW * s;
   }
-  double *m = metric + cell * 7 * n3 + q;
+  double *m = metric + cell * metric_stride(n) + q;
   m[0] = JxW;
   for (int e = 0; e < 6; ++e) m[(e + 1) * n3] = G[e];
   if (metric32) {
-    float *m32 = metric32 + cell * 7 * n3 + q;
+    float *m32 = metric32 + cell * metric_stride(n) + q;
     m32[0] = (float)JxW;
     for (int e = 0; e < 6; ++e) m32[(e + 1) * n3] = (float)G[e];
   }
@@ -754,8 +757,8 @@ __global__ void velb_kernel(const double *vert, int nc0, int nc1, int nc2, int P
   A[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
   for (int a = 0; a < 3; ++a) {
     const double b = w * (A[a][0] * u[0] + A[a][1] * u[1] + A[a][2] * u[2]);
-    velb[cell * 3 * n3 + a * n3 + q] = b;
-    if (velb32) velb32[cell * 3 * n3 + a * n3 + q] = (float)b;
+    velb[cell * velb_stride(n) + a * n3 + q] = b;
+    if (velb32) velb32[cell * velb_stride(n) + a * n3 + q] = (float)b;
   }
 }
 
@@ -863,7 +866,8 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
     }
     MPDG_CUDA(cudaMalloc(&d_xw, sizeof(xw)));
     MPDG_CUDA(cudaMemcpy(d_xw, xw, sizeof(xw), cudaMemcpyHostToDevice));
-    m.d_metric64 = dev_alloc<double>((size_t)m.n_cells * 7 * n3, m.device_bytes);
+    m.d_metric64 = dev_alloc<double>((size_t)m.n_cells * metric_stride(n), m.device_bytes);
+    MPDG_CUDA(cudaMemset(m.d_metric64, 0, sizeof(double) * m.n_cells * metric_stride(n)));
     const long total = m.n_cells * n3;
     metric_kernel<<<grid_for(total, 256), 256>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col,
                                                  m.d_metric64, nullptr, d_xw, d_xw + kMaxN);
@@ -908,7 +912,7 @@ void ensure_metric32(Mesh &m, cudaStream_t s)
 {
   if (m.uniform || m.metric32_ready) return;
   const int n = m.degree + 1, n3 = n * n * n;
-  const long total = m.n_cells * 7 * n3;
+  const long total = m.n_cells * metric_stride(n);
   m.d_metric32 = dev_alloc<float>(total, m.device_bytes);
   cast_kernel<<<grid_for(total, 256), 256, 0, s>>>(m.d_metric64, m.d_metric32, total);
   MPDG_LAUNCHED();
@@ -920,6 +924,8 @@ void build_op_device_data(Op &op)
   Mesh &m = *op.mesh;
   const int p = m.degree, n = p + 1, n3 = n * n * n;
   const bool want32 = (op.d.precision_mask & (1 << MPDG_FP32)) != 0;
+  op.d_err = dev_alloc<int>(1, op.device_bytes);
+  MPDG_CUDA(cudaMemset(op.d_err, 0, sizeof(int)));
   if (want32) ensure_metric32(m, op.stream);
   if (op.d.vel_kind == MPDG_VEL_NONE) return;
   if (!m.uniform) {
@@ -936,8 +942,12 @@ void build_op_device_data(Op &op)
     MPDG_CUDA(cudaMalloc(&d_xw, sizeof(xw)));
     MPDG_CUDA(cudaMemcpy(d_xw, xw, sizeof(xw), cudaMemcpyHostToDevice));
     const long total = m.n_cells * n3;
-    op.d_velb64 = dev_alloc<double>((size_t)m.n_cells * 3 * n3, op.device_bytes);
-    if (want32) op.d_velb32 = dev_alloc<float>((size_t)m.n_cells * 3 * n3, op.device_bytes);
+    op.d_velb64 = dev_alloc<double>((size_t)m.n_cells * velb_stride(n), op.device_bytes);
+    MPDG_CUDA(cudaMemset(op.d_velb64, 0, sizeof(double) * m.n_cells * velb_stride(n)));
+    if (want32) {
+      op.d_velb32 = dev_alloc<float>((size_t)m.n_cells * velb_stride(n), op.device_bytes);
+      MPDG_CUDA(cudaMemset(op.d_velb32, 0, sizeof(float) * m.n_cells * velb_stride(n)));
+    }
     velb_kernel<<<grid_for(total, 256), 256>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col,
                                                op.d.vel_kind, op.d.vel_param[0], op.d.vel_param[1],
                                                op.d.vel_param[2], op.d_velb64, op.d_velb32, d_xw,
@@ -990,6 +1000,7 @@ KP<Real> base_params(Op &op)
   KP<Real> k{};
   k.NX = m.NX;
   k.NY = m.NY;
+  for (int d = 0; d < 3; ++d) k.nc[d] = m.nc[d];
   for (int d = 0; d < 3; ++d) {
     k.h[d] = (Real)m.h[d];
     k.origin[d] = (Real)m.origin[d];
@@ -1071,19 +1082,80 @@ bool uses_kT(const Op &op)
 
 }  // namespace
 
+namespace {
+
+int g_num_sms = 0;
+
+int num_sms()
+{
+  if (g_num_sms == 0) {
+    int dev = 0;
+    MPDG_CUDA(cudaGetDevice(&dev));
+    MPDG_CUDA(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return g_num_sms;
+}
+
+template <int P, typename Real, int GEOM, bool KT>
+void run_warp_apply(Op &op, KP<Real> k)
+{
+  Mesh &m = *op.mesh;
+  constexpr int n = P + 1, CPW = WCfg<n>::cpw;
+  const bool gvel = GEOM == GEOM_GENERAL && op.d.vel_kind != MPDG_VEL_NONE;
+  const size_t smem = sizeof(Real) * kWarpsPerCTA * warp_smem_elems<P, Real, GEOM>(gvel);
+  auto kern = warp_apply_kernel<P, Real, GEOM, KT>;
+  static int configured_smem = -1, blocks_per_sm = 0;  // per instantiation
+  if (configured_smem != (int)smem) {
+    MPDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MPDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerCTA * 32, smem));
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+    configured_smem = (int)smem;
+  }
+  const long resident = (long)num_sms() * blocks_per_sm;
+  for (int c = 0; c < 8; ++c) {
+    const Colour &C = m.colour[c];
+    if (C.count == 0) continue;
+    colour_params(k, C);
+    const long groups = (C.count + CPW - 1) / CPW;
+    const long blocks = std::min(resident, (groups + kWarpsPerCTA - 1) / kWarpsPerCTA);
+    kern<<<(unsigned)blocks, kWarpsPerCTA * 32, smem, op.stream>>>(k, op.d_err);
+    MPDG_LAUNCHED();
+  }
+}
+
+template <typename Real, int GEOM, bool KT>
+void warp_apply_degree(Op &op, const KP<Real> &k)
+{
+  switch (op.mesh->degree) {
+    case 1: run_warp_apply<1, Real, GEOM, KT>(op, k); break;
+    case 2: run_warp_apply<2, Real, GEOM, KT>(op, k); break;
+    case 3: run_warp_apply<3, Real, GEOM, KT>(op, k); break;
+    case 4: run_warp_apply<4, Real, GEOM, KT>(op, k); break;
+    default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+  }
+}
+
+}  // namespace
+
 template <typename Real>
 void launch_apply(Op &op, Real *dst, const Real *src)
 {
   Mesh &m = *op.mesh;
   if (!m.uniform && sizeof(Real) == 4) ensure_metric32(m, op.stream);
+  if (!m.uniform && op.d.vel_kind != MPDG_VEL_NONE && sizeof(Real) == 4 && !op.d_velb32)
+    throw Error{MPDG_ERR_ARG, "the FP32 form was not prepared for this operator (precision_mask)"};
   KP<Real> k = base_params<Real>(op);
   k.src = src;
   k.dst = dst;
   const bool kt = uses_kT(op);
   if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
-  MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * m.N, op.stream));
-  if (kt) dispatch_degree<Real, MODE_LINEAR, true>(op, k);
-  else dispatch_degree<Real, MODE_LINEAR, false>(op, k);
+  if (m.uniform) {
+    if (kt) warp_apply_degree<Real, GEOM_UNIFORM, true>(op, k);
+    else warp_apply_degree<Real, GEOM_UNIFORM, false>(op, k);
+  } else {
+    if (kt) warp_apply_degree<Real, GEOM_GENERAL, true>(op, k);
+    else warp_apply_degree<Real, GEOM_GENERAL, false>(op, k);
+  }
 }
 
 template void launch_apply<double>(Op &, double *, const double *);
@@ -1215,7 +1287,7 @@ __global__ void l2_cells_kernel(const double *u, long NX, long NY, int nc0, int 
         }
     for (int q = 0; q < n3; ++q) {
       const int qi = q % n, qj = (q / n) % n, qk = q / (n * n);
-      const double JxW = metric ? metric[cell * 7 * n3 + q] : hx * hy * hz * T.w[qi] * T.w[qj] * T.w[qk];
+      const double JxW = metric ? metric[cell * metric_stride(n) + q] : hx * hy * hz * T.w[qi] * T.w[qj] * T.w[qk];
       s += b[q] * b[q] * JxW;
     }
   }

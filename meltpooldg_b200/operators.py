@@ -163,6 +163,12 @@ class _MatrixFreeOperator:
     def compute_diagonal(self, diag):
         A.check(A.lib().mpdg_compute_diagonal(self._h, _dptr(diag)), "compute_diagonal")
 
+    def device_error(self):
+        """Reads and clears the device error word (an expired bounded wait)."""
+        f = C.c_int()
+        A.check(A.lib().mpdg_op_device_error(self._h, C.byref(f)), "device_error")
+        return f.value
+
     def l2_norm(self, u):
         v = C.c_double()
         A.check(A.lib().mpdg_l2_norm(self._h, _dptr(u), C.byref(v)), "l2_norm")
