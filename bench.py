@@ -152,9 +152,10 @@ def run_reference(args, rank, world):
     mask = boundary_mask(NC, DEGREE)
     n_dofs = int(np.prod([n * DEGREE + 1 for n in NC]))
     T = np.random.Generator(np.random.PCG64(3)).uniform(300.0, 3000.0, n_dofs)
-    # each step: a fixed sample of cells sized to ~4 s
+    # each step: a fixed sample of cells, sized so the whole run takes ~2.5 minutes
+    per_step = max(0.05, min(4.0, 150.0 / (args.steps + args.warmup)))
     _, _, _, _ = cpu_reference_rate(V, T, mask, n_dofs, target_seconds=0.5)
-    rate0, sample, threads, dt0 = cpu_reference_rate(V, T, mask, n_dofs, target_seconds=4.0)
+    rate0, sample, threads, dt0 = cpu_reference_rate(V, T, mask, n_dofs, target_seconds=per_step)
     frac = float(sample.split(" of ")[0]) / np.prod(NC)
     for _ in range(args.warmup):
         cpu_reference_rate(V, T, mask, n_dofs, cell_fraction=frac)
