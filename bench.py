@@ -32,7 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "mat-free DoFs/s & solves/s, FP32+FP64-refined vs FP64 at 1e-10; p50/p99 latency"
-NC, DEGREE = (64, 64, 64), 4
+NC, DEGREE = [64, 64, 64], 4
 DT, K0, K_ALPHA = 1e-3, 1.0, 1e-3
 
 # dram__bytes_read.sum + dram__bytes_write.sum per apply of the FP64 cell kernel
@@ -238,16 +238,18 @@ def run_ours(args, rank, world):
     apply32_s = e0.elapsed_time(e1) / 1e3 / args.steps
 
     # end to end through the host-buffer C-ABI call (pinned host buffers)
-    hsrc = torch.empty(N, dtype=torch.float64).pin_memory()
-    hdst = torch.empty(N, dtype=torch.float64).pin_memory()
-    hsrc.copy_(src.cpu())
-    hs, hd = hsrc.numpy(), hdst.numpy()
-    op.vmult_host(hd, hs)
-    e2e_steps = max(3, args.steps // 2)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    e2e_s = float("nan")
+    if not args.no_e2e:
+        hsrc = torch.empty(N, dtype=torch.float64).pin_memory()
+        hdst = torch.empty(N, dtype=torch.float64).pin_memory()
+        hsrc.copy_(src.cpu())
+        hs, hd = hsrc.numpy(), hdst.numpy()
         op.vmult_host(hd, hs)
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
+        e2e_steps = max(3, min(50, args.steps // 2))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            op.vmult_host(hd, hs)
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
 
     peak, peak_kind = load_peaks()
     E = int(np.prod(NC))
@@ -314,8 +316,9 @@ def run_ours(args, rank, world):
                        "l2": "inputs larger than L2 (metric stream 1.8 GB per apply)"},
             "roofline": roof,
             "cpu_baseline": cpu,
-            "e2e": {"value": N / e2e_s, "unit": "DoFs/s", "h2d_bytes_per_step": 8 * N,
-                    "d2h_bytes_per_step": 8 * N, "call": "mpdg_vmult_host (pinned host buffers)"},
+            "e2e": None if args.no_e2e else {
+                "value": N / e2e_s, "unit": "DoFs/s", "h2d_bytes_per_step": 8 * N,
+                "d2h_bytes_per_step": 8 * N, "call": "mpdg_vmult_host (pinned host buffers)"},
             "fp32_apply": {"value": N / apply32_s, "unit": "DoFs/s"},
             "solves": solves,
             "gpu_launches": launches,
@@ -334,7 +337,11 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cells", type=int, default=64,
+                    help="cells per direction (64 is the benchmark workload; smaller sizes for profiling)")
     args = ap.parse_args()
+    NC[:] = [args.cells] * 3
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if world > 1 and args.impl == "ours":
