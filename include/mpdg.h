@@ -133,7 +133,11 @@ mpdg_status mpdg_op_reset_time_increment(mpdg_op *op, double dt);
  * include/meltpooldg/linear_algebra/utilities_matrixfree.hpp:39-101) */
 mpdg_status mpdg_op_use_dirichlet(mpdg_op *op, int use_dirichlet);
 /* state vectors the operator reads (temperature for k(T) and the Newton residual);
- * device pointer, FP64, n_dofs; an FP32 copy is made for the FP32 form */
+ * device pointer, FP64, n_dofs; an FP32 copy is made for the FP32 form.  The
+ * operator folds k(T) into its per-quadrature-point coefficients when this is
+ * called: a caller that changes the field's values in place calls it again
+ * before the next vmult (the reference re-reads T in every vmult,
+ * heat_diffuse_operator.cpp:1000-1012). */
 mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *device_values);
 mpdg_status mpdg_op_set_stream(mpdg_op *op, void *cuda_stream);
 /* reads and clears the operator's device error word: nonzero when a bounded

@@ -2,17 +2,21 @@
 // operator_kernels.cu after the shared tables and kernel parameters.
 //
 // Layout and schedule:
+//  * the operator's coefficients are merged per quadrature point before the
+//    apply (merge_kernel): c_mass JxW and c_diff k(T_q) JxW J^-1 J^-T, so that
+//    k(T) costs nothing per apply (T is fixed during a linear solve, as in the
+//    reference's Newton step);
 //  * a warp owns CPW = 32 / n^2 cells (n = degree + 1; one cell for Q4, two
 //    for Q3, three for Q2, eight for Q1); lane (i, j) of a cell keeps the DoF
 //    column (i, j, 0..n-1) in registers, so z-contractions are register FMAs
 //    and x/y contractions go through a per-cell shared tile with __syncwarp
 //    only -- no block-wide barrier anywhere in the cell pipeline;
-//  * warps are persistent over the cells of one parity colour; the per-cell
-//    geometry stream (JxW and the six entries of JxW J^-1 J^-T per quadrature
-//    point, padded to 16 bytes per cell) of the warp's next cells is brought
-//    into shared memory by one TMA bulk copy (cp.async.bulk + mbarrier
-//    complete_tx) issued before the gather and the interpolation, which hide
-//    its latency;
+//  * warps are persistent over the cells of one parity colour and software
+//    pipelined: the coefficient block of the warp's next cells (padded to 16
+//    bytes per cell) is brought into shared memory by one TMA bulk copy
+//    (cp.async.bulk + mbarrier complete_tx) issued as soon as the stage is
+//    read, and the next cells' src columns are loaded into registers while the
+//    current cells are computed;
 //  * scatter is atomic-free: the colours run in order 0..7 and, for every DoF,
 //    the cell whose parity bits are zero in all directions in which the DoF is
 //    shared with a neighbour is the first to touch it; that cell stores, later
@@ -84,60 +88,66 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t *bar, unsigned phase,
 }
 
 // ---- warp-synchronous contraction passes (tile layout t[k*n*n + j*n + i])
+// Sc: table in constant memory (uniform index: z passes); Ss: the same table in
+// shared memory (lane-dependent rows: x and y passes)
 
 template <int n, typename Real>
-__device__ __forceinline__ void w_to_qp(const Real *S, Real *t, int i, int j, const Real (&u)[n],
-                                        Real (&v)[n])
+__device__ __forceinline__ void w_to_qp(const Real *Sc, const Real *Ss, Real *t, bool wr, int i,
+                                        int j, const Real (&u)[n], Real (&v)[n])
 {
   Real a[n];
-  cz<n, Real, false>(S, u, a);
-  put<n>(t, i, j, a);
+  cz<n, Real, false>(Sc, u, a);
+  if (wr) put<n>(t, i, j, a);
   __syncwarp();
-  cy<n, Real, false>(S, t, i, j, v);
+  cy<n, Real, false>(Ss, t, i, j, v);
   __syncwarp();
-  put<n>(t, i, j, v);
+  if (wr) put<n>(t, i, j, v);
   __syncwarp();
-  cx<n, Real, false>(S, t, i, j, a);
+  cx<n, Real, false>(Ss, t, i, j, a);
   __syncwarp();
 #pragma unroll
   for (int k = 0; k < n; ++k) v[k] = a[k];
 }
 
 template <int n, typename Real>
-__device__ __forceinline__ void w_grad_qp(const Real *Dc, Real *t, int i, int j, const Real (&v)[n],
-                                          Real (&gx)[n], Real (&gy)[n], Real (&gz)[n])
+__device__ __forceinline__ void w_grad_qp(const Real *Dcc, const Real *Dcs, Real *t, bool wr, int i,
+                                          int j, const Real (&v)[n], Real (&gx)[n], Real (&gy)[n],
+                                          Real (&gz)[n])
 {
-  put<n>(t, i, j, v);
+  if (wr) put<n>(t, i, j, v);
   __syncwarp();
-  cx<n, Real, false>(Dc, t, i, j, gx);
-  cy<n, Real, false>(Dc, t, i, j, gy);
-  cz<n, Real, false>(Dc, v, gz);
+  cx<n, Real, false>(Dcs, t, i, j, gx);
+  cy<n, Real, false>(Dcs, t, i, j, gy);
+  cz<n, Real, false>(Dcc, v, gz);
   __syncwarp();
 }
 
 template <int n, typename Real>
-__device__ __forceinline__ void w_from_qp(const Real *S, const Real *Dc, Real *t0, Real *t1, int i,
-                                          int j, const Real (&val)[n], const Real (&fx)[n],
+__device__ __forceinline__ void w_from_qp(const Real *Sc, const Real *Ss, const Real *Dcc,
+                                          const Real *Dcs, Real *t0, Real *t1, bool wr, int i, int j,
+                                          const Real (&val)[n], const Real (&fx)[n],
                                           const Real (&fy)[n], const Real (&fz)[n], Real (&out)[n])
 {
   Real a[n], b[n];
-  put<n>(t0, i, j, fx);
-  put<n>(t1, i, j, fy);
+  if (wr) {
+    put<n>(t0, i, j, fx);
+    put<n>(t1, i, j, fy);
+  }
   __syncwarp();
-  cx<n, Real, true>(Dc, t0, i, j, a);
-  cy<n, Real, true>(Dc, t1, i, j, b);
-  cz<n, Real, true>(Dc, fz, out);
+  cx<n, Real, true>(Dcs, t0, i, j, a);
+  cy<n, Real, true>(Dcs, t1, i, j, b);
+  cz<n, Real, true>(Dcc, fz, out);
 #pragma unroll
   for (int k = 0; k < n; ++k) a[k] += b[k] + out[k] + val[k];
   __syncwarp();
-  put<n>(t0, i, j, a);
+  if (wr) put<n>(t0, i, j, a);
   __syncwarp();
-  cx<n, Real, true>(S, t0, i, j, b);
+  cx<n, Real, true>(Ss, t0, i, j, b);
   __syncwarp();
-  put<n>(t0, i, j, b);
+  if (wr) put<n>(t0, i, j, b);
   __syncwarp();
-  cy<n, Real, true>(S, t0, i, j, a);
-  cz<n, Real, true>(S, a, out);
+  cy<n, Real, true>(Ss, t0, i, j, a);
+  cz<n, Real, true>(Sc, a, out);
   __syncwarp();
 }
 
@@ -147,11 +157,29 @@ __host__ __device__ constexpr int warp_smem_elems(bool vel)
 {
   constexpr int n = P + 1, n3 = n * n * n, CPW = WCfg<n>::cpw;
   return (GEOM == GEOM_GENERAL ? CPW * (metric_stride(n) + (vel ? velb_stride(n) : 0)) : 0) +
-         2 * (CPW + 1) * n3;
+         2 * CPW * n3;
 }
 
-template <int P, typename Real, int GEOM, bool KT>
-__global__ void __launch_bounds__(kWarpsPerCTA * 32) warp_apply_kernel(const KP<Real> p, int *err)
+// cell (ix, iy, iz) of colour-local index cidx
+__device__ __forceinline__ void colour_cell(int cidx, const int cn[3], const int par[3], int &ix,
+                                            int &iy, int &iz)
+{
+  const int a = cidx % cn[0], r = cidx / cn[0];
+  ix = 2 * a + par[0];
+  iy = 2 * (r % cn[1]) + par[1];
+  iz = 2 * (r / cn[1]) + par[2];
+}
+
+// resident CTAs per SM requested from the register allocator
+template <int P, typename Real>
+struct WOcc {
+  static constexpr int min_blocks = (sizeof(Real) == 8) ? (P == 4 ? 4 : P >= 2 ? 5 : 6)
+                                                       : (P == 4 ? 6 : P == 3 ? 7 : 8);
+};
+
+template <int P, typename Real, int GEOM>
+__global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
+    warp_apply_kernel(const KP<Real> p, int *err)
 {
   constexpr int n = P + 1, n2 = n * n, n3 = n2 * n, CPW = WCfg<n>::cpw;
   constexpr int MS = metric_stride(n), VS = velb_stride(n);
@@ -172,62 +200,88 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32) warp_apply_kernel(const KP<
   __syncthreads();
 
   Real *wsm = reinterpret_cast<Real *>(smem_raw) + warp * warp_smem_elems<P, Real, GEOM>(gvel);
-  Real *stage = wsm;                                    // CPW * MS
-  Real *vstage = wsm + (GEOM == GEOM_GENERAL ? CPW * MS : 0);  // CPW * VS
+  Real *stage = wsm;
+  Real *vstage = wsm + (GEOM == GEOM_GENERAL ? CPW * MS : 0);
   Real *tiles = wsm + (GEOM == GEOM_GENERAL ? CPW * (MS + (gvel ? VS : 0)) : 0);
 
   const int sub = lane / n2, l = lane % n2, i = l % n, j = l / n;
   const bool lane_ok = sub < CPW;
-  Real *t0 = tiles + sub * n3;               // idle lanes get the scratch tile CPW
-  Real *t1 = tiles + (CPW + 1 + sub) * n3;
+  const int s_sub = lane_ok ? sub : 0;
+  Real *t0 = tiles + s_sub * n3;
+  Real *t1 = tiles + (CPW + s_sub) * n3;
   const long zs = p.NX * p.NY;
+  const int count = (int)p.ccount;
+  const int gstride = gridDim.x * kWarpsPerCTA;
   unsigned phase = 0;
 
-  for (long group = (long)blockIdx.x * kWarpsPerCTA + warp; group * CPW < p.ccount;
-       group += (long)gridDim.x * kWarpsPerCTA) {
-    const long c0 = group * CPW;
-    const int ncell = (int)min((long)CPW, p.ccount - c0);
-    if (GEOM == GEOM_GENERAL && lane == 0) {
-      fence_proxy_async();
-      const unsigned mb = ncell * MS * sizeof(Real), vb = gvel ? ncell * VS * sizeof(Real) : 0;
-      mbar_expect_tx(&bars[warp], mb + vb);
-      bulk_g2s(stage, p.metric + (p.cfirst + c0) * MS, mb, &bars[warp]);
-      if (gvel) bulk_g2s(vstage, p.velb + (p.cfirst + c0) * VS, vb, &bars[warp]);
-    }
-    const long cidx = c0 + sub;
-    const bool active = lane_ok && sub < ncell;
+  auto issue_stage = [&](int grp) {
+    const int c0 = grp * CPW;
+    const int ncell = min(CPW, count - c0);
+    const unsigned mb = ncell * MS * sizeof(Real), vb = gvel ? ncell * VS * sizeof(Real) : 0;
+    fence_proxy_async();
+    mbar_expect_tx(&bars[warp], mb + vb);
+    bulk_g2s(stage, p.metric + (p.cfirst + c0) * (long)MS, mb, &bars[warp]);
+    if (gvel) bulk_g2s(vstage, p.velb + (p.cfirst + c0) * (long)VS, vb, &bars[warp]);
+  };
+  // gathers the src column of the lane's cell in group grp (zeros when idle)
+  auto gather = [&](int grp, Real (&A)[n]) {
+    const int cidx = grp * CPW + sub;
+    const bool act = lane_ok && grp * CPW < count && cidx < count;
     int ix = 0, iy = 0, iz = 0;
-    if (active) {
-      const long a = cidx % p.cn[0], b = (cidx / p.cn[0]) % p.cn[1], c = cidx / ((long)p.cn[0] * p.cn[1]);
-      ix = 2 * (int)a + p.par[0];
-      iy = 2 * (int)b + p.par[1];
-      iz = 2 * (int)c + p.par[2];
-    }
-    const long cell = p.cfirst + cidx;
+    if (act) colour_cell(cidx, p.cn, p.par, ix, iy, iz);
     const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
-    const bool bflag = active && p.cell_flags && (p.cell_flags[cell] & 1);
-
-    Real u[n];
+    const bool bf = act && p.cell_flags && (p.cell_flags[p.cfirst + cidx] & 1);
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       Real v = 0;
-      if (active) {
+      if (act) {
         v = p.src[g0 + k * zs];
-        if (p.masked_read && bflag && p.dmask[g0 + k * zs]) v = 0;
+        if (p.masked_read && bf && p.dmask[g0 + k * zs]) v = 0;
       }
-      u[k] = v;
+      A[k] = v;
     }
-    Real Tq[n], Tgx[n], Tgy[n], Tgz[n];
-    if (KT) {
-      Real tl[n];
+  };
+
+  int group = blockIdx.x * kWarpsPerCTA + warp;
+  if (GEOM == GEOM_GENERAL && lane == 0 && group * CPW < count) issue_stage(group);
+  Real A[n];
+  gather(group, A);
+
+  for (; group * CPW < count; group += gstride) {
+    const int gnext = group + gstride;
+    const bool has_next = gnext * CPW < count;
+    const int cidx = group * CPW + sub;
+    const bool active = lane_ok && cidx < count;
+    int ix = 0, iy = 0, iz = 0;
+    if (active) colour_cell(cidx, p.cn, p.par, ix, iy, iz);
+    const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
+    const bool bflag = active && p.cell_flags && (p.cell_flags[p.cfirst + cidx] & 1);
+
+    // store-or-add decision and the early loads of the values to add to
+    const bool sx = (i == 0 && ix > 0) || (i == P && ix < p.nc[0] - 1);
+    const bool sy = (j == 0 && iy > 0) || (j == P && iy < p.nc[1] - 1);
+    const bool later_xy = (sx && (ix & 1)) || (sy && (iy & 1));
+    Real dpre[n];
+    unsigned first_bits = 0, mask_bits = 0;
 #pragma unroll
-      for (int k = 0; k < n; ++k) tl[k] = active ? p.T[g0 + k * zs] : Real(0);
-      w_to_qp<n>(sS, t1, i, j, tl, Tq);
-      if (p.full_tangent) w_grad_qp<n>(sDc, t1, i, j, Tq, Tgx, Tgy, Tgz);
+    for (int k = 0; k < n; ++k) {
+      const long g = g0 + k * zs;
+      const bool sz = (k == 0 && iz > 0) || (k == P && iz < p.nc[2] - 1);
+      const bool first = !(later_xy || (sz && (iz & 1)));
+      const bool masked = p.masked_write && bflag && p.dmask[g];
+      first_bits |= (unsigned)first << k;
+      mask_bits |= (unsigned)masked << k;
+      dpre[k] = (active && !first && !masked) ? p.dst[g] : Real(0);
     }
+
+    Real u[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) u[k] = A[k];
+    if (has_next) gather(gnext, A);
+
     Real uq[n], gx[n], gy[n], gz[n];
-    w_to_qp<n>(sS, t0, i, j, u, uq);
-    w_grad_qp<n>(sDc, t0, i, j, uq, gx, gy, gz);
+    w_to_qp<n>(T.S, sS, t0, lane_ok, i, j, u, uq);
+    w_grad_qp<n>(T.Dc, sDc, t0, lane_ok, i, j, uq, gx, gy, gz);
 
     if (GEOM == GEOM_GENERAL) {
       mbar_wait_bounded(&bars[warp], phase, err);
@@ -235,79 +289,55 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32) warp_apply_kernel(const KP<
     }
 
     Real val[n], fx[n], fy[n], fz[n];
-    const Real *ms = stage + (lane_ok ? sub : 0) * MS + j * n + i;
-    const Real *vs = vstage + (lane_ok ? sub : 0) * VS + j * n + i;
+    const Real *ms = stage + s_sub * MS + j * n + i;
+    const Real *vs = vstage + s_sub * VS + j * n + i;
 #pragma unroll
     for (int k = 0; k < n; ++k) {
-      Real JxW, G00, G01, G02, G11, G12, G22, b0 = 0, b1 = 0, b2 = 0;
+      Real b0 = 0, b1 = 0, b2 = 0;
       if (GEOM == GEOM_GENERAL) {
         const Real *m = ms + k * n2;
-        JxW = m[0];
-        G00 = m[n3];
-        G01 = m[2 * n3];
-        G02 = m[3 * n3];
-        G11 = m[4 * n3];
-        G12 = m[5 * n3];
-        G22 = m[6 * n3];
+        const Real cm = m[0], G00 = m[n3], G01 = m[2 * n3], G02 = m[3 * n3], G11 = m[4 * n3],
+                   G12 = m[5 * n3], G22 = m[6 * n3];
         if (gvel) {
-          b0 = vs[k * n2];
-          b1 = vs[k * n2 + n3];
-          b2 = vs[k * n2 + 2 * n3];
+          b0 = p.c_vel * vs[k * n2];
+          b1 = p.c_vel * vs[k * n2 + n3];
+          b2 = p.c_vel * vs[k * n2 + 2 * n3];
         }
+        val[k] = cm * uq[k] + (b0 * gx[k] + b1 * gy[k] + b2 * gz[k]);
+        fx[k] = G00 * gx[k] + G01 * gy[k] + G02 * gz[k];
+        fy[k] = G01 * gx[k] + G11 * gy[k] + G12 * gz[k];
+        fz[k] = G02 * gx[k] + G12 * gy[k] + G22 * gz[k];
       } else {
-        JxW = p.h[0] * p.h[1] * p.h[2] * T.w[i] * T.w[j] * T.w[k];
-        G00 = JxW / (p.h[0] * p.h[0]);
-        G11 = JxW / (p.h[1] * p.h[1]);
-        G22 = JxW / (p.h[2] * p.h[2]);
-        G01 = G02 = G12 = 0;
+        const Real JxW = p.h[0] * p.h[1] * p.h[2] * T.w[i] * T.w[j] * T.w[k];
         if (has_vel) {
           Real uv[3];
           uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, k, uv);
-          b0 = JxW * uv[0] / p.h[0];
-          b1 = JxW * uv[1] / p.h[1];
-          b2 = JxW * uv[2] / p.h[2];
+          b0 = p.c_vel * JxW * uv[0] / p.h[0];
+          b1 = p.c_vel * JxW * uv[1] / p.h[1];
+          b2 = p.c_vel * JxW * uv[2] / p.h[2];
         }
+        val[k] = p.c_mass * JxW * uq[k] + (b0 * gx[k] + b1 * gy[k] + b2 * gz[k]);
+        const Real kd = p.c_diff * JxW;
+        fx[k] = kd / (p.h[0] * p.h[0]) * gx[k];
+        fy[k] = kd / (p.h[1] * p.h[1]) * gy[k];
+        fz[k] = kd / (p.h[2] * p.h[2]) * gz[k];
       }
-      const Real kq = KT ? p.c_diff * (Real(1) + p.k_alpha * Tq[k]) : p.c_diff;
-      val[k] = p.c_mass * JxW * uq[k] + p.c_vel * (b0 * gx[k] + b1 * gy[k] + b2 * gz[k]);
-      if (GEOM == GEOM_GENERAL) {
-        fx[k] = kq * (G00 * gx[k] + G01 * gy[k] + G02 * gz[k]);
-        fy[k] = kq * (G01 * gx[k] + G11 * gy[k] + G12 * gz[k]);
-        fz[k] = kq * (G02 * gx[k] + G12 * gy[k] + G22 * gz[k]);
-      } else {
-        fx[k] = kq * G00 * gx[k];
-        fy[k] = kq * G11 * gy[k];
-        fz[k] = kq * G22 * gz[k];
-      }
-      if (KT && p.full_tangent) {
-        const Real dk = p.c_diff * p.k_alpha * uq[k];
-        if (GEOM == GEOM_GENERAL) {
-          fx[k] += dk * (G00 * Tgx[k] + G01 * Tgy[k] + G02 * Tgz[k]);
-          fy[k] += dk * (G01 * Tgx[k] + G11 * Tgy[k] + G12 * Tgz[k]);
-          fz[k] += dk * (G02 * Tgx[k] + G12 * Tgy[k] + G22 * Tgz[k]);
-        } else {
-          fx[k] += dk * G00 * Tgx[k];
-          fy[k] += dk * G11 * Tgy[k];
-          fz[k] += dk * G22 * Tgz[k];
-        }
-      }
+    }
+    if (GEOM == GEOM_GENERAL) {
+      // the stage is consumed: start the next group's copy now
+      __syncwarp();
+      if (lane == 0 && has_next) issue_stage(gnext);
     }
 
     Real out[n];
-    w_from_qp<n>(sS, sDc, t0, t1, i, j, val, fx, fy, fz, out);
+    w_from_qp<n>(T.S, sS, T.Dc, sDc, t0, t1, lane_ok, i, j, val, fx, fy, fz, out);
 
     if (active) {
-      const bool sx = (i == 0 && ix > 0) || (i == P && ix < p.nc[0] - 1);
-      const bool sy = (j == 0 && iy > 0) || (j == P && iy < p.nc[1] - 1);
-      const bool later_xy = (sx && (ix & 1)) || (sy && (iy & 1));
 #pragma unroll
       for (int k = 0; k < n; ++k) {
         const long g = g0 + k * zs;
-        const bool sz = (k == 0 && iz > 0) || (k == P && iz < p.nc[2] - 1);
-        const bool first = !(later_xy || (sz && (iz & 1)));
-        const bool masked = p.masked_write && bflag && p.dmask[g];
-        if (first) p.dst[g] = masked ? Real(0) : out[k];
-        else if (!masked) p.dst[g] += out[k];
+        if ((first_bits >> k) & 1) p.dst[g] = ((mask_bits >> k) & 1) ? Real(0) : out[k];
+        else if (!((mask_bits >> k) & 1)) p.dst[g] = dpre[k] + out[k];
       }
     }
   }

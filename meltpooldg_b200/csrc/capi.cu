@@ -139,7 +139,7 @@ mpdg_status mpdg_op_destroy(mpdg_op *op)
   if (!op) return MPDG_OK;
   Op &o = op->o;
   free_workspace(o);
-  for (void *p : {(void *)o.d_err, (void *)o.T32, (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32,
+  for (void *p : {(void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32, (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32,
                   (void *)o.d_trig64})
     if (p) cudaFree(p);
   delete op;
@@ -149,6 +149,7 @@ mpdg_status mpdg_op_destroy(mpdg_op *op)
 mpdg_status mpdg_op_reset_time_increment(mpdg_op *op, double dt)
 {
   if (!op || !(dt > 0.0)) return MPDG_ERR_ARG;
+  if (op->o.d.dt != dt) invalidate_coef(op->o);
   op->o.d.dt = dt;
   return MPDG_OK;
 }
@@ -166,6 +167,7 @@ mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *values)
     if (!op) throw Error{MPDG_ERR_ARG, "null operator"};
     if (field != MPDG_FIELD_TEMPERATURE) throw Error{MPDG_ERR_ARG, "unknown field"};
     op->o.T64 = values;
+    invalidate_coef(op->o);
     if (values && (op->o.d.precision_mask & (1 << MPDG_FP32))) ensure_T32(op->o);
     return MPDG_OK;
   });

@@ -86,6 +86,11 @@ struct Op {
   double *d_trig64 = nullptr;
   Workspace *ws = nullptr;
   int *d_err = nullptr;                // device error word (bounded waits that expired)
+  // merged per-quadrature-point coefficients for the general-geometry apply:
+  // [cell][7][n^3] = c_mass JxW, c_diff k(T_q) G (G = JxW J^-1 J^-T, 6 entries)
+  double *d_coef64 = nullptr;
+  float *d_coef32 = nullptr;
+  bool coef64_ok = false, coef32_ok = false;
   size_t device_bytes = 0;
 };
 
@@ -94,6 +99,8 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
 void ensure_metric32(Mesh &m, cudaStream_t s);
 void build_op_device_data(Op &op);
 void ensure_T32(Op &op);
+// marks the merged coefficient stream stale (new temperature field or dt)
+void invalidate_coef(Op &op);
 
 template <typename Real>
 void launch_apply(Op &op, Real *dst, const Real *src);

@@ -632,6 +632,63 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
   }
 }
 
+// ----------------------------------------------------- coefficient merge
+// coef[cell][0][q] = c_mass JxW, coef[cell][1+e][q] = c_diff k(T_q) G_e: the
+// per-quadrature-point data of the general-geometry apply, rebuilt whenever T
+// or dt change (T is constant during a linear solve)
+
+struct ColourSet {
+  Colour c[8];
+};
+
+template <int P, bool KT>
+__global__ void __launch_bounds__(128) merge_kernel(const KP<double> p, const ColourSet cs,
+                                                    long n_cells, double *coef64, float *coef32)
+{
+  constexpr int n = P + 1, n2 = n * n, n3 = n2 * n, CPB = Cfg<n>::cpb, MS = metric_stride(n);
+  __shared__ double sm[CPB][n3];
+  __shared__ double sS[n2];
+  const Tables<double> &T = tab<double>(P);
+  const int tid = threadIdx.x, slot = threadIdx.y;
+  const int i = tid % n, j = tid / n;
+  if (slot == 0) sS[tid] = T.S[tid];
+  __syncthreads();
+  const long cell = (long)blockIdx.x * CPB + slot;
+  const bool active = cell < n_cells;
+  int c = 0;
+  while (c < 7 && cell >= cs.c[c + 1].first) ++c;
+  const Colour &C = cs.c[c];
+  const long cidx = active ? cell - C.first : 0;
+  const int ix = 2 * (int)(cidx % C.cn[0]) + C.par[0];
+  const int iy = 2 * (int)((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
+  const int iz = 2 * (int)(cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
+  double Tq[n];
+  if (KT) {
+    const long zs = p.NX * p.NY;
+    const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
+    double tl[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) tl[k] = active ? p.T[g0 + k * zs] : 0.0;
+    to_qp<n>(sS, sm[slot], i, j, tl, Tq);
+  }
+  if (!active) return;
+#pragma unroll
+  for (int k = 0; k < n; ++k) {
+    const int q = k * n2 + j * n + i;
+    const double *m = p.metric + cell * MS + q;
+    const double kq = KT ? p.c_diff * (1.0 + p.k_alpha * Tq[k]) : p.c_diff;
+    double v[7];
+    v[0] = p.c_mass * m[0];
+#pragma unroll
+    for (int e = 1; e < 7; ++e) v[e] = kq * m[e * n3];
+#pragma unroll
+    for (int e = 0; e < 7; ++e) {
+      coef64[cell * MS + e * n3 + q] = v[e];
+      if (coef32) coef32[cell * MS + e * n3 + q] = (float)v[e];
+    }
+  }
+}
+
 // ------------------------------------------------------ geometry kernels
 
 // per (cell, qp): JxW and G = JxW J^-1 J^-T of the trilinear map, colour-major
@@ -926,7 +983,6 @@ void build_op_device_data(Op &op)
   const bool want32 = (op.d.precision_mask & (1 << MPDG_FP32)) != 0;
   op.d_err = dev_alloc<int>(1, op.device_bytes);
   MPDG_CUDA(cudaMemset(op.d_err, 0, sizeof(int)));
-  if (want32) ensure_metric32(m, op.stream);
   if (op.d.vel_kind == MPDG_VEL_NONE) return;
   if (!m.uniform) {
     Colour *d_col = nullptr;
@@ -1096,14 +1152,14 @@ int num_sms()
   return g_num_sms;
 }
 
-template <int P, typename Real, int GEOM, bool KT>
+template <int P, typename Real, int GEOM>
 void run_warp_apply(Op &op, KP<Real> k)
 {
   Mesh &m = *op.mesh;
   constexpr int n = P + 1, CPW = WCfg<n>::cpw;
   const bool gvel = GEOM == GEOM_GENERAL && op.d.vel_kind != MPDG_VEL_NONE;
   const size_t smem = sizeof(Real) * kWarpsPerCTA * warp_smem_elems<P, Real, GEOM>(gvel);
-  auto kern = warp_apply_kernel<P, Real, GEOM, KT>;
+  auto kern = warp_apply_kernel<P, Real, GEOM>;
   static int configured_smem = -1, blocks_per_sm = 0;  // per instantiation
   if (configured_smem != (int)smem) {
     MPDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1123,39 +1179,99 @@ void run_warp_apply(Op &op, KP<Real> k)
   }
 }
 
-template <typename Real, int GEOM, bool KT>
+template <typename Real, int GEOM>
 void warp_apply_degree(Op &op, const KP<Real> &k)
 {
   switch (op.mesh->degree) {
-    case 1: run_warp_apply<1, Real, GEOM, KT>(op, k); break;
-    case 2: run_warp_apply<2, Real, GEOM, KT>(op, k); break;
-    case 3: run_warp_apply<3, Real, GEOM, KT>(op, k); break;
-    case 4: run_warp_apply<4, Real, GEOM, KT>(op, k); break;
+    case 1: run_warp_apply<1, Real, GEOM>(op, k); break;
+    case 2: run_warp_apply<2, Real, GEOM>(op, k); break;
+    case 3: run_warp_apply<3, Real, GEOM>(op, k); break;
+    case 4: run_warp_apply<4, Real, GEOM>(op, k); break;
     default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
   }
 }
 
+template <int P, bool KT>
+void run_merge(Op &op, KP<double> k, double *c64, float *c32)
+{
+  Mesh &m = *op.mesh;
+  constexpr int n = P + 1, CPB = Cfg<n>::cpb;
+  ColourSet cs;
+  for (int c = 0; c < 8; ++c) cs.c[c] = m.colour[c];
+  const unsigned grid = (unsigned)((m.n_cells + CPB - 1) / CPB);
+  merge_kernel<P, KT><<<grid, dim3(n * n, CPB), 0, op.stream>>>(k, cs, m.n_cells, c64, c32);
+  MPDG_LAUNCHED();
+}
+
+// builds the merged coefficient stream of `op` in the requested precision
+void ensure_coef(Op &op, bool want32)
+{
+  Mesh &m = *op.mesh;
+  if (op.coef64_ok && (!want32 || op.coef32_ok)) return;
+  const size_t count = (size_t)m.n_cells * metric_stride(m.n);
+  if (!op.d_coef64) {
+    op.d_coef64 = dev_alloc<double>(count, op.device_bytes);
+    MPDG_CUDA(cudaMemsetAsync(op.d_coef64, 0, sizeof(double) * count, op.stream));
+  }
+  if (want32 && !op.d_coef32) {
+    op.d_coef32 = dev_alloc<float>(count, op.device_bytes);
+    MPDG_CUDA(cudaMemsetAsync(op.d_coef32, 0, sizeof(float) * count, op.stream));
+  }
+  KP<double> k = base_params<double>(op);
+  const bool kt = uses_kT(op);
+  if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
+  float *c32 = want32 ? op.d_coef32 : nullptr;
+  switch (m.degree) {
+    case 1: kt ? run_merge<1, true>(op, k, op.d_coef64, c32) : run_merge<1, false>(op, k, op.d_coef64, c32); break;
+    case 2: kt ? run_merge<2, true>(op, k, op.d_coef64, c32) : run_merge<2, false>(op, k, op.d_coef64, c32); break;
+    case 3: kt ? run_merge<3, true>(op, k, op.d_coef64, c32) : run_merge<3, false>(op, k, op.d_coef64, c32); break;
+    case 4: kt ? run_merge<4, true>(op, k, op.d_coef64, c32) : run_merge<4, false>(op, k, op.d_coef64, c32); break;
+    default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+  }
+  op.coef64_ok = true;
+  op.coef32_ok = want32;
+}
+
 }  // namespace
+
+void invalidate_coef(Op &op)
+{
+  op.coef64_ok = false;
+  op.coef32_ok = false;
+}
 
 template <typename Real>
 void launch_apply(Op &op, Real *dst, const Real *src)
 {
   Mesh &m = *op.mesh;
-  if (!m.uniform && sizeof(Real) == 4) ensure_metric32(m, op.stream);
+  const bool kt = uses_kT(op);
+  const bool full = op.d.kind == MPDG_OP_HEAT && op.d.full_tangent;
   if (!m.uniform && op.d.vel_kind != MPDG_VEL_NONE && sizeof(Real) == 4 && !op.d_velb32)
     throw Error{MPDG_ERR_ARG, "the FP32 form was not prepared for this operator (precision_mask)"};
   KP<Real> k = base_params<Real>(op);
   k.src = src;
   k.dst = dst;
-  const bool kt = uses_kT(op);
   if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
-  if (m.uniform) {
-    if (kt) warp_apply_degree<Real, GEOM_UNIFORM, true>(op, k);
-    else warp_apply_degree<Real, GEOM_UNIFORM, false>(op, k);
-  } else {
-    if (kt) warp_apply_degree<Real, GEOM_GENERAL, true>(op, k);
-    else warp_apply_degree<Real, GEOM_GENERAL, false>(op, k);
+  if (!full && !m.uniform) {
+    // general geometry: merged coefficient stream (k(T), c_mass, c_diff folded in)
+    ensure_coef(op, sizeof(Real) == 4);
+    if constexpr (sizeof(Real) == 8) k.metric = op.d_coef64;
+    else k.metric = op.d_coef32;
+    warp_apply_degree<Real, GEOM_GENERAL>(op, k);
+    return;
   }
+  if (!full && !kt) {
+    warp_apply_degree<Real, GEOM_UNIFORM>(op, k);
+    return;
+  }
+  // full Newton tangent, or k(T) on a uniform mesh: block kernel on raw geometry
+  if (!m.uniform && sizeof(Real) == 4) {
+    ensure_metric32(m, op.stream);
+    k.metric = (const Real *)(const void *)m.d_metric32;
+  }
+  MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * m.N, op.stream));
+  if (kt) dispatch_degree<Real, MODE_LINEAR, true>(op, k);
+  else dispatch_degree<Real, MODE_LINEAR, false>(op, k);
 }
 
 template void launch_apply<double>(Op &, double *, const double *);

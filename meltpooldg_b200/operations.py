@@ -91,6 +91,7 @@ class HeatDiffuseOperation:
 
     def solve(self):
         T = self.temperature
+        self.op.set_temperature(T)
         T_old = T.clone()
         rhs = torch.empty_like(T)
         dx = torch.empty_like(T)
@@ -105,6 +106,7 @@ class HeatDiffuseOperation:
                 self.newton_iterations.append(i)
                 return T
             T.add_(dx)
+            self.op.set_temperature(T)  # the operator linearises about the updated T
         raise RuntimeError("Newton-Raphson did not converge (ExcNewtonDidNotConverge)")
 
     def l2_norm(self):
