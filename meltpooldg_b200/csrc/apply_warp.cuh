@@ -151,14 +151,17 @@ __device__ __forceinline__ void w_from_qp(const Real *Sc, const Real *Ss, const 
   __syncwarp();
 }
 
-// dynamic shared memory per warp, in units of Real
+// dynamic shared memory per warp, in units of Real, rounded up to a multiple of
+// 8 elements so that every warp's stage starts on a 32-byte boundary (bulk
+// copies need 16-byte aligned shared-memory destinations)
 template <int P, typename Real, int GEOM>
 __host__ __device__ constexpr int warp_smem_elems(bool vel)
 {
   constexpr int n = P + 1, n3 = n * n * n, CPW = WCfg<n>::cpw;
-  return (GEOM == GEOM_GENERAL ? CPW * (metric_stride(n) + (vel ? velb_stride(n) : 0)) : 0) +
-         2 * CPW * n3;
+  return (((GEOM == GEOM_GENERAL ? CPW * (metric_stride(n) + (vel ? velb_stride(n) : 0)) : 0) +
+           2 * CPW * n3) + 7) / 8 * 8;
 }
+constexpr int kSmemAlign = 128;  // the dynamic shared-memory base is aligned by hand
 
 // cell (ix, iy, iz) of colour-local index cidx
 __device__ __forceinline__ void colour_cell(int cidx, const int cn[3], const int par[3], int &ix,
@@ -199,7 +202,8 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   fence_mbar_init();
   __syncthreads();
 
-  Real *wsm = reinterpret_cast<Real *>(smem_raw) + warp * warp_smem_elems<P, Real, GEOM>(gvel);
+  unsigned char *base = smem_raw + ((kSmemAlign - (smem_u32(smem_raw) & (kSmemAlign - 1))) & (kSmemAlign - 1));
+  Real *wsm = reinterpret_cast<Real *>(base) + warp * warp_smem_elems<P, Real, GEOM>(gvel);
   Real *stage = wsm;
   Real *vstage = wsm + (GEOM == GEOM_GENERAL ? CPW * MS : 0);
   Real *tiles = wsm + (GEOM == GEOM_GENERAL ? CPW * (MS + (gvel ? VS : 0)) : 0);

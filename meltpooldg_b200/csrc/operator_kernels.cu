@@ -1158,7 +1158,17 @@ void run_warp_apply(Op &op, KP<Real> k)
   Mesh &m = *op.mesh;
   constexpr int n = P + 1, CPW = WCfg<n>::cpw;
   const bool gvel = GEOM == GEOM_GENERAL && op.d.vel_kind != MPDG_VEL_NONE;
-  const size_t smem = sizeof(Real) * kWarpsPerCTA * warp_smem_elems<P, Real, GEOM>(gvel);
+  const size_t per_warp = sizeof(Real) * warp_smem_elems<P, Real, GEOM>(gvel);
+  const size_t smem = per_warp * kWarpsPerCTA + kSmemAlign;
+  // bulk-copy alignment contract, checked before any launch: 16-byte aligned
+  // shared destinations, global sources and sizes
+  static_assert((metric_stride(n) * sizeof(Real)) % 16 == 0, "metric stride");
+  static_assert((velb_stride(n) * sizeof(Real)) % 16 == 0, "velocity stride");
+  if (per_warp % 16 != 0) throw Error{MPDG_ERR_ARG, "per-warp shared memory not 16-byte aligned"};
+  if (GEOM == GEOM_GENERAL && ((uintptr_t)k.metric % 16 != 0 || (gvel && (uintptr_t)k.velb % 16 != 0)))
+    throw Error{MPDG_ERR_ARG, "coefficient stream not 16-byte aligned"};
+  if (GEOM == GEOM_GENERAL && (!k.metric || (gvel && !k.velb)))
+    throw Error{MPDG_ERR_ARG, "coefficient stream missing"};
   auto kern = warp_apply_kernel<P, Real, GEOM>;
   static int configured_smem = -1, blocks_per_sm = 0;  // per instantiation
   if (configured_smem != (int)smem) {
