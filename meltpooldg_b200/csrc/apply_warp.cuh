@@ -227,29 +227,31 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     bulk_g2s(stage, p.metric + (p.cfirst + c0) * (long)MS, mb, &bars[warp]);
     if (gvel) bulk_g2s(vstage, p.velb + (p.cfirst + c0) * (long)VS, vb, &bars[warp]);
   };
-  // gathers the src column of the lane's cell in group grp (zeros when idle)
-  auto gather = [&](int grp, Real (&A)[n]) {
+  // raw src column and constrained-DoF mask of the lane's cell in group grp;
+  // nothing here consumes a load, so the loads stay in flight while the
+  // current group is computed
+  const bool use_mask = p.cell_mask != nullptr && (p.masked_read || p.masked_write);
+  auto gather = [&](int grp, Real (&A)[n], uint4 &cm) {
     const int cidx = grp * CPW + sub;
     const bool act = lane_ok && grp * CPW < count && cidx < count;
     int ix = 0, iy = 0, iz = 0;
     if (act) colour_cell(cidx, p.cn, p.par, ix, iy, iz);
     const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
-    const bool bf = act && p.cell_flags && (p.cell_flags[p.cfirst + cidx] & 1);
 #pragma unroll
-    for (int k = 0; k < n; ++k) {
-      Real v = 0;
-      if (act) {
-        v = p.src[g0 + k * zs];
-        if (p.masked_read && bf && p.dmask[g0 + k * zs]) v = 0;
-      }
-      A[k] = v;
-    }
+    for (int k = 0; k < n; ++k) A[k] = act ? p.src[g0 + k * zs] : Real(0);
+    cm = (act && use_mask) ? p.cell_mask[p.cfirst + cidx] : make_uint4(0u, 0u, 0u, 0u);
+  };
+  auto mask_bit = [&](const uint4 &cm, int k) -> bool {
+    const int b = k * n2 + l;
+    const unsigned w = (b < 32) ? cm.x : (b < 64) ? cm.y : (b < 96) ? cm.z : cm.w;
+    return (w >> (b & 31)) & 1u;
   };
 
   int group = blockIdx.x * kWarpsPerCTA + warp;
   if (GEOM == GEOM_GENERAL && lane == 0 && group * CPW < count) issue_stage(group);
   Real A[n];
-  gather(group, A);
+  uint4 cmA;
+  gather(group, A, cmA);
 
   for (; group * CPW < count; group += gstride) {
     const int gnext = group + gstride;
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     int ix = 0, iy = 0, iz = 0;
     if (active) colour_cell(cidx, p.cn, p.par, ix, iy, iz);
     const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
-    const bool bflag = active && p.cell_flags && (p.cell_flags[p.cfirst + cidx] & 1);
+    const uint4 cm = cmA;
 
     // store-or-add decision and the early loads of the values to add to
     const bool sx = (i == 0 && ix > 0) || (i == P && ix < p.nc[0] - 1);
@@ -272,7 +274,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
       const long g = g0 + k * zs;
       const bool sz = (k == 0 && iz > 0) || (k == P && iz < p.nc[2] - 1);
       const bool first = !(later_xy || (sz && (iz & 1)));
-      const bool masked = p.masked_write && bflag && p.dmask[g];
+      const bool masked = p.masked_write && mask_bit(cm, k);
       first_bits |= (unsigned)first << k;
       mask_bits |= (unsigned)masked << k;
       dpre[k] = (active && !first && !masked) ? p.dst[g] : Real(0);
@@ -280,8 +282,8 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
 
     Real u[n];
 #pragma unroll
-    for (int k = 0; k < n; ++k) u[k] = A[k];
-    if (has_next) gather(gnext, A);
+    for (int k = 0; k < n; ++k) u[k] = (p.masked_read && mask_bit(cm, k)) ? Real(0) : A[k];
+    if (has_next) gather(gnext, A, cmA);
 
     Real uq[n], gx[n], gy[n], gz[n];
     w_to_qp<n>(T.S, sS, t0, lane_ok, i, j, u, uq);

@@ -91,7 +91,7 @@ mpdg_status mpdg_mesh_destroy(mpdg_mesh *mesh)
   if (!mesh) return MPDG_OK;
   Mesh &m = mesh->m;
   for (void *p : {(void *)m.d_vert, (void *)m.d_metric64, (void *)m.d_metric32, (void *)m.d_dmask,
-                  (void *)m.d_cell_flags})
+                  (void *)m.d_cell_flags, (void *)m.d_cell_mask})
     if (p) cudaFree(p);
   delete mesh;
   return MPDG_OK;

@@ -66,6 +66,8 @@ struct Mesh {
   float *d_metric32 = nullptr;
   uint8_t *d_dmask = nullptr;          // Dirichlet mask per DoF (nullptr: none)
   uint8_t *d_cell_flags = nullptr;     // per colour-major cell: bit0 touches a constrained DoF
+  uint32_t *d_cell_mask = nullptr;     // per colour-major cell: 128-bit mask of its constrained
+                                       // local DoFs (bit k*n*n + j*n + i)
   bool has_dirichlet = false;
   size_t device_bytes = 0;
   bool metric32_ready = false;

@@ -170,6 +170,7 @@ struct KP {
   const Real *trig;       // UNIFORM vortex: sin(pi x), cos(pi x), sin(pi y), cos(pi y)
   const uint8_t *dmask;
   const uint8_t *cell_flags;
+  const uint4 *cell_mask;
   long NX, NY;
   int nc[3];
   int trig_stride;
@@ -937,6 +938,7 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
   // Dirichlet mask and per-cell flags
   if (host_mask) {
     std::vector<uint8_t> flags(m.n_cells, 0);
+    std::vector<uint32_t> cmask(4 * (size_t)m.n_cells, 0u);
     bool any = false;
     for (int c = 0; c < 8; ++c) {
       const Colour &C = m.colour[c];
@@ -945,11 +947,15 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
         const int iy = 2 * (int)((k / C.cn[0]) % C.cn[1]) + C.par[1];
         const int iz = 2 * (int)(k / ((long)C.cn[0] * C.cn[1])) + C.par[2];
         uint8_t f = 0;
-        for (int kk = 0; kk <= p && !f; ++kk)
-          for (int jj = 0; jj <= p && !f; ++jj)
-            for (int ii = 0; ii <= p && !f; ++ii) {
+        for (int kk = 0; kk <= p; ++kk)
+          for (int jj = 0; jj <= p; ++jj)
+            for (int ii = 0; ii <= p; ++ii) {
               const long g = ((long)(iz * p + kk) * m.NY + (iy * p + jj)) * m.NX + (ix * p + ii);
-              if (host_mask[g]) f = 1;
+              if (host_mask[g]) {
+                f = 1;
+                const int bit = (kk * n + jj) * n + ii;
+                cmask[4 * (C.first + k) + bit / 32] |= 1u << (bit % 32);
+              }
             }
         flags[C.first + k] = f;
         any = any || f;
@@ -961,6 +967,9 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
       MPDG_CUDA(cudaMemcpy(m.d_dmask, host_mask, m.N, cudaMemcpyHostToDevice));
       m.d_cell_flags = dev_alloc<uint8_t>(m.n_cells, m.device_bytes);
       MPDG_CUDA(cudaMemcpy(m.d_cell_flags, flags.data(), m.n_cells, cudaMemcpyHostToDevice));
+      m.d_cell_mask = dev_alloc<uint32_t>(4 * (size_t)m.n_cells, m.device_bytes);
+      MPDG_CUDA(cudaMemcpy(m.d_cell_mask, cmask.data(), sizeof(uint32_t) * cmask.size(),
+                           cudaMemcpyHostToDevice));
     }
   }
 }
@@ -1077,6 +1086,7 @@ KP<Real> base_params(Op &op)
   k.trig_stride = std::max(m.nc[0], m.nc[1]) * m.n;
   k.dmask = m.d_dmask;
   k.cell_flags = m.d_cell_flags;
+  k.cell_mask = reinterpret_cast<const uint4 *>(m.d_cell_mask);
   const bool heat = op.d.kind == MPDG_OP_HEAT;
   k.c_mass = (Real)(heat ? op.d.rho_cp / op.d.dt : 1.0 / op.d.dt);
   k.c_vel = (Real)(heat ? op.d.rho_cp : op.d.theta);
