@@ -139,6 +139,8 @@ mpdg_status mpdg_op_use_dirichlet(mpdg_op *op, int use_dirichlet);
  * before the next vmult (the reference re-reads T in every vmult,
  * heat_diffuse_operator.cpp:1000-1012). */
 mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *device_values);
+/* the same with host values, copied into operator-owned device memory */
+mpdg_status mpdg_op_set_field_host(mpdg_op *op, int field, const double *host_values);
 mpdg_status mpdg_op_set_stream(mpdg_op *op, void *cuda_stream);
 /* reads and clears the operator's device error word: nonzero when a bounded
  * device-side wait (bulk-copy completion) expired; synchronises the stream */
@@ -157,6 +159,7 @@ mpdg_status mpdg_vmult_host(mpdg_op *op, double *dst_host, const double *src_hos
  * (heat: heat_diffuse_operator.cpp:271-284, threshold 1e-10;
  *  advection-diffusion: advection_diffusion_operator.cpp:401-446, threshold 1e-14 max(1,|d|inf)) */
 mpdg_status mpdg_compute_inverse_diagonal(mpdg_op *op, double *inv_diag);
+mpdg_status mpdg_compute_inverse_diagonal_host(mpdg_op *op, double *inv_diag_host);
 /* the diagonal itself (before inversion; constrained entries 1) */
 mpdg_status mpdg_compute_diagonal(mpdg_op *op, double *diag);
 
@@ -166,6 +169,9 @@ mpdg_status mpdg_compute_diagonal(mpdg_op *op, double *diag);
  * advection-diffusion (advection_diffusion_operator.cpp:276-358): src = phi_old,
  *   heat_source must be NULL; written to all DoFs unless Dirichlet rows are selected. */
 mpdg_status mpdg_create_rhs(mpdg_op *op, double *dst, const double *src, const double *heat_source);
+/* host-buffer form of mpdg_create_rhs (dst_host in/out) */
+mpdg_status mpdg_create_rhs_host(mpdg_op *op, double *dst_host, const double *src_host,
+                                 const double *heat_source_host);
 
 /* LinearSolver::solve, include/meltpooldg/linear_algebra/linear_solver.hpp:26-134,
  * with the Jacobi preconditioner of preconditioner_jacobi.hpp:29-88 (or the

@@ -100,6 +100,9 @@ def lib():
     L.mpdg_op_use_dirichlet.argtypes = [vp, C.c_int]
     L.mpdg_op_set_field.argtypes = [vp, C.c_int, vp]
     L.mpdg_op_set_stream.argtypes = [vp, vp]
+    L.mpdg_op_set_field_host.argtypes = [vp, C.c_int, dp]
+    L.mpdg_compute_inverse_diagonal_host.argtypes = [vp, dp]
+    L.mpdg_create_rhs_host.argtypes = [vp, dp, dp, dp]
     L.mpdg_op_device_error.argtypes = [vp, C.POINTER(C.c_int)]
     L.mpdg_vmult.argtypes = [vp, vp, vp]
     L.mpdg_vmult_f32.argtypes = [vp, vp, vp]

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "mpdg_internal.h"
 #include "vector_kernels.cuh"
@@ -139,7 +140,7 @@ mpdg_status mpdg_op_destroy(mpdg_op *op)
   if (!op) return MPDG_OK;
   Op &o = op->o;
   free_workspace(o);
-  for (void *p : {(void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32, (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32,
+  for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32, (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32,
                   (void *)o.d_trig64})
     if (p) cudaFree(p);
   delete op;
@@ -169,6 +170,26 @@ mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *values)
     op->o.T64 = values;
     invalidate_coef(op->o);
     if (values && (op->o.d.precision_mask & (1 << MPDG_FP32))) ensure_T32(op->o);
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_op_set_field_host(mpdg_op *op, int field, const double *values)
+{
+  return guarded([&]() -> int {
+    if (!op || !values) throw Error{MPDG_ERR_ARG, "null argument"};
+    if (field != MPDG_FIELD_TEMPERATURE) throw Error{MPDG_ERR_ARG, "unknown field"};
+    Op &o = op->o;
+    const size_t bytes = sizeof(double) * o.mesh->N;
+    if (!o.T_own) {
+      MPDG_CUDA(cudaMalloc(&o.T_own, bytes));
+      o.device_bytes += bytes;
+    }
+    MPDG_CUDA(cudaMemcpyAsync(o.T_own, values, bytes, cudaMemcpyHostToDevice, o.stream));
+    MPDG_CUDA(cudaStreamSynchronize(o.stream));
+    o.T64 = o.T_own;
+    invalidate_coef(o);
+    if (o.d.precision_mask & (1 << MPDG_FP32)) ensure_T32(o);
     return MPDG_OK;
   });
 }
@@ -245,6 +266,62 @@ mpdg_status mpdg_compute_inverse_diagonal(mpdg_op *op, double *inv_diag)
     if (!op || !inv_diag) throw Error{MPDG_ERR_ARG, "null argument"};
     launch_diagonal(op->o, inv_diag);
     launch_invert_diagonal(op->o, inv_diag);
+    return MPDG_OK;
+  });
+}
+
+namespace {
+// device staging of host vectors for the *_host entry points
+struct HostStage {
+  explicit HostStage(Op &o) : o(o) {}
+  double *up(const double *h)
+  {
+    if (!h) return nullptr;
+    double *d = nullptr;
+    const size_t bytes = sizeof(double) * o.mesh->N;
+    MPDG_CUDA(cudaMallocAsync(&d, bytes, o.stream));
+    bufs.push_back(d);
+    MPDG_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, o.stream));
+    return d;
+  }
+  void down(double *h, const double *d)
+  {
+    MPDG_CUDA(cudaMemcpyAsync(h, d, sizeof(double) * o.mesh->N, cudaMemcpyDeviceToHost, o.stream));
+  }
+  ~HostStage()
+  {
+    for (double *d : bufs) cudaFreeAsync(d, o.stream);
+    cudaStreamSynchronize(o.stream);
+  }
+  Op &o;
+  std::vector<double *> bufs;
+};
+}  // namespace
+
+mpdg_status mpdg_compute_inverse_diagonal_host(mpdg_op *op, double *inv_diag_host)
+{
+  return guarded([&]() -> int {
+    if (!op || !inv_diag_host) throw Error{MPDG_ERR_ARG, "null argument"};
+    HostStage st(op->o);
+    double *d = st.up(inv_diag_host);
+    launch_diagonal(op->o, d);
+    launch_invert_diagonal(op->o, d);
+    st.down(inv_diag_host, d);
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_create_rhs_host(mpdg_op *op, double *dst_host, const double *src_host,
+                                 const double *heat_source_host)
+{
+  return guarded([&]() -> int {
+    if (!op || !dst_host || !src_host) throw Error{MPDG_ERR_ARG, "null argument"};
+    HostStage st(op->o);
+    double *d = st.up(dst_host);
+    const double *s = st.up(src_host);
+    const double *q = st.up(heat_source_host);
+    launch_rhs(op->o, d, s, q);
+    st.down(dst_host, d);
     return MPDG_OK;
   });
 }

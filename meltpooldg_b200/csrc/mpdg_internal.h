@@ -80,7 +80,8 @@ struct Op {
   mpdg_op_desc d{};
   bool use_dirichlet = true;
   cudaStream_t stream = nullptr;
-  const double *T64 = nullptr;         // caller-owned temperature (device)
+  const double *T64 = nullptr;         // temperature (device): caller-owned, or T_own
+  double *T_own = nullptr;             // operator-owned copy set from host values
   float *T32 = nullptr;                // FP32 copy of T
   double *d_velb64 = nullptr;          // general geometry + velocity: [cell][3][n^3]
   float *d_velb32 = nullptr;
