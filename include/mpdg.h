@@ -183,6 +183,27 @@ mpdg_status mpdg_solve_host(mpdg_op *op, const mpdg_solver_desc *desc, double *x
                             const double *b_host, mpdg_solve_report *report);
 void mpdg_solver_desc_default(mpdg_solver_desc *desc);
 
+/* Jacobi-preconditioned CG (FP64) that allocates no device or pinned host
+ * memory: for callers that cannot allocate while they solve -- a host whose
+ * device memory is owned by its own pool or arena, a time loop that must not
+ * synchronise the device (cudaMalloc/cudaFree do), an application that allows
+ * no driver allocation after start-up.  It has no counterpart in the
+ * reference (which allocates its solver vectors per solve).
+ *
+ * Scratch (the CG vectors, the inverse diagonal, reduction partials and
+ * scalars) lives in one fixed __device__ array that every GPU loading the
+ * library holds until exit; problems larger than 262,144 DoFs are rejected
+ * with MPDG_ERR_SIZE.  The first call on a device resolves the array's device
+ * address (cudaGetSymbolAddress) with that device current: make that first
+ * call before any stream capture.  On a general (non-uniform) mesh the
+ * operator's coefficient stream must exist already (one mpdg_vmult first),
+ * else MPDG_ERR_ARG.  All calls on a device share the array: calls whose work
+ * overlaps on the GPU race and must be serialised by the caller.  Semantics as
+ * mpdg_solve with solver CG and preconditioner Jacobi; x holds the start. */
+mpdg_status mpdg_solve_cg_noalloc(mpdg_op *op, double *x, const double *b, double rel_tolerance,
+                                  double abs_tolerance, int max_iterations,
+                                  mpdg_solve_report *report);
+
 /* integrated L2 norm of a DoF vector (VectorTools::compute_norm,
  * source/utilities/vector_tools.cpp:170-201), FP64 */
 mpdg_status mpdg_l2_norm(mpdg_op *op, const double *u, double *norm);

@@ -115,6 +115,8 @@ def lib():
     L.mpdg_solver_desc_default.argtypes = [C.POINTER(SolverDesc)]
     L.mpdg_solver_desc_default.restype = None
     L.mpdg_l2_norm.argtypes = [vp, vp, dp]
+    L.mpdg_solve_cg_noalloc.argtypes = [vp, vp, vp, C.c_double, C.c_double, C.c_int,
+                                        C.POINTER(SolveReport)]
     _lib = L
     return L
 

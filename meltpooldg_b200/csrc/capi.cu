@@ -392,6 +392,21 @@ mpdg_status mpdg_solve_host(mpdg_op *op, const mpdg_solver_desc *desc, double *x
   return st;
 }
 
+mpdg_status mpdg_solve_cg_noalloc(mpdg_op *op, double *x, const double *b, double rel_tolerance,
+                                  double abs_tolerance, int max_iterations,
+                                  mpdg_solve_report *report)
+{
+  mpdg_solve_report local{};
+  int st = guarded([&]() -> int {
+    if (!op || !x || !b) throw Error{MPDG_ERR_ARG, "null argument"};
+    if (max_iterations < 1) throw Error{MPDG_ERR_ARG, "max_iterations must be positive"};
+    return solve_cg_noalloc(op->o, x, b, rel_tolerance, abs_tolerance, max_iterations, local);
+  });
+  local.status = st;
+  if (report) *report = local;
+  return st;
+}
+
 mpdg_status mpdg_l2_norm(mpdg_op *op, const double *u, double *norm)
 {
   return guarded([&]() -> int {

@@ -110,6 +110,10 @@ void launch_apply(Op &op, Real *dst, const Real *src);
 void launch_rhs(Op &op, double *dst, const double *src, const double *heat_source);
 void launch_diagonal(Op &op, double *diag);
 void launch_invert_diagonal(Op &op, double *diag);
+// inversion with a given threshold (no reduction, no allocation)
+void launch_invert_with_threshold(Op &op, double *diag, double thr);
+// true when an FP64 apply on `op` builds nothing lazily (no device allocation)
+bool apply_ready_without_allocation(const Op &op);
 double l2_norm_integrated(Op &op, const double *u);
 
 // ---- vector kernels (vector_kernels.cu)
@@ -124,5 +128,7 @@ double linf(const double *a, long n, cudaStream_t s);
 // ---- solvers (solvers.cu)
 int solve(Op &op, const mpdg_solver_desc &desc, double *x, const double *b, mpdg_solve_report &rep);
 void free_workspace(Op &op);
+int solve_cg_noalloc(Op &op, double *x, const double *b, double rel_tol, double abs_tol, int max_it,
+                     mpdg_solve_report &rep);
 
 }  // namespace mpdg

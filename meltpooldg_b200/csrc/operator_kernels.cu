@@ -1372,6 +1372,22 @@ void launch_invert_diagonal(Op &op, double *diag)
   MPDG_LAUNCHED();
 }
 
+void launch_invert_with_threshold(Op &op, double *diag, double thr)
+{
+  Mesh &m = *op.mesh;
+  const uint8_t *mask = (op.use_dirichlet && m.has_dirichlet) ? m.d_dmask : nullptr;
+  invert_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, mask, thr);
+  MPDG_LAUNCHED();
+}
+
+bool apply_ready_without_allocation(const Op &op)
+{
+  const Mesh &m = *op.mesh;
+  const bool full = op.d.kind == MPDG_OP_HEAT && op.d.full_tangent;
+  if (!full && !m.uniform) return op.coef64_ok;  // merged stream already built
+  return true;                                   // nothing is built lazily on these paths
+}
+
 }  // namespace mpdg
 
 namespace mpdg {
