@@ -92,7 +92,7 @@ typedef struct {
   double chebyshev_range;   /* lambda_min = lambda_max / range, default 30 */
   double chebyshev_safety;  /* lambda_max scaled by this, default 1.2 */
   int mixed_precision;      /* 1: FP32 inner CG + FP64 defect correction */
-  double inner_tolerance;   /* relative reduction of each inner FP32 solve, default 1e-4 */
+  double inner_tolerance;   /* relative reduction of each inner FP32 solve, default 3e-6 */
   int max_outer;            /* defect-correction steps, default 20 */
 } mpdg_solver_desc;
 

@@ -350,7 +350,7 @@ void mpdg_solver_desc_default(mpdg_solver_desc *d)
   d->chebyshev_range = 30.0;
   d->chebyshev_safety = 1.2;
   d->mixed_precision = 0;
-  d->inner_tolerance = 1e-4;
+  d->inner_tolerance = 3e-6;  // two defect-correction steps reach 1e-10
   d->max_outer = 20;
 }
 

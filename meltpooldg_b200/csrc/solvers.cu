@@ -286,27 +286,29 @@ int gmres(Op &op, Workspace &w, const Prec &P, const double *b, double *x, doubl
   return status;
 }
 
+// deterministic start vector in [-1, 1) (splitmix64 of the index and the
+// seed), zero on constrained DoFs, whose rows of A are zero
+__global__ void lanczos_start_kernel(double *v, long n, const uint8_t *mask, unsigned long long seed)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    unsigned long long z = seed + 0x9e3779b97f4a7c15ull * (unsigned long long)(i + 1);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);  // [0,1)
+    v[i] = (mask && mask[i]) ? 0.0 : 2.0 * u - 1.0;
+  }
+}
+
 // largest eigenvalue of D^-1 A from CG-Lanczos on A x = start
 double lanczos_lmax(Op &op, Workspace &w, int steps, int &applies)
 {
   const long N = op.mesh->N;
   cudaStream_t s = op.stream;
-  std::vector<double> h(N);
-  std::mt19937_64 rng(4);
-  std::uniform_real_distribution<double> U(-1.0, 1.0);
-  for (long i = 0; i < N; ++i) h[i] = U(rng);
   double *start = w.cd;
-  MPDG_CUDA(cudaMemcpyAsync(start, h.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
-  if (op.use_dirichlet && op.mesh->has_dirichlet) {
-    // constrained rows of A are zero: keep the start vector in the free space
-    std::vector<uint8_t> mk(N);
-    MPDG_CUDA(cudaMemcpyAsync(mk.data(), op.mesh->d_dmask, N, cudaMemcpyDeviceToHost, s));
-    MPDG_CUDA(cudaStreamSynchronize(s));
-    for (long i = 0; i < N; ++i)
-      if (mk[i]) h[i] = 0.0;
-    MPDG_CUDA(cudaMemcpyAsync(start, h.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
-  }
-  MPDG_CUDA(cudaStreamSynchronize(s));
+  const uint8_t *mask = (op.use_dirichlet && op.mesh->has_dirichlet) ? op.mesh->d_dmask : nullptr;
+  lanczos_start_kernel<<<1184, 256, 0, s>>>(start, N, mask, 4ull);
+  MPDG_LAUNCHED();
   double *r = w.r, *z = w.z, *p = w.p, *Ap = w.Ap, *sc = w.scal;
   dev_copy<double>(N, start, r, s);
   dev_mul<double>(N, w.invd, r, z, s);
@@ -411,7 +413,7 @@ int solve(Op &op, const mpdg_solver_desc &d, double *x, const double *b, mpdg_so
     res0 = std::sqrt(fetch(op, w, w.scal + kRR));
     res = res0;
     const double tol = std::fmax(abs_tol, rel * res0);
-    const double inner = d.inner_tolerance > 0 ? d.inner_tolerance : 1e-4;
+    const double inner = d.inner_tolerance > 0 ? d.inner_tolerance : 3e-6;
     const int max_outer = d.max_outer > 0 ? d.max_outer : 20;
     int outer = 0, total = 0;
     status = std::isfinite(res0) ? MPDG_OK : MPDG_ERR_NAN;

@@ -257,7 +257,7 @@ class LinearSolverData:
     chebyshev_range: float = 30.0
     chebyshev_safety: float = 1.2
     mixed_precision: bool = False
-    inner_tolerance: float = 1e-4
+    inner_tolerance: float = 3e-6
     max_outer: int = 20
 
     def desc(self):
