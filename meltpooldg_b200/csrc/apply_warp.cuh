@@ -151,180 +151,6 @@ __device__ __forceinline__ void w_from_qp(const Real *Sc, const Real *Ss, const 
   __syncwarp();
 }
 
-// ---- paired, vectorised passes (the production path)
-// A tile is written in the layout its next pass reads: for an x-pass rows run
-// along i (Tx[k][j][r]), for a y-pass along j (Ty[k][i][r]).  Rows are padded
-// to PT elements (16 bytes) and read with 128-bit shared loads; one row read
-// feeds two contractions (value and derivative tables).
-
-template <int n, typename Real>
-struct Pitch {
-  static constexpr int vw = 16 / (int)sizeof(Real);
-  static constexpr int v = (n + vw - 1) / vw * vw;
-};
-
-template <int PT, typename Real>
-__device__ __forceinline__ void load_row(const Real *p, Real (&v)[PT])
-{
-  if constexpr (sizeof(Real) == 8) {
-#pragma unroll
-    for (int r = 0; r < PT; r += 2) {
-      const double2 t = *reinterpret_cast<const double2 *>(p + r);
-      v[r] = t.x;
-      v[r + 1] = t.y;
-    }
-  } else {
-#pragma unroll
-    for (int r = 0; r < PT; r += 4) {
-      const float4 t = *reinterpret_cast<const float4 *>(p + r);
-      v[r] = t.x;
-      v[r + 1] = t.y;
-      v[r + 2] = t.z;
-      v[r + 3] = t.w;
-    }
-  }
-}
-
-template <int n, int PT, typename Real>
-__device__ __forceinline__ Real dotn(const Real (&a)[PT], const Real (&b)[PT])
-{
-  Real s = 0;
-#pragma unroll
-  for (int r = 0; r < n; ++r) s += a[r] * b[r];
-  return s;
-}
-
-template <int n, int PT, typename Real>
-__device__ __forceinline__ void put_x(Real *t, int i, int j, const Real (&v)[n])
-{
-#pragma unroll
-  for (int k = 0; k < n; ++k) t[(k * n + j) * PT + i] = v[k];
-}
-
-template <int n, int PT, typename Real>
-__device__ __forceinline__ void put_y(Real *t, int i, int j, const Real (&v)[n])
-{
-#pragma unroll
-  for (int k = 0; k < n; ++k) t[(k * n + i) * PT + j] = v[k];
-}
-
-// shared tables: S[q][i], D[q][i] (Gauss-Lobatto basis and its derivative at
-// the Gauss points) and their transposes, rows padded to PT
-template <int n, typename Real>
-struct SmemTables {
-  static constexpr int PT = Pitch<n, Real>::v;
-  __align__(16) Real S[n * PT];
-  __align__(16) Real D[n * PT];
-  __align__(16) Real St[n * PT];
-  __align__(16) Real Dt[n * PT];
-};
-
-// nodal column u -> value uq and reference gradient (gx, gy, gz) at the
-// lane's Gauss points; Ta, Tb, Tc: the cell's three tiles
-template <int n, typename Real>
-__device__ __forceinline__ void w_evaluate(const Tables<Real> &T, const SmemTables<n, Real> &st,
-                                           Real *Ta, Real *Tb, Real *Tc, bool wr, int i, int j,
-                                           const Real (&u)[n], Real (&uq)[n], Real (&gx)[n],
-                                           Real (&gy)[n], Real (&gz)[n])
-{
-  constexpr int PT = Pitch<n, Real>::v;
-  Real a[n];
-  cz<n, Real, false>(T.S, u, a);
-  if (wr) put_y<n, PT>(Ta, i, j, a);
-  __syncwarp();
-  Real b[n], c[n];
-  {
-    Real sj[PT], dj[PT];
-    load_row<PT>(st.S + j * PT, sj);
-    load_row<PT>(st.D + j * PT, dj);
-#pragma unroll
-    for (int k = 0; k < n; ++k) {
-      Real row[PT];
-      load_row<PT>(Ta + (k * n + i) * PT, row);
-      b[k] = dotn<n>(sj, row);
-      c[k] = dotn<n>(dj, row);
-    }
-  }
-  if (wr) {
-    put_x<n, PT>(Tb, i, j, b);
-    put_x<n, PT>(Tc, i, j, c);
-  }
-  __syncwarp();
-  {
-    Real si[PT], di[PT];
-    load_row<PT>(st.S + i * PT, si);
-    load_row<PT>(st.D + i * PT, di);
-#pragma unroll
-    for (int k = 0; k < n; ++k) {
-      Real r1[PT], r2[PT];
-      load_row<PT>(Tb + (k * n + j) * PT, r1);
-      load_row<PT>(Tc + (k * n + j) * PT, r2);
-      uq[k] = dotn<n>(si, r1);
-      gx[k] = dotn<n>(di, r1);
-      gy[k] = dotn<n>(si, r2);
-    }
-  }
-  cz<n, Real, false>(T.Dc, uq, gz);
-  __syncwarp();
-}
-
-// test with (val, reference flux fx, fy, fz) and return the nodal column
-template <int n, typename Real>
-__device__ __forceinline__ void w_integrate(const Tables<Real> &T, const SmemTables<n, Real> &st,
-                                            Real *Ta, Real *Tb, Real *Tc, bool wr, int i, int j,
-                                            const Real (&val)[n], const Real (&fx)[n],
-                                            const Real (&fy)[n], const Real (&fz)[n],
-                                            Real (&out)[n])
-{
-  constexpr int PT = Pitch<n, Real>::v;
-  Real w[n];
-  cz<n, Real, true>(T.Dc, fz, w);
-#pragma unroll
-  for (int k = 0; k < n; ++k) w[k] += val[k];
-  if (wr) {
-    put_x<n, PT>(Ta, i, j, w);
-    put_x<n, PT>(Tb, i, j, fx);
-    put_x<n, PT>(Tc, i, j, fy);
-  }
-  __syncwarp();
-  Real p1[n], p2[n];
-  {
-    Real si[PT], di[PT];
-    load_row<PT>(st.St + i * PT, si);
-    load_row<PT>(st.Dt + i * PT, di);
-#pragma unroll
-    for (int k = 0; k < n; ++k) {
-      Real rw[PT], rf[PT], ry[PT];
-      load_row<PT>(Ta + (k * n + j) * PT, rw);
-      load_row<PT>(Tb + (k * n + j) * PT, rf);
-      load_row<PT>(Tc + (k * n + j) * PT, ry);
-      p1[k] = dotn<n>(si, rw) + dotn<n>(di, rf);
-      p2[k] = dotn<n>(si, ry);
-    }
-  }
-  __syncwarp();
-  if (wr) {
-    put_y<n, PT>(Ta, i, j, p1);
-    put_y<n, PT>(Tb, i, j, p2);
-  }
-  __syncwarp();
-  Real q[n];
-  {
-    Real sj[PT], dj[PT];
-    load_row<PT>(st.St + j * PT, sj);
-    load_row<PT>(st.Dt + j * PT, dj);
-#pragma unroll
-    for (int k = 0; k < n; ++k) {
-      Real r1[PT], r2[PT];
-      load_row<PT>(Ta + (k * n + i) * PT, r1);
-      load_row<PT>(Tb + (k * n + i) * PT, r2);
-      q[k] = dotn<n>(sj, r1) + dotn<n>(dj, r2);
-    }
-  }
-  cz<n, Real, true>(T.S, q, out);
-  __syncwarp();
-}
-
 // dynamic shared memory per warp, in units of Real, rounded up to a multiple of
 // 8 elements so that every warp's stage starts on a 32-byte boundary (bulk
 // copies need 16-byte aligned shared-memory destinations)
@@ -332,10 +158,8 @@ template <int P, typename Real, int GEOM>
 __host__ __device__ constexpr int warp_smem_elems(bool vel)
 {
   constexpr int n = P + 1, n3 = n * n * n, CPW = WCfg<n>::cpw;
-  constexpr int tile = n * n * Pitch<n, Real>::v;
-  (void)n3;
   return (((GEOM == GEOM_GENERAL ? CPW * (metric_stride(n) + (vel ? velb_stride(n) : 0)) : 0) +
-           3 * CPW * tile) + 7) / 8 * 8;
+           2 * CPW * n3) + 7) / 8 * 8;
 }
 constexpr int kSmemAlign = 128;  // the dynamic shared-memory base is aligned by hand
 
@@ -353,7 +177,7 @@ __device__ __forceinline__ void colour_cell(int cidx, const int cn[3], const int
 template <int P, typename Real>
 struct WOcc {
   static constexpr int min_blocks = (sizeof(Real) == 8) ? (P == 4 ? 4 : P >= 2 ? 5 : 6)
-                                                       : (P == 4 ? 5 : P == 3 ? 6 : P == 2 ? 6 : 8);
+                                                       : (P == 4 ? 6 : P == 3 ? 7 : 8);
 };
 
 template <int P, typename Real, int GEOM>
@@ -364,20 +188,15 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   constexpr int MS = metric_stride(n), VS = velb_stride(n);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bars[kWarpsPerCTA];
-  __shared__ SmemTables<n, Real> st;
-  constexpr int PT = Pitch<n, Real>::v, TILE = n * n * PT;
+  __shared__ Real sS[n2], sDc[n2];
   const Tables<Real> &T = tab<Real>(P);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool has_vel = p.vel_kind != MPDG_VEL_NONE;
   const bool gvel = GEOM == GEOM_GENERAL && has_vel;
 
-  for (int t = threadIdx.x; t < n * PT; t += blockDim.x) {
-    const int a = t / PT, b = t % PT;
-    const bool in = b < n;
-    st.S[t] = in ? T.S[a * n + b] : Real(0);
-    st.D[t] = in ? T.D[a * n + b] : Real(0);
-    st.St[t] = in ? T.S[b * n + a] : Real(0);
-    st.Dt[t] = in ? T.D[b * n + a] : Real(0);
+  for (int t = threadIdx.x; t < n2; t += blockDim.x) {
+    sS[t] = T.S[t];
+    sDc[t] = T.Dc[t];
   }
   if (lane == 0) mbar_init(&bars[warp], 1);
   fence_mbar_init();
@@ -392,9 +211,8 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   const int sub = lane / n2, l = lane % n2, i = l % n, j = l / n;
   const bool lane_ok = sub < CPW;
   const int s_sub = lane_ok ? sub : 0;
-  Real *Ta = tiles + s_sub * TILE;
-  Real *Tb = tiles + (CPW + s_sub) * TILE;
-  Real *Tc = tiles + (2 * CPW + s_sub) * TILE;
+  Real *t0 = tiles + s_sub * n3;
+  Real *t1 = tiles + (CPW + s_sub) * n3;
   const long zs = p.NX * p.NY;
   const int count = (int)p.ccount;
   const int gstride = gridDim.x * kWarpsPerCTA;
@@ -468,7 +286,8 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     if (has_next) gather(gnext, A, cmA);
 
     Real uq[n], gx[n], gy[n], gz[n];
-    w_evaluate<n>(T, st, Ta, Tb, Tc, lane_ok, i, j, u, uq, gx, gy, gz);
+    w_to_qp<n>(T.S, sS, t0, lane_ok, i, j, u, uq);
+    w_grad_qp<n>(T.Dc, sDc, t0, lane_ok, i, j, uq, gx, gy, gz);
 
     if (GEOM == GEOM_GENERAL) {
       mbar_wait_bounded(&bars[warp], phase, err);
@@ -517,7 +336,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     }
 
     Real out[n];
-    w_integrate<n>(T, st, Ta, Tb, Tc, lane_ok, i, j, val, fx, fy, fz, out);
+    w_from_qp<n>(T.S, sS, T.Dc, sDc, t0, t1, lane_ok, i, j, val, fx, fy, fz, out);
 
     if (active) {
 #pragma unroll
