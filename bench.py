@@ -1,5 +1,6 @@
-"""Benchmark of the matrix-free heat operator on the config-2 workload.
+"""Benchmark of the matrix-free operators.
 
+Default workload (`--workload heat`, config 2):
 Workload (synthetic, seeded): unit cube, 64^3 hexahedra with interior vertices
 displaced by U[-0.1h, 0.1h] (PCG64 seed 2), FE_Q(4) (16,974,593 DoFs), heat
 operator M/dt + div(k(T) grad) with k(T) = k0 (1 + 1e-3 T), k0 = 1, rho c_p = 1,
@@ -11,6 +12,13 @@ timed steps the same operator is solved with CG + Chebyshev(5)/Jacobi to a
 relative residual of 1e-10 in the plain FP64 form and in the FP32-inner /
 FP64-defect-correction form (solves/s, iterations, error against the FP64
 solution, p50/p99 latency over repeated solves).
+
+`--workload advdiff` (config 3): unit cube, 128^3 uniform cells, FE_Q(2)
+(16,974,593 DoFs), theta-scheme advection-diffusion (theta = 0.5, D = 1e-3,
+dt = 1e-3) with u = (sin pi x cos pi y, -cos pi x sin pi y, 0) evaluated in the
+kernel; the solve is one time step of phi0 = tanh(d / 0.01),
+d = 0.25 - |x - (0.5, 0.75, 0.5)|, with GMRES(30) + Jacobi to 1e-10 in FP64 and
+in FP32-inner / FP64-defect-correction form.
 
 `--impl reference` times the CPU restatement of the reference's operator
 (the reference itself needs deal.II/Trilinos/p4est/MPI, which this image does
@@ -34,6 +42,8 @@ sys.path.insert(0, ROOT)
 METRIC = "mat-free DoFs/s & solves/s, FP32+FP64-refined vs FP64 at 1e-10; p50/p99 latency"
 NC, DEGREE = [64, 64, 64], 4
 DT, K0, K_ALPHA = 1e-3, 1.0, 1e-3
+WORKLOAD = {"name": "heat"}
+THETA, DIFFUSIVITY = 0.5, 1e-3
 
 # dram__bytes_read.sum + dram__bytes_write.sum per apply of the FP64 cell kernel
 # (8 colour launches), from the ncu capture summarised in
@@ -42,10 +52,15 @@ MEASURED_TRAFFIC_BYTES = None
 
 
 def algorithmic_bytes(n_dofs, n_cells, degree, real_bytes):
-    """src + dst + T (one read/write each) + the metric stream (JxW and the 6
-    entries of JxW J^-1 J^-T per quadrature point)."""
+    """Bytes one apply must move: src read + dst write, plus, on the perturbed
+    (general) mesh, the merged coefficient stream (c_mass JxW and the 6 entries
+    of c_diff k(T_q) JxW J^-1 J^-T per quadrature point).  The uniform
+    advection-diffusion mesh has no coefficient stream (geometry and velocity
+    are computed in the kernel)."""
     nq = (degree + 1) ** 3
-    return real_bytes * (3 * n_dofs) + real_bytes * 7 * nq * n_cells
+    if WORKLOAD["name"] == "advdiff":
+        return real_bytes * 2 * n_dofs
+    return real_bytes * (2 * n_dofs) + real_bytes * 7 * nq * n_cells
 
 
 def load_peaks():
@@ -113,6 +128,10 @@ class ClockSampler:
 
 def build_problem():
     import meltpooldg_b200 as M
+    if WORKLOAD["name"] == "advdiff":
+        V = M.box_vertices(NC)
+        mesh = M.Mesh(V, NC, DEGREE, None)
+        return M, V, None, mesh, None
     V = M.box_vertices(NC, perturb=0.1, seed=2)
     mask = M.boundary_mask(NC, DEGREE)
     mesh = M.Mesh(V, NC, DEGREE, mask)
@@ -120,11 +139,38 @@ def build_problem():
     return M, V, mask, mesh, T
 
 
+def make_operator(M, mesh, T):
+    import torch
+    if WORKLOAD["name"] == "advdiff":
+        return M.AdvectionDiffusionOperator(mesh, DT, theta=THETA, diffusivity=DIFFUSIVITY,
+                                            velocity="vortex", precisions=("fp64", "fp32")), None
+    op = M.HeatDiffuseOperator(mesh, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA,
+                               precisions=("fp64", "fp32"))
+    Td = torch.tensor(T, device="cuda")
+    op.set_temperature(Td)
+    return op, Td
+
+
+def oracle_operator(O, T, mask):
+    if WORKLOAD["name"] == "advdiff":
+        return O.Operator(O.ADVDIFF, DT, theta=THETA, diffusivity=DIFFUSIVITY, vel_kind=O.VEL_VORTEX)
+    return O.Operator(O.HEAT, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA, temperature=T, dirichlet=mask)
+
+
+def workload_config(N, E):
+    if WORKLOAD["name"] == "advdiff":
+        return {"workload": "advection-diffusion operator apply, Q2, 128^3 uniform hex cells, "
+                            "vortex velocity, theta=0.5, D=1e-3",
+                "n_dofs": N, "cells": E, "degree": DEGREE}
+    return {"workload": "heat operator apply, Q4, 64^3 perturbed hex cells, k(T)=k0(1+1e-3T)",
+            "n_dofs": N, "cells": E, "degree": DEGREE}
+
+
 def cpu_reference_rate(V, T, mask, n_dofs, target_seconds=10.0, cell_fraction=None):
     """Oracle apply over a contiguous block of cells; returns (DoFs/s, sample text, threads)."""
     from oracle import oracle as O
     om = O.Mesh(3, DEGREE, NC, V)
-    op = O.Operator(O.HEAT, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA, temperature=T, dirichlet=mask)
+    op = oracle_operator(O, T, mask)
     src = np.random.Generator(np.random.PCG64(0)).uniform(-1.0, 1.0, n_dofs)
     n_cells = int(np.prod(NC))
     # calibrate on a small block, then time a block of ~target_seconds
@@ -148,10 +194,13 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     from meltpooldg_b200.operators import box_vertices, boundary_mask
-    V = box_vertices(NC, perturb=0.1, seed=2)
-    mask = boundary_mask(NC, DEGREE)
     n_dofs = int(np.prod([n * DEGREE + 1 for n in NC]))
-    T = np.random.Generator(np.random.PCG64(3)).uniform(300.0, 3000.0, n_dofs)
+    if WORKLOAD["name"] == "advdiff":
+        V, mask, T = box_vertices(NC), None, None
+    else:
+        V = box_vertices(NC, perturb=0.1, seed=2)
+        mask = boundary_mask(NC, DEGREE)
+        T = np.random.Generator(np.random.PCG64(3)).uniform(300.0, 3000.0, n_dofs)
     # each step: a fixed sample of cells, sized so the whole run takes ~2.5 minutes
     per_step = max(0.05, min(4.0, 150.0 / (args.steps + args.warmup)))
     _, _, _, _ = cpu_reference_rate(V, T, mask, n_dofs, target_seconds=0.5)
@@ -170,9 +219,8 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "heat operator apply, Q4, 64^3 perturbed hex cells, k(T)=k0(1+1e-3T)",
-                   "n_dofs": n_dofs, "cells": int(np.prod(NC)), "degree": DEGREE,
-                   "sample": f"{frac:.5f} of the cells per step"},
+        "config": dict(workload_config(n_dofs, int(np.prod(NC))),
+                       sample=f"{frac:.5f} of the cells per step"),
         "cpu_baseline": {"value": value, "unit": "DoFs/s", "cores": threads, "kind": "port",
                          "sample": f"{frac * np.prod(NC):.0f} cells of one apply per step"},
         "e2e": {"value": value, "unit": "DoFs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -189,10 +237,7 @@ def run_ours(args, rank, world):
     torch.cuda.set_device(local)
     M, V, mask, mesh, T = build_problem()
     N = mesh.n_dofs
-    op = M.HeatDiffuseOperator(mesh, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA,
-                               precisions=("fp64", "fp32"))
-    Td = torch.tensor(T, device="cuda")
-    op.set_temperature(Td)
+    op, Td = make_operator(M, mesh, T)
     rng = np.random.Generator(np.random.PCG64(0))
     src = torch.tensor(rng.uniform(-1.0, 1.0, N), device="cuda")
     dst = torch.empty_like(src)
@@ -253,6 +298,8 @@ def run_ours(args, rank, world):
 
     peak, peak_kind = load_peaks()
     E = int(np.prod(NC))
+    geom = "UNIFORM" if WORKLOAD["name"] == "advdiff" else "GENERAL"
+    kernel_name = f"warp_apply_kernel<{DEGREE},double,{geom}> x 8 colour launches"
     b64 = algorithmic_bytes(N, E, DEGREE, 8)
     b32 = algorithmic_bytes(N, E, DEGREE, 4)
     roof = {"bound": "hbm", "achieved": b64 / apply_s / 1e9, "peak": peak, "unit": "GB/s",
@@ -266,19 +313,31 @@ def run_ours(args, rank, world):
     # solves: CG + Chebyshev(5)/Jacobi to 1e-10, FP64 and FP32-inner/FP64-refined
     solves = None
     if not args.no_solve:
-        xs = torch.tensor(np.random.Generator(np.random.PCG64(5)).uniform(-1, 1, N), device="cuda")
-        xs[torch.tensor(mask.astype(bool), device="cuda")] = 0.0
-        b = torch.empty_like(xs)
-        op.vmult(b, xs)
-        solves = {}
+        if WORKLOAD["name"] == "advdiff":
+            # one theta-scheme step of the tanh level set
+            X = [np.linspace(0.0, 1.0, n * DEGREE + 1) for n in NC]  # Q2 Gauss-Lobatto nodes are uniform
+            Z, Y, Xg = np.meshgrid(X[2], X[1], X[0], indexing="ij")
+            d = 0.25 - np.sqrt((Xg - 0.5) ** 2 + (Y - 0.75) ** 2 + (Z - 0.5) ** 2)
+            phi0 = torch.tensor(np.tanh(d / 0.01).reshape(-1), device="cuda")
+            b = torch.zeros_like(phi0)
+            op.create_rhs(b, phi0)
+            xs = None
+            solver_type, prec = "GMRES", "Diagonal"
+        else:
+            xs = torch.tensor(np.random.Generator(np.random.PCG64(5)).uniform(-1, 1, N), device="cuda")
+            xs[torch.tensor(mask.astype(bool), device="cuda")] = 0.0
+            b = torch.empty_like(xs)
+            op.vmult(b, xs)
+            solver_type, prec = "CG", "Chebyshev"
+        solves = {"solver": f"{solver_type} + {prec}"}
         ref_x = None
         for form, mixed in (("fp64", False), ("fp32_refined", True)):
-            data = M.LinearSolverData(solver_type="CG", preconditioner_type="Chebyshev",
+            data = M.LinearSolverData(solver_type=solver_type, preconditioner_type=prec,
                                       rel_tolerance=1e-10, abs_tolerance=1e-20, mixed_precision=mixed)
             lat = []
             rep = None
             for r in range(args.solve_reps):
-                x = torch.zeros_like(xs)
+                x = torch.zeros_like(b)
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
                 M.LinearSolver.solve(op, x, b, data)
@@ -296,7 +355,7 @@ def run_ours(args, rank, world):
                 "operator_applies": rep["operator_applies"],
                 "relative_residual": rep["final_residual"] / rep["initial_residual"],
                 "max_rel_error_vs_fp64_solution": err,
-                "max_rel_error_vs_exact": float((x - xs).abs().max() / xs.abs().max()),
+                "max_rel_error_vs_exact": None if xs is None else float((x - xs).abs().max() / xs.abs().max()),
             }
         solves["speedup_fp32_refined_vs_fp64"] = (solves["fp32_refined"]["solves_per_s"] /
                                                   solves["fp64"]["solves_per_s"])
@@ -311,9 +370,9 @@ def run_ours(args, rank, world):
             "metric": METRIC, "value": value, "unit": "DoFs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "heat operator apply, Q4, 64^3 perturbed hex cells, k(T)=k0(1+1e-3T)",
-                       "n_dofs": N, "cells": E, "degree": DEGREE, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (metric stream 1.8 GB per apply)"},
+            "config": dict(workload_config(N, E), parallelism=f"replicas x{world}",
+                           l2=("inputs larger than L2: src/dst 2 x 136 MB" if WORKLOAD["name"] == "advdiff"
+                               else "inputs larger than L2: coefficient stream 1.8 GB per apply")),
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": None if args.no_e2e else {
@@ -338,10 +397,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cells", type=int, default=64,
-                    help="cells per direction (64 is the benchmark workload; smaller sizes for profiling)")
+    ap.add_argument("--cells", type=int, default=0,
+                    help="cells per direction (default: the workload's; smaller sizes for profiling)")
+    ap.add_argument("--workload", default="heat", choices=["heat", "advdiff"])
     args = ap.parse_args()
-    NC[:] = [args.cells] * 3
+    WORKLOAD["name"] = args.workload
+    global DEGREE
+    if args.workload == "advdiff":
+        DEGREE = 2
+        NC[:] = [args.cells or 128] * 3
+    else:
+        NC[:] = [args.cells or 64] * 3
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if world > 1 and args.impl == "ours":

@@ -24,8 +24,10 @@ struct Workspace {
   // FP32 vectors
   float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *Ap32 = nullptr, *x32 = nullptr,
         *invd32 = nullptr, *cd32 = nullptr, *ct32 = nullptr;
-  double *V = nullptr;  // GMRES basis
+  double *V = nullptr;  // GMRES basis (FP64)
   int V_cols = 0;
+  float *V32 = nullptr;  // GMRES basis (FP32 inner solves)
+  int V32_cols = 0;
   double *partial = nullptr;  // reduction partials: 64 groups of kRedBlocks
   double *scal = nullptr;     // device scalars (kNScalars) + GMRES h (64)
   double *host = nullptr;     // pinned host mirror
@@ -185,30 +187,62 @@ int pcg(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero, d
   }
 }
 
-// right-preconditioned restarted GMRES (classical Gram-Schmidt applied twice)
-int gmres(Op &op, Workspace &w, const Prec &P, const double *b, double *x, double rel_tol,
+template <typename R>
+R *&gmres_basis(Workspace &w, int *&cols);
+template <>
+double *&gmres_basis<double>(Workspace &w, int *&cols)
+{
+  cols = &w.V_cols;
+  return w.V;
+}
+template <>
+float *&gmres_basis<float>(Workspace &w, int *&cols)
+{
+  cols = &w.V32_cols;
+  return w.V32;
+}
+
+template <typename R>
+void dot_any(const R *a, const R *b, long n, double *partial, double *out, cudaStream_t s)
+{
+  if constexpr (sizeof(R) == 8) dev_dot(a, b, n, partial, out, s);
+  else dev_dot_f(a, b, n, partial, out, s);
+}
+
+// right-preconditioned restarted GMRES (classical Gram-Schmidt applied twice),
+// vectors in R, Hessenberg and dot products in FP64
+template <typename R>
+int gmres(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero, double rel_tol,
           double abs_tol, int max_it, int restart, int &iters, double &res0, double &res,
           int &applies)
 {
   const long N = op.mesh->N;
   cudaStream_t s = op.stream;
-  V<double> v = vecs(w, (double *)nullptr);
+  V<R> v = vecs(w, (R *)nullptr);
   const int m = std::max(1, std::min(restart, 60));
-  if (!w.V || w.V_cols < m + 1) {
-    if (w.V) cudaFree(w.V);
-    w.V = walloc<double>(w, (size_t)N * (m + 1));
-    w.V_cols = m + 1;
+  int *cols = nullptr;
+  R *&VB = gmres_basis<R>(w, cols);
+  if (!VB || *cols < m + 1) {
+    if (VB) cudaFree(VB);
+    VB = walloc<R>(w, (size_t)N * (m + 1));
+    *cols = m + 1;
   }
   std::vector<double> H((m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), y(m), h(m + 1);
   iters = 0;
   double tol = -1.0;
   int status = MPDG_ERR_NOT_CONVERGED;
+  bool first = true;
   while (true) {
-    launch_apply<double>(op, v.Ap, x);
-    ++applies;
-    dev_copy<double>(N, b, w.V, s);
-    dev_axpby<double>(N, -1.0, v.Ap, 1.0, w.V, s);
-    dev_dot(w.V, w.V, N, w.partial, w.scal + kRR, s);
+    if (first && x_is_zero) {
+      dev_copy<R>(N, b, VB, s);
+    } else {
+      launch_apply<R>(op, v.Ap, x);
+      ++applies;
+      dev_copy<R>(N, b, VB, s);
+      dev_axpby<R>(N, -1.0, v.Ap, 1.0, VB, s);
+    }
+    first = false;
+    dot_any<R>(VB, VB, N, w.partial, w.scal + kRR, s);
     const double beta = std::sqrt(fetch(op, w, w.scal + kRR));
     if (tol < 0.0) {
       res0 = beta;
@@ -221,29 +255,29 @@ int gmres(Op &op, Workspace &w, const Prec &P, const double *b, double *x, doubl
       break;
     }
     if (iters >= max_it) break;
-    dev_axpby<double>(N, 0.0, w.V, 1.0 / beta, w.V, s);
+    dev_axpby<R>(N, 0.0, VB, 1.0 / beta, VB, s);
     std::fill(g.begin(), g.end(), 0.0);
     g[0] = beta;
     int j = 0;
     bool done = false;
     for (; j < m && iters < max_it; ++j) {
-      double *vj = w.V + (long)j * N, *vn = w.V + (long)(j + 1) * N;
-      prec_apply<double>(op, P, v, vj, v.z, applies);
-      launch_apply<double>(op, vn, v.z);
+      R *vj = VB + (long)j * N, *vn = VB + (long)(j + 1) * N;
+      prec_apply<R>(op, P, v, vj, v.z, applies);
+      launch_apply<R>(op, vn, v.z);
       ++applies;
       // two passes of classical Gram-Schmidt
       for (int k = 0; k <= j; ++k) h[k] = 0.0;
       for (int pass = 0; pass < 2; ++pass) {
-        dev_mdot(w.V, N, j + 1, vn, w.partial, w.scal + kNScalars, s);
+        dev_mdot<R>(VB, N, j + 1, vn, w.partial, w.scal + kNScalars, s);
         MPDG_CUDA(cudaMemcpyAsync(w.host, w.scal + kNScalars, sizeof(double) * (j + 1),
                                   cudaMemcpyDeviceToHost, s));
         MPDG_CUDA(cudaStreamSynchronize(s));
         for (int k = 0; k <= j; ++k) h[k] += w.host[k];
-        dev_mgs_update(w.V, N, j + 1, w.scal + kNScalars, vn, s);
+        dev_mgs_update<R>(VB, N, j + 1, w.scal + kNScalars, vn, s);
       }
-      dev_dot(vn, vn, N, w.partial, w.scal + kRR, s);
+      dot_any<R>(vn, vn, N, w.partial, w.scal + kRR, s);
       const double hn = std::sqrt(fetch(op, w, w.scal + kRR));
-      dev_axpby<double>(N, 0.0, vn, hn > 0 ? 1.0 / hn : 0.0, vn, s);
+      dev_axpby<R>(N, 0.0, vn, hn > 0 ? 1.0 / hn : 0.0, vn, s);
       for (int k = 0; k <= j; ++k) H[k * m + j] = h[k];
       H[(j + 1) * m + j] = hn;
       for (int k = 0; k < j; ++k) {
@@ -273,9 +307,9 @@ int gmres(Op &op, Workspace &w, const Prec &P, const double *b, double *x, doubl
       y[k] = t / H[k * m + k];
     }
     MPDG_CUDA(cudaMemcpyAsync(w.scal + kNScalars, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, s));
-    dev_combine(w.V, N, j, w.scal + kNScalars, v.ct, s);
-    prec_apply<double>(op, P, v, v.ct, v.z, applies);
-    dev_axpby<double>(N, 1.0, v.z, 1.0, x, s);
+    dev_combine<R>(VB, N, j, w.scal + kNScalars, v.ct, s);
+    prec_apply<R>(op, P, v, v.ct, v.z, applies);
+    dev_axpby<R>(N, 1.0, v.z, 1.0, x, s);
     MPDG_CUDA(cudaStreamSynchronize(s));  // y is read from pageable memory
     if (done) {
       status = MPDG_OK;
@@ -395,11 +429,10 @@ int solve(Op &op, const mpdg_solver_desc &d, double *x, const double *b, mpdg_so
     if (d.solver == MPDG_SOLVER_CG)
       status = pcg<double>(op, w, P, b, x, false, rel, abs_tol, max_it, it, res0, res, applies);
     else
-      status = gmres(op, w, P, b, x, rel, abs_tol, max_it, d.gmres_restart > 0 ? d.gmres_restart : 30,
-                     it, res0, res, applies);
+      status = gmres<double>(op, w, P, b, x, false, rel, abs_tol, max_it,
+                             d.gmres_restart > 0 ? d.gmres_restart : 30, it, res0, res, applies);
     rep.iterations = it;
   } else {
-    if (d.solver != MPDG_SOLVER_CG) throw Error{MPDG_ERR_UNSUPPORTED, "mixed precision uses CG"};
     Workspace &w32 = ws32(op);
     if (op.T64) ensure_T32(op);
     cast_down_kernel<<<1184, 256, 0, s>>>(w.invd, w32.invd32, N);
@@ -428,8 +461,12 @@ int solve(Op &op, const mpdg_solver_desc &d, double *x, const double *b, mpdg_so
       int it = 0;
       double r0i = 0, ri = 0;
       // the inner CG reads its rhs from z32 (copied into r32 by pcg)
-      int st = pcg<float>(op, w32, P, w32.z32, w32.x32, true, inner, 0.0,
-                          std::max(1, max_it - total), it, r0i, ri, applies);
+      int st = (d.solver == MPDG_SOLVER_CG)
+                   ? pcg<float>(op, w32, P, w32.z32, w32.x32, true, inner, 0.0,
+                                std::max(1, max_it - total), it, r0i, ri, applies)
+                   : gmres<float>(op, w32, P, w32.z32, w32.x32, true, inner, 0.0,
+                                  std::max(1, max_it - total), d.gmres_restart > 0 ? d.gmres_restart : 30,
+                                  it, r0i, ri, applies);
       total += it;
       if (st == MPDG_ERR_NAN) {
         status = st;
@@ -464,6 +501,7 @@ void free_workspace(Op &op)
   for (void *p : {(void *)w.r, (void *)w.z, (void *)w.p, (void *)w.Ap, (void *)w.invd, (void *)w.cd,
                   (void *)w.ct, (void *)w.r32, (void *)w.z32, (void *)w.p32, (void *)w.Ap32,
                   (void *)w.x32, (void *)w.invd32, (void *)w.cd32, (void *)w.ct32, (void *)w.V,
+                  (void *)w.V32,
                   (void *)w.partial, (void *)w.scal})
     if (p) cudaFree(p);
   if (w.host) cudaFreeHost(w.host);

@@ -97,37 +97,40 @@ __global__ void __launch_bounds__(kRedThreads) finish_kernel(const double *parti
   }
 }
 
-// multi-dot: partial[k][block] = V_k . w for k < m  (V rows of stride n)
-__global__ void __launch_bounds__(kRedThreads) mdot_partial_kernel(const double *V, long n, int m,
-                                                                   const double *w, double *partial)
+// multi-dot: partial[k][block] = V_k . w for k < m  (V rows of stride n), FP64 accumulation
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads) mdot_partial_kernel(const R *V, long n, int m,
+                                                                   const R *w, double *partial)
 {
   for (int k = 0; k < m; ++k) {
     double s = 0.0;
-    const double *v = V + (long)k * n;
+    const R *v = V + (long)k * n;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-      s += v[i] * w[i];
+      s += (double)v[i] * (double)w[i];
     s = block_sum(s);
     if (threadIdx.x == 0) partial[(long)k * kRedBlocks + blockIdx.x] = s;
   }
 }
 
 // w -= sum_k h[k] V_k
-__global__ void mgs_update_kernel(const double *V, long n, int m, const double *h, double *w)
+template <typename R>
+__global__ void mgs_update_kernel(const R *V, long n, int m, const double *h, R *w)
 {
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    double s = w[i];
-    for (int k = 0; k < m; ++k) s -= h[k] * V[(long)k * n + i];
-    w[i] = s;
+    double s = (double)w[i];
+    for (int k = 0; k < m; ++k) s -= h[k] * (double)V[(long)k * n + i];
+    w[i] = (R)s;
   }
 }
 
-// x += sum_k y[k] V_k
-__global__ void combine_kernel(const double *V, long n, int m, const double *y, double *x)
+// x = sum_k y[k] V_k
+template <typename R>
+__global__ void combine_kernel(const R *V, long n, int m, const double *y, R *x)
 {
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int k = 0; k < m; ++k) s += y[k] * V[(long)k * n + i];
-    x[i] = s;
+    for (int k = 0; k < m; ++k) s += y[k] * (double)V[(long)k * n + i];
+    x[i] = (R)s;
   }
 }
 
@@ -268,26 +271,34 @@ void dev_linf(const double *a, long n, double *partial, double *out, cudaStream_
   MPDG_LAUNCHED();
 }
 
-void dev_mdot(const double *V, long n, int m, const double *w, double *partial, double *out,
-              cudaStream_t s)
+template <typename R>
+void dev_mdot(const R *V, long n, int m, const R *w, double *partial, double *out, cudaStream_t s)
 {
-  mdot_partial_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(V, n, m, w, partial);
+  mdot_partial_kernel<R><<<kRedBlocks, kRedThreads, 0, s>>>(V, n, m, w, partial);
   MPDG_LAUNCHED();
   finish_kernel<<<m, kRedThreads, 0, s>>>(partial, m, out, 0);
   MPDG_LAUNCHED();
 }
+template void dev_mdot<double>(const double *, long, int, const double *, double *, double *, cudaStream_t);
+template void dev_mdot<float>(const float *, long, int, const float *, double *, double *, cudaStream_t);
 
-void dev_mgs_update(const double *V, long n, int m, const double *h, double *w, cudaStream_t s)
+template <typename R>
+void dev_mgs_update(const R *V, long n, int m, const double *h, R *w, cudaStream_t s)
 {
-  mgs_update_kernel<<<vgrid(n), 256, 0, s>>>(V, n, m, h, w);
+  mgs_update_kernel<R><<<vgrid(n), 256, 0, s>>>(V, n, m, h, w);
   MPDG_LAUNCHED();
 }
+template void dev_mgs_update<double>(const double *, long, int, const double *, double *, cudaStream_t);
+template void dev_mgs_update<float>(const float *, long, int, const double *, float *, cudaStream_t);
 
-void dev_combine(const double *V, long n, int m, const double *y, double *x, cudaStream_t s)
+template <typename R>
+void dev_combine(const R *V, long n, int m, const double *y, R *x, cudaStream_t s)
 {
-  combine_kernel<<<vgrid(n), 256, 0, s>>>(V, n, m, y, x);
+  combine_kernel<R><<<vgrid(n), 256, 0, s>>>(V, n, m, y, x);
   MPDG_LAUNCHED();
 }
+template void dev_combine<double>(const double *, long, int, const double *, double *, cudaStream_t);
+template void dev_combine<float>(const float *, long, int, const double *, float *, cudaStream_t);
 
 template <typename R>
 void dev_axpby(long n, double a, const R *x, double b, R *y, cudaStream_t s)

@@ -14,10 +14,12 @@ enum { kRZ = 0, kRZNEW = 1, kPAP = 2, kRR = 3, kNScalars = 8 };
 void dev_dot(const double *a, const double *b, long n, double *partial, double *out, cudaStream_t s);
 void dev_dot_f(const float *a, const float *b, long n, double *partial, double *out, cudaStream_t s);
 void dev_linf(const double *a, long n, double *partial, double *out, cudaStream_t s);
-void dev_mdot(const double *V, long n, int m, const double *w, double *partial, double *out,
-              cudaStream_t s);
-void dev_mgs_update(const double *V, long n, int m, const double *h, double *w, cudaStream_t s);
-void dev_combine(const double *V, long n, int m, const double *y, double *x, cudaStream_t s);
+template <typename R>
+void dev_mdot(const R *V, long n, int m, const R *w, double *partial, double *out, cudaStream_t s);
+template <typename R>
+void dev_mgs_update(const R *V, long n, int m, const double *h, R *w, cudaStream_t s);
+template <typename R>
+void dev_combine(const R *V, long n, int m, const double *y, R *x, cudaStream_t s);
 template <typename R>
 void dev_axpby(long n, double a, const R *x, double b, R *y, cudaStream_t s);
 void dev_residual(long n, const double *b, double *y, cudaStream_t s);
