@@ -91,15 +91,16 @@ typedef struct {
   int lanczos_steps;        /* eigenvalue estimate steps, default 10 */
   double chebyshev_range;   /* lambda_min = lambda_max / range, default 30 */
   double chebyshev_safety;  /* lambda_max scaled by this, default 1.2 */
-  int mixed_precision;      /* 1: FP32 inner CG + FP64 defect correction */
-  double inner_tolerance;   /* relative reduction of each inner FP32 solve, default 3e-6 */
-  int max_outer;            /* defect-correction steps, default 20 */
+  int mixed_precision;      /* 1: FP32 operator/preconditioner, FP64 defects, dots and update */
+  double inner_tolerance;   /* GMRES: relative reduction of each inner FP32 solve, default 3e-6 */
+  int max_outer;            /* GMRES: defect-correction steps, default 20 */
+  double reliable_delta;    /* CG: FP64 defect whenever the FP32 residual fell by this, default 0.1 */
 } mpdg_solver_desc;
 
 typedef struct {
   int status;               /* MPDG_OK or an error code */
   int iterations;           /* Krylov iterations (sum of inner ones when mixed) */
-  int outer_iterations;     /* defect-correction steps (mixed) */
+  int outer_iterations;     /* mixed: FP64 defect evaluations (CG) / correction steps (GMRES) */
   int operator_applies;     /* all operator applies, any precision */
   double initial_residual;  /* |b - A x0|_2 */
   double final_residual;    /* |b - A x|_2 in FP64 */

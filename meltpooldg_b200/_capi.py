@@ -58,7 +58,8 @@ class SolverDesc(C.Structure):
                 ("gmres_restart", C.c_int), ("chebyshev_degree", C.c_int),
                 ("lanczos_steps", C.c_int), ("chebyshev_range", C.c_double),
                 ("chebyshev_safety", C.c_double), ("mixed_precision", C.c_int),
-                ("inner_tolerance", C.c_double), ("max_outer", C.c_int)]
+                ("inner_tolerance", C.c_double), ("max_outer", C.c_int),
+                ("reliable_delta", C.c_double)]
 
 
 class SolveReport(C.Structure):

@@ -163,17 +163,18 @@ __host__ __device__ constexpr int warp_smem_elems(bool vel)
 }
 constexpr int kSmemAlign = 128;  // the dynamic shared-memory base is aligned by hand
 
-// cell (ix, iy, iz) of colour-local index cidx
-__device__ __forceinline__ void colour_cell(int cidx, const int cn[3], const int par[3], int &ix,
-                                            int &iy, int &iz)
+// cell (ix, iy, iz) of colour-local index cidx, by multiply-shift division
+template <typename KPT>
+__device__ __forceinline__ void colour_cell(int cidx, const KPT &p, int &ix, int &iy, int &iz)
 {
-  const int a = cidx % cn[0], r = cidx / cn[0];
-  ix = 2 * a + par[0];
-  iy = 2 * (r % cn[1]) + par[1];
-  iz = 2 * (r / cn[1]) + par[2];
+  const unsigned x = (unsigned)cidx;
+  const unsigned q0 = (unsigned)(((unsigned long long)x * p.div0_magic) >> 40);   // x / cn0
+  const unsigned q01 = (unsigned)(((unsigned long long)x * p.div01_magic) >> 40); // x / (cn0 cn1)
+  ix = 2 * (int)(x - q0 * (unsigned)p.cn[0]) + p.par[0];
+  iy = 2 * (int)(q0 - q01 * (unsigned)p.cn[1]) + p.par[1];
+  iz = 2 * (int)q01 + p.par[2];
 }
 
-// resident CTAs per SM requested from the register allocator
 template <int P, typename Real>
 struct WOcc {
   static constexpr int min_blocks = (sizeof(Real) == 8) ? (P == 4 ? 4 : P >= 2 ? 5 : 6)
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     const int cidx = grp * CPW + sub;
     const bool act = lane_ok && grp * CPW < count && cidx < count;
     int ix = 0, iy = 0, iz = 0;
-    if (act) colour_cell(cidx, p.cn, p.par, ix, iy, iz);
+    if (act) colour_cell(cidx, p, ix, iy, iz);
     const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
 #pragma unroll
     for (int k = 0; k < n; ++k) A[k] = act ? p.src[g0 + k * zs] : Real(0);
@@ -259,7 +260,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     const int cidx = group * CPW + sub;
     const bool active = lane_ok && cidx < count;
     int ix = 0, iy = 0, iz = 0;
-    if (active) colour_cell(cidx, p.cn, p.par, ix, iy, iz);
+    if (active) colour_cell(cidx, p, ix, iy, iz);
     const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
     const uint4 cm = cmA;
 
@@ -314,19 +315,20 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
         fy[k] = G01 * gx[k] + G11 * gy[k] + G12 * gz[k];
         fz[k] = G02 * gx[k] + G12 * gy[k] + G22 * gz[k];
       } else {
-        const Real JxW = p.h[0] * p.h[1] * p.h[2] * T.w[i] * T.w[j] * T.w[k];
+        const Real JxW = p.hvol * T.w[i] * T.w[j] * T.w[k];
         if (has_vel) {
           Real uv[3];
           uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, k, uv);
-          b0 = p.c_vel * JxW * uv[0] / p.h[0];
-          b1 = p.c_vel * JxW * uv[1] / p.h[1];
-          b2 = p.c_vel * JxW * uv[2] / p.h[2];
+          const Real cj = p.c_vel * JxW;
+          b0 = cj * uv[0] * p.ih[0];
+          b1 = cj * uv[1] * p.ih[1];
+          b2 = cj * uv[2] * p.ih[2];
         }
         val[k] = p.c_mass * JxW * uq[k] + (b0 * gx[k] + b1 * gy[k] + b2 * gz[k]);
         const Real kd = p.c_diff * JxW;
-        fx[k] = kd / (p.h[0] * p.h[0]) * gx[k];
-        fy[k] = kd / (p.h[1] * p.h[1]) * gy[k];
-        fz[k] = kd / (p.h[2] * p.h[2]) * gz[k];
+        fx[k] = kd * p.ih2[0] * gx[k];
+        fy[k] = kd * p.ih2[1] * gy[k];
+        fz[k] = kd * p.ih2[2] * gz[k];
       }
     }
     if (GEOM == GEOM_GENERAL) {

@@ -352,6 +352,7 @@ void mpdg_solver_desc_default(mpdg_solver_desc *d)
   d->mixed_precision = 0;
   d->inner_tolerance = 3e-6;  // two defect-correction steps reach 1e-10
   d->max_outer = 20;
+  d->reliable_delta = 0.1;
 }
 
 mpdg_status mpdg_solve(mpdg_op *op, const mpdg_solver_desc *desc, double *x, const double *b,

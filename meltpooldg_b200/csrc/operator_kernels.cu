@@ -175,7 +175,12 @@ struct KP {
   int nc[3];
   int trig_stride;
   int par[3], cn[3];
+  // exact division of a colour-local cell index by cn[0] and cn[0]*cn[1]:
+  // q = (x * magic) >> 40 with magic = ceil(2^40 / d), exact for x * d < 2^40
+  unsigned long long div0_magic, div01_magic;
   long ccount, cfirst;
+  // uniform geometry: 1/h, 1/h^2 and the cell volume, so the kernels divide nothing
+  Real ih[3], ih2[3], hvol;
   Real h[3], origin[3];
   Real c_mass, c_vel, c_diff, k_alpha;
   int vel_kind;
@@ -1072,6 +1077,11 @@ KP<Real> base_params(Op &op)
     k.vel_param[d] = (Real)op.d.vel_param[d];
   }
   k.vel_kind = op.d.vel_kind;
+  for (int d = 0; d < 3; ++d) {
+    k.ih[d] = (Real)(1.0 / m.h[d]);
+    k.ih2[d] = (Real)(1.0 / (m.h[d] * m.h[d]));
+  }
+  k.hvol = (Real)(m.h[0] * m.h[1] * m.h[2]);
   if constexpr (sizeof(Real) == 8) {
     k.metric = m.d_metric64;
     k.velb = op.d_velb64;
@@ -1108,6 +1118,14 @@ void colour_params(KP<Real> &k, const Colour &C)
   }
   k.ccount = C.count;
   k.cfirst = C.first;
+  const unsigned long long two40 = 1ull << 40;
+  const unsigned long long d0 = (unsigned long long)std::max(1, C.cn[0]);
+  const unsigned long long d01 = d0 * (unsigned long long)std::max(1, C.cn[1]);
+  k.div0_magic = (two40 + d0 - 1) / d0;
+  k.div01_magic = (two40 + d01 - 1) / d01;
+  // exactness of the magic division: x * d < 2^40 for every cell index x
+  if ((unsigned long long)C.count * d01 >= two40)
+    throw Error{MPDG_ERR_SIZE, "mesh too large for the colour index arithmetic"};
 }
 
 template <int P, typename Real, int MODE, bool KT>

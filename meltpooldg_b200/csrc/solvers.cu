@@ -187,6 +187,74 @@ int pcg(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero, d
   }
 }
 
+// FP32-inner CG with reliable updates: one FP32 CG recurrence (operator and
+// preconditioner in FP32, dot products accumulated in FP64) on the system
+// scaled by 1/|r0|; the solution is accumulated in FP64 (x += |r0| alpha p),
+// and whenever the iterated FP32 residual has dropped by `delta` since the
+// last true residual, the FP64 defect b - A x is computed and replaces it.
+// The search direction is kept, so no Krylov information is lost to restarts.
+int pcg_reliable(Op &op, Workspace &w, const Prec &P, const double *b, double *x, double rel_tol,
+                 double abs_tol, int max_it, double delta, int &iters, int &updates, double &res0,
+                 double &res, int &applies)
+{
+  const long N = op.mesh->N;
+  cudaStream_t s = op.stream;
+  V<float> v = vecs(w, (float *)nullptr);
+  double *sc = w.scal;
+  auto true_residual = [&]() {
+    launch_apply<double>(op, w.Ap, x);
+    ++applies;
+    dev_copy<double>(N, b, w.r, s);
+    dev_axpby<double>(N, -1.0, w.Ap, 1.0, w.r, s);
+    dev_dot(w.r, w.r, N, w.partial, sc + kRR, s);
+    return std::sqrt(fetch(op, w, sc + kRR));
+  };
+  res0 = true_residual();
+  res = res0;
+  iters = 0;
+  updates = 0;
+  if (!std::isfinite(res0)) return MPDG_ERR_NAN;
+  const double tol = std::fmax(abs_tol, rel_tol * res0);
+  if (res0 <= tol) return MPDG_OK;
+  const double scale = res0;
+  dev_scale_copy<float>(N, 1.0 / scale, w.r, v.r, s);
+  auto precondition = [&]() {
+    prec_apply<float>(op, P, v, v.r, v.z, applies);
+    dev_dot_f(v.r, v.z, N, w.partial, sc + kRZNEW, s);
+  };
+  precondition();
+  dev_copy<float>(N, v.z, v.p, s);
+  // rz <- rz_new
+  MPDG_CUDA(cudaMemcpyAsync(sc + kRZ, sc + kRZNEW, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  double rmax = 1.0;  // iterated residual at the last true residual, scaled
+  const bool fused_jacobi = P.kind == MPDG_PREC_JACOBI;
+  while (true) {
+    launch_apply<float>(op, v.Ap, v.p);
+    ++applies;
+    dev_dot_f(v.p, v.Ap, N, w.partial, sc + kPAP, s);
+    dev_cg_update<float, double>(N, sc, x, v.r, v.p, v.Ap, fused_jacobi ? v.invd : nullptr, v.z,
+                                 w.partial, s, scale);
+    ++iters;
+    const double rel = std::sqrt(fetch(op, w, sc + kRR));
+    if (!std::isfinite(rel)) return MPDG_ERR_NAN;
+    bool replaced = false;
+    if (rel * scale <= tol || rel < delta * rmax) {
+      res = true_residual();
+      ++updates;
+      if (!std::isfinite(res)) return MPDG_ERR_NAN;
+      if (res <= tol) return MPDG_OK;
+      dev_scale_copy<float>(N, 1.0 / scale, w.r, v.r, s);
+      rmax = res / scale;
+      replaced = true;
+    } else {
+      res = rel * scale;
+    }
+    if (iters >= max_it) return MPDG_ERR_NOT_CONVERGED;
+    if (!fused_jacobi || replaced) precondition();
+    dev_cg_direction<float>(N, sc, v.p, v.z, s);
+  }
+}
+
 template <typename R>
 R *&gmres_basis(Workspace &w, int *&cols);
 template <>
@@ -437,6 +505,22 @@ int solve(Op &op, const mpdg_solver_desc &d, double *x, const double *b, mpdg_so
     if (op.T64) ensure_T32(op);
     cast_down_kernel<<<1184, 256, 0, s>>>(w.invd, w32.invd32, N);
     MPDG_LAUNCHED();
+    if (d.solver == MPDG_SOLVER_CG) {
+      // CG: reliable updates (one FP32 Krylov recurrence, FP64 defects)
+      int it = 0, upd = 0;
+      status = pcg_reliable(op, w32, P, b, x, rel, abs_tol, max_it,
+                            (d.reliable_delta > 0 && d.reliable_delta < 1) ? d.reliable_delta : 0.1, it,
+                            upd, res0, res, applies);
+      rep.iterations = it;
+      rep.outer_iterations = upd;
+      MPDG_CUDA(cudaStreamSynchronize(s));
+      rep.status = status;
+      rep.operator_applies = applies;
+      rep.initial_residual = res0;
+      rep.final_residual = res;
+      rep.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      return status;
+    }
     // FP64 defect: r = b - A x
     launch_apply<double>(op, w.Ap, x);
     ++applies;
@@ -461,12 +545,9 @@ int solve(Op &op, const mpdg_solver_desc &d, double *x, const double *b, mpdg_so
       int it = 0;
       double r0i = 0, ri = 0;
       // the inner CG reads its rhs from z32 (copied into r32 by pcg)
-      int st = (d.solver == MPDG_SOLVER_CG)
-                   ? pcg<float>(op, w32, P, w32.z32, w32.x32, true, inner, 0.0,
-                                std::max(1, max_it - total), it, r0i, ri, applies)
-                   : gmres<float>(op, w32, P, w32.z32, w32.x32, true, inner, 0.0,
-                                  std::max(1, max_it - total), d.gmres_restart > 0 ? d.gmres_restart : 30,
-                                  it, r0i, ri, applies);
+      int st = gmres<float>(op, w32, P, w32.z32, w32.x32, true, inner, 0.0,
+                            std::max(1, max_it - total), d.gmres_restart > 0 ? d.gmres_restart : 30,
+                            it, r0i, ri, applies);
       total += it;
       if (st == MPDG_ERR_NAN) {
         status = st;

@@ -175,12 +175,13 @@ template <typename R, typename RX>
 __global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long n, const double *s, RX *x,
                                                                 R *r, const R *p, const R *Ap,
                                                                 const R *invd, R *z,
-                                                                double *partial)
+                                                                double *partial, double xscale)
 {
   const double alpha = s[kRZ] / s[kPAP];
+  const double xa = alpha * xscale;
   double rr = 0.0, rz = 0.0;
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    x[i] = (RX)((double)x[i] + alpha * (double)p[i]);
+    x[i] = (RX)((double)x[i] + xa * (double)p[i]);
     const R ri = (R)((double)r[i] - alpha * (double)Ap[i]);
     r[i] = ri;
     rr += (double)ri * (double)ri;
@@ -344,9 +345,10 @@ template void dev_mul<float>(long, const float *, const float *, float *, cudaSt
 
 template <typename R, typename RX>
 void dev_cg_update(long n, double *s, RX *x, R *r, const R *p, const R *Ap, const R *invd, R *z,
-                   double *partial, cudaStream_t st)
+                   double *partial, cudaStream_t st, double xscale)
 {
-  cg_update_kernel<R, RX><<<kRedBlocks, kRedThreads, 0, st>>>(n, s, x, r, p, Ap, invd, z, partial);
+  cg_update_kernel<R, RX><<<kRedBlocks, kRedThreads, 0, st>>>(n, s, x, r, p, Ap, invd, z, partial,
+                                                              xscale);
   MPDG_LAUNCHED();
   // rr -> s[kRR]; rz -> s[kRZNEW]
   finish_kernel<<<1, kRedThreads, 0, st>>>(partial, 1, s + kRR, 0);
@@ -358,10 +360,13 @@ void dev_cg_update(long n, double *s, RX *x, R *r, const R *p, const R *Ap, cons
 }
 template void dev_cg_update<double, double>(long, double *, double *, double *, const double *,
                                             const double *, const double *, double *, double *,
-                                            cudaStream_t);
+                                            cudaStream_t, double);
 template void dev_cg_update<float, float>(long, double *, float *, float *, const float *,
                                           const float *, const float *, float *, double *,
-                                          cudaStream_t);
+                                          cudaStream_t, double);
+template void dev_cg_update<float, double>(long, double *, double *, float *, const float *,
+                                           const float *, const float *, float *, double *,
+                                           cudaStream_t, double);
 
 template <typename R>
 void dev_cg_direction(long n, double *s, R *p, const R *z, cudaStream_t st)

@@ -31,7 +31,7 @@ template <typename R>
 void dev_mul(long n, const R *d, const R *x, R *y, cudaStream_t s);
 template <typename R, typename RX>
 void dev_cg_update(long n, double *s, RX *x, R *r, const R *p, const R *Ap, const R *invd, R *z,
-                   double *partial, cudaStream_t st);
+                   double *partial, cudaStream_t st, double xscale = 1.0);
 template <typename R>
 void dev_cg_direction(long n, double *s, R *p, const R *z, cudaStream_t st);
 template <typename R>

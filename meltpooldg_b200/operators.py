@@ -259,6 +259,7 @@ class LinearSolverData:
     mixed_precision: bool = False
     inner_tolerance: float = 3e-6
     max_outer: int = 20
+    reliable_delta: float = 0.1
 
     def desc(self):
         d = A.SolverDesc()
@@ -277,6 +278,7 @@ class LinearSolverData:
         d.mixed_precision = int(self.mixed_precision)
         d.inner_tolerance = self.inner_tolerance
         d.max_outer = self.max_outer
+        d.reliable_delta = self.reliable_delta
         return d
 
 
