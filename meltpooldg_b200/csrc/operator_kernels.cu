@@ -113,8 +113,6 @@ void lagrange(int n, const double *z, int i, double t, double &v, double &d)
 
 bool g_tables_ready = false;
 
-void upload_pair_tables(const Tables<double> *t64);
-
 void upload_tables()
 {
   if (g_tables_ready) return;
@@ -151,7 +149,6 @@ void upload_tables()
   }
   MPDG_CUDA(cudaMemcpyToSymbol(c_tab64, t64, sizeof(t64)));
   MPDG_CUDA(cudaMemcpyToSymbol(c_tab32, t32, sizeof(t32)));
-  upload_pair_tables(t64);
   g_tables_ready = true;
 }
 
@@ -325,31 +322,6 @@ __device__ __forceinline__ void uniform_velocity(const KP<Real> &p, const Tables
 }
 
 #include "apply_warp.cuh"
-#include "apply_pair.cuh"
-
-namespace {
-// row pairs of the 1D tables for the packed FP32 register passes
-void upload_pair_tables(const Tables<double> *t64)
-{
-  static PairTables pt[kMaxDegree + 1];
-  std::memset(pt, 0, sizeof(pt));
-  for (int p = 1; p <= kMaxDegree; ++p) {
-    const int n = p + 1, np = (n + 1) / 2;
-    const Tables<double> &t = t64[p];
-    auto at = [&](const double *M, int r, int c) { return (r < n && c < n) ? (float)M[r * n + c] : 0.f; };
-    for (int q = 0; q < np; ++q) {
-      for (int k = 0; k < n; ++k) {
-        pt[p].S[q * n + k] = make_float2(at(t.S, 2 * q, k), at(t.S, 2 * q + 1, k));
-        pt[p].St[q * n + k] = make_float2(at(t.S, k, 2 * q), at(t.S, k, 2 * q + 1));
-        pt[p].Dc[q * n + k] = make_float2(at(t.Dc, 2 * q, k), at(t.Dc, 2 * q + 1, k));
-        pt[p].Dct[q * n + k] = make_float2(at(t.Dc, k, 2 * q), at(t.Dc, k, 2 * q + 1));
-      }
-      pt[p].w[q] = make_float2((float)t.w[2 * q], 2 * q + 1 < n ? (float)t.w[2 * q + 1] : 0.f);
-    }
-  }
-  MPDG_CUDA(cudaMemcpyToSymbol(c_pair, pt, sizeof(pt)));
-}
-}  // namespace
 
 // ------------------------------------------------------------ the cell kernel
 
@@ -1245,60 +1217,8 @@ void run_warp_apply(Op &op, KP<Real> k)
   }
 }
 
-template <int P, int GEOM>
-void run_pair_apply(Op &op, KP<float> k)
-{
-  Mesh &m = *op.mesh;
-  constexpr int n = P + 1, CPW = WCfg<n>::cpw;
-  const bool gvel = GEOM == GEOM_GENERAL && op.d.vel_kind != MPDG_VEL_NONE;
-  const size_t per_warp = sizeof(float) * pair_smem_floats<P, GEOM>(gvel);
-  const size_t smem = per_warp * kWarpsPerCTA + kSmemAlign;
-  if (per_warp % 16 != 0) throw Error{MPDG_ERR_ARG, "per-warp shared memory not 16-byte aligned"};
-  if (GEOM == GEOM_GENERAL && ((uintptr_t)k.metric % 16 != 0 || (gvel && (uintptr_t)k.velb % 16 != 0)))
-    throw Error{MPDG_ERR_ARG, "coefficient stream not 16-byte aligned"};
-  if (GEOM == GEOM_GENERAL && (!k.metric || (gvel && !k.velb)))
-    throw Error{MPDG_ERR_ARG, "coefficient stream missing"};
-  auto kern = warp_apply_f2_kernel<P, GEOM>;
-  static int configured_smem = -1, blocks_per_sm = 0;
-  if (configured_smem != (int)smem) {
-    MPDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    MPDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerCTA * 32, smem));
-    if (blocks_per_sm < 1) blocks_per_sm = 1;
-    configured_smem = (int)smem;
-  }
-  const long resident = (long)num_sms() * blocks_per_sm;
-  for (int c = 0; c < 8; ++c) {
-    const Colour &C = m.colour[c];
-    if (C.count == 0) continue;
-    colour_params(k, C);
-    const long groups = (C.count + CPW - 1) / CPW;
-    const long blocks = std::min(resident, (groups + kWarpsPerCTA - 1) / kWarpsPerCTA);
-    kern<<<(unsigned)blocks, kWarpsPerCTA * 32, smem, op.stream>>>(k, op.d_err);
-    MPDG_LAUNCHED();
-  }
-}
-
-template <typename Real, int GEOM>
-void warp_apply_degree_scalar(Op &op, const KP<Real> &k);
-
 template <typename Real, int GEOM>
 void warp_apply_degree(Op &op, const KP<Real> &k)
-{
-  if constexpr (sizeof(Real) == 4) {
-    // FP32: packed FP32x2 plane pairs
-    switch (op.mesh->degree) {
-      case 1: run_pair_apply<1, GEOM>(op, k); return;
-      case 2: run_pair_apply<2, GEOM>(op, k); return;
-      case 3: run_pair_apply<3, GEOM>(op, k); return;
-      case 4: run_pair_apply<4, GEOM>(op, k); return;
-      default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
-    }
-  }
-  warp_apply_degree_scalar<Real, GEOM>(op, k);
-}
-
-template <typename Real, int GEOM>
-void warp_apply_degree_scalar(Op &op, const KP<Real> &k)
 {
   switch (op.mesh->degree) {
     case 1: run_warp_apply<1, Real, GEOM>(op, k); break;
