@@ -212,6 +212,79 @@ mpdg_status mpdg_l2_norm(mpdg_op *op, const double *u, double *norm);
 /* number of kernels this library launched since load (its own kernels only) */
 int64_t mpdg_kernel_launches(void);
 
+/* ------------------------------------------------------- batched solves
+ * Many independent problems advanced together on one GPU.  The reference
+ * solves one problem per process (LinearSolver::solve, linear_solver.hpp:26-134,
+ * called from heat_transfer_operation.cpp:300-330 and
+ * advection_diffusion_operation.cpp:228-262); a batch holds each admitted
+ * problem's vectors resident in device memory and advances every running
+ * problem by one Krylov step per CUDA-graph launch: one batched FP32 operator
+ * apply per degree and colour over all problems' cells, per-problem FP64 dots
+ * and norms, FP64 solution, and FP64 defects b - A x (FP64 operator) that
+ * replace the FP32 residual whenever it has dropped by the reliable-update
+ * factor, so the reported residual is an FP64 one.  Heat problems run CG,
+ * advection-diffusion problems BiCGStab, both Jacobi-preconditioned.  A
+ * problem's result does not depend on which other problems share the batch. */
+typedef struct mpdg_batch mpdg_batch;
+
+typedef struct {
+  int kind;              /* MPDG_OP_HEAT (CG) or MPDG_OP_ADVDIFF (BiCGStab) */
+  int degree;            /* 1..4 */
+  int nc;                /* cells per direction of the unit cube, 2..400 */
+  int dirichlet;         /* homogeneous Dirichlet on all faces (1) or none (0) */
+  int vel_kind;          /* advection-diffusion: MPDG_VEL_VORTEX or MPDG_VEL_NONE */
+  int max_iterations;    /* 0: the batch default */
+  double dt;             /* time increment */
+  double rho_cp, k0;     /* heat: rho c_p and conductivity */
+  double theta, diffusivity;         /* advection-diffusion */
+  double rel_tolerance, abs_tolerance;
+  uint64_t rhs_seed;     /* right-hand side: values in [-1,1) from this seed (0 on Dirichlet DoFs) */
+} mpdg_problem_desc;
+
+/* budget_bytes bounds the device memory of all admitted problems' vectors;
+ * capacity is the maximum number of problems held at once */
+mpdg_status mpdg_batch_create(int64_t budget_bytes, int capacity, double reliable_delta,
+                              mpdg_batch **batch);
+mpdg_status mpdg_batch_destroy(mpdg_batch *batch);
+/* device bytes a problem takes in a batch (its admission footprint) and its DoF count */
+mpdg_status mpdg_problem_bytes(const mpdg_problem_desc *desc, int64_t *bytes, int64_t *n_dofs);
+/* the seeded right-hand side of a problem, on the host (the values a batch uses) */
+mpdg_status mpdg_problem_rhs_host(const mpdg_problem_desc *desc, double *b_host);
+/* the FP64 Jacobi diagonal a batch uses for a problem (constrained entries 1) */
+mpdg_status mpdg_problem_diagonal_host(const mpdg_problem_desc *desc, double *diag_host);
+/* admits a problem: MPDG_ERR_BUDGET when its footprint does not fit the free
+ * budget or no slot is free (nothing is admitted then).  rhs_host may be NULL
+ * (seeded right-hand side) or n_dofs values.  Admission only enqueues work. */
+mpdg_status mpdg_batch_submit(mpdg_batch *batch, const mpdg_problem_desc *desc, const double *rhs_host,
+                              int64_t *ticket);
+/* runs up to max_steps Krylov steps (graph launches), checking every
+ * poll_steps steps whether problems are still running; returns the steps run
+ * and the problems still running */
+mpdg_status mpdg_batch_run(mpdg_batch *batch, int max_steps, int poll_steps, int *steps, int *running);
+/* state of one problem: report->status is 1 while it runs, else its final status */
+mpdg_status mpdg_batch_poll(mpdg_batch *batch, int64_t ticket, mpdg_solve_report *report);
+/* copies a finished problem's solution to the host (x_host may be NULL), fills
+ * the report and releases the problem's slot and memory */
+mpdg_status mpdg_batch_take(mpdg_batch *batch, int64_t ticket, double *x_host, mpdg_solve_report *report);
+/* picks the resident CTAs per SM of the batched apply by timing the current
+ * membership (call once problems are admitted); returns the choice and its time */
+mpdg_status mpdg_batch_autotune(mpdg_batch *batch, int *ctas_per_sm, double *apply_ms);
+/* device bytes admitted now */
+mpdg_status mpdg_batch_used_bytes(mpdg_batch *batch, int64_t *bytes);
+
+/* Serving loop: requests arrive at arrival_s[i] seconds after the call starts
+ * (ascending).  Each arrived request is admitted as soon as its footprint fits
+ * the batch's budget and a slot is free (first come, first served), joins the
+ * running problems at the next step, and leaves the batch when it finishes:
+ * its solution is copied to the host (into x_host[i] when x_host and
+ * x_host[i] are not NULL, else into a staging buffer) and its latency
+ * (completion - arrival) recorded.  poll_steps graph steps run between checks
+ * of finished problems.  latency_s, x_norm (|x|_2, FP64) and reports may be
+ * NULL; wall_s receives the time from the start to the last completion. */
+mpdg_status mpdg_serve(mpdg_batch *batch, const mpdg_problem_desc *requests, const double *arrival_s,
+                       int n_requests, int poll_steps, double **x_host, double *latency_s,
+                       double *x_norm, mpdg_solve_report *reports, double *wall_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,14 @@ class SolveReport(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ProblemDesc(C.Structure):
+    _fields_ = [("kind", C.c_int), ("degree", C.c_int), ("nc", C.c_int), ("dirichlet", C.c_int),
+                ("vel_kind", C.c_int), ("max_iterations", C.c_int), ("dt", C.c_double),
+                ("rho_cp", C.c_double), ("k0", C.c_double), ("theta", C.c_double),
+                ("diffusivity", C.c_double), ("rel_tolerance", C.c_double),
+                ("abs_tolerance", C.c_double), ("rhs_seed", C.c_uint64)]
+
+
 _lib = None
 
 
@@ -118,6 +126,21 @@ def lib():
     L.mpdg_l2_norm.argtypes = [vp, vp, dp]
     L.mpdg_solve_cg_noalloc.argtypes = [vp, vp, vp, C.c_double, C.c_double, C.c_int,
                                         C.POINTER(SolveReport)]
+    pd = C.POINTER(ProblemDesc)
+    i64p, ip = C.POINTER(C.c_int64), C.POINTER(C.c_int)
+    L.mpdg_batch_create.argtypes = [C.c_int64, C.c_int, C.c_double, C.POINTER(vp)]
+    L.mpdg_batch_destroy.argtypes = [vp]
+    L.mpdg_problem_bytes.argtypes = [pd, i64p, i64p]
+    L.mpdg_problem_rhs_host.argtypes = [pd, dp]
+    L.mpdg_problem_diagonal_host.argtypes = [pd, dp]
+    L.mpdg_batch_submit.argtypes = [vp, pd, dp, i64p]
+    L.mpdg_batch_run.argtypes = [vp, C.c_int, C.c_int, ip, ip]
+    L.mpdg_batch_poll.argtypes = [vp, C.c_int64, C.POINTER(SolveReport)]
+    L.mpdg_batch_take.argtypes = [vp, C.c_int64, dp, C.POINTER(SolveReport)]
+    L.mpdg_batch_autotune.argtypes = [vp, ip, dp]
+    L.mpdg_batch_used_bytes.argtypes = [vp, i64p]
+    L.mpdg_serve.argtypes = [vp, pd, dp, C.c_int, C.c_int, C.POINTER(dp), dp, dp,
+                             C.POINTER(SolveReport), dp]
     _lib = L
     return L
 

@@ -29,23 +29,6 @@ std::atomic<int64_t> g_launches{0};
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 void count_launch(int n) { g_launches += n; }
 
-template <typename F>
-int guarded(F &&f)
-{
-  try {
-    return f();
-  } catch (const Error &e) {
-    set_last_error(e.msg);
-    return e.status;
-  } catch (const std::bad_alloc &) {
-    set_last_error("host allocation failed");
-    return MPDG_ERR_ALLOC;
-  } catch (...) {
-    set_last_error("unknown error");
-    return MPDG_ERR_ARG;
-  }
-}
-
 }  // namespace mpdg
 
 using namespace mpdg;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -28,6 +29,24 @@ struct Error {
 
 void set_last_error(const std::string &msg);
 void count_launch(int n = 1);
+
+// runs the body of an extern "C" entry: internal errors become status codes
+template <typename F>
+int guarded(F &&f)
+{
+  try {
+    return f();
+  } catch (const Error &e) {
+    set_last_error(e.msg);
+    return e.status;
+  } catch (const std::bad_alloc &) {
+    set_last_error("host allocation failed");
+    return MPDG_ERR_ALLOC;
+  } catch (...) {
+    set_last_error("unknown error");
+    return MPDG_ERR_ARG;
+  }
+}
 
 #define MPDG_CUDA(call)                                                               \
   do {                                                                                \
@@ -97,7 +116,41 @@ struct Op {
   size_t device_bytes = 0;
 };
 
+// ---- batched apply over many solves (batch_apply.cuh / batch.cu)
+struct BatchSeg {
+  int slot;                        // solve slot
+  int nc;                          // cells per direction
+  int cn[3], par[3];               // this colour's cells per direction and parity
+  int count;                       // cells of this colour
+  unsigned long long div0_magic, div01_magic;
+  long NX;                         // DoFs per direction (nc*p + 1)
+};
+
+struct BatchSlotParams {
+  double c_mass, c_vel, c_diff;    // heat: rho_cp/dt, rho_cp, k0; advdiff: 1/dt, theta, theta D
+  double hvol, ih, ih2, h;
+  int vel_kind, dirichlet;
+};
+
+// segment tables of one batch membership: per degree (1..4) and colour
+struct BatchApplyPlan {
+  BatchSeg *segs[kMaxDegree + 1][8] = {};
+  int *prefix[kMaxDegree + 1][8] = {};
+  int nseg[kMaxDegree + 1][8] = {};
+  int groups[kMaxDegree + 1][8] = {};
+};
+
+// cells per warp of the warp-per-cell kernels for degree p (32 / (p+1)^2)
+int cells_per_warp(int degree);
+template <typename Real>
+void launch_batch_apply(const BatchApplyPlan &plan, const BatchSlotParams *params, Real *const *src,
+                        Real *const *dst, const int *active, int blocks_per_sm_cap, cudaStream_t s);
+
 // ---- operator kernels (operator_kernels.cu)
+// 1D tables of degree p on [0,1]: GLL Lagrange basis values S[q*(p+1)+i] and
+// derivatives D at the p+1 Gauss points x with weights w
+void shape_1d(int p, double *S, double *D, double *w, double *x);
+
 void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_general);
 void ensure_metric32(Mesh &m, cudaStream_t s);
 void build_op_device_data(Op &op);

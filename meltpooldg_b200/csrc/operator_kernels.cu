@@ -154,6 +154,16 @@ void upload_tables()
 
 }  // namespace
 
+void shape_1d(int p, double *S, double *D, double *w, double *x)
+{
+  const int n = p + 1;
+  double zl[kMaxN];
+  gauss(n, x, w);
+  lobatto(n, zl);
+  for (int q = 0; q < n; ++q)
+    for (int i = 0; i < n; ++i) lagrange(n, zl, i, x[q], S[q * n + i], D[q * n + i]);
+}
+
 // ------------------------------------------------------------ kernel params
 
 enum { MODE_LINEAR = 0, MODE_HEAT_RESIDUAL = 1 };
@@ -322,6 +332,7 @@ __device__ __forceinline__ void uniform_velocity(const KP<Real> &p, const Tables
 }
 
 #include "apply_warp.cuh"
+#include "batch_apply.cuh"
 
 // ------------------------------------------------------------ the cell kernel
 
@@ -1498,5 +1509,60 @@ double l2_norm_integrated(Op &op, const double *u)
   for (double v : h) s += v;
   return std::sqrt(s);
 }
+
+}  // namespace mpdg
+
+namespace mpdg {
+
+int cells_per_warp(int degree)
+{
+  switch (degree) {
+    case 1: return WCfg<2>::cpw;
+    case 2: return WCfg<3>::cpw;
+    case 3: return WCfg<4>::cpw;
+    case 4: return WCfg<5>::cpw;
+    default: return 1;
+  }
+}
+
+namespace {
+template <int P, typename Real>
+void run_batch_apply(const BatchApplyPlan &plan, const BatchSlotParams *params, Real *const *src,
+                     Real *const *dst, const int *active, int cap, cudaStream_t s)
+{
+  auto kern = batch_apply_kernel<P, Real>;
+  static int blocks_per_sm = 0;
+  if (!blocks_per_sm) {
+    upload_tables();
+    MPDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerCTA * 32, 0));
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  const int bps = (cap > 0) ? std::min(cap, blocks_per_sm) : blocks_per_sm;
+  for (int c = 0; c < 8; ++c) {
+    const int groups = plan.groups[P][c];
+    if (groups == 0) continue;
+    const long blocks = std::min((long)num_sms() * bps, (long)(groups + kWarpsPerCTA - 1) / kWarpsPerCTA);
+    kern<<<(unsigned)blocks, kWarpsPerCTA * 32, 0, s>>>(plan.segs[P][c], plan.prefix[P][c],
+                                                        plan.nseg[P][c], groups, params, src, dst, active);
+    MPDG_LAUNCHED();
+  }
+}
+}  // namespace
+
+template <typename Real>
+void launch_batch_apply(const BatchApplyPlan &plan, const BatchSlotParams *params, Real *const *src,
+                        Real *const *dst, const int *active, int cap, cudaStream_t s)
+{
+  run_batch_apply<1, Real>(plan, params, src, dst, active, cap, s);
+  run_batch_apply<2, Real>(plan, params, src, dst, active, cap, s);
+  run_batch_apply<3, Real>(plan, params, src, dst, active, cap, s);
+  run_batch_apply<4, Real>(plan, params, src, dst, active, cap, s);
+}
+template void launch_batch_apply<double>(const BatchApplyPlan &, const BatchSlotParams *,
+                                         double *const *, double *const *, const int *, int,
+                                         cudaStream_t);
+template void launch_batch_apply<float>(const BatchApplyPlan &, const BatchSlotParams *,
+                                        float *const *, float *const *, const int *, int,
+                                        cudaStream_t);
 
 }  // namespace mpdg
