@@ -305,7 +305,7 @@ def run_ours(args, rank, world):
     roof = {"bound": "hbm", "achieved": b64 / apply_s / 1e9, "peak": peak, "unit": "GB/s",
             "frac": b64 / apply_s / 1e9 / peak,
             "traffic": MEASURED_TRAFFIC_BYTES,
-            "algorithmic_bytes": b64, "kernel": "cell_kernel<4,double,GENERAL,LINEAR,kT> x 8 colours",
+            "algorithmic_bytes": b64, "kernel": kernel_name,
             "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
             "fp32": {"achieved": b32 / apply32_s / 1e9, "frac": b32 / apply32_s / 1e9 / peak,
                      "algorithmic_bytes": b32}}
@@ -386,6 +386,267 @@ def run_ours(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------- batched solves
+BATCH_SIZE = 256
+
+
+def batch_problems(n=BATCH_SIZE):
+    """256 heat problems: n^3 cells with n ~ U{8..48}, degree ~ U{2,3,4},
+    k0 log-uniform in [1, 100], rho c_p = 1, dt = 1e-3, Dirichlet on all faces,
+    seeded right-hand sides (seed 100 + i); PCG64 seed 4 draws the shapes."""
+    from meltpooldg_b200 import batch as B
+    rng = np.random.Generator(np.random.PCG64(4))
+    out = []
+    for i in range(n):
+        nc = int(rng.integers(8, 49))
+        p = int(rng.choice([2, 3, 4]))
+        k0 = float(np.exp(rng.uniform(0.0, np.log(100.0))))
+        out.append(B.Problem(kind=B.OP_HEAT, degree=p, nc=nc, k0=k0, dt=1e-3, rho_cp=1.0,
+                             rel_tolerance=1e-10, rhs_seed=100 + i))
+    return out
+
+
+def serve_requests(n_req, rate=200.0):
+    """Poisson arrivals (mean rate req/s, PCG64 seed 7): cells n^3 with
+    n = min(96, round(LogNormal(ln 24, 0.5))), degree ~ U{2,3,4}, half heat
+    (k0 = 1, rho c_p = 1) and half advection-diffusion (vortex velocity,
+    theta = 0.5, D = 1e-3), dt = 1e-3, tolerance 1e-10, seeds 1000 + i."""
+    from meltpooldg_b200 import batch as B
+    rng = np.random.Generator(np.random.PCG64(7))
+    arr = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    out = []
+    for i in range(n_req):
+        nc = int(min(96, max(2, round(float(rng.lognormal(np.log(24.0), 0.5))))))
+        p = int(rng.choice([2, 3, 4]))
+        kind = B.OP_HEAT if rng.uniform() < 0.5 else B.OP_ADVDIFF
+        out.append(B.Problem(kind=kind, degree=p, nc=nc, dt=1e-3, k0=1.0, rho_cp=1.0, theta=0.5,
+                             diffusivity=1e-3, rel_tolerance=1e-10, rhs_seed=1000 + i))
+    return out, arr
+
+
+def single_fp64_solve(M, prob, b_host):
+    """The plain FP64 GPU form of one problem: its own mesh and operator, CG
+    (heat) or GMRES(30) (advection-diffusion) with Jacobi to 1e-10; returns
+    (x on host, iterations)."""
+    import torch
+    nc = (prob.nc,) * 3
+    mesh = M.Mesh(M.box_vertices(nc), nc, prob.degree, M.boundary_mask(nc, prob.degree))
+    if prob.kind == 0:
+        op = M.HeatDiffuseOperator(mesh, prob.dt, rho_cp=prob.rho_cp, k0=prob.k0)
+        data = M.LinearSolverData(solver_type="CG", rel_tolerance=1e-10, abs_tolerance=0.0)
+    else:
+        op = M.AdvectionDiffusionOperator(mesh, prob.dt, theta=prob.theta, diffusivity=prob.diffusivity,
+                                          velocity="vortex")
+        data = M.LinearSolverData(solver_type="GMRES", rel_tolerance=1e-10, abs_tolerance=0.0)
+    b = torch.from_numpy(b_host).to("cuda")
+    x = torch.zeros_like(b)
+    its = M.LinearSolver.solve(op, x, b, data)
+    xh = x.cpu().numpy()
+    op.close()
+    mesh.close()
+    return xh, its
+
+
+def run_batch(args, rank, world):
+    """Config 4: 256 independent heat solves advanced together, one graph launch
+    per Krylov step.  A step is one whole batch: admission of the 256 problems
+    (device right-hand sides), the solve of all to 1e-10, release."""
+    import torch
+    import meltpooldg_b200 as M
+    from meltpooldg_b200 import batch as B
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    probs = batch_problems()
+    n_dofs = [p.n_dofs for p in probs]
+    N_total = int(sum(n_dofs))
+    budget = 150 * 10**9
+
+    def one_batch(e2e=False, tune=False, keep=False):
+        rhs = [p.rhs() for p in probs] if e2e else None
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with B.Batch(budget, capacity=len(probs)) as bt:
+            ts = [bt.submit(p, rhs=rhs[i] if e2e else None) for i, p in enumerate(probs)]
+            tune_res = bt.autotune() if tune else None
+            steps, _ = bt.run(poll_steps=16)
+            res = [bt.take(t, p.n_dofs if (e2e or keep) else None) for t, p in zip(ts, probs)]
+        t1 = time.perf_counter()
+        return t1 - t0, steps, res, tune_res
+
+    # warm-up (also the autotuner's pass over this membership)
+    _, _, _, tune_res = one_batch(tune=True)
+    cap, apply_ms = tune_res
+    for _ in range(max(0, args.warmup - 1)):
+        one_batch()
+    launches0 = M.kernel_launches()
+    times, graph_steps = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            dt, st, res, _ = one_batch()
+            times.append(dt)
+            graph_steps.append(st)
+    launches = M.kernel_launches() - launches0
+    reps = [r for _, r in res]
+    t_step = float(np.mean(times))
+    value = len(probs) * world / t_step
+
+    # end to end: host right-hand sides in, host solutions out
+    e2e_t, _, res_e2e, _ = one_batch(e2e=True)
+
+    # the plain FP64 GPU form of the same problems, one after another
+    t0 = time.perf_counter()
+    errs, its64 = [], []
+    for p, (xb, rb) in zip(probs, res_e2e):
+        x64, it = single_fp64_solve(M, p, p.rhs())
+        its64.append(it)
+        errs.append(float(np.linalg.norm(xb - x64) / max(np.linalg.norm(x64), 1e-300)))
+    t64 = time.perf_counter() - t0
+
+    peak, peak_kind = load_peaks()
+    b_apply = 2 * 4 * N_total  # FP32 src read + dst write of every problem
+    roof = {"bound": "hbm", "achieved": b_apply / (apply_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+            "frac": b_apply / (apply_ms * 1e-3) / 1e9 / peak, "traffic": None,
+            "algorithmic_bytes": b_apply,
+            "kernel": "batch_apply_kernel<P,float> (P = 2, 3, 4) x 8 colour launches each, all 256 problems",
+            "apply_ms": apply_ms, "autotuned_ctas_per_sm": cap,
+            "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_batch_rate(probs, its64, args.cpu_seconds)
+    if rank == 0:
+        iters = [r["iterations"] for r in reps]
+        line = {
+            "metric": "batched heat solves/s at 1e-10 (FP32 apply, FP64 residuals)", "value": value,
+            "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 apply / f64 residuals", "data": "synthetic",
+            "config": {"workload": "256 heat solves, n^3 cells n~U{8..48}, Q2/Q3/Q4, k0 log-uniform [1,100], "
+                                   "dt=1e-3, seeded rhs, CG + Jacobi to 1e-10",
+                       "n_dofs_total": N_total, "problems": len(probs),
+                       "l2": f"inputs larger than L2: {N_total * 44 / 1e9:.1f} GB resident",
+                       "timing": "host clock around synchronous batch calls (admission to release)"},
+            "roofline": roof, "cpu_baseline": cpu,
+            "e2e": {"value": len(probs) / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": 8 * N_total,
+                    "d2h_bytes_per_step": 8 * N_total,
+                    "call": "mpdg_batch_submit (host rhs) / mpdg_batch_run / mpdg_batch_take (host x)"},
+            "fp64_plain": {"solves_per_s": len(probs) / t64, "seconds": t64,
+                           "iterations_mean": float(np.mean(its64)),
+                           "speedup_batched_vs_fp64": value / (len(probs) / t64)},
+            "batched": {"graph_steps": graph_steps[-1], "iterations_mean": float(np.mean(iters)),
+                        "iterations_max": int(max(iters)),
+                        "all_converged": all(r["status"] == 0 for r in reps),
+                        "max_rel_residual": max(r["final_residual"] / r["initial_residual"] for r in reps),
+                        "max_rel_error_vs_fp64_solution": max(errs),
+                        "iteration_diff_vs_fp64_max": int(max(abs(a - b) for a, b in zip(iters, its64)))},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
+def cpu_batch_rate(probs, its64, seconds):
+    """Oracle FP64 CG + Jacobi solves of the smallest problems of the batch
+    until about `seconds` of CPU time; the rate per DoF-iteration scales to the
+    whole batch (sum of n_dofs x FP64 iterations)."""
+    from oracle import oracle as O
+    from meltpooldg_b200 import box_vertices
+    order = np.argsort([p.n_dofs for p in probs])
+    spent, work, done = 0.0, 0.0, 0
+    for i in order:
+        p = probs[i]
+        nc = (p.nc,) * 3
+        om = O.Mesh(3, p.degree, nc, box_vertices(nc))
+        op = O.Operator(O.HEAT, p.dt, rho_cp=p.rho_cp, k0=p.k0, dirichlet=om.boundary_face_mask())
+        b = p.rhs()
+        t0 = time.perf_counter()
+        inv = O.inverse_diagonal(om, op)
+        _, it, _, ok = O.cg(om, op, b, inv_diag=inv, rel_tol=1e-10, abs_tol=0.0)
+        spent += time.perf_counter() - t0
+        work += p.n_dofs * max(it, 1)
+        done += 1
+        if spent > seconds:
+            break
+    total_work = float(sum(p.n_dofs * max(it, 1) for p, it in zip(probs, its64)))
+    rate = len(probs) / (spent * total_work / work)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": rate, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"oracle CG+Jacobi of the {done} smallest problems ({spent:.1f} s), scaled by "
+                      f"n_dofs x iterations to all {len(probs)}"}
+
+
+def run_serve(args, rank, world):
+    """Config 5: Poisson stream of heat / advection-diffusion requests served by
+    the library's loop (continuous batching, 150 GB admission budget), against
+    the plain FP64 GPU form serving the same stream one request at a time."""
+    import torch
+    import meltpooldg_b200 as M
+    from meltpooldg_b200 import batch as B
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    n_req = args.requests
+    probs, arr = serve_requests(n_req)
+    budget = 150 * 10**9
+    # warm-up: a short stream
+    wp, wa = serve_requests(max(8, args.warmup * 4))
+    with B.Batch(budget, capacity=4096) as bt:
+        bt.serve(wp, wa * 0.0, poll_steps=4)
+    keep = list(range(0, n_req, max(1, n_req // 32)))
+    launches0 = M.kernel_launches()
+    with ClockSampler(local) as clk:
+        with B.Batch(budget, capacity=4096) as bt:
+            out = bt.serve(probs, arr, poll_steps=args.poll_steps, keep_solutions=keep)
+    launches = M.kernel_launches() - launches0
+    lat = np.sort(out["latency_s"])
+    reps = out["reports"]
+    value = n_req / out["wall_s"]
+
+    # plain FP64 GPU form on the same stream: one request at a time, FIFO
+    fp64 = None
+    if not args.no_fp64_arm:
+        n64 = min(n_req, args.fp64_requests)
+        lat64, errs = [], []
+        t0 = time.perf_counter()
+        for i in range(n64):
+            now = time.perf_counter() - t0
+            if arr[i] > now:
+                time.sleep(arr[i] - now)
+            x64, _ = single_fp64_solve(M, probs[i], probs[i].rhs())
+            lat64.append(time.perf_counter() - t0 - arr[i])
+            if out["solutions"] is not None and out["solutions"][i] is not None:
+                xb = out["solutions"][i]
+                errs.append(float(np.linalg.norm(xb - x64) / max(np.linalg.norm(x64), 1e-300)))
+        wall64 = time.perf_counter() - t0
+        lat64 = np.sort(np.asarray(lat64))
+        fp64 = {"requests": n64, "solves_per_s": n64 / wall64,
+                "p50_ms": 1e3 * float(np.percentile(lat64, 50)), "p99_ms": 1e3 * float(np.percentile(lat64, 99)),
+                "max_rel_error_batched_vs_fp64": max(errs) if errs else None,
+                "compared_solutions": len(errs)}
+    if rank == 0:
+        n_dofs = np.array([p.n_dofs for p in probs])
+        line = {
+            "metric": "served solves/s at 1e-10 with p50/p99 latency (continuous batching)",
+            "value": value, "unit": "solves/s", "n_gpus": world, "steps": 1, "warmup": args.warmup,
+            "ms_per_step": 1e3 * out["wall_s"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 apply / f64 residuals", "data": "synthetic",
+            "config": {"workload": f"Poisson stream, 200 req/s, {n_req} requests, n=min(96, LogNormal(ln 24, 0.5)), "
+                                   "Q2/Q3/Q4, 50% heat (CG) / 50% advection-diffusion (BiCGStab), 150 GB budget",
+                       "n_dofs_mean": float(n_dofs.mean()), "n_dofs_max": int(n_dofs.max()),
+                       "poll_steps": args.poll_steps,
+                       "timing": "host clock (request arrival to solution on the host)"},
+            "latency": {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                        "max_ms": 1e3 * float(lat[-1])},
+            "all_converged": all(r["status"] == 0 for r in reps),
+            "max_rel_residual": max(r["final_residual"] / max(r["initial_residual"], 1e-300) for r in reps),
+            "fp64_plain": fp64,
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(8 * n_dofs.sum()),
+                    "call": "mpdg_serve (device right-hand sides, solutions copied to the host)"},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -399,8 +660,15 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cells", type=int, default=0,
                     help="cells per direction (default: the workload's; smaller sizes for profiling)")
-    ap.add_argument("--workload", default="heat", choices=["heat", "advdiff"])
+    ap.add_argument("--workload", default="heat", choices=["heat", "advdiff", "batch", "serve"])
+    ap.add_argument("--requests", type=int, default=20000, help="serve: requests in the stream")
+    ap.add_argument("--poll-steps", type=int, default=4, help="serve: graph steps between checks")
+    ap.add_argument("--no-fp64-arm", action="store_true", help="serve: skip the plain FP64 arm")
+    ap.add_argument("--fp64-requests", type=int, default=2000,
+                    help="serve: requests of the stream the plain FP64 arm serves")
     args = ap.parse_args()
+    if args.workload in ("batch", "serve") and args.steps == 400:
+        args.steps = 2 if args.workload == "batch" else 1
     WORKLOAD["name"] = args.workload
     global DEGREE
     if args.workload == "advdiff":
@@ -418,6 +686,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload == "batch":
+            run_batch(args, rank, world)
+        elif args.workload == "serve":
+            run_serve(args, rank, world)
         else:
             run_ours(args, rank, world)
     finally:

@@ -155,10 +155,11 @@ class Batch:
         check(lib().mpdg_batch_used_bytes(self._h, C.byref(b)), "mpdg_batch_used_bytes")
         return int(b.value)
 
-    def serve(self, problems, arrival_s, poll_steps: int = 4, keep_solutions: bool = False):
+    def serve(self, problems, arrival_s, poll_steps: int = 4, keep_solutions=False):
         """Runs the library's serving loop over requests arriving at arrival_s
         (seconds from the call, ascending).  Returns a dict with per-request
-        latency_s, x_norm, reports, the wall time, and the solutions when asked."""
+        latency_s, x_norm, reports, the wall time, and the solutions when asked
+        (keep_solutions: True for all, or an iterable of request indices)."""
         n = len(problems)
         arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
         if arr.size != n:
@@ -170,10 +171,13 @@ class Batch:
         wall = C.c_double()
         sols = None
         xptrs = None
-        if keep_solutions:
-            sols = [np.empty(p.n_dofs, dtype=np.float64) for p in problems]
+        if keep_solutions is not False and keep_solutions is not None:
+            keep = set(range(n)) if keep_solutions is True else set(int(i) for i in keep_solutions)
+            sols = [np.empty(p.n_dofs, dtype=np.float64) if i in keep else None
+                    for i, p in enumerate(problems)]
             xptrs = (C.POINTER(C.c_double) * max(1, n))(
-                *[s.ctypes.data_as(C.POINTER(C.c_double)) for s in sols])
+                *[s.ctypes.data_as(C.POINTER(C.c_double)) if s is not None else C.POINTER(C.c_double)()
+                  for s in sols])
         dp = C.POINTER(C.c_double)
         check(lib().mpdg_serve(self._h, descs, arr.ctypes.data_as(dp), n, int(poll_steps), xptrs,
                                lat.ctypes.data_as(dp), xn.ctypes.data_as(dp), reps, C.byref(wall)),

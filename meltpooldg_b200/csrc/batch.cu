@@ -3,19 +3,23 @@
 // graph launch per Krylov step for all of them.
 //
 // Each admitted problem owns a slot: FP64 x, b and defect vectors, FP32 r, z,
-// p, Ap (and the BiCGStab vectors) and its FP32 inverse diagonal.  One step of
-// the graph runs, for every active slot at once,
-//   * the batched FP32 operator apply (one launch per degree and colour over a
-//     segment table of all slots' cells, batch_apply.cuh);
+// p, Ap (and the BiCGStab vectors), its FP32 inverse diagonal and its chunk
+// partials, all from a stream-ordered memory pool.  One graph step runs, for
+// every running slot at once,
+//   * device schedules: the running heat slots, the running advection-diffusion
+//     slots and (mid-step) the slots that take an FP64 defect, each as
+//     compacted per-colour cell-group lists and vector-chunk lists;
+//   * the batched FP32 operator applies (one launch per colour over all
+//     scheduled slots of any degree, batch_apply.cuh);
 //   * chunked vector kernels whose per-slot scalars live on the device, with
 //     per-slot reductions over fixed chunks (deterministic, so a problem gives
-//     the same result alone and in any mix);
+//     the same bits alone and in any mix);
 //   * the reliable-update decision, and for the slots that take it the FP64
 //     apply and defect b - A x that replaces the FP32 residual.
 // Heat problems (symmetric) use CG, advection-diffusion problems BiCGStab,
 // both with Jacobi preconditioning, FP32 operator and FP64 solution, defects,
-// dots and norms.  The host only replays the graph and polls how many slots
-// are still running; membership changes rebuild the tables and the graph.
+// dots and norms.  The graph does not depend on which slots are in use, so
+// admission and release never re-capture it: they only write slot tables.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,11 +36,9 @@
 
 namespace mpdg {
 
-constexpr int kChunk = 8192;  // vector elements per reduction chunk
-
-struct BatchChunk {
-  int slot, begin, end;
-};
+constexpr int kChunk = 8192;        // vector elements per reduction chunk
+constexpr int kChunkBlocks = 148 * 8;  // grid of the chunked vector kernels
+constexpr int kSchedThreads = 1024;
 
 enum { SL_RUNNING = 0, SL_CONVERGED = 1, SL_NOT_CONVERGED = 2, SL_BREAKDOWN = 3, SL_NAN = 4 };
 
@@ -44,22 +46,32 @@ enum { SL_RUNNING = 0, SL_CONVERGED = 1, SL_NOT_CONVERGED = 2, SL_BREAKDOWN = 3,
 struct SlotScalars {
   double rz, rz_new, pap, rr;          // CG
   double rho, rho_new, alpha, omega;   // BiCGStab
-  double tv, tt, ts;                   // BiCGStab dots (t.v... see kernels)
   double scale, tol, rmax, res, res0;
   int active, need_defect, iters, defects, status, max_it, kind, pad;
+};
+
+// device pointer tables, one entry per slot
+struct BatchTables {
+  double **x, **b, **r64;
+  float **r, **z, **p, **Ap, **invd, **rh, **v, **sv, **t;
+  double **part;   // 4 partial sums per vector chunk
+  SlotInfo *info;
+};
+
+struct SlotPtrs {
+  double *x, *b, *r64;
+  float *r, *z, *p, *Ap, *invd, *rh, *v, *sv, *t;
+  double *part;
 };
 
 struct BatchSlot {
   bool used = false;
   int64_t ticket = -1;
+  long admit_seq = 0;
   mpdg_problem_desc desc{};
   long N = 0;
   size_t bytes = 0;
-  double *x = nullptr, *b = nullptr, *r64 = nullptr;
-  float *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr, *invd = nullptr;
-  float *rh = nullptr, *v = nullptr, *sv = nullptr, *t = nullptr;  // BiCGStab: r-hat, v, s, t
-  double t_admit = 0;
-  int first_chunk = 0, n_chunks = 0;
+  SlotPtrs v{};
 };
 
 struct Batch {
@@ -68,33 +80,27 @@ struct Batch {
   int capacity = 0;
   double delta = 0.1;
   int max_it = 20000;
-  cudaStream_t stream = nullptr;
-  cudaMemPool_t pool = nullptr;  // slot vectors: stream-ordered, kept by the pool after release
+  cudaStream_t stream = nullptr;       // graph steps, admission, release
+  cudaStream_t copy_stream = nullptr;  // results of finished slots (serving)
+  cudaMemPool_t pool = nullptr;        // slot vectors: stream-ordered, kept by the pool after release
   std::vector<BatchSlot> slots;
   int64_t next_ticket = 0;
-  // device tables (capacity entries)
+  BatchTables tab{};
   SlotScalars *d_sc = nullptr;
   BatchSlotParams *d_params = nullptr;
-  int *d_active = nullptr;  // [2][capacity]: running flags, then the per-kind masks of a step
-  int *d_defect = nullptr;
-  double **d_x = nullptr, **d_b = nullptr, **d_r64 = nullptr;
-  float **d_r = nullptr, **d_z = nullptr, **d_p = nullptr, **d_Ap = nullptr, **d_invd = nullptr;
-  float **d_rh = nullptr, **d_v = nullptr, **d_sv = nullptr, **d_t = nullptr;
-  int *d_running = nullptr;     // number of running slots (polled by the host)
-  int *h_running = nullptr;     // pinned
-  SlotScalars *h_sc = nullptr;  // pinned copy of the scalars (polling)
-  double *d_adm = nullptr;      // admission scratch: reduction partials and |b|^2
-  // membership-dependent
-  BatchChunk *d_chunks = nullptr;
-  int n_chunks = 0;
-  int *d_slot_chunk = nullptr;  // [capacity][2]: first chunk, count
-  double *d_part = nullptr;     // chunk partials, 4 per chunk
-  BatchApplyPlan plan;
-  std::vector<void *> plan_allocs;
+  int *d_active = nullptr;   // running flags
+  int *d_defect = nullptr;   // FP64 defect flags of the current step
+  int *d_running = nullptr;  // number of running slots (polled by the host)
+  int *h_running = nullptr;  // pinned
+  int *h_active[2] = {nullptr, nullptr};  // pinned snapshots of the running flags
+  SlotScalars *h_sc = nullptr;            // pinned copy of the scalars
+  double *h_norm = nullptr;               // pinned
+  double *d_adm = nullptr;   // admission scratch: reduction partials and |b|^2
+  double *d_res = nullptr;   // result scratch of the copy stream
+  BatchSchedule sched[3];    // heat slots, advection-diffusion slots, defect slots
   cudaGraphExec_t graph = nullptr;
-  int64_t step_kernels = 0;     // kernels of one graph step
-  bool dirty = true;
-  int tuned_cap = 0;            // resident CTAs per SM of the batched apply (0 = occupancy maximum)
+  int64_t step_kernels = 0;  // kernels of one graph step
+  int tuned_cap = 0;         // resident CTAs per SM of the batched apply (0 = occupancy maximum)
   double tuned_ms = 0;
 };
 
@@ -300,59 +306,183 @@ __global__ void bk_diag_values(const double *F, long NX, long N, double c_mass, 
   }
 }
 
-#define FOR_CHUNK(ch)                                                            \
-  for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {                    \
-    const BatchChunk ch = chunks[ci];
+// ---------------------------------------------------------------- schedule
 
-#define END_FOR_CHUNK }
-
-// p.Ap partials (CG) / rh.v partials (BiCGStab), per chunk of active slots
-__global__ void bk_dot_pap(const BatchChunk *chunks, int n_chunks, const int *active, float *const *A,
-                           float *const *B, double *part)
+__device__ __forceinline__ int sched_find(const int *__restrict__ prefix, int n, int g)
 {
-  FOR_CHUNK(ch)
-    double s = 0.0;
-    if (active[ch.slot]) {
-      const float *a = A[ch.slot], *bb = B[ch.slot];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) s += (double)a[i] * (double)bb[i];
-    }
-    s = bblock_sum(s);
-    if (threadIdx.x == 0) part[4 * ci] = s;
-  END_FOR_CHUNK
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 
-// sums per slot: out[slot-field] = sum over the slot's chunks of part[4c + k]
-template <int K>
-__device__ double slot_sum(const double *part, const int *slot_chunk, int s)
+// exclusive block scan of two counters over kSchedThreads threads, with totals
+__device__ void block_scan2(int a, int b, int &ea, int &eb, int &ta, int &tb)
 {
-  const int c0 = slot_chunk[2 * s], nc = slot_chunk[2 * s + 1];
+  __shared__ int wa[32], wb[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int ia = a, ib = b;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int xa = __shfl_up_sync(0xffffffffu, ia, o), xb = __shfl_up_sync(0xffffffffu, ib, o);
+    if (lane >= o) {
+      ia += xa;
+      ib += xb;
+    }
+  }
+  if (lane == 31) {
+    wa[w] = ia;
+    wb[w] = ib;
+  }
+  __syncthreads();
+  if (w == 0) {
+    int va = wa[lane], vb = wb[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int xa = __shfl_up_sync(0xffffffffu, va, o), xb = __shfl_up_sync(0xffffffffu, vb, o);
+      if (lane >= o) {
+        va += xa;
+        vb += xb;
+      }
+    }
+    wa[lane] = va;
+    wb[lane] = vb;
+  }
+  __syncthreads();
+  const int oa = w ? wa[w - 1] : 0, ob = w ? wb[w - 1] : 0;
+  ea = oa + ia - a;
+  eb = ob + ib - b;
+  ta = wa[31];
+  tb = wb[31];
+  __syncthreads();
+}
+
+// Compacts the flagged slots (optionally of one kind): block c < 8 lists the
+// slots with cells of colour c and the prefix of their warp groups, block 8
+// the slots with the prefix of their vector chunks.  Slot order is kept.
+__global__ void __launch_bounds__(kSchedThreads)
+    bk_schedule(const int *flags, int kind, const SlotInfo *info, int cap, BatchSchedule S)
+{
+  const int c = blockIdx.x;
+  const int per = (cap + kSchedThreads - 1) / kSchedThreads;
+  const int s0 = min(cap, (int)threadIdx.x * per), s1 = min(cap, s0 + per);
+  int cnt = 0, sum = 0;
+  for (int s = s0; s < s1; ++s) {
+    if (!flags[s] || (kind >= 0 && info[s].kind != kind)) continue;
+    const int w = (c < 8) ? info[s].col[c].groups : info[s].n_chunks;
+    if (w > 0) {
+      ++cnt;
+      sum += w;
+    }
+  }
+  int ec, es, tc, ts;
+  block_scan2(cnt, sum, ec, es, tc, ts);
+  int *slot_out = (c < 8) ? S.seg_slot + (size_t)c * cap : S.act_slot;
+  int *pre_out = (c < 8) ? S.seg_prefix + (size_t)c * cap : S.chunk_prefix;
+  for (int s = s0; s < s1; ++s) {
+    if (!flags[s] || (kind >= 0 && info[s].kind != kind)) continue;
+    const int w = (c < 8) ? info[s].col[c].groups : info[s].n_chunks;
+    if (w > 0) {
+      slot_out[ec] = s;
+      pre_out[ec] = es;
+      ++ec;
+      es += w;
+    }
+  }
+  if (threadIdx.x == 0) {
+    if (c < 8) {
+      S.hdr->n_seg[c] = tc;
+      S.hdr->total_groups[c] = ts;
+    } else {
+      S.hdr->n_slots = tc;
+      S.hdr->total_chunks = ts;
+    }
+  }
+}
+
+__global__ void bk_bind_slot(BatchTables T, int s, SlotPtrs v, SlotInfo info)
+{
+  T.x[s] = v.x;
+  T.b[s] = v.b;
+  T.r64[s] = v.r64;
+  T.r[s] = v.r;
+  T.z[s] = v.z;
+  T.p[s] = v.p;
+  T.Ap[s] = v.Ap;
+  T.invd[s] = v.invd;
+  T.rh[s] = v.rh;
+  T.v[s] = v.v;
+  T.sv[s] = v.sv;
+  T.t[s] = v.t;
+  T.part[s] = v.part;
+  T.info[s] = info;
+}
+
+// loop over the scheduled vector chunks: slot s, elements [begin, end), the
+// chunk's 4 partial sums at part
+#define FOR_CHUNK(S)                                                       \
+  {                                                                        \
+    const int n_act_ = (S).hdr->n_slots, tot_ = (S).hdr->total_chunks;     \
+    for (int k_ = blockIdx.x; k_ < tot_; k_ += gridDim.x) {                \
+      const int ix_ = sched_find((S).chunk_prefix, n_act_, k_);            \
+      const int s = (S).act_slot[ix_];                                     \
+      const int lc_ = k_ - (S).chunk_prefix[ix_];                          \
+      const long begin = (long)lc_ * kChunk;                               \
+      const long end = min(T.info[s].N, begin + (long)kChunk);             \
+      [[maybe_unused]] double *part = T.part[s] + 4 * lc_;
+
+#define END_FOR_CHUNK \
+  }                   \
+  }
+
+// sum over the slot's chunks of partial K (fixed order: deterministic)
+template <int K>
+__device__ double slot_sum(const BatchTables &T, int s)
+{
+  const double *p = T.part[s];
+  const int nc = T.info[s].n_chunks;
   double v = 0.0;
-  for (int c = c0; c < c0 + nc; ++c) v += part[4 * c + K];
+  for (int c = 0; c < nc; ++c) v += p[4 * c + K];
   return v;
 }
 
-__global__ void bk_finish_pap(SlotScalars *sc, const int *active, const double *part, const int *slot_chunk,
-                              int n_slots)
+// ------------------------------------------------------ CG (heat problems)
+
+// p.Ap partials
+__global__ void bk_dot_pap(BatchSchedule S, BatchTables T, const int *active)
 {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n_slots || !active[s]) return;
-  sc[s].pap = slot_sum<0>(part, slot_chunk, s);
+  FOR_CHUNK(S)
+    double d = 0.0;
+    if (active[s]) {
+      const float *a = T.p[s], *b = T.Ap[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) d += (double)a[i] * (double)b[i];
+    }
+    d = bblock_sum(d);
+    if (threadIdx.x == 0) part[0] = d;
+  END_FOR_CHUNK
 }
 
-// CG: alpha = rz / pap; x += scale alpha p; r -= alpha Ap; z = invd r; partials r.r, r.z
-__global__ void bk_cg_update(const BatchChunk *chunks, int n_chunks, const int *active,
-                             const SlotScalars *sc, double *const *X, float *const *R, float *const *Z,
-                             float *const *Pv, float *const *APv, float *const *ID, double *part)
+__global__ void bk_finish_pap(SlotScalars *sc, const int *active, BatchTables T, int n_slots)
 {
-  FOR_CHUNK(ch)
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_slots || !active[s] || sc[s].kind != MPDG_OP_HEAT) return;
+  sc[s].pap = slot_sum<0>(T, s);
+}
+
+// alpha = rz / pap; x += scale alpha p; r -= alpha Ap; z = invd r; partials r.r, r.z
+__global__ void bk_cg_update(BatchSchedule S, BatchTables T, const int *active, const SlotScalars *sc)
+{
+  FOR_CHUNK(S)
     double rr = 0.0, rz = 0.0;
-    const int s = ch.slot;
     if (active[s] && sc[s].kind == MPDG_OP_HEAT) {
       const double alpha = sc[s].rz / sc[s].pap, xa = alpha * sc[s].scale;
-      double *x = X[s];
-      float *r = R[s], *z = Z[s];
-      const float *p = Pv[s], *ap = APv[s], *id = ID[s];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+      double *x = T.x[s];
+      float *r = T.r[s], *z = T.z[s];
+      const float *p = T.p[s], *ap = T.Ap[s], *id = T.invd[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) {
         x[i] += xa * (double)p[i];
         const float ri = (float)((double)r[i] - alpha * (double)ap[i]);
         r[i] = ri;
@@ -365,15 +495,15 @@ __global__ void bk_cg_update(const BatchChunk *chunks, int n_chunks, const int *
     rr = bblock_sum(rr);
     rz = bblock_sum(rz);
     if (threadIdx.x == 0) {
-      part[4 * ci + 1] = rr;
-      part[4 * ci + 2] = rz;
+      part[1] = rr;
+      part[2] = rz;
     }
   END_FOR_CHUNK
 }
 
 // per-slot bookkeeping after the FP32 update; decides the FP64 defect
-__global__ void bk_cg_decide(SlotScalars *sc, int *active, int *defect, const double *part,
-                             const int *slot_chunk, int n_slots, double delta)
+__global__ void bk_cg_decide(SlotScalars *sc, int *active, int *defect, BatchTables T, int n_slots,
+                             double delta)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_slots) return;
@@ -385,8 +515,8 @@ __global__ void bk_cg_decide(SlotScalars *sc, int *active, int *defect, const do
     active[s] = 0;
     return;
   }
-  q.rr = slot_sum<1>(part, slot_chunk, s);
-  q.rz_new = slot_sum<2>(part, slot_chunk, s);
+  q.rr = slot_sum<1>(T, s);
+  q.rz_new = slot_sum<2>(T, s);
   q.iters += 1;
   const double rel = sqrt(q.rr);
   if (!isfinite(rel)) {
@@ -399,32 +529,30 @@ __global__ void bk_cg_decide(SlotScalars *sc, int *active, int *defect, const do
 }
 
 // defect b - A x (A x already in r64) for flagged slots, partials of |d|^2
-__global__ void bk_defect(const BatchChunk *chunks, int n_chunks, const int *defect,
-                          double *const *B, double *const *R64, double *part)
+__global__ void bk_defect(BatchSchedule S, BatchTables T, const int *defect)
 {
-  FOR_CHUNK(ch)
-    double s = 0.0;
-    if (defect[ch.slot]) {
-      const double *b = B[ch.slot];
-      double *r = R64[ch.slot];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+  FOR_CHUNK(S)
+    double d2 = 0.0;
+    if (defect[s]) {
+      const double *b = T.b[s];
+      double *r = T.r64[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) {
         const double d = b[i] - r[i];
         r[i] = d;
-        s += d * d;
+        d2 += d * d;
       }
     }
-    s = bblock_sum(s);
-    if (threadIdx.x == 0) part[4 * ci + 3] = s;
+    d2 = bblock_sum(d2);
+    if (threadIdx.x == 0) part[3] = d2;
   END_FOR_CHUNK
 }
 
-__global__ void bk_defect_decide(SlotScalars *sc, int *active, int *defect, const double *part,
-                                 const int *slot_chunk, int n_slots)
+__global__ void bk_defect_decide(SlotScalars *sc, int *active, int *defect, BatchTables T, int n_slots)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_slots || !defect[s]) return;
   SlotScalars &q = sc[s];
-  q.res = sqrt(slot_sum<3>(part, slot_chunk, s));
+  q.res = sqrt(slot_sum<3>(T, s));
   q.defects += 1;
   if (!isfinite(q.res)) {
     q.status = SL_NAN;
@@ -444,19 +572,16 @@ __global__ void bk_defect_decide(SlotScalars *sc, int *active, int *defect, cons
 }
 
 // replacement of the FP32 residual by the FP64 defect (CG), partials of r.z
-__global__ void bk_cg_replace(const BatchChunk *chunks, int n_chunks, const int *defect,
-                              const SlotScalars *sc, double *const *R64, float *const *R, float *const *Z,
-                              float *const *ID, double *part)
+__global__ void bk_cg_replace(BatchSchedule S, BatchTables T, const int *defect, const SlotScalars *sc)
 {
-  FOR_CHUNK(ch)
+  FOR_CHUNK(S)
     double rz = 0.0;
-    const int s = ch.slot;
     if (defect[s] && sc[s].kind == MPDG_OP_HEAT) {
       const double is = 1.0 / sc[s].scale;
-      const double *d = R64[s];
-      float *r = R[s], *z = Z[s];
-      const float *id = ID[s];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+      const double *d = T.r64[s];
+      float *r = T.r[s], *z = T.z[s];
+      const float *id = T.invd[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) {
         const float ri = (float)(d[i] * is);
         r[i] = ri;
         const float zi = id[i] * ri;
@@ -465,30 +590,26 @@ __global__ void bk_cg_replace(const BatchChunk *chunks, int n_chunks, const int 
       }
     }
     rz = bblock_sum(rz);
-    if (threadIdx.x == 0) part[4 * ci + 2] = rz;
+    if (threadIdx.x == 0) part[2] = rz;
   END_FOR_CHUNK
 }
 
-__global__ void bk_cg_replace_finish(SlotScalars *sc, const int *defect, const double *part,
-                                     const int *slot_chunk, int n_slots)
+__global__ void bk_cg_replace_finish(SlotScalars *sc, const int *defect, BatchTables T, int n_slots)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_slots || !defect[s] || sc[s].kind != MPDG_OP_HEAT) return;
-  sc[s].rz_new = slot_sum<2>(part, slot_chunk, s);
+  sc[s].rz_new = slot_sum<2>(T, s);
 }
 
 // p = z + beta p
-__global__ void bk_cg_direction(const BatchChunk *chunks, int n_chunks, const int *active,
-                                const SlotScalars *sc, float *const *Z, float *const *Pv)
+__global__ void bk_cg_direction(BatchSchedule S, BatchTables T, const int *active, const SlotScalars *sc)
 {
-  FOR_CHUNK(ch)
-    const int s = ch.slot;
+  FOR_CHUNK(S)
     if (active[s] && sc[s].kind == MPDG_OP_HEAT) {
       const double beta = sc[s].rz_new / sc[s].rz;
-      const float *z = Z[s];
-      float *p = Pv[s];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x)
-        p[i] = (float)((double)z[i] + beta * (double)p[i]);
+      const float *z = T.z[s];
+      float *p = T.p[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) p[i] = (float)((double)z[i] + beta * (double)p[i]);
     }
   END_FOR_CHUNK
 }
@@ -512,30 +633,40 @@ __global__ void bk_count_running(const int *active, int n_slots, int *out)
   if (threadIdx.x == 0) *out = cnt;
 }
 
-// ---------------- BiCGStab (right-preconditioned by Jacobi), advection-diffusion slots
-// state: r (residual, scaled), rh (shadow), p, v = A M p, s, t = A M s; M = diag(invd)
-// phase A (after v = A (invd p) in Ap): alpha = rho / (rh . v)
-__global__ void bk_bicg_alpha_partials(const BatchChunk *chunks, int n_chunks, const int *active,
-                                       const SlotScalars *sc, float *const *RH, float *const *V,
-                                       double *part)
+// ------------------------- BiCGStab (advection-diffusion problems), right-preconditioned by Jacobi
+// state: r (scaled residual), rh (shadow), p, v = A M p, s, t = A M s; M = diag(invd)
+
+// z = invd p for the first apply
+__global__ void bk_bicg_precond_p(BatchSchedule S, BatchTables T, const int *active, const SlotScalars *sc)
 {
-  FOR_CHUNK(ch)
-    double s = 0.0;
-    if (active[ch.slot] && sc[ch.slot].kind == MPDG_OP_ADVDIFF) {
-      const float *rh = RH[ch.slot], *v = V[ch.slot];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) s += (double)rh[i] * (double)v[i];
+  FOR_CHUNK(S)
+    if (active[s] && sc[s].kind == MPDG_OP_ADVDIFF) {
+      const float *p = T.p[s], *id = T.invd[s];
+      float *z = T.z[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) z[i] = id[i] * p[i];
     }
-    s = bblock_sum(s);
-    if (threadIdx.x == 0) part[4 * ci] = s;
   END_FOR_CHUNK
 }
 
-__global__ void bk_bicg_alpha(SlotScalars *sc, int *active, const double *part, const int *slot_chunk,
-                              int n_slots)
+// after v = A z: partials rh.v
+__global__ void bk_bicg_alpha_partials(BatchSchedule S, BatchTables T, const int *active, const SlotScalars *sc)
+{
+  FOR_CHUNK(S)
+    double d = 0.0;
+    if (active[s] && sc[s].kind == MPDG_OP_ADVDIFF) {
+      const float *rh = T.rh[s], *v = T.v[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) d += (double)rh[i] * (double)v[i];
+    }
+    d = bblock_sum(d);
+    if (threadIdx.x == 0) part[0] = d;
+  END_FOR_CHUNK
+}
+
+__global__ void bk_bicg_alpha(SlotScalars *sc, int *active, BatchTables T, int n_slots)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_slots || !active[s] || sc[s].kind != MPDG_OP_ADVDIFF) return;
-  const double rv = slot_sum<0>(part, slot_chunk, s);
+  const double rv = slot_sum<0>(T, s);
   if (!(rv != 0.0) || !isfinite(rv)) {
     sc[s].status = SL_BREAKDOWN;
     active[s] = 0;
@@ -544,18 +675,15 @@ __global__ void bk_bicg_alpha(SlotScalars *sc, int *active, const double *part, 
   sc[s].alpha = sc[s].rho / rv;
 }
 
-// s = r - alpha v, (into sv); z = invd s (into z) for the second apply
-__global__ void bk_bicg_s(const BatchChunk *chunks, int n_chunks, const int *active, const SlotScalars *sc,
-                          float *const *R, float *const *V, float *const *SV, float *const *Z,
-                          float *const *ID)
+// s = r - alpha v (into sv); z = invd s for the second apply
+__global__ void bk_bicg_s(BatchSchedule S, BatchTables T, const int *active, const SlotScalars *sc)
 {
-  FOR_CHUNK(ch)
-    const int s = ch.slot;
+  FOR_CHUNK(S)
     if (active[s] && sc[s].kind == MPDG_OP_ADVDIFF) {
       const double a = sc[s].alpha;
-      const float *r = R[s], *v = V[s], *id = ID[s];
-      float *sv = SV[s], *z = Z[s];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+      const float *r = T.r[s], *v = T.v[s], *id = T.invd[s];
+      float *sv = T.sv[s], *z = T.z[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) {
         const float si = (float)((double)r[i] - a * (double)v[i]);
         sv[i] = si;
         z[i] = id[i] * si;
@@ -565,16 +693,13 @@ __global__ void bk_bicg_s(const BatchChunk *chunks, int n_chunks, const int *act
 }
 
 // after t = A z: partials t.s and t.t
-__global__ void bk_bicg_omega_partials(const BatchChunk *chunks, int n_chunks, const int *active,
-                                       const SlotScalars *sc, float *const *T, float *const *SV,
-                                       double *part)
+__global__ void bk_bicg_omega_partials(BatchSchedule S, BatchTables T, const int *active, const SlotScalars *sc)
 {
-  FOR_CHUNK(ch)
+  FOR_CHUNK(S)
     double ts = 0.0, tt = 0.0;
-    const int s = ch.slot;
     if (active[s] && sc[s].kind == MPDG_OP_ADVDIFF) {
-      const float *t = T[s], *sv = SV[s];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+      const float *t = T.t[s], *sv = T.sv[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) {
         ts += (double)t[i] * (double)sv[i];
         tt += (double)t[i] * (double)t[i];
       }
@@ -582,36 +707,31 @@ __global__ void bk_bicg_omega_partials(const BatchChunk *chunks, int n_chunks, c
     ts = bblock_sum(ts);
     tt = bblock_sum(tt);
     if (threadIdx.x == 0) {
-      part[4 * ci] = ts;
-      part[4 * ci + 1] = tt;
+      part[0] = ts;
+      part[1] = tt;
     }
   END_FOR_CHUNK
 }
 
-__global__ void bk_bicg_omega(SlotScalars *sc, int *active, const double *part, const int *slot_chunk,
-                              int n_slots)
+__global__ void bk_bicg_omega(SlotScalars *sc, const int *active, BatchTables T, int n_slots)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_slots || !active[s] || sc[s].kind != MPDG_OP_ADVDIFF) return;
-  const double ts = slot_sum<0>(part, slot_chunk, s), tt = slot_sum<1>(part, slot_chunk, s);
+  const double ts = slot_sum<0>(T, s), tt = slot_sum<1>(T, s);
   sc[s].omega = (tt > 0.0) ? ts / tt : 0.0;
 }
 
 // x += scale (alpha invd p + omega invd s); r = s - omega t; partials r.r and rh.r
-__global__ void bk_bicg_update(const BatchChunk *chunks, int n_chunks, const int *active,
-                               const SlotScalars *sc, double *const *X, float *const *R, float *const *Pv,
-                               float *const *SV, float *const *T, float *const *RH, float *const *ID,
-                               double *part)
+__global__ void bk_bicg_update(BatchSchedule S, BatchTables T, const int *active, const SlotScalars *sc)
 {
-  FOR_CHUNK(ch)
+  FOR_CHUNK(S)
     double rr = 0.0, rhr = 0.0;
-    const int s = ch.slot;
     if (active[s] && sc[s].kind == MPDG_OP_ADVDIFF) {
       const double a = sc[s].alpha, w = sc[s].omega, scl = sc[s].scale;
-      double *x = X[s];
-      float *r = R[s];
-      const float *p = Pv[s], *sv = SV[s], *t = T[s], *rh = RH[s], *id = ID[s];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+      double *x = T.x[s];
+      float *r = T.r[s];
+      const float *p = T.p[s], *sv = T.sv[s], *t = T.t[s], *rh = T.rh[s], *id = T.invd[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) {
         x[i] += scl * (a * (double)(id[i] * p[i]) + w * (double)(id[i] * sv[i]));
         const float ri = (float)((double)sv[i] - w * (double)t[i]);
         r[i] = ri;
@@ -622,21 +742,19 @@ __global__ void bk_bicg_update(const BatchChunk *chunks, int n_chunks, const int
     rr = bblock_sum(rr);
     rhr = bblock_sum(rhr);
     if (threadIdx.x == 0) {
-      part[4 * ci + 1] = rr;
-      part[4 * ci + 2] = rhr;
+      part[1] = rr;
+      part[2] = rhr;
     }
   END_FOR_CHUNK
 }
 
-__global__ void bk_bicg_decide(SlotScalars *sc, int *active, int *defect, const double *part,
-                               const int *slot_chunk, int n_slots, double delta)
+__global__ void bk_bicg_decide(SlotScalars *sc, int *active, int *defect, BatchTables T, int n_slots, double delta)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n_slots) return;
-  if (!active[s] || sc[s].kind != MPDG_OP_ADVDIFF) return;
+  if (s >= n_slots || !active[s] || sc[s].kind != MPDG_OP_ADVDIFF) return;
   SlotScalars &q = sc[s];
-  q.rr = slot_sum<1>(part, slot_chunk, s);
-  q.rho_new = slot_sum<2>(part, slot_chunk, s);
+  q.rr = slot_sum<1>(T, s);
+  q.rho_new = slot_sum<2>(T, s);
   q.iters += 1;
   const double rel = sqrt(q.rr);
   if (!isfinite(rel)) {
@@ -648,19 +766,16 @@ __global__ void bk_bicg_decide(SlotScalars *sc, int *active, int *defect, const 
   if (q.res <= q.tol || rel < delta * q.rmax || q.iters >= q.max_it || !(q.omega != 0.0)) defect[s] = 1;
 }
 
-// restart from the FP64 defect: r = rh = d / scale, p = r, rho = r.r
-__global__ void bk_bicg_replace(const BatchChunk *chunks, int n_chunks, const int *defect,
-                                const SlotScalars *sc, double *const *R64, float *const *R,
-                                float *const *RH, float *const *Pv, double *part)
+// restart from the FP64 defect: r = rh = p = d / scale, rho = r.r
+__global__ void bk_bicg_replace(BatchSchedule S, BatchTables T, const int *defect, const SlotScalars *sc)
 {
-  FOR_CHUNK(ch)
+  FOR_CHUNK(S)
     double rr = 0.0;
-    const int s = ch.slot;
     if (defect[s] && sc[s].kind == MPDG_OP_ADVDIFF) {
       const double is = 1.0 / sc[s].scale;
-      const double *d = R64[s];
-      float *r = R[s], *rh = RH[s], *p = Pv[s];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) {
+      const double *d = T.r64[s];
+      float *r = T.r[s], *rh = T.rh[s], *p = T.p[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x) {
         const float ri = (float)(d[i] * is);
         r[i] = ri;
         rh[i] = ri;
@@ -669,31 +784,28 @@ __global__ void bk_bicg_replace(const BatchChunk *chunks, int n_chunks, const in
       }
     }
     rr = bblock_sum(rr);
-    if (threadIdx.x == 0) part[4 * ci + 2] = rr;
+    if (threadIdx.x == 0) part[2] = rr;
   END_FOR_CHUNK
 }
 
-__global__ void bk_bicg_replace_finish(SlotScalars *sc, const int *defect, const double *part,
-                                       const int *slot_chunk, int n_slots)
+__global__ void bk_bicg_replace_finish(SlotScalars *sc, const int *defect, BatchTables T, int n_slots)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_slots || !defect[s] || sc[s].kind != MPDG_OP_ADVDIFF) return;
-  sc[s].rho = slot_sum<2>(part, slot_chunk, s);
+  sc[s].rho = slot_sum<2>(T, s);
   sc[s].rho_new = sc[s].rho;
 }
 
 // p = r + beta (p - omega v), beta = (rho_new / rho) (alpha / omega); skipped right after a restart
-__global__ void bk_bicg_direction(const BatchChunk *chunks, int n_chunks, const int *active,
-                                  const int *defect, const SlotScalars *sc, float *const *R,
-                                  float *const *Pv, float *const *V)
+__global__ void bk_bicg_direction(BatchSchedule S, BatchTables T, const int *active, const int *defect,
+                                  const SlotScalars *sc)
 {
-  FOR_CHUNK(ch)
-    const int s = ch.slot;
+  FOR_CHUNK(S)
     if (active[s] && !defect[s] && sc[s].kind == MPDG_OP_ADVDIFF) {
       const double beta = (sc[s].rho_new / sc[s].rho) * (sc[s].alpha / sc[s].omega), w = sc[s].omega;
-      const float *r = R[s], *v = V[s];
-      float *p = Pv[s];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x)
+      const float *r = T.r[s], *v = T.v[s];
+      float *p = T.p[s];
+      for (long i = begin + threadIdx.x; i < end; i += blockDim.x)
         p[i] = (float)((double)r[i] + beta * ((double)p[i] - w * (double)v[i]));
     }
   END_FOR_CHUNK
@@ -706,31 +818,8 @@ __global__ void bk_bicg_shift(SlotScalars *sc, const int *active, int n_slots)
   sc[s].rho = sc[s].rho_new;
 }
 
-// z = invd p for the first BiCGStab apply (right preconditioning)
-__global__ void bk_bicg_precond_p(const BatchChunk *chunks, int n_chunks, const int *active,
-                                  const SlotScalars *sc, float *const *Pv, float *const *Z,
-                                  float *const *ID)
-{
-  FOR_CHUNK(ch)
-    const int s = ch.slot;
-    if (active[s] && sc[s].kind == MPDG_OP_ADVDIFF) {
-      const float *p = Pv[s], *id = ID[s];
-      float *z = Z[s];
-      for (int i = ch.begin + threadIdx.x; i < ch.end; i += blockDim.x) z[i] = id[i] * p[i];
-    }
-  END_FOR_CHUNK
-}
-
-// active mask restricted to one kind (for the applies of the BiCGStab phases)
-__global__ void bk_kind_mask(const SlotScalars *sc, const int *active, int *out, int kind, int n_slots)
-{
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < n_slots) out[s] = (active[s] && sc[s].kind == kind) ? 1 : 0;
-}
-
 }  // namespace
 }  // namespace mpdg
-
 
 namespace mpdg {
 namespace {
@@ -839,6 +928,7 @@ void rhs_host(const mpdg_problem_desc &d, double *b)
   }
 }
 
+
 template <typename T>
 T *palloc(Batch &B, size_t n)
 {
@@ -850,19 +940,56 @@ T *palloc(Batch &B, size_t n)
 
 void free_slot_vectors(Batch &B, BatchSlot &S)
 {
-  for (void *p : {(void *)S.x, (void *)S.b, (void *)S.r64, (void *)S.r, (void *)S.z, (void *)S.p,
-                  (void *)S.Ap, (void *)S.invd, (void *)S.rh, (void *)S.v, (void *)S.sv, (void *)S.t})
+  const SlotPtrs &v = S.v;
+  for (void *p : {(void *)v.x, (void *)v.b, (void *)v.r64, (void *)v.r, (void *)v.z, (void *)v.p, (void *)v.Ap,
+                  (void *)v.invd, (void *)v.rh, (void *)v.v, (void *)v.sv, (void *)v.t, (void *)v.part})
     if (p) cudaFreeAsync(p, B.stream);
 }
 
-template <typename T>
-void ptr_table(Batch &B, T *BatchSlot::*field, T **dev)
+unsigned long long magic40(unsigned long long d) { return ((1ull << 40) + d - 1) / d; }
+
+SlotInfo slot_info(const mpdg_problem_desc &d)
 {
-  std::vector<T *> h(B.capacity, nullptr);
-  for (int s = 0; s < B.capacity; ++s)
-    if (B.slots[s].used) h[s] = B.slots[s].*field;
-  MPDG_CUDA(cudaMemcpyAsync(dev, h.data(), sizeof(T *) * B.capacity, cudaMemcpyHostToDevice, B.stream));
-  MPDG_CUDA(cudaStreamSynchronize(B.stream));  // h is a temporary
+  SlotInfo I{};
+  I.degree = d.degree;
+  I.nc = d.nc;
+  I.kind = d.kind;
+  I.NX = (long)d.nc * d.degree + 1;
+  I.N = I.NX * I.NX * I.NX;
+  I.n_chunks = (int)((I.N + kChunk - 1) / kChunk);
+  const int cpw = cells_per_warp(d.degree);
+  for (int c = 0; c < 8; ++c) {
+    int cn[3];
+    for (int k = 0; k < 3; ++k) cn[k] = (d.nc - ((c >> k) & 1) + 1) / 2;
+    SlotColour &C = I.col[c];
+    const long count = (long)cn[0] * cn[1] * cn[2];
+    C.count = (int)count;
+    C.cn0 = cn[0];
+    C.cn1 = cn[1];
+    C.groups = (int)((count + cpw - 1) / cpw);
+    C.m0 = magic40((unsigned long long)cn[0]);
+    C.m01 = magic40((unsigned long long)cn[0] * (unsigned long long)cn[1]);
+  }
+  return I;
+}
+
+void alloc_schedule(BatchSchedule &S, int cap)
+{
+  S.cap = cap;
+  S.hdr = balloc<BatchScheduleHeader>(1);
+  S.seg_slot = balloc<int>(8 * (size_t)cap);
+  S.seg_prefix = balloc<int>(8 * (size_t)cap);
+  S.act_slot = balloc<int>(cap);
+  S.chunk_prefix = balloc<int>(cap);
+  MPDG_CUDA(cudaMemset(S.hdr, 0, sizeof(BatchScheduleHeader)));
+}
+
+void free_schedule(BatchSchedule &S)
+{
+  for (void *p : {(void *)S.hdr, (void *)S.seg_slot, (void *)S.seg_prefix, (void *)S.act_slot,
+                  (void *)S.chunk_prefix})
+    if (p) cudaFree(p);
+  S = BatchSchedule{};
 }
 
 void drop_graph(Batch &B)
@@ -873,161 +1000,70 @@ void drop_graph(Batch &B)
   }
 }
 
-void free_plan(Batch &B)
-{
-  for (void *p : B.plan_allocs) cudaFree(p);
-  B.plan_allocs.clear();
-  B.plan = BatchApplyPlan{};
-  if (B.d_chunks) cudaFree(B.d_chunks);
-  if (B.d_part) cudaFree(B.d_part);
-  B.d_chunks = nullptr;
-  B.d_part = nullptr;
-  B.n_chunks = 0;
-  drop_graph(B);
-}
-
-// tables of the current membership: chunks, per-slot chunk ranges, apply segments, pointers
-void rebuild_tables(Batch &B)
-{
-  MPDG_CUDA(cudaStreamSynchronize(B.stream));
-  free_plan(B);
-  std::vector<BatchChunk> chunks;
-  std::vector<int> slot_chunk(2 * (size_t)B.capacity, 0);
-  for (int s = 0; s < B.capacity; ++s) {
-    BatchSlot &S = B.slots[s];
-    if (!S.used) continue;
-    S.first_chunk = (int)chunks.size();
-    for (long b = 0; b < S.N; b += kChunk) chunks.push_back({s, (int)b, (int)std::min(S.N, b + kChunk)});
-    S.n_chunks = (int)chunks.size() - S.first_chunk;
-    slot_chunk[2 * s] = S.first_chunk;
-    slot_chunk[2 * s + 1] = S.n_chunks;
-  }
-  B.n_chunks = (int)chunks.size();
-  if (B.n_chunks) {
-    B.d_chunks = balloc<BatchChunk>(B.n_chunks);
-    MPDG_CUDA(cudaMemcpy(B.d_chunks, chunks.data(), sizeof(BatchChunk) * B.n_chunks, cudaMemcpyHostToDevice));
-    B.d_part = balloc<double>(4 * (size_t)B.n_chunks);
-  }
-  MPDG_CUDA(cudaMemcpy(B.d_slot_chunk, slot_chunk.data(), sizeof(int) * 2 * B.capacity, cudaMemcpyHostToDevice));
-  for (int p = 1; p <= kMaxDegree; ++p) {
-    const int cpw = cells_per_warp(p);
-    for (int c = 0; c < 8; ++c) {
-      std::vector<BatchSeg> segs;
-      std::vector<int> prefix;
-      long groups = 0;
-      for (int s = 0; s < B.capacity; ++s) {
-        const BatchSlot &S = B.slots[s];
-        if (!S.used || S.desc.degree != p) continue;
-        BatchSeg g{};
-        g.slot = s;
-        g.nc = S.desc.nc;
-        long count = 1;
-        for (int d = 0; d < 3; ++d) {
-          g.par[d] = (c >> d) & 1;
-          g.cn[d] = (S.desc.nc - g.par[d] + 1) / 2;
-          count *= g.cn[d];
-        }
-        if (count == 0) continue;
-        g.count = (int)count;
-        const unsigned long long d0 = (unsigned long long)g.cn[0], d01 = d0 * (unsigned long long)g.cn[1];
-        g.div0_magic = ((1ull << 40) + d0 - 1) / d0;
-        g.div01_magic = ((1ull << 40) + d01 - 1) / d01;
-        g.NX = (long)S.desc.nc * p + 1;
-        prefix.push_back((int)groups);
-        segs.push_back(g);
-        groups += (count + cpw - 1) / cpw;
-      }
-      if (segs.empty()) continue;
-      if (groups > INT32_MAX / 2) throw Error{MPDG_ERR_SIZE, "batch too large for one apply launch"};
-      BatchSeg *ds = balloc<BatchSeg>(segs.size());
-      B.plan_allocs.push_back(ds);
-      int *dp = balloc<int>(prefix.size());
-      B.plan_allocs.push_back(dp);
-      MPDG_CUDA(cudaMemcpy(ds, segs.data(), sizeof(BatchSeg) * segs.size(), cudaMemcpyHostToDevice));
-      MPDG_CUDA(cudaMemcpy(dp, prefix.data(), sizeof(int) * prefix.size(), cudaMemcpyHostToDevice));
-      B.plan.segs[p][c] = ds;
-      B.plan.prefix[p][c] = dp;
-      B.plan.nseg[p][c] = (int)segs.size();
-      B.plan.groups[p][c] = (int)groups;
-    }
-  }
-  ptr_table<double>(B, &BatchSlot::x, B.d_x);
-  ptr_table<double>(B, &BatchSlot::b, B.d_b);
-  ptr_table<double>(B, &BatchSlot::r64, B.d_r64);
-  ptr_table<float>(B, &BatchSlot::r, B.d_r);
-  ptr_table<float>(B, &BatchSlot::z, B.d_z);
-  ptr_table<float>(B, &BatchSlot::p, B.d_p);
-  ptr_table<float>(B, &BatchSlot::Ap, B.d_Ap);
-  ptr_table<float>(B, &BatchSlot::invd, B.d_invd);
-  ptr_table<float>(B, &BatchSlot::rh, B.d_rh);
-  ptr_table<float>(B, &BatchSlot::v, B.d_v);
-  ptr_table<float>(B, &BatchSlot::sv, B.d_sv);
-  ptr_table<float>(B, &BatchSlot::t, B.d_t);
-  B.dirty = false;
-}
-
 // one Krylov step of every running slot (the body of the graph)
-void enqueue_step(Batch &B, int cap)
+void enqueue_step(Batch &B, int blocks)
 {
   cudaStream_t st = B.stream;
-  const int S = B.capacity, nc = B.n_chunks;
-  const unsigned gs = (unsigned)((S + 255) / 256), gc = (unsigned)std::max(1, std::min(nc, 148 * 8));
-  int *kmask = B.d_active + S;
-#define BK(kernel, grid, ...)                            \
-  do {                                                   \
-    kernel<<<grid, 256, 0, st>>>(__VA_ARGS__);           \
-    MPDG_LAUNCHED();                                     \
+  const int S = B.capacity;
+  const unsigned gs = (unsigned)((S + 255) / 256), gc = kChunkBlocks;
+  const BatchTables &T = B.tab;
+  const BatchSchedule &SH = B.sched[0], &SA = B.sched[1], &SD = B.sched[2];
+#define BK(kernel, grid, ...)                  \
+  do {                                         \
+    kernel<<<grid, 256, 0, st>>>(__VA_ARGS__); \
+    MPDG_LAUNCHED();                           \
   } while (0)
+  bk_schedule<<<9, kSchedThreads, 0, st>>>(B.d_active, MPDG_OP_HEAT, T.info, S, SH);
+  MPDG_LAUNCHED();
+  bk_schedule<<<9, kSchedThreads, 0, st>>>(B.d_active, MPDG_OP_ADVDIFF, T.info, S, SA);
+  MPDG_LAUNCHED();
   // CG on the heat problems: Ap = A p (FP32), alpha, x/r/z update
-  BK(bk_kind_mask, gs, B.d_sc, B.d_active, kmask, MPDG_OP_HEAT, S);
-  launch_batch_apply<float>(B.plan, B.d_params, B.d_p, B.d_Ap, kmask, cap, st);
-  BK(bk_dot_pap, gc, B.d_chunks, nc, kmask, B.d_p, B.d_Ap, B.d_part);
-  BK(bk_finish_pap, gs, B.d_sc, kmask, B.d_part, B.d_slot_chunk, S);
-  BK(bk_cg_update, gc, B.d_chunks, nc, kmask, B.d_sc, B.d_x, B.d_r, B.d_z, B.d_p, B.d_Ap, B.d_invd, B.d_part);
-  BK(bk_cg_decide, gs, B.d_sc, B.d_active, B.d_defect, B.d_part, B.d_slot_chunk, S, B.delta);
+  launch_batch_apply<float>(SH, T.info, B.d_params, T.p, T.Ap, B.d_active, blocks, st);
+  BK(bk_dot_pap, gc, SH, T, B.d_active);
+  BK(bk_finish_pap, gs, B.d_sc, B.d_active, T, S);
+  BK(bk_cg_update, gc, SH, T, B.d_active, B.d_sc);
+  BK(bk_cg_decide, gs, B.d_sc, B.d_active, B.d_defect, T, S, B.delta);
   // BiCGStab on the advection-diffusion problems: v = A M p, alpha, s, t = A M s, omega, update
-  BK(bk_kind_mask, gs, B.d_sc, B.d_active, kmask, MPDG_OP_ADVDIFF, S);
-  BK(bk_bicg_precond_p, gc, B.d_chunks, nc, kmask, B.d_sc, B.d_p, B.d_z, B.d_invd);
-  launch_batch_apply<float>(B.plan, B.d_params, B.d_z, B.d_v, kmask, cap, st);
-  BK(bk_bicg_alpha_partials, gc, B.d_chunks, nc, kmask, B.d_sc, B.d_rh, B.d_v, B.d_part);
-  BK(bk_bicg_alpha, gs, B.d_sc, B.d_active, B.d_part, B.d_slot_chunk, S);
-  BK(bk_kind_mask, gs, B.d_sc, B.d_active, kmask, MPDG_OP_ADVDIFF, S);
-  BK(bk_bicg_s, gc, B.d_chunks, nc, kmask, B.d_sc, B.d_r, B.d_v, B.d_sv, B.d_z, B.d_invd);
-  launch_batch_apply<float>(B.plan, B.d_params, B.d_z, B.d_t, kmask, cap, st);
-  BK(bk_bicg_omega_partials, gc, B.d_chunks, nc, kmask, B.d_sc, B.d_t, B.d_sv, B.d_part);
-  BK(bk_bicg_omega, gs, B.d_sc, B.d_active, B.d_part, B.d_slot_chunk, S);
-  BK(bk_bicg_update, gc, B.d_chunks, nc, kmask, B.d_sc, B.d_x, B.d_r, B.d_p, B.d_sv, B.d_t, B.d_rh, B.d_invd,
-     B.d_part);
-  BK(bk_bicg_decide, gs, B.d_sc, B.d_active, B.d_defect, B.d_part, B.d_slot_chunk, S, B.delta);
+  BK(bk_bicg_precond_p, gc, SA, T, B.d_active, B.d_sc);
+  launch_batch_apply<float>(SA, T.info, B.d_params, T.z, T.v, B.d_active, blocks, st);
+  BK(bk_bicg_alpha_partials, gc, SA, T, B.d_active, B.d_sc);
+  BK(bk_bicg_alpha, gs, B.d_sc, B.d_active, T, S);
+  BK(bk_bicg_s, gc, SA, T, B.d_active, B.d_sc);
+  launch_batch_apply<float>(SA, T.info, B.d_params, T.z, T.t, B.d_active, blocks, st);
+  BK(bk_bicg_omega_partials, gc, SA, T, B.d_active, B.d_sc);
+  BK(bk_bicg_omega, gs, B.d_sc, B.d_active, T, S);
+  BK(bk_bicg_update, gc, SA, T, B.d_active, B.d_sc);
+  BK(bk_bicg_decide, gs, B.d_sc, B.d_active, B.d_defect, T, S, B.delta);
   // FP64 defects b - A x of the slots whose FP32 residual dropped by delta (or that look converged)
-  launch_batch_apply<double>(B.plan, B.d_params, B.d_x, B.d_r64, B.d_defect, cap, st);
-  BK(bk_defect, gc, B.d_chunks, nc, B.d_defect, B.d_b, B.d_r64, B.d_part);
-  BK(bk_defect_decide, gs, B.d_sc, B.d_active, B.d_defect, B.d_part, B.d_slot_chunk, S);
-  BK(bk_cg_replace, gc, B.d_chunks, nc, B.d_defect, B.d_sc, B.d_r64, B.d_r, B.d_z, B.d_invd, B.d_part);
-  BK(bk_cg_replace_finish, gs, B.d_sc, B.d_defect, B.d_part, B.d_slot_chunk, S);
-  BK(bk_bicg_replace, gc, B.d_chunks, nc, B.d_defect, B.d_sc, B.d_r64, B.d_r, B.d_rh, B.d_p, B.d_part);
-  BK(bk_bicg_replace_finish, gs, B.d_sc, B.d_defect, B.d_part, B.d_slot_chunk, S);
+  bk_schedule<<<9, kSchedThreads, 0, st>>>(B.d_defect, -1, T.info, S, SD);
+  MPDG_LAUNCHED();
+  launch_batch_apply<double>(SD, T.info, B.d_params, T.x, T.r64, B.d_defect, blocks, st);
+  BK(bk_defect, gc, SD, T, B.d_defect);
+  BK(bk_defect_decide, gs, B.d_sc, B.d_active, B.d_defect, T, S);
+  BK(bk_cg_replace, gc, SD, T, B.d_defect, B.d_sc);
+  BK(bk_cg_replace_finish, gs, B.d_sc, B.d_defect, T, S);
+  BK(bk_bicg_replace, gc, SD, T, B.d_defect, B.d_sc);
+  BK(bk_bicg_replace_finish, gs, B.d_sc, B.d_defect, T, S);
   // search directions and scalar shifts
-  BK(bk_cg_direction, gc, B.d_chunks, nc, B.d_active, B.d_sc, B.d_z, B.d_p);
-  BK(bk_bicg_direction, gc, B.d_chunks, nc, B.d_active, B.d_defect, B.d_sc, B.d_r, B.d_p, B.d_v);
+  BK(bk_cg_direction, gc, SH, T, B.d_active, B.d_sc);
+  BK(bk_bicg_direction, gc, SA, T, B.d_active, B.d_defect, B.d_sc);
   BK(bk_cg_shift, gs, B.d_sc, B.d_active, S);
   BK(bk_bicg_shift, gs, B.d_sc, B.d_active, S);
   BK(bk_count_running, 1, B.d_active, S, B.d_running);
 #undef BK
 }
 
+// the step graph; independent of the slots in use, so captured once (again
+// only when the autotuner changes the apply's grid)
 void ensure_graph(Batch &B)
 {
-  if (B.dirty) rebuild_tables(B);
   if (B.graph) return;
-  // one-time launcher set-up (tables, occupancy) must not happen inside the capture
-  launch_batch_apply<float>(BatchApplyPlan{}, nullptr, nullptr, nullptr, nullptr, 0, B.stream);
-  launch_batch_apply<double>(BatchApplyPlan{}, nullptr, nullptr, nullptr, nullptr, 0, B.stream);
+  const int blocks = batch_apply_blocks(B.tuned_cap);  // set-up of the launchers outside the capture
   const int64_t before = mpdg_kernel_launches();
   cudaGraph_t g = nullptr;
   MPDG_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
   try {
-    enqueue_step(B, B.tuned_cap);
+    enqueue_step(B, blocks);
   } catch (...) {
     cudaStreamEndCapture(B.stream, &g);
     if (g) cudaGraphDestroy(g);
@@ -1057,41 +1093,52 @@ int find_slot(const Batch &B, int64_t ticket)
   return -1;
 }
 
+int used_slots(const Batch &B)
+{
+  int k = 0;
+  for (const BatchSlot &S : B.slots) k += S.used ? 1 : 0;
+  return k;
+}
+
 // admission of one problem: slot vectors from the pool, Jacobi diagonal,
-// right-hand side, initial state.  Only enqueues work on the batch stream.
-int admit(Batch &B, const mpdg_problem_desc &d, const double *b_host, int64_t &ticket)
+// right-hand side, initial state, slot tables.  Only enqueues work on the
+// batch stream; returns the slot or -1 when the budget or the slots are full.
+int admit(Batch &B, const mpdg_problem_desc &d, const double *b_host, int64_t &ticket, long seq = 0)
 {
   check_desc(d);
   const long N = problem_dofs(d);
   const size_t bytes = slot_bytes(N, d.kind);
-  if (B.used + (int64_t)bytes > B.budget) return MPDG_ERR_BUDGET;
+  if (B.used + (int64_t)bytes > B.budget) return -1;
   int s = -1;
   for (int k = 0; k < B.capacity; ++k)
     if (!B.slots[k].used) {
       s = k;
       break;
     }
-  if (s < 0) return MPDG_ERR_BUDGET;
+  if (s < 0) return -1;
+  const SlotInfo info = slot_info(d);
   BatchSlot &S = B.slots[s];
   S = BatchSlot{};
   S.desc = d;
   S.N = N;
   S.bytes = bytes;
+  SlotPtrs &v = S.v;
   try {
-    S.x = palloc<double>(B, N);
-    S.b = palloc<double>(B, N);
-    S.r64 = palloc<double>(B, N);
-    S.r = palloc<float>(B, N);
-    S.z = palloc<float>(B, N);
-    S.p = palloc<float>(B, N);
-    S.Ap = palloc<float>(B, N);
-    S.invd = palloc<float>(B, N);
+    v.x = palloc<double>(B, N);
+    v.b = palloc<double>(B, N);
+    v.r64 = palloc<double>(B, N);
+    v.r = palloc<float>(B, N);
+    v.z = palloc<float>(B, N);
+    v.p = palloc<float>(B, N);
+    v.Ap = palloc<float>(B, N);
+    v.invd = palloc<float>(B, N);
     if (d.kind == MPDG_OP_ADVDIFF) {
-      S.rh = palloc<float>(B, N);
-      S.v = palloc<float>(B, N);
-      S.sv = palloc<float>(B, N);
-      S.t = palloc<float>(B, N);
+      v.rh = palloc<float>(B, N);
+      v.v = palloc<float>(B, N);
+      v.sv = palloc<float>(B, N);
+      v.t = palloc<float>(B, N);
     }
+    v.part = palloc<double>(B, 4 * (size_t)info.n_chunks);
   } catch (...) {
     free_slot_vectors(B, S);
     S = BatchSlot{};
@@ -1100,21 +1147,23 @@ int admit(Batch &B, const mpdg_problem_desc &d, const double *b_host, int64_t &t
   S.used = true;
   B.used += (int64_t)bytes;
   cudaStream_t st = B.stream;
-  const long NX = (long)d.nc * d.degree + 1;
-  enqueue_diagonal(d, S.r64, S.invd, nullptr, st);  // r64 is free scratch until the first defect
+  const long NX = info.NX;
+  enqueue_diagonal(d, v.r64, v.invd, nullptr, st);  // r64 is free scratch until the first defect
   if (b_host) {
-    MPDG_CUDA(cudaMemcpyAsync(S.b, b_host, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    MPDG_CUDA(cudaMemcpyAsync(v.b, b_host, sizeof(double) * N, cudaMemcpyHostToDevice, st));
     if (d.dirichlet) {
-      bk_set_boundary<<<grid1(N), 256, 0, st>>>(S.b, N, NX, 0.0);
+      bk_set_boundary<<<grid1(N), 256, 0, st>>>(v.b, N, NX, 0.0);
       MPDG_LAUNCHED();
     }
   } else {
-    bk_rhs<<<grid1(N), 256, 0, st>>>(S.b, N, NX, d.dirichlet, (unsigned long long)d.rhs_seed);
+    bk_rhs<<<grid1(N), 256, 0, st>>>(v.b, N, NX, d.dirichlet, (unsigned long long)d.rhs_seed);
     MPDG_LAUNCHED();
   }
-  dev_dot(S.b, S.b, N, B.d_adm, B.d_adm + kAdmBB, st);
-  bk_init_vectors<<<kRedBlocks, 256, 0, st>>>(S.b, B.d_adm + kAdmBB, S.x, S.r, S.z, S.p, S.invd, S.rh, N,
+  dev_dot(v.b, v.b, N, B.d_adm, B.d_adm + kAdmBB, st);
+  bk_init_vectors<<<kRedBlocks, 256, 0, st>>>(v.b, B.d_adm + kAdmBB, v.x, v.r, v.z, v.p, v.invd, v.rh, N,
                                               B.d_adm + kAdmInit);
+  MPDG_LAUNCHED();
+  bk_bind_slot<<<1, 1, 0, st>>>(B.tab, s, v, info);
   MPDG_LAUNCHED();
   const double rel = (d.rel_tolerance > 0.0 || d.abs_tolerance > 0.0) ? d.rel_tolerance : 1e-10;
   bk_init_scalars<<<1, 256, 0, st>>>(B.d_sc, B.d_active, B.d_defect, B.d_params, s, B.d_adm + kAdmInit,
@@ -1123,21 +1172,19 @@ int admit(Batch &B, const mpdg_problem_desc &d, const double *b_host, int64_t &t
                                      slot_params(d));
   MPDG_LAUNCHED();
   S.ticket = B.next_ticket++;
-  S.t_admit = now_s();
+  S.admit_seq = seq;
   ticket = S.ticket;
-  B.dirty = true;
-  return MPDG_OK;
+  return s;
 }
 
 void release(Batch &B, int s)
 {
   BatchSlot &S = B.slots[s];
+  MPDG_CUDA(cudaMemsetAsync(B.d_active + s, 0, sizeof(int), B.stream));
+  MPDG_CUDA(cudaMemsetAsync(B.d_defect + s, 0, sizeof(int), B.stream));
   free_slot_vectors(B, S);
   B.used -= (int64_t)S.bytes;
   S = BatchSlot{};
-  MPDG_CUDA(cudaMemsetAsync(B.d_active + s, 0, sizeof(int), B.stream));
-  MPDG_CUDA(cudaMemsetAsync(B.d_defect + s, 0, sizeof(int), B.stream));
-  B.dirty = true;
 }
 
 void report_of(const SlotScalars &q, mpdg_solve_report &rep)
@@ -1155,17 +1202,11 @@ void report_of(const SlotScalars &q, mpdg_solve_report &rep)
   rep.final_residual = q.res;
 }
 
-void fetch_scalars(Batch &B)
+void launch_steps(Batch &B, int k)
 {
-  MPDG_CUDA(cudaMemcpyAsync(B.h_sc, B.d_sc, sizeof(SlotScalars) * B.capacity, cudaMemcpyDeviceToHost, B.stream));
-  MPDG_CUDA(cudaStreamSynchronize(B.stream));
-}
-
-int used_slots(const Batch &B)
-{
-  int k = 0;
-  for (const BatchSlot &S : B.slots) k += S.used ? 1 : 0;
-  return k;
+  ensure_graph(B);
+  for (int i = 0; i < k; ++i) MPDG_CUDA(cudaGraphLaunch(B.graph, B.stream));
+  count_launch((int)(k * B.step_kernels));
 }
 
 // up to max_steps graph launches, reading the running count every poll steps
@@ -1173,14 +1214,11 @@ int run_steps(Batch &B, int max_steps, int poll, int &running)
 {
   running = 0;
   if (used_slots(B) == 0 || max_steps <= 0) return 0;
-  ensure_graph(B);
-  if (B.n_chunks == 0) return 0;
   poll = std::max(1, poll);
   int steps = 0;
   while (steps < max_steps) {
     const int k = std::min(poll, max_steps - steps);
-    for (int i = 0; i < k; ++i) MPDG_CUDA(cudaGraphLaunch(B.graph, B.stream));
-    count_launch((int)(k * B.step_kernels));
+    launch_steps(B, k);
     steps += k;
     MPDG_CUDA(cudaMemcpyAsync(B.h_running, B.d_running, sizeof(int), cudaMemcpyDeviceToHost, B.stream));
     MPDG_CUDA(cudaStreamSynchronize(B.stream));
@@ -1190,31 +1228,124 @@ int run_steps(Batch &B, int max_steps, int poll, int &running)
   return steps;
 }
 
-double slot_norm(Batch &B, const BatchSlot &S)
-{
-  dev_dot(S.x, S.x, S.N, B.d_adm, B.d_adm + kAdmNorm, B.stream);
-  double v = 0.0;
-  MPDG_CUDA(cudaMemcpyAsync(&v, B.d_adm + kAdmNorm, sizeof(double), cudaMemcpyDeviceToHost, B.stream));
-  MPDG_CUDA(cudaStreamSynchronize(B.stream));
-  return std::sqrt(v);
-}
-
 void destroy_batch(Batch &B)
 {
   if (B.stream) cudaStreamSynchronize(B.stream);
-  for (int s = 0; s < B.capacity; ++s)
+  if (B.copy_stream) cudaStreamSynchronize(B.copy_stream);
+  for (int s = 0; s < B.capacity && s < (int)B.slots.size(); ++s)
     if (B.slots[s].used) free_slot_vectors(B, B.slots[s]);
   if (B.stream) cudaStreamSynchronize(B.stream);
-  free_plan(B);
-  for (void *p : {(void *)B.d_sc, (void *)B.d_params, (void *)B.d_active, (void *)B.d_defect, (void *)B.d_x,
-                  (void *)B.d_b, (void *)B.d_r64, (void *)B.d_r, (void *)B.d_z, (void *)B.d_p, (void *)B.d_Ap,
-                  (void *)B.d_invd, (void *)B.d_rh, (void *)B.d_v, (void *)B.d_sv, (void *)B.d_t,
-                  (void *)B.d_running, (void *)B.d_adm, (void *)B.d_slot_chunk})
+  drop_graph(B);
+  for (BatchSchedule &S : B.sched) free_schedule(S);
+  const BatchTables &T = B.tab;
+  for (void *p : {(void *)T.x, (void *)T.b, (void *)T.r64, (void *)T.r, (void *)T.z, (void *)T.p,
+                  (void *)T.Ap, (void *)T.invd, (void *)T.rh, (void *)T.v, (void *)T.sv, (void *)T.t,
+                  (void *)T.part, (void *)T.info, (void *)B.d_sc, (void *)B.d_params, (void *)B.d_active,
+                  (void *)B.d_defect, (void *)B.d_running, (void *)B.d_adm, (void *)B.d_res})
     if (p) cudaFree(p);
-  if (B.h_running) cudaFreeHost(B.h_running);
-  if (B.h_sc) cudaFreeHost(B.h_sc);
+  for (void *p : {(void *)B.h_running, (void *)B.h_active[0], (void *)B.h_active[1], (void *)B.h_sc,
+                  (void *)B.h_norm})
+    if (p) cudaFreeHost(p);
   if (B.pool) cudaMemPoolDestroy(B.pool);
   if (B.stream) cudaStreamDestroy(B.stream);
+  if (B.copy_stream) cudaStreamDestroy(B.copy_stream);
+}
+
+// Serving loop.  Two groups of poll_steps graph steps are kept in flight, each
+// followed by a snapshot of the running flags; while the GPU runs the newer
+// group the host reads the older snapshot, copies the finished slots' results
+// on the copy stream (their data no longer changes) and releases them, and
+// admits the requests that have arrived.
+void serve(Batch &B, const mpdg_problem_desc *req, const double *arr, int n, int poll, double **x_host,
+           double *latency, double *x_norm, mpdg_solve_report *reports, double &wall)
+{
+  long max_n = 0;
+  for (int i = 0; i < n; ++i) {
+    check_desc(req[i]);
+    if (i && arr[i] < arr[i - 1]) throw Error{MPDG_ERR_ARG, "arrival times must ascend"};
+    const long N = problem_dofs(req[i]);
+    if ((int64_t)slot_bytes(N, req[i].kind) > B.budget)
+      throw Error{MPDG_ERR_BUDGET, "a request is larger than the whole budget"};
+    max_n = std::max(max_n, N);
+  }
+  poll = std::max(1, poll);
+  double *staging = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  struct Poll {
+    int buf;
+    long seq;
+  };
+  std::deque<Poll> pend;
+  std::vector<int> slot_req(B.capacity, -1);
+  int next = 0, done = 0, buf = 1;
+  long seq = 0;
+  const double t0 = now_s();
+  double t_last = t0;
+  try {
+    if (max_n) MPDG_CUDA(cudaHostAlloc((void **)&staging, sizeof(double) * max_n, cudaHostAllocDefault));
+    for (cudaEvent_t &e : ev) MPDG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    while (done < n) {
+      const double t = now_s() - t0;
+      while (next < n && arr[next] <= t) {
+        int64_t tk = -1;
+        const int s = admit(B, req[next], nullptr, tk, ++seq);
+        if (s < 0) break;  // waits for memory or a slot
+        slot_req[s] = next;
+        ++next;
+      }
+      const int used = used_slots(B);
+      if (used > 0 && pend.size() < 2) {
+        launch_steps(B, poll);
+        buf ^= 1;
+        MPDG_CUDA(cudaMemcpyAsync(B.h_active[buf], B.d_active, sizeof(int) * B.capacity, cudaMemcpyDeviceToHost,
+                                  B.stream));
+        MPDG_CUDA(cudaEventRecord(ev[buf], B.stream));
+        pend.push_back({buf, ++seq});
+        if (pend.size() < 2) continue;
+      }
+      if (pend.empty()) {
+        if (next < n) {
+          const double wait = arr[next] - (now_s() - t0);
+          if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
+        }
+        continue;
+      }
+      const Poll P = pend.front();
+      pend.pop_front();
+      MPDG_CUDA(cudaEventSynchronize(ev[P.buf]));
+      const int *act = B.h_active[P.buf];
+      for (int s = 0; s < B.capacity; ++s) {
+        BatchSlot &S = B.slots[s];
+        if (!S.used || S.admit_seq >= P.seq || act[s]) continue;
+        const int i = slot_req[s];
+        cudaStream_t cs = B.copy_stream;
+        dev_dot(S.v.x, S.v.x, S.N, B.d_res, B.d_res + kAdmNorm, cs);
+        MPDG_CUDA(cudaMemcpyAsync(B.h_norm, B.d_res + kAdmNorm, sizeof(double), cudaMemcpyDeviceToHost, cs));
+        MPDG_CUDA(cudaMemcpyAsync(B.h_sc + s, B.d_sc + s, sizeof(SlotScalars), cudaMemcpyDeviceToHost, cs));
+        double *dst = (x_host && x_host[i]) ? x_host[i] : staging;
+        MPDG_CUDA(cudaMemcpyAsync(dst, S.v.x, sizeof(double) * S.N, cudaMemcpyDeviceToHost, cs));
+        MPDG_CUDA(cudaStreamSynchronize(cs));
+        t_last = now_s();
+        if (latency) latency[i] = (t_last - t0) - arr[i];
+        if (x_norm) x_norm[i] = std::sqrt(*B.h_norm);
+        if (reports) report_of(B.h_sc[s], reports[i]);
+        release(B, s);
+        slot_req[s] = -1;
+        ++done;
+      }
+    }
+    MPDG_CUDA(cudaStreamSynchronize(B.stream));
+  } catch (...) {
+    cudaStreamSynchronize(B.stream);
+    cudaStreamSynchronize(B.copy_stream);
+    if (staging) cudaFreeHost(staging);
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+    throw;
+  }
+  if (staging) cudaFreeHost(staging);
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  wall = t_last - t0;
 }
 
 }  // namespace
@@ -1243,6 +1374,7 @@ mpdg_status mpdg_batch_create(int64_t budget_bytes, int capacity, double reliabl
       B.delta = reliable_delta;
       MPDG_CUDA(cudaGetDevice(&B.device));
       MPDG_CUDA(cudaStreamCreateWithFlags(&B.stream, cudaStreamNonBlocking));
+      MPDG_CUDA(cudaStreamCreateWithFlags(&B.copy_stream, cudaStreamNonBlocking));
       cudaMemPoolProps props{};
       props.allocType = cudaMemAllocationTypePinned;
       props.location.type = cudaMemLocationTypeDevice;
@@ -1251,31 +1383,40 @@ mpdg_status mpdg_batch_create(int64_t budget_bytes, int capacity, double reliabl
       uint64_t keep = UINT64_MAX;
       MPDG_CUDA(cudaMemPoolSetAttribute(B.pool, cudaMemPoolAttrReleaseThreshold, &keep));
       B.slots.resize(capacity);
+      BatchTables &T = B.tab;
+      T.x = balloc<double *>(capacity);
+      T.b = balloc<double *>(capacity);
+      T.r64 = balloc<double *>(capacity);
+      T.r = balloc<float *>(capacity);
+      T.z = balloc<float *>(capacity);
+      T.p = balloc<float *>(capacity);
+      T.Ap = balloc<float *>(capacity);
+      T.invd = balloc<float *>(capacity);
+      T.rh = balloc<float *>(capacity);
+      T.v = balloc<float *>(capacity);
+      T.sv = balloc<float *>(capacity);
+      T.t = balloc<float *>(capacity);
+      T.part = balloc<double *>(capacity);
+      T.info = balloc<SlotInfo>(capacity);
       B.d_sc = balloc<SlotScalars>(capacity);
       B.d_params = balloc<BatchSlotParams>(capacity);
-      B.d_active = balloc<int>(2 * (size_t)capacity);
+      B.d_active = balloc<int>(capacity);
       B.d_defect = balloc<int>(capacity);
-      B.d_x = balloc<double *>(capacity);
-      B.d_b = balloc<double *>(capacity);
-      B.d_r64 = balloc<double *>(capacity);
-      B.d_r = balloc<float *>(capacity);
-      B.d_z = balloc<float *>(capacity);
-      B.d_p = balloc<float *>(capacity);
-      B.d_Ap = balloc<float *>(capacity);
-      B.d_invd = balloc<float *>(capacity);
-      B.d_rh = balloc<float *>(capacity);
-      B.d_v = balloc<float *>(capacity);
-      B.d_sv = balloc<float *>(capacity);
-      B.d_t = balloc<float *>(capacity);
       B.d_running = balloc<int>(1);
       B.d_adm = balloc<double>(kAdmDoubles);
-      B.d_slot_chunk = balloc<int>(2 * (size_t)capacity);
+      B.d_res = balloc<double>(kAdmDoubles);
+      for (BatchSchedule &S : B.sched) alloc_schedule(S, capacity);
+      MPDG_CUDA(cudaMemset(T.info, 0, sizeof(SlotInfo) * capacity));
       MPDG_CUDA(cudaMemset(B.d_sc, 0, sizeof(SlotScalars) * capacity));
-      MPDG_CUDA(cudaMemset(B.d_active, 0, sizeof(int) * 2 * capacity));
+      MPDG_CUDA(cudaMemset(B.d_active, 0, sizeof(int) * capacity));
       MPDG_CUDA(cudaMemset(B.d_defect, 0, sizeof(int) * capacity));
-      MPDG_CUDA(cudaMemset(B.d_slot_chunk, 0, sizeof(int) * 2 * capacity));
+      MPDG_CUDA(cudaMemset(B.d_running, 0, sizeof(int)));
       MPDG_CUDA(cudaHostAlloc((void **)&B.h_running, sizeof(int), cudaHostAllocDefault));
+      for (int k = 0; k < 2; ++k)
+        MPDG_CUDA(cudaHostAlloc((void **)&B.h_active[k], sizeof(int) * capacity, cudaHostAllocDefault));
       MPDG_CUDA(cudaHostAlloc((void **)&B.h_sc, sizeof(SlotScalars) * capacity, cudaHostAllocDefault));
+      MPDG_CUDA(cudaHostAlloc((void **)&B.h_norm, sizeof(double), cudaHostAllocDefault));
+      MPDG_CUDA(cudaDeviceSynchronize());
     } catch (...) {
       destroy_batch(B);
       delete h;
@@ -1342,9 +1483,9 @@ mpdg_status mpdg_batch_submit(mpdg_batch *batch, const mpdg_problem_desc *desc, 
 {
   return guarded([&]() -> int {
     if (!batch || !desc || !ticket) throw Error{MPDG_ERR_ARG, "null argument"};
-    const int rc = admit(batch->b, *desc, rhs, *ticket);
-    if (rc == MPDG_ERR_BUDGET) set_last_error("problem does not fit the free budget or no slot is free");
-    return rc;
+    if (admit(batch->b, *desc, rhs, *ticket) < 0)
+      throw Error{MPDG_ERR_BUDGET, "problem does not fit the free budget or no slot is free"};
+    return MPDG_OK;
   });
 }
 
@@ -1386,7 +1527,7 @@ mpdg_status mpdg_batch_take(mpdg_batch *batch, int64_t ticket, double *x_host, m
     if (B.h_sc[s].status == SL_RUNNING) throw Error{MPDG_ERR_ARG, "problem still running"};
     const BatchSlot &S = B.slots[s];
     if (x_host) {
-      MPDG_CUDA(cudaMemcpyAsync(x_host, S.x, sizeof(double) * S.N, cudaMemcpyDeviceToHost, B.stream));
+      MPDG_CUDA(cudaMemcpyAsync(x_host, S.v.x, sizeof(double) * S.N, cudaMemcpyDeviceToHost, B.stream));
       MPDG_CUDA(cudaStreamSynchronize(B.stream));
     }
     if (report) report_of(B.h_sc[s], *report);
@@ -1401,38 +1542,45 @@ mpdg_status mpdg_batch_autotune(mpdg_batch *batch, int *ctas_per_sm, double *app
     if (!batch) throw Error{MPDG_ERR_ARG, "null argument"};
     Batch &B = batch->b;
     if (used_slots(B) == 0) throw Error{MPDG_ERR_ARG, "autotuning needs admitted problems"};
-    if (B.dirty) rebuild_tables(B);
     std::vector<int> ones(B.capacity, 0);
     for (int s = 0; s < B.capacity; ++s) ones[s] = B.slots[s].used ? 1 : 0;
     int *d_all = balloc<int>(B.capacity);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int best_cap = 0;
     double best = 1e30;
+    const BatchSchedule &SD = B.sched[2];  // scratch schedule outside the graph steps
     try {
+      MPDG_CUDA(cudaStreamSynchronize(B.stream));
       MPDG_CUDA(cudaMemcpy(d_all, ones.data(), sizeof(int) * B.capacity, cudaMemcpyHostToDevice));
+      bk_schedule<<<9, kSchedThreads, 0, B.stream>>>(d_all, -1, B.tab.info, B.capacity, SD);
+      MPDG_LAUNCHED();
       MPDG_CUDA(cudaEventCreate(&e0));
       MPDG_CUDA(cudaEventCreate(&e1));
       for (int cap : {1, 2, 3, 4, 6, 8, 0}) {
-        launch_batch_apply<float>(B.plan, B.d_params, B.d_p, B.d_Ap, d_all, cap, B.stream);
+        const int blocks = batch_apply_blocks(cap);
+        launch_batch_apply<float>(SD, B.tab.info, B.d_params, B.tab.p, B.tab.Ap, d_all, blocks, B.stream);
         MPDG_CUDA(cudaEventRecord(e0, B.stream));
         const int reps = 5;
-        for (int r = 0; r < reps; ++r) launch_batch_apply<float>(B.plan, B.d_params, B.d_p, B.d_Ap, d_all, cap, B.stream);
+        for (int r = 0; r < reps; ++r)
+          launch_batch_apply<float>(SD, B.tab.info, B.d_params, B.tab.p, B.tab.Ap, d_all, blocks, B.stream);
         MPDG_CUDA(cudaEventRecord(e1, B.stream));
         MPDG_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         MPDG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         const double t = ms / reps;
-        if (t < best * 0.98) {  // prefer the earlier (smaller) cap unless clearly faster
+        if (t < best * 0.98) {  // prefer the smaller cap unless clearly faster
           best = t;
           best_cap = cap;
         }
       }
     } catch (...) {
+      cudaStreamSynchronize(B.stream);
       cudaFree(d_all);
       if (e0) cudaEventDestroy(e0);
       if (e1) cudaEventDestroy(e1);
       throw;
     }
+    MPDG_CUDA(cudaStreamSynchronize(B.stream));
     cudaFree(d_all);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1460,62 +1608,9 @@ mpdg_status mpdg_serve(mpdg_batch *batch, const mpdg_problem_desc *req, const do
     if (!batch || (!req && n > 0) || (!arrival_s && n > 0) || n < 0) throw Error{MPDG_ERR_ARG, "null argument"};
     Batch &B = batch->b;
     if (used_slots(B) != 0) throw Error{MPDG_ERR_ARG, "serving starts on an empty batch"};
-    long max_n = 0;
-    for (int i = 0; i < n; ++i) {
-      check_desc(req[i]);
-      if (i && arrival_s[i] < arrival_s[i - 1]) throw Error{MPDG_ERR_ARG, "arrival times must ascend"};
-      const long N = problem_dofs(req[i]);
-      if ((int64_t)slot_bytes(N, req[i].kind) > B.budget)
-        throw Error{MPDG_ERR_BUDGET, "a request is larger than the whole budget"};
-      max_n = std::max(max_n, N);
-    }
-    double *staging = nullptr;
-    if (max_n) MPDG_CUDA(cudaHostAlloc((void **)&staging, sizeof(double) * max_n, cudaHostAllocDefault));
-    std::vector<int> slot_req(B.capacity, -1);
-    int next = 0, done = 0;
-    const double t0 = now_s();
-    double t_last = t0;
-    try {
-      while (done < n) {
-        const double t = now_s() - t0;
-        while (next < n && arrival_s[next] <= t) {
-          int64_t tk = -1;
-          if (admit(B, req[next], nullptr, tk) != MPDG_OK) break;  // waits for memory or a slot
-          slot_req[find_slot(B, tk)] = next;
-          ++next;
-        }
-        if (used_slots(B) == 0) {
-          if (next < n) {
-            const double wait = arrival_s[next] - (now_s() - t0);
-            if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.05)));
-          }
-          continue;
-        }
-        int running = 0;
-        run_steps(B, std::max(1, poll_steps), std::max(1, poll_steps), running);
-        fetch_scalars(B);
-        for (int s = 0; s < B.capacity; ++s) {
-          if (!B.slots[s].used || B.h_sc[s].status == SL_RUNNING) continue;
-          const int i = slot_req[s];
-          const BatchSlot &S = B.slots[s];
-          if (x_norm) x_norm[i] = slot_norm(B, S);
-          double *dst = (x_host && x_host[i]) ? x_host[i] : staging;
-          MPDG_CUDA(cudaMemcpyAsync(dst, S.x, sizeof(double) * S.N, cudaMemcpyDeviceToHost, B.stream));
-          MPDG_CUDA(cudaStreamSynchronize(B.stream));
-          t_last = now_s();
-          if (latency_s) latency_s[i] = (t_last - t0) - arrival_s[i];
-          if (reports) report_of(B.h_sc[s], reports[i]);
-          release(B, s);
-          slot_req[s] = -1;
-          ++done;
-        }
-      }
-    } catch (...) {
-      if (staging) cudaFreeHost(staging);
-      throw;
-    }
-    if (staging) cudaFreeHost(staging);
-    if (wall_s) *wall_s = t_last - t0;
+    double wall = 0.0;
+    serve(B, req, arrival_s, n, poll_steps, x_host, latency_s, x_norm, reports, wall);
+    if (wall_s) *wall_s = wall;
     return MPDG_OK;
   });
 }

@@ -117,13 +117,18 @@ struct Op {
 };
 
 // ---- batched apply over many solves (batch_apply.cuh / batch.cu)
-struct BatchSeg {
-  int slot;                        // solve slot
-  int nc;                          // cells per direction
-  int cn[3], par[3];               // this colour's cells per direction and parity
-  int count;                       // cells of this colour
-  unsigned long long div0_magic, div01_magic;
-  long NX;                         // DoFs per direction (nc*p + 1)
+// per problem and colour: cells of the colour, cells per direction in x and y,
+// warp groups (cells per warp packed), magic divisors of cn0 and cn0*cn1
+struct SlotColour {
+  int count, cn0, cn1, groups;
+  unsigned long long m0, m01;
+};
+
+// static description of a batch slot (written when a problem is admitted)
+struct SlotInfo {
+  int degree, nc, kind, n_chunks;
+  long NX, N;
+  SlotColour col[8];
 };
 
 struct BatchSlotParams {
@@ -132,19 +137,31 @@ struct BatchSlotParams {
   int vel_kind, dirichlet;
 };
 
-// segment tables of one batch membership: per degree (1..4) and colour
-struct BatchApplyPlan {
-  BatchSeg *segs[kMaxDegree + 1][8] = {};
-  int *prefix[kMaxDegree + 1][8] = {};
-  int nseg[kMaxDegree + 1][8] = {};
-  int groups[kMaxDegree + 1][8] = {};
+// compacted work list of the flagged slots, rebuilt on the device every step:
+// per colour the flagged slots with cells of that colour and the prefix of
+// their warp groups; the flagged slots with the prefix of their vector chunks
+struct BatchScheduleHeader {
+  int n_seg[8], total_groups[8];
+  int n_slots, total_chunks;
+};
+
+struct BatchSchedule {
+  BatchScheduleHeader *hdr = nullptr;
+  int *seg_slot = nullptr;    // [8][cap]
+  int *seg_prefix = nullptr;  // [8][cap]
+  int *act_slot = nullptr;    // [cap]
+  int *chunk_prefix = nullptr;  // [cap]
+  int cap = 0;
 };
 
 // cells per warp of the warp-per-cell kernels for degree p (32 / (p+1)^2)
 int cells_per_warp(int degree);
+// persistent grid of the batched apply: SMs x min(cap, occupancy) (cap 0: occupancy)
+int batch_apply_blocks(int ctas_per_sm_cap);
+// one launch per colour over the scheduled slots whose mask entry is set
 template <typename Real>
-void launch_batch_apply(const BatchApplyPlan &plan, const BatchSlotParams *params, Real *const *src,
-                        Real *const *dst, const int *active, int blocks_per_sm_cap, cudaStream_t s);
+void launch_batch_apply(const BatchSchedule &sched, const SlotInfo *info, const BatchSlotParams *params,
+                        Real *const *src, Real *const *dst, const int *mask, int blocks, cudaStream_t s);
 
 // ---- operator kernels (operator_kernels.cu)
 // 1D tables of degree p on [0,1]: GLL Lagrange basis values S[q*(p+1)+i] and

@@ -993,7 +993,7 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
 void ensure_metric32(Mesh &m, cudaStream_t s)
 {
   if (m.uniform || m.metric32_ready) return;
-  const int n = m.degree + 1, n3 = n * n * n;
+  const int n = m.degree + 1;
   const long total = m.n_cells * metric_stride(n);
   m.d_metric32 = dev_alloc<float>(total, m.device_bytes);
   cast_kernel<<<grid_for(total, 256), 256, 0, s>>>(m.d_metric64, m.d_metric32, total);
@@ -1526,43 +1526,41 @@ int cells_per_warp(int degree)
 }
 
 namespace {
-template <int P, typename Real>
-void run_batch_apply(const BatchApplyPlan &plan, const BatchSlotParams *params, Real *const *src,
-                     Real *const *dst, const int *active, int cap, cudaStream_t s)
+template <typename Real>
+int batch_occupancy()
 {
-  auto kern = batch_apply_kernel<P, Real>;
   static int blocks_per_sm = 0;
   if (!blocks_per_sm) {
     upload_tables();
-    MPDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerCTA * 32, 0));
+    MPDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, batch_apply_kernel<Real>,
+                                                            kWarpsPerCTA * 32, 0));
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
-  const int bps = (cap > 0) ? std::min(cap, blocks_per_sm) : blocks_per_sm;
-  for (int c = 0; c < 8; ++c) {
-    const int groups = plan.groups[P][c];
-    if (groups == 0) continue;
-    const long blocks = std::min((long)num_sms() * bps, (long)(groups + kWarpsPerCTA - 1) / kWarpsPerCTA);
-    kern<<<(unsigned)blocks, kWarpsPerCTA * 32, 0, s>>>(plan.segs[P][c], plan.prefix[P][c],
-                                                        plan.nseg[P][c], groups, params, src, dst, active);
-    MPDG_LAUNCHED();
-  }
+  return blocks_per_sm;
 }
 }  // namespace
 
-template <typename Real>
-void launch_batch_apply(const BatchApplyPlan &plan, const BatchSlotParams *params, Real *const *src,
-                        Real *const *dst, const int *active, int cap, cudaStream_t s)
+int batch_apply_blocks(int cap)
 {
-  run_batch_apply<1, Real>(plan, params, src, dst, active, cap, s);
-  run_batch_apply<2, Real>(plan, params, src, dst, active, cap, s);
-  run_batch_apply<3, Real>(plan, params, src, dst, active, cap, s);
-  run_batch_apply<4, Real>(plan, params, src, dst, active, cap, s);
+  const int occ = std::min(batch_occupancy<float>(), batch_occupancy<double>());
+  return num_sms() * ((cap > 0) ? std::min(cap, occ) : occ);
 }
-template void launch_batch_apply<double>(const BatchApplyPlan &, const BatchSlotParams *,
-                                         double *const *, double *const *, const int *, int,
-                                         cudaStream_t);
-template void launch_batch_apply<float>(const BatchApplyPlan &, const BatchSlotParams *,
-                                        float *const *, float *const *, const int *, int,
-                                        cudaStream_t);
+
+template <typename Real>
+void launch_batch_apply(const BatchSchedule &sched, const SlotInfo *info, const BatchSlotParams *params,
+                        Real *const *src, Real *const *dst, const int *mask, int blocks, cudaStream_t s)
+{
+  batch_occupancy<Real>();  // tables uploaded before any launch (and before graph capture)
+  for (int c = 0; c < 8; ++c) {
+    batch_apply_kernel<Real><<<(unsigned)blocks, kWarpsPerCTA * 32, 0, s>>>(
+        c, sched.hdr, sched.seg_slot + (size_t)c * sched.cap, sched.seg_prefix + (size_t)c * sched.cap, info,
+        params, src, dst, mask);
+    MPDG_LAUNCHED();
+  }
+}
+template void launch_batch_apply<double>(const BatchSchedule &, const SlotInfo *, const BatchSlotParams *,
+                                         double *const *, double *const *, const int *, int, cudaStream_t);
+template void launch_batch_apply<float>(const BatchSchedule &, const SlotInfo *, const BatchSlotParams *,
+                                        float *const *, float *const *, const int *, int, cudaStream_t);
 
 }  // namespace mpdg
