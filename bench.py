@@ -456,7 +456,7 @@ def run_batch(args, rank, world):
     from meltpooldg_b200 import batch as B
     local = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(local)
-    probs = batch_problems()
+    probs = batch_problems(args.problems)
     n_dofs = [p.n_dofs for p in probs]
     N_total = int(sum(n_dofs))
     budget = 150 * 10**9
@@ -507,7 +507,7 @@ def run_batch(args, rank, world):
     roof = {"bound": "hbm", "achieved": b_apply / (apply_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
             "frac": b_apply / (apply_ms * 1e-3) / 1e9 / peak, "traffic": None,
             "algorithmic_bytes": b_apply,
-            "kernel": "batch_apply_kernel<P,float> (P = 2, 3, 4) x 8 colour launches each, all 256 problems",
+            "kernel": f"batch_apply_kernel<float> x 8 colour launches over all {len(probs)} problems",
             "apply_ms": apply_ms, "autotuned_ctas_per_sm": cap,
             "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
     cpu = None
@@ -520,7 +520,7 @@ def run_batch(args, rank, world):
             "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 apply / f64 residuals", "data": "synthetic",
-            "config": {"workload": "256 heat solves, n^3 cells n~U{8..48}, Q2/Q3/Q4, k0 log-uniform [1,100], "
+            "config": {"workload": f"{len(probs)} heat solves, n^3 cells n~U{{8..48}}, Q2/Q3/Q4, k0 log-uniform [1,100], "
                                    "dt=1e-3, seeded rhs, CG + Jacobi to 1e-10",
                        "n_dofs_total": N_total, "problems": len(probs),
                        "l2": f"inputs larger than L2: {N_total * 44 / 1e9:.1f} GB resident",
@@ -661,6 +661,8 @@ def main():
     ap.add_argument("--cells", type=int, default=0,
                     help="cells per direction (default: the workload's; smaller sizes for profiling)")
     ap.add_argument("--workload", default="heat", choices=["heat", "advdiff", "batch", "serve"])
+    ap.add_argument("--problems", type=int, default=BATCH_SIZE,
+                    help="batch: problems in the batch (the first of the seeded sequence)")
     ap.add_argument("--requests", type=int, default=20000, help="serve: requests in the stream")
     ap.add_argument("--poll-steps", type=int, default=4, help="serve: graph steps between checks")
     ap.add_argument("--no-fp64-arm", action="store_true", help="serve: skip the plain FP64 arm")
