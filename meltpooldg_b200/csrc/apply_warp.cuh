@@ -87,68 +87,133 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t *bar, unsigned phase,
   }
 }
 
-// ---- warp-synchronous contraction passes (tile layout t[k*n*n + j*n + i])
-// Sc: table in constant memory (uniform index: z passes); Ss: the same table in
-// shared memory (lane-dependent rows: x and y passes)
+// ---- warp-synchronous sum factorisation with line ownership.
+// The n^2 lanes of a cell own one 1D line of the n^3 tensor at a time, in one
+// of three layouts (lane l = a + n b):
+//   Z: lane (a, b) = (i, j) holds v[k], k = 0..n-1
+//   X: lane (a, b) = (j, k) holds v[i]
+//   Y: lane (a, b) = (i, k) holds v[j]
+// Every 1D contraction runs in registers on the owned line (tables in
+// constant memory, compile-time indices); the layout changes go through the
+// cell's shared tile t[k n^2 + j n + i] with n stores and n loads per lane.
+// The former scheme read n^2 tile values per lane for each x or y pass.
 
 template <int n, typename Real>
-__device__ __forceinline__ void w_to_qp(const Real *Sc, const Real *Ss, Real *t, bool wr, int i,
-                                        int j, const Real (&u)[n], Real (&v)[n])
+__device__ __forceinline__ void putZ(Real *t, int a, int b, const Real (&v)[n])
 {
-  Real a[n];
-  cz<n, Real, false>(Sc, u, a);
-  if (wr) put<n>(t, i, j, a);
-  __syncwarp();
-  cy<n, Real, false>(Ss, t, i, j, v);
-  __syncwarp();
-  if (wr) put<n>(t, i, j, v);
-  __syncwarp();
-  cx<n, Real, false>(Ss, t, i, j, a);
-  __syncwarp();
 #pragma unroll
-  for (int k = 0; k < n; ++k) v[k] = a[k];
+  for (int k = 0; k < n; ++k) t[k * n * n + b * n + a] = v[k];
+}
+template <int n, typename Real>
+__device__ __forceinline__ void getZ(const Real *t, int a, int b, Real (&v)[n])
+{
+#pragma unroll
+  for (int k = 0; k < n; ++k) v[k] = t[k * n * n + b * n + a];
+}
+template <int n, typename Real>
+__device__ __forceinline__ void putX(Real *t, int a, int b, const Real (&v)[n])
+{
+#pragma unroll
+  for (int i = 0; i < n; ++i) t[b * n * n + a * n + i] = v[i];
+}
+template <int n, typename Real>
+__device__ __forceinline__ void getX(const Real *t, int a, int b, Real (&v)[n])
+{
+#pragma unroll
+  for (int i = 0; i < n; ++i) v[i] = t[b * n * n + a * n + i];
+}
+template <int n, typename Real>
+__device__ __forceinline__ void putY(Real *t, int a, int b, const Real (&v)[n])
+{
+#pragma unroll
+  for (int j = 0; j < n; ++j) t[b * n * n + j * n + a] = v[j];
+}
+template <int n, typename Real>
+__device__ __forceinline__ void getY(const Real *t, int a, int b, Real (&v)[n])
+{
+#pragma unroll
+  for (int j = 0; j < n; ++j) v[j] = t[b * n * n + j * n + a];
 }
 
+// nodal values u (Z layout) -> values uq and collocation gradients gx, gy, gz
+// at the Gauss points, all in Z layout.  S, Dc: tables in constant memory.
 template <int n, typename Real>
-__device__ __forceinline__ void w_grad_qp(const Real *Dcc, const Real *Dcs, Real *t, bool wr, int i,
-                                          int j, const Real (&v)[n], Real (&gx)[n], Real (&gy)[n],
-                                          Real (&gz)[n])
+__device__ __forceinline__ void l_forward(const Real *S, const Real *Dc, Real *t0, Real *t1, bool wr, int a,
+                                          int b, const Real (&u)[n], Real (&uq)[n], Real (&gx)[n],
+                                          Real (&gy)[n], Real (&gz)[n])
 {
-  if (wr) put<n>(t, i, j, v);
+  Real v[n], w[n];
+  cz<n, Real, false>(S, u, v);  // z: nodes -> Gauss points
+  if (wr) putZ<n>(t0, a, b, v);
   __syncwarp();
-  cx<n, Real, false>(Dcs, t, i, j, gx);
-  cy<n, Real, false>(Dcs, t, i, j, gy);
-  cz<n, Real, false>(Dcc, v, gz);
+  getX<n>(t0, a, b, w);
   __syncwarp();
-}
-
-template <int n, typename Real>
-__device__ __forceinline__ void w_from_qp(const Real *Sc, const Real *Ss, const Real *Dcc,
-                                          const Real *Dcs, Real *t0, Real *t1, bool wr, int i, int j,
-                                          const Real (&val)[n], const Real (&fx)[n],
-                                          const Real (&fy)[n], const Real (&fz)[n], Real (&out)[n])
-{
-  Real a[n], b[n];
+  cz<n, Real, false>(S, w, v);  // x
+  if (wr) putX<n>(t0, a, b, v);
+  __syncwarp();
+  getY<n>(t0, a, b, w);
+  __syncwarp();
+  cz<n, Real, false>(S, w, v);   // y: v = values at the Gauss points (Y layout)
+  cz<n, Real, false>(Dc, v, w);  // d/dy (Y layout)
   if (wr) {
-    put<n>(t0, i, j, fx);
-    put<n>(t1, i, j, fy);
+    putY<n>(t0, a, b, v);
+    putY<n>(t1, a, b, w);
   }
   __syncwarp();
-  cx<n, Real, true>(Dcs, t0, i, j, a);
-  cy<n, Real, true>(Dcs, t1, i, j, b);
-  cz<n, Real, true>(Dcc, fz, out);
+  getZ<n>(t0, a, b, uq);
+  getX<n>(t0, a, b, w);
+  getZ<n>(t1, a, b, gy);
+  __syncwarp();
+  cz<n, Real, false>(Dc, uq, gz);  // d/dz (Z layout)
+  cz<n, Real, false>(Dc, w, v);    // d/dx (X layout)
+  if (wr) putX<n>(t0, a, b, v);
+  __syncwarp();
+  getZ<n>(t0, a, b, gx);
+  __syncwarp();
+}
+
+// test functions: out = S^T (val + Dc_x^T fx + Dc_y^T fy + Dc_z^T fz) in all
+// three directions; inputs at the Gauss points and output at the nodes, Z layout
+template <int n, typename Real>
+__device__ __forceinline__ void l_backward(const Real *S, const Real *Dc, Real *t0, Real *t1, bool wr, int a,
+                                           int b, const Real (&val)[n], const Real (&fx)[n],
+                                           const Real (&fy)[n], const Real (&fz)[n], Real (&out)[n])
+{
+  Real A[n], B[n], C[n], w[n];
+  cz<n, Real, true>(Dc, fz, A);
 #pragma unroll
-  for (int k = 0; k < n; ++k) a[k] += b[k] + out[k] + val[k];
+  for (int k = 0; k < n; ++k) A[k] += val[k];  // Z layout
+  if (wr) {
+    putZ<n>(t0, a, b, fx);
+    putZ<n>(t1, a, b, fy);
+  }
   __syncwarp();
-  if (wr) put<n>(t0, i, j, a);
+  getX<n>(t0, a, b, w);
+  getY<n>(t1, a, b, C);
   __syncwarp();
-  cx<n, Real, true>(Ss, t0, i, j, b);
+  cz<n, Real, true>(Dc, w, B);  // x part (X layout)
+  cz<n, Real, true>(Dc, C, w);  // y part (Y layout)
+  if (wr) {
+    putZ<n>(t0, a, b, A);
+    putX<n>(t1, a, b, B);
+  }
   __syncwarp();
-  if (wr) put<n>(t0, i, j, b);
+  getY<n>(t0, a, b, A);
+  getY<n>(t1, a, b, B);
   __syncwarp();
-  cy<n, Real, true>(Ss, t0, i, j, a);
-  cz<n, Real, true>(Sc, a, out);
+#pragma unroll
+  for (int q = 0; q < n; ++q) C[q] = w[q] + A[q] + B[q];  // sum in Y layout
+  cz<n, Real, true>(S, C, w);  // y: Gauss points -> nodes
+  if (wr) putY<n>(t0, a, b, w);
   __syncwarp();
+  getX<n>(t0, a, b, C);
+  __syncwarp();
+  cz<n, Real, true>(S, C, w);  // x
+  if (wr) putX<n>(t0, a, b, w);
+  __syncwarp();
+  getZ<n>(t0, a, b, C);
+  __syncwarp();
+  cz<n, Real, true>(S, C, out);  // z
 }
 
 // dynamic shared memory per warp, in units of Real, rounded up to a multiple of
@@ -177,8 +242,8 @@ __device__ __forceinline__ void colour_cell(int cidx, const KPT &p, int &ix, int
 
 template <int P, typename Real>
 struct WOcc {
-  static constexpr int min_blocks = (sizeof(Real) == 8) ? (P == 4 ? 4 : P >= 2 ? 5 : 6)
-                                                       : (P == 4 ? 6 : P == 3 ? 7 : 8);
+  static constexpr int min_blocks = (sizeof(Real) == 8) ? (P == 4 ? 3 : P == 3 ? 4 : P == 2 ? 5 : 6)
+                                                       : (P == 4 ? 5 : P == 3 ? 6 : P == 2 ? 7 : 8);
 };
 
 template <int P, typename Real, int GEOM>
@@ -189,16 +254,11 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   constexpr int MS = metric_stride(n), VS = velb_stride(n);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bars[kWarpsPerCTA];
-  __shared__ Real sS[n2], sDc[n2];
   const Tables<Real> &T = tab<Real>(P);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool has_vel = p.vel_kind != MPDG_VEL_NONE;
   const bool gvel = GEOM == GEOM_GENERAL && has_vel;
 
-  for (int t = threadIdx.x; t < n2; t += blockDim.x) {
-    sS[t] = T.S[t];
-    sDc[t] = T.Dc[t];
-  }
   if (lane == 0) mbar_init(&bars[warp], 1);
   fence_mbar_init();
   __syncthreads();
@@ -287,14 +347,17 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     if (has_next) gather(gnext, A, cmA);
 
     Real uq[n], gx[n], gy[n], gz[n];
-    w_to_qp<n>(T.S, sS, t0, lane_ok, i, j, u, uq);
-    w_grad_qp<n>(T.Dc, sDc, t0, lane_ok, i, j, uq, gx, gy, gz);
+    l_forward<n>(T.S, T.Dc, t0, t1, lane_ok, i, j, u, uq, gx, gy, gz);
 
     if (GEOM == GEOM_GENERAL) {
       mbar_wait_bounded(&bars[warp], phase, err);
       phase ^= 1;
     }
 
+    // velocity parts that do not vary along the lane's z column (uniform mesh)
+    Real uv0[3] = {0, 0, 0};
+    if (GEOM != GEOM_GENERAL && has_vel && p.vel_kind != MPDG_VEL_ROTATION)
+      uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, 0, uv0);
     Real val[n], fx[n], fy[n], fz[n];
     const Real *ms = stage + s_sub * MS + j * n + i;
     const Real *vs = vstage + s_sub * VS + j * n + i;
@@ -317,8 +380,8 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
       } else {
         const Real JxW = p.hvol * T.w[i] * T.w[j] * T.w[k];
         if (has_vel) {
-          Real uv[3];
-          uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, k, uv);
+          Real uv[3] = {uv0[0], uv0[1], uv0[2]};
+          if (p.vel_kind == MPDG_VEL_ROTATION) uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, k, uv);
           const Real cj = p.c_vel * JxW;
           b0 = cj * uv[0] * p.ih[0];
           b1 = cj * uv[1] * p.ih[1];
@@ -338,7 +401,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     }
 
     Real out[n];
-    w_from_qp<n>(T.S, sS, T.Dc, sDc, t0, t1, lane_ok, i, j, val, fx, fy, fz, out);
+    l_backward<n>(T.S, T.Dc, t0, t1, lane_ok, i, j, val, fx, fy, fz, out);
 
     if (active) {
 #pragma unroll

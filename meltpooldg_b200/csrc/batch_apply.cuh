@@ -12,9 +12,6 @@
 // warp_apply_kernel.
 #pragma once
 
-// per-degree offsets of the shared-memory copies of the S and Dc tables
-__host__ __device__ constexpr int batch_tab_off(int P) { return P == 1 ? 0 : P == 2 ? 4 : P == 3 ? 13 : 29; }
-constexpr int kBatchTabElems = 54;     // sum of (P+1)^2 for P = 1..4
 constexpr int kBatchTileElems = 256;   // max over P of 2 * cells_per_warp * (P+1)^3
 
 __device__ __forceinline__ int batch_find(const int *__restrict__ prefix, int n, int g)
@@ -31,8 +28,7 @@ __device__ __forceinline__ int batch_find(const int *__restrict__ prefix, int n,
 template <int P, typename Real>
 __device__ __forceinline__ void batch_cell(int colour, int local_group, const SlotInfo &I,
                                            const BatchSlotParams &Q, const Real *__restrict__ src,
-                                           Real *__restrict__ dst, const Real *sS, const Real *sDc,
-                                           Real *tiles, int lane)
+                                           Real *__restrict__ dst, Real *tiles, int lane)
 {
   constexpr int n = P + 1, n2 = n * n, n3 = n2 * n, CPW = WCfg<n>::cpw;
   static_assert(2 * CPW * n3 <= kBatchTileElems, "tile area");
@@ -67,8 +63,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Sl
     u[k] = (act && !masked) ? src[g0 + k * zs] : Real(0);
   }
   Real uq[n], gx[n], gy[n], gz[n];
-  w_to_qp<n>(T.S, sS, t0, lane_ok, i, j, u, uq);
-  w_grad_qp<n>(T.Dc, sDc, t0, lane_ok, i, j, uq, gx, gy, gz);
+  l_forward<n>(T.S, T.Dc, t0, t1, lane_ok, i, j, u, uq, gx, gy, gz);
   Real val[n], fx[n], fy[n], fz[n];
   const Real hvol = (Real)Q.hvol, ih = (Real)Q.ih, ih2 = (Real)Q.ih2;
   const Real c_mass = (Real)Q.c_mass, c_vel = (Real)Q.c_vel, c_diff = (Real)Q.c_diff;
@@ -91,7 +86,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Sl
     fz[k] = kd * gz[k];
   }
   Real out[n];
-  w_from_qp<n>(T.S, sS, T.Dc, sDc, t0, t1, lane_ok, i, j, val, fx, fy, fz, out);
+  l_backward<n>(T.S, T.Dc, t0, t1, lane_ok, i, j, val, fx, fy, fz, out);
   if (act) {
     const int nc = I.nc;
     const bool sx = (i == 0 && ix > 0) || (i == P && ix < nc - 1);
@@ -118,19 +113,9 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, 4)
                        Real *const *__restrict__ src_ptrs, Real *const *__restrict__ dst_ptrs,
                        const int *__restrict__ mask)
 {
-  __shared__ Real sS[kBatchTabElems], sDc[kBatchTabElems];
   __shared__ Real tiles_all[kWarpsPerCTA][kBatchTileElems];
   const int total = hdr->total_groups[colour], nseg = hdr->n_seg[colour];
   if (total == 0) return;
-  for (int P = 1; P <= kMaxDegree; ++P) {
-    const Tables<Real> &T = tab<Real>(P);
-    const int n2 = (P + 1) * (P + 1);
-    for (int t = threadIdx.x; t < n2; t += blockDim.x) {
-      sS[batch_tab_off(P) + t] = T.S[t];
-      sDc[batch_tab_off(P) + t] = T.Dc[t];
-    }
-  }
-  __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   Real *tiles = tiles_all[warp];
   for (int g = blockIdx.x * kWarpsPerCTA + warp; g < total; g += gridDim.x * kWarpsPerCTA) {
@@ -143,10 +128,10 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, 4)
     Real *dst = dst_ptrs[s];
     const int lg = g - seg_prefix[k];
     switch (I.degree) {
-      case 1: batch_cell<1, Real>(colour, lg, I, Q, src, dst, sS + batch_tab_off(1), sDc + batch_tab_off(1), tiles, lane); break;
-      case 2: batch_cell<2, Real>(colour, lg, I, Q, src, dst, sS + batch_tab_off(2), sDc + batch_tab_off(2), tiles, lane); break;
-      case 3: batch_cell<3, Real>(colour, lg, I, Q, src, dst, sS + batch_tab_off(3), sDc + batch_tab_off(3), tiles, lane); break;
-      default: batch_cell<4, Real>(colour, lg, I, Q, src, dst, sS + batch_tab_off(4), sDc + batch_tab_off(4), tiles, lane); break;
+      case 1: batch_cell<1, Real>(colour, lg, I, Q, src, dst, tiles, lane); break;
+      case 2: batch_cell<2, Real>(colour, lg, I, Q, src, dst, tiles, lane); break;
+      case 3: batch_cell<3, Real>(colour, lg, I, Q, src, dst, tiles, lane); break;
+      default: batch_cell<4, Real>(colour, lg, I, Q, src, dst, tiles, lane); break;
     }
   }
 }
