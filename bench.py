@@ -20,6 +20,16 @@ kernel; the solve is one time step of phi0 = tanh(d / 0.01),
 d = 0.25 - |x - (0.5, 0.75, 0.5)|, with GMRES(30) + Jacobi to 1e-10 in FP64 and
 in FP32-inner / FP64-defect-correction form.
 
+`--workload c1` (config 1): unit cube, 16^3 uniform cells, FE_Q(2) (35,937
+DoFs), heat operator M/dt + Laplace (k = 1, dt = 1e-3), Dirichlet faces; one
+vmult per step (launch-latency bound), then CG + Jacobi to 1e-10 with
+b = A x*, x* ~ U[-1, 1] (seed 1).
+
+`--workload batch` (config 4): 256 independent heat solves advanced together
+(see `batch_problems`); `--workload serve` (config 5): a Poisson request
+stream served by the library's continuous-batching loop (see
+`serve_requests`), each against the plain FP64 GPU form.
+
 `--impl reference` times the CPU restatement of the reference's operator
 (the reference itself needs deal.II/Trilinos/p4est/MPI, which this image does
 not have) on a bounded sample of the same workload with all host threads.
@@ -45,20 +55,33 @@ DT, K0, K_ALPHA = 1e-3, 1.0, 1e-3
 WORKLOAD = {"name": "heat"}
 THETA, DIFFUSIVITY = 0.5, 1e-3
 
-# dram__bytes_read.sum + dram__bytes_write.sum per apply of the FP64 cell kernel
-# (8 colour launches), from the ncu capture summarised in
-# profiles/heat_apply_q4_kT_fp64.md; None until a capture exists.
-MEASURED_TRAFFIC_BYTES = None
+# dram__bytes_read.sum + dram__bytes_write.sum of the FP64 warp apply kernel,
+# per apply (8 colour launches), heat workload at 64^3 cells: the 48^3 capture
+# of profiles/warp_apply_q4_general_48c.md (288.8 MB over two colour launches,
+# 1155 MB per apply of 110,592 cells) scaled by the cells of an apply
+# (262,144 / 110,592); traffic grows with the cells processed.
+MEASURED_TRAFFIC_BYTES = {("heat", 64): 2.738e9}
 
 
 def algorithmic_bytes(n_dofs, n_cells, degree, real_bytes):
-    """Bytes one apply must move: src read + dst write, plus, on the perturbed
-    (general) mesh, the merged coefficient stream (c_mass JxW and the 6 entries
-    of c_diff k(T_q) JxW J^-1 J^-T per quadrature point).  The uniform
-    advection-diffusion mesh has no coefficient stream (geometry and velocity
-    are computed in the kernel)."""
+    """Algorithmic bytes of one apply (the accounting of the hot-path scope
+    table): s (N_src + N_dst) + s N_aux + s G + 4 E, with N_aux = N (the
+    temperature read for k(T)) and G = 10 geometry values per quadrature point
+    (J^-T and JxW) on the perturbed heat mesh, and N_aux = G = 0 on the uniform
+    advection-diffusion mesh; 4 E = one cell index per cell."""
     nq = (degree + 1) ** 3
-    if WORKLOAD["name"] == "advdiff":
+    if WORKLOAD["name"] in ("advdiff", "c1"):
+        return real_bytes * 2 * n_dofs + 4 * n_cells
+    return real_bytes * (3 * n_dofs) + real_bytes * 10 * nq * n_cells + 4 * n_cells
+
+
+def streamed_bytes(n_dofs, n_cells, degree, real_bytes):
+    """Bytes this implementation must stream per apply: src read, dst write and,
+    on the perturbed mesh, the merged coefficient stream (c_mass JxW and the 6
+    entries of c_diff k(T_q) JxW J^-1 J^-T per quadrature point, which folds the
+    temperature and the geometry into 7 values)."""
+    nq = (degree + 1) ** 3
+    if WORKLOAD["name"] in ("advdiff", "c1"):
         return real_bytes * 2 * n_dofs
     return real_bytes * (2 * n_dofs) + real_bytes * 7 * nq * n_cells
 
@@ -86,7 +109,7 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                 stderr=subprocess.DEVNULL)
             # wait for the first sample so the timed region is covered
             t0 = time.time()
@@ -132,6 +155,10 @@ def build_problem():
         V = M.box_vertices(NC)
         mesh = M.Mesh(V, NC, DEGREE, None)
         return M, V, None, mesh, None
+    if WORKLOAD["name"] == "c1":
+        V = M.box_vertices(NC)
+        mask = M.boundary_mask(NC, DEGREE)
+        return M, V, mask, M.Mesh(V, NC, DEGREE, mask), None
     V = M.box_vertices(NC, perturb=0.1, seed=2)
     mask = M.boundary_mask(NC, DEGREE)
     mesh = M.Mesh(V, NC, DEGREE, mask)
@@ -144,6 +171,8 @@ def make_operator(M, mesh, T):
     if WORKLOAD["name"] == "advdiff":
         return M.AdvectionDiffusionOperator(mesh, DT, theta=THETA, diffusivity=DIFFUSIVITY,
                                             velocity="vortex", precisions=("fp64", "fp32")), None
+    if WORKLOAD["name"] == "c1":
+        return M.HeatDiffuseOperator(mesh, DT, rho_cp=1.0, k0=1.0, precisions=("fp64", "fp32")), None
     op = M.HeatDiffuseOperator(mesh, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA,
                                precisions=("fp64", "fp32"))
     Td = torch.tensor(T, device="cuda")
@@ -154,6 +183,8 @@ def make_operator(M, mesh, T):
 def oracle_operator(O, T, mask):
     if WORKLOAD["name"] == "advdiff":
         return O.Operator(O.ADVDIFF, DT, theta=THETA, diffusivity=DIFFUSIVITY, vel_kind=O.VEL_VORTEX)
+    if WORKLOAD["name"] == "c1":
+        return O.Operator(O.HEAT, DT, rho_cp=1.0, k0=1.0, dirichlet=mask)
     return O.Operator(O.HEAT, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA, temperature=T, dirichlet=mask)
 
 
@@ -161,6 +192,9 @@ def workload_config(N, E):
     if WORKLOAD["name"] == "advdiff":
         return {"workload": "advection-diffusion operator apply, Q2, 128^3 uniform hex cells, "
                             "vortex velocity, theta=0.5, D=1e-3",
+                "n_dofs": N, "cells": E, "degree": DEGREE}
+    if WORKLOAD["name"] == "c1":
+        return {"workload": "heat operator apply, Q2, 16^3 uniform hex cells, k=1, dt=1e-3, Dirichlet faces",
                 "n_dofs": N, "cells": E, "degree": DEGREE}
     return {"workload": "heat operator apply, Q4, 64^3 perturbed hex cells, k(T)=k0(1+1e-3T)",
             "n_dofs": N, "cells": E, "degree": DEGREE}
@@ -197,6 +231,8 @@ def run_reference(args, rank, world):
     n_dofs = int(np.prod([n * DEGREE + 1 for n in NC]))
     if WORKLOAD["name"] == "advdiff":
         V, mask, T = box_vertices(NC), None, None
+    elif WORKLOAD["name"] == "c1":
+        V, mask, T = box_vertices(NC), boundary_mask(NC, DEGREE), None
     else:
         V = box_vertices(NC, perturb=0.1, seed=2)
         mask = boundary_mask(NC, DEGREE)
@@ -298,17 +334,25 @@ def run_ours(args, rank, world):
 
     peak, peak_kind = load_peaks()
     E = int(np.prod(NC))
-    geom = "UNIFORM" if WORKLOAD["name"] == "advdiff" else "GENERAL"
+    geom = "UNIFORM" if WORKLOAD["name"] in ("advdiff", "c1") else "GENERAL"
     kernel_name = f"warp_apply_kernel<{DEGREE},double,{geom}> x 8 colour launches"
     b64 = algorithmic_bytes(N, E, DEGREE, 8)
     b32 = algorithmic_bytes(N, E, DEGREE, 4)
+    st64 = streamed_bytes(N, E, DEGREE, 8)
+    st32 = streamed_bytes(N, E, DEGREE, 4)
+    traffic = MEASURED_TRAFFIC_BYTES.get((WORKLOAD["name"], NC[0]))
     roof = {"bound": "hbm", "achieved": b64 / apply_s / 1e9, "peak": peak, "unit": "GB/s",
             "frac": b64 / apply_s / 1e9 / peak,
-            "traffic": MEASURED_TRAFFIC_BYTES,
+            "traffic": traffic,
+            "traffic_note": None if traffic is None else
+            "ncu dram read+write per apply (8 launches), 48^3 capture scaled by cells",
             "algorithmic_bytes": b64, "kernel": kernel_name,
             "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+            "streamed": {"bytes": st64, "achieved": st64 / apply_s / 1e9,
+                         "frac": st64 / apply_s / 1e9 / peak},
             "fp32": {"achieved": b32 / apply32_s / 1e9, "frac": b32 / apply32_s / 1e9 / peak,
-                     "algorithmic_bytes": b32}}
+                     "algorithmic_bytes": b32, "streamed_bytes": st32,
+                     "streamed_frac": st32 / apply32_s / 1e9 / peak}}
 
     # solves: CG + Chebyshev(5)/Jacobi to 1e-10, FP64 and FP32-inner/FP64-refined
     solves = None
@@ -324,11 +368,12 @@ def run_ours(args, rank, world):
             xs = None
             solver_type, prec = "GMRES", "Diagonal"
         else:
-            xs = torch.tensor(np.random.Generator(np.random.PCG64(5)).uniform(-1, 1, N), device="cuda")
+            seed = 1 if WORKLOAD["name"] == "c1" else 5
+            xs = torch.tensor(np.random.Generator(np.random.PCG64(seed)).uniform(-1, 1, N), device="cuda")
             xs[torch.tensor(mask.astype(bool), device="cuda")] = 0.0
             b = torch.empty_like(xs)
             op.vmult(b, xs)
-            solver_type, prec = "CG", "Chebyshev"
+            solver_type, prec = ("CG", "Diagonal") if WORKLOAD["name"] == "c1" else ("CG", "Chebyshev")
         solves = {"solver": f"{solver_type} + {prec}"}
         ref_x = None
         for form, mixed in (("fp64", False), ("fp32_refined", True)):
@@ -371,8 +416,9 @@ def run_ours(args, rank, world):
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(workload_config(N, E), parallelism=f"replicas x{world}",
-                           l2=("inputs larger than L2: src/dst 2 x 136 MB" if WORKLOAD["name"] == "advdiff"
-                               else "inputs larger than L2: coefficient stream 1.8 GB per apply")),
+                           l2={"advdiff": "inputs larger than L2: src/dst 2 x 136 MB",
+                               "c1": "inputs smaller than L2 (0.6 MB): launch-latency bound, L2 not flushed",
+                               }.get(WORKLOAD["name"], "inputs larger than L2: coefficient stream 1.8 GB per apply")),
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": None if args.no_e2e else {
@@ -503,7 +549,8 @@ def run_batch(args, rank, world):
     t64 = time.perf_counter() - t0
 
     peak, peak_kind = load_peaks()
-    b_apply = 2 * 4 * N_total  # FP32 src read + dst write of every problem
+    E_total = int(sum(p.nc ** 3 for p in probs))
+    b_apply = 2 * 4 * N_total + 4 * E_total  # FP32 src read + dst write and a cell index, every problem
     roof = {"bound": "hbm", "achieved": b_apply / (apply_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
             "frac": b_apply / (apply_ms * 1e-3) / 1e9 / peak, "traffic": None,
             "algorithmic_bytes": b_apply,
@@ -534,7 +581,7 @@ def run_batch(args, rank, world):
                            "speedup_batched_vs_fp64": value / (len(probs) / t64)},
             "batched": {"graph_steps": graph_steps[-1], "iterations_mean": float(np.mean(iters)),
                         "iterations_max": int(max(iters)),
-                        "all_converged": all(r["status"] == 0 for r in reps),
+            "all_converged": all(r["status"] == 0 for r in reps),
                         "max_rel_residual": max(r["final_residual"] / r["initial_residual"] for r in reps),
                         "max_rel_error_vs_fp64_solution": max(errs),
                         "iteration_diff_vs_fp64_max": int(max(abs(a - b) for a, b in zip(iters, its64)))},
@@ -572,6 +619,22 @@ def cpu_batch_rate(probs, its64, seconds):
     return {"value": rate, "unit": "solves/s", "cores": threads, "kind": "port",
             "sample": f"oracle CG+Jacobi of the {done} smallest problems ({spent:.1f} s), scaled by "
                       f"n_dofs x iterations to all {len(probs)}"}
+
+
+def serve_work(probs, reps, wall):
+    """Iterations per kind and the operator applies the stream needed:
+    DoF-applies = sum of n_dofs x applies (CG: 1 per iteration, BiCGStab: 2)."""
+    out = {}
+    total = 0.0
+    for kind, name in ((0, "heat"), (1, "advdiff")):
+        its = [r["iterations"] for p, r in zip(probs, reps) if p.kind == kind]
+        work = sum(p.n_dofs * r["operator_applies"] for p, r in zip(probs, reps) if p.kind == kind)
+        total += work
+        if its:
+            out[name] = {"requests": len(its), "iterations_mean": float(np.mean(its)),
+                         "iterations_max": int(max(its)), "dof_applies": float(work)}
+    out["dof_applies_per_s"] = total / wall
+    return out
 
 
 def run_serve(args, rank, world):
@@ -635,6 +698,8 @@ def run_serve(args, rank, world):
                        "timing": "host clock (request arrival to solution on the host)"},
             "latency": {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
                         "max_ms": 1e3 * float(lat[-1])},
+            "loop": out["stats"],
+            "work": serve_work(probs, reps, out["wall_s"]),
             "all_converged": all(r["status"] == 0 for r in reps),
             "max_rel_residual": max(r["final_residual"] / max(r["initial_residual"], 1e-300) for r in reps),
             "fp64_plain": fp64,
@@ -660,7 +725,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cells", type=int, default=0,
                     help="cells per direction (default: the workload's; smaller sizes for profiling)")
-    ap.add_argument("--workload", default="heat", choices=["heat", "advdiff", "batch", "serve"])
+    ap.add_argument("--workload", default="heat", choices=["heat", "advdiff", "c1", "batch", "serve"])
     ap.add_argument("--problems", type=int, default=BATCH_SIZE,
                     help="batch: problems in the batch (the first of the seeded sequence)")
     ap.add_argument("--requests", type=int, default=20000, help="serve: requests in the stream")
@@ -676,6 +741,9 @@ def main():
     if args.workload == "advdiff":
         DEGREE = 2
         NC[:] = [args.cells or 128] * 3
+    elif args.workload == "c1":
+        DEGREE = 2
+        NC[:] = [args.cells or 16] * 3
     else:
         NC[:] = [args.cells or 64] * 3
     world = int(os.environ.get("WORLD_SIZE", "1"))

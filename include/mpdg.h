@@ -271,6 +271,11 @@ mpdg_status mpdg_batch_take(mpdg_batch *batch, int64_t ticket, double *x_host, m
 mpdg_status mpdg_batch_autotune(mpdg_batch *batch, int *ctas_per_sm, double *apply_ms);
 /* device bytes admitted now */
 mpdg_status mpdg_batch_used_bytes(mpdg_batch *batch, int64_t *bytes);
+/* counters of the last mpdg_serve call (n <= 9 values): host seconds spent in
+ * admission, in result copies, waiting for the GPU and in graph launches;
+ * graph steps launched; requests admitted and finished; most problems
+ * resident at once; polls of the running flags */
+mpdg_status mpdg_batch_stats(mpdg_batch *batch, double *stats, int n);
 
 /* Serving loop: requests arrive at arrival_s[i] seconds after the call starts
  * (ascending).  Each arrived request is admitted as soon as its footprint fits

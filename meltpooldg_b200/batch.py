@@ -182,8 +182,13 @@ class Batch:
         check(lib().mpdg_serve(self._h, descs, arr.ctypes.data_as(dp), n, int(poll_steps), xptrs,
                                lat.ctypes.data_as(dp), xn.ctypes.data_as(dp), reps, C.byref(wall)),
               "mpdg_serve")
+        st = (C.c_double * 9)()
+        check(lib().mpdg_batch_stats(self._h, st, 9), "mpdg_batch_stats")
+        names = ("admit_s", "results_s", "wait_gpu_s", "launch_s", "graph_steps", "admitted", "finished",
+                 "max_resident", "polls")
         return {"latency_s": lat, "x_norm": xn, "reports": [reps[i].as_dict() for i in range(n)],
-                "wall_s": float(wall.value), "solutions": sols}
+                "wall_s": float(wall.value), "solutions": sols,
+                "stats": {k: float(v) for k, v in zip(names, st)}}
 
     def close(self):
         if getattr(self, "_h", None):

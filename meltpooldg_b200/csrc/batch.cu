@@ -102,6 +102,12 @@ struct Batch {
   int64_t step_kernels = 0;  // kernels of one graph step
   int tuned_cap = 0;         // resident CTAs per SM of the batched apply (0 = occupancy maximum)
   double tuned_ms = 0;
+  double *d_norms = nullptr;  // |x|^2 of finished slots (serving)
+  double *h_norms = nullptr;  // pinned
+  // serving counters: host seconds in admission, in result copies, waiting for
+  // the GPU, in graph launches; graph steps, admitted, finished, most slots
+  // resident at once, polls
+  double stats[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -825,9 +831,9 @@ namespace mpdg {
 namespace {
 
 // admission scratch layout (doubles): [0, R) reduction partials, [R] |b|^2,
-// [R+8, 2R+8) initialisation partials, [2R+16] |x|^2
+// [R+8, 2R+8) initialisation partials
 constexpr int kAdmDoubles = 2 * kRedBlocks + 32;
-constexpr int kAdmBB = kRedBlocks, kAdmInit = kRedBlocks + 8, kAdmNorm = 2 * kRedBlocks + 16;
+constexpr int kAdmBB = kRedBlocks, kAdmInit = kRedBlocks + 8;
 
 size_t slot_bytes(long N, int kind)
 {
@@ -929,12 +935,25 @@ void rhs_host(const mpdg_problem_desc &d, double *b)
 }
 
 
+// Slot vectors come from the batch's stream-ordered pool.  Freed blocks stay
+// in the pool for reuse; when a request of a new size does not fit the device
+// any more, the pool's unused blocks are returned (after the stream has
+// drained, so no freed block is still in use) and the allocation is retried.
 template <typename T>
 T *palloc(Batch &B, size_t n)
 {
   void *p = nullptr;
-  const cudaError_t e = cudaMallocFromPoolAsync(&p, n * sizeof(T), B.pool, B.stream);
-  if (e != cudaSuccess) throw Error{MPDG_ERR_ALLOC, std::string("device pool: ") + cudaGetErrorString(e)};
+  cudaError_t e = cudaMallocFromPoolAsync(&p, n * sizeof(T), B.pool, B.stream);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    MPDG_CUDA(cudaStreamSynchronize(B.stream));
+    MPDG_CUDA(cudaMemPoolTrimTo(B.pool, 0));
+    e = cudaMallocFromPoolAsync(&p, n * sizeof(T), B.pool, B.stream);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error{MPDG_ERR_ALLOC, std::string("device pool: ") + cudaGetErrorString(e)};
+  }
   return (T *)p;
 }
 
@@ -1001,7 +1020,7 @@ void drop_graph(Batch &B)
 }
 
 // one Krylov step of every running slot (the body of the graph)
-void enqueue_step(Batch &B, int blocks)
+void enqueue_step(Batch &B, int cap)
 {
   cudaStream_t st = B.stream;
   const int S = B.capacity;
@@ -1018,18 +1037,18 @@ void enqueue_step(Batch &B, int blocks)
   bk_schedule<<<9, kSchedThreads, 0, st>>>(B.d_active, MPDG_OP_ADVDIFF, T.info, S, SA);
   MPDG_LAUNCHED();
   // CG on the heat problems: Ap = A p (FP32), alpha, x/r/z update
-  launch_batch_apply<float>(SH, T.info, B.d_params, T.p, T.Ap, B.d_active, blocks, st);
+  launch_batch_apply<float>(SH, T.info, B.d_params, T.p, T.Ap, B.d_active, cap, st);
   BK(bk_dot_pap, gc, SH, T, B.d_active);
   BK(bk_finish_pap, gs, B.d_sc, B.d_active, T, S);
   BK(bk_cg_update, gc, SH, T, B.d_active, B.d_sc);
   BK(bk_cg_decide, gs, B.d_sc, B.d_active, B.d_defect, T, S, B.delta);
   // BiCGStab on the advection-diffusion problems: v = A M p, alpha, s, t = A M s, omega, update
   BK(bk_bicg_precond_p, gc, SA, T, B.d_active, B.d_sc);
-  launch_batch_apply<float>(SA, T.info, B.d_params, T.z, T.v, B.d_active, blocks, st);
+  launch_batch_apply<float>(SA, T.info, B.d_params, T.z, T.v, B.d_active, cap, st);
   BK(bk_bicg_alpha_partials, gc, SA, T, B.d_active, B.d_sc);
   BK(bk_bicg_alpha, gs, B.d_sc, B.d_active, T, S);
   BK(bk_bicg_s, gc, SA, T, B.d_active, B.d_sc);
-  launch_batch_apply<float>(SA, T.info, B.d_params, T.z, T.t, B.d_active, blocks, st);
+  launch_batch_apply<float>(SA, T.info, B.d_params, T.z, T.t, B.d_active, cap, st);
   BK(bk_bicg_omega_partials, gc, SA, T, B.d_active, B.d_sc);
   BK(bk_bicg_omega, gs, B.d_sc, B.d_active, T, S);
   BK(bk_bicg_update, gc, SA, T, B.d_active, B.d_sc);
@@ -1037,7 +1056,7 @@ void enqueue_step(Batch &B, int blocks)
   // FP64 defects b - A x of the slots whose FP32 residual dropped by delta (or that look converged)
   bk_schedule<<<9, kSchedThreads, 0, st>>>(B.d_defect, -1, T.info, S, SD);
   MPDG_LAUNCHED();
-  launch_batch_apply<double>(SD, T.info, B.d_params, T.x, T.r64, B.d_defect, blocks, st);
+  launch_batch_apply<double>(SD, T.info, B.d_params, T.x, T.r64, B.d_defect, cap, st);
   BK(bk_defect, gc, SD, T, B.d_defect);
   BK(bk_defect_decide, gs, B.d_sc, B.d_active, B.d_defect, T, S);
   BK(bk_cg_replace, gc, SD, T, B.d_defect, B.d_sc);
@@ -1058,12 +1077,12 @@ void enqueue_step(Batch &B, int blocks)
 void ensure_graph(Batch &B)
 {
   if (B.graph) return;
-  const int blocks = batch_apply_blocks(B.tuned_cap);  // set-up of the launchers outside the capture
+  batch_apply_setup();  // set-up of the launchers outside the capture
   const int64_t before = mpdg_kernel_launches();
   cudaGraph_t g = nullptr;
   MPDG_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
   try {
-    enqueue_step(B, blocks);
+    enqueue_step(B, B.tuned_cap);
   } catch (...) {
     cudaStreamEndCapture(B.stream, &g);
     if (g) cudaGraphDestroy(g);
@@ -1241,10 +1260,11 @@ void destroy_batch(Batch &B)
   for (void *p : {(void *)T.x, (void *)T.b, (void *)T.r64, (void *)T.r, (void *)T.z, (void *)T.p,
                   (void *)T.Ap, (void *)T.invd, (void *)T.rh, (void *)T.v, (void *)T.sv, (void *)T.t,
                   (void *)T.part, (void *)T.info, (void *)B.d_sc, (void *)B.d_params, (void *)B.d_active,
-                  (void *)B.d_defect, (void *)B.d_running, (void *)B.d_adm, (void *)B.d_res})
+                  (void *)B.d_defect, (void *)B.d_running, (void *)B.d_adm, (void *)B.d_res,
+                  (void *)B.d_norms})
     if (p) cudaFree(p);
   for (void *p : {(void *)B.h_running, (void *)B.h_active[0], (void *)B.h_active[1], (void *)B.h_sc,
-                  (void *)B.h_norm})
+                  (void *)B.h_norm, (void *)B.h_norms})
     if (p) cudaFreeHost(p);
   if (B.pool) cudaMemPoolDestroy(B.pool);
   if (B.stream) cudaStreamDestroy(B.stream);
@@ -1277,6 +1297,8 @@ void serve(Batch &B, const mpdg_problem_desc *req, const double *arr, int n, int
   };
   std::deque<Poll> pend;
   std::vector<int> slot_req(B.capacity, -1);
+  double *st = B.stats;
+  for (int k = 0; k < 9; ++k) st[k] = 0.0;
   int next = 0, done = 0, buf = 1;
   long seq = 0;
   const double t0 = now_s();
@@ -1286,21 +1308,34 @@ void serve(Batch &B, const mpdg_problem_desc *req, const double *arr, int n, int
     for (cudaEvent_t &e : ev) MPDG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     while (done < n) {
       const double t = now_s() - t0;
+      const double ta = now_s();
       while (next < n && arr[next] <= t) {
         int64_t tk = -1;
-        const int s = admit(B, req[next], nullptr, tk, ++seq);
+        int s = -1;
+        try {
+          s = admit(B, req[next], nullptr, tk, ++seq);
+        } catch (const Error &e) {
+          // the device itself is full (other users of the GPU): wait for running slots
+          if (e.status != MPDG_ERR_ALLOC || used_slots(B) == 0) throw;
+        }
         if (s < 0) break;  // waits for memory or a slot
         slot_req[s] = next;
         ++next;
+        st[5] += 1;
       }
+      st[0] += now_s() - ta;
       const int used = used_slots(B);
+      st[7] = std::max(st[7], (double)used);
       if (used > 0 && pend.size() < 2) {
+        const double tl = now_s();
         launch_steps(B, poll);
         buf ^= 1;
         MPDG_CUDA(cudaMemcpyAsync(B.h_active[buf], B.d_active, sizeof(int) * B.capacity, cudaMemcpyDeviceToHost,
                                   B.stream));
         MPDG_CUDA(cudaEventRecord(ev[buf], B.stream));
         pend.push_back({buf, ++seq});
+        st[3] += now_s() - tl;
+        st[4] += poll;
         if (pend.size() < 2) continue;
       }
       if (pend.empty()) {
@@ -1312,27 +1347,42 @@ void serve(Batch &B, const mpdg_problem_desc *req, const double *arr, int n, int
       }
       const Poll P = pend.front();
       pend.pop_front();
+      const double tw = now_s();
       MPDG_CUDA(cudaEventSynchronize(ev[P.buf]));
+      st[2] += now_s() - tw;
+      st[8] += 1;
       const int *act = B.h_active[P.buf];
+      // results of every slot that had finished by the snapshot: their data no
+      // longer changes, so the copies run on the copy stream beside the steps
+      const double tf = now_s();
+      std::vector<int> fin;
+      cudaStream_t cs = B.copy_stream;
       for (int s = 0; s < B.capacity; ++s) {
         BatchSlot &S = B.slots[s];
         if (!S.used || S.admit_seq >= P.seq || act[s]) continue;
         const int i = slot_req[s];
-        cudaStream_t cs = B.copy_stream;
-        dev_dot(S.v.x, S.v.x, S.N, B.d_res, B.d_res + kAdmNorm, cs);
-        MPDG_CUDA(cudaMemcpyAsync(B.h_norm, B.d_res + kAdmNorm, sizeof(double), cudaMemcpyDeviceToHost, cs));
+        fin.push_back(s);
+        dev_dot(S.v.x, S.v.x, S.N, B.d_res, B.d_norms + s, cs);
+        MPDG_CUDA(cudaMemcpyAsync(B.h_norms + s, B.d_norms + s, sizeof(double), cudaMemcpyDeviceToHost, cs));
         MPDG_CUDA(cudaMemcpyAsync(B.h_sc + s, B.d_sc + s, sizeof(SlotScalars), cudaMemcpyDeviceToHost, cs));
         double *dst = (x_host && x_host[i]) ? x_host[i] : staging;
         MPDG_CUDA(cudaMemcpyAsync(dst, S.v.x, sizeof(double) * S.N, cudaMemcpyDeviceToHost, cs));
+      }
+      if (!fin.empty()) {
         MPDG_CUDA(cudaStreamSynchronize(cs));
         t_last = now_s();
-        if (latency) latency[i] = (t_last - t0) - arr[i];
-        if (x_norm) x_norm[i] = std::sqrt(*B.h_norm);
-        if (reports) report_of(B.h_sc[s], reports[i]);
-        release(B, s);
-        slot_req[s] = -1;
-        ++done;
+        for (int s : fin) {
+          const int i = slot_req[s];
+          if (latency) latency[i] = (t_last - t0) - arr[i];
+          if (x_norm) x_norm[i] = std::sqrt(B.h_norms[s]);
+          if (reports) report_of(B.h_sc[s], reports[i]);
+          release(B, s);
+          slot_req[s] = -1;
+          ++done;
+        }
+        st[6] += (double)fin.size();
       }
+      st[1] += now_s() - tf;
     }
     MPDG_CUDA(cudaStreamSynchronize(B.stream));
   } catch (...) {
@@ -1380,7 +1430,8 @@ mpdg_status mpdg_batch_create(int64_t budget_bytes, int capacity, double reliabl
       props.location.type = cudaMemLocationTypeDevice;
       props.location.id = B.device;
       MPDG_CUDA(cudaMemPoolCreate(&B.pool, &props));
-      uint64_t keep = UINT64_MAX;
+      // blocks up to the budget stay reserved between releases and admissions
+      uint64_t keep = (uint64_t)budget_bytes;
       MPDG_CUDA(cudaMemPoolSetAttribute(B.pool, cudaMemPoolAttrReleaseThreshold, &keep));
       B.slots.resize(capacity);
       BatchTables &T = B.tab;
@@ -1405,6 +1456,7 @@ mpdg_status mpdg_batch_create(int64_t budget_bytes, int capacity, double reliabl
       B.d_running = balloc<int>(1);
       B.d_adm = balloc<double>(kAdmDoubles);
       B.d_res = balloc<double>(kAdmDoubles);
+      B.d_norms = balloc<double>(capacity);
       for (BatchSchedule &S : B.sched) alloc_schedule(S, capacity);
       MPDG_CUDA(cudaMemset(T.info, 0, sizeof(SlotInfo) * capacity));
       MPDG_CUDA(cudaMemset(B.d_sc, 0, sizeof(SlotScalars) * capacity));
@@ -1416,6 +1468,7 @@ mpdg_status mpdg_batch_create(int64_t budget_bytes, int capacity, double reliabl
         MPDG_CUDA(cudaHostAlloc((void **)&B.h_active[k], sizeof(int) * capacity, cudaHostAllocDefault));
       MPDG_CUDA(cudaHostAlloc((void **)&B.h_sc, sizeof(SlotScalars) * capacity, cudaHostAllocDefault));
       MPDG_CUDA(cudaHostAlloc((void **)&B.h_norm, sizeof(double), cudaHostAllocDefault));
+      MPDG_CUDA(cudaHostAlloc((void **)&B.h_norms, sizeof(double) * capacity, cudaHostAllocDefault));
       MPDG_CUDA(cudaDeviceSynchronize());
     } catch (...) {
       destroy_batch(B);
@@ -1557,12 +1610,11 @@ mpdg_status mpdg_batch_autotune(mpdg_batch *batch, int *ctas_per_sm, double *app
       MPDG_CUDA(cudaEventCreate(&e0));
       MPDG_CUDA(cudaEventCreate(&e1));
       for (int cap : {1, 2, 3, 4, 6, 8, 0}) {
-        const int blocks = batch_apply_blocks(cap);
-        launch_batch_apply<float>(SD, B.tab.info, B.d_params, B.tab.p, B.tab.Ap, d_all, blocks, B.stream);
+        launch_batch_apply<float>(SD, B.tab.info, B.d_params, B.tab.p, B.tab.Ap, d_all, cap, B.stream);
         MPDG_CUDA(cudaEventRecord(e0, B.stream));
         const int reps = 5;
         for (int r = 0; r < reps; ++r)
-          launch_batch_apply<float>(SD, B.tab.info, B.d_params, B.tab.p, B.tab.Ap, d_all, blocks, B.stream);
+          launch_batch_apply<float>(SD, B.tab.info, B.d_params, B.tab.p, B.tab.Ap, d_all, cap, B.stream);
         MPDG_CUDA(cudaEventRecord(e1, B.stream));
         MPDG_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -1597,6 +1649,13 @@ mpdg_status mpdg_batch_used_bytes(mpdg_batch *batch, int64_t *bytes)
 {
   if (!batch || !bytes) return MPDG_ERR_ARG;
   *bytes = batch->b.used;
+  return MPDG_OK;
+}
+
+mpdg_status mpdg_batch_stats(mpdg_batch *batch, double *stats, int n)
+{
+  if (!batch || !stats || n < 0) return MPDG_ERR_ARG;
+  for (int k = 0; k < n && k < 9; ++k) stats[k] = batch->b.stats[k];
   return MPDG_OK;
 }
 

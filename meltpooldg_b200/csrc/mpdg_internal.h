@@ -156,12 +156,13 @@ struct BatchSchedule {
 
 // cells per warp of the warp-per-cell kernels for degree p (32 / (p+1)^2)
 int cells_per_warp(int degree);
-// persistent grid of the batched apply: SMs x min(cap, occupancy) (cap 0: occupancy)
-int batch_apply_blocks(int ctas_per_sm_cap);
-// one launch per colour over the scheduled slots whose mask entry is set
+// one-time set-up of the batched apply (tables, occupancy): before any graph capture
+void batch_apply_setup();
+// one launch per colour over the scheduled slots whose mask entry is set; persistent
+// grid of SMs x min(cap, occupancy) CTAs (cap 0: the occupancy maximum)
 template <typename Real>
 void launch_batch_apply(const BatchSchedule &sched, const SlotInfo *info, const BatchSlotParams *params,
-                        Real *const *src, Real *const *dst, const int *mask, int blocks, cudaStream_t s);
+                        Real *const *src, Real *const *dst, const int *mask, int cap, cudaStream_t s);
 
 // ---- operator kernels (operator_kernels.cu)
 // 1D tables of degree p on [0,1]: GLL Lagrange basis values S[q*(p+1)+i] and

@@ -1540,17 +1540,18 @@ int batch_occupancy()
 }
 }  // namespace
 
-int batch_apply_blocks(int cap)
+void batch_apply_setup()
 {
-  const int occ = std::min(batch_occupancy<float>(), batch_occupancy<double>());
-  return num_sms() * ((cap > 0) ? std::min(cap, occ) : occ);
+  batch_occupancy<float>();
+  batch_occupancy<double>();
 }
 
 template <typename Real>
 void launch_batch_apply(const BatchSchedule &sched, const SlotInfo *info, const BatchSlotParams *params,
-                        Real *const *src, Real *const *dst, const int *mask, int blocks, cudaStream_t s)
+                        Real *const *src, Real *const *dst, const int *mask, int cap, cudaStream_t s)
 {
-  batch_occupancy<Real>();  // tables uploaded before any launch (and before graph capture)
+  const int occ = batch_occupancy<Real>();  // tables uploaded before any launch (and before graph capture)
+  const int blocks = num_sms() * ((cap > 0) ? std::min(cap, occ) : occ);
   for (int c = 0; c < 8; ++c) {
     batch_apply_kernel<Real><<<(unsigned)blocks, kWarpsPerCTA * 32, 0, s>>>(
         c, sched.hdr, sched.seg_slot + (size_t)c * sched.cap, sched.seg_prefix + (size_t)c * sched.cap, info,
