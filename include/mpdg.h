@@ -78,6 +78,11 @@ typedef struct {
   int vel_kind;
   double vel_param[3];
   int precision_mask;       /* bit MPDG_FP64 / bit MPDG_FP32: forms to prepare (0 = FP64) */
+  /* heat: convective (Robin) faces, heat_diffuse_operator.cpp:1088-1129: tangent alpha u v,
+   * residual -alpha (T - t_inf) v on the box faces with bit 2*direction + side set
+   * (side 0: the low face, 1: the high face); 0 = none */
+  double robin_alpha, robin_t_inf;
+  int robin_faces;
 } mpdg_op_desc;
 
 typedef struct {

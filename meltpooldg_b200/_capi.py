@@ -49,7 +49,8 @@ class OpDesc(C.Structure):
     _fields_ = [("kind", C.c_int), ("dt", C.c_double), ("rho_cp", C.c_double), ("k0", C.c_double),
                 ("k_alpha", C.c_double), ("full_tangent", C.c_int), ("theta", C.c_double),
                 ("diffusivity", C.c_double), ("vel_kind", C.c_int), ("vel_param", C.c_double * 3),
-                ("precision_mask", C.c_int)]
+                ("precision_mask", C.c_int), ("robin_alpha", C.c_double),
+                ("robin_t_inf", C.c_double), ("robin_faces", C.c_int)]
 
 
 class SolverDesc(C.Structure):

@@ -1283,6 +1283,149 @@ void ensure_coef(Op &op, bool want32)
 
 }  // namespace
 
+// ---------------------------------------------------------- Robin boundary faces
+// Heat operator faces with a convective condition (heat_diffuse_operator.cpp:1088-1129):
+// tangent alpha u v, residual -alpha (T - T_inf) v, on the box faces flagged in
+// robin_faces (bit 2 d + s: direction d, side s).  One warp per face; lane
+// (a, b) owns the face DoF at tangential positions (a, b) and the face
+// quadrature point (q_a, q_b) = (a, b) of QGauss(p+1)^2 with the surface element
+// |dx/dxi_t0 x dx/dxi_t1| of the trilinear map.  The 2D face mass is sum
+// factorised through a per-warp shared tile.  Faces of one plane run in four
+// parity colours, so the scatter adds without atomics.
+enum { ROBIN_APPLY = 0, ROBIN_RESIDUAL = 1, ROBIN_DIAGONAL = 2 };
+
+template <int P, typename Real>
+__global__ void __launch_bounds__(128) robin_kernel(const double *vert, int nc0, int nc1, int nc2, int d, int s,
+                                                    int colour, long NX, long NY, double alpha, double t_inf,
+                                                    int mode, const Real *src, Real *dst,
+                                                    const uint8_t *rmask, const uint8_t *wmask)
+{
+  constexpr int n = P + 1, n2 = n * n;
+  __shared__ Real tile[4][n2];
+  const Tables<Real> &T = tab<Real>(P);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nc[3] = {nc0, nc1, nc2};
+  const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
+  const int pa = colour & 1, pb = (colour >> 1) & 1;
+  const int ca = (nc[t0] - pa + 1) / 2, cb = (nc[t1] - pb + 1) / 2;
+  const long f = (long)blockIdx.x * 4 + warp;
+  if (f >= (long)ca * cb) return;  // warp-uniform
+  const int fa = 2 * (int)(f % ca) + pa, fb = 2 * (int)(f / ca) + pb;
+  int cell[3];
+  cell[d] = s ? nc[d] - 1 : 0;
+  cell[t0] = fa;
+  cell[t1] = fb;
+  const bool on = lane < n2;
+  const int a = on ? lane % n : 0, b = on ? lane / n : 0;
+  int loc[3];
+  loc[d] = s ? P : 0;
+  loc[t0] = a;
+  loc[t1] = b;
+  const long g = ((long)(cell[2] * P + loc[2]) * NY + (cell[1] * P + loc[1])) * NX + (cell[0] * P + loc[0]);
+  // surface element at the lane's face quadrature point
+  double xi[3];
+  xi[d] = s ? 1.0 : 0.0;
+  xi[t0] = (double)T.x[a];
+  xi[t1] = (double)T.x[b];
+  double Ja[3] = {0, 0, 0}, Jb[3] = {0, 0, 0};
+  for (int v = 0; v < 8; ++v) {
+    const int bv[3] = {v & 1, (v >> 1) & 1, (v >> 2) & 1};
+    const long vid = ((long)(cell[2] + bv[2]) * (nc1 + 1) + (cell[1] + bv[1])) * (nc0 + 1) + (cell[0] + bv[0]);
+    double fv[3], dfv[3];
+    for (int e = 0; e < 3; ++e) {
+      fv[e] = bv[e] ? xi[e] : 1.0 - xi[e];
+      dfv[e] = bv[e] ? 1.0 : -1.0;
+    }
+    double da = dfv[t0], db = dfv[t1];
+    for (int e = 0; e < 3; ++e)
+      if (e != t0) da *= fv[e];
+    for (int e = 0; e < 3; ++e)
+      if (e != t1) db *= fv[e];
+    for (int e = 0; e < 3; ++e) {
+      Ja[e] += vert[vid * 3 + e] * da;
+      Jb[e] += vert[vid * 3 + e] * db;
+    }
+  }
+  const double cr[3] = {Ja[1] * Jb[2] - Ja[2] * Jb[1], Ja[2] * Jb[0] - Ja[0] * Jb[2],
+                        Ja[0] * Jb[1] - Ja[1] * Jb[0]};
+  const double jxw = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) * (double)T.w[a] * (double)T.w[b];
+  Real *t = tile[warp];
+  Real out;
+  if (mode == ROBIN_DIAGONAL) {
+    if (on) t[b * n + a] = (Real)(alpha * jxw);
+    __syncwarp();
+    out = 0;
+    for (int qb = 0; qb < n; ++qb)
+      for (int qa = 0; qa < n; ++qa) {
+        const Real sa = T.S[qa * n + a], sb = T.S[qb * n + b];
+        out += sa * sa * sb * sb * t[qb * n + qa];
+      }
+  } else {
+    Real u = 0;
+    if (on) {
+      if (mode == ROBIN_RESIDUAL) u = (Real)t_inf - src[g];
+      else u = (rmask && rmask[g]) ? Real(0) : src[g];
+    }
+    // values at the face quadrature points: along t0, then t1
+    if (on) t[b * n + a] = u;
+    __syncwarp();
+    Real w = 0;
+    for (int r = 0; r < n; ++r) w += T.S[a * n + r] * t[b * n + r];
+    __syncwarp();
+    if (on) t[b * n + a] = w;
+    __syncwarp();
+    Real uq = 0;
+    for (int r = 0; r < n; ++r) uq += T.S[b * n + r] * t[r * n + a];
+    __syncwarp();
+    // tested with the face shape functions: transposed passes
+    if (on) t[b * n + a] = (Real)(alpha * jxw) * uq;
+    __syncwarp();
+    w = 0;
+    for (int r = 0; r < n; ++r) w += T.S[r * n + a] * t[b * n + r];
+    __syncwarp();
+    if (on) t[b * n + a] = w;
+    __syncwarp();
+    out = 0;
+    for (int r = 0; r < n; ++r) out += T.S[r * n + b] * t[r * n + a];
+  }
+  if (on && !(wmask && wmask[g])) dst[g] += out;
+}
+
+template <typename Real>
+void launch_robin(Op &op, Real *dst, const Real *src, int mode)
+{
+  const mpdg_op_desc &D = op.d;
+  if (D.kind != MPDG_OP_HEAT || !D.robin_faces || D.robin_alpha == 0.0) return;
+  Mesh &m = *op.mesh;
+  upload_tables();
+  const bool mask = op.use_dirichlet && m.has_dirichlet;
+  const uint8_t *rmask = (mode == ROBIN_APPLY && mask) ? m.d_dmask : nullptr;
+  const uint8_t *wmask = mask ? m.d_dmask : nullptr;
+  for (int d = 0; d < 3; ++d)
+    for (int s = 0; s < 2; ++s) {
+      if (!(D.robin_faces & (1 << (2 * d + s)))) continue;
+      const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
+      for (int c = 0; c < 4; ++c) {
+        const long ca = (m.nc[t0] - (c & 1) + 1) / 2, cb = (m.nc[t1] - ((c >> 1) & 1) + 1) / 2;
+        const long faces = ca * cb;
+        if (faces == 0) continue;
+        const unsigned grid = (unsigned)((faces + 3) / 4);
+#define MPDG_ROBIN(PP)                                                                                   \
+  robin_kernel<PP, Real><<<grid, 128, 0, op.stream>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], d, s, c, m.NX, \
+                                                      m.NY, D.robin_alpha, D.robin_t_inf, mode, src, dst, \
+                                                      rmask, wmask)
+        switch (m.degree) {
+          case 1: MPDG_ROBIN(1); break;
+          case 2: MPDG_ROBIN(2); break;
+          case 3: MPDG_ROBIN(3); break;
+          default: MPDG_ROBIN(4); break;
+        }
+#undef MPDG_ROBIN
+        MPDG_LAUNCHED();
+      }
+    }
+}
+
 void invalidate_coef(Op &op)
 {
   op.coef64_ok = false;
@@ -1290,7 +1433,17 @@ void invalidate_coef(Op &op)
 }
 
 template <typename Real>
+void launch_cells(Op &op, Real *dst, const Real *src);
+
+template <typename Real>
 void launch_apply(Op &op, Real *dst, const Real *src)
+{
+  launch_cells<Real>(op, dst, src);
+  launch_robin<Real>(op, dst, src, ROBIN_APPLY);
+}
+
+template <typename Real>
+void launch_cells(Op &op, Real *dst, const Real *src)
 {
   Mesh &m = *op.mesh;
   const bool kt = uses_kT(op);
@@ -1336,6 +1489,7 @@ void launch_rhs(Op &op, double *dst, const double *src, const double *heat_sourc
     if (!op.T64) throw Error{MPDG_ERR_ARG, "heat residual needs the temperature field"};
     k.q_src = heat_source;
     dispatch_degree<double, MODE_HEAT_RESIDUAL, false>(op, k);
+    launch_robin<double>(op, dst, op.T64, ROBIN_RESIDUAL);
   } else {
     if (heat_source) throw Error{MPDG_ERR_ARG, "advection-diffusion rhs takes no heat source"};
     // phi_old/dt N - (1-theta) vel.grad phi_old N - (1-theta) D grad phi_old . grad N
@@ -1382,6 +1536,7 @@ void launch_diagonal(Op &op, double *diag)
     case 4: kt ? run_diag<4, true>(op, k) : run_diag<4, false>(op, k); break;
     default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
   }
+  launch_robin<double>(op, diag, nullptr, ROBIN_DIAGONAL);
   if (op.use_dirichlet && m.has_dirichlet) {
     set_masked_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, m.d_dmask, 1.0);
     MPDG_LAUNCHED();

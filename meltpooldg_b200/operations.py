@@ -71,10 +71,12 @@ class HeatDiffuseOperation:
 
     def __init__(self, mesh, dt, rho_cp=1.0, k0=1.0, k_alpha=0.0, full_tangent=False,
                  linear_solver: LinearSolverData = None, residual_tolerance=1e-9,
-                 field_correction_tolerance=1e-10, max_nonlinear_iterations=10, device="cuda"):
+                 field_correction_tolerance=1e-10, max_nonlinear_iterations=10, device="cuda",
+                 robin_alpha=0.0, robin_t_inf=0.0, robin_faces=()):
         self.mesh = mesh
         self.op = HeatDiffuseOperator(mesh, dt, rho_cp=rho_cp, k0=k0, k_alpha=k_alpha,
-                                      full_tangent=full_tangent)
+                                      full_tangent=full_tangent, robin_alpha=robin_alpha,
+                                      robin_t_inf=robin_t_inf, robin_faces=robin_faces)
         self.data = linear_solver or LinearSolverData(solver_type="GMRES", preconditioner_type="Diagonal")
         self.res_tol = residual_tolerance
         self.dx_tol = field_correction_tolerance

@@ -190,13 +190,20 @@ class HeatDiffuseOperator(_MatrixFreeOperator):
     """Tangent and residual of the heat equation
     (HeatDiffuseMultiPhaseOperator, source/heat/heat_diffuse_operator.cpp):
     v = rho_cp/dt u + rho_cp vel.grad u, g = k(T) grad u, k(T) = k0 (1 + k_alpha T).
-    `full_tangent` adds the Newton term dk/dT grad(T) u (non-symmetric)."""
+    `full_tangent` adds the Newton term dk/dT grad(T) u (non-symmetric).
+    `robin_faces` lists the box faces (direction, side) with the convective
+    condition of heat_diffuse_operator.cpp:1088-1129 (tangent alpha u v,
+    residual -alpha (T - t_inf) v)."""
 
     def __init__(self, mesh, dt, rho_cp=1.0, k0=1.0, k_alpha=0.0, full_tangent=False,
-                 velocity=None, precisions=("fp64",)):
+                 velocity=None, precisions=("fp64",), robin_alpha=0.0, robin_t_inf=0.0,
+                 robin_faces=()):
         vk, vp = _velocity(velocity)
         d = A.OpDesc(A.OP_HEAT, dt, rho_cp, k0, k_alpha, int(full_tangent), 0.0, 0.0, vk,
                      (C.c_double * 3)(*vp), 0)
+        d.robin_alpha = float(robin_alpha)
+        d.robin_t_inf = float(robin_t_inf)
+        d.robin_faces = sum(1 << (2 * int(dd) + int(ss)) for dd, ss in robin_faces)
         super().__init__(mesh, d, precisions)
 
     def set_temperature(self, T):

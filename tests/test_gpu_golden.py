@@ -45,3 +45,23 @@ def test_unidirectional_heat_golden_on_gpu(cuda):
         opn.solve()
         got.append("%.5e" % opn.l2_norm())
     assert got == GOLDEN["unidirectional_heat_transfer"]["printed"]
+
+
+def test_unidirectional_heat_convection_golden_on_gpu(cuda):
+    """unidirectional_heat_transfer_with_convection (2D Q1 32^2, Robin face at
+    x = 0.1 with alpha = 25, T_inf = 300, steel properties, dt = 0.01) extruded
+    to one layer of unit depth: the Robin face terms run on the device."""
+    import meltpooldg_b200 as M
+    from meltpooldg_b200.operations import HeatDiffuseOperation
+    nc = (32, 32, 1)
+    V = M.box_vertices(nc, (0.0, 0.0, 0.0), (0.1, 0.1, 1.0))
+    mesh = M.Mesh(V, nc, 1)
+    opn = HeatDiffuseOperation(mesh, 0.01, rho_cp=7850.0 * 460.0, k0=55.563, residual_tolerance=5e-9,
+                               linear_solver=M.LinearSolverData(rel_tolerance=1e-12),
+                               robin_alpha=25.0, robin_t_inf=300.0, robin_faces=[(0, 1)])
+    opn.set_initial_condition(np.full(mesh.n_dofs, 1000.0))
+    got = []
+    for _ in range(5):
+        opn.solve()
+        got.append("%.5e" % opn.l2_norm())
+    assert got == GOLDEN["unidirectional_heat_transfer_with_convection"]["printed"]
