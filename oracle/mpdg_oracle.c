@@ -1104,3 +1104,195 @@ double orc_estimate_lambda_max(const orc_mesh *m, const orc_op *op, const double
   free(Ap);
   return hi;
 }
+
+
+/* ============================================================ hanging nodes
+ * Two-level meshes (see mpdg_oracle.h).  Brute force: per cell the element
+ * matrix A_K (element_matrix) and the local-to-global constraint weights C_K;
+ * dst += C_K^T A_K C_K src.  deal.II applies the same constraints inside
+ * FEEvaluation::read_dof_values / distribute_local_to_global for meshes with
+ * hanging nodes (refinement 2:1). */
+
+void orc2_hanging_matrix(int degree, double *P)
+{
+  const int n = degree + 1;
+  double z[MAXN], xs[MAXN], S[MAXN * MAXN], D[MAXN * MAXN];
+  orc_gauss_lobatto(n, z);
+  for (int s = 0; s < 2; ++s) {
+    for (int j = 0; j < n; ++j) xs[j] = 0.5 * (s + z[j]);
+    orc_shape_tables(n, xs, n, S, D);
+    for (int j = 0; j < n; ++j)
+      for (int jp = 0; jp < n; ++jp) P[(s * n + j) * n + jp] = S[j * n + jp];
+  }
+}
+
+long orc2_n_dofs(const orc_mesh2 *m) { return orc_n_dofs(&m->coarse) + orc_n_dofs(&m->fine); }
+
+/* constraint weights of the local DoFs of a cell: up to n^2 (global, weight) each */
+typedef struct {
+  int cnt[MAXN3];
+  long g[MAXN3][MAXN * MAXN];
+  double w[MAXN3][MAXN * MAXN];
+} cmap_t;
+
+static void cell_cmap(const geo_t *gc, const geo_t *gf, int fine, int ix, int iy, int iz, const double *P,
+                      cmap_t *cm)
+{
+  const int n = gf->n, p = gf->p;
+  const long Nc = gc->N;
+  const geo_t *g = fine ? gf : gc;
+  long idx[MAXN3];
+  cell_dofs(g, ix, iy, iz, idx);
+  for (int t = 0; t < n * n * n; ++t) {
+    const int i = t % n, j = (t / n) % n, k = t / (n * n);
+    if (fine && ix == 0 && i == 0) {
+      const int cy = iy / 2, sy = iy % 2, cz = iz / 2, sz = iz % 2;
+      int c = 0;
+      for (int kp = 0; kp < n; ++kp)
+        for (int jp = 0; jp < n; ++jp) {
+          cm->g[t][c] = ((long)(cz * p + kp) * gc->NY + (cy * p + jp)) * gc->NX + (gc->NX - 1);
+          cm->w[t][c] = P[(sy * n + j) * n + jp] * P[(sz * n + k) * n + kp];
+          ++c;
+        }
+      cm->cnt[t] = c;
+    } else {
+      cm->cnt[t] = 1;
+      cm->g[t][0] = (fine ? Nc : 0) + idx[t];
+      cm->w[t][0] = 1.0;
+    }
+  }
+}
+
+static int hanging_slot(const geo_t *gc, const geo_t *gf, long gidx)
+{
+  if (gidx < gc->N) return 0;
+  return ((gidx - gc->N) % gf->NX) == 0;
+}
+
+static void orc2_check(const orc_mesh2 *m, const orc_op *op)
+{
+  if (m->coarse.dim != 3 || m->fine.dim != 3 || m->coarse.degree != m->fine.degree ||
+      m->fine.nc[1] != 2 * m->coarse.nc[1] || m->fine.nc[2] != 2 * m->coarse.nc[2] ||
+      op->temperature || op->robin_faces || op->vel_kind == ORC_VEL_NODAL || op->full_tangent) {
+    fprintf(stderr, "orc2: unsupported two-level configuration\n");
+    abort();
+  }
+}
+
+void orc2_vmult(const orc_mesh2 *m, const orc_op *op, double *dst, const double *src)
+{
+  orc2_check(m, op);
+  geo_t gc, gf;
+  geo_init(&m->coarse, &gc);
+  geo_init(&m->fine, &gf);
+  const int n = gc.n, nqt = n * n * n;
+  double P[2 * MAXN * MAXN];
+  orc2_hanging_matrix(gc.p, P);
+  const long N = gc.N + gf.N;
+  memset(dst, 0, sizeof(double) * N);
+  double *A = (double *)malloc(sizeof(double) * nqt * nqt);
+  cmap_t *cm = (cmap_t *)malloc(sizeof(cmap_t));
+  for (int fine = 0; fine < 2; ++fine) {
+    const geo_t *g = fine ? &gf : &gc;
+    const orc_mesh *mm = fine ? &m->fine : &m->coarse;
+    for (int iz = 0; iz < g->nc[2]; ++iz)
+      for (int iy = 0; iy < g->nc[1]; ++iy)
+        for (int ix = 0; ix < g->nc[0]; ++ix) {
+          long idx[MAXN3];
+          cell_dofs(g, ix, iy, iz, idx);
+          element_matrix(mm, op, g, ix, iy, iz, idx, A);
+          cell_cmap(&gc, &gf, fine, ix, iy, iz, P, cm);
+          double ul[MAXN3];
+          for (int t = 0; t < nqt; ++t) {
+            double v = 0.0;
+            for (int c = 0; c < cm->cnt[t]; ++c) {
+              const long gg = cm->g[t][c];
+              if (!(op->dirichlet && op->dirichlet[gg])) v += cm->w[t][c] * src[gg];
+            }
+            ul[t] = v;
+          }
+          for (int t = 0; t < nqt; ++t) {
+            double o = 0.0;
+            for (int u = 0; u < nqt; ++u) o += A[t * nqt + u] * ul[u];
+            for (int c = 0; c < cm->cnt[t]; ++c) {
+              const long gg = cm->g[t][c];
+              if (!(op->dirichlet && op->dirichlet[gg]) && !hanging_slot(&gc, &gf, gg))
+                dst[gg] += cm->w[t][c] * o;
+            }
+          }
+        }
+  }
+  free(A);
+  free(cm);
+}
+
+void orc2_diagonal(const orc_mesh2 *m, const orc_op *op, double *diag)
+{
+  orc2_check(m, op);
+  geo_t gc, gf;
+  geo_init(&m->coarse, &gc);
+  geo_init(&m->fine, &gf);
+  const int n = gc.n, nqt = n * n * n;
+  double P[2 * MAXN * MAXN];
+  orc2_hanging_matrix(gc.p, P);
+  const long N = gc.N + gf.N;
+  memset(diag, 0, sizeof(double) * N);
+  double *A = (double *)malloc(sizeof(double) * nqt * nqt);
+  cmap_t *cm = (cmap_t *)malloc(sizeof(cmap_t));
+  for (int fine = 0; fine < 2; ++fine) {
+    const geo_t *g = fine ? &gf : &gc;
+    const orc_mesh *mm = fine ? &m->fine : &m->coarse;
+    for (int iz = 0; iz < g->nc[2]; ++iz)
+      for (int iy = 0; iy < g->nc[1]; ++iy)
+        for (int ix = 0; ix < g->nc[0]; ++ix) {
+          long idx[MAXN3];
+          cell_dofs(g, ix, iy, iz, idx);
+          element_matrix(mm, op, g, ix, iy, iz, idx, A);
+          cell_cmap(&gc, &gf, fine, ix, iy, iz, P, cm);
+          /* (C^T A C)_{gg} = sum_{t,u} w_t(g) A_tu w_u(g) */
+          for (int t = 0; t < nqt; ++t)
+            for (int c = 0; c < cm->cnt[t]; ++c) {
+              const long gg = cm->g[t][c];
+              if (hanging_slot(&gc, &gf, gg)) continue;
+              double s = 0.0;
+              for (int u = 0; u < nqt; ++u)
+                for (int d = 0; d < cm->cnt[u]; ++d)
+                  if (cm->g[u][d] == gg) s += A[t * nqt + u] * cm->w[u][d];
+              diag[gg] += cm->w[t][c] * s;
+            }
+        }
+  }
+  for (long i = 0; i < N; ++i)
+    if ((op->dirichlet && op->dirichlet[i]) || hanging_slot(&gc, &gf, i)) diag[i] = 1.0;
+  free(A);
+  free(cm);
+}
+
+void orc2_distribute(const orc_mesh2 *m, double *u)
+{
+  geo_t gc, gf;
+  geo_init(&m->coarse, &gc);
+  geo_init(&m->fine, &gf);
+  const int n = gc.n, p = gc.p;
+  double P[2 * MAXN * MAXN];
+  orc2_hanging_matrix(p, P);
+  for (long Z = 0; Z < gf.NZ; ++Z)
+    for (long Y = 0; Y < gf.NY; ++Y) {
+      /* the fine cell (iy, iz) containing the node, any of them (continuous trace) */
+      const int iy = (int)((Y == gf.NY - 1) ? gf.nc[1] - 1 : Y / p), j = (int)(Y - (long)iy * p);
+      const int iz = (int)((Z == gf.NZ - 1) ? gf.nc[2] - 1 : Z / p), k = (int)(Z - (long)iz * p);
+      const int cy = iy / 2, sy = iy % 2, cz = iz / 2, sz = iz % 2;
+      double v = 0.0;
+      for (int kp = 0; kp < n; ++kp)
+        for (int jp = 0; jp < n; ++jp)
+          v += P[(sy * n + j) * n + jp] * P[(sz * n + k) * n + kp] *
+               u[((long)(cz * p + kp) * gc.NY + (cy * p + jp)) * gc.NX + (gc.NX - 1)];
+      u[gc.N + (Z * gf.NY + Y) * gf.NX] = v;
+    }
+}
+
+void orc2_dof_coordinates(const orc_mesh2 *m, double *xyz)
+{
+  orc_dof_coordinates(&m->coarse, xyz);
+  orc_dof_coordinates(&m->fine, xyz + 3 * orc_n_dofs(&m->coarse));
+}

@@ -107,6 +107,33 @@ double orc_estimate_lambda_max(const orc_mesh *m, const orc_op *op, const double
 void orc_prec_apply(const orc_mesh *m, const orc_op *op, const orc_prec *P, double *z,
                     const double *r);
 
+/* ------------------------------------------------------------ hanging nodes
+ * Two-level mesh: a coarse block and a fine block refined 2:1 in y and z,
+ * meeting at the plane normal to x where the coarse block ends (coarse cells
+ * ix = nc[0]-1, fine cells ix = 0).  fine.nc[1] = 2 coarse.nc[1], fine.nc[2] =
+ * 2 coarse.nc[2]; the fine interface vertices lie on the coarse faces.
+ * Global vector: the coarse block's DoFs (lexicographic), then the fine
+ * block's (lexicographic, all of its lattice).  The fine DoFs on the interface
+ * plane hang on the coarse face (deal.II hanging-node constraints of a 2:1
+ * refined face): the value of fine DoF (j, k) of subface (sy, sz) is the coarse
+ * face interpolant  sum_{j',k'} P[sy][j][j'] P[sz][k][k'] u_c(j', k'),
+ * P[s][j][j'] = coarse Lagrange basis j' at (s + z_j) / 2.  The operator is
+ * sum_K C_K^T A_K C_K; the hanging DoFs are constrained like Dirichlet DoFs
+ * (read through the constraint, output 0, diagonal 1).  dim 3, constant
+ * coefficients (no k(T) field, no Robin faces, analytic velocities). */
+typedef struct {
+  orc_mesh coarse, fine;
+} orc_mesh2;
+
+long orc2_n_dofs(const orc_mesh2 *m);
+/* P[s][j][j'] of degree p (2 x n x n) */
+void orc2_hanging_matrix(int degree, double *P);
+void orc2_vmult(const orc_mesh2 *m, const orc_op *op, double *dst, const double *src);
+void orc2_diagonal(const orc_mesh2 *m, const orc_op *op, double *diag);
+/* values of the hanging fine DoFs from the coarse DoFs (the constraint distribution) */
+void orc2_distribute(const orc_mesh2 *m, double *u);
+void orc2_dof_coordinates(const orc_mesh2 *m, double *xyz);
+
 #ifdef __cplusplus
 }
 #endif

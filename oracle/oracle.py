@@ -40,6 +40,10 @@ class _Op(C.Structure):
     ]
 
 
+class _Mesh2(C.Structure):
+    _fields_ = [("coarse", _Mesh), ("fine", _Mesh)]
+
+
 class _Prec(C.Structure):
     _fields_ = [("type", C.c_int), ("inv_diag", _dp), ("degree", C.c_int),
                 ("lambda_min", C.c_double), ("lambda_max", C.c_double)]
@@ -81,6 +85,14 @@ def lib():
         L.orc_prec_apply.argtypes = [P_m, P_o, P_p, _dp, _dp]
         L.orc_gauss_legendre.argtypes = [C.c_int, _dp, _dp]
         L.orc_gauss_lobatto.argtypes = [C.c_int, _dp]
+        P_m2 = C.POINTER(_Mesh2)
+        L.orc2_n_dofs.restype = C.c_long
+        L.orc2_n_dofs.argtypes = [P_m2]
+        L.orc2_hanging_matrix.argtypes = [C.c_int, _dp]
+        L.orc2_vmult.argtypes = [P_m2, P_o, _dp, _dp]
+        L.orc2_diagonal.argtypes = [P_m2, P_o, _dp]
+        L.orc2_distribute.argtypes = [P_m2, _dp]
+        L.orc2_dof_coordinates.argtypes = [P_m2, _dp]
         _lib = L
     return _lib
 
@@ -292,3 +304,77 @@ def gauss_lobatto(n):
     x = np.zeros(n)
     lib().orc_gauss_lobatto(n, _ptr(x))
     return x
+
+
+# ------------------------------------------------------------ hanging nodes
+
+class Mesh2:
+    """Two-level mesh (orc_mesh2): a coarse block of nc cells on
+    [lo, (xm, hi_y, hi_z)] and a fine block of (ncf_x, 2 nc_y, 2 nc_z) cells on
+    [(xm, lo_y, lo_z), hi]; the fine DoFs on the plane x = xm hang on the coarse
+    faces.  Interior vertices of each block may be perturbed; boundary vertices
+    (the interface included) stay on the regular lattice."""
+
+    def __init__(self, degree, nc, ncf_x, lo=(0.0, 0.0, 0.0), xm=0.5, hi=(1.0, 1.0, 1.0), perturb=0.0,
+                 seed=None):
+        nc = tuple(int(v) for v in nc)
+        ncf = (int(ncf_x), 2 * nc[1], 2 * nc[2])
+        Vc = box_vertices(3, nc, lo, (xm, hi[1], hi[2]), perturb, seed)
+        Vf = box_vertices(3, ncf, (xm, lo[1], lo[2]), hi, perturb, None if seed is None else seed + 1)
+        self.degree = degree
+        self.coarse = Mesh(3, degree, nc, Vc)
+        self.fine = Mesh(3, degree, ncf, Vf)
+        self._c = _Mesh2(self.coarse._c, self.fine._c)
+        self.n_coarse = self.coarse.n_dofs
+        self.n_dofs = self.coarse.n_dofs + self.fine.n_dofs
+
+    def hanging_mask(self):
+        """uint8 mask of the hanging fine DoFs (the fine block's x = xm plane)."""
+        m = np.zeros(self.n_dofs, dtype=np.uint8)
+        m[self.n_coarse:] = (self.fine.grid_index()[:, 0] == 0)
+        return m
+
+    def boundary_face_mask(self, faces=None):
+        """Dirichlet mask of the outer box faces ((direction, side) pairs; default
+        all six): x = lo on the coarse block, x = hi on the fine block, the
+        y and z faces on both.  The hanging plane is not part of it."""
+        if faces is None:
+            faces = [(d, s) for d in range(3) for s in (0, 1)]
+        fc = [f for f in faces if f != (0, 1)]
+        ff = [f for f in faces if f != (0, 0)]
+        mc = self.coarse.boundary_face_mask(fc) if fc else np.zeros(self.n_coarse, np.uint8)
+        mf = self.fine.boundary_face_mask(ff) if ff else np.zeros(self.fine.n_dofs, np.uint8)
+        return np.concatenate([mc, mf]).astype(np.uint8)
+
+    def dof_coordinates(self):
+        x = np.zeros((self.n_dofs, 3))
+        lib().orc2_dof_coordinates(C.byref(self._c), _ptr(x))
+        return x
+
+
+def hanging_matrix(degree):
+    """P[s, j, j'] = coarse Lagrange basis j' at the fine node (s + z_j) / 2."""
+    n = degree + 1
+    P = np.zeros(2 * n * n)
+    lib().orc2_hanging_matrix(degree, _ptr(P))
+    return P.reshape(2, n, n)
+
+
+def vmult2(mesh2, op, src):
+    src = np.ascontiguousarray(src, np.float64)
+    dst = np.zeros(mesh2.n_dofs)
+    lib().orc2_vmult(C.byref(mesh2._c), C.byref(op._c), _ptr(dst), _ptr(src))
+    return dst
+
+
+def diagonal2(mesh2, op):
+    d = np.zeros(mesh2.n_dofs)
+    lib().orc2_diagonal(C.byref(mesh2._c), C.byref(op._c), _ptr(d))
+    return d
+
+
+def distribute2(mesh2, u):
+    """u with its hanging fine DoFs set to the coarse face interpolant."""
+    u = np.array(u, dtype=np.float64)
+    lib().orc2_distribute(C.byref(mesh2._c), _ptr(u))
+    return u
