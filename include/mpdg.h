@@ -120,6 +120,21 @@ int mpdg_version(void);
 /* ------------------------------------------------------------------ meshes */
 /* replaces ScratchData::build / MatrixFree::reinit: source/core/scratch_data.cpp:191-268 */
 mpdg_status mpdg_mesh_create(const mpdg_mesh_desc *desc, mpdg_mesh **mesh);
+/* Two-level mesh with hanging nodes: a coarse block and a fine block that
+ * refines it 2:1 in y and z (fine->nc[1] = 2 coarse->nc[1], fine->nc[2] =
+ * 2 coarse->nc[2]), meeting at the coarse block's x = max face, on which the
+ * fine block's x = min face lies (its interface vertices on the coarse faces'
+ * bilinear maps at the half points).  The fine DoFs on that plane hang on the
+ * coarse faces: their values are the coarse faces' interpolants, as deal.II's
+ * hanging-node constraints on a 2:1 refined face (read_dof_values /
+ * distribute_local_to_global with constraints, matrix_free cell loops of
+ * heat_diffuse_operator.cpp:199-241).  Vectors hold the coarse block's DoFs,
+ * then the fine block's (both lexicographic); the hanging DoFs are constrained
+ * like Dirichlet DoFs (read through the interpolation, output 0, diagonal 1).
+ * Operators on it take constant coefficients (no k(T), Robin faces or full
+ * tangent) and support vmult, the diagonal and the solvers. */
+mpdg_status mpdg_mesh_create_two_level(const mpdg_mesh_desc *coarse, const mpdg_mesh_desc *fine,
+                                       mpdg_mesh **mesh);
 mpdg_status mpdg_mesh_destroy(mpdg_mesh *mesh);
 /* n_dofs of the mesh (ScratchData::get_dof_handler(idx).n_dofs()) */
 mpdg_status mpdg_mesh_n_dofs(const mpdg_mesh *mesh, int64_t *n_dofs);

@@ -102,6 +102,7 @@ def lib():
     L.mpdg_kernel_launches.restype = C.c_int64
     L.mpdg_mesh_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(vp)]
     L.mpdg_mesh_destroy.argtypes = [vp]
+    L.mpdg_mesh_create_two_level.argtypes = [C.POINTER(MeshDesc), C.POINTER(MeshDesc), C.POINTER(vp)]
     L.mpdg_mesh_n_dofs.argtypes = [vp, C.POINTER(C.c_int64)]
     L.mpdg_mesh_device_bytes.argtypes = [vp, C.POINTER(C.c_int64)]
     L.mpdg_op_create.argtypes = [vp, C.POINTER(OpDesc), C.POINTER(vp)]

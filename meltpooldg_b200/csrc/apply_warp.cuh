@@ -246,7 +246,7 @@ struct WOcc {
                                                        : (P == 4 ? 5 : P == 3 ? 6 : P == 2 ? 7 : 8);
 };
 
-template <int P, typename Real, int GEOM>
+template <int P, typename Real, int GEOM, bool HANG = false>
 __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     warp_apply_kernel(const KP<Real> p, int *err)
 {
@@ -298,8 +298,33 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     int ix = 0, iy = 0, iz = 0;
     if (act) colour_cell(cidx, p, ix, iy, iz);
     const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
+    if (HANG && act && ix == 0 && i == 0) {
+      // hanging DoF (0, j, k): the coarse face's interpolant at the fine node,
+      // H along y then along z (subface iy % 2, iz % 2 of coarse face (iy/2, iz/2))
+      const int cy = iy >> 1, sy = iy & 1, cz = iz >> 1, sz = iz & 1;
+      Real sk[n];
 #pragma unroll
-    for (int k = 0; k < n; ++k) A[k] = act ? p.src[g0 + k * zs] : Real(0);
+      for (int kp = 0; kp < n; ++kp) {
+        Real sacc = 0;
+#pragma unroll
+        for (int jp = 0; jp < n; ++jp) {
+          const long gc = ((long)(cz * P + kp) * p.hNYc + (cy * P + jp)) * p.hNXc + (p.hNXc - 1);
+          const Real c = (p.masked_read && p.hmask && p.hmask[gc]) ? Real(0) : p.hsrc[gc];
+          sacc += T.H[(sy * n + j) * n + jp] * c;
+        }
+        sk[kp] = sacc;
+      }
+#pragma unroll
+      for (int k = 0; k < n; ++k) {
+        Real sacc = 0;
+#pragma unroll
+        for (int kp = 0; kp < n; ++kp) sacc += T.H[(sz * n + k) * n + kp] * sk[kp];
+        A[k] = sacc;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < n; ++k) A[k] = act ? p.src[g0 + k * zs] : Real(0);
+    }
     cm = (act && use_mask) ? p.cell_mask[p.cfirst + cidx] : make_uint4(0u, 0u, 0u, 0u);
   };
   auto mask_bit = [&](const uint4 &cm, int k) -> bool {
@@ -324,6 +349,9 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
     const uint4 cm = cmA;
 
+    // hanging lane of the fine block: its column is the coarse face's interpolant,
+    // its slots are never written (stored 0 by the first cell), its result is staged
+    const bool hl = HANG && active && ix == 0 && i == 0;
     // store-or-add decision and the early loads of the values to add to
     const bool sx = (i == 0 && ix > 0) || (i == P && ix < p.nc[0] - 1);
     const bool sy = (j == 0 && iy > 0) || (j == P && iy < p.nc[1] - 1);
@@ -338,7 +366,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
       const bool masked = p.masked_write && mask_bit(cm, k);
       first_bits |= (unsigned)first << k;
       mask_bits |= (unsigned)masked << k;
-      dpre[k] = (active && !first && !masked) ? p.dst[g] : Real(0);
+      dpre[k] = (active && !first && !masked && !hl) ? p.dst[g] : Real(0);
     }
 
     Real u[n];
@@ -403,12 +431,46 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     Real out[n];
     l_backward<n>(T.S, T.Dc, t0, t1, lane_ok, i, j, val, fx, fy, fz, out);
 
+    if (HANG && __any_sync(0xffffffffu, hl)) {
+      // transposed interpolation of the hanging results onto the coarse face:
+      // H^T along z in registers, then along y across the cell's i = 0 lanes
+      Real w[n];
+#pragma unroll
+      for (int kp = 0; kp < n; ++kp) {
+        Real sacc = 0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) sacc += T.H[((iz & 1) * n + k) * n + kp] * out[k];
+        w[kp] = sacc;
+      }
+      if (hl) {
+#pragma unroll
+        for (int kp = 0; kp < n; ++kp) t0[j * n + kp] = w[kp];
+      }
+      __syncwarp();
+      if (hl) {
+        Real *st = p.hstage + ((long)iz * p.hnc1 + iy) * n * n;
+#pragma unroll
+        for (int kp = 0; kp < n; ++kp) {
+          Real sacc = 0;
+#pragma unroll
+          for (int jj = 0; jj < n; ++jj) sacc += T.H[((iy & 1) * n + jj) * n + j] * t0[jj * n + kp];
+          st[kp * n + j] = sacc;
+        }
+      }
+      __syncwarp();
+    }
+
     if (active) {
 #pragma unroll
       for (int k = 0; k < n; ++k) {
         const long g = g0 + k * zs;
-        if ((first_bits >> k) & 1) p.dst[g] = ((mask_bits >> k) & 1) ? Real(0) : out[k];
-        else if (!((mask_bits >> k) & 1)) p.dst[g] = dpre[k] + out[k];
+        if (hl) {
+          if ((first_bits >> k) & 1) p.dst[g] = Real(0);
+        } else if ((first_bits >> k) & 1) {
+          p.dst[g] = ((mask_bits >> k) & 1) ? Real(0) : out[k];
+        } else if (!((mask_bits >> k) & 1)) {
+          p.dst[g] = dpre[k] + out[k];
+        }
       }
     }
   }

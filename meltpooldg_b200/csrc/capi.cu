@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cmath>
 #include <chrono>
 #include <cstring>
 #include <mutex>
@@ -59,6 +60,7 @@ mpdg_status mpdg_mesh_create(const mpdg_mesh_desc *desc, mpdg_mesh **out)
     m.n_cells = (long)m.nc[0] * m.nc[1] * m.nc[2];
     const long nv = (long)(m.nc[0] + 1) * (m.nc[1] + 1) * (m.nc[2] + 1);
     m.vertices.assign(desc->vertices, desc->vertices + nv * 3);
+    m.N_own = m.N;
     try {
       build_mesh_device_data(m, desc->dirichlet_mask, desc->geometry == MPDG_GEOM_GENERAL);
     } catch (...) {
@@ -70,13 +72,99 @@ mpdg_status mpdg_mesh_create(const mpdg_mesh_desc *desc, mpdg_mesh **out)
   });
 }
 
+mpdg_status mpdg_mesh_create_two_level(const mpdg_mesh_desc *coarse, const mpdg_mesh_desc *fine, mpdg_mesh **out)
+{
+  return guarded([&]() -> int {
+    if (!coarse || !fine || !out || !coarse->vertices || !fine->vertices) throw Error{MPDG_ERR_ARG, "null argument"};
+    if (coarse->degree != fine->degree) throw Error{MPDG_ERR_ARG, "both blocks carry the same degree"};
+    if (fine->nc[1] != 2 * coarse->nc[1] || fine->nc[2] != 2 * coarse->nc[2])
+      throw Error{MPDG_ERR_ARG, "the fine block refines the coarse interface 2:1 in y and z"};
+    // the fine block's interface plane hangs on the coarse faces: it is not part
+    // of the fine block's Dirichlet set
+    const long NXf = (long)fine->nc[0] * fine->degree + 1, NYf = (long)fine->nc[1] * fine->degree + 1,
+               NZf = (long)fine->nc[2] * fine->degree + 1;
+    std::vector<uint8_t> fmask;
+    mpdg_mesh_desc fd = *fine;
+    if (fine->dirichlet_mask) {
+      fmask.assign(fine->dirichlet_mask, fine->dirichlet_mask + NXf * NYf * NZf);
+      for (long r = 0; r < NYf * NZf; ++r) fmask[r * NXf] = 0;
+      fd.dirichlet_mask = fmask.data();
+    }
+    mpdg_mesh *hc = nullptr, *hf = nullptr;
+    int st = mpdg_mesh_create(coarse, &hc);
+    if (st != MPDG_OK) return st;
+    st = mpdg_mesh_create(&fd, &hf);
+    if (st != MPDG_OK) {
+      mpdg_mesh_destroy(hc);
+      return st;
+    }
+    Mesh &m = hc->m;
+    Mesh *f = new Mesh(std::move(hf->m));
+    hf->m = Mesh{};
+    delete hf;
+    m.fine = f;
+    try {
+      // the fine interface vertices must lie on the coarse faces (bilinear face
+      // map at the half points)
+      const int c0 = coarse->nc[0], c1 = coarse->nc[1], c2 = coarse->nc[2];
+      auto cv = [&](int vy, int vz, int a) {
+        return m.vertices[(((long)vz * (c1 + 1) + vy) * (c0 + 1) + c0) * 3 + a];
+      };
+      double scale = 0.0;
+      for (double v : m.vertices) scale = std::fmax(scale, std::fabs(v));
+      for (int vz = 0; vz <= 2 * c2; ++vz)
+        for (int vy = 0; vy <= 2 * c1; ++vy) {
+          const int cy = std::min(vy / 2, c1 - 1), cz = std::min(vz / 2, c2 - 1);
+          const double ty = 0.5 * (vy - 2 * cy), tz = 0.5 * (vz - 2 * cz);
+          for (int a = 0; a < 3; ++a) {
+            const double want = (1 - ty) * (1 - tz) * cv(cy, cz, a) + ty * (1 - tz) * cv(cy + 1, cz, a) +
+                                (1 - ty) * tz * cv(cy, cz + 1, a) + ty * tz * cv(cy + 1, cz + 1, a);
+            const double got = f->vertices[(((long)vz * (2 * c1 + 1) + vy) * (fine->nc[0] + 1)) * 3 + a];
+            if (std::fabs(got - want) > 1e-12 * std::fmax(1.0, scale))
+              throw Error{MPDG_ERR_ARG, "fine interface vertices do not lie on the coarse faces"};
+          }
+        }
+      // whole-vector masks: Dirichlet (both blocks) or hanging, and hanging only
+      const long Nc = m.N_own, Nf = f->N_own, N = Nc + Nf;
+      std::vector<uint8_t> tdir(N, 0), thang(N, 0);
+      if (coarse->dirichlet_mask)
+        for (long i = 0; i < Nc; ++i) tdir[i] = coarse->dirichlet_mask[i] ? 1 : 0;
+      if (fd.dirichlet_mask)
+        for (long i = 0; i < Nf; ++i) tdir[Nc + i] = fd.dirichlet_mask[i] ? 1 : 0;
+      for (long r = 0; r < NYf * NZf; ++r) tdir[Nc + r * NXf] = thang[Nc + r * NXf] = 1;
+      MPDG_CUDA(cudaMalloc(&m.d_tmask_dir, N));
+      MPDG_CUDA(cudaMalloc(&m.d_tmask_hang, N));
+      MPDG_CUDA(cudaMemcpy(m.d_tmask_dir, tdir.data(), N, cudaMemcpyHostToDevice));
+      MPDG_CUDA(cudaMemcpy(m.d_tmask_hang, thang.data(), N, cudaMemcpyHostToDevice));
+      m.device_bytes += 2 * N + f->device_bytes;
+      m.N = N;
+    } catch (...) {
+      mpdg_mesh_destroy(hc);
+      throw;
+    }
+    *out = hc;
+    return MPDG_OK;
+  });
+}
+
+namespace {
+void free_mesh_arrays(Mesh &m)
+{
+  for (void *p : {(void *)m.d_vert, (void *)m.d_metric64, (void *)m.d_metric32, (void *)m.d_dmask,
+                  (void *)m.d_cell_flags, (void *)m.d_cell_mask, (void *)m.d_tmask_dir, (void *)m.d_tmask_hang})
+    if (p) cudaFree(p);
+}
+}  // namespace
+
 mpdg_status mpdg_mesh_destroy(mpdg_mesh *mesh)
 {
   if (!mesh) return MPDG_OK;
   Mesh &m = mesh->m;
-  for (void *p : {(void *)m.d_vert, (void *)m.d_metric64, (void *)m.d_metric32, (void *)m.d_dmask,
-                  (void *)m.d_cell_flags, (void *)m.d_cell_mask})
-    if (p) cudaFree(p);
+  free_mesh_arrays(m);
+  if (m.fine) {
+    free_mesh_arrays(*m.fine);
+    delete m.fine;
+  }
   delete mesh;
   return MPDG_OK;
 }
@@ -102,13 +190,32 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     if (desc->kind != MPDG_OP_HEAT && desc->kind != MPDG_OP_ADVDIFF) throw Error{MPDG_ERR_ARG, "unknown operator kind"};
     if (!(desc->dt > 0.0)) throw Error{MPDG_ERR_ARG, "time increment must be positive"};
     if (desc->vel_kind < MPDG_VEL_NONE || desc->vel_kind > MPDG_VEL_CONST) throw Error{MPDG_ERR_ARG, "unknown velocity kind"};
+    Mesh &mm = mesh->m;
+    if (mm.fine && (desc->k_alpha != 0.0 || desc->full_tangent || (desc->robin_faces && desc->robin_alpha != 0.0)))
+      throw Error{MPDG_ERR_UNSUPPORTED,
+                  "two-level meshes take constant coefficients: no k(T) law, full tangent or Robin faces"};
     auto *h = new mpdg_op();
     Op &o = h->o;
-    o.mesh = &mesh->m;
+    o.mesh = &mm;
     o.d = *desc;
     if (o.d.precision_mask == 0) o.d.precision_mask = 1 << MPDG_FP64;
     try {
       build_op_device_data(o);
+      if (mm.fine) {
+        o.fine = new Op();
+        Op &f = *o.fine;
+        f.mesh = mm.fine;
+        f.d = o.d;
+        f.stream = o.stream;
+        f.hang_NXc = mm.NX;
+        f.hang_NYc = mm.NY;
+        build_op_device_data(f);
+        const int n = mm.degree + 1;
+        const size_t bytes = sizeof(double) * (size_t)mm.fine->nc[1] * mm.fine->nc[2] * n * n;
+        MPDG_CUDA(cudaMalloc(&f.d_stage, bytes));
+        MPDG_CUDA(cudaMemset(f.d_stage, 0, bytes));
+        f.device_bytes += bytes;
+      }
     } catch (...) {
       mpdg_op_destroy(h);
       throw;
@@ -118,14 +225,25 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
   });
 }
 
+namespace {
+void free_op_arrays(Op &o)
+{
+  free_workspace(o);
+  for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32,
+                  (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32, (void *)o.d_trig64, o.d_stage})
+    if (p) cudaFree(p);
+}
+}  // namespace
+
 mpdg_status mpdg_op_destroy(mpdg_op *op)
 {
   if (!op) return MPDG_OK;
   Op &o = op->o;
-  free_workspace(o);
-  for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32, (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32,
-                  (void *)o.d_trig64})
-    if (p) cudaFree(p);
+  free_op_arrays(o);
+  if (o.fine) {
+    free_op_arrays(*o.fine);
+    delete o.fine;
+  }
   delete op;
   return MPDG_OK;
 }
@@ -135,6 +253,10 @@ mpdg_status mpdg_op_reset_time_increment(mpdg_op *op, double dt)
   if (!op || !(dt > 0.0)) return MPDG_ERR_ARG;
   if (op->o.d.dt != dt) invalidate_coef(op->o);
   op->o.d.dt = dt;
+  if (op->o.fine) {
+    if (op->o.fine->d.dt != dt) invalidate_coef(*op->o.fine);
+    op->o.fine->d.dt = dt;
+  }
   return MPDG_OK;
 }
 
@@ -142,6 +264,7 @@ mpdg_status mpdg_op_use_dirichlet(mpdg_op *op, int use_dirichlet)
 {
   if (!op) return MPDG_ERR_ARG;
   op->o.use_dirichlet = use_dirichlet != 0;
+  if (op->o.fine) op->o.fine->use_dirichlet = use_dirichlet != 0;
   return MPDG_OK;
 }
 
@@ -150,6 +273,7 @@ mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *values)
   return guarded([&]() -> int {
     if (!op) throw Error{MPDG_ERR_ARG, "null operator"};
     if (field != MPDG_FIELD_TEMPERATURE) throw Error{MPDG_ERR_ARG, "unknown field"};
+    if (op->o.fine) throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take no temperature field"};
     op->o.T64 = values;
     invalidate_coef(op->o);
     if (values && (op->o.d.precision_mask & (1 << MPDG_FP32))) ensure_T32(op->o);
@@ -192,6 +316,7 @@ mpdg_status mpdg_op_set_stream(mpdg_op *op, void *stream)
 {
   if (!op) return MPDG_ERR_ARG;
   op->o.stream = (cudaStream_t)stream;
+  if (op->o.fine) op->o.fine->stream = (cudaStream_t)stream;
   return MPDG_OK;
 }
 

@@ -90,6 +90,15 @@ struct Mesh {
   bool has_dirichlet = false;
   size_t device_bytes = 0;
   bool metric32_ready = false;
+  // Two-level mesh (hanging nodes): this mesh is the coarse block and `fine`
+  // the fine block, refined 2:1 in y and z, meeting at the coarse block's
+  // x = max face.  Vectors hold the coarse block's N_own DoFs, then the fine
+  // block's; N is their sum.  The fine DoFs on the interface plane hang on the
+  // coarse faces (read through the interpolation, never written).
+  Mesh *fine = nullptr;
+  long N_own = 0;
+  uint8_t *d_tmask_dir = nullptr;   // whole vector: Dirichlet or hanging
+  uint8_t *d_tmask_hang = nullptr;  // whole vector: hanging only
 };
 
 struct Workspace;  // solver vectors (solvers.cu)
@@ -114,6 +123,14 @@ struct Op {
   float *d_coef32 = nullptr;
   bool coef64_ok = false, coef32_ok = false;
   size_t device_bytes = 0;
+  // two-level mesh: the fine block's operator and the per-interface-cell stage
+  // of the hanging DoFs' contributions to the coarse DoFs
+  Op *fine = nullptr;
+  void *d_stage = nullptr;
+  // set on the fine block's operator for one apply: where the hanging DoFs read from
+  const void *hang_src = nullptr;
+  const uint8_t *hang_mask = nullptr;
+  long hang_NXc = 0, hang_NYc = 0;  // the coarse lattice the hanging DoFs read from
 };
 
 // ---- batched apply over many solves (batch_apply.cuh / batch.cu)

@@ -32,6 +32,9 @@ struct Tables {
   Real Dc[kMaxN * kMaxN];  // Dc[q*n+r] = l_r'(x_q): collocation derivative on Gauss points
   Real w[kMaxN];           // Gauss weights on [0,1]
   Real x[kMaxN];           // Gauss points on [0,1]
+  // hanging-node interpolation of a 2:1 refined face: H[(s*n + j)*n + j'] =
+  // Gauss-Lobatto basis j' at the fine node (s + z_j) / 2 of subface s
+  Real H[2 * kMaxN * kMaxN];
 };
 
 __constant__ Tables<double> c_tab64[kMaxDegree + 1];
@@ -137,6 +140,14 @@ void upload_tables()
         t64[p].Dc[q * n + i] = d;
       }
     }
+    for (int sub = 0; sub < 2; ++sub)
+      for (int j = 0; j < n; ++j)
+        for (int jp = 0; jp < n; ++jp) {
+          double v, d;
+          lagrange(n, zl, jp, 0.5 * (sub + zl[j]), v, d);
+          t64[p].H[(sub * n + j) * n + jp] = v;
+        }
+    for (int k = 0; k < 2 * kMaxN * kMaxN; ++k) t32[p].H[k] = (float)t64[p].H[k];
     for (int k = 0; k < kMaxN * kMaxN; ++k) {
       t32[p].S[k] = (float)t64[p].S[k];
       t32[p].D[k] = (float)t64[p].D[k];
@@ -196,6 +207,13 @@ struct KP {
   int vel_kind;
   Real vel_param[3];
   int masked_read, masked_write, full_tangent;
+  // fine block of a two-level mesh: the hanging DoFs (cells ix = 0, i = 0) read
+  // the coarse face through the interpolation H and stage their contributions
+  const Real *hsrc;      // coarse block's values (null: no hanging DoFs)
+  Real *hstage;          // [fine interface cell iz*hnc1 + iy][k' n + j']
+  const uint8_t *hmask;  // coarse block's Dirichlet mask (or null)
+  long hNXc, hNYc;       // coarse lattice
+  int hnc1;              // fine cells in y
 };
 
 template <int n>
@@ -1081,6 +1099,12 @@ KP<Real> base_params(Op &op)
   KP<Real> k{};
   k.NX = m.NX;
   k.NY = m.NY;
+  k.hsrc = (const Real *)op.hang_src;
+  k.hstage = (Real *)op.d_stage;
+  k.hmask = op.hang_mask;
+  k.hNXc = op.hang_NXc;
+  k.hNYc = op.hang_NYc;
+  k.hnc1 = m.nc[1];
   for (int d = 0; d < 3; ++d) k.nc[d] = m.nc[d];
   for (int d = 0; d < 3; ++d) {
     k.h[d] = (Real)m.h[d];
@@ -1191,7 +1215,7 @@ int num_sms()
   return g_num_sms;
 }
 
-template <int P, typename Real, int GEOM>
+template <int P, typename Real, int GEOM, bool HANG>
 void run_warp_apply(Op &op, KP<Real> k)
 {
   Mesh &m = *op.mesh;
@@ -1208,7 +1232,7 @@ void run_warp_apply(Op &op, KP<Real> k)
     throw Error{MPDG_ERR_ARG, "coefficient stream not 16-byte aligned"};
   if (GEOM == GEOM_GENERAL && (!k.metric || (gvel && !k.velb)))
     throw Error{MPDG_ERR_ARG, "coefficient stream missing"};
-  auto kern = warp_apply_kernel<P, Real, GEOM>;
+  auto kern = warp_apply_kernel<P, Real, GEOM, HANG>;
   static int configured_smem = -1, blocks_per_sm = 0;  // per instantiation
   if (configured_smem != (int)smem) {
     MPDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1231,11 +1255,12 @@ void run_warp_apply(Op &op, KP<Real> k)
 template <typename Real, int GEOM>
 void warp_apply_degree(Op &op, const KP<Real> &k)
 {
+  const bool hang = k.hsrc != nullptr;
   switch (op.mesh->degree) {
-    case 1: run_warp_apply<1, Real, GEOM>(op, k); break;
-    case 2: run_warp_apply<2, Real, GEOM>(op, k); break;
-    case 3: run_warp_apply<3, Real, GEOM>(op, k); break;
-    case 4: run_warp_apply<4, Real, GEOM>(op, k); break;
+    case 1: hang ? run_warp_apply<1, Real, GEOM, true>(op, k) : run_warp_apply<1, Real, GEOM, false>(op, k); break;
+    case 2: hang ? run_warp_apply<2, Real, GEOM, true>(op, k) : run_warp_apply<2, Real, GEOM, false>(op, k); break;
+    case 3: hang ? run_warp_apply<3, Real, GEOM, true>(op, k) : run_warp_apply<3, Real, GEOM, false>(op, k); break;
+    case 4: hang ? run_warp_apply<4, Real, GEOM, true>(op, k) : run_warp_apply<4, Real, GEOM, false>(op, k); break;
     default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
   }
 }
@@ -1432,14 +1457,108 @@ void invalidate_coef(Op &op)
   op.coef32_ok = false;
 }
 
+// ------------------------------------------------------------ hanging nodes
+// Adds the staged contributions of the fine interface cells to the coarse DoFs
+// of the interface plane: one thread per coarse DoF (Y, Z) sums, in a fixed
+// order, the stage entries of the (up to 4) coarse faces containing it times
+// their 4 subfaces, so the result is deterministic.
+template <typename Real>
+__global__ void hang_fold_kernel(const Real *stage, Real *dst, long NXc, long NYc, long NZc, int P, int ncc1,
+                                 int ncc2, int ncf1, const uint8_t *cmask)
+{
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= NYc * NZc) return;
+  const int Y = (int)(t % NYc), Z = (int)(t / NYc);
+  const int n = P + 1;
+  int cys[2], czs[2], ny = 0, nz = 0;
+  const int qy = Y / P, qz = Z / P;
+  if (Y % P == 0) {
+    if (qy >= 1) cys[ny++] = qy - 1;
+    if (qy < ncc1) cys[ny++] = qy;
+  } else {
+    cys[ny++] = qy;
+  }
+  if (Z % P == 0) {
+    if (qz >= 1) czs[nz++] = qz - 1;
+    if (qz < ncc2) czs[nz++] = qz;
+  } else {
+    czs[nz++] = qz;
+  }
+  Real sum = 0;
+  for (int b = 0; b < nz; ++b)
+    for (int a = 0; a < ny; ++a) {
+      const int cy = cys[a], cz = czs[b], jp = Y - cy * P, kp = Z - cz * P;
+      for (int sz = 0; sz < 2; ++sz)
+        for (int sy = 0; sy < 2; ++sy) {
+          const long fi = (long)(2 * cz + sz) * ncf1 + (2 * cy + sy);
+          sum += stage[fi * n * n + kp * n + jp];
+        }
+    }
+  const long g = ((long)Z * NYc + Y) * NXc + (NXc - 1);
+  if (!(cmask && cmask[g])) dst[g] += sum;
+}
+
+// probe of the interface plane for the diagonal: x = 1 at the coarse interface
+// DoFs (Y, Z) with Y % n == a and Z % n == b, 0 elsewhere
+__global__ void hang_probe_kernel(double *x, long N, long NXc, long NYc, long NZc, int n, int a, int b)
+{
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < N; t += (long)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (t < NXc * NYc * NZc && t % NXc == NXc - 1) {
+      const long Y = (t / NXc) % NYc, Z = t / (NXc * NYc);
+      v = (Y % n == a && Z % n == b) ? 1.0 : 0.0;
+    }
+    x[t] = v;
+  }
+}
+
+__global__ void hang_probe_take_kernel(double *diag, const double *y, long NXc, long NYc, long NZc, int n, int a,
+                                       int b)
+{
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= NYc * NZc) return;
+  const long Y = t % NYc, Z = t / NYc;
+  if (Y % n != a || Z % n != b) return;
+  const long g = (Z * NYc + Y) * NXc + (NXc - 1);
+  diag[g] = y[g];
+}
+
 template <typename Real>
 void launch_cells(Op &op, Real *dst, const Real *src);
+
+// the fine block of a two-level mesh, after the coarse block: its hanging DoFs
+// read the coarse values of src, their contributions fold into dst's coarse part
+template <typename Real>
+void launch_fine_block(Op &op, Real *dst, const Real *src)
+{
+  Op &f = *op.fine;
+  Mesh &m = *op.mesh;
+  const bool mask = op.use_dirichlet && m.has_dirichlet;
+  f.use_dirichlet = op.use_dirichlet;
+  f.hang_src = src;
+  f.hang_mask = mask ? m.d_dmask : nullptr;
+  try {
+    launch_cells<Real>(f, dst + m.N_own, src + m.N_own);
+  } catch (...) {
+    f.hang_src = nullptr;
+    throw;
+  }
+  f.hang_src = nullptr;
+  const Mesh &fm = *f.mesh;
+  const long cnt = m.NY * m.NZ;
+  hang_fold_kernel<Real><<<grid_for(cnt, 256), 256, 0, op.stream>>>(
+      (const Real *)f.d_stage, dst, m.NX, m.NY, m.NZ, m.degree, m.nc[1], m.nc[2], fm.nc[1], mask ? m.d_dmask : nullptr);
+  MPDG_LAUNCHED();
+}
+
+
 
 template <typename Real>
 void launch_apply(Op &op, Real *dst, const Real *src)
 {
   launch_cells<Real>(op, dst, src);
   launch_robin<Real>(op, dst, src, ROBIN_APPLY);
+  if (op.fine) launch_fine_block<Real>(op, dst, src);
 }
 
 template <typename Real>
@@ -1471,7 +1590,7 @@ void launch_cells(Op &op, Real *dst, const Real *src)
     ensure_metric32(m, op.stream);
     k.metric = (const Real *)(const void *)m.d_metric32;
   }
-  MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * m.N, op.stream));
+  MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * m.N_own, op.stream));
   if (kt) dispatch_degree<Real, MODE_LINEAR, true>(op, k);
   else dispatch_degree<Real, MODE_LINEAR, false>(op, k);
 }
@@ -1481,6 +1600,7 @@ template void launch_apply<float>(Op &, float *, const float *);
 
 void launch_rhs(Op &op, double *dst, const double *src, const double *heat_source)
 {
+  if (op.fine) throw Error{MPDG_ERR_UNSUPPORTED, "create_rhs on two-level meshes"};
   KP<double> k = base_params<double>(op);
   k.src = src;
   k.dst = dst;
@@ -1521,14 +1641,72 @@ void run_diag(Op &op, KP<double> k)
 }
 }  // namespace
 
+void launch_block_diagonal(Op &op, double *diag);
+
+// Diagonal of a two-level mesh: each block's local diagonal, then the coarse
+// interface DoFs by probing.  A probe sets 1 at the interface DoFs with
+// (Y % n, Z % n) = (a, b).  Two such DoFs are at least n apart in Y or Z, so
+// they share neither a coarse cell nor a coarse face (and so no fine interface
+// cell): the full apply returns each probed DoF's exact diagonal entry.
+// n^2 probes, each one apply.
+void launch_composite_diagonal(Op &op, double *diag)
+{
+  Mesh &m = *op.mesh;
+  launch_block_diagonal(op, diag);
+  Op &f = *op.fine;
+  f.use_dirichlet = op.use_dirichlet;
+  launch_block_diagonal(f, diag + m.N_own);
+  double *x = nullptr, *y = nullptr;
+  MPDG_CUDA(cudaMalloc(&x, sizeof(double) * m.N));
+  const cudaError_t e = cudaMalloc(&y, sizeof(double) * m.N);
+  if (e != cudaSuccess) {
+    cudaFree(x);
+    throw Error{MPDG_ERR_ALLOC, "diagonal probes"};
+  }
+  try {
+    const int n = m.degree + 1;
+    const long cnt = m.NY * m.NZ;
+    for (int b = 0; b < n; ++b)
+      for (int a = 0; a < n; ++a) {
+        hang_probe_kernel<<<grid_for(std::min(m.N, 148L * 1024), 256), 256, 0, op.stream>>>(x, m.N, m.NX, m.NY,
+                                                                                           m.NZ, n, a, b);
+        MPDG_LAUNCHED();
+        launch_apply<double>(op, y, x);
+        hang_probe_take_kernel<<<grid_for(cnt, 256), 256, 0, op.stream>>>(diag, y, m.NX, m.NY, m.NZ, n, a, b);
+        MPDG_LAUNCHED();
+      }
+    const uint8_t *tm = op.use_dirichlet ? m.d_tmask_dir : m.d_tmask_hang;
+    set_masked_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, tm, 1.0);
+    MPDG_LAUNCHED();
+    MPDG_CUDA(cudaStreamSynchronize(op.stream));
+  } catch (...) {
+    cudaStreamSynchronize(op.stream);
+    cudaFree(x);
+    cudaFree(y);
+    throw;
+  }
+  cudaFree(x);
+  cudaFree(y);
+}
+
 void launch_diagonal(Op &op, double *diag)
+{
+  if (op.fine) {
+    launch_composite_diagonal(op, diag);
+    return;
+  }
+  launch_block_diagonal(op, diag);
+}
+
+void launch_block_diagonal(Op &op, double *diag)
 {
   Mesh &m = *op.mesh;
   KP<double> k = base_params<double>(op);
   k.dst = diag;
   const bool kt = uses_kT(op);
   if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
-  MPDG_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * m.N, op.stream));
+  MPDG_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * m.N_own, op.stream));
+
   switch (m.degree) {
     case 1: kt ? run_diag<1, true>(op, k) : run_diag<1, false>(op, k); break;
     case 2: kt ? run_diag<2, true>(op, k) : run_diag<2, false>(op, k); break;
@@ -1538,9 +1716,18 @@ void launch_diagonal(Op &op, double *diag)
   }
   launch_robin<double>(op, diag, nullptr, ROBIN_DIAGONAL);
   if (op.use_dirichlet && m.has_dirichlet) {
-    set_masked_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, m.d_dmask, 1.0);
+    set_masked_kernel<<<grid_for(m.N_own, 256), 256, 0, op.stream>>>(diag, m.N_own, m.d_dmask, 1.0);
     MPDG_LAUNCHED();
   }
+}
+
+// DoFs whose diagonal (and inverse) is 1: Dirichlet DoFs when selected, and the
+// hanging DoFs of a two-level mesh always
+const uint8_t *constraint_mask(const Op &op)
+{
+  const Mesh &m = *op.mesh;
+  if (m.fine) return op.use_dirichlet ? m.d_tmask_dir : m.d_tmask_hang;
+  return (op.use_dirichlet && m.has_dirichlet) ? m.d_dmask : nullptr;
 }
 
 void launch_invert_diagonal(Op &op, double *diag)
@@ -1551,21 +1738,20 @@ void launch_invert_diagonal(Op &op, double *diag)
     // advection_diffusion_operator.cpp:436-439
     thr = 1e-14 * std::fmax(1.0, linf(diag, m.N, op.stream));
   }
-  const uint8_t *mask = (op.use_dirichlet && m.has_dirichlet) ? m.d_dmask : nullptr;
-  invert_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, mask, thr);
+  invert_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, constraint_mask(op), thr);
   MPDG_LAUNCHED();
 }
 
 void launch_invert_with_threshold(Op &op, double *diag, double thr)
 {
   Mesh &m = *op.mesh;
-  const uint8_t *mask = (op.use_dirichlet && m.has_dirichlet) ? m.d_dmask : nullptr;
-  invert_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, mask, thr);
+  invert_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, constraint_mask(op), thr);
   MPDG_LAUNCHED();
 }
 
 bool apply_ready_without_allocation(const Op &op)
 {
+  if (op.fine && !apply_ready_without_allocation(*op.fine)) return false;
   const Mesh &m = *op.mesh;
   const bool full = op.d.kind == MPDG_OP_HEAT && op.d.full_tangent;
   if (!full && !m.uniform) return op.coef64_ok;  // merged stream already built
@@ -1639,6 +1825,7 @@ __global__ void l2_cells_kernel(const double *u, long NX, long NY, int nc0, int 
 
 double l2_norm_integrated(Op &op, const double *u)
 {
+  if (op.fine) throw Error{MPDG_ERR_UNSUPPORTED, "integrated norms on two-level meshes"};
   Mesh &m = *op.mesh;
   const int blocks = 256;
   Colour *d_col = nullptr;

@@ -88,6 +88,41 @@ class Mesh:
             pass
 
 
+class TwoLevelMesh(Mesh):
+    """Mesh with hanging nodes (mpdg_mesh_create_two_level): a coarse block
+    and a fine block refining it 2:1 in y and z, meeting at the coarse block's
+    x = max face; the fine DoFs on that plane hang on the coarse faces.
+    Vectors are [coarse block DoFs, fine block DoFs]; the hanging DoFs are
+    constrained (kept at 0 in right-hand sides, like Dirichlet DoFs)."""
+
+    def __init__(self, coarse_vertices, nc_coarse, fine_vertices, nc_fine, degree, coarse_mask=None,
+                 fine_mask=None, geometry="auto"):
+        L = A.lib()
+        self.degree = int(degree)
+        self.nc_coarse = tuple(int(v) for v in nc_coarse)
+        self.nc_fine = tuple(int(v) for v in nc_fine)
+        keep = []
+
+        def desc(V, nc, mask):
+            V = np.ascontiguousarray(V, dtype=np.float64).reshape(-1, 3)
+            m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+            keep.extend([V, m])
+            return A.MeshDesc(3, self.degree, (C.c_int * 3)(*nc), V.ctypes.data_as(C.POINTER(C.c_double)),
+                              None if m is None else m.ctypes.data_as(C.POINTER(C.c_uint8)),
+                              A.GEOM_GENERAL if geometry == "general" else A.GEOM_AUTO)
+
+        dc = desc(coarse_vertices, self.nc_coarse, coarse_mask)
+        df = desc(fine_vertices, self.nc_fine, fine_mask)
+        h = C.c_void_p()
+        A.check(L.mpdg_mesh_create_two_level(C.byref(dc), C.byref(df), C.byref(h)), "mpdg_mesh_create_two_level")
+        self._h = h
+        n = C.c_int64()
+        L.mpdg_mesh_n_dofs(h, C.byref(n))
+        self.n_dofs = int(n.value)
+        self.n_coarse = int(np.prod([c * self.degree + 1 for c in self.nc_coarse]))
+        self.mask = None
+
+
 def box_vertices(nc, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), perturb=0.0, seed=None):
     """Vertices (x fastest) of an nc[0] x nc[1] x nc[2] box; interior vertices
     displaced by U[-perturb h, perturb h] per coordinate (PCG64(seed))."""
