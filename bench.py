@@ -149,6 +149,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def job_seconds(t_local, world):
+    """The job's time: the maximum of the ranks' device-timed regions (one
+    all-reduce; on NCCL through a CUDA tensor, on gloo through a CPU one)."""
+    if world <= 1:
+        return t_local
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    tt = torch.tensor([t_local], dtype=torch.float64, device=dev)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt)
+
+
+def replica_throughput(units_per_rank, world, t_job):
+    """Whole-job throughput of N independent replicas (weak scaling, no exchange
+    step): all ranks' units over the slowest rank's time."""
+    return units_per_rank * world / t_job
+
+
 def build_problem():
     import meltpooldg_b200 as M
     if WORKLOAD["name"] == "advdiff":
@@ -300,12 +319,8 @@ def run_ours(args, rank, world):
     launches = M.kernel_launches() - launches0
     barrier()
     t = e0.elapsed_time(e1) / 1e3
-    t_max = t
-    if world > 1:
-        tt = torch.tensor([t], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt)
-    value = N * args.steps * world / t_max
+    t_max = job_seconds(t, world)
+    value = replica_throughput(N * args.steps, world, t_max)
     apply_s = t / args.steps
 
     # FP32 apply
