@@ -30,6 +30,20 @@ def test_vortex_golden(name, dim, refinements):
         assert abs(g - r) / r < VORTEX_RTOL, (g, r)
 
 
+@pytest.mark.parametrize("name,dim,refinements", [
+    ("advection_diffusion_vortex_mf_inflow_outflow", 2, 5),
+    ("advection_diffusion_vortex_mf_inflow_outflow_3d", 3, 3),
+])
+def test_vortex_inflow_outflow_golden(name, dim, refinements):
+    """Inflow/outflow constraints: every boundary DoF with u . n <= 0 is fixed
+    to -1 after each solve (advection_diffusion_operation.cpp:371-499)."""
+    got = cases.vortex_case(dim, refinements, inflow_outflow=True)
+    ref = GOLDEN[name]["values"]
+    assert len(got) == len(ref) == 5
+    for g, r in zip(got, ref):
+        assert abs(g - r) / r < VORTEX_RTOL, (g, r)
+
+
 def _fmt(v):
     return "%.5e" % v
 
