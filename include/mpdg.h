@@ -163,6 +163,13 @@ mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *device_value
 /* the same with host values, copied into operator-owned device memory */
 mpdg_status mpdg_op_set_field_host(mpdg_op *op, int field, const double *host_values);
 mpdg_status mpdg_op_set_stream(mpdg_op *op, void *cuda_stream);
+/* inflow/outflow constraints of the advection-diffusion operator
+ * (AdvectionDiffusionOperator::set_inflow_outflow_bc / do_pre_vmult /
+ * do_post_vmult, advection_diffusion_operator.cpp:537-578): identity rows at
+ * the flagged DoFs (host mask, n_dofs bytes; NULL clears).  vmult reads src as
+ * 0 there and returns src there; the inverse diagonal is 1 there
+ * (:438-445).  src is not modified (the reference zeroes it in place). */
+mpdg_status mpdg_op_set_inflow_outflow(mpdg_op *op, const uint8_t *host_mask);
 /* reads and clears the operator's device error word: nonzero when a bounded
  * device-side wait (bulk-copy completion) expired; synchronises the stream */
 mpdg_status mpdg_op_device_error(mpdg_op *op, int *flag);

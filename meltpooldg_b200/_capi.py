@@ -111,6 +111,7 @@ def lib():
     L.mpdg_op_use_dirichlet.argtypes = [vp, C.c_int]
     L.mpdg_op_set_field.argtypes = [vp, C.c_int, vp]
     L.mpdg_op_set_stream.argtypes = [vp, vp]
+    L.mpdg_op_set_inflow_outflow.argtypes = [vp, C.POINTER(C.c_uint8)]
     L.mpdg_op_set_field_host.argtypes = [vp, C.c_int, dp]
     L.mpdg_compute_inverse_diagonal_host.argtypes = [vp, dp]
     L.mpdg_create_rhs_host.argtypes = [vp, dp, dp, dp]

@@ -230,7 +230,8 @@ void free_op_arrays(Op &o)
 {
   free_workspace(o);
   for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32,
-                  (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32, (void *)o.d_trig64, o.d_stage})
+                  (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32, (void *)o.d_trig64, o.d_stage,
+                  (void *)o.d_io, o.io_tmp})
     if (p) cudaFree(p);
 }
 }  // namespace
@@ -308,6 +309,27 @@ mpdg_status mpdg_op_device_error(mpdg_op *op, int *flag)
     MPDG_CUDA(cudaStreamSynchronize(op->o.stream));
     MPDG_CUDA(cudaMemcpy(flag, op->o.d_err, sizeof(int), cudaMemcpyDeviceToHost));
     MPDG_CUDA(cudaMemset(op->o.d_err, 0, sizeof(int)));
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_op_set_inflow_outflow(mpdg_op *op, const uint8_t *host_mask)
+{
+  return guarded([&]() -> int {
+    if (!op) throw Error{MPDG_ERR_ARG, "null operator"};
+    Op &o = op->o;
+    if (o.d_io) {
+      MPDG_CUDA(cudaStreamSynchronize(o.stream));
+      cudaFree(o.d_io);
+      o.d_io = nullptr;
+    }
+    if (!host_mask) return MPDG_OK;
+    const long N = o.mesh->N;
+    bool any = false;
+    for (long i = 0; i < N && !any; ++i) any = host_mask[i] != 0;
+    if (!any) return MPDG_OK;
+    MPDG_CUDA(cudaMalloc(&o.d_io, N));
+    MPDG_CUDA(cudaMemcpy(o.d_io, host_mask, N, cudaMemcpyHostToDevice));
     return MPDG_OK;
   });
 }

@@ -131,6 +131,11 @@ struct Op {
   const void *hang_src = nullptr;
   const uint8_t *hang_mask = nullptr;
   long hang_NXc = 0, hang_NYc = 0;  // the coarse lattice the hanging DoFs read from
+  // inflow/outflow constraints (advection_diffusion_operator.cpp:545-578): identity
+  // rows at the flagged DoFs; the source there is read as 0 and copied to the result
+  uint8_t *d_io = nullptr;
+  void *io_tmp = nullptr;
+  size_t io_tmp_bytes = 0;
 };
 
 // ---- batched apply over many solves (batch_apply.cuh / batch.cu)

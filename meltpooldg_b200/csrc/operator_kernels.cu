@@ -1554,11 +1554,48 @@ void launch_fine_block(Op &op, Real *dst, const Real *src)
 
 
 template <typename Real>
+__global__ void io_pre_kernel(Real *tmp, const Real *src, const uint8_t *io, long n)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    tmp[i] = io[i] ? Real(0) : src[i];
+}
+
+template <typename Real>
+__global__ void io_post_kernel(Real *dst, const Real *src, const uint8_t *io, long n)
+{
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    if (io[i]) dst[i] = src[i];
+}
+
+template <typename Real>
 void launch_apply(Op &op, Real *dst, const Real *src)
 {
-  launch_cells<Real>(op, dst, src);
-  launch_robin<Real>(op, dst, src, ROBIN_APPLY);
-  if (op.fine) launch_fine_block<Real>(op, dst, src);
+  const Real *in = src;
+  const long N = op.mesh->N;
+  const unsigned grid = (unsigned)std::min(grid_for(N, 256), (unsigned)(148 * 16));
+  if (op.d_io) {
+    // do_pre_vmult: the constrained entries of src read as 0 (in a copy; the
+    // caller's src is not modified)
+    const size_t bytes = sizeof(Real) * (size_t)N;
+    if (op.io_tmp_bytes < bytes) {
+      if (op.io_tmp) cudaFree(op.io_tmp);
+      op.io_tmp = nullptr;
+      op.io_tmp_bytes = 0;
+      MPDG_CUDA(cudaMalloc(&op.io_tmp, bytes));
+      op.io_tmp_bytes = bytes;
+    }
+    io_pre_kernel<Real><<<grid, 256, 0, op.stream>>>((Real *)op.io_tmp, src, op.d_io, N);
+    MPDG_LAUNCHED();
+    in = (const Real *)op.io_tmp;
+  }
+  launch_cells<Real>(op, dst, in);
+  launch_robin<Real>(op, dst, in, ROBIN_APPLY);
+  if (op.fine) launch_fine_block<Real>(op, dst, in);
+  if (op.d_io) {
+    // do_post_vmult: identity rows
+    io_post_kernel<Real><<<grid, 256, 0, op.stream>>>(dst, src, op.d_io, N);
+    MPDG_LAUNCHED();
+  }
 }
 
 template <typename Real>
@@ -1740,6 +1777,10 @@ void launch_invert_diagonal(Op &op, double *diag)
   }
   invert_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, constraint_mask(op), thr);
   MPDG_LAUNCHED();
+  if (op.d_io) {  // advection_diffusion_operator.cpp:438-445
+    set_masked_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, op.d_io, 1.0);
+    MPDG_LAUNCHED();
+  }
 }
 
 void launch_invert_with_threshold(Op &op, double *diag, double thr)

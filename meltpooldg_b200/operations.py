@@ -23,11 +23,22 @@ from .operators import (AdvectionDiffusionOperator, HeatDiffuseOperator, LinearS
 
 
 class AdvectionDiffusionOperation:
+    """`inflow_outflow` = (mask, values): DoFs fixed to values after each solve
+    through identity rows of the operator instead of Dirichlet constraints
+    (create_inflow_outflow_constraints and solve,
+    advection_diffusion_operation.cpp:227-294, 371-499)."""
+
     def __init__(self, mesh, dt, theta=0.5, diffusivity=0.0, velocity=None, dirichlet_values=None,
-                 linear_solver: LinearSolverData = None, device="cuda"):
+                 linear_solver: LinearSolverData = None, device="cuda", inflow_outflow=None):
         self.mesh = mesh
         self.op = AdvectionDiffusionOperator(mesh, dt, theta=theta, diffusivity=diffusivity,
                                              velocity=velocity)
+        self.io = None
+        if inflow_outflow is not None:
+            io_mask, io_vals = inflow_outflow
+            io_mask = np.asarray(io_mask, np.uint8)
+            self.io = (torch.tensor(io_mask.astype(bool), device=device),
+                       torch.tensor(np.where(io_mask == 1, np.asarray(io_vals, np.float64), 0.0), device=device))
         self.data = linear_solver or LinearSolverData(solver_type="GMRES", preconditioner_type="Diagonal")
         self.device = device
         N = mesh.n_dofs
@@ -49,16 +60,28 @@ class AdvectionDiffusionOperation:
         op = self.op
         old = self.solution.clone()
         rhs = torch.empty_like(old)
+        bc = self.bc_values
+        if self.io is not None:
+            # the lifting includes the inflow values; the identity rows are off
+            # while it is computed (utilities_matrixfree.hpp:39-101)
+            bc = bc.clone()
+            bc[self.io[0]] = self.io[1][self.io[0]]
+            op.set_inflow_outflow(None)
         op.reset_dof_index(with_dirichlet=False)
-        op.vmult(rhs, self.bc_values)
+        op.vmult(rhs, bc)
         rhs.neg_()
         op.create_rhs(rhs, old)
         op.reset_dof_index(with_dirichlet=True)
         rhs[self.mask] = 0.0
+        if self.io is not None:
+            rhs[self.io[0]] = 0.0
+            op.set_inflow_outflow(self.io[0].cpu().numpy().astype(np.uint8))
         x = old.clone()
         it = LinearSolver.solve(op, x, rhs, self.data)
         self.iterations.append(it)
         x[self.mask] = self.bc_values[self.mask]
+        if self.io is not None:
+            x[self.io[0]] = self.io[1][self.io[0]]
         self.solution = x
         return x
 

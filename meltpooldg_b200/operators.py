@@ -265,6 +265,17 @@ class AdvectionDiffusionOperator(_MatrixFreeOperator):
                      (C.c_double * 3)(*vp), 0)
         super().__init__(mesh, d, precisions)
 
+    def set_inflow_outflow(self, mask):
+        """Identity rows at the flagged DoFs (set_inflow_outflow_bc +
+        do_pre_vmult/do_post_vmult, advection_diffusion_operator.cpp:537-578);
+        None clears."""
+        if mask is None:
+            A.check(A.lib().mpdg_op_set_inflow_outflow(self._h, None), "set_inflow_outflow")
+            return
+        m = np.ascontiguousarray(mask, np.uint8)
+        A.check(A.lib().mpdg_op_set_inflow_outflow(self._h, m.ctypes.data_as(C.POINTER(C.c_uint8))),
+                "set_inflow_outflow")
+
     def create_rhs(self, dst, src):
         """dst += phi_old/dt N - (1-theta) vel.grad phi_old N - (1-theta) D grad phi_old.grad N
         (advection_diffusion_operator.cpp:276-358)."""

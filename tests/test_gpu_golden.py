@@ -65,3 +65,22 @@ def test_unidirectional_heat_convection_golden_on_gpu(cuda):
         opn.solve()
         got.append("%.5e" % opn.l2_norm())
     assert got == GOLDEN["unidirectional_heat_transfer_with_convection"]["printed"]
+
+
+@pytest.mark.parametrize("name", ["advection_diffusion_vortex_mf_inflow_outflow_3d"])
+def test_vortex_inflow_outflow_golden_on_gpu(cuda, name):
+    """advection_diffusion_vortex_mf_inflow_outflow_3d: the u . n <= 0 boundary
+    DoFs carry identity rows in the operator (mpdg_op_set_inflow_outflow) and are
+    set to -1 after each solve; no Dirichlet constraints."""
+    import meltpooldg_b200 as M
+    from meltpooldg_b200.operations import AdvectionDiffusionOperation
+    from oracle import cases
+    om, phi0, _ = cases.vortex_setup(3, 3)
+    io = cases.vortex_io_mask(om, 4.0)
+    mesh = M.Mesh(om.vert, (8, 8, 8), 1, None)
+    opn = AdvectionDiffusionOperation(mesh, 0.01, theta=0.5, diffusivity=0.0, velocity=("rotation", 4.0),
+                                      inflow_outflow=(io, np.full(mesh.n_dofs, -1.0)))
+    opn.set_initial_condition(phi0)
+    for r in GOLDEN[name]["values"]:
+        opn.solve()
+        assert abs(opn.l2_norm() - r) / r < 5e-8

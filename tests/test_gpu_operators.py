@@ -166,6 +166,40 @@ def test_heat_robin_faces(cuda, p):
     assert relerr(rhs.cpu().numpy(), ref) < TOL64
 
 
+def test_inflow_outflow_identity_rows(cuda):
+    """Identity rows (do_pre_vmult / do_post_vmult): src read as 0 at the
+    flagged DoFs, result there equal to src; inverse diagonal 1 there."""
+    import torch
+    import meltpooldg_b200 as M
+    nc, p = (4, 3, 3), 2
+    gm, om = meshes(nc, p, 0.1, seed=9)
+    R = rng(77)
+    io = (R.uniform(size=gm.n_dofs) < 0.2).astype(np.uint8)
+    src = R.uniform(-1, 1, gm.n_dofs)
+    op = M.AdvectionDiffusionOperator(gm, 1e-2, theta=0.5, diffusivity=0.02, velocity="vortex",
+                                      precisions=("fp64", "fp32"))
+    oop = O.Operator(O.ADVDIFF, 1e-2, theta=0.5, diffusivity=0.02, vel_kind=O.VEL_VORTEX)
+    ref = O.vmult(om, oop, np.where(io == 1, 0.0, src))
+    ref[io == 1] = src[io == 1]
+    d_src = dev(src)
+    op.set_inflow_outflow(io)
+    dst = torch.empty_like(d_src)
+    op.vmult(dst, d_src)
+    assert relerr(dst.cpu().numpy(), ref) < TOL64
+    assert torch.equal(d_src, dev(src))  # src is not modified
+    d32 = torch.empty(gm.n_dofs, dtype=torch.float32, device="cuda")
+    op.vmult(d32, dev(src, torch.float32))
+    assert relerr(d32.double().cpu().numpy(), ref) < TOL32
+    inv = torch.empty_like(d_src)
+    op.compute_inverse_diagonal_from_matrixfree(inv)
+    want = O.inverse_diagonal(om, oop)
+    want[io == 1] = 1.0
+    assert relerr(inv.cpu().numpy(), want) < TOL64
+    op.set_inflow_outflow(None)
+    op.vmult(dst, d_src)
+    assert relerr(dst.cpu().numpy(), O.vmult(om, oop, src)) < TOL64
+
+
 def test_c1_vmult_full_size(cuda):
     """Config 1: 16^3 Q2 unit cube, Dirichlet on all faces, src ~ U[-1,1] seed 0."""
     import torch
