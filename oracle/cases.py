@@ -109,13 +109,14 @@ def vortex_setup(dim, refinements, degree=1):
 
 
 def vortex_case(dim, refinements, n_steps=5, dt=0.01, velocity_scale=4.0, theta=0.5,
-                diffusivity=0.0, solver=None, inflow_outflow=False):
+                diffusivity=0.0, solver=None, inflow_outflow=False, supg=False):
     """Returns the per-step integrated L2 norms.  `solver(op, rhs, x0, inv)` can
     replace the oracle GMRES (used to drive the GPU path through the same case).
     With `inflow_outflow` the constrained set is the u . n <= 0 boundary DoFs and
     the initial field keeps its values there until the first solve sets them
     (the constraint is applied after each solve,
-    advection_diffusion_operation.cpp:286-294)."""
+    advection_diffusion_operation.cpp:286-294).  `supg` switches on the SUPG
+    terms with the automatic parameter h_K / max |u| (coefficient -1)."""
     mesh, phi, mask = vortex_setup(dim, refinements)
     phi = phi.copy()
     if inflow_outflow:
@@ -123,7 +124,7 @@ def vortex_case(dim, refinements, n_steps=5, dt=0.01, velocity_scale=4.0, theta=
     else:
         phi[mask == 1] = -1.0
     op_nobc = O.Operator(O.ADVDIFF, dt, theta=theta, diffusivity=diffusivity,
-                         vel_kind=O.VEL_ROTATION, vel_param=(velocity_scale, 0.0, 0.0))
+                         vel_kind=O.VEL_ROTATION, vel_param=(velocity_scale, 0.0, 0.0), supg=supg)
     op = op_nobc.with_dirichlet(mask)
     bc = np.where(mask == 1, -1.0, 0.0)
     norms = []

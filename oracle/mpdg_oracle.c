@@ -112,6 +112,10 @@ typedef struct {
   long n_cells;
   double xq[MAXN], wq[MAXN];
   double S[MAXN * MAXN], D[MAXN * MAXN];
+  /* Dc[q*n+r]: derivative of the Lagrange polynomial r on the Gauss points at
+   * x_q (exact on values of degree < n); D2 = Dc D: second derivatives of the
+   * Gauss-Lobatto basis at the Gauss points */
+  double Dc[MAXN * MAXN], D2[MAXN * MAXN];
 } geo_t;
 
 static void geo_init(const orc_mesh *m, geo_t *g)
@@ -129,6 +133,25 @@ static void geo_init(const orc_mesh *m, geo_t *g)
   g->n_cells = (long)g->nc[0] * g->nc[1] * g->nc[2];
   orc_gauss_legendre(g->n, g->xq, g->wq);
   orc_shape_tables(g->n, g->xq, g->n, g->S, g->D);
+  const int n = g->n;
+  for (int q = 0; q < n; ++q)
+    for (int r = 0; r < n; ++r) {
+      double d = 0.0;
+      for (int k = 0; k < n; ++k) {
+        if (k == r) continue;
+        double t = 1.0 / (g->xq[r] - g->xq[k]);
+        for (int j = 0; j < n; ++j)
+          if (j != r && j != k) t *= (g->xq[q] - g->xq[j]) / (g->xq[r] - g->xq[j]);
+        d += t;
+      }
+      g->Dc[q * n + r] = d;
+    }
+  for (int q = 0; q < n; ++q)
+    for (int i = 0; i < n; ++i) {
+      double s2 = 0.0;
+      for (int r = 0; r < n; ++r) s2 += g->Dc[q * n + r] * g->D[r * n + i];
+      g->D2[q * n + i] = s2;
+    }
 }
 
 long orc_n_dofs(const orc_mesh *m)
@@ -400,6 +423,55 @@ static void tangent_qp(const orc_op *op, int dim, const qdata_t *qd, double u, c
 
 static int cell_colour(int ix, int iy, int iz) { return (ix & 1) | ((iy & 1) << 1) | ((iz & 1) << 2); }
 
+/* SUPG parameter of a cell (compute_stabilization_parameter,
+ * advection_diffusion_operator.cpp:499-533; cell size = diameter / sqrt(dim),
+ * scratch_data.cpp:249-266) */
+static double cell_tau(const orc_mesh *m, const orc_op *op, const geo_t *g, int ix, int iy, int iz,
+                       const qdata_t *qd)
+{
+  if (!op->supg || op->kind != ORC_ADVDIFF) return 0.0;
+  const int dim = g->dim, nqt = g->n * g->n * ((dim == 3) ? g->n : 1);
+  double vc[8][3];
+  cell_vertices(m, g, ix, iy, iz, vc);
+  const int pairs3[4][2] = {{0, 7}, {1, 6}, {2, 5}, {3, 4}}, pairs2[2][2] = {{0, 3}, {1, 2}};
+  double diam = 0.0;
+  for (int k = 0; k < ((dim == 3) ? 4 : 2); ++k) {
+    const int a = (dim == 3) ? pairs3[k][0] : pairs2[k][0], b = (dim == 3) ? pairs3[k][1] : pairs2[k][1];
+    double d2 = 0.0;
+    for (int c = 0; c < dim; ++c) d2 += (vc[a][c] - vc[b][c]) * (vc[a][c] - vc[b][c]);
+    diam = fmax(diam, sqrt(d2));
+  }
+  const double h = diam / sqrt((double)dim);
+  if (op->supg_coefficient >= 0.0) return op->supg_coefficient * h;
+  double umax = 0.0;
+  for (int q = 0; q < nqt; ++q) {
+    double s2 = 0.0;
+    for (int a = 0; a < dim; ++a) s2 += qd[q].vel[a] * qd[q].vel[a];
+    umax = fmax(umax, sqrt(s2));
+  }
+  return (umax >= 1e-6) ? h / umax : 0.0;
+}
+
+/* physical Laplacian at the quadrature points from the reference gradients
+ * (axis-aligned cells: J^-1 diagonal) */
+static void laplacian_qp(const geo_t *g, double ug[3][MAXN3], const qdata_t *qd, double *lap)
+{
+  const int dim = g->dim, nqt = g->n * g->n * ((dim == 3) ? g->n : 1);
+  double t[MAXN3];
+  for (int q = 0; q < nqt; ++q) lap[q] = 0.0;
+  for (int d = 0; d < dim; ++d) {
+    contract(g, g->Dc, 0, d, ug[d], t);
+    for (int q = 0; q < nqt; ++q) {
+      for (int e = 0; e < dim; ++e)
+        if (e != d && (fabs(qd[q].Ji[d][e]) > 1e-12 * fabs(qd[q].Ji[d][d]))) {
+          fprintf(stderr, "orc: SUPG with diffusion needs axis-aligned cells\n");
+          abort();
+        }
+      lap[q] += qd[q].Ji[d][d] * qd[q].Ji[d][d] * t[q];
+    }
+  }
+}
+
 /* one cell of the sum-factorised tangent; adds into dst (caller guarantees no race) */
 static void apply_cell(const orc_mesh *m, const orc_op *op, const geo_t *g, int ix, int iy,
                        int iz, double *dst, const double *src)
@@ -409,15 +481,22 @@ static void apply_cell(const orc_mesh *m, const orc_op *op, const geo_t *g, int 
   cell_dofs(g, ix, iy, iz, idx);
   static __thread qdata_t qd[MAXN3];
   cell_qdata(m, op, g, ix, iy, iz, idx, qd);
-  double ul[MAXN3], uv[MAXN3], ug[3][MAXN3], out[MAXN3];
+  double ul[MAXN3], uv[MAXN3], ug[3][MAXN3], out[MAXN3], lap[MAXN3];
   for (int t = 0; t < nqt; ++t)
     ul[t] = (op->dirichlet && op->dirichlet[idx[t]]) ? 0.0 : src[idx[t]];
   evaluate(g, ul, uv, ug);
+  const double tau = cell_tau(m, op, g, ix, iy, iz, qd);
+  const int supg = op->supg && op->kind == ORC_ADVDIFF;
+  if (supg && op->diffusivity != 0.0) laplacian_qp(g, ug, qd, lap);
   for (int q = 0; q < nqt; ++q) {
     double gu[3] = {0, 0, 0}, v, f[3];
     for (int a = 0; a < dim; ++a)
       for (int b = 0; b < dim; ++b) gu[a] += qd[q].Ji[b][a] * ug[b][q];
     tangent_qp(op, dim, &qd[q], uv[q], gu, &v, f);
+    if (supg) {
+      const double r = v - ((op->diffusivity != 0.0) ? op->theta * op->diffusivity * lap[q] : 0.0);
+      for (int a = 0; a < dim; ++a) f[a] += tau * qd[q].vel[a] * r;
+    }
     uv[q] = v * qd[q].JxW;
     for (int b = 0; b < dim; ++b) {
       double s = 0.0;
@@ -562,6 +641,14 @@ static void element_matrix(const orc_mesh *m, const orc_op *op, const geo_t *g, 
   cell_vertices(m, g, ix, iy, iz, vc);
   memset(A, 0, sizeof(double) * nqt * nqt);
   static __thread double phi[MAXN3], gphi[MAXN3][3];
+  double tau = 0.0;
+  if (op->supg && op->kind == ORC_ADVDIFF) {
+    static __thread qdata_t qdc[MAXN3];
+    orc_op plain = *op;
+    plain.temperature = NULL;
+    cell_qdata(m, &plain, g, ix, iy, iz, idx, qdc);
+    tau = cell_tau(m, op, g, ix, iy, iz, qdc);
+  }
   for (int qz = 0; qz < nz; ++qz)
     for (int qy = 0; qy < n; ++qy)
       for (int qx = 0; qx < n; ++qx) {
@@ -610,6 +697,19 @@ static void element_matrix(const orc_mesh *m, const orc_op *op, const geo_t *g, 
         for (int j = 0; j < nqt; ++j) {
           double v, fl[3];
           tangent_qp(op, dim, &qd, phi[j], gphi[j], &v, fl);
+          if (op->supg && op->kind == ORC_ADVDIFF) {
+            /* Laplacian of basis j (axis-aligned cells) */
+            int c[3] = {j % n, (j / n) % n, j / (n * n)};
+            double lapj = 0.0;
+            for (int d = 0; d < dim; ++d) {
+              double pr = qd.Ji[d][d] * qd.Ji[d][d] * g->D2[qq[d] * n + c[d]];
+              for (int e = 0; e < dim; ++e)
+                if (e != d) pr *= g->S[qq[e] * n + c[e]];
+              lapj += pr;
+            }
+            const double r = v - op->theta * op->diffusivity * lapj;
+            for (int a = 0; a < dim; ++a) fl[a] += tau * qd.vel[a] * r;
+          }
           for (int i = 0; i < nqt; ++i)
             A[i * nqt + j] += (v * phi[i] + fl[0] * gphi[i][0] + fl[1] * gphi[i][1] +
                                fl[2] * gphi[i][2]) * qd.JxW;
@@ -782,20 +882,28 @@ void orc_rhs_advdiff(const orc_mesh *m, const orc_op *op, double *dst, const dou
       cell_dofs(&g, ix, iy, iz, idx);
       static __thread qdata_t qd[MAXN3];
       cell_qdata(m, &op2, &g, ix, iy, iz, idx, qd);
-      double ul[MAXN3], uv[MAXN3], ug[3][MAXN3], out[MAXN3];
+      double ul[MAXN3], uv[MAXN3], ug[3][MAXN3], out[MAXN3], lap[MAXN3];
       for (int t = 0; t < nqt; ++t) ul[t] = phi_old[idx[t]];
       evaluate(&g, ul, uv, ug);
+      const int supg = op->supg && op->kind == ORC_ADVDIFF;
+      const double tau = cell_tau(m, op, &g, ix, iy, iz, qd);
+      if (supg && op->diffusivity != 0.0) laplacian_qp(&g, ug, qd, lap);
       for (int q = 0; q < nqt; ++q) {
         double gp[3] = {0, 0, 0}, vg = 0.0;
         for (int a = 0; a < dim; ++a) {
           for (int b = 0; b < dim; ++b) gp[a] += qd[q].Ji[b][a] * ug[b][q];
           vg += qd[q].vel[a] * gp[a];
         }
-        uv[q] = (uv[q] / op->dt - (1.0 - op->theta) * vg) * qd[q].JxW;
+        const double res = uv[q] / op->dt - (1.0 - op->theta) * vg;
+        uv[q] = res * qd[q].JxW;
+        /* SUPG: tau vel (res + (1 - theta) D lap) tested with grad N */
+        const double rs = supg ? res + ((op->diffusivity != 0.0) ? (1.0 - op->theta) * op->diffusivity * lap[q] : 0.0)
+                               : 0.0;
         for (int b = 0; b < dim; ++b) {
           double s = 0.0;
-          for (int a = 0; a < dim; ++a) s += qd[q].Ji[b][a] * gp[a];
-          ug[b][q] = -(1.0 - op->theta) * op->diffusivity * s * qd[q].JxW;
+          for (int a = 0; a < dim; ++a)
+            s += qd[q].Ji[b][a] * (-(1.0 - op->theta) * op->diffusivity * gp[a] + (supg ? tau * qd[q].vel[a] * rs : 0.0));
+          ug[b][q] = s * qd[q].JxW;
         }
       }
       memset(out, 0, sizeof(double) * nqt);

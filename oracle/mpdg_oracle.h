@@ -68,6 +68,11 @@ typedef struct {
   const double *vel_nodal;
   /* homogeneous Dirichlet mask: constrained DoFs are read as 0 and never written */
   const unsigned char *dirichlet;
+  /* advection-diffusion SUPG (advection_diffusion_operator.cpp:450-533): flux
+   * += tau_K vel (residual), tau_K = h_K / max_q |vel| (coefficient < 0) or
+   * coefficient h_K, h_K = cell diameter / sqrt(dim); axis-aligned cells */
+  int supg;
+  double supg_coefficient;
 } orc_op;
 
 typedef struct {

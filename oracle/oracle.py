@@ -37,6 +37,7 @@ class _Op(C.Structure):
         ("theta", C.c_double), ("diffusivity", C.c_double),
         ("vel_kind", C.c_int), ("vel_param", C.c_double * 3), ("vel_nodal", _dp),
         ("dirichlet", _u8p),
+        ("supg", C.c_int), ("supg_coefficient", C.c_double),
     ]
 
 
@@ -167,7 +168,7 @@ class Operator:
     def __init__(self, kind, dt, rho_cp=1.0, k0=1.0, k_alpha=0.0, full_tangent=False,
                  temperature=None, robin_alpha=0.0, robin_t_inf=0.0, robin_faces=0,
                  theta=0.5, diffusivity=0.0, vel_kind=VEL_NONE, vel_param=(0.0, 0.0, 0.0),
-                 vel_nodal=None, dirichlet=None):
+                 vel_nodal=None, dirichlet=None, supg=False, supg_coefficient=-1.0):
         self.temperature = None if temperature is None else np.ascontiguousarray(temperature, np.float64)
         self.vel_nodal = None if vel_nodal is None else np.ascontiguousarray(vel_nodal, np.float64)
         self.dirichlet = None if dirichlet is None else np.ascontiguousarray(dirichlet, np.uint8)
@@ -175,11 +176,12 @@ class Operator:
         self._c = _Op(kind, dt, rho_cp, k0, k_alpha, int(full_tangent), _ptr(self.temperature),
                       robin_alpha, robin_t_inf, robin_faces, theta, diffusivity, vel_kind,
                       (C.c_double * 3)(*vel_param), _ptr(self.vel_nodal),
-                      _ptr(self.dirichlet, _u8p))
+                      _ptr(self.dirichlet, _u8p), int(bool(supg)), float(supg_coefficient))
         self.params = dict(kind=kind, dt=dt, rho_cp=rho_cp, k0=k0, k_alpha=k_alpha,
                            full_tangent=full_tangent, robin_alpha=robin_alpha,
                            robin_t_inf=robin_t_inf, robin_faces=robin_faces, theta=theta,
-                           diffusivity=diffusivity, vel_kind=vel_kind, vel_param=vel_param)
+                           diffusivity=diffusivity, vel_kind=vel_kind, vel_param=vel_param, supg=supg,
+                           supg_coefficient=supg_coefficient)
 
     def with_dirichlet(self, mask):
         p = dict(self.params)

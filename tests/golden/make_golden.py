@@ -26,6 +26,9 @@ CASES = {
     "advection_diffusion_vortex_mf_inflow_outflow": (
         "applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf_inflow_outflow.mpirun=4.output",
         r"\|\| advected field \|\|L2 = ([0-9.eE+-]+)"),
+    "advection_diffusion_vortex_mf_supg": (
+        "applications/mp-advec-diff/cases/tests/advection_diffusion_vortex_mf_supg.mpirun=4.output",
+        r"\|\| advected field \|\|L2 = ([0-9.eE+-]+)"),
     "unidirectional_heat_transfer": (
         "applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/"
         "unidirectional_heat_transfer.mpirun=4.output",

@@ -44,6 +44,16 @@ def test_vortex_inflow_outflow_golden(name, dim, refinements):
         assert abs(g - r) / r < VORTEX_RTOL, (g, r)
 
 
+def test_vortex_supg_golden():
+    """SUPG stabilisation with the automatic parameter h_K / max_q |u|
+    (advection_diffusion_operator.cpp:450-533)."""
+    got = cases.vortex_case(2, 5, supg=True)
+    ref = GOLDEN["advection_diffusion_vortex_mf_supg"]["values"]
+    assert len(got) == len(ref) == 5
+    for g, r in zip(got, ref):
+        assert abs(g - r) / r < VORTEX_RTOL, (g, r)
+
+
 def _fmt(v):
     return "%.5e" % v
 
