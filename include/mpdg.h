@@ -83,6 +83,15 @@ typedef struct {
    * (side 0: the low face, 1: the high face); 0 = none */
   double robin_alpha, robin_t_inf;
   int robin_faces;
+  /* advection-diffusion: SUPG stabilisation (AdvectionDiffusionData::conv_stab,
+   * advection_diffusion_operator.cpp:276-358, 450-533): the flux gains
+   * tau_K u (u/dt + theta u.grad u - theta D lap u) (right-hand side:
+   * tau_K u (phi/dt - (1-theta) u.grad phi + (1-theta) D lap phi)), with
+   * tau_K = supg_coefficient h_K, or h_K / max_q |u| when supg_coefficient < 0,
+   * h_K = cell diameter / sqrt(3).  With diffusion the cells must be axis-aligned
+   * boxes.  The diagonal is built by probing (n^3 applies). */
+  int supg;
+  double supg_coefficient;
 } mpdg_op_desc;
 
 typedef struct {

@@ -50,7 +50,8 @@ class OpDesc(C.Structure):
                 ("k_alpha", C.c_double), ("full_tangent", C.c_int), ("theta", C.c_double),
                 ("diffusivity", C.c_double), ("vel_kind", C.c_int), ("vel_param", C.c_double * 3),
                 ("precision_mask", C.c_int), ("robin_alpha", C.c_double),
-                ("robin_t_inf", C.c_double), ("robin_faces", C.c_int)]
+                ("robin_t_inf", C.c_double), ("robin_faces", C.c_int), ("supg", C.c_int),
+                ("supg_coefficient", C.c_double)]
 
 
 class SolverDesc(C.Structure):

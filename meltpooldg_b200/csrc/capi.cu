@@ -154,6 +154,19 @@ void free_mesh_arrays(Mesh &m)
                   (void *)m.d_cell_flags, (void *)m.d_cell_mask, (void *)m.d_tmask_dir, (void *)m.d_tmask_hang})
     if (p) cudaFree(p);
 }
+
+// every vertex is (X[a], Y[b], Z[c]): all cells are axis-aligned boxes
+bool axis_aligned_lattice(const Mesh &m)
+{
+  const long V0 = m.nc[0] + 1, V1 = m.nc[1] + 1, V2 = m.nc[2] + 1;
+  const auto at = [&](long a, long b, long c, int d) { return m.vertices[(size_t)(((c * V1 + b) * V0 + a) * 3 + d)]; };
+  for (long c = 0; c < V2; ++c)
+    for (long b = 0; b < V1; ++b)
+      for (long a = 0; a < V0; ++a)
+        if (at(a, b, c, 0) != at(a, 0, 0, 0) || at(a, b, c, 1) != at(0, b, 0, 1) || at(a, b, c, 2) != at(0, 0, c, 2))
+          return false;
+  return true;
+}
 }  // namespace
 
 mpdg_status mpdg_mesh_destroy(mpdg_mesh *mesh)
@@ -194,6 +207,12 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     if (mm.fine && (desc->k_alpha != 0.0 || desc->full_tangent || (desc->robin_faces && desc->robin_alpha != 0.0)))
       throw Error{MPDG_ERR_UNSUPPORTED,
                   "two-level meshes take constant coefficients: no k(T) law, full tangent or Robin faces"};
+    if (desc->supg && desc->kind != MPDG_OP_ADVDIFF)
+      throw Error{MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator"};
+    if (desc->supg && mm.fine) throw Error{MPDG_ERR_UNSUPPORTED, "SUPG on two-level meshes"};
+    if (desc->supg && desc->diffusivity != 0.0 && !mm.uniform && !axis_aligned_lattice(mm))
+      throw Error{MPDG_ERR_UNSUPPORTED,
+                  "SUPG with diffusion needs axis-aligned cells (its Laplacian drops the Jacobian derivatives)"};
     auto *h = new mpdg_op();
     Op &o = h->o;
     o.mesh = &mm;
@@ -231,6 +250,7 @@ void free_op_arrays(Op &o)
   free_workspace(o);
   for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32,
                   (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32, (void *)o.d_trig64, o.d_stage,
+                  (void *)o.d_tau64, (void *)o.d_tau32,
                   (void *)o.d_io, o.io_tmp})
     if (p) cudaFree(p);
 }

@@ -114,6 +114,8 @@ struct Op {
   double *d_velb64 = nullptr;          // general geometry + velocity: [cell][3][n^3]
   float *d_velb32 = nullptr;
   float *d_trig32 = nullptr;           // uniform vortex velocity: sin/cos tables
+  double *d_tau64 = nullptr;           // SUPG: tau_K per colour-major cell
+  float *d_tau32 = nullptr;
   double *d_trig64 = nullptr;
   Workspace *ws = nullptr;
   int *d_err = nullptr;                // device error word (bounded waits that expired)

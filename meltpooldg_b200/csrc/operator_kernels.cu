@@ -177,7 +177,9 @@ void shape_1d(int p, double *S, double *D, double *w, double *x)
 
 // ------------------------------------------------------------ kernel params
 
-enum { MODE_LINEAR = 0, MODE_HEAT_RESIDUAL = 1 };
+// MODE_SUPG: MODE_LINEAR plus the advection-diffusion SUPG flux
+// tau_K u (c_mass u + c_vel u.grad u - c_diff lap u) (advection_diffusion_operator.cpp:450-495)
+enum { MODE_LINEAR = 0, MODE_HEAT_RESIDUAL = 1, MODE_SUPG = 2 };
 enum { GEOM_UNIFORM = 0, GEOM_GENERAL = 1 };
 
 template <typename Real>
@@ -189,6 +191,8 @@ struct KP {
   const Real *metric;     // GENERAL: [cell][7][n^3] = JxW, G00 G01 G02 G11 G12 G22
   const Real *velb;       // GENERAL + velocity: [cell][3][n^3] = JxW J^-1 u
   const Real *trig;       // UNIFORM vortex: sin(pi x), cos(pi x), sin(pi y), cos(pi y)
+  const Real *tau;        // SUPG: per colour-major cell tau_K
+  int supg_lap;           // SUPG with diffusion: the Laplacian term (axis-aligned cells)
   const uint8_t *dmask;
   const uint8_t *cell_flags;
   const uint4 *cell_mask;
@@ -391,7 +395,7 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
     Real v = 0;
     if (active) {
       v = p.src[g0 + k * zs];
-      if (MODE == MODE_LINEAR && p.masked_read && bflag && p.dmask[g0 + k * zs]) v = 0;
+      if (MODE != MODE_HEAT_RESIDUAL && p.masked_read && bflag && p.dmask[g0 + k * zs]) v = 0;
     }
     u[k] = v;
   }
@@ -424,6 +428,19 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
   } else {
     to_qp<n>(sS, t0, i, j, u, uq);
     grad_qp<n>(sDc, t0, i, j, uq, gx, gy, gz);
+  }
+
+  // SUPG with diffusion: second reference derivatives d2/dxi_d^2 at the Gauss
+  // points, by collocation differentiation of the gradient along its own axis
+  Real gxx[n], gyy[n], gzz[n];
+  if (MODE == MODE_SUPG && p.supg_lap) {
+    put<n>(t0, i, j, gx);
+    put<n>(t1, i, j, gy);
+    __syncthreads();
+    cx<n, Real, false>(sDc, t0, i, j, gxx);
+    cy<n, Real, false>(sDc, t1, i, j, gyy);
+    cz<n, Real, false>(sDc, gz, gzz);
+    __syncthreads();
   }
 
   // quadrature-point kernel
@@ -489,6 +506,23 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
       fx[k] = kq * f0;
       fy[k] = kq * f1;
       fz[k] = kq * f2;
+      if (MODE == MODE_SUPG) {
+        // tau_K u r tested with grad N: reference flux tau_K r JxW J^-1 u = tau_K r b,
+        // with u.grad u = adv / JxW and, on axis-aligned cells,
+        // lap u = sum_d (J^-1)_dd^2 d2u/dxi_d^2 = sum_d G_dd / JxW d2u/dxi_d^2
+        const Real tau = active ? p.tau[cell] : Real(0);
+        Real r = p.c_mass * uq[k] + p.c_vel * adv / JxW;
+        if (p.supg_lap) {
+          const Real lap = (GEOM == GEOM_GENERAL)
+                               ? (G00 * gxx[k] + G11 * gyy[k] + G22 * gzz[k]) / JxW
+                               : p.ih2[0] * gxx[k] + p.ih2[1] * gyy[k] + p.ih2[2] * gzz[k];
+          r -= p.c_diff * lap;
+        }
+        const Real tr = tau * r;
+        fx[k] += tr * b0;
+        fy[k] += tr * b1;
+        fz[k] += tr * b2;
+      }
       if (KT && p.full_tangent) {
         // dk/dT grad T du, tested with grad N: G (reference grad T) scaled by u
         const Real dk = p.c_diff * p.k_alpha * uq[k];
@@ -854,6 +888,91 @@ __global__ void velb_kernel(const double *vert, int nc0, int nc1, int nc2, int P
   }
 }
 
+// per colour-major cell: the SUPG parameter tau_K (compute_stabilization_parameter,
+// advection_diffusion_operator.cpp:499-533): coefficient h_K, or, for a negative
+// coefficient, h_K / max_q |u(x_q)| (0 when that maximum is below 1e-6), with the
+// cell size h_K = diameter / sqrt(3) (scratch_data.cpp:249-266); the diameter of
+// a hexahedron is its longest main diagonal
+__global__ void tau_kernel(const double *vert, int nc0, int nc1, int nc2, int P, const Colour *colours,
+                           int vel_kind, double s0, double s1, double s2, double coef, const double *xq_all,
+                           double *tau64, float *tau32)
+{
+  const int n = P + 1;
+  const long cell = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long n_cells = (long)nc0 * nc1 * nc2;
+  if (cell >= n_cells) return;
+  int c = 0;
+  while (c < 7 && cell >= colours[c + 1].first) ++c;
+  const Colour &C = colours[c];
+  const long cidx = cell - C.first;
+  const int ix = 2 * (int)(cidx % C.cn[0]) + C.par[0];
+  const int iy = 2 * (int)((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
+  const int iz = 2 * (int)(cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
+  double V[8][3];
+  for (int v = 0; v < 8; ++v) {
+    const long vid = ((long)(iz + ((v >> 2) & 1)) * (nc1 + 1) + (iy + ((v >> 1) & 1))) * (nc0 + 1) + (ix + (v & 1));
+    for (int a = 0; a < 3; ++a) V[v][a] = vert[vid * 3 + a];
+  }
+  double diam = 0.0;
+  for (int d = 0; d < 4; ++d) {
+    double s = 0.0;
+    for (int a = 0; a < 3; ++a) s += (V[d][a] - V[7 - d][a]) * (V[d][a] - V[7 - d][a]);
+    diam = fmax(diam, sqrt(s));
+  }
+  const double h = diam / sqrt(3.0);
+  double tau;
+  if (coef >= 0.0) {
+    tau = coef * h;
+  } else {
+    double umax = 0.0;
+    for (int q = 0; q < n * n * n; ++q) {
+      const double xi[3] = {xq_all[q % n], xq_all[(q / n) % n], xq_all[q / (n * n)]};
+      double x[3] = {0, 0, 0};
+      for (int v = 0; v < 8; ++v) {
+        const double B = ((v & 1) ? xi[0] : 1 - xi[0]) * (((v >> 1) & 1) ? xi[1] : 1 - xi[1]) *
+                         (((v >> 2) & 1) ? xi[2] : 1 - xi[2]);
+        for (int a = 0; a < 3; ++a) x[a] += V[v][a] * B;
+      }
+      double u[3] = {0, 0, 0};
+      if (vel_kind == MPDG_VEL_VORTEX) {
+        u[0] = sin(M_PI * x[0]) * cos(M_PI * x[1]);
+        u[1] = -cos(M_PI * x[0]) * sin(M_PI * x[1]);
+      } else if (vel_kind == MPDG_VEL_ROTATION) {
+        u[0] = s0 * x[2];
+        u[2] = -s0 * x[0];
+      } else if (vel_kind == MPDG_VEL_CONST) {
+        u[0] = s0;
+        u[1] = s1;
+        u[2] = s2;
+      }
+      umax = fmax(umax, sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]));
+    }
+    tau = (umax >= 1e-6) ? h / umax : 0.0;
+  }
+  tau64[cell] = tau;
+  if (tau32) tau32[cell] = (float)tau;
+}
+
+// probing of the diagonal: x = 1 at the DoFs of one residue class (X, Y, Z) mod
+// n = (a, b, c), else 0.  Two such DoFs are n apart in some direction and share
+// no cell, so A x holds each probed DoF's exact diagonal entry there.
+__global__ void lattice_probe_kernel(double *x, long N, long NX, long NY, int n, int a, int b, int c)
+{
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (long)gridDim.x * blockDim.x) {
+    const long X = g % NX, Y = (g / NX) % NY, Z = g / (NX * NY);
+    x[g] = (X % n == a && Y % n == b && Z % n == c) ? 1.0 : 0.0;
+  }
+}
+
+__global__ void lattice_take_kernel(double *diag, const double *y, long N, long NX, long NY, int n, int a, int b,
+                                    int c)
+{
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < N; g += (long)gridDim.x * blockDim.x) {
+    const long X = g % NX, Y = (g / NX) % NY, Z = g / (NX * NY);
+    if (X % n == a && Y % n == b && Z % n == c) diag[g] = y[g];
+  }
+}
+
 __global__ void cast_kernel(const double *a, float *b, long n)
 {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1026,6 +1145,25 @@ void build_op_device_data(Op &op)
   const bool want32 = (op.d.precision_mask & (1 << MPDG_FP32)) != 0;
   op.d_err = dev_alloc<int>(1, op.device_bytes);
   MPDG_CUDA(cudaMemset(op.d_err, 0, sizeof(int)));
+  if (op.d.kind == MPDG_OP_ADVDIFF && op.d.supg) {
+    Colour *d_col = nullptr;
+    double *d_xq = nullptr;
+    double xq[kMaxN], wq[kMaxN];
+    gauss(n, xq, wq);
+    MPDG_CUDA(cudaMalloc(&d_col, sizeof(m.colour)));
+    MPDG_CUDA(cudaMemcpy(d_col, m.colour, sizeof(m.colour), cudaMemcpyHostToDevice));
+    MPDG_CUDA(cudaMalloc(&d_xq, sizeof(xq)));
+    MPDG_CUDA(cudaMemcpy(d_xq, xq, sizeof(xq), cudaMemcpyHostToDevice));
+    op.d_tau64 = dev_alloc<double>((size_t)m.n_cells, op.device_bytes);
+    if (want32) op.d_tau32 = dev_alloc<float>((size_t)m.n_cells, op.device_bytes);
+    tau_kernel<<<grid_for(m.n_cells, 128), 128>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col, op.d.vel_kind,
+                                                  op.d.vel_param[0], op.d.vel_param[1], op.d.vel_param[2],
+                                                  op.d.supg_coefficient, d_xq, op.d_tau64, op.d_tau32);
+    MPDG_LAUNCHED();
+    MPDG_CUDA(cudaDeviceSynchronize());
+    cudaFree(d_col);
+    cudaFree(d_xq);
+  }
   if (op.d.vel_kind == MPDG_VEL_NONE) return;
   if (!m.uniform) {
     Colour *d_col = nullptr;
@@ -1122,12 +1260,15 @@ KP<Real> base_params(Op &op)
     k.velb = op.d_velb64;
     k.trig = op.d_trig64;
     k.T = op.T64;
+    k.tau = op.d_tau64;
   } else {
     k.metric = m.d_metric32;
     k.velb = op.d_velb32;
     k.trig = op.d_trig32;
     k.T = op.T32;
+    k.tau = op.d_tau32;
   }
+  k.supg_lap = op.d.kind == MPDG_OP_ADVDIFF && op.d.supg && op.d.diffusivity != 0.0;
   k.trig_stride = std::max(m.nc[0], m.nc[1]) * m.n;
   k.dmask = m.d_dmask;
   k.cell_flags = m.d_cell_flags;
@@ -1193,6 +1334,8 @@ void dispatch_degree(Op &op, const KP<Real> &k)
     default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
   }
 }
+
+bool supg(const Op &op) { return op.d.kind == MPDG_OP_ADVDIFF && op.d.supg; }
 
 bool uses_kT(const Op &op)
 {
@@ -1610,6 +1753,17 @@ void launch_cells(Op &op, Real *dst, const Real *src)
   k.src = src;
   k.dst = dst;
   if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
+  if (supg(op)) {
+    // SUPG: block kernel with the stabilisation flux (raw geometry on general meshes)
+    if (!k.tau) throw Error{MPDG_ERR_ARG, "the FP32 form was not prepared for this operator (precision_mask)"};
+    if (!m.uniform && sizeof(Real) == 4) {
+      ensure_metric32(m, op.stream);
+      k.metric = (const Real *)(const void *)m.d_metric32;
+    }
+    MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * m.N_own, op.stream));
+    dispatch_degree<Real, MODE_SUPG, false>(op, k);
+    return;
+  }
   if (!full && !m.uniform) {
     // general geometry: merged coefficient stream (k(T), c_mass, c_diff folded in)
     ensure_coef(op, sizeof(Real) == 4);
@@ -1655,7 +1809,10 @@ void launch_rhs(Op &op, double *dst, const double *src, const double *heat_sourc
     k.c_diff = -(1.0 - op.d.theta) * op.d.diffusivity;
     k.k_alpha = 0.0;
     k.full_tangent = 0;
-    dispatch_degree<double, MODE_LINEAR, false>(op, k);
+    // SUPG: + tau_K u (phi_old/dt - (1-theta) u.grad phi_old + (1-theta) D lap phi_old)
+    // tested with grad N (advection_diffusion_operator.cpp:336-346)
+    if (supg(op)) dispatch_degree<double, MODE_SUPG, false>(op, k);
+    else dispatch_degree<double, MODE_LINEAR, false>(op, k);
   }
 }
 
@@ -1735,9 +1892,54 @@ void launch_diagonal(Op &op, double *diag)
   launch_block_diagonal(op, diag);
 }
 
+// Diagonal of a SUPG operator by probing: n^3 residue classes, one apply each
+// (the SUPG element matrix has no product-of-1D-tables diagonal of the kind
+// diag_kernel sums; MatrixFreeTools::compute_diagonal does the same unit sweeps
+// cell by cell)
+void launch_probe_diagonal(Op &op, double *diag)
+{
+  Mesh &m = *op.mesh;
+  double *x = nullptr, *y = nullptr;
+  MPDG_CUDA(cudaMalloc(&x, sizeof(double) * m.N));
+  const cudaError_t e = cudaMalloc(&y, sizeof(double) * m.N);
+  if (e != cudaSuccess) {
+    cudaFree(x);
+    throw Error{MPDG_ERR_ALLOC, "diagonal probes"};
+  }
+  try {
+    const int n = m.degree + 1;
+    const unsigned grid = grid_for(std::min(m.N, 148L * 1024), 256);
+    for (int c = 0; c < n; ++c)
+      for (int b = 0; b < n; ++b)
+        for (int a = 0; a < n; ++a) {
+          lattice_probe_kernel<<<grid, 256, 0, op.stream>>>(x, m.N, m.NX, m.NY, n, a, b, c);
+          MPDG_LAUNCHED();
+          launch_cells<double>(op, y, x);
+          lattice_take_kernel<<<grid, 256, 0, op.stream>>>(diag, y, m.N, m.NX, m.NY, n, a, b, c);
+          MPDG_LAUNCHED();
+        }
+    if (op.use_dirichlet && m.has_dirichlet) {
+      set_masked_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, m.d_dmask, 1.0);
+      MPDG_LAUNCHED();
+    }
+    MPDG_CUDA(cudaStreamSynchronize(op.stream));
+  } catch (...) {
+    cudaStreamSynchronize(op.stream);
+    cudaFree(x);
+    cudaFree(y);
+    throw;
+  }
+  cudaFree(x);
+  cudaFree(y);
+}
+
 void launch_block_diagonal(Op &op, double *diag)
 {
   Mesh &m = *op.mesh;
+  if (supg(op)) {
+    launch_probe_diagonal(op, diag);
+    return;
+  }
   KP<double> k = base_params<double>(op);
   k.dst = diag;
   const bool kt = uses_kT(op);
@@ -1795,6 +1997,7 @@ bool apply_ready_without_allocation(const Op &op)
   if (op.fine && !apply_ready_without_allocation(*op.fine)) return false;
   const Mesh &m = *op.mesh;
   const bool full = op.d.kind == MPDG_OP_HEAT && op.d.full_tangent;
+  if (supg(op)) return false;                    // the diagonal probes allocate
   if (!full && !m.uniform) return op.coef64_ok;  // merged stream already built
   return true;                                   // nothing is built lazily on these paths
 }

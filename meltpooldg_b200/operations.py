@@ -26,13 +26,16 @@ class AdvectionDiffusionOperation:
     """`inflow_outflow` = (mask, values): DoFs fixed to values after each solve
     through identity rows of the operator instead of Dirichlet constraints
     (create_inflow_outflow_constraints and solve,
-    advection_diffusion_operation.cpp:227-294, 371-499)."""
+    advection_diffusion_operation.cpp:227-294, 371-499).  `supg`,
+    `supg_coefficient`: the "convection stabilization" settings
+    (AdvectionDiffusionData::conv_stab)."""
 
     def __init__(self, mesh, dt, theta=0.5, diffusivity=0.0, velocity=None, dirichlet_values=None,
-                 linear_solver: LinearSolverData = None, device="cuda", inflow_outflow=None):
+                 linear_solver: LinearSolverData = None, device="cuda", inflow_outflow=None, supg=False,
+                 supg_coefficient=-1.0):
         self.mesh = mesh
         self.op = AdvectionDiffusionOperator(mesh, dt, theta=theta, diffusivity=diffusivity,
-                                             velocity=velocity)
+                                             velocity=velocity, supg=supg, supg_coefficient=supg_coefficient)
         self.io = None
         if inflow_outflow is not None:
             io_mask, io_vals = inflow_outflow

@@ -256,13 +256,17 @@ class HeatDiffuseOperator(_MatrixFreeOperator):
 class AdvectionDiffusionOperator(_MatrixFreeOperator):
     """theta-scheme advection-diffusion tangent
     (source/level_set/advection_diffusion_operator.cpp): v = u/dt + theta vel.grad u,
-    g = theta D grad u."""
+    g = theta D grad u.  `supg` adds the SUPG flux tau_K u (u/dt + theta u.grad u
+    - theta D lap u) with tau_K = supg_coefficient h_K, or h_K / max_q |u| for a
+    negative coefficient (ConvectionStabilizationData, advection_diffusion_operator.cpp:450-533)."""
 
     def __init__(self, mesh, dt, theta=0.5, diffusivity=0.0, velocity=None,
-                 precisions=("fp64",)):
+                 precisions=("fp64",), supg=False, supg_coefficient=-1.0):
         vk, vp = _velocity(velocity)
         d = A.OpDesc(A.OP_ADVDIFF, dt, 0.0, 0.0, 0.0, 0, theta, diffusivity, vk,
                      (C.c_double * 3)(*vp), 0)
+        d.supg = int(bool(supg))
+        d.supg_coefficient = float(supg_coefficient)
         super().__init__(mesh, d, precisions)
 
     def set_inflow_outflow(self, mask):
