@@ -142,29 +142,108 @@ def vortex_case(dim, refinements, n_steps=5, dt=0.01, velocity_scale=4.0, theta=
     return norms
 
 
+def smoothed_heaviside(distance, eps):
+    """CharacteristicFunctions::smoothed_heaviside (utilities/characteristic_functions.hpp:18-28)."""
+    d = np.asarray(distance, np.float64)
+    mid = (d + eps) / (2.0 * eps) + np.sin(np.pi * d / eps) / (2.0 * np.pi)
+    return np.where(d > eps, 1.0, np.where(d <= -eps, 0.0, mid))
+
+
 def unidirectional_heat_case(n_steps=5, dt=1e-4, k=1.0, rho=1.0, cp=1.0, convection=0.0,
-                             t_inf=300.0, refinements=5):
-    """Returns the per-step integrated L2 norms of T after Newton convergence."""
+                             t_inf=300.0, refinements=5, emissivity=0.0, rad_t_inf=300.0, velocity=0.0,
+                             material=None, two_phase=False, solidification=False,
+                             residual_tolerance=5e-9, solver=None, mesh=None):
+    """Returns the per-step integrated L2 norms of T after Newton convergence
+    (newton_raphson_solver.cpp:24-80 with field_correction_tolerance 1e-10,
+    nonlinear_solver_data.hpp:13-18).
+
+    The case (unidirectional_heat_transfer.cpp): [0,0.1]^2, convective and
+    radiative faces at x = 0.1 (:196-209); T0 = LinearTemp(1960, 1980) with
+    solidification, 1000 with a convective or radiative face, else
+    LinearTemp(0, 0.1) (:213-227); velocity (-v, 0) (:51-67); with two phases
+    the heaviside of the level set 0.05 - y (:73-90), or with solidification
+    the covected 0.2/3 - x - v t (:98-116), both with eps = 0.01, interpolated
+    at the nodes at the new time each step (heat_transfer_application.cpp:67-70).
+    `material` is an oracle phase-law dict; None is the single-phase (k, rho, cp).
+    `solver(op, rhs, T_old)` can replace the oracle GMRES; `mesh` the default mesh."""
     n = 2 ** refinements
-    mesh = O.Mesh.box(2, 1, [n, n], lo=[0.0, 0.0], hi=[0.1, 0.1])
+    mesh = mesh or O.Mesh.box(2, 1, [n, n], lo=[0.0, 0.0], hi=[0.1, 0.1])
     x = mesh.dof_coordinates()
-    T = np.full(mesh.n_dofs, 1000.0) if convection > 0.0 else x[:, 0].copy()
-    robin_faces = (1 << (2 * 0 + 1)) if convection > 0.0 else 0
+    if solidification:
+        T = 1960.0 + 20.0 * x[:, 0] / 0.1
+    elif convection > 0.0 or emissivity > 0.0:
+        T = np.full(mesh.n_dofs, 1000.0)
+    else:
+        T = x[:, 0].copy()
+    faces = 1 << (2 * 0 + 1)
+    kw = dict(rho_cp=rho * cp, k0=k, robin_alpha=convection, robin_t_inf=t_inf,
+              robin_faces=faces if convection > 0.0 else 0, rad_emissivity=emissivity,
+              rad_t_inf=rad_t_inf, rad_faces=faces if emissivity > 0.0 else 0, material=material)
+    if velocity != 0.0:
+        kw.update(vel_kind=O.VEL_CONST, vel_param=(-velocity, 0.0, 0.0))
     norms = []
+    t = 0.0
     for _ in range(n_steps):
+        t += dt
+        H = None
+        if two_phase:
+            H = smoothed_heaviside(0.1 * 2.0 / 3.0 - x[:, 0] - velocity * t, 0.01) if solidification \
+                else smoothed_heaviside(0.05 - x[:, 1], 0.01)
         T_old = T.copy()
-        op = O.Operator(O.HEAT, dt, rho_cp=rho * cp, k0=k, temperature=T,
-                        robin_alpha=convection, robin_t_inf=t_inf, robin_faces=robin_faces)
+        op = O.Operator(O.HEAT, dt, temperature=T, temperature_old=T_old, heaviside=H, **kw)
         inv = O.inverse_diagonal(mesh, op)
         for _it in range(10):
             op = op.with_temperature(T)
             rhs = O.rhs_heat(mesh, op, T_old)
-            dx, _, _, ok = O.gmres(mesh, op, rhs, inv_diag=inv, rel_tol=1e-12, abs_tol=1e-20)
-            assert ok
-            if np.linalg.norm(rhs) < 5e-9 and np.linalg.norm(dx) < 1e-10:
+            if solver is None:
+                dx, _, _, ok = O.gmres(mesh, op, rhs, inv_diag=inv, rel_tol=1e-12, abs_tol=1e-20)
+                assert ok
+            else:
+                dx = solver(op, rhs, T_old)
+            if np.linalg.norm(rhs) < residual_tolerance and np.linalg.norm(dx) < 1e-10:
                 break
             T = T + dx
         else:
             raise RuntimeError("Newton did not converge")
         norms.append(O.l2_norm(mesh, T))
     return norms
+
+
+
+# Parameters of the reference's unidirectional heat-transfer test cases
+# (applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/*.json):
+# material "gas" is the single phase; phase laws index (gas, liquid, solid).
+_STEEL = dict(k=55.563, rho=7850.0, cp=460.0)
+_GAS_LIQUID = dict(kind=O.MAT_GAS_LIQUID, rho=(3925.0, 7850.0, 0.0), cp=(230.0, 460.0, 0.0),
+                   k=(27.7815, 55.563, 0.0))
+_LIQUID_SOLID = dict(kind=O.MAT_LIQUID_SOLID, rho=(0.0, 7850.0, 7850.0), cp=(0.0, 460.0, 700.0),
+                     k=(0.0, 55.563, 17.0), solidus=1966.0, liquidus=1974.0)
+_GAS_LIQUID_SOLID = dict(kind=O.MAT_GAS_LIQUID_SOLID, rho=(3925.0, 7850.0, 7850.0), cp=(230.0, 460.0, 700.0),
+                         k=(27.7815, 55.563, 17.0), solidus=1966.0, liquidus=1974.0, two_phase_sharp=True)
+HEAT_CASES = {
+    "unidirectional_heat_transfer_with_radiation": dict(dt=0.01, emissivity=0.98, **_STEEL),
+    "unidirectional_heat_transfer_with_radiation_and_convection":
+        dict(dt=0.01, emissivity=0.98, convection=25.0, **_STEEL),
+    "unidirectional_heat_transfer_with_velocity":
+        dict(dt=0.001, emissivity=0.98, convection=25.0, velocity=0.01, residual_tolerance=1e-6, **_STEEL),
+    "unidirectional_heat_transfer_with_two_phase":
+        dict(dt=0.001, emissivity=0.98, convection=25.0, velocity=0.01, residual_tolerance=1e-6,
+             material=_GAS_LIQUID, two_phase=True),
+    "unidirectional_heat_transfer_with_two_phase_rho_times_cp":
+        dict(dt=0.001, emissivity=0.98, convection=25.0, velocity=0.01, residual_tolerance=1e-6,
+             material=dict(_GAS_LIQUID, volume_specific=True), two_phase=True),
+    "unidirectional_heat_transfer_with_velocity_and_solidification":
+        dict(dt=0.01, velocity=0.005, residual_tolerance=1e-7, material=_LIQUID_SOLID, solidification=True),
+    "unidirectional_heat_transfer_with_two_phase_and_solidification":
+        dict(dt=1.0, velocity=1e-4, residual_tolerance=1e-7, material=_GAS_LIQUID_SOLID, two_phase=True,
+             solidification=True),
+}
+
+
+def printed_match(got, printed):
+    """The reference prints ||T|| with 6 digits of a norm it sums from float cell
+    norms (source/utilities/vector_tools.cpp:151): a value matches when it is
+    within half a unit of the last printed digit plus that float noise (5e-8)."""
+    ref = float(printed)
+    half = 0.5 * 10.0 ** (int(printed.lower().split("e")[1]) - 5)
+    return abs(got - ref) <= half + 5e-8 * abs(ref)

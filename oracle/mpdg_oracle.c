@@ -355,7 +355,73 @@ static void integrate(const geo_t *g, const double *val, double grad[3][MAXN3], 
 typedef struct {
   double JxW, Ji[3][3], x[3], vel[3];
   double T, gradT[3]; /* physical */
+  double Told, H;     /* T_old and the heaviside at the point */
 } qdata_t;
+
+/* ----------------------------------------------------------- material laws
+ * (rho c_p, k, d(rho c_p)/dT, dk/dT) at a point: Material::compute_parameters_internal
+ * (material.templates.hpp:213-500) with the solid fraction of :748-760, the cubic
+ * solid/liquid interpolation of :546-600 (level_set_tools.hpp:66-90) and the gas
+ * weight of compute_two_phase_fluid_property (:513-523); rho c_p = rho * c_p and its
+ * derivative by the product rule (heat_diffuse_operator.cpp:1176-1199) unless the
+ * volume-specific capacity is interpolated itself */
+static double ls_value(double fs, double vl, double vs)
+{
+  if (fs == 0.0) return vl;
+  if (fs == 1.0) return vs;
+  return vl + (vs - vl) * (-2.0 * fs * fs * fs + 3.0 * fs * fs);
+}
+
+static double ls_deriv(double fs, double inv_mushy, double vl, double vs)
+{
+  if (fs == 0.0 || fs == 1.0) return 0.0;
+  return -inv_mushy * (vs - vl) * (-6.0 * fs * fs + 6.0 * fs);
+}
+
+static int mat_has_T(const orc_op *op)
+{
+  return op->material == ORC_MAT_LIQUID_SOLID || op->material == ORC_MAT_GAS_LIQUID_SOLID;
+}
+
+static void mat_eval(const orc_op *op, double T, double H, double *rc, double *k, double *drc, double *dk)
+{
+  if (op->material == ORC_MAT_LINEAR) {
+    *rc = op->rho_cp;
+    *k = op->k0 * (1.0 + op->k_alpha * T);
+    *drc = 0.0;
+    *dk = op->k0 * op->k_alpha;
+    return;
+  }
+  const int gas = op->material == ORC_MAT_GAS_LIQUID || op->material == ORC_MAT_GAS_LIQUID_SOLID;
+  const int sol = mat_has_T(op);
+  const double inv_mushy = sol ? 1.0 / (op->liquidus - op->solidus) : 0.0;
+  double fs = 0.0;
+  if (sol) fs = op->solid_liquid_sharp ? (T < op->solidus ? 1.0 : 0.0)
+                                       : fmin(fmax((op->liquidus - T) * inv_mushy, 0.0), 1.0);
+  const double w = gas ? (op->two_phase_sharp ? (H > 0.5 ? 1.0 : 0.0) : H) : 1.0;
+  double v[4], dv[4]; /* rho, c_p, k, rho c_p of the liquid(-solid) phase */
+  const double rcl = op->mat_rho[1] * op->mat_cp[1], rcs = op->mat_rho[2] * op->mat_cp[2];
+  const double vl[4] = {op->mat_rho[1], op->mat_cp[1], op->mat_k[1], rcl};
+  const double vs[4] = {op->mat_rho[2], op->mat_cp[2], op->mat_k[2], rcs};
+  const double vg[4] = {op->mat_rho[0], op->mat_cp[0], op->mat_k[0], op->mat_rho[0] * op->mat_cp[0]};
+  for (int e = 0; e < 4; ++e) {
+    v[e] = sol ? ls_value(fs, vl[e], vs[e]) : vl[e];
+    dv[e] = sol ? ls_deriv(fs, inv_mushy, vl[e], vs[e]) : 0.0;
+    if (gas) {
+      v[e] = (1.0 - w) * vg[e] + w * v[e];
+      dv[e] = w * dv[e];
+    }
+  }
+  *k = v[2];
+  *dk = dv[2];
+  if (op->volume_specific) {
+    *rc = v[3];
+    *drc = dv[3];
+  } else {
+    *rc = v[0] * v[1];
+    *drc = dv[1] * v[0] + dv[0] * v[1];
+  }
+}
 
 static void cell_qdata(const orc_mesh *m, const orc_op *op, const geo_t *g, int ix, int iy,
                        int iz, const long *idx, qdata_t *qd)
@@ -369,6 +435,17 @@ static void cell_qdata(const orc_mesh *m, const orc_op *op, const geo_t *g, int 
   if (haveT) {
     for (int t = 0; t < nqt; ++t) Tl[t] = op->temperature[idx[t]];
     evaluate(g, Tl, Tv, Tg);
+  }
+  double Ov[MAXN3], Hv[MAXN3];
+  if (op->temperature_old) {
+    double l[MAXN3];
+    for (int t = 0; t < nqt; ++t) l[t] = op->temperature_old[idx[t]];
+    evaluate(g, l, Ov, NULL);
+  }
+  if (op->heaviside) {
+    double l[MAXN3];
+    for (int t = 0; t < nqt; ++t) l[t] = op->heaviside[idx[t]];
+    evaluate(g, l, Hv, NULL);
   }
   double Vv[3][MAXN3];
   if (op->vel_kind == ORC_VEL_NODAL)
@@ -393,6 +470,8 @@ static void cell_qdata(const orc_mesh *m, const orc_op *op, const geo_t *g, int 
           velocity_at(op, dim, qd[q].x, qd[q].vel);
         }
         qd[q].T = haveT ? Tv[q] : 0.0;
+        qd[q].Told = op->temperature_old ? Ov[q] : 0.0;
+        qd[q].H = op->heaviside ? Hv[q] : 0.0;
         for (int a = 0; a < 3; ++a) {
           double s = 0.0;
           if (haveT)
@@ -410,11 +489,17 @@ static void tangent_qp(const orc_op *op, int dim, const qdata_t *qd, double u, c
   double vgu = 0.0;
   for (int a = 0; a < dim; ++a) vgu += qd->vel[a] * gu[a];
   if (op->kind == ORC_HEAT) {
-    const double k = op->k0 * (1.0 + op->k_alpha * qd->T);
-    const double dk = op->k0 * op->k_alpha;
-    *v = op->rho_cp / op->dt * u + op->rho_cp * vgu;
-    for (int a = 0; a < 3; ++a)
-      f[a] = k * gu[a] + (op->full_tangent ? dk * qd->gradT[a] * u : 0.0);
+    /* heat_diffuse_operator.cpp:1040-1062 */
+    double rc, k, drc, dk;
+    mat_eval(op, qd->T, qd->H, &rc, &k, &drc, &dk);
+    *v = rc / op->dt * u + rc * vgu;
+    const int deriv = (op->material == ORC_MAT_LINEAR) ? op->full_tangent : mat_has_T(op);
+    for (int a = 0; a < 3; ++a) f[a] = k * gu[a] + (deriv ? dk * qd->gradT[a] * u : 0.0);
+    if (deriv && op->material != ORC_MAT_LINEAR) {
+      double vgT = 0.0;
+      for (int a = 0; a < dim; ++a) vgT += qd->vel[a] * qd->gradT[a];
+      *v += drc / op->dt * (qd->T - qd->Told) * u + drc * vgT * u;
+    }
   } else {
     *v = u / op->dt + op->theta * vgu;
     for (int a = 0; a < 3; ++a) f[a] = op->theta * op->diffusivity * gu[a];
@@ -512,20 +597,47 @@ static void apply_cell(const orc_mesh *m, const orc_op *op, const geo_t *g, int 
 
 /* ------------------------------------------------------------ Robin faces (heat) */
 
-/* face f of a cell: direction d, side s; returns the n^(dim-1) local dof indices,
- * face quadrature JxW and point coordinates; values of the face shape functions
- * are products of 1D S tables (nodal on GL nodes, so the face trace uses the
- * face's own dofs only). */
-static void robin_face_matrix_apply(const orc_mesh *m, const geo_t *g, int ix, int iy, int iz,
-                                    int d, int s, double alpha, const double *ul_cell,
-                                    double *out_cell, double *diag_cell)
+/* Boundary-face terms of the heat operator on face (d, s) of a cell: convection
+ * (robin_faces, coefficient alpha) and radiation (rad_faces, emissivity eps),
+ * heat_diffuse_operator.cpp:1088-1129 (tangent) and :719-778 (residual).
+ * TANGENT: (alpha + 4 eps sigma T_q^3) u_q tested with N, or its diagonal;
+ * RESIDUAL: -alpha (T_q - T_inf) - eps sigma (T_q^4 - T_rad^4) tested with N.
+ * T_q is the face interpolant of op->temperature.  Face shape functions are
+ * products of 1D S tables (nodal on GL nodes, so the trace uses the face's own
+ * dofs only). */
+enum { ROB_TANGENT = 0, ROB_RESIDUAL = 1 };
+
+static void face_terms(const orc_op *op, int d, int s, int *conv, int *rad)
+{
+  const int bit = 1 << (2 * d + s);
+  *conv = op->kind == ORC_HEAT && (op->robin_faces & bit) && op->robin_alpha != 0.0;
+  *rad = op->kind == ORC_HEAT && (op->rad_faces & bit) && op->rad_emissivity != 0.0;
+}
+
+static int has_face_terms(const orc_op *op)
+{
+  for (int f = 0; f < 6; ++f) {
+    int c, r;
+    face_terms(op, f / 2, f % 2, &c, &r);
+    if (c || r) return 1;
+  }
+  return 0;
+}
+
+static void robin_face_apply(const orc_mesh *m, const orc_op *op, const geo_t *g, int ix, int iy, int iz,
+                             int d, int s, int mode, const long *idx, const double *ul_cell, double *out_cell,
+                             double *diag_cell)
 {
   const int n = g->n, dim = g->dim;
+  int conv, rad;
+  face_terms(op, d, s, &conv, &rad);
+  if (!conv && !rad) return;
+  const double es = op->rad_emissivity * ORC_STEFAN_BOLTZMANN;
   double vc[8][3];
   cell_vertices(m, g, ix, iy, iz, vc);
   int t0 = (d == 0) ? 1 : 0;           /* tangential directions */
   int t1 = (dim == 3) ? ((d == 2) ? 1 : 2) : -1;
-  const int nq1 = (dim == 3) ? n : 1;
+  const int nq1 = (dim == 3) ? n : 1, nb = (dim == 3) ? n : 1;
   for (int qb = 0; qb < nq1; ++qb)
     for (int qa = 0; qa < n; ++qa) {
       double xi[3] = {0, 0, 0};
@@ -545,8 +657,7 @@ static void robin_face_matrix_apply(const orc_mesh *m, const geo_t *g, int ix, i
       }
       const double JxW = ds * w;
       /* face dofs: local index with coordinate d fixed to 0 or p */
-      double uq = 0.0;
-      const int nb = (dim == 3) ? n : 1;
+      double uq = 0.0, Tq = 0.0;
       for (int b = 0; b < nb; ++b)
         for (int a = 0; a < n; ++a) {
           int c[3] = {0, 0, 0};
@@ -556,19 +667,25 @@ static void robin_face_matrix_apply(const orc_mesh *m, const geo_t *g, int ix, i
           int li = (c[2] * n + c[1]) * n + c[0];
           double phi = g->S[qa * n + a] * ((t1 >= 0) ? g->S[qb * n + b] : 1.0);
           if (ul_cell) uq += phi * ul_cell[li];
-          if (diag_cell) diag_cell[li] += alpha * phi * phi * JxW;
+          if (op->temperature) Tq += phi * op->temperature[idx[li]];
         }
-      if (out_cell)
-        for (int b = 0; b < nb; ++b)
-          for (int a = 0; a < n; ++a) {
-            int c[3] = {0, 0, 0};
-            c[d] = s ? n - 1 : 0;
-            c[t0] = a;
-            if (t1 >= 0) c[t1] = b;
-            int li = (c[2] * n + c[1]) * n + c[0];
-            double phi = g->S[qa * n + a] * ((t1 >= 0) ? g->S[qb * n + b] : 1.0);
-            out_cell[li] += alpha * uq * phi * JxW;
-          }
+      const double coef = (conv ? op->robin_alpha : 0.0) + (rad ? 4.0 * es * Tq * Tq * Tq : 0.0);
+      double val = coef * uq;
+      if (mode == ROB_RESIDUAL)
+        val = -(conv ? op->robin_alpha * (Tq - op->robin_t_inf) : 0.0) -
+              (rad ? es * (Tq * Tq * Tq * Tq - op->rad_t_inf * op->rad_t_inf * op->rad_t_inf * op->rad_t_inf)
+                   : 0.0);
+      for (int b = 0; b < nb; ++b)
+        for (int a = 0; a < n; ++a) {
+          int c[3] = {0, 0, 0};
+          c[d] = s ? n - 1 : 0;
+          c[t0] = a;
+          if (t1 >= 0) c[t1] = b;
+          int li = (c[2] * n + c[1]) * n + c[0];
+          double phi = g->S[qa * n + a] * ((t1 >= 0) ? g->S[qb * n + b] : 1.0);
+          if (diag_cell) diag_cell[li] += coef * phi * phi * JxW;
+          if (out_cell) out_cell[li] += val * phi * JxW;
+        }
     }
 }
 
@@ -581,15 +698,16 @@ static int cell_on_face(const geo_t *g, int ix, int iy, int iz, int d, int s)
 static void apply_robin(const orc_mesh *m, const orc_op *op, const geo_t *g, double *dst,
                         const double *src)
 {
-  if (op->kind != ORC_HEAT || !op->robin_faces || op->robin_alpha == 0.0) return;
+  if (!has_face_terms(op)) return;
   const int n = g->n, dim = g->dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
   for (int iz = 0; iz < g->nc[2]; ++iz)
     for (int iy = 0; iy < g->nc[1]; ++iy)
       for (int ix = 0; ix < g->nc[0]; ++ix)
         for (int d = 0; d < dim; ++d)
           for (int s = 0; s < 2; ++s) {
-            if (!(op->robin_faces & (1 << (2 * d + s)))) continue;
-            if (!cell_on_face(g, ix, iy, iz, d, s)) continue;
+            int conv, rad;
+            face_terms(op, d, s, &conv, &rad);
+            if (!(conv || rad) || !cell_on_face(g, ix, iy, iz, d, s)) continue;
             long idx[MAXN3];
             double ul[MAXN3], out[MAXN3];
             cell_dofs(g, ix, iy, iz, idx);
@@ -597,7 +715,7 @@ static void apply_robin(const orc_mesh *m, const orc_op *op, const geo_t *g, dou
               ul[t] = (op->dirichlet && op->dirichlet[idx[t]]) ? 0.0 : src[idx[t]];
               out[t] = 0.0;
             }
-            robin_face_matrix_apply(m, g, ix, iy, iz, d, s, op->robin_alpha, ul, out, NULL);
+            robin_face_apply(m, op, g, ix, iy, iz, d, s, ROB_TANGENT, idx, ul, out, NULL);
             for (int t = 0; t < nqt; ++t)
               if (!(op->dirichlet && op->dirichlet[idx[t]])) dst[idx[t]] += out[t];
           }
@@ -677,8 +795,12 @@ static void element_matrix(const orc_mesh *m, const orc_op *op, const geo_t *g, 
           }
         }
         /* fields at this point by direct summation */
-        qd.T = 0.0;
+        qd.T = qd.Told = qd.H = 0.0;
         qd.gradT[0] = qd.gradT[1] = qd.gradT[2] = 0.0;
+        for (int t = 0; t < nqt; ++t) {
+          if (op->temperature_old) qd.Told += op->temperature_old[idx[t]] * phi[t];
+          if (op->heaviside) qd.H += op->heaviside[idx[t]] * phi[t];
+        }
         if (op->temperature)
           for (int t = 0; t < nqt; ++t) {
             double Tt = op->temperature[idx[t]];
@@ -764,11 +886,10 @@ void orc_diagonal(const orc_mesh *m, const orc_op *op, double *diag)
         element_matrix(m, op, &g, ix, iy, iz, idx, A);
         double dc[MAXN3];
         for (int i = 0; i < nqt; ++i) dc[i] = A[i * nqt + i];
-        if (op->kind == ORC_HEAT && op->robin_faces && op->robin_alpha != 0.0)
-          for (int d = 0; d < dim; ++d)
-            for (int s = 0; s < 2; ++s)
-              if ((op->robin_faces & (1 << (2 * d + s))) && cell_on_face(&g, ix, iy, iz, d, s))
-                robin_face_matrix_apply(m, &g, ix, iy, iz, d, s, op->robin_alpha, NULL, NULL, dc);
+        for (int d = 0; d < dim; ++d)
+          for (int s = 0; s < 2; ++s)
+            if (cell_on_face(&g, ix, iy, iz, d, s))
+              robin_face_apply(m, op, &g, ix, iy, iz, d, s, ROB_TANGENT, idx, NULL, NULL, dc);
         for (int i = 0; i < nqt; ++i)
           if (!(op->dirichlet && op->dirichlet[idx[i]])) diag[idx[i]] += dc[i];
       }
@@ -820,11 +941,13 @@ void orc_rhs_heat(const orc_mesh *m, const orc_op *op, double *dst, const double
       evaluate(&g, ol, ov, NULL);
       evaluate(&g, ql, qv, NULL);
       for (int q = 0; q < nqt; ++q) {
-        const double k = op->k0 * (1.0 + op->k_alpha * qd[q].T);
-        double v = op->rho_cp / op->dt * (qd[q].T - ov[q]) - qv[q];
+        /* heat_diffuse_operator.cpp:482-518 */
+        double rc, k, drc, dk;
+        mat_eval(op, qd[q].T, qd[q].H, &rc, &k, &drc, &dk);
+        double v = rc / op->dt * (qd[q].T - ov[q]) - qv[q];
         double vg = 0.0;
         for (int a = 0; a < dim; ++a) vg += qd[q].gradT[a] * qd[q].vel[a];
-        v += op->rho_cp * vg;
+        v += rc * vg;
         val[q] = -v * qd[q].JxW;
         for (int b = 0; b < dim; ++b) {
           double s = 0.0;
@@ -838,26 +961,19 @@ void orc_rhs_heat(const orc_mesh *m, const orc_op *op, double *dst, const double
         if (!(scatter_mask && scatter_mask[idx[t]])) dst[idx[t]] += out[t];
     }
   }
-  /* Robin faces: -alpha (T - T_inf) tested with N (heat_diffuse_operator.cpp:760-770) */
-  if (op->robin_faces && op->robin_alpha != 0.0) {
+  /* convective and radiative faces (heat_diffuse_operator.cpp:719-778) */
+  if (has_face_terms(op)) {
     for (int iz = 0; iz < g.nc[2]; ++iz)
       for (int iy = 0; iy < g.nc[1]; ++iy)
         for (int ix = 0; ix < g.nc[0]; ++ix)
           for (int d = 0; d < dim; ++d)
             for (int s = 0; s < 2; ++s) {
-              if (!(op->robin_faces & (1 << (2 * d + s))) || !cell_on_face(&g, ix, iy, iz, d, s))
-                continue;
+              if (!cell_on_face(&g, ix, iy, iz, d, s)) continue;
               long idx[MAXN3];
-              double ul[MAXN3], out[MAXN3], one[MAXN3];
+              double out[MAXN3];
               cell_dofs(&g, ix, iy, iz, idx);
-              for (int t = 0; t < nqt; ++t) {
-                ul[t] = -(op->temperature ? op->temperature[idx[t]] : 0.0);
-                one[t] = op->robin_t_inf;
-                out[t] = 0.0;
-              }
-              /* -alpha T + alpha T_inf (the constant is reproduced exactly by the nodal basis) */
-              for (int t = 0; t < nqt; ++t) ul[t] += one[t];
-              robin_face_matrix_apply(m, &g, ix, iy, iz, d, s, op->robin_alpha, ul, out, NULL);
+              for (int t = 0; t < nqt; ++t) out[t] = 0.0;
+              robin_face_apply(m, op, &g, ix, iy, iz, d, s, ROB_RESIDUAL, idx, NULL, out, NULL);
               for (int t = 0; t < nqt; ++t)
                 if (!(scatter_mask && scatter_mask[idx[t]])) dst[idx[t]] += out[t];
             }
@@ -1281,7 +1397,8 @@ static void orc2_check(const orc_mesh2 *m, const orc_op *op)
 {
   if (m->coarse.dim != 3 || m->fine.dim != 3 || m->coarse.degree != m->fine.degree ||
       m->fine.nc[1] != 2 * m->coarse.nc[1] || m->fine.nc[2] != 2 * m->coarse.nc[2] ||
-      op->temperature || op->robin_faces || op->vel_kind == ORC_VEL_NODAL || op->full_tangent) {
+      op->temperature || op->robin_faces || op->rad_faces || op->vel_kind == ORC_VEL_NODAL || op->full_tangent ||
+      op->material != ORC_MAT_LINEAR) {
     fprintf(stderr, "orc2: unsupported two-level configuration\n");
     abort();
   }

@@ -41,6 +41,12 @@ enum {
 };
 
 enum { ORC_PREC_IDENTITY = 0, ORC_PREC_JACOBI = 1, ORC_PREC_CHEBYSHEV = 2 };
+/* heat material laws (MaterialTypes, Material::compute_parameters_internal,
+ * include/meltpooldg/core/material.templates.hpp:213-500): LINEAR is rho_cp and
+ * k(T) = k0 (1 + k_alpha T); the phase laws interpolate gas / liquid / solid
+ * properties by the level-set heaviside H and the solid fraction f_s(T) */
+enum { ORC_MAT_LINEAR = 0, ORC_MAT_GAS_LIQUID = 1, ORC_MAT_LIQUID_SOLID = 2, ORC_MAT_GAS_LIQUID_SOLID = 3 };
+#define ORC_STEFAN_BOLTZMANN 5.670374419e-8
 
 typedef struct {
   int dim;             /* 2 or 3 */
@@ -73,6 +79,19 @@ typedef struct {
    * coefficient h_K, h_K = cell diameter / sqrt(dim); axis-aligned cells */
   int supg;
   double supg_coefficient;
+  /* heat: radiative faces (heat_diffuse_operator.cpp:766-772, 1122-1124): tangent
+   * 4 eps sigma T^3 u v, residual -eps sigma (T^4 - T_inf^4) v; bits as robin_faces */
+  double rad_emissivity, rad_t_inf;
+  int rad_faces;
+  /* heat: material law (ORC_MAT_*); phase properties index 0 gas, 1 liquid, 2 solid */
+  int material;
+  double mat_rho[3], mat_cp[3], mat_k[3];
+  double solidus, liquidus;
+  int two_phase_sharp;      /* weight heaviside(H, 0.5) instead of H */
+  int solid_liquid_sharp;   /* f_s = T < solidus instead of the mushy-zone ramp */
+  int volume_specific;      /* interpolate rho*c_p itself instead of rho and c_p */
+  const double *temperature_old; /* T_old: solidification terms of the tangent */
+  const double *heaviside;       /* level set as heaviside, nodal (two-phase laws) */
 } orc_op;
 
 typedef struct {

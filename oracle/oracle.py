@@ -19,6 +19,7 @@ LIB_PATH = os.path.join(HERE, "libmpdg_oracle.so")
 HEAT, ADVDIFF = 0, 1
 VEL_NONE, VEL_ROTATION, VEL_VORTEX, VEL_CONST, VEL_NODAL = 0, 1, 2, 3, 4
 PREC_IDENTITY, PREC_JACOBI, PREC_CHEBYSHEV = 0, 1, 2
+MAT_LINEAR, MAT_GAS_LIQUID, MAT_LIQUID_SOLID, MAT_GAS_LIQUID_SOLID = 0, 1, 2, 3
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)
@@ -38,6 +39,11 @@ class _Op(C.Structure):
         ("vel_kind", C.c_int), ("vel_param", C.c_double * 3), ("vel_nodal", _dp),
         ("dirichlet", _u8p),
         ("supg", C.c_int), ("supg_coefficient", C.c_double),
+        ("rad_emissivity", C.c_double), ("rad_t_inf", C.c_double), ("rad_faces", C.c_int),
+        ("material", C.c_int), ("mat_rho", C.c_double * 3), ("mat_cp", C.c_double * 3),
+        ("mat_k", C.c_double * 3), ("solidus", C.c_double), ("liquidus", C.c_double),
+        ("two_phase_sharp", C.c_int), ("solid_liquid_sharp", C.c_int), ("volume_specific", C.c_int),
+        ("temperature_old", _dp), ("heaviside", _dp),
     ]
 
 
@@ -162,34 +168,67 @@ class Mesh:
         return mask.astype(np.uint8)
 
 
+def _arr(a, dtype=np.float64):
+    return None if a is None else np.ascontiguousarray(a, dtype)
+
+
 class Operator:
-    """Parameters of one heat or advection-diffusion operator (oracle side)."""
+    """Parameters of one heat or advection-diffusion operator (oracle side).
+
+    `material` selects a phase law of the heat operator: a dict with `kind`
+    (MAT_GAS_LIQUID, MAT_LIQUID_SOLID, MAT_GAS_LIQUID_SOLID), `rho`, `cp`, `k`
+    (each (gas, liquid, solid)), `solidus`, `liquidus` and the flags
+    `two_phase_sharp`, `solid_liquid_sharp`, `volume_specific`; None keeps
+    rho_cp and k(T) = k0 (1 + k_alpha T).  `temperature_old` and `heaviside` are
+    the nodal fields those laws read."""
 
     def __init__(self, kind, dt, rho_cp=1.0, k0=1.0, k_alpha=0.0, full_tangent=False,
                  temperature=None, robin_alpha=0.0, robin_t_inf=0.0, robin_faces=0,
                  theta=0.5, diffusivity=0.0, vel_kind=VEL_NONE, vel_param=(0.0, 0.0, 0.0),
-                 vel_nodal=None, dirichlet=None, supg=False, supg_coefficient=-1.0):
-        self.temperature = None if temperature is None else np.ascontiguousarray(temperature, np.float64)
-        self.vel_nodal = None if vel_nodal is None else np.ascontiguousarray(vel_nodal, np.float64)
-        self.dirichlet = None if dirichlet is None else np.ascontiguousarray(dirichlet, np.uint8)
+                 vel_nodal=None, dirichlet=None, supg=False, supg_coefficient=-1.0,
+                 rad_emissivity=0.0, rad_t_inf=0.0, rad_faces=0, material=None,
+                 temperature_old=None, heaviside=None):
+        self.temperature = _arr(temperature)
+        self.vel_nodal = _arr(vel_nodal)
+        self.dirichlet = _arr(dirichlet, np.uint8)
+        self.temperature_old = _arr(temperature_old)
+        self.heaviside = _arr(heaviside)
         self.kind, self.dt = kind, dt
+        mat = material or {}
+        three = C.c_double * 3
         self._c = _Op(kind, dt, rho_cp, k0, k_alpha, int(full_tangent), _ptr(self.temperature),
                       robin_alpha, robin_t_inf, robin_faces, theta, diffusivity, vel_kind,
-                      (C.c_double * 3)(*vel_param), _ptr(self.vel_nodal),
-                      _ptr(self.dirichlet, _u8p), int(bool(supg)), float(supg_coefficient))
+                      three(*vel_param), _ptr(self.vel_nodal),
+                      _ptr(self.dirichlet, _u8p), int(bool(supg)), float(supg_coefficient),
+                      rad_emissivity, rad_t_inf, rad_faces, int(mat.get("kind", MAT_LINEAR)),
+                      three(*mat.get("rho", (0, 0, 0))), three(*mat.get("cp", (0, 0, 0))),
+                      three(*mat.get("k", (0, 0, 0))), float(mat.get("solidus", 0.0)),
+                      float(mat.get("liquidus", 0.0)), int(bool(mat.get("two_phase_sharp", False))),
+                      int(bool(mat.get("solid_liquid_sharp", False))),
+                      int(bool(mat.get("volume_specific", False))),
+                      _ptr(self.temperature_old), _ptr(self.heaviside))
         self.params = dict(kind=kind, dt=dt, rho_cp=rho_cp, k0=k0, k_alpha=k_alpha,
                            full_tangent=full_tangent, robin_alpha=robin_alpha,
                            robin_t_inf=robin_t_inf, robin_faces=robin_faces, theta=theta,
                            diffusivity=diffusivity, vel_kind=vel_kind, vel_param=vel_param, supg=supg,
-                           supg_coefficient=supg_coefficient)
+                           supg_coefficient=supg_coefficient, rad_emissivity=rad_emissivity,
+                           rad_t_inf=rad_t_inf, rad_faces=rad_faces, material=material)
+        self.fields = dict(temperature=self.temperature, vel_nodal=self.vel_nodal, dirichlet=self.dirichlet,
+                           temperature_old=self.temperature_old, heaviside=self.heaviside)
+
+    def _with(self, **kw):
+        f = dict(self.fields)
+        f.update(kw)
+        return Operator(**self.params, **f)
 
     def with_dirichlet(self, mask):
-        p = dict(self.params)
-        return Operator(**p, temperature=self.temperature, vel_nodal=self.vel_nodal, dirichlet=mask)
+        return self._with(dirichlet=mask)
 
     def with_temperature(self, T):
-        p = dict(self.params)
-        return Operator(**p, temperature=T, vel_nodal=self.vel_nodal, dirichlet=self.dirichlet)
+        return self._with(temperature=T)
+
+    def with_fields(self, **kw):
+        return self._with(**kw)
 
 
 # ----------------------------------------------------------- operations

@@ -37,6 +37,34 @@ CASES = {
         "applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/"
         "unidirectional_heat_transfer_with_convection.mpirun=4.output",
         r"\|\|solution\|\| = ([0-9.eE+-]+)"),
+    "unidirectional_heat_transfer_with_radiation": (
+        "applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/"
+        "unidirectional_heat_transfer_with_radiation.mpirun=4.output",
+        r"\|\|solution\|\| = ([0-9.eE+-]+)"),
+    "unidirectional_heat_transfer_with_radiation_and_convection": (
+        "applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/"
+        "unidirectional_heat_transfer_with_radiation_and_convection.mpirun=4.output",
+        r"\|\|solution\|\| = ([0-9.eE+-]+)"),
+    "unidirectional_heat_transfer_with_velocity": (
+        "applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/"
+        "unidirectional_heat_transfer_with_velocity.mpirun=4.output",
+        r"\|\|solution\|\| = ([0-9.eE+-]+)"),
+    "unidirectional_heat_transfer_with_two_phase": (
+        "applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/"
+        "unidirectional_heat_transfer_with_two_phase.mpirun=4.output",
+        r"\|\|solution\|\| = ([0-9.eE+-]+)"),
+    "unidirectional_heat_transfer_with_two_phase_rho_times_cp": (
+        "applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/"
+        "unidirectional_heat_transfer_with_two_phase_rho_times_cp.mpirun=4.output",
+        r"\|\|solution\|\| = ([0-9.eE+-]+)"),
+    "unidirectional_heat_transfer_with_velocity_and_solidification": (
+        "applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/"
+        "unidirectional_heat_transfer_with_velocity_and_solidification.mpirun=4.output",
+        r"\|\|solution\|\| = ([0-9.eE+-]+)"),
+    "unidirectional_heat_transfer_with_two_phase_and_solidification": (
+        "applications/mp-heat-transfer/cases/unidirectional_heat_transfer/tests/"
+        "unidirectional_heat_transfer_with_two_phase_and_solidification.mpirun=4.output",
+        r"\|\|solution\|\| = ([0-9.eE+-]+)"),
 }
 
 

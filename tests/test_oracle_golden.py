@@ -63,6 +63,17 @@ def test_unidirectional_heat_golden():
     assert [_fmt(v) for v in got] == GOLDEN["unidirectional_heat_transfer"]["printed"]
 
 
+@pytest.mark.parametrize("name", sorted(cases.HEAT_CASES))
+def test_unidirectional_heat_phase_laws_and_radiation_golden(name):
+    """Radiative faces, velocity, gas/liquid and liquid/solid material laws
+    (material.templates.hpp:213-760; heat_diffuse_operator.cpp:719-778, 955-1129)."""
+    got = cases.unidirectional_heat_case(**cases.HEAT_CASES[name])
+    printed = GOLDEN[name]["printed"]
+    assert len(got) == len(printed) == 5
+    for g, p in zip(got, printed):
+        assert cases.printed_match(g, p), (name, g, p)
+
+
 def test_unidirectional_heat_convection_golden():
     got = cases.unidirectional_heat_case(dt=0.01, k=55.563, rho=7850.0, cp=460.0, convection=25.0)
     assert [_fmt(v) for v in got] == GOLDEN["unidirectional_heat_transfer_with_convection"]["printed"]
