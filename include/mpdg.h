@@ -49,7 +49,19 @@ enum {
 enum { MPDG_GEOM_AUTO = 0, MPDG_GEOM_GENERAL = 1 };
 enum { MPDG_SOLVER_CG = 0, MPDG_SOLVER_GMRES = 1 };
 enum { MPDG_PREC_IDENTITY = 0, MPDG_PREC_JACOBI = 1, MPDG_PREC_CHEBYSHEV = 2 };
-enum { MPDG_FIELD_TEMPERATURE = 0 };
+enum { MPDG_FIELD_TEMPERATURE = 0, MPDG_FIELD_TEMPERATURE_OLD = 1, MPDG_FIELD_HEAVISIDE = 2 };
+/* heat material laws (MaterialTypes; Material::compute_parameters_internal,
+ * include/meltpooldg/core/material.templates.hpp:213-760).  LINEAR: rho_cp and
+ * k(T) = k0 (1 + k_alpha T).  The phase laws interpolate the gas / liquid / solid
+ * properties by the level-set heaviside H (MPDG_FIELD_HEAVISIDE; weight H, or
+ * H > 0.5 when two_phase_sharp) and the solid fraction
+ * f_s = clamp((liquidus - T) / (liquidus - solidus), 0, 1) (or T < solidus when
+ * solid_liquid_sharp) with the cubic 3 f_s^2 - 2 f_s^3; rho c_p = rho * c_p, or
+ * the interpolated rho*c_p when volume_specific.  Laws with a solid phase add
+ * the Newton terms d(rho c_p)/dT ((T - T_old)/dt + u.grad T) du and
+ * dk/dT grad T du (heat_diffuse_operator.cpp:1040-1062) and read
+ * MPDG_FIELD_TEMPERATURE_OLD.  Latent heat (apparent capacity) is not offered. */
+enum { MPDG_MAT_LINEAR = 0, MPDG_MAT_GAS_LIQUID = 1, MPDG_MAT_LIQUID_SOLID = 2, MPDG_MAT_GAS_LIQUID_SOLID = 3 };
 
 typedef struct mpdg_mesh mpdg_mesh;
 typedef struct mpdg_op mpdg_op;
@@ -92,6 +104,16 @@ typedef struct {
    * boxes.  The diagonal is built by probing (n^3 applies). */
   int supg;
   double supg_coefficient;
+  /* heat: radiative faces (heat_diffuse_operator.cpp:766-772, 1122-1124): tangent
+   * 4 eps sigma T^3 u v, residual -eps sigma (T^4 - rad_t_inf^4) v on the faces
+   * flagged as in robin_faces; sigma = 5.670374419e-8 */
+  double rad_emissivity, rad_t_inf;
+  int rad_faces;
+  /* heat: material law (MPDG_MAT_*); phase properties indexed gas, liquid, solid */
+  int material;
+  double mat_rho[3], mat_cp[3], mat_k[3];
+  double solidus, liquidus;
+  int two_phase_sharp, solid_liquid_sharp, volume_specific;
 } mpdg_op_desc;
 
 typedef struct {

@@ -22,7 +22,8 @@ VEL_NONE, VEL_ROTATION, VEL_VORTEX, VEL_CONST = 0, 1, 2, 3
 GEOM_AUTO, GEOM_GENERAL = 0, 1
 SOLVER_CG, SOLVER_GMRES = 0, 1
 PREC_IDENTITY, PREC_JACOBI, PREC_CHEBYSHEV = 0, 1, 2
-FIELD_TEMPERATURE = 0
+FIELD_TEMPERATURE, FIELD_TEMPERATURE_OLD, FIELD_HEAVISIDE = 0, 1, 2
+MAT_LINEAR, MAT_GAS_LIQUID, MAT_LIQUID_SOLID, MAT_GAS_LIQUID_SOLID = 0, 1, 2, 3
 
 _STATUS_NAMES = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_ALLOC", -4: "ERR_NOT_CONVERGED",
                  -5: "ERR_BREAKDOWN", -6: "ERR_NAN", -7: "ERR_UNSUPPORTED", -8: "ERR_BUDGET",
@@ -51,7 +52,11 @@ class OpDesc(C.Structure):
                 ("diffusivity", C.c_double), ("vel_kind", C.c_int), ("vel_param", C.c_double * 3),
                 ("precision_mask", C.c_int), ("robin_alpha", C.c_double),
                 ("robin_t_inf", C.c_double), ("robin_faces", C.c_int), ("supg", C.c_int),
-                ("supg_coefficient", C.c_double)]
+                ("supg_coefficient", C.c_double), ("rad_emissivity", C.c_double),
+                ("rad_t_inf", C.c_double), ("rad_faces", C.c_int), ("material", C.c_int),
+                ("mat_rho", C.c_double * 3), ("mat_cp", C.c_double * 3), ("mat_k", C.c_double * 3),
+                ("solidus", C.c_double), ("liquidus", C.c_double), ("two_phase_sharp", C.c_int),
+                ("solid_liquid_sharp", C.c_int), ("volume_specific", C.c_int)]
 
 
 class SolverDesc(C.Structure):

@@ -207,6 +207,14 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     if (mm.fine && (desc->k_alpha != 0.0 || desc->full_tangent || (desc->robin_faces && desc->robin_alpha != 0.0)))
       throw Error{MPDG_ERR_UNSUPPORTED,
                   "two-level meshes take constant coefficients: no k(T) law, full tangent or Robin faces"};
+    if (desc->material < MPDG_MAT_LINEAR || desc->material > MPDG_MAT_GAS_LIQUID_SOLID)
+      throw Error{MPDG_ERR_ARG, "unknown material law"};
+    if (desc->material != MPDG_MAT_LINEAR && desc->kind != MPDG_OP_HEAT)
+      throw Error{MPDG_ERR_ARG, "material laws apply to the heat operator"};
+    if (law_has_solid(desc->material) && !desc->solid_liquid_sharp && !(desc->liquidus > desc->solidus))
+      throw Error{MPDG_ERR_ARG, "the mushy zone needs liquidus > solidus"};
+    if (mm.fine && (desc->material != MPDG_MAT_LINEAR || (desc->rad_faces && desc->rad_emissivity != 0.0)))
+      throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take constant coefficients: no material law or radiation"};
     if (desc->supg && desc->kind != MPDG_OP_ADVDIFF)
       throw Error{MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator"};
     if (desc->supg && mm.fine) throw Error{MPDG_ERR_UNSUPPORTED, "SUPG on two-level meshes"};
@@ -250,7 +258,8 @@ void free_op_arrays(Op &o)
   free_workspace(o);
   for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32,
                   (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32, (void *)o.d_trig64, o.d_stage,
-                  (void *)o.d_tau64, (void *)o.d_tau32,
+                  (void *)o.d_tau64, (void *)o.d_tau32, (void *)o.Told_own, (void *)o.H_own, (void *)o.Told32,
+                  (void *)o.H32,
                   (void *)o.d_io, o.io_tmp})
     if (p) cudaFree(p);
 }
@@ -289,13 +298,28 @@ mpdg_status mpdg_op_use_dirichlet(mpdg_op *op, int use_dirichlet)
   return MPDG_OK;
 }
 
+namespace {
+// the device pointer slot and the operator-owned buffer of a field
+void field_slots(Op &o, int field, const double **&slot, double **&own)
+{
+  switch (field) {
+    case MPDG_FIELD_TEMPERATURE: slot = &o.T64; own = &o.T_own; return;
+    case MPDG_FIELD_TEMPERATURE_OLD: slot = &o.Told64; own = &o.Told_own; return;
+    case MPDG_FIELD_HEAVISIDE: slot = &o.H64; own = &o.H_own; return;
+    default: throw Error{MPDG_ERR_ARG, "unknown field"};
+  }
+}
+}  // namespace
+
 mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *values)
 {
   return guarded([&]() -> int {
     if (!op) throw Error{MPDG_ERR_ARG, "null operator"};
-    if (field != MPDG_FIELD_TEMPERATURE) throw Error{MPDG_ERR_ARG, "unknown field"};
-    if (op->o.fine) throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take no temperature field"};
-    op->o.T64 = values;
+    const double **slot = nullptr;
+    double **own = nullptr;
+    field_slots(op->o, field, slot, own);
+    if (op->o.fine) throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take no fields"};
+    *slot = values;
     invalidate_coef(op->o);
     if (values && (op->o.d.precision_mask & (1 << MPDG_FP32))) ensure_T32(op->o);
     return MPDG_OK;
@@ -306,16 +330,19 @@ mpdg_status mpdg_op_set_field_host(mpdg_op *op, int field, const double *values)
 {
   return guarded([&]() -> int {
     if (!op || !values) throw Error{MPDG_ERR_ARG, "null argument"};
-    if (field != MPDG_FIELD_TEMPERATURE) throw Error{MPDG_ERR_ARG, "unknown field"};
     Op &o = op->o;
+    const double **slot = nullptr;
+    double **own = nullptr;
+    field_slots(o, field, slot, own);
+    if (o.fine) throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take no fields"};
     const size_t bytes = sizeof(double) * o.mesh->N;
-    if (!o.T_own) {
-      MPDG_CUDA(cudaMalloc(&o.T_own, bytes));
+    if (!*own) {
+      MPDG_CUDA(cudaMalloc(own, bytes));
       o.device_bytes += bytes;
     }
-    MPDG_CUDA(cudaMemcpyAsync(o.T_own, values, bytes, cudaMemcpyHostToDevice, o.stream));
+    MPDG_CUDA(cudaMemcpyAsync(*own, values, bytes, cudaMemcpyHostToDevice, o.stream));
     MPDG_CUDA(cudaStreamSynchronize(o.stream));
-    o.T64 = o.T_own;
+    *slot = *own;
     invalidate_coef(o);
     if (o.d.precision_mask & (1 << MPDG_FP32)) ensure_T32(o);
     return MPDG_OK;

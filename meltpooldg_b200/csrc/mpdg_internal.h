@@ -111,6 +111,11 @@ struct Op {
   const double *T64 = nullptr;         // temperature (device): caller-owned, or T_own
   double *T_own = nullptr;             // operator-owned copy set from host values
   float *T32 = nullptr;                // FP32 copy of T
+  // material-law fields: T_old (laws with a solid phase) and the level-set
+  // heaviside (two-phase laws), caller-owned or set from host values
+  const double *Told64 = nullptr, *H64 = nullptr;
+  double *Told_own = nullptr, *H_own = nullptr;
+  float *Told32 = nullptr, *H32 = nullptr;  // FP32: T - T_old and the heaviside
   double *d_velb64 = nullptr;          // general geometry + velocity: [cell][3][n^3]
   float *d_velb32 = nullptr;
   float *d_trig32 = nullptr;           // uniform vortex velocity: sin/cos tables
@@ -197,6 +202,8 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
 void ensure_metric32(Mesh &m, cudaStream_t s);
 void build_op_device_data(Op &op);
 void ensure_T32(Op &op);
+inline bool law_has_solid(int mat) { return mat == MPDG_MAT_LIQUID_SOLID || mat == MPDG_MAT_GAS_LIQUID_SOLID; }
+inline bool law_two_phase(int mat) { return mat == MPDG_MAT_GAS_LIQUID || mat == MPDG_MAT_GAS_LIQUID_SOLID; }
 // marks the merged coefficient stream stale (new temperature field or dt)
 void invalidate_coef(Op &op);
 

@@ -192,6 +192,12 @@ struct KP {
   const Real *velb;       // GENERAL + velocity: [cell][3][n^3] = JxW J^-1 u
   const Real *trig;       // UNIFORM vortex: sin(pi x), cos(pi x), sin(pi y), cos(pi y)
   const Real *tau;        // SUPG: per colour-major cell tau_K
+  // heat material law (MPDG_MAT_*); LINEAR uses c_mass, c_vel, c_diff, k_alpha
+  int mat, two_phase_sharp, solid_sharp, vol_specific;
+  Real mrho[3], mcp[3], mk[3], solidus, liquidus, inv_mushy, dt_inv;
+  const Real *Told;       // T_old (laws with a solid phase), or T - T_old when told_inc
+  int told_inc;
+  const Real *Hs;         // level-set heaviside (two-phase laws)
   int supg_lap;           // SUPG with diffusion: the Laplacian term (axis-aligned cells)
   const uint8_t *dmask;
   const uint8_t *cell_flags;
@@ -353,6 +359,70 @@ __device__ __forceinline__ void uniform_velocity(const KP<Real> &p, const Tables
   }
 }
 
+// --------------------------------------------------------- material laws
+// (rho c_p / dt, rho c_p, k) at a quadrature point and their T derivatives
+// (Material::compute_parameters_internal, material.templates.hpp:213-760; the
+// solid fraction of :748-760, the cubic solid/liquid interpolation of :546-600,
+// the gas weight of :513-523; rho c_p by the product rule,
+// heat_diffuse_operator.cpp:1176-1199)
+template <typename Real>
+__device__ __forceinline__ Real ls_value(Real fs, Real vl, Real vs)
+{
+  if (fs == Real(0)) return vl;
+  if (fs == Real(1)) return vs;
+  return vl + (vs - vl) * (Real(-2) * fs * fs * fs + Real(3) * fs * fs);
+}
+
+template <typename Real>
+__device__ __forceinline__ Real ls_deriv(Real fs, Real inv_mushy, Real vl, Real vs)
+{
+  if (fs == Real(0) || fs == Real(1)) return Real(0);
+  return -inv_mushy * (vs - vl) * (Real(-6) * fs * fs + Real(6) * fs);
+}
+
+template <typename Real>
+__device__ __forceinline__ void law_eval(const KP<Real> &p, Real T, Real H, Real &cm, Real &cv, Real &kq,
+                                         Real &dcm, Real &dcv, Real &dk)
+{
+  if (p.mat == MPDG_MAT_LINEAR) {
+    cm = p.c_mass;
+    cv = p.c_vel;
+    kq = p.c_diff * (Real(1) + p.k_alpha * T);
+    dk = p.c_diff * p.k_alpha;
+    dcm = dcv = Real(0);
+    return;
+  }
+  const bool gas = p.mat == MPDG_MAT_GAS_LIQUID || p.mat == MPDG_MAT_GAS_LIQUID_SOLID;
+  const bool sol = p.mat == MPDG_MAT_LIQUID_SOLID || p.mat == MPDG_MAT_GAS_LIQUID_SOLID;
+  Real fs = 0;
+  if (sol) {
+    fs = p.solid_sharp ? (T < p.solidus ? Real(1) : Real(0))
+                       : fmin(fmax((p.liquidus - T) * p.inv_mushy, Real(0)), Real(1));
+  }
+  const Real w = gas ? (p.two_phase_sharp ? (H > Real(0.5) ? Real(1) : Real(0)) : H) : Real(1);
+  Real v[4], dv[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const Real vl = (e == 0) ? p.mrho[1] : (e == 1) ? p.mcp[1] : (e == 2) ? p.mk[1] : p.mrho[1] * p.mcp[1];
+    const Real vs = (e == 0) ? p.mrho[2] : (e == 1) ? p.mcp[2] : (e == 2) ? p.mk[2] : p.mrho[2] * p.mcp[2];
+    const Real vg = (e == 0) ? p.mrho[0] : (e == 1) ? p.mcp[0] : (e == 2) ? p.mk[0] : p.mrho[0] * p.mcp[0];
+    v[e] = sol ? ls_value(fs, vl, vs) : vl;
+    dv[e] = sol ? ls_deriv(fs, p.inv_mushy, vl, vs) : Real(0);
+    if (gas) {
+      v[e] = (Real(1) - w) * vg + w * v[e];
+      dv[e] = w * dv[e];
+    }
+  }
+  const Real rc = p.vol_specific ? v[3] : v[0] * v[1];
+  const Real drc = p.vol_specific ? dv[3] : dv[1] * v[0] + dv[0] * v[1];
+  cm = rc * p.dt_inv;
+  cv = rc;
+  kq = v[2];
+  dcm = drc * p.dt_inv;
+  dcv = drc;
+  dk = dv[2];
+}
+
 #include "apply_warp.cuh"
 #include "batch_apply.cuh"
 
@@ -409,6 +479,21 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
     for (int k = 0; k < n; ++k) tl[k] = active ? p.T[g0 + k * zs] : Real(0);
     to_qp<n>(sS, t1, i, j, tl, Tq);
     if (MODE == MODE_HEAT_RESIDUAL || p.full_tangent) grad_qp<n>(sDc, t1, i, j, Tq, Tgx, Tgy, Tgz);
+  }
+  // material-law fields at the Gauss points: heaviside (two-phase laws), T_old
+  // (Newton terms of laws with a solid phase)
+  Real Hq[n], Oq[n];
+  if (needT && p.Hs) {
+    Real hl[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) hl[k] = active ? p.Hs[g0 + k * zs] : Real(0);
+    to_qp<n>(sS, t1, i, j, hl, Hq);
+  }
+  if (KT && MODE != MODE_HEAT_RESIDUAL && p.full_tangent && p.Told) {
+    Real ol[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) ol[k] = active ? p.Told[g0 + k * zs] : Real(0);
+    to_qp<n>(sS, t1, i, j, ol, Oq);
   }
   Real oq[n], hq[n];
   if (MODE == MODE_HEAT_RESIDUAL) {
@@ -482,8 +567,8 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
         b2 = JxW * uv[2] / p.h[2];
       }
     }
-    Real kq = p.c_diff;
-    if (needT) kq = p.c_diff * (Real(1) + p.k_alpha * Tq[k]);
+    Real cm = p.c_mass, cv = p.c_vel, kq = p.c_diff, dcm = 0, dcv = 0, dk = 0;
+    if (needT) law_eval<Real>(p, Tq[k], p.Hs ? Hq[k] : Real(0), cm, cv, kq, dcm, dcv, dk);
     const Real adv = b0 * gx[k] + b1 * gy[k] + b2 * gz[k];
     Real f0, f1, f2;
     if (GEOM == GEOM_GENERAL) {
@@ -497,12 +582,12 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
     }
     if (MODE == MODE_HEAT_RESIDUAL) {
       // -( rho_cp/dt (T - T_old) - q + rho_cp vel.grad T ) N - k(T) grad T . grad N
-      val[k] = -(p.c_mass * JxW * (uq[k] - oq[k]) - JxW * hq[k] + p.c_vel * adv);
+      val[k] = -(cm * JxW * (uq[k] - oq[k]) - JxW * hq[k] + cv * adv);
       fx[k] = -kq * f0;
       fy[k] = -kq * f1;
       fz[k] = -kq * f2;
     } else {
-      val[k] = p.c_mass * JxW * uq[k] + p.c_vel * adv;
+      val[k] = cm * JxW * uq[k] + cv * adv;
       fx[k] = kq * f0;
       fy[k] = kq * f1;
       fz[k] = kq * f2;
@@ -525,15 +610,20 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
       }
       if (KT && p.full_tangent) {
         // dk/dT grad T du, tested with grad N: G (reference grad T) scaled by u
-        const Real dk = p.c_diff * p.k_alpha * uq[k];
+        const Real du = dk * uq[k];
         if (GEOM == GEOM_GENERAL) {
-          fx[k] += dk * (G00 * Tgx[k] + G01 * Tgy[k] + G02 * Tgz[k]);
-          fy[k] += dk * (G01 * Tgx[k] + G11 * Tgy[k] + G12 * Tgz[k]);
-          fz[k] += dk * (G02 * Tgx[k] + G12 * Tgy[k] + G22 * Tgz[k]);
+          fx[k] += du * (G00 * Tgx[k] + G01 * Tgy[k] + G02 * Tgz[k]);
+          fy[k] += du * (G01 * Tgx[k] + G11 * Tgy[k] + G12 * Tgz[k]);
+          fz[k] += du * (G02 * Tgx[k] + G12 * Tgy[k] + G22 * Tgz[k]);
         } else {
-          fx[k] += dk * G00 * Tgx[k];
-          fy[k] += dk * G11 * Tgy[k];
-          fz[k] += dk * G22 * Tgz[k];
+          fx[k] += du * G00 * Tgx[k];
+          fy[k] += du * G11 * Tgy[k];
+          fz[k] += du * G22 * Tgz[k];
+        }
+        // d(rho c_p)/dT ((T - T_old)/dt + u.grad T) du tested with N
+        if (p.Told) {
+          const Real dT = p.told_inc ? Oq[k] : Tq[k] - Oq[k];
+          val[k] += (dcm * dT * JxW + dcv * (b0 * Tgx[k] + b1 * Tgy[k] + b2 * Tgz[k])) * uq[k];
         }
       }
     }
@@ -621,6 +711,19 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
     to_qp<n>(tb[3], t, i, j, tl, Tq);
     if (p.full_tangent) grad_qp<n>(tb[4], t, i, j, Tq, Tgx, Tgy, Tgz);
   }
+  Real Hq[n], Oq[n];
+  if (KT && p.Hs) {
+    Real hl[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) hl[k] = active ? p.Hs[g0 + k * zs] : Real(0);
+    to_qp<n>(tb[3], t, i, j, hl, Hq);
+  }
+  if (KT && p.full_tangent && p.Told) {
+    Real ol[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) ol[k] = active ? p.Told[g0 + k * zs] : Real(0);
+    to_qp<n>(tb[3], t, i, j, ol, Oq);
+  }
   Real Fm[n], F00[n], F11[n], F22[n], F01[n], F02[n], F12[n], Fb0[n], Fb1[n], Fb2[n];
 #pragma unroll
   for (int k = 0; k < n; ++k) {
@@ -654,9 +757,11 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
         b2 = JxW * uv[2] / p.h[2];
       }
     }
-    Real kq = p.c_diff;
-    if (KT) kq = p.c_diff * (Real(1) + p.k_alpha * Tq[k]);
-    Fm[k] = p.c_mass * JxW;
+    Real cm = p.c_mass, cv = p.c_vel, kq = p.c_diff, dcm = 0, dcv = 0, dk = 0;
+    if (KT) law_eval<Real>(p, Tq[k], p.Hs ? Hq[k] : Real(0), cm, cv, kq, dcm, dcv, dk);
+    Fm[k] = cm * JxW;
+    if (KT && p.full_tangent && p.Told)
+      Fm[k] += dcm * (Tq[k] - Oq[k]) * JxW + dcv * (b0 * Tgx[k] + b1 * Tgy[k] + b2 * Tgz[k]);
     F00[k] = kq * G00;
     F11[k] = kq * G11;
     F22[k] = kq * G22;
@@ -665,9 +770,8 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
     F12[k] = 2 * kq * G12;
     // velocity term phi_i (b . grad phi_i), plus the full-tangent term
     // grad phi_i . (dk G gradT) phi_i, which has the same table structure
-    Real e0 = p.c_vel * b0, e1 = p.c_vel * b1, e2 = p.c_vel * b2;
+    Real e0 = cv * b0, e1 = cv * b1, e2 = cv * b2;
     if (KT && p.full_tangent) {
-      const Real dk = p.c_diff * p.k_alpha;
       e0 += dk * (G00 * Tgx[k] + G01 * Tgy[k] + G02 * Tgz[k]);
       e1 += dk * (G01 * Tgx[k] + G11 * Tgy[k] + G12 * Tgz[k]);
       e2 += dk * (G02 * Tgx[k] + G12 * Tgy[k] + G22 * Tgz[k]);
@@ -1219,13 +1323,31 @@ void build_op_device_data(Op &op)
   }
 }
 
+__global__ void diff_cast_kernel(const double *a, const double *b, float *c, long n)
+{
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) c[i] = (float)(a[i] - b[i]);
+}
+
+// FP32 copies of the fields the FP32 form reads: T, the heaviside, and the
+// increment T - T_old (formed in FP64: the float copies of T and T_old would
+// lose its digits to cancellation)
 void ensure_T32(Op &op)
 {
-  if (!op.T64) return;
   const long N = op.mesh->N;
-  if (!op.T32) op.T32 = dev_alloc<float>(N, op.device_bytes);
-  cast_kernel<<<grid_for(N, 256), 256, 0, op.stream>>>(op.T64, op.T32, N);
-  MPDG_LAUNCHED();
+  const double *src[2] = {op.T64, op.H64};
+  float **dst[2] = {&op.T32, &op.H32};
+  for (int f = 0; f < 2; ++f) {
+    if (!src[f]) continue;
+    if (!*dst[f]) *dst[f] = dev_alloc<float>(N, op.device_bytes);
+    cast_kernel<<<grid_for(N, 256), 256, 0, op.stream>>>(src[f], *dst[f], N);
+    MPDG_LAUNCHED();
+  }
+  if (op.T64 && op.Told64) {
+    if (!op.Told32) op.Told32 = dev_alloc<float>(N, op.device_bytes);
+    diff_cast_kernel<<<grid_for(N, 256), 256, 0, op.stream>>>(op.T64, op.Told64, op.Told32, N);
+    MPDG_LAUNCHED();
+  }
 }
 
 namespace {
@@ -1279,6 +1401,31 @@ KP<Real> base_params(Op &op)
   k.c_diff = (Real)(heat ? op.d.k0 : op.d.theta * op.d.diffusivity);
   k.k_alpha = (Real)(heat ? op.d.k_alpha : 0.0);
   k.full_tangent = heat && op.d.full_tangent;
+  // heat material law
+  const bool law = heat && op.d.material != MPDG_MAT_LINEAR;
+  const bool law_T = law && law_has_solid(op.d.material), law_H = law && law_two_phase(op.d.material);
+  k.mat = law ? op.d.material : MPDG_MAT_LINEAR;
+  k.two_phase_sharp = op.d.two_phase_sharp;
+  k.solid_sharp = op.d.solid_liquid_sharp;
+  k.vol_specific = op.d.volume_specific;
+  for (int e = 0; e < 3; ++e) {
+    k.mrho[e] = (Real)op.d.mat_rho[e];
+    k.mcp[e] = (Real)op.d.mat_cp[e];
+    k.mk[e] = (Real)op.d.mat_k[e];
+  }
+  k.solidus = (Real)op.d.solidus;
+  k.liquidus = (Real)op.d.liquidus;
+  k.inv_mushy = law_T ? (Real)(1.0 / (op.d.liquidus - op.d.solidus)) : Real(0);
+  k.dt_inv = (Real)(1.0 / op.d.dt);
+  if (law_T) k.full_tangent = 1;  // heat_diffuse_operator.cpp:1040-1055 (do_solidification)
+  if constexpr (sizeof(Real) == 8) {
+    k.Told = law_T ? op.Told64 : nullptr;
+    k.Hs = law_H ? op.H64 : nullptr;
+  } else {
+    k.Told = law_T ? op.Told32 : nullptr;  // T - T_old
+    k.told_inc = 1;
+    k.Hs = law_H ? op.H32 : nullptr;
+  }
   const bool mask = op.use_dirichlet && m.has_dirichlet;
   k.masked_read = mask;
   k.masked_write = mask;
@@ -1339,7 +1486,20 @@ bool supg(const Op &op) { return op.d.kind == MPDG_OP_ADVDIFF && op.d.supg; }
 
 bool uses_kT(const Op &op)
 {
-  return op.d.kind == MPDG_OP_HEAT && (op.d.k_alpha != 0.0 || op.d.full_tangent);
+  return op.d.kind == MPDG_OP_HEAT && (op.d.k_alpha != 0.0 || op.d.full_tangent || op.d.material != MPDG_MAT_LINEAR);
+}
+
+bool uses_law(const Op &op) { return op.d.kind == MPDG_OP_HEAT && op.d.material != MPDG_MAT_LINEAR; }
+
+// the fields a material law reads must be set before it is applied
+template <typename Real>
+void check_law_fields(const Op &op, const KP<Real> &k)
+{
+  if (!uses_law(op)) return;
+  if (law_has_solid(op.d.material) && !k.Told)
+    throw Error{MPDG_ERR_ARG, "this material law needs the T_old field (MPDG_FIELD_TEMPERATURE_OLD)"};
+  if (law_two_phase(op.d.material) && !k.Hs)
+    throw Error{MPDG_ERR_ARG, "this material law needs the heaviside field (MPDG_FIELD_HEAVISIDE)"};
 }
 
 }  // namespace
@@ -1464,8 +1624,9 @@ enum { ROBIN_APPLY = 0, ROBIN_RESIDUAL = 1, ROBIN_DIAGONAL = 2 };
 
 template <int P, typename Real>
 __global__ void __launch_bounds__(128) robin_kernel(const double *vert, int nc0, int nc1, int nc2, int d, int s,
-                                                    int colour, long NX, long NY, double alpha, double t_inf,
-                                                    int mode, const Real *src, Real *dst,
+                                                    int colour, long NX, long NY, int conv, double alpha,
+                                                    double t_inf, int rad, double es, double t_rad, int mode,
+                                                    const Real *src, const Real *Tf, Real *dst,
                                                     const uint8_t *rmask, const uint8_t *wmask)
 {
   constexpr int n = P + 1, n2 = n * n;
@@ -1518,9 +1679,32 @@ __global__ void __launch_bounds__(128) robin_kernel(const double *vert, int nc0,
                         Ja[0] * Jb[1] - Ja[1] * Jb[0]};
   const double jxw = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) * (double)T.w[a] * (double)T.w[b];
   Real *t = tile[warp];
+  // face interpolation: lane (a, b) holds a nodal value and receives the value
+  // at face quadrature point (a, b), along t0 then t1
+  const auto interp = [&](Real v) -> Real {
+    if (on) t[b * n + a] = v;
+    __syncwarp();
+    Real w = 0;
+    for (int r = 0; r < n; ++r) w += T.S[a * n + r] * t[b * n + r];
+    __syncwarp();
+    if (on) t[b * n + a] = w;
+    __syncwarp();
+    Real q = 0;
+    for (int r = 0; r < n; ++r) q += T.S[b * n + r] * t[r * n + a];
+    __syncwarp();
+    return q;
+  };
+  // T at the point: the residual's argument, or the linearisation point of the
+  // radiative tangent
+  Real Tq = 0;
+  if (rad || mode == ROBIN_RESIDUAL) {
+    const Real *Ts = (mode == ROBIN_RESIDUAL) ? src : Tf;
+    Tq = interp(on ? Ts[g] : Real(0));
+  }
+  const Real coef = (conv ? (Real)alpha : Real(0)) + (rad ? Real(4) * (Real)es * Tq * Tq * Tq : Real(0));
   Real out;
   if (mode == ROBIN_DIAGONAL) {
-    if (on) t[b * n + a] = (Real)(alpha * jxw);
+    if (on) t[b * n + a] = coef * (Real)jxw;
     __syncwarp();
     out = 0;
     for (int qb = 0; qb < n; ++qb)
@@ -1529,26 +1713,18 @@ __global__ void __launch_bounds__(128) robin_kernel(const double *vert, int nc0,
         out += sa * sa * sb * sb * t[qb * n + qa];
       }
   } else {
-    Real u = 0;
-    if (on) {
-      if (mode == ROBIN_RESIDUAL) u = (Real)t_inf - src[g];
-      else u = (rmask && rmask[g]) ? Real(0) : src[g];
+    Real val;
+    if (mode == ROBIN_RESIDUAL) {
+      const Real tr = (Real)t_rad, T2 = Tq * Tq;
+      val = -(conv ? (Real)alpha * (Tq - (Real)t_inf) : Real(0)) -
+            (rad ? (Real)es * (T2 * T2 - tr * tr * tr * tr) : Real(0));
+    } else {
+      val = coef * interp(on ? ((rmask && rmask[g]) ? Real(0) : src[g]) : Real(0));
     }
-    // values at the face quadrature points: along t0, then t1
-    if (on) t[b * n + a] = u;
+    // tested with the face shape functions: transposed passes
+    if (on) t[b * n + a] = val * (Real)jxw;
     __syncwarp();
     Real w = 0;
-    for (int r = 0; r < n; ++r) w += T.S[a * n + r] * t[b * n + r];
-    __syncwarp();
-    if (on) t[b * n + a] = w;
-    __syncwarp();
-    Real uq = 0;
-    for (int r = 0; r < n; ++r) uq += T.S[b * n + r] * t[r * n + a];
-    __syncwarp();
-    // tested with the face shape functions: transposed passes
-    if (on) t[b * n + a] = (Real)(alpha * jxw) * uq;
-    __syncwarp();
-    w = 0;
     for (int r = 0; r < n; ++r) w += T.S[r * n + a] * t[b * n + r];
     __syncwarp();
     if (on) t[b * n + a] = w;
@@ -1563,15 +1739,24 @@ template <typename Real>
 void launch_robin(Op &op, Real *dst, const Real *src, int mode)
 {
   const mpdg_op_desc &D = op.d;
-  if (D.kind != MPDG_OP_HEAT || !D.robin_faces || D.robin_alpha == 0.0) return;
+  if (D.kind != MPDG_OP_HEAT) return;
+  const bool any_conv = D.robin_faces && D.robin_alpha != 0.0, any_rad = D.rad_faces && D.rad_emissivity != 0.0;
+  if (!any_conv && !any_rad) return;
   Mesh &m = *op.mesh;
+  const Real *Tf = nullptr;
+  if constexpr (sizeof(Real) == 8) Tf = op.T64;
+  else Tf = op.T32;
+  if (any_rad && !Tf) throw Error{MPDG_ERR_ARG, "radiative faces need the temperature field"};
+  const double es = D.rad_emissivity * 5.670374419e-8;  // Stefan-Boltzmann constant
   upload_tables();
   const bool mask = op.use_dirichlet && m.has_dirichlet;
   const uint8_t *rmask = (mode == ROBIN_APPLY && mask) ? m.d_dmask : nullptr;
   const uint8_t *wmask = mask ? m.d_dmask : nullptr;
   for (int d = 0; d < 3; ++d)
     for (int s = 0; s < 2; ++s) {
-      if (!(D.robin_faces & (1 << (2 * d + s)))) continue;
+      const int bit = 1 << (2 * d + s);
+      const int conv = any_conv && (D.robin_faces & bit), rad = any_rad && (D.rad_faces & bit);
+      if (!conv && !rad) continue;
       const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
       for (int c = 0; c < 4; ++c) {
         const long ca = (m.nc[t0] - (c & 1) + 1) / 2, cb = (m.nc[t1] - ((c >> 1) & 1) + 1) / 2;
@@ -1580,8 +1765,8 @@ void launch_robin(Op &op, Real *dst, const Real *src, int mode)
         const unsigned grid = (unsigned)((faces + 3) / 4);
 #define MPDG_ROBIN(PP)                                                                                   \
   robin_kernel<PP, Real><<<grid, 128, 0, op.stream>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], d, s, c, m.NX, \
-                                                      m.NY, D.robin_alpha, D.robin_t_inf, mode, src, dst, \
-                                                      rmask, wmask)
+                                                      m.NY, conv, D.robin_alpha, D.robin_t_inf, rad, es,   \
+                                                      D.rad_t_inf, mode, src, Tf, dst, rmask, wmask)
         switch (m.degree) {
           case 1: MPDG_ROBIN(1); break;
           case 2: MPDG_ROBIN(2); break;
@@ -1753,6 +1938,7 @@ void launch_cells(Op &op, Real *dst, const Real *src)
   k.src = src;
   k.dst = dst;
   if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
+  check_law_fields(op, k);
   if (supg(op)) {
     // SUPG: block kernel with the stabilisation flux (raw geometry on general meshes)
     if (!k.tau) throw Error{MPDG_ERR_ARG, "the FP32 form was not prepared for this operator (precision_mask)"};
@@ -1764,7 +1950,8 @@ void launch_cells(Op &op, Real *dst, const Real *src)
     dispatch_degree<Real, MODE_SUPG, false>(op, k);
     return;
   }
-  if (!full && !m.uniform) {
+  const bool law = uses_law(op);
+  if (!full && !law && !m.uniform) {
     // general geometry: merged coefficient stream (k(T), c_mass, c_diff folded in)
     ensure_coef(op, sizeof(Real) == 4);
     if constexpr (sizeof(Real) == 8) k.metric = op.d_coef64;
@@ -1776,7 +1963,7 @@ void launch_cells(Op &op, Real *dst, const Real *src)
     warp_apply_degree<Real, GEOM_UNIFORM>(op, k);
     return;
   }
-  // full Newton tangent, or k(T) on a uniform mesh: block kernel on raw geometry
+  // full Newton tangent, material laws, or k(T) on a uniform mesh: block kernel on raw geometry
   if (!m.uniform && sizeof(Real) == 4) {
     ensure_metric32(m, op.stream);
     k.metric = (const Real *)(const void *)m.d_metric32;
@@ -1798,6 +1985,7 @@ void launch_rhs(Op &op, double *dst, const double *src, const double *heat_sourc
   k.masked_read = 0;  // read_dof_values_plain
   if (op.d.kind == MPDG_OP_HEAT) {
     if (!op.T64) throw Error{MPDG_ERR_ARG, "heat residual needs the temperature field"};
+    check_law_fields(op, k);
     k.q_src = heat_source;
     dispatch_degree<double, MODE_HEAT_RESIDUAL, false>(op, k);
     launch_robin<double>(op, dst, op.T64, ROBIN_RESIDUAL);
@@ -1944,6 +2132,7 @@ void launch_block_diagonal(Op &op, double *diag)
   k.dst = diag;
   const bool kt = uses_kT(op);
   if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
+  check_law_fields(op, k);
   MPDG_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * m.N_own, op.stream));
 
   switch (m.degree) {
@@ -1998,6 +2187,7 @@ bool apply_ready_without_allocation(const Op &op)
   const Mesh &m = *op.mesh;
   const bool full = op.d.kind == MPDG_OP_HEAT && op.d.full_tangent;
   if (supg(op)) return false;                    // the diagonal probes allocate
+  if (uses_law(op)) return true;                 // block kernel on raw geometry
   if (!full && !m.uniform) return op.coef64_ok;  // merged stream already built
   return true;                                   // nothing is built lazily on these paths
 }

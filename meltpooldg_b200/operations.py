@@ -93,16 +93,27 @@ class AdvectionDiffusionOperation:
 
 
 class HeatDiffuseOperation:
-    """One heat time step with Newton-Raphson (constant or k(T) conductivity)."""
+    """One heat time step with Newton-Raphson (HeatDiffuseOperation::solve,
+    source/heat/heat_diffuse_operation.cpp; newton_raphson_solver.cpp:24-80).
+    `heaviside(t)` returns the nodal level-set heaviside at time t for the
+    two-phase laws (re-interpolated before every step,
+    heat_transfer_application.cpp:67-70)."""
 
     def __init__(self, mesh, dt, rho_cp=1.0, k0=1.0, k_alpha=0.0, full_tangent=False,
                  linear_solver: LinearSolverData = None, residual_tolerance=1e-9,
                  field_correction_tolerance=1e-10, max_nonlinear_iterations=10, device="cuda",
-                 robin_alpha=0.0, robin_t_inf=0.0, robin_faces=()):
+                 robin_alpha=0.0, robin_t_inf=0.0, robin_faces=(), rad_emissivity=0.0, rad_t_inf=0.0,
+                 rad_faces=(), velocity=None, material=None, heaviside=None):
         self.mesh = mesh
         self.op = HeatDiffuseOperator(mesh, dt, rho_cp=rho_cp, k0=k0, k_alpha=k_alpha,
                                       full_tangent=full_tangent, robin_alpha=robin_alpha,
-                                      robin_t_inf=robin_t_inf, robin_faces=robin_faces)
+                                      robin_t_inf=robin_t_inf, robin_faces=robin_faces,
+                                      rad_emissivity=rad_emissivity, rad_t_inf=rad_t_inf, rad_faces=rad_faces,
+                                      velocity=velocity, material=material)
+        self.dt = dt
+        self.time = 0.0
+        self.heaviside = heaviside
+        self.H = None
         self.data = linear_solver or LinearSolverData(solver_type="GMRES", preconditioner_type="Diagonal")
         self.res_tol = residual_tolerance
         self.dx_tol = field_correction_tolerance
@@ -119,8 +130,13 @@ class HeatDiffuseOperation:
 
     def solve(self):
         T = self.temperature
+        self.time += self.dt
+        if self.heaviside is not None:
+            self.H = torch.tensor(np.asarray(self.heaviside(self.time), np.float64), device=self.device)
+            self.op.set_heaviside(self.H)
         self.op.set_temperature(T)
         T_old = T.clone()
+        self.op.set_temperature_old(T_old)
         rhs = torch.empty_like(T)
         dx = torch.empty_like(T)
         for i in range(self.max_nl):

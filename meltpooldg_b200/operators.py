@@ -228,17 +228,40 @@ class HeatDiffuseOperator(_MatrixFreeOperator):
     `full_tangent` adds the Newton term dk/dT grad(T) u (non-symmetric).
     `robin_faces` lists the box faces (direction, side) with the convective
     condition of heat_diffuse_operator.cpp:1088-1129 (tangent alpha u v,
-    residual -alpha (T - t_inf) v)."""
+    residual -alpha (T - t_inf) v); `rad_faces` those with the radiative one
+    (tangent 4 eps sigma T^3 u v, residual -eps sigma (T^4 - rad_t_inf^4) v).
+    `material` selects a phase law (Material, material.templates.hpp:213-760):
+    a dict with `kind` ("gas_liquid", "liquid_solid", "gas_liquid_solid"),
+    `rho`, `cp`, `k` as (gas, liquid, solid) and `solidus`, `liquidus`,
+    `two_phase_sharp`, `solid_liquid_sharp`, `volume_specific`; the laws read
+    the heaviside (`set_heaviside`) and, with a solid phase, T_old
+    (`set_temperature_old`)."""
+
+    MATERIALS = {"gas_liquid": A.MAT_GAS_LIQUID, "liquid_solid": A.MAT_LIQUID_SOLID,
+                 "gas_liquid_solid": A.MAT_GAS_LIQUID_SOLID}
 
     def __init__(self, mesh, dt, rho_cp=1.0, k0=1.0, k_alpha=0.0, full_tangent=False,
                  velocity=None, precisions=("fp64",), robin_alpha=0.0, robin_t_inf=0.0,
-                 robin_faces=()):
+                 robin_faces=(), rad_emissivity=0.0, rad_t_inf=0.0, rad_faces=(), material=None):
         vk, vp = _velocity(velocity)
         d = A.OpDesc(A.OP_HEAT, dt, rho_cp, k0, k_alpha, int(full_tangent), 0.0, 0.0, vk,
                      (C.c_double * 3)(*vp), 0)
         d.robin_alpha = float(robin_alpha)
         d.robin_t_inf = float(robin_t_inf)
         d.robin_faces = sum(1 << (2 * int(dd) + int(ss)) for dd, ss in robin_faces)
+        d.rad_emissivity = float(rad_emissivity)
+        d.rad_t_inf = float(rad_t_inf)
+        d.rad_faces = sum(1 << (2 * int(dd) + int(ss)) for dd, ss in rad_faces)
+        if material:
+            kind = material["kind"]
+            d.material = self.MATERIALS[kind] if isinstance(kind, str) else int(kind)
+            for name in ("rho", "cp", "k"):
+                setattr(d, "mat_" + name, (C.c_double * 3)(*[float(v) for v in material.get(name, (0, 0, 0))]))
+            d.solidus = float(material.get("solidus", 0.0))
+            d.liquidus = float(material.get("liquidus", 0.0))
+            d.two_phase_sharp = int(bool(material.get("two_phase_sharp", False)))
+            d.solid_liquid_sharp = int(bool(material.get("solid_liquid_sharp", False)))
+            d.volume_specific = int(bool(material.get("volume_specific", False)))
         super().__init__(mesh, d, precisions)
 
     def set_temperature(self, T):
@@ -246,6 +269,16 @@ class HeatDiffuseOperator(_MatrixFreeOperator):
         vector the reference operator holds by reference)."""
         self._fields["T"] = T
         A.check(A.lib().mpdg_op_set_field(self._h, A.FIELD_TEMPERATURE, _dptr(T)), "set_field")
+
+    def set_temperature_old(self, T_old):
+        """T_old of the Newton terms of laws with a solid phase (`temperature_old`)."""
+        self._fields["T_old"] = T_old
+        A.check(A.lib().mpdg_op_set_field(self._h, A.FIELD_TEMPERATURE_OLD, _dptr(T_old)), "set_field")
+
+    def set_heaviside(self, H):
+        """The level set as heaviside of the two-phase laws (`level_set_as_heaviside`)."""
+        self._fields["H"] = H
+        A.check(A.lib().mpdg_op_set_field(self._h, A.FIELD_HEAVISIDE, _dptr(H)), "set_field")
 
     def create_rhs(self, dst, src, heat_source=None):
         """dst += -R(T): Newton residual with T the operator's temperature and
