@@ -211,6 +211,21 @@ mpdg_status mpdg_op_device_error(mpdg_op *op, int *flag);
 mpdg_status mpdg_vmult(mpdg_op *op, double *dst, const double *src);
 /* the same operator applied in FP32 (operator data and vectors in FP32) */
 mpdg_status mpdg_vmult_f32(mpdg_op *op, float *dst, const float *src);
+/* dst[v] = A src[v] for n_vectors device vectors (host arrays of device
+ * pointers; no destination may overlap any vector).  Operators whose apply is
+ * the plain cell kernel (no boundary faces, inflow rows, hanging nodes, SUPG or
+ * phase law) read each cell's coefficients once per pass of up to 4 vectors;
+ * the others apply the vectors in turn.  Replaces the n vmult calls of
+ * LeastSquaresProjection::vmult (include/meltpooldg/linear_algebra/predictor.hpp:37-46). */
+mpdg_status mpdg_vmult_multi(mpdg_op *op, int n_vectors, double *const *dst, const double *const *src);
+mpdg_status mpdg_vmult_multi_f32(mpdg_op *op, int n_vectors, float *const *dst, const float *const *src);
+/* LeastSquaresProjection::vmult (predictor.hpp:37-80): solution = sum_s c_s old[s]
+ * minimising |A sum_s c_s old[s] - rhs| over the first old solutions whose images
+ * stay independent (modified Gram-Schmidt, stop when the new image's squared norm
+ * falls below 1e-16 of the first's).  n_old = 1..32 device vectors; *n_used (may
+ * be NULL) receives how many were used (0: the first image is zero, solution = 0). */
+mpdg_status mpdg_predict_lsq(mpdg_op *op, int n_old, const double *const *old_solutions, const double *rhs,
+                             double *solution, int *n_used);
 /* host-buffer form: copies src to the device, applies, copies dst back */
 mpdg_status mpdg_vmult_host(mpdg_op *op, double *dst_host, const double *src_host);
 

@@ -246,10 +246,14 @@ struct WOcc {
                                                        : (P == 4 ? 5 : P == 3 ? 6 : P == 2 ? 7 : 8);
 };
 
-template <int P, typename Real, int GEOM, bool HANG = false>
+// MULTI: applies the operator to p.nvec (<= kMaxMultiVec) vectors msrc[v] ->
+// mdst[v] (msrc[0] = src, mdst[0] = dst) in one pass: each group's coefficient
+// block is staged once and serves every vector
+template <int P, typename Real, int GEOM, bool HANG = false, bool MULTI = false>
 __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     warp_apply_kernel(const KP<Real> p, int *err)
 {
+  static_assert(!(HANG && MULTI), "the multi-vector apply has no hanging-node path");
   constexpr int n = P + 1, n2 = n * n, n3 = n2 * n, CPW = WCfg<n>::cpw;
   constexpr int MS = metric_stride(n), VS = velb_stride(n);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -292,6 +296,16 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   // nothing here consumes a load, so the loads stay in flight while the
   // current group is computed
   const bool use_mask = p.cell_mask != nullptr && (p.masked_read || p.masked_write);
+  // column of vector src_v for the lane's cell in group grp (multi-vector apply)
+  auto gather_col = [&](int grp, const Real *src_v, Real (&B)[n]) {
+    const int cidx = grp * CPW + sub;
+    const bool act = lane_ok && cidx < count;
+    int ix = 0, iy = 0, iz = 0;
+    if (act) colour_cell(cidx, p, ix, iy, iz);
+    const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
+#pragma unroll
+    for (int k = 0; k < n; ++k) B[k] = act ? src_v[g0 + k * zs] : Real(0);
+  };
   auto gather = [&](int grp, Real (&A)[n], uint4 &cm) {
     const int cidx = grp * CPW + sub;
     const bool act = lane_ok && grp * CPW < count && cidx < count;
@@ -356,28 +370,41 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     const bool sx = (i == 0 && ix > 0) || (i == P && ix < p.nc[0] - 1);
     const bool sy = (j == 0 && iy > 0) || (j == P && iy < p.nc[1] - 1);
     const bool later_xy = (sx && (ix & 1)) || (sy && (iy & 1));
-    Real dpre[n];
     unsigned first_bits = 0, mask_bits = 0;
 #pragma unroll
     for (int k = 0; k < n; ++k) {
-      const long g = g0 + k * zs;
       const bool sz = (k == 0 && iz > 0) || (k == P && iz < p.nc[2] - 1);
       const bool first = !(later_xy || (sz && (iz & 1)));
       const bool masked = p.masked_write && mask_bit(cm, k);
       first_bits |= (unsigned)first << k;
       mask_bits |= (unsigned)masked << k;
-      dpre[k] = (active && !first && !masked && !hl) ? p.dst[g] : Real(0);
+    }
+    const int nv = MULTI ? p.nvec : 1;
+    for (int v = 0; v < nv; ++v) {
+    Real *dst_v = (MULTI && v > 0) ? p.mdst[v] : p.dst;
+    Real dpre[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k) {
+      const bool first = (first_bits >> k) & 1, masked = (mask_bits >> k) & 1;
+      dpre[k] = (active && !first && !masked && !hl) ? dst_v[g0 + k * zs] : Real(0);
     }
 
     Real u[n];
+    if (!MULTI || v == 0) {
 #pragma unroll
-    for (int k = 0; k < n; ++k) u[k] = (p.masked_read && mask_bit(cm, k)) ? Real(0) : A[k];
-    if (has_next) gather(gnext, A, cmA);
+      for (int k = 0; k < n; ++k) u[k] = (p.masked_read && mask_bit(cm, k)) ? Real(0) : A[k];
+      if (has_next) gather(gnext, A, cmA);
+    } else {
+      Real B[n];
+      gather_col(group, p.msrc[v], B);
+#pragma unroll
+      for (int k = 0; k < n; ++k) u[k] = (p.masked_read && mask_bit(cm, k)) ? Real(0) : B[k];
+    }
 
     Real uq[n], gx[n], gy[n], gz[n];
     l_forward<n>(T.S, T.Dc, t0, t1, lane_ok, i, j, u, uq, gx, gy, gz);
 
-    if (GEOM == GEOM_GENERAL) {
+    if (GEOM == GEOM_GENERAL && v == 0) {
       mbar_wait_bounded(&bars[warp], phase, err);
       phase ^= 1;
     }
@@ -386,6 +413,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     Real uv0[3] = {0, 0, 0};
     if (GEOM != GEOM_GENERAL && has_vel && p.vel_kind != MPDG_VEL_ROTATION)
       uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, 0, uv0);
+
     Real val[n], fx[n], fy[n], fz[n];
     const Real *ms = stage + s_sub * MS + j * n + i;
     const Real *vs = vstage + s_sub * VS + j * n + i;
@@ -422,8 +450,8 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
         fz[k] = kd * p.ih2[2] * gz[k];
       }
     }
-    if (GEOM == GEOM_GENERAL) {
-      // the stage is consumed: start the next group's copy now
+    if (GEOM == GEOM_GENERAL && v == nv - 1) {
+      // the stage is consumed by every vector: start the next group's copy now
       __syncwarp();
       if (lane == 0 && has_next) issue_stage(gnext);
     }
@@ -465,13 +493,14 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
       for (int k = 0; k < n; ++k) {
         const long g = g0 + k * zs;
         if (hl) {
-          if ((first_bits >> k) & 1) p.dst[g] = Real(0);
+          if ((first_bits >> k) & 1) dst_v[g] = Real(0);
         } else if ((first_bits >> k) & 1) {
-          p.dst[g] = ((mask_bits >> k) & 1) ? Real(0) : out[k];
+          dst_v[g] = ((mask_bits >> k) & 1) ? Real(0) : out[k];
         } else if (!((mask_bits >> k) & 1)) {
-          p.dst[g] = dpre[k] + out[k];
+          dst_v[g] = dpre[k] + out[k];
         }
       }
     }
+    }  // vectors
   }
 }

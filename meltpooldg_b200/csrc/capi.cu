@@ -259,7 +259,7 @@ void free_op_arrays(Op &o)
   for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32,
                   (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32, (void *)o.d_trig64, o.d_stage,
                   (void *)o.d_tau64, (void *)o.d_tau32, (void *)o.Told_own, (void *)o.H_own, (void *)o.Told32,
-                  (void *)o.H32,
+                  (void *)o.H32, (void *)o.lsq_buf,
                   (void *)o.d_io, o.io_tmp})
     if (p) cudaFree(p);
 }
@@ -394,6 +394,37 @@ mpdg_status mpdg_vmult(mpdg_op *op, double *dst, const double *src)
   return guarded([&]() -> int {
     if (!op || !dst || !src) throw Error{MPDG_ERR_ARG, "null argument"};
     launch_apply<double>(op->o, dst, src);
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_vmult_multi(mpdg_op *op, int n_vectors, double *const *dst, const double *const *src)
+{
+  return guarded([&]() -> int {
+    if (!op || !dst || !src || n_vectors < 1) throw Error{MPDG_ERR_ARG, "null argument or no vectors"};
+    launch_apply_multi<double>(op->o, n_vectors, dst, src);
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_vmult_multi_f32(mpdg_op *op, int n_vectors, float *const *dst, const float *const *src)
+{
+  return guarded([&]() -> int {
+    if (!op || !dst || !src || n_vectors < 1) throw Error{MPDG_ERR_ARG, "null argument or no vectors"};
+    Op &o = op->o;
+    if (o.T64 && !o.T32) ensure_T32(o);
+    launch_apply_multi<float>(o, n_vectors, dst, src);
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_predict_lsq(mpdg_op *op, int n_old, const double *const *old_solutions, const double *rhs,
+                             double *solution, int *n_used)
+{
+  return guarded([&]() -> int {
+    if (!op || !old_solutions) throw Error{MPDG_ERR_ARG, "null argument"};
+    const int used = predict_lsq(op->o, n_old, old_solutions, rhs, solution);
+    if (n_used) *n_used = used;
     return MPDG_OK;
   });
 }

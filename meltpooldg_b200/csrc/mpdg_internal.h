@@ -141,6 +141,9 @@ struct Op {
   // inflow/outflow constraints (advection_diffusion_operator.cpp:545-578): identity
   // rows at the flagged DoFs; the source there is read as 0 and copied to the result
   uint8_t *d_io = nullptr;
+  // least-squares predictor: images of the old solutions (lsq_cols vectors of N)
+  double *lsq_buf = nullptr;
+  int lsq_cols = 0;
   void *io_tmp = nullptr;
   size_t io_tmp_bytes = 0;
 };
@@ -209,6 +212,11 @@ void invalidate_coef(Op &op);
 
 template <typename Real>
 void launch_apply(Op &op, Real *dst, const Real *src);
+template <typename Real>
+void launch_apply_multi(Op &op, int nvec, Real *const *dst, const Real *const *src);
+constexpr int kMaxLsqVectors = 32;
+// returns the number of old solutions used (predictor.cu)
+int predict_lsq(Op &op, int n_old, const double *const *old, const double *rhs, double *solution);
 void launch_rhs(Op &op, double *dst, const double *src, const double *heat_source);
 void launch_diagonal(Op &op, double *diag);
 void launch_invert_diagonal(Op &op, double *diag);

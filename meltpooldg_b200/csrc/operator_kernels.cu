@@ -180,6 +180,7 @@ void shape_1d(int p, double *S, double *D, double *w, double *x)
 // MODE_SUPG: MODE_LINEAR plus the advection-diffusion SUPG flux
 // tau_K u (c_mass u + c_vel u.grad u - c_diff lap u) (advection_diffusion_operator.cpp:450-495)
 enum { MODE_LINEAR = 0, MODE_HEAT_RESIDUAL = 1, MODE_SUPG = 2 };
+constexpr int kMaxMultiVec = 4;
 enum { GEOM_UNIFORM = 0, GEOM_GENERAL = 1 };
 
 template <typename Real>
@@ -197,6 +198,10 @@ struct KP {
   Real mrho[3], mcp[3], mk[3], solidus, liquidus, inv_mushy, dt_inv;
   const Real *Told;       // T_old (laws with a solid phase), or T - T_old when told_inc
   int told_inc;
+  // multi-vector apply: nvec operands msrc[v] -> mdst[v]
+  int nvec;
+  const Real *msrc[kMaxMultiVec];
+  Real *mdst[kMaxMultiVec];
   const Real *Hs;         // level-set heaviside (two-phase laws)
   int supg_lap;           // SUPG with diffusion: the Laplacian term (axis-aligned cells)
   const uint8_t *dmask;
@@ -1391,6 +1396,7 @@ KP<Real> base_params(Op &op)
     k.tau = op.d_tau32;
   }
   k.supg_lap = op.d.kind == MPDG_OP_ADVDIFF && op.d.supg && op.d.diffusivity != 0.0;
+  k.nvec = 1;
   k.trig_stride = std::max(m.nc[0], m.nc[1]) * m.n;
   k.dmask = m.d_dmask;
   k.cell_flags = m.d_cell_flags;
@@ -1518,7 +1524,7 @@ int num_sms()
   return g_num_sms;
 }
 
-template <int P, typename Real, int GEOM, bool HANG>
+template <int P, typename Real, int GEOM, bool HANG, bool MULTI = false>
 void run_warp_apply(Op &op, KP<Real> k)
 {
   Mesh &m = *op.mesh;
@@ -1535,7 +1541,7 @@ void run_warp_apply(Op &op, KP<Real> k)
     throw Error{MPDG_ERR_ARG, "coefficient stream not 16-byte aligned"};
   if (GEOM == GEOM_GENERAL && (!k.metric || (gvel && !k.velb)))
     throw Error{MPDG_ERR_ARG, "coefficient stream missing"};
-  auto kern = warp_apply_kernel<P, Real, GEOM, HANG>;
+  auto kern = warp_apply_kernel<P, Real, GEOM, HANG, MULTI>;
   static int configured_smem = -1, blocks_per_sm = 0;  // per instantiation
   if (configured_smem != (int)smem) {
     MPDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1559,6 +1565,16 @@ template <typename Real, int GEOM>
 void warp_apply_degree(Op &op, const KP<Real> &k)
 {
   const bool hang = k.hsrc != nullptr;
+  if (k.nvec > 1) {
+    switch (op.mesh->degree) {
+      case 1: run_warp_apply<1, Real, GEOM, false, true>(op, k); break;
+      case 2: run_warp_apply<2, Real, GEOM, false, true>(op, k); break;
+      case 3: run_warp_apply<3, Real, GEOM, false, true>(op, k); break;
+      case 4: run_warp_apply<4, Real, GEOM, false, true>(op, k); break;
+      default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+    }
+    return;
+  }
   switch (op.mesh->degree) {
     case 1: hang ? run_warp_apply<1, Real, GEOM, true>(op, k) : run_warp_apply<1, Real, GEOM, false>(op, k); break;
     case 2: hang ? run_warp_apply<2, Real, GEOM, true>(op, k) : run_warp_apply<2, Real, GEOM, false>(op, k); break;
@@ -1975,6 +1991,59 @@ void launch_cells(Op &op, Real *dst, const Real *src)
 
 template void launch_apply<double>(Op &, double *, const double *);
 template void launch_apply<float>(Op &, float *, const float *);
+
+// dst[v] = A src[v] for nvec vectors.  Operators whose apply is the plain warp
+// kernel (no faces, constraints rows, hanging nodes, SUPG or phase law) take up
+// to kMaxMultiVec vectors per pass, reading each cell's coefficients once;
+// the others apply the vectors one after the other.
+template <typename Real>
+void launch_apply_multi(Op &op, int nvec, Real *const *dst, const Real *const *src)
+{
+  Mesh &m = *op.mesh;
+  const long N = m.N;
+  for (int a = 0; a < nvec; ++a) {
+    if (!dst[a] || !src[a]) throw Error{MPDG_ERR_ARG, "null vector"};
+    for (int b = 0; b < nvec; ++b) {
+      const bool over_ds = dst[a] < src[b] + N && src[b] < dst[a] + N;
+      const bool over_dd = a != b && dst[a] < dst[b] + N && dst[b] < dst[a] + N;
+      if (over_ds || over_dd) throw Error{MPDG_ERR_ARG, "multi-vector apply: destinations overlap a vector"};
+    }
+  }
+  const mpdg_op_desc &D = op.d;
+  const bool heat = D.kind == MPDG_OP_HEAT;
+  const bool faces = heat && ((D.robin_faces && D.robin_alpha != 0.0) || (D.rad_faces && D.rad_emissivity != 0.0));
+  const bool full = heat && D.full_tangent;
+  const bool fused = !op.fine && !op.d_io && !faces && !supg(op) && !full && !uses_law(op) &&
+                     (!m.uniform || !uses_kT(op));
+  if (!fused) {
+    for (int v = 0; v < nvec; ++v) launch_apply<Real>(op, dst[v], src[v]);
+    return;
+  }
+  if (!m.uniform && D.vel_kind != MPDG_VEL_NONE && sizeof(Real) == 4 && !op.d_velb32)
+    throw Error{MPDG_ERR_ARG, "the FP32 form was not prepared for this operator (precision_mask)"};
+  KP<Real> k = base_params<Real>(op);
+  if (uses_kT(op) && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
+  if (!m.uniform) {
+    ensure_coef(op, sizeof(Real) == 4);
+    if constexpr (sizeof(Real) == 8) k.metric = op.d_coef64;
+    else k.metric = op.d_coef32;
+  }
+  for (int c = 0; c < nvec; c += kMaxMultiVec) {
+    const int cnt = std::min(kMaxMultiVec, nvec - c);
+    k.src = src[c];
+    k.dst = dst[c];
+    k.nvec = cnt;
+    for (int v = 0; v < cnt; ++v) {
+      k.msrc[v] = src[c + v];
+      k.mdst[v] = dst[c + v];
+    }
+    if (m.uniform) warp_apply_degree<Real, GEOM_UNIFORM>(op, k);
+    else warp_apply_degree<Real, GEOM_GENERAL>(op, k);
+  }
+}
+
+template void launch_apply_multi<double>(Op &, int, double *const *, const double *const *);
+template void launch_apply_multi<float>(Op &, int, float *const *, const float *const *);
 
 void launch_rhs(Op &op, double *dst, const double *src, const double *heat_source)
 {

@@ -169,6 +169,17 @@ class _MatrixFreeOperator:
         self._desc = desc
         self._fields = {}
 
+    def vmult_multi(self, dsts, srcs):
+        """dsts[v] = A srcs[v] for a list of tensors of one precision, several
+        vectors per pass (mpdg_vmult_multi)."""
+        if len(dsts) != len(srcs) or not dsts:
+            raise ValueError("vmult_multi needs equally many destinations and sources")
+        n = len(dsts)
+        d = (C.c_void_p * n)(*[t.data_ptr() for t in dsts])
+        s = (C.c_void_p * n)(*[t.data_ptr() for t in srcs])
+        f = A.lib().mpdg_vmult_multi_f32 if dsts[0].dtype == torch.float32 else A.lib().mpdg_vmult_multi
+        A.check(f(self._h, n, d, s), "vmult_multi")
+
     # OperatorBase::reset_time_increment (operator_base.hpp:41-46)
     def reset_time_increment(self, dt):
         A.check(A.lib().mpdg_op_reset_time_increment(self._h, float(dt)), "reset_time_increment")

@@ -419,3 +419,35 @@ def distribute2(mesh2, u):
     u = np.array(u, dtype=np.float64)
     lib().orc2_distribute(C.byref(mesh2._c), _ptr(u))
     return u
+
+
+# ------------------------------------------------------ least-squares predictor
+
+def lsq_projection(mesh, op, old_solutions, rhs):
+    """LeastSquaresProjection::vmult (include/meltpooldg/linear_algebra/predictor.hpp:37-80):
+    images w_s = A x_s orthogonalised in place by modified Gram-Schmidt
+    (P(0,s) = w_s.w_0; w_s -= P(j,s)/P(j,j) w_j, P(j+1,s) = w_s.w_{j+1}), stop
+    when P(s,s) < 1e-16 P(0,0); back substitution of P c = (w_s.b); returns
+    (sum_s c_s x_s, number of old solutions used)."""
+    k = len(old_solutions)
+    w = [vmult(mesh, op, x) for x in old_solutions]
+    P = np.zeros((k, k))
+    step = 0
+    while step < k:
+        P[0, step] = w[step] @ w[0]
+        for j in range(step):
+            w[step] = w[step] + (-P[j, step] / P[j, j]) * w[j]
+            P[j + 1, step] = w[step] @ w[j + 1]
+        if P[step, step] < 1e-16 * P[0, 0]:
+            break
+        step += 1
+    c = [w[s] @ rhs for s in range(step)]
+    for s in range(step - 1, -1, -1):
+        acc = c[s]
+        for j in range(s + 1, step):
+            acc -= c[j] * P[s, j]
+        c[s] = acc / P[s, s]
+    x = np.zeros_like(rhs)
+    for s in range(step):
+        x = x + c[s] * old_solutions[s]
+    return x, step
