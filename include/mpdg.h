@@ -166,6 +166,33 @@ mpdg_status mpdg_mesh_create(const mpdg_mesh_desc *desc, mpdg_mesh **mesh);
  * tangent) and support vmult, the diagonal and the solvers. */
 mpdg_status mpdg_mesh_create_two_level(const mpdg_mesh_desc *coarse, const mpdg_mesh_desc *fine,
                                        mpdg_mesh **mesh);
+/* Mapped mesh: the ingestion form of an unstructured hexahedral mesh, as a
+ * deal.II host holds it (DoFHandler cell->DoF maps, AffineConstraints;
+ * utilities/amr.hpp:55, utilities/constraints.hpp:117-135).  Each cell gives its
+ * 8 corners (trilinear map, corner v = x-bit + 2 y-bit + 4 z-bit) and its
+ * (degree+1)^3 global DoFs, lexicographic within the cell (x fastest).  The
+ * homogeneous affine constraints (hanging nodes) read
+ * x[constrained_dofs[c]] = sum_{e in [offsets[c], offsets[c+1])} weights[e] x[masters[e]],
+ * masters unconstrained.  The operator is sum_K C_K^T A_K C_K as the reference's
+ * cell loops with constraints form it: constrained DoFs are read through their
+ * constraint, written to their masters and stay 0; diagonal 1 there.  Cells are
+ * coloured greedily (no two cells of a colour share a DoF; at most 64 colours),
+ * so the scatter is atomic-free and deterministic.  Operators on it take the
+ * heat operator with constant coefficients or the advection-diffusion operator
+ * (prescribed velocity); vmult, the diagonal, create_rhs and the solvers. */
+typedef struct {
+  int degree;                        /* 1..4 */
+  int64_t n_cells, n_dofs;
+  const double *cell_vertices;       /* host, n_cells x 8 x 3 */
+  const int64_t *cell_dofs;          /* host, n_cells x (degree+1)^3 */
+  const uint8_t *dirichlet_mask;     /* host, n_dofs entries (1 = constrained) or NULL */
+  int64_t n_constraints;
+  const int64_t *constrained_dofs;   /* n_constraints */
+  const int64_t *constraint_offsets; /* n_constraints + 1 */
+  const int64_t *constraint_masters;
+  const double *constraint_weights;
+} mpdg_mapped_mesh_desc;
+mpdg_status mpdg_mesh_create_mapped(const mpdg_mapped_mesh_desc *desc, mpdg_mesh **mesh);
 mpdg_status mpdg_mesh_destroy(mpdg_mesh *mesh);
 /* n_dofs of the mesh (ScratchData::get_dof_handler(idx).n_dofs()) */
 mpdg_status mpdg_mesh_n_dofs(const mpdg_mesh *mesh, int64_t *n_dofs);

@@ -46,6 +46,14 @@ class MeshDesc(C.Structure):
                 ("geometry", C.c_int)]
 
 
+class MappedMeshDesc(C.Structure):
+    _fields_ = [("degree", C.c_int), ("n_cells", C.c_int64), ("n_dofs", C.c_int64),
+                ("cell_vertices", C.POINTER(C.c_double)), ("cell_dofs", C.POINTER(C.c_int64)),
+                ("dirichlet_mask", C.POINTER(C.c_uint8)), ("n_constraints", C.c_int64),
+                ("constrained_dofs", C.POINTER(C.c_int64)), ("constraint_offsets", C.POINTER(C.c_int64)),
+                ("constraint_masters", C.POINTER(C.c_int64)), ("constraint_weights", C.POINTER(C.c_double))]
+
+
 class OpDesc(C.Structure):
     _fields_ = [("kind", C.c_int), ("dt", C.c_double), ("rho_cp", C.c_double), ("k0", C.c_double),
                 ("k_alpha", C.c_double), ("full_tangent", C.c_int), ("theta", C.c_double),
@@ -109,6 +117,7 @@ def lib():
     L.mpdg_mesh_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(vp)]
     L.mpdg_mesh_destroy.argtypes = [vp]
     L.mpdg_mesh_create_two_level.argtypes = [C.POINTER(MeshDesc), C.POINTER(MeshDesc), C.POINTER(vp)]
+    L.mpdg_mesh_create_mapped.argtypes = [C.POINTER(MappedMeshDesc), C.POINTER(vp)]
     L.mpdg_mesh_n_dofs.argtypes = [vp, C.POINTER(C.c_int64)]
     L.mpdg_mesh_device_bytes.argtypes = [vp, C.POINTER(C.c_int64)]
     L.mpdg_op_create.argtypes = [vp, C.POINTER(OpDesc), C.POINTER(vp)]

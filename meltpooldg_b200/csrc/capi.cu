@@ -72,6 +72,28 @@ mpdg_status mpdg_mesh_create(const mpdg_mesh_desc *desc, mpdg_mesh **out)
   });
 }
 
+mpdg_status mpdg_mesh_create_mapped(const mpdg_mapped_mesh_desc *desc, mpdg_mesh **out)
+{
+  return guarded([&]() -> int {
+    if (!desc || !out || !desc->cell_vertices || !desc->cell_dofs) throw Error{MPDG_ERR_ARG, "null argument"};
+    if (desc->degree < 1 || desc->degree > kMaxDegree) throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+    if (desc->n_cells < 1 || desc->n_dofs < 1) throw Error{MPDG_ERR_ARG, "empty mesh"};
+    if (desc->n_constraints < 0 ||
+        (desc->n_constraints > 0 && (!desc->constrained_dofs || !desc->constraint_offsets ||
+                                     !desc->constraint_masters || !desc->constraint_weights)))
+      throw Error{MPDG_ERR_ARG, "constraint arrays missing"};
+    auto *h = new mpdg_mesh();
+    try {
+      build_mapped_mesh(h->m, *desc);
+    } catch (...) {
+      mpdg_mesh_destroy(h);
+      throw;
+    }
+    *out = h;
+    return MPDG_OK;
+  });
+}
+
 mpdg_status mpdg_mesh_create_two_level(const mpdg_mesh_desc *coarse, const mpdg_mesh_desc *fine, mpdg_mesh **out)
 {
   return guarded([&]() -> int {
@@ -151,7 +173,10 @@ namespace {
 void free_mesh_arrays(Mesh &m)
 {
   for (void *p : {(void *)m.d_vert, (void *)m.d_metric64, (void *)m.d_metric32, (void *)m.d_dmask,
-                  (void *)m.d_cell_flags, (void *)m.d_cell_mask, (void *)m.d_tmask_dir, (void *)m.d_tmask_hang})
+                  (void *)m.d_cell_flags, (void *)m.d_cell_mask, (void *)m.d_tmask_dir, (void *)m.d_tmask_hang,
+                  (void *)m.d_cmap, (void *)m.d_cellvert, (void *)m.d_cons_dof, (void *)m.d_cons_ptr,
+                  (void *)m.d_cons_mast, (void *)m.d_cons_w, (void *)m.d_mast_dof, (void *)m.d_mast_ptr,
+                  (void *)m.d_mast_cons, (void *)m.d_mast_w, (void *)m.d_cons_of, (void *)m.d_ccells})
     if (p) cudaFree(p);
 }
 
@@ -218,6 +243,11 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     if (desc->supg && desc->kind != MPDG_OP_ADVDIFF)
       throw Error{MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator"};
     if (desc->supg && mm.fine) throw Error{MPDG_ERR_UNSUPPORTED, "SUPG on two-level meshes"};
+    if (mm.mapped && (desc->k_alpha != 0.0 || desc->full_tangent || desc->material != MPDG_MAT_LINEAR ||
+                      desc->supg || (desc->robin_faces && desc->robin_alpha != 0.0) ||
+                      (desc->rad_faces && desc->rad_emissivity != 0.0)))
+      throw Error{MPDG_ERR_UNSUPPORTED,
+                  "mapped meshes take constant coefficients: no k(T) or phase law, full tangent, faces or SUPG"};
     if (desc->supg && desc->diffusivity != 0.0 && !mm.uniform && !axis_aligned_lattice(mm))
       throw Error{MPDG_ERR_UNSUPPORTED,
                   "SUPG with diffusion needs axis-aligned cells (its Laplacian drops the Jacobian derivatives)"};
@@ -365,6 +395,7 @@ mpdg_status mpdg_op_set_inflow_outflow(mpdg_op *op, const uint8_t *host_mask)
   return guarded([&]() -> int {
     if (!op) throw Error{MPDG_ERR_ARG, "null operator"};
     Op &o = op->o;
+    if (o.mesh->mapped && host_mask) throw Error{MPDG_ERR_UNSUPPORTED, "inflow/outflow rows on mapped meshes"};
     if (o.d_io) {
       MPDG_CUDA(cudaStreamSynchronize(o.stream));
       cudaFree(o.d_io);

@@ -97,6 +97,22 @@ struct Mesh {
   // coarse faces (read through the interpolation, never written).
   Mesh *fine = nullptr;
   long N_own = 0;
+  // Mapped mesh (mpdg_mesh_create_mapped): cells given by their corners and
+  // their cell->DoF map, coloured greedily so that no two cells of a colour
+  // share a DoF; homogeneous affine constraints distributed before and
+  // condensed after the cell loop.
+  bool mapped = false;
+  std::vector<Colour> mcol;          // count and first of each colour (cn = {count, 1, 1})
+  int *d_cmap = nullptr;             // [colour-major cell][n^3] global DoFs
+  double *d_cellvert = nullptr;      // [colour-major cell][8][3] corners
+  long n_cons = 0, n_masters = 0;
+  long *d_cons_dof = nullptr, *d_cons_ptr = nullptr, *d_cons_mast = nullptr;  // per constraint
+  double *d_cons_w = nullptr;
+  long *d_mast_dof = nullptr, *d_mast_ptr = nullptr, *d_mast_cons = nullptr;  // per master
+  double *d_mast_w = nullptr;
+  int *d_cons_of = nullptr;          // per DoF: its constraint index, or -1
+  std::vector<long> ccells;          // colour-major cells that touch a constrained DoF
+  long *d_ccells = nullptr;
   uint8_t *d_tmask_dir = nullptr;   // whole vector: Dirichlet or hanging
   uint8_t *d_tmask_hang = nullptr;  // whole vector: hanging only
 };
@@ -205,6 +221,7 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
 void ensure_metric32(Mesh &m, cudaStream_t s);
 void build_op_device_data(Op &op);
 void ensure_T32(Op &op);
+void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d);
 inline bool law_has_solid(int mat) { return mat == MPDG_MAT_LIQUID_SOLID || mat == MPDG_MAT_GAS_LIQUID_SOLID; }
 inline bool law_two_phase(int mat) { return mat == MPDG_MAT_GAS_LIQUID || mat == MPDG_MAT_GAS_LIQUID_SOLID; }
 // marks the merged coefficient stream stale (new temperature field or dt)

@@ -15,6 +15,7 @@
 // results into dst with plain loads and stores (atomic-free, deterministic).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -198,6 +199,10 @@ struct KP {
   Real mrho[3], mcp[3], mk[3], solidus, liquidus, inv_mushy, dt_inv;
   const Real *Told;       // T_old (laws with a solid phase), or T - T_old when told_inc
   int told_inc;
+  // mapped mesh: cell->DoF map [colour-major cell][n^3]; skip the cells that
+  // touch a constrained DoF in the diagonal kernel
+  const int *cmap;
+  int skip_constrained;
   // multi-vector apply: nvec operands msrc[v] -> mdst[v]
   int nvec;
   const Real *msrc[kMaxMultiVec];
@@ -230,6 +235,13 @@ struct KP {
   long hNXc, hNYc;       // coarse lattice
   int hnc1;              // fine cells in y
 };
+
+// mapped meshes (mapped.cuh)
+template <typename Real>
+void launch_mapped_apply(Op &op, Real *dst, const Real *src);
+template <typename Real>
+void mapped_condense(Op &op, Real *dst);
+void launch_mapped_diagonal(Op &op, double *diag);
 
 template <int n>
 struct Cfg {
@@ -461,6 +473,11 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
   const long cell = p.cfirst + cidx;
   const long zs = p.NX * p.NY;
   const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
+  // global DoFs of the thread's column: the lattice, or the cell->DoF map of a
+  // mapped mesh
+  long gk[n];
+#pragma unroll
+  for (int k = 0; k < n; ++k) gk[k] = (p.cmap && active) ? (long)p.cmap[cell * n3 + k * n2 + j * n + i] : g0 + k * zs;
   const bool bflag = active && p.cell_flags && (p.cell_flags[cell] & 1);
   Real *t0 = sm[slot][0], *t1 = sm[slot][1];
 
@@ -469,8 +486,8 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
   for (int k = 0; k < n; ++k) {
     Real v = 0;
     if (active) {
-      v = p.src[g0 + k * zs];
-      if (MODE != MODE_HEAT_RESIDUAL && p.masked_read && bflag && p.dmask[g0 + k * zs]) v = 0;
+      v = p.src[gk[k]];
+      if (MODE != MODE_HEAT_RESIDUAL && p.masked_read && bflag && p.dmask[gk[k]]) v = 0;
     }
     u[k] = v;
   }
@@ -481,7 +498,7 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
   if (needT) {
     Real tl[n];
 #pragma unroll
-    for (int k = 0; k < n; ++k) tl[k] = active ? p.T[g0 + k * zs] : Real(0);
+    for (int k = 0; k < n; ++k) tl[k] = active ? p.T[gk[k]] : Real(0);
     to_qp<n>(sS, t1, i, j, tl, Tq);
     if (MODE == MODE_HEAT_RESIDUAL || p.full_tangent) grad_qp<n>(sDc, t1, i, j, Tq, Tgx, Tgy, Tgz);
   }
@@ -491,13 +508,13 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
   if (needT && p.Hs) {
     Real hl[n];
 #pragma unroll
-    for (int k = 0; k < n; ++k) hl[k] = active ? p.Hs[g0 + k * zs] : Real(0);
+    for (int k = 0; k < n; ++k) hl[k] = active ? p.Hs[gk[k]] : Real(0);
     to_qp<n>(sS, t1, i, j, hl, Hq);
   }
   if (KT && MODE != MODE_HEAT_RESIDUAL && p.full_tangent && p.Told) {
     Real ol[n];
 #pragma unroll
-    for (int k = 0; k < n; ++k) ol[k] = active ? p.Told[g0 + k * zs] : Real(0);
+    for (int k = 0; k < n; ++k) ol[k] = active ? p.Told[gk[k]] : Real(0);
     to_qp<n>(sS, t1, i, j, ol, Oq);
   }
   Real oq[n], hq[n];
@@ -506,7 +523,7 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
     to_qp<n>(sS, t0, i, j, u, oq);
     Real ql[n];
 #pragma unroll
-    for (int k = 0; k < n; ++k) ql[k] = (active && p.q_src) ? p.q_src[g0 + k * zs] : Real(0);
+    for (int k = 0; k < n; ++k) ql[k] = (active && p.q_src) ? p.q_src[gk[k]] : Real(0);
     to_qp<n>(sS, t0, i, j, ql, hq);
 #pragma unroll
     for (int k = 0; k < n; ++k) {
@@ -640,7 +657,7 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
   if (active) {
 #pragma unroll
     for (int k = 0; k < n; ++k) {
-      const long g = g0 + k * zs;
+      const long g = gk[k];
       if (p.masked_write && bflag && p.dmask[g]) continue;
       p.dst[g] += out[k];
     }
@@ -705,14 +722,20 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
   const long cell = p.cfirst + cidx;
   const long zs = p.NX * p.NY;
   const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
+  long gk[n];
+#pragma unroll
+  for (int k = 0; k < n; ++k) gk[k] = (p.cmap && active) ? (long)p.cmap[cell * n3 + k * n2 + j * n + i] : g0 + k * zs;
   const bool bflag = active && p.cell_flags && (p.cell_flags[cell] & 1);
+  // cells of a mapped mesh that touch a constrained DoF get their diagonal share
+  // from their element matrices (skip_constrained)
+  const bool wr = active && !(p.skip_constrained && p.cell_flags && (p.cell_flags[cell] & 2));
   Real *t = sm[slot];
 
   Real Tq[n], Tgx[n], Tgy[n], Tgz[n];
   if (KT) {
     Real tl[n];
 #pragma unroll
-    for (int k = 0; k < n; ++k) tl[k] = active ? p.T[g0 + k * zs] : Real(0);
+    for (int k = 0; k < n; ++k) tl[k] = active ? p.T[gk[k]] : Real(0);
     to_qp<n>(tb[3], t, i, j, tl, Tq);
     if (p.full_tangent) grad_qp<n>(tb[4], t, i, j, Tq, Tgx, Tgy, Tgz);
   }
@@ -720,13 +743,13 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
   if (KT && p.Hs) {
     Real hl[n];
 #pragma unroll
-    for (int k = 0; k < n; ++k) hl[k] = active ? p.Hs[g0 + k * zs] : Real(0);
+    for (int k = 0; k < n; ++k) hl[k] = active ? p.Hs[gk[k]] : Real(0);
     to_qp<n>(tb[3], t, i, j, hl, Hq);
   }
   if (KT && p.full_tangent && p.Told) {
     Real ol[n];
 #pragma unroll
-    for (int k = 0; k < n; ++k) ol[k] = active ? p.Told[g0 + k * zs] : Real(0);
+    for (int k = 0; k < n; ++k) ol[k] = active ? p.Told[gk[k]] : Real(0);
     to_qp<n>(tb[3], t, i, j, ol, Oq);
   }
   Real Fm[n], F00[n], F11[n], F22[n], F01[n], F02[n], F12[n], Fb0[n], Fb1[n], Fb2[n];
@@ -800,10 +823,10 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
     diag_term<n>(t, i, j, F02, SD, SS, SD, acc);
     diag_term<n>(t, i, j, F12, SS, SD, SD, acc);
   }
-  if (active) {
+  if (wr) {
 #pragma unroll
     for (int k = 0; k < n; ++k) {
-      const long g = g0 + k * zs;
+      const long g = gk[k];
       if (p.masked_write && bflag && p.dmask[g]) continue;
       p.dst[g] += acc[k];
     }
@@ -870,16 +893,16 @@ __global__ void __launch_bounds__(128) merge_kernel(const KP<double> p, const Co
 // ------------------------------------------------------ geometry kernels
 
 // per (cell, qp): JxW and G = JxW J^-1 J^-T of the trilinear map, colour-major
-__global__ void metric_kernel(const double *vert, int nc0, int nc1, int nc2, int P,
-                              const Colour *colours, double *metric, float *metric32,
-                              const double *xq_all, const double *wq_all)
+// corners of colour-major cell `cell`: from the vertex lattice, or, on a
+// mapped mesh, from the per-cell corners (cellvert, [cell][8][3])
+__device__ __forceinline__ void cell_corners(const double *vert, int nc0, int nc1, const Colour *colours,
+                                             const double *cellvert, long cell, double V[8][3])
 {
-  const int n = P + 1, n3 = n * n * n;
-  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long n_cells = (long)nc0 * nc1 * nc2;
-  if (gid >= n_cells * n3) return;
-  const long cell = gid / n3;
-  const int q = (int)(gid % n3);
+  if (cellvert) {
+    for (int v = 0; v < 8; ++v)
+      for (int a = 0; a < 3; ++a) V[v][a] = cellvert[(cell * 8 + v) * 3 + a];
+    return;
+  }
   int c = 0;
   while (c < 7 && cell >= colours[c + 1].first) ++c;
   const Colour &C = colours[c];
@@ -887,18 +910,34 @@ __global__ void metric_kernel(const double *vert, int nc0, int nc1, int nc2, int
   const int ix = 2 * (int)(cidx % C.cn[0]) + C.par[0];
   const int iy = 2 * (int)((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
   const int iz = 2 * (int)(cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
+  for (int v = 0; v < 8; ++v) {
+    const long vid = ((long)(iz + ((v >> 2) & 1)) * (nc1 + 1) + (iy + ((v >> 1) & 1))) * (nc0 + 1) + (ix + (v & 1));
+    for (int a = 0; a < 3; ++a) V[v][a] = vert[vid * 3 + a];
+  }
+}
+
+__global__ void metric_kernel(const double *vert, int nc0, int nc1, long n_cells, int P,
+                              const Colour *colours, const double *cellvert, double *metric, float *metric32,
+                              const double *xq_all, const double *wq_all)
+{
+  const int n = P + 1, n3 = n * n * n;
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= n_cells * n3) return;
+  const long cell = gid / n3;
+  const int q = (int)(gid % n3);
+  double V[8][3];
+  cell_corners(vert, nc0, nc1, colours, cellvert, cell, V);
   const int qi = q % n, qj = (q / n) % n, qk = q / (n * n);
   const double xi[3] = {xq_all[qi], xq_all[qj], xq_all[qk]};
   const double w = wq_all[qi] * wq_all[qj] * wq_all[qk];
   double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
   for (int v = 0; v < 8; ++v) {
     const int bx = v & 1, by = (v >> 1) & 1, bz = (v >> 2) & 1;
-    const long vid = ((long)(iz + bz) * (nc1 + 1) + (iy + by)) * (nc0 + 1) + (ix + bx);
     const double f[3] = {bx ? xi[0] : 1 - xi[0], by ? xi[1] : 1 - xi[1], bz ? xi[2] : 1 - xi[2]};
     const double df[3] = {bx ? 1.0 : -1.0, by ? 1.0 : -1.0, bz ? 1.0 : -1.0};
     const double dB[3] = {df[0] * f[1] * f[2], f[0] * df[1] * f[2], f[0] * f[1] * df[2]};
     for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) J[a][b] += vert[vid * 3 + a] * dB[b];
+      for (int b = 0; b < 3; ++b) J[a][b] += V[v][a] * dB[b];
   }
   const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
                      J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
@@ -933,38 +972,31 @@ __global__ void metric_kernel(const double *vert, int nc0, int nc1, int nc2, int
 }
 
 // per (cell, qp): b = JxW J^-1 u(x_q) for a prescribed velocity on a general mesh
-__global__ void velb_kernel(const double *vert, int nc0, int nc1, int nc2, int P,
-                            const Colour *colours, int vel_kind, double s0, double s1, double s2,
-                            double *velb, float *velb32, const double *xq_all,
+__global__ void velb_kernel(const double *vert, int nc0, int nc1, long n_cells, int P,
+                            const Colour *colours, const double *cellvert, int vel_kind, double s0, double s1,
+                            double s2, double *velb, float *velb32, const double *xq_all,
                             const double *wq_all)
 {
   const int n = P + 1, n3 = n * n * n;
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long n_cells = (long)nc0 * nc1 * nc2;
   if (gid >= n_cells * n3) return;
   const long cell = gid / n3;
   const int q = (int)(gid % n3);
-  int c = 0;
-  while (c < 7 && cell >= colours[c + 1].first) ++c;
-  const Colour &C = colours[c];
-  const long cidx = cell - C.first;
-  const int ix = 2 * (int)(cidx % C.cn[0]) + C.par[0];
-  const int iy = 2 * (int)((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
-  const int iz = 2 * (int)(cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
+  double V[8][3];
+  cell_corners(vert, nc0, nc1, colours, cellvert, cell, V);
   const int qi = q % n, qj = (q / n) % n, qk = q / (n * n);
   const double xi[3] = {xq_all[qi], xq_all[qj], xq_all[qk]};
   const double w = wq_all[qi] * wq_all[qj] * wq_all[qk];
   double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, x[3] = {0, 0, 0};
   for (int v = 0; v < 8; ++v) {
     const int bx = v & 1, by = (v >> 1) & 1, bz = (v >> 2) & 1;
-    const long vid = ((long)(iz + bz) * (nc1 + 1) + (iy + by)) * (nc0 + 1) + (ix + bx);
     const double f[3] = {bx ? xi[0] : 1 - xi[0], by ? xi[1] : 1 - xi[1], bz ? xi[2] : 1 - xi[2]};
     const double df[3] = {bx ? 1.0 : -1.0, by ? 1.0 : -1.0, bz ? 1.0 : -1.0};
     const double dB[3] = {df[0] * f[1] * f[2], f[0] * df[1] * f[2], f[0] * f[1] * df[2]};
     const double B = f[0] * f[1] * f[2];
     for (int a = 0; a < 3; ++a) {
-      x[a] += vert[vid * 3 + a] * B;
-      for (int b = 0; b < 3; ++b) J[a][b] += vert[vid * 3 + a] * dB[b];
+      x[a] += V[v][a] * B;
+      for (int b = 0; b < 3; ++b) J[a][b] += V[v][a] * dB[b];
     }
   }
   double u[3] = {0, 0, 0};
@@ -1189,7 +1221,7 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
     m.d_metric64 = dev_alloc<double>((size_t)m.n_cells * metric_stride(n), m.device_bytes);
     MPDG_CUDA(cudaMemset(m.d_metric64, 0, sizeof(double) * m.n_cells * metric_stride(n)));
     const long total = m.n_cells * n3;
-    metric_kernel<<<grid_for(total, 256), 256>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col,
+    metric_kernel<<<grid_for(total, 256), 256>>>(m.d_vert, m.nc[0], m.nc[1], m.n_cells, p, d_col, nullptr,
                                                  m.d_metric64, nullptr, d_xw, d_xw + kMaxN);
     MPDG_LAUNCHED();
     MPDG_CUDA(cudaDeviceSynchronize());
@@ -1294,7 +1326,7 @@ void build_op_device_data(Op &op)
       op.d_velb32 = dev_alloc<float>((size_t)m.n_cells * velb_stride(n), op.device_bytes);
       MPDG_CUDA(cudaMemset(op.d_velb32, 0, sizeof(float) * m.n_cells * velb_stride(n)));
     }
-    velb_kernel<<<grid_for(total, 256), 256>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col,
+    velb_kernel<<<grid_for(total, 256), 256>>>(m.d_vert, m.nc[0], m.nc[1], m.n_cells, p, d_col, m.d_cellvert,
                                                op.d.vel_kind, op.d.vel_param[0], op.d.vel_param[1],
                                                op.d.vel_param[2], op.d_velb64, op.d_velb32, d_xw,
                                                d_xw + kMaxN);
@@ -1396,6 +1428,7 @@ KP<Real> base_params(Op &op)
     k.tau = op.d_tau32;
   }
   k.supg_lap = op.d.kind == MPDG_OP_ADVDIFF && op.d.supg && op.d.diffusivity != 0.0;
+  k.cmap = m.d_cmap;
   k.nvec = 1;
   k.trig_stride = std::max(m.nc[0], m.nc[1]) * m.n;
   k.dmask = m.d_dmask;
@@ -1438,6 +1471,11 @@ KP<Real> base_params(Op &op)
   return k;
 }
 
+// the colours of a mesh: the 8 parity colours of a lattice, or a mapped
+// mesh's greedy colours
+inline int n_colours(const Mesh &m) { return m.mapped ? (int)m.mcol.size() : 8; }
+inline const Colour *colours(const Mesh &m) { return m.mapped ? m.mcol.data() : m.colour; }
+
 template <typename Real>
 void colour_params(KP<Real> &k, const Colour &C)
 {
@@ -1463,8 +1501,8 @@ void run_cells(Op &op, KP<Real> k)
   Mesh &m = *op.mesh;
   constexpr int n = P + 1, CPB = Cfg<n>::cpb;
   const dim3 block(n * n, CPB);
-  for (int c = 0; c < 8; ++c) {
-    const Colour &C = m.colour[c];
+  for (int c = 0; c < n_colours(m); ++c) {
+    const Colour &C = colours(m)[c];
     if (C.count == 0) continue;
     colour_params(k, C);
     const unsigned grid = (unsigned)((C.count + CPB - 1) / CPB);
@@ -1914,6 +1952,10 @@ __global__ void io_post_kernel(Real *dst, const Real *src, const uint8_t *io, lo
 template <typename Real>
 void launch_apply(Op &op, Real *dst, const Real *src)
 {
+  if (op.mesh->mapped) {
+    launch_mapped_apply<Real>(op, dst, src);
+    return;
+  }
   const Real *in = src;
   const long N = op.mesh->N;
   const unsigned grid = (unsigned)std::min(grid_for(N, 256), (unsigned)(148 * 16));
@@ -2071,6 +2113,8 @@ void launch_rhs(Op &op, double *dst, const double *src, const double *heat_sourc
     if (supg(op)) dispatch_degree<double, MODE_SUPG, false>(op, k);
     else dispatch_degree<double, MODE_LINEAR, false>(op, k);
   }
+  // integrate_scatter through the constraints: the constrained rows go to their masters
+  if (op.mesh->mapped) mapped_condense<double>(op, dst);
 }
 
 namespace {
@@ -2080,8 +2124,8 @@ void run_diag(Op &op, KP<double> k)
   Mesh &m = *op.mesh;
   constexpr int n = P + 1, CPB = Cfg<n>::cpb;
   const dim3 block(n * n, CPB);
-  for (int c = 0; c < 8; ++c) {
-    const Colour &C = m.colour[c];
+  for (int c = 0; c < n_colours(m); ++c) {
+    const Colour &C = colours(m)[c];
     if (C.count == 0) continue;
     colour_params(k, C);
     const unsigned grid = (unsigned)((C.count + CPB - 1) / CPB);
@@ -2091,6 +2135,8 @@ void run_diag(Op &op, KP<double> k)
   }
 }
 }  // namespace
+
+#include "mapped.cuh"
 
 void launch_block_diagonal(Op &op, double *diag);
 
@@ -2142,6 +2188,10 @@ void launch_composite_diagonal(Op &op, double *diag)
 
 void launch_diagonal(Op &op, double *diag)
 {
+  if (op.mesh->mapped) {
+    launch_mapped_diagonal(op, diag);
+    return;
+  }
   if (op.fine) {
     launch_composite_diagonal(op, diag);
     return;
@@ -2223,7 +2273,7 @@ void launch_block_diagonal(Op &op, double *diag)
 const uint8_t *constraint_mask(const Op &op)
 {
   const Mesh &m = *op.mesh;
-  if (m.fine) return op.use_dirichlet ? m.d_tmask_dir : m.d_tmask_hang;
+  if (m.fine || m.mapped) return op.use_dirichlet ? m.d_tmask_dir : m.d_tmask_hang;
   return (op.use_dirichlet && m.has_dirichlet) ? m.d_dmask : nullptr;
 }
 
@@ -2256,6 +2306,7 @@ bool apply_ready_without_allocation(const Op &op)
   const Mesh &m = *op.mesh;
   const bool full = op.d.kind == MPDG_OP_HEAT && op.d.full_tangent;
   if (supg(op)) return false;                    // the diagonal probes allocate
+  if (m.mapped) return m.n_cons == 0;            // constraints: operand copy and element matrices
   if (uses_law(op)) return true;                 // block kernel on raw geometry
   if (!full && !m.uniform) return op.coef64_ok;  // merged stream already built
   return true;                                   // nothing is built lazily on these paths
@@ -2329,6 +2380,7 @@ __global__ void l2_cells_kernel(const double *u, long NX, long NY, int nc0, int 
 double l2_norm_integrated(Op &op, const double *u)
 {
   if (op.fine) throw Error{MPDG_ERR_UNSUPPORTED, "integrated norms on two-level meshes"};
+  if (op.mesh->mapped) throw Error{MPDG_ERR_UNSUPPORTED, "integrated norms on mapped meshes"};
   Mesh &m = *op.mesh;
   const int blocks = 256;
   Colour *d_col = nullptr;

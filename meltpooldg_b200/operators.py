@@ -123,6 +123,42 @@ class TwoLevelMesh(Mesh):
         self.mask = None
 
 
+class MappedMesh(Mesh):
+    """Unstructured hexahedral mesh in the ingestion form
+    (mpdg_mesh_create_mapped): each cell's 8 corners (x fastest), its
+    (degree+1)^3 global DoFs (lexicographic within the cell), a Dirichlet mask,
+    and homogeneous constraints {dof: [(master, weight), ...]} (hanging nodes;
+    masters unconstrained).  Vectors use the caller's DoF numbering; the
+    constrained DoFs stay 0 in results, like Dirichlet DoFs."""
+
+    def __init__(self, cell_vertices, cell_dofs, n_dofs, degree, dirichlet_mask=None, constraints=None):
+        L = A.lib()
+        self.degree = int(degree)
+        n3 = (self.degree + 1) ** 3
+        self.cell_vertices = np.ascontiguousarray(cell_vertices, np.float64).reshape(-1, 8, 3)
+        self.cell_dofs = np.ascontiguousarray(cell_dofs, np.int64).reshape(-1, n3)
+        self.n_dofs = int(n_dofs)
+        self.mask = None if dirichlet_mask is None else np.ascontiguousarray(dirichlet_mask, np.uint8)
+        cons = sorted((int(g), list(ent)) for g, ent in (constraints or {}).items())
+        self._cdofs = np.ascontiguousarray([g for g, _ in cons] or [0], np.int64)
+        off = np.zeros(len(cons) + 1, np.int64)
+        for i, (_, ent) in enumerate(cons):
+            off[i + 1] = off[i] + len(ent)
+        self._coff = off
+        self._cmast = np.ascontiguousarray([m for _, ent in cons for m, _ in ent] or [0], np.int64)
+        self._cw = np.ascontiguousarray([w for _, ent in cons for _, w in ent] or [0.0], np.float64)
+        i64 = C.POINTER(C.c_int64)
+        d = A.MappedMeshDesc(self.degree, self.cell_dofs.shape[0], self.n_dofs,
+                             self.cell_vertices.ctypes.data_as(C.POINTER(C.c_double)),
+                             self.cell_dofs.ctypes.data_as(i64),
+                             None if self.mask is None else self.mask.ctypes.data_as(C.POINTER(C.c_uint8)),
+                             len(cons), self._cdofs.ctypes.data_as(i64), self._coff.ctypes.data_as(i64),
+                             self._cmast.ctypes.data_as(i64), self._cw.ctypes.data_as(C.POINTER(C.c_double)))
+        h = C.c_void_p()
+        A.check(L.mpdg_mesh_create_mapped(C.byref(d), C.byref(h)), "mpdg_mesh_create_mapped")
+        self._h = h
+
+
 def box_vertices(nc, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), perturb=0.0, seed=None):
     """Vertices (x fastest) of an nc[0] x nc[1] x nc[2] box; interior vertices
     displaced by U[-perturb h, perturb h] per coordinate (PCG64(seed))."""

@@ -751,14 +751,14 @@ void orc_vmult(const orc_mesh *m, const orc_op *op, double *dst, const double *s
 
 /* ----------------------------------------------- brute-force element matrices */
 
+static void element_matrix_vc(const orc_op *op, const geo_t *g, double vc[8][3], const long *idx, double tau,
+                              double *A);
+
 static void element_matrix(const orc_mesh *m, const orc_op *op, const geo_t *g, int ix, int iy,
                            int iz, const long *idx, double *A /* nqt x nqt */)
 {
-  const int n = g->n, dim = g->dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
   double vc[8][3];
   cell_vertices(m, g, ix, iy, iz, vc);
-  memset(A, 0, sizeof(double) * nqt * nqt);
-  static __thread double phi[MAXN3], gphi[MAXN3][3];
   double tau = 0.0;
   if (op->supg && op->kind == ORC_ADVDIFF) {
     static __thread qdata_t qdc[MAXN3];
@@ -767,6 +767,17 @@ static void element_matrix(const orc_mesh *m, const orc_op *op, const geo_t *g, 
     cell_qdata(m, &plain, g, ix, iy, iz, idx, qdc);
     tau = cell_tau(m, op, g, ix, iy, iz, qdc);
   }
+  element_matrix_vc(op, g, vc, idx, tau, A);
+}
+
+/* element matrix of the cell with corners vc (x fastest) and global DoFs idx
+ * (the fields are read through idx) */
+static void element_matrix_vc(const orc_op *op, const geo_t *g, double vc[8][3], const long *idx, double tau,
+                              double *A)
+{
+  const int n = g->n, dim = g->dim, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+  memset(A, 0, sizeof(double) * nqt * nqt);
+  static __thread double phi[MAXN3], gphi[MAXN3][3];
   for (int qz = 0; qz < nz; ++qz)
     for (int qy = 0; qy < n; ++qy)
       for (int qx = 0; qx < n; ++qx) {
@@ -1520,4 +1531,139 @@ void orc2_dof_coordinates(const orc_mesh2 *m, double *xyz)
 {
   orc_dof_coordinates(&m->coarse, xyz);
   orc_dof_coordinates(&m->fine, xyz + 3 * orc_n_dofs(&m->coarse));
+}
+
+/* ------------------------------------------------------------- mapped meshes
+ * Unstructured hexahedral meshes given by each cell's corners and its cell->DoF
+ * map (the form a deal.II DoFHandler / MatrixFree layout takes after renumbering
+ * each cell's DoFs lexicographically), with homogeneous affine constraints
+ * (AffineConstraints lines: x_c = sum_e w_e x_{m_e}; masters unconstrained).
+ * The operator is sum_K C_K^T A_K C_K as in read_dof_values /
+ * distribute_local_to_global with constraints (heat_diffuse_operator.cpp:
+ * 199-241): constrained DoFs are read through their constraint and never
+ * written; Dirichlet DoFs are read as 0 and never written. */
+static void mapped_entries(const orc_mapped *m, long gidx, long *cnt, const long **g, const double **w,
+                           long *own, double *one)
+{
+  if (m->cons_ptr && m->cons_ptr[gidx + 1] > m->cons_ptr[gidx]) {
+    *cnt = m->cons_ptr[gidx + 1] - m->cons_ptr[gidx];
+    *g = m->cons_idx + m->cons_ptr[gidx];
+    *w = m->cons_w + m->cons_ptr[gidx];
+  } else {
+    *own = gidx;
+    *one = 1.0;
+    *cnt = 1;
+    *g = own;
+    *w = one;
+  }
+}
+
+static int mapped_constrained(const orc_mapped *m, long gidx)
+{
+  return m->cons_ptr && m->cons_ptr[gidx + 1] > m->cons_ptr[gidx];
+}
+
+static void mapped_geo(const orc_mapped *m, geo_t *g)
+{
+  orc_mesh dummy = {3, m->degree, {1, 1, 1}, NULL};
+  geo_init(&dummy, g);
+}
+
+static void mapped_cell(const orc_mapped *m, long K, double vc[8][3], long *idx, int nqt)
+{
+  for (int v = 0; v < 8; ++v)
+    for (int a = 0; a < 3; ++a) vc[v][a] = m->cell_vertices[(K * 8 + v) * 3 + a];
+  for (int t = 0; t < nqt; ++t) idx[t] = m->cell_dofs[K * nqt + t];
+}
+
+void orcm_vmult(const orc_mapped *m, const orc_op *op, double *dst, const double *src)
+{
+  geo_t g;
+  mapped_geo(m, &g);
+  const int n = g.n, nqt = n * n * n;
+  memset(dst, 0, sizeof(double) * m->n_dofs);
+  double *A = (double *)malloc(sizeof(double) * nqt * nqt);
+  for (long K = 0; K < m->n_cells; ++K) {
+    double vc[8][3], ul[MAXN3];
+    long idx[MAXN3];
+    mapped_cell(m, K, vc, idx, nqt);
+    element_matrix_vc(op, &g, vc, idx, 0.0, A);
+    for (int t = 0; t < nqt; ++t) {
+      long cnt, own;
+      double one, v = 0.0;
+      const long *gg;
+      const double *ww;
+      mapped_entries(m, idx[t], &cnt, &gg, &ww, &own, &one);
+      for (long e = 0; e < cnt; ++e)
+        if (!(op->dirichlet && op->dirichlet[gg[e]])) v += ww[e] * src[gg[e]];
+      ul[t] = v;
+    }
+    for (int t = 0; t < nqt; ++t) {
+      double o = 0.0;
+      for (int u = 0; u < nqt; ++u) o += A[t * nqt + u] * ul[u];
+      long cnt, own;
+      double one;
+      const long *gg;
+      const double *ww;
+      mapped_entries(m, idx[t], &cnt, &gg, &ww, &own, &one);
+      for (long e = 0; e < cnt; ++e)
+        if (!(op->dirichlet && op->dirichlet[gg[e]]) && !mapped_constrained(m, gg[e])) dst[gg[e]] += ww[e] * o;
+    }
+  }
+  free(A);
+}
+
+/* (C^T A C)_gg = sum_K sum_{t,u} w_t(g) A_K(t,u) w_u(g); Dirichlet and
+ * constrained DoFs get 1 */
+void orcm_diagonal(const orc_mapped *m, const orc_op *op, double *diag)
+{
+  geo_t g;
+  mapped_geo(m, &g);
+  const int n = g.n, nqt = n * n * n;
+  memset(diag, 0, sizeof(double) * m->n_dofs);
+  double *A = (double *)malloc(sizeof(double) * nqt * nqt);
+  for (long K = 0; K < m->n_cells; ++K) {
+    double vc[8][3];
+    long idx[MAXN3];
+    mapped_cell(m, K, vc, idx, nqt);
+    element_matrix_vc(op, &g, vc, idx, 0.0, A);
+    /* distinct targets of the cell and their weights per local DoF */
+    long tg[4 * MAXN3];
+    int nt = 0;
+    for (int t = 0; t < nqt; ++t) {
+      long cnt, own;
+      double one;
+      const long *gg;
+      const double *ww;
+      mapped_entries(m, idx[t], &cnt, &gg, &ww, &own, &one);
+      for (long e = 0; e < cnt; ++e) {
+        int found = 0;
+        for (int q = 0; q < nt; ++q) found |= tg[q] == gg[e];
+        if (!found && nt < 4 * MAXN3) tg[nt++] = gg[e];
+      }
+    }
+    for (int q = 0; q < nt; ++q) {
+      const long target = tg[q];
+      if (mapped_constrained(m, target) || (op->dirichlet && op->dirichlet[target])) continue;
+      double wt[MAXN3];
+      for (int t = 0; t < nqt; ++t) {
+        long cnt, own;
+        double one;
+        const long *gg;
+        const double *ww;
+        mapped_entries(m, idx[t], &cnt, &gg, &ww, &own, &one);
+        wt[t] = 0.0;
+        for (long e = 0; e < cnt; ++e)
+          if (gg[e] == target) wt[t] += ww[e];
+      }
+      double s = 0.0;
+      for (int t = 0; t < nqt; ++t)
+        if (wt[t] != 0.0)
+          for (int u = 0; u < nqt; ++u) s += wt[t] * A[t * nqt + u] * wt[u];
+      diag[target] += s;
+    }
+  }
+  for (long i = 0; i < m->n_dofs; ++i)
+    if (mapped_constrained(m, i) || (op->dirichlet && op->dirichlet[i])) diag[i] = 1.0;
+  free(A);
 }

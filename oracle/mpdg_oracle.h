@@ -158,6 +158,24 @@ void orc2_diagonal(const orc_mesh2 *m, const orc_op *op, double *diag);
 void orc2_distribute(const orc_mesh2 *m, double *u);
 void orc2_dof_coordinates(const orc_mesh2 *m, double *xyz);
 
+/* ------------------------------------------------------------- mapped meshes
+ * Unstructured hexahedra: each cell's 8 corners (x fastest) and its cell->DoF
+ * map (n^3 per cell, lexicographic), homogeneous affine constraints as CSR over
+ * all DoFs (cons_ptr[N+1]; an empty range = unconstrained).  dim 3, constant
+ * coefficients or fields read through the map; no faces, no SUPG. */
+typedef struct {
+  int degree;
+  long n_cells, n_dofs;
+  const double *cell_vertices;
+  const long *cell_dofs;
+  const long *cons_ptr;
+  const long *cons_idx;
+  const double *cons_w;
+} orc_mapped;
+
+void orcm_vmult(const orc_mapped *m, const orc_op *op, double *dst, const double *src);
+void orcm_diagonal(const orc_mapped *m, const orc_op *op, double *diag);
+
 #ifdef __cplusplus
 }
 #endif

@@ -51,6 +51,14 @@ class _Mesh2(C.Structure):
     _fields_ = [("coarse", _Mesh), ("fine", _Mesh)]
 
 
+_lp = C.POINTER(C.c_long)
+
+
+class _Mapped(C.Structure):
+    _fields_ = [("degree", C.c_int), ("n_cells", C.c_long), ("n_dofs", C.c_long), ("cell_vertices", _dp),
+                ("cell_dofs", _lp), ("cons_ptr", _lp), ("cons_idx", _lp), ("cons_w", _dp)]
+
+
 class _Prec(C.Structure):
     _fields_ = [("type", C.c_int), ("inv_diag", _dp), ("degree", C.c_int),
                 ("lambda_min", C.c_double), ("lambda_max", C.c_double)]
@@ -100,6 +108,9 @@ def lib():
         L.orc2_diagonal.argtypes = [P_m2, P_o, _dp]
         L.orc2_distribute.argtypes = [P_m2, _dp]
         L.orc2_dof_coordinates.argtypes = [P_m2, _dp]
+        P_mm = C.POINTER(_Mapped)
+        L.orcm_vmult.argtypes = [P_mm, P_o, _dp, _dp]
+        L.orcm_diagonal.argtypes = [P_mm, P_o, _dp]
         _lib = L
     return _lib
 
@@ -451,3 +462,104 @@ def lsq_projection(mesh, op, old_solutions, rhs):
     for s in range(step):
         x = x + c[s] * old_solutions[s]
     return x, step
+
+
+# ------------------------------------------------------------- mapped meshes
+
+def _cell_corners(vert, nc, ix, iy, iz):
+    V = vert.reshape(nc[2] + 1, nc[1] + 1, nc[0] + 1, 3)
+    return np.array([V[iz + (v >> 2 & 1), iy + (v >> 1 & 1), ix + (v & 1)] for v in range(8)])
+
+
+class MappedMesh:
+    """Unstructured hexahedral mesh in the ingestion form (orc_mapped): each
+    cell's 8 corners (x fastest), its n^3 global DoFs (lexicographic within the
+    cell), and homogeneous constraints {dof: [(master, weight), ...]}."""
+
+    def __init__(self, degree, cell_vertices, cell_dofs, n_dofs, constraints=None):
+        self.degree = int(degree)
+        n = degree + 1
+        self.cell_vertices = np.ascontiguousarray(cell_vertices, np.float64).reshape(-1, 8, 3)
+        self.cell_dofs = np.ascontiguousarray(cell_dofs, np.int64).reshape(-1, n ** 3)
+        self.n_cells = self.cell_dofs.shape[0]
+        self.n_dofs = int(n_dofs)
+        self.constraints = dict(constraints or {})
+        ptr = np.zeros(self.n_dofs + 1, np.int64)
+        idx, w = [], []
+        for g in range(self.n_dofs):
+            ent = self.constraints.get(g, [])
+            ptr[g + 1] = ptr[g] + len(ent)
+            idx += [m for m, _ in ent]
+            w += [x for _, x in ent]
+        self.cons_ptr = ptr
+        self.cons_idx = np.ascontiguousarray(idx if idx else [0], np.int64)
+        self.cons_w = np.ascontiguousarray(w if w else [0.0], np.float64)
+        self._c = _Mapped(self.degree, self.n_cells, self.n_dofs, _ptr(self.cell_vertices),
+                          self.cell_dofs.ctypes.data_as(_lp), ptr.ctypes.data_as(_lp),
+                          self.cons_idx.ctypes.data_as(_lp), _ptr(self.cons_w))
+
+    def constrained_mask(self):
+        m = np.zeros(self.n_dofs, np.uint8)
+        m[list(self.constraints)] = 1
+        return m
+
+
+def mapped_from_mesh(mesh, perm=None, cell_order=None):
+    """The structured 3D mesh `mesh` in the ingestion form; `perm[g]` renumbers
+    DoF g, `cell_order` lists the cells (lexicographic index) in the order given."""
+    p, nc = mesh.degree, mesh.nc
+    n = p + 1
+    NX, NY = mesh.shape[0], mesh.shape[1]
+    cells = list(cell_order) if cell_order is not None else range(nc[0] * nc[1] * nc[2])
+    verts, dofs = [], []
+    for c in cells:
+        ix, iy, iz = c % nc[0], (c // nc[0]) % nc[1], c // (nc[0] * nc[1])
+        verts.append(_cell_corners(mesh.vert, nc, ix, iy, iz))
+        k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+        g = ((iz * p + k) * NY + (iy * p + j)) * NX + (ix * p + i)
+        g = g.reshape(-1)
+        dofs.append(g if perm is None else np.asarray(perm)[g])
+    return MappedMesh(p, np.array(verts), np.array(dofs), mesh.n_dofs)
+
+
+def mapped_from_mesh2(m2):
+    """The two-level mesh `m2` in the ingestion form: its cells (coarse, then
+    fine), its DoF numbering, and the hanging constraints of the fine DoFs on
+    the interface plane (weights: the coarse face's Lagrange basis at the fine
+    node, hanging_matrix)."""
+    p = m2.degree
+    n = p + 1
+    mc = mapped_from_mesh(m2.coarse)
+    mf = mapped_from_mesh(m2.fine)
+    P = hanging_matrix(p)
+    NXc, NYc = m2.coarse.shape[0], m2.coarse.shape[1]
+    NXf, NYf, NZf = m2.fine.shape
+    ncf = m2.fine.nc
+    cons = {}
+    for Zf in range(NZf):
+        for Yf in range(NYf):
+            iy, iz = min(Yf // p, ncf[1] - 1), min(Zf // p, ncf[2] - 1)
+            j, k = Yf - iy * p, Zf - iz * p
+            sy, cy, sz, cz = iy % 2, iy // 2, iz % 2, iz // 2
+            ent = []
+            for kp in range(n):
+                for jp in range(n):
+                    w = P[sy, j, jp] * P[sz, k, kp]
+                    if abs(w) > 1e-14:
+                        ent.append((((cz * p + kp) * NYc + (cy * p + jp)) * NXc + (NXc - 1), float(w)))
+            cons[m2.n_coarse + (Zf * NYf + Yf) * NXf] = ent
+    return MappedMesh(p, np.concatenate([mc.cell_vertices, mf.cell_vertices]),
+                      np.concatenate([mc.cell_dofs, mf.cell_dofs + m2.n_coarse]), m2.n_dofs, cons)
+
+
+def mapped_vmult(mm, op, src):
+    src = np.ascontiguousarray(src, np.float64)
+    dst = np.zeros(mm.n_dofs)
+    lib().orcm_vmult(C.byref(mm._c), C.byref(op._c), _ptr(dst), _ptr(src))
+    return dst
+
+
+def mapped_diagonal(mm, op):
+    d = np.zeros(mm.n_dofs)
+    lib().orcm_diagonal(C.byref(mm._c), C.byref(op._c), _ptr(d))
+    return d

@@ -1,0 +1,161 @@
+"""Mapped meshes (mpdg_mesh_create_mapped, the ingestion form of an
+unstructured mesh) on the device against the oracle's mapped operator:
+vmult (FP64 1e-12, FP32 2e-5) and the diagonal (1e-12) on structured meshes
+handed over with a random DoF numbering and cell order, and on the two-level
+mesh handed over with its hanging-node constraints; equal to the structured
+and two-level device paths on the same meshes; CG iteration counts as the
+oracle's; create_rhs as the structured path's."""
+import numpy as np
+import pytest
+
+from gpu_helpers import dev, meshes, relerr, rng
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 2e-5
+
+
+def device_mesh(mm, mask):
+    import meltpooldg_b200 as M
+    return M.MappedMesh(mm.cell_vertices, mm.cell_dofs, mm.n_dofs, mm.degree, dirichlet_mask=mask,
+                        constraints=mm.constraints)
+
+
+def _ops(gm, kind, mask, prec=("fp64", "fp32")):
+    import meltpooldg_b200 as M
+    if kind == "heat":
+        return (M.HeatDiffuseOperator(gm, 1e-2, rho_cp=2.0, k0=1.5, precisions=prec),
+                O.Operator(O.HEAT, 1e-2, rho_cp=2.0, k0=1.5, dirichlet=mask))
+    return (M.AdvectionDiffusionOperator(gm, 1e-2, theta=0.5, diffusivity=0.05, velocity="vortex", precisions=prec),
+            O.Operator(O.ADVDIFF, 1e-2, theta=0.5, diffusivity=0.05, vel_kind=O.VEL_VORTEX, dirichlet=mask))
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+@pytest.mark.parametrize("kind", ["heat", "advdiff"])
+def test_mapped_structured_renumbered(cuda, p, kind):
+    import torch
+    import meltpooldg_b200 as M
+    nc = (3, 4, 2)
+    mask_s = M.boundary_mask(nc, p, faces=[(0, 0), (1, 1)])
+    gs, om = meshes(nc, p, 0.1, seed=p, mask=mask_s, lo=(-1, -1, -1), hi=(1, 1, 1))
+    R = rng(50 + p)
+    perm = R.permutation(om.n_dofs)
+    mm = O.mapped_from_mesh(om, perm=perm, cell_order=R.permutation(om.n_cells))
+    mask = np.empty_like(mask_s)
+    mask[perm] = mask_s
+    gm = device_mesh(mm, mask)
+    op, oop = _ops(gm, kind, mask)
+    x = R.uniform(-1, 1, om.n_dofs)
+    ref = O.mapped_vmult(mm, oop, x)
+    y = torch.empty(om.n_dofs, dtype=torch.float64, device="cuda")
+    op.vmult(y, dev(x))
+    assert relerr(y.cpu().numpy(), ref) < TOL64
+    y32 = torch.empty(om.n_dofs, dtype=torch.float32, device="cuda")
+    op.vmult(y32, dev(x, torch.float32))
+    assert relerr(y32.double().cpu().numpy(), ref) < TOL32
+    d = torch.empty_like(y)
+    op.compute_diagonal(d)
+    assert relerr(d.cpu().numpy(), O.mapped_diagonal(mm, oop)) < TOL64
+    # the structured path on the same mesh, renumbered
+    ops, _ = _ops(gs, kind, mask_s, prec=("fp64",))
+    xs = x[perm]
+    ys = torch.empty_like(y)
+    ops.vmult(ys, dev(xs))
+    assert relerr(y.cpu().numpy()[perm], ys.cpu().numpy()) < TOL64
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+@pytest.mark.parametrize("kind", ["heat", "advdiff"])
+def test_mapped_hanging_constraints(cuda, p, kind):
+    import torch
+    import meltpooldg_b200 as M
+    m2 = O.Mesh2(p, (2, 2, 2), 2, perturb=0.1, seed=20 + p)
+    mask = m2.boundary_face_mask()
+    mm = O.mapped_from_mesh2(m2)
+    gm = device_mesh(mm, mask)
+    op, oop = _ops(gm, kind, mask)
+    x = rng(60 + p).uniform(-1, 1, m2.n_dofs)
+    ref = O.mapped_vmult(mm, oop, x)
+    y = torch.empty(m2.n_dofs, dtype=torch.float64, device="cuda")
+    op.vmult(y, dev(x))
+    assert relerr(y.cpu().numpy(), ref) < TOL64
+    assert relerr(ref, O.vmult2(m2, oop, x)) < 1e-14
+    y32 = torch.empty(m2.n_dofs, dtype=torch.float32, device="cuda")
+    op.vmult(y32, dev(x, torch.float32))
+    assert relerr(y32.double().cpu().numpy(), ref) < TOL32
+    d = torch.empty_like(y)
+    op.compute_diagonal(d)
+    assert relerr(d.cpu().numpy(), O.mapped_diagonal(mm, oop)) < TOL64
+    # the two-level device path on the same mesh
+    nc_f = (2, 4, 4)
+    gt = M.TwoLevelMesh(m2.coarse.vert, (2, 2, 2), m2.fine.vert, nc_f, p, mask[:m2.n_coarse], mask[m2.n_coarse:])
+    ot, _ = _ops(gt, kind, mask, prec=("fp64",))
+    yt = torch.empty_like(y)
+    ot.vmult(yt, dev(x))
+    assert relerr(y.cpu().numpy(), yt.cpu().numpy()) < TOL64
+
+
+@pytest.mark.parametrize("p", [2, 3])
+def test_mapped_cg_iterations_match_oracle(cuda, p):
+    import torch
+    import meltpooldg_b200 as M
+    m2 = O.Mesh2(p, (2, 3, 2), 2, perturb=0.1, seed=30 + p)
+    mask = m2.boundary_face_mask()
+    mm = O.mapped_from_mesh2(m2)
+    gm = device_mesh(mm, mask)
+    op, oop = _ops(gm, "heat", mask, prec=("fp64",))
+    fixed = mm.constrained_mask().astype(bool) | mask.astype(bool)
+    R = rng(70 + p)
+    xs = R.uniform(-1, 1, m2.n_dofs)
+    xs[fixed] = 0.0
+    b = O.mapped_vmult(mm, oop, xs)
+    inv = 1.0 / O.mapped_diagonal(mm, oop)
+    x, r = np.zeros_like(b), b.copy()
+    z = inv * r
+    pdir, rz, res0, its_ref = z.copy(), r @ z, np.linalg.norm(b), 0
+    for it in range(1, 2000):
+        Ap = O.mapped_vmult(mm, oop, pdir)
+        alpha = rz / (pdir @ Ap)
+        x += alpha * pdir
+        r -= alpha * Ap
+        if np.linalg.norm(r) <= 1e-10 * res0:
+            its_ref = it
+            break
+        z = inv * r
+        rz_new = r @ z
+        pdir = z + (rz_new / rz) * pdir
+        rz = rz_new
+    xd = torch.zeros(m2.n_dofs, dtype=torch.float64, device="cuda")
+    its = M.LinearSolver.solve(op, xd, dev(b), M.LinearSolverData(solver_type="CG", preconditioner_type="Diagonal",
+                                                                  rel_tolerance=1e-10, abs_tolerance=0.0))
+    assert abs(its - its_ref) <= 1, (its, its_ref)
+    assert np.linalg.norm(xd.cpu().numpy() - x) <= 1e-8 * np.linalg.norm(x)
+
+
+def test_mapped_rhs_equals_structured(cuda):
+    import torch
+    import meltpooldg_b200 as M
+    p, nc = 2, (3, 3, 3)
+    gs, om = meshes(nc, p, 0.1, seed=4, lo=(-1, -1, -1), hi=(1, 1, 1))
+    perm = rng(80).permutation(om.n_dofs)
+    gm = device_mesh(O.mapped_from_mesh(om, perm=perm), None)
+    ops, _ = _ops(gs, "advdiff", None, prec=("fp64",))
+    opm, _ = _ops(gm, "advdiff", None, prec=("fp64",))
+    phi = rng(81).uniform(-1, 1, om.n_dofs)
+    rs = torch.zeros(om.n_dofs, dtype=torch.float64, device="cuda")
+    ops.create_rhs(rs, dev(phi))
+    phim = np.empty_like(phi)
+    phim[perm] = phi
+    rm = torch.zeros_like(rs)
+    opm.create_rhs(rm, dev(phim))
+    assert relerr(rm.cpu().numpy()[perm], rs.cpu().numpy()) < TOL64
+
+
+def test_mapped_rejects_chained_constraints(cuda):
+    import meltpooldg_b200 as M
+    om = O.Mesh.box(3, 1, [2, 1, 1])
+    mm = O.mapped_from_mesh(om)
+    with pytest.raises(Exception, match="masters"):
+        M.MappedMesh(mm.cell_vertices, mm.cell_dofs, mm.n_dofs, 1, constraints={0: [(1, 1.0)], 1: [(2, 1.0)]})

@@ -1,0 +1,46 @@
+"""CPU checks of the oracle's mapped-mesh operator (the ingestion form of an
+unstructured mesh: per-cell corners, cell->DoF map, affine constraints):
+it reproduces the structured oracle on the same mesh, is invariant under
+renumbering the DoFs and reordering the cells, and with the hanging-node
+constraints of a two-level mesh reproduces the two-level oracle."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_mapped_equals_structured_and_is_permutation_invariant(p):
+    m = O.Mesh.box(3, p, [3, 2, 4], perturb=0.1, seed=1)
+    mask = m.boundary_face_mask([(0, 0), (2, 1)])
+    op = O.Operator(O.ADVDIFF, 1e-2, theta=0.5, diffusivity=0.1, vel_kind=O.VEL_VORTEX, dirichlet=mask)
+    x = np.random.default_rng(p).uniform(-1, 1, m.n_dofs)
+    a = O.vmult(m, op, x)
+    assert np.abs(O.mapped_vmult(O.mapped_from_mesh(m), op, x) - a).max() <= 1e-14 * np.abs(a).max()
+    assert np.abs(O.mapped_diagonal(O.mapped_from_mesh(m), op) - O.diagonal(m, op)).max() <= 1e-14 * np.abs(
+        O.diagonal(m, op)).max()
+    R = np.random.default_rng(10 + p)
+    perm = R.permutation(m.n_dofs)
+    mp = O.mapped_from_mesh(m, perm=perm, cell_order=R.permutation(m.n_cells))
+    opp = op.with_dirichlet(mask[np.argsort(perm)])
+    xp = np.empty_like(x)
+    xp[perm] = x
+    assert np.abs(O.mapped_vmult(mp, opp, xp)[perm] - a).max() <= 1e-14 * np.abs(a).max()
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+@pytest.mark.parametrize("kind", [O.HEAT, O.ADVDIFF])
+def test_mapped_hanging_constraints_equal_two_level(p, kind):
+    m2 = O.Mesh2(p, (2, 2, 2), 2, perturb=0.1, seed=3)
+    mask = m2.boundary_face_mask()
+    if kind == O.HEAT:
+        op = O.Operator(O.HEAT, 1e-2, rho_cp=2.0, k0=1.5, dirichlet=mask)
+    else:
+        op = O.Operator(O.ADVDIFF, 1e-2, theta=0.5, diffusivity=0.05, vel_kind=O.VEL_VORTEX, dirichlet=mask)
+    mm = O.mapped_from_mesh2(m2)
+    assert set(mm.constraints) == set(np.flatnonzero(m2.hanging_mask()))
+    x = np.random.default_rng(p).uniform(-1, 1, m2.n_dofs)
+    a = O.vmult2(m2, op, x)
+    assert np.abs(O.mapped_vmult(mm, op, x) - a).max() <= 1e-14 * np.abs(a).max()
+    d = O.diagonal2(m2, op)
+    assert np.abs(O.mapped_diagonal(mm, op) - d).max() <= 1e-13 * np.abs(d).max()
