@@ -86,6 +86,23 @@ def streamed_bytes(n_dofs, n_cells, degree, real_bytes):
     return real_bytes * (2 * n_dofs) + real_bytes * 7 * nq * n_cells
 
 
+def algorithmic_flops(n_cells, degree):
+    """Algorithmic flops of one apply (the hot-path scope table's secondary
+    roofline): E (24 n^4 + c_q n^3), c_q = 20 on Cartesian heat cells, 45 on
+    general geometry (the J^-T transforms), 60 with the analytic velocity."""
+    n = degree + 1
+    c_q = {"advdiff": 60, "c1": 20}.get(WORKLOAD["name"], 45)
+    return n_cells * (24 * n ** 4 + c_q * n ** 3)
+
+
+def fma_peaks(M):
+    """Measured FMA throughput (GFLOP/s) in FP64 and FP32 (mpdg_fma_peak)."""
+    import ctypes as C
+    g64, g32 = C.c_double(0.0), C.c_double(0.0)
+    M._capi.check(M._capi.lib().mpdg_fma_peak(C.byref(g64), C.byref(g32)), "fma_peak")
+    return g64.value, g32.value
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -366,6 +383,8 @@ def run_ours(args, rank, world):
 
     peak, peak_kind = load_peaks()
     E = int(np.prod(NC))
+    f64_peak, f32_peak = fma_peaks(M)
+    flops = algorithmic_flops(E, DEGREE)
     geom = "UNIFORM" if WORKLOAD["name"] in ("advdiff", "c1") else "GENERAL"
     kernel_name = f"warp_apply_kernel<{DEGREE},double,{geom}> x 8 colour launches"
     b64 = algorithmic_bytes(N, E, DEGREE, 8)
@@ -384,7 +403,13 @@ def run_ours(args, rank, world):
                          "frac": st64 / apply_s / 1e9 / peak},
             "fp32": {"achieved": b32 / apply32_s / 1e9, "frac": b32 / apply32_s / 1e9 / peak,
                      "algorithmic_bytes": b32, "streamed_bytes": st32,
-                     "streamed_frac": st32 / apply32_s / 1e9 / peak}}
+                     "streamed_frac": st32 / apply32_s / 1e9 / peak},
+            "flops": {"per_apply": flops, "unit": "GFLOP/s",
+                      "fp64": {"achieved": flops / apply_s / 1e9, "peak": f64_peak,
+                               "frac": flops / apply_s / 1e9 / f64_peak},
+                      "fp32": {"achieved": flops / apply32_s / 1e9, "peak": f32_peak,
+                               "frac": flops / apply32_s / 1e9 / f32_peak},
+                      "peak_source": "mpdg_fma_peak: FMA chains measured on this GPU (8 per thread, 8 CTAs per SM)"}}
 
     # solves: CG + Chebyshev(5)/Jacobi to 1e-10, FP64 and FP32-inner/FP64-refined
     solves = None

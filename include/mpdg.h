@@ -245,6 +245,9 @@ mpdg_status mpdg_vmult_f32(mpdg_op *op, float *dst, const float *src);
  * the others apply the vectors in turn.  Replaces the n vmult calls of
  * LeastSquaresProjection::vmult (include/meltpooldg/linear_algebra/predictor.hpp:37-46). */
 mpdg_status mpdg_vmult_multi(mpdg_op *op, int n_vectors, double *const *dst, const double *const *src);
+/* measured FMA throughput of the current GPU (GFLOP/s, 2 flops per FMA) in
+ * FP64 and FP32: the arithmetic ceiling the apply's flop rate is reported against */
+mpdg_status mpdg_fma_peak(double *gflops64, double *gflops32);
 mpdg_status mpdg_vmult_multi_f32(mpdg_op *op, int n_vectors, float *const *dst, const float *const *src);
 /* LeastSquaresProjection::vmult (predictor.hpp:37-80): solution = sum_s c_s old[s]
  * minimising |A sum_s c_s old[s] - rhs| over the first old solutions whose images

@@ -134,6 +134,7 @@ def lib():
     L.mpdg_vmult.argtypes = [vp, vp, vp]
     L.mpdg_vmult_f32.argtypes = [vp, vp, vp]
     L.mpdg_vmult_multi.argtypes = [vp, C.c_int, C.POINTER(vp), C.POINTER(vp)]
+    L.mpdg_fma_peak.argtypes = [dp, dp]
     L.mpdg_vmult_multi_f32.argtypes = [vp, C.c_int, C.POINTER(vp), C.POINTER(vp)]
     L.mpdg_predict_lsq.argtypes = [vp, C.c_int, C.POINTER(vp), vp, vp, C.POINTER(C.c_int)]
     L.mpdg_vmult_host.argtypes = [vp, dp, dp]

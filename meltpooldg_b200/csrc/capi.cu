@@ -429,6 +429,15 @@ mpdg_status mpdg_vmult(mpdg_op *op, double *dst, const double *src)
   });
 }
 
+mpdg_status mpdg_fma_peak(double *gflops64, double *gflops32)
+{
+  return guarded([&]() -> int {
+    if (!gflops64 || !gflops32) throw Error{MPDG_ERR_ARG, "null argument"};
+    fma_peak(*gflops64, *gflops32);
+    return MPDG_OK;
+  });
+}
+
 mpdg_status mpdg_vmult_multi(mpdg_op *op, int n_vectors, double *const *dst, const double *const *src)
 {
   return guarded([&]() -> int {

@@ -221,6 +221,7 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
 void ensure_metric32(Mesh &m, cudaStream_t s);
 void build_op_device_data(Op &op);
 void ensure_T32(Op &op);
+void fma_peak(double &gflops64, double &gflops32);
 void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d);
 inline bool law_has_solid(int mat) { return mat == MPDG_MAT_LIQUID_SOLID || mat == MPDG_MAT_GAS_LIQUID_SOLID; }
 inline bool law_two_phase(int mat) { return mat == MPDG_MAT_GAS_LIQUID || mat == MPDG_MAT_GAS_LIQUID_SOLID; }
