@@ -289,7 +289,7 @@ void free_op_arrays(Op &o)
   for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32,
                   (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32, (void *)o.d_trig64, o.d_stage,
                   (void *)o.d_tau64, (void *)o.d_tau32, (void *)o.Told_own, (void *)o.H_own, (void *)o.Told32,
-                  (void *)o.H32, (void *)o.lsq_buf,
+                  (void *)o.H32, (void *)o.lsq_buf, (void *)o.host_stage,
                   (void *)o.d_io, o.io_tmp})
     if (p) cudaFree(p);
 }
@@ -486,14 +486,16 @@ mpdg_status mpdg_vmult_host(mpdg_op *op, double *dst_host, const double *src_hos
     if (!op || !dst_host || !src_host) throw Error{MPDG_ERR_ARG, "null argument"};
     Op &o = op->o;
     const size_t bytes = sizeof(double) * o.mesh->N;
-    double *d_src = nullptr, *d_dst = nullptr;
-    MPDG_CUDA(cudaMallocAsync(&d_src, bytes, o.stream));
-    MPDG_CUDA(cudaMallocAsync(&d_dst, bytes, o.stream));
+    // device staging kept by the operator between calls: a vmult from host
+    // buffers costs its two PCIe copies and the apply, no allocation
+    if (!o.host_stage) {
+      MPDG_CUDA(cudaMalloc(&o.host_stage, 2 * bytes));
+      o.device_bytes += 2 * bytes;
+    }
+    double *d_src = o.host_stage, *d_dst = o.host_stage + o.mesh->N;
     MPDG_CUDA(cudaMemcpyAsync(d_src, src_host, bytes, cudaMemcpyHostToDevice, o.stream));
     launch_apply<double>(o, d_dst, d_src);
     MPDG_CUDA(cudaMemcpyAsync(dst_host, d_dst, bytes, cudaMemcpyDeviceToHost, o.stream));
-    MPDG_CUDA(cudaFreeAsync(d_src, o.stream));
-    MPDG_CUDA(cudaFreeAsync(d_dst, o.stream));
     MPDG_CUDA(cudaStreamSynchronize(o.stream));
     return MPDG_OK;
   });

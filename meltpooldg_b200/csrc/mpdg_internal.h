@@ -157,6 +157,8 @@ struct Op {
   // inflow/outflow constraints (advection_diffusion_operator.cpp:545-578): identity
   // rows at the flagged DoFs; the source there is read as 0 and copied to the result
   uint8_t *d_io = nullptr;
+  // device copies of the host vectors of mpdg_vmult_host (src, dst)
+  double *host_stage = nullptr;
   // least-squares predictor: images of the old solutions (lsq_cols vectors of N)
   double *lsq_buf = nullptr;
   int lsq_cols = 0;
