@@ -179,7 +179,8 @@ mpdg_status mpdg_mesh_create_two_level(const mpdg_mesh_desc *coarse, const mpdg_
  * coloured greedily (no two cells of a colour share a DoF; at most 64 colours),
  * so the scatter is atomic-free and deterministic.  Operators on it take the
  * heat operator with constant coefficients or the advection-diffusion operator
- * (prescribed velocity); vmult, the diagonal, create_rhs and the solvers. */
+ * (prescribed velocity); vmult, the diagonal, create_rhs, the solvers and the
+ * integrated L2 norm. */
 typedef struct {
   int degree;                        /* 1..4 */
   int64_t n_cells, n_dofs;

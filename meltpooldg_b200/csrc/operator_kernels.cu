@@ -2319,26 +2319,31 @@ namespace mpdg {
 // per-cell integrated L2 norm squared (one thread per cell), summed per block
 template <int P>
 __global__ void l2_cells_kernel(const double *u, long NX, long NY, int nc0, int nc1, long n_cells,
-                                const Colour *colours, const double *metric, double hx, double hy,
-                                double hz, double *partial)
+                                const Colour *colours, const int *cmap, const double *metric, double hx,
+                                double hy, double hz, double *partial)
 {
   constexpr int n = P + 1, n3 = n * n * n;
   const Tables<double> &T = tab<double>(P);
   double s = 0.0;
   for (long cell = (long)blockIdx.x * blockDim.x + threadIdx.x; cell < n_cells;
        cell += (long)gridDim.x * blockDim.x) {
-    int c = 0;
-    while (c < 7 && cell >= colours[c + 1].first) ++c;
-    const Colour &C = colours[c];
-    const long cidx = cell - C.first;
-    const int ix = 2 * (int)(cidx % C.cn[0]) + C.par[0];
-    const int iy = 2 * (int)((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
-    const int iz = 2 * (int)(cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
     double a[n3], b[n3];
-    for (int k = 0; k < n; ++k)
-      for (int j = 0; j < n; ++j)
-        for (int i = 0; i < n; ++i)
-          a[(k * n + j) * n + i] = u[((long)(iz * P + k) * NY + (iy * P + j)) * NX + (ix * P + i)];
+    if (cmap) {
+      // mapped mesh: the cell's DoFs through its cell->DoF map
+      for (int t = 0; t < n3; ++t) a[t] = u[cmap[cell * n3 + t]];
+    } else {
+      int c = 0;
+      while (c < 7 && cell >= colours[c + 1].first) ++c;
+      const Colour &C = colours[c];
+      const long cidx = cell - C.first;
+      const int ix = 2 * (int)(cidx % C.cn[0]) + C.par[0];
+      const int iy = 2 * (int)((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
+      const int iz = 2 * (int)(cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
+      for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j)
+          for (int i = 0; i < n; ++i)
+            a[(k * n + j) * n + i] = u[((long)(iz * P + k) * NY + (iy * P + j)) * NX + (ix * P + i)];
+    }
     // x, y, z interpolation to the Gauss points
     for (int k = 0; k < n; ++k)
       for (int j = 0; j < n; ++j)
@@ -2380,7 +2385,6 @@ __global__ void l2_cells_kernel(const double *u, long NX, long NY, int nc0, int 
 double l2_norm_integrated(Op &op, const double *u)
 {
   if (op.fine) throw Error{MPDG_ERR_UNSUPPORTED, "integrated norms on two-level meshes"};
-  if (op.mesh->mapped) throw Error{MPDG_ERR_UNSUPPORTED, "integrated norms on mapped meshes"};
   Mesh &m = *op.mesh;
   const int blocks = 256;
   Colour *d_col = nullptr;
@@ -2390,10 +2394,10 @@ double l2_norm_integrated(Op &op, const double *u)
   MPDG_CUDA(cudaMalloc(&partial, sizeof(double) * blocks));
   const double *met = m.uniform ? nullptr : m.d_metric64;
   switch (m.degree) {
-    case 1: l2_cells_kernel<1><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, met, m.h[0], m.h[1], m.h[2], partial); break;
-    case 2: l2_cells_kernel<2><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, met, m.h[0], m.h[1], m.h[2], partial); break;
-    case 3: l2_cells_kernel<3><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, met, m.h[0], m.h[1], m.h[2], partial); break;
-    case 4: l2_cells_kernel<4><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, met, m.h[0], m.h[1], m.h[2], partial); break;
+    case 1: l2_cells_kernel<1><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, m.d_cmap, met, m.h[0], m.h[1], m.h[2], partial); break;
+    case 2: l2_cells_kernel<2><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, m.d_cmap, met, m.h[0], m.h[1], m.h[2], partial); break;
+    case 3: l2_cells_kernel<3><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, m.d_cmap, met, m.h[0], m.h[1], m.h[2], partial); break;
+    case 4: l2_cells_kernel<4><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, m.d_cmap, met, m.h[0], m.h[1], m.h[2], partial); break;
     default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
   }
   MPDG_LAUNCHED();
