@@ -177,10 +177,11 @@ mpdg_status mpdg_mesh_create_two_level(const mpdg_mesh_desc *coarse, const mpdg_
  * cell loops with constraints form it: constrained DoFs are read through their
  * constraint, written to their masters and stay 0; diagonal 1 there.  Cells are
  * coloured greedily (no two cells of a colour share a DoF; at most 64 colours),
- * so the scatter is atomic-free and deterministic.  Operators on it take the
- * heat operator with constant coefficients or the advection-diffusion operator
- * (prescribed velocity); vmult, the diagonal, create_rhs, the solvers and the
- * integrated L2 norm. */
+ * so the scatter is atomic-free and deterministic.  Operators on it: the heat
+ * operator (k(T) and the phase laws only without constraints) and the
+ * advection-diffusion operator (prescribed velocity), without boundary faces
+ * or SUPG; vmult, the diagonal, create_rhs, the solvers and the integrated L2
+ * norm. */
 typedef struct {
   int degree;                        /* 1..4 */
   int64_t n_cells, n_dofs;

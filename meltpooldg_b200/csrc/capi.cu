@@ -243,11 +243,13 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     if (desc->supg && desc->kind != MPDG_OP_ADVDIFF)
       throw Error{MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator"};
     if (desc->supg && mm.fine) throw Error{MPDG_ERR_UNSUPPORTED, "SUPG on two-level meshes"};
-    if (mm.mapped && (desc->k_alpha != 0.0 || desc->full_tangent || desc->material != MPDG_MAT_LINEAR ||
-                      desc->supg || (desc->robin_faces && desc->robin_alpha != 0.0) ||
+    if (mm.mapped && (desc->supg || (desc->robin_faces && desc->robin_alpha != 0.0) ||
                       (desc->rad_faces && desc->rad_emissivity != 0.0)))
+      throw Error{MPDG_ERR_UNSUPPORTED, "mapped meshes take no boundary faces or SUPG"};
+    if (mm.mapped && mm.n_cons > 0 &&
+        (desc->k_alpha != 0.0 || desc->full_tangent || desc->material != MPDG_MAT_LINEAR))
       throw Error{MPDG_ERR_UNSUPPORTED,
-                  "mapped meshes take constant coefficients: no k(T) or phase law, full tangent, faces or SUPG"};
+                  "mapped meshes with constraints take constant coefficients (no k(T), phase law or full tangent)"};
     if (desc->supg && desc->diffusivity != 0.0 && !mm.uniform && !axis_aligned_lattice(mm))
       throw Error{MPDG_ERR_UNSUPPORTED,
                   "SUPG with diffusion needs axis-aligned cells (its Laplacian drops the Jacobian derivatives)"};

@@ -361,8 +361,12 @@ void launch_mapped_apply(Op &op, Real *dst, const Real *src)
     if (op.d.vel_kind != MPDG_VEL_NONE && !op.d_velb32)
       throw Error{MPDG_ERR_ARG, "the FP32 form was not prepared for this operator (precision_mask)"};
   }
+  const bool kt = uses_kT(op);
+  if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
+  check_law_fields(op, k);
   MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * N, op.stream));
-  dispatch_degree<Real, MODE_LINEAR, false>(op, k);
+  if (kt) dispatch_degree<Real, MODE_LINEAR, true>(op, k);
+  else dispatch_degree<Real, MODE_LINEAR, false>(op, k);
   mapped_condense<Real>(op, dst);
 }
 
@@ -460,12 +464,15 @@ void launch_mapped_diagonal(Op &op, double *diag)
   KP<double> k = base_params<double>(op);
   k.dst = diag;
   k.skip_constrained = 1;
+  const bool kt = uses_kT(op);
+  if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
+  check_law_fields(op, k);
   MPDG_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * m.N, op.stream));
   switch (m.degree) {
-    case 1: run_diag<1, false>(op, k); mapped_constrained_diagonal<1>(op, diag); break;
-    case 2: run_diag<2, false>(op, k); mapped_constrained_diagonal<2>(op, diag); break;
-    case 3: run_diag<3, false>(op, k); mapped_constrained_diagonal<3>(op, diag); break;
-    case 4: run_diag<4, false>(op, k); mapped_constrained_diagonal<4>(op, diag); break;
+    case 1: kt ? run_diag<1, true>(op, k) : run_diag<1, false>(op, k); mapped_constrained_diagonal<1>(op, diag); break;
+    case 2: kt ? run_diag<2, true>(op, k) : run_diag<2, false>(op, k); mapped_constrained_diagonal<2>(op, diag); break;
+    case 3: kt ? run_diag<3, true>(op, k) : run_diag<3, false>(op, k); mapped_constrained_diagonal<3>(op, diag); break;
+    case 4: kt ? run_diag<4, true>(op, k) : run_diag<4, false>(op, k); mapped_constrained_diagonal<4>(op, diag); break;
     default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
   }
   const uint8_t *tm = op.use_dirichlet ? m.d_tmask_dir : m.d_tmask_hang;
