@@ -268,3 +268,30 @@ def test_solidification_golden_through_a_mapped_mesh(cuda):
     for printed in golden[name]["printed"]:
         opn.solve()
         assert cases.printed_match(opn.l2_norm(), printed), (opn.l2_norm(), printed)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+@pytest.mark.parametrize("kind", ["heat", "advdiff"])
+def test_locally_refined_mesh(cuda, p, kind):
+    """A 3^3 mesh with a column of refined cells (face and edge hanging nodes,
+    perturbed coarse vertices) through refine_box: vmult, FP32 and the
+    diagonal against the oracle's mapped operator."""
+    import torch
+    from meltpooldg_b200.refine import refine_box
+    V = O.box_vertices(3, (3, 3, 3), [-1.0] * 3, [1.0] * 3, 0.1, 11)
+    r = refine_box((3, 3, 3), p, [13, 4, 22], vertices=V)
+    mm = O.MappedMesh(p, r["cell_vertices"], r["cell_dofs"], r["n_dofs"], r["constraints"])
+    mask = r["boundary"]
+    gm = device_mesh(mm, mask)
+    op, oop = _ops(gm, kind, mask)
+    x = rng(100 + p).uniform(-1, 1, mm.n_dofs)
+    ref = O.mapped_vmult(mm, oop, x)
+    y = torch.empty(mm.n_dofs, dtype=torch.float64, device="cuda")
+    op.vmult(y, dev(x))
+    assert relerr(y.cpu().numpy(), ref) < TOL64
+    y32 = torch.empty(mm.n_dofs, dtype=torch.float32, device="cuda")
+    op.vmult(y32, dev(x, torch.float32))
+    assert relerr(y32.double().cpu().numpy(), ref) < TOL32
+    d = torch.empty_like(y)
+    op.compute_diagonal(d)
+    assert relerr(d.cpu().numpy(), O.mapped_diagonal(mm, oop)) < TOL64
