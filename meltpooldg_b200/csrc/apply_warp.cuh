@@ -249,11 +249,15 @@ struct WOcc {
 // MULTI: applies the operator to p.nvec (<= kMaxMultiVec) vectors msrc[v] ->
 // mdst[v] (msrc[0] = src, mdst[0] = dst) in one pass: each group's coefficient
 // block is staged once and serves every vector
-template <int P, typename Real, int GEOM, bool HANG = false, bool MULTI = false>
+// MAPPED: a mapped mesh's cells, gathered and scattered through the
+// cell->DoF map p.cmap; dst is cleared before the colours and every cell adds
+// (the mesh's greedy colouring keeps the cells of a launch apart)
+template <int P, typename Real, int GEOM, bool HANG = false, bool MULTI = false, bool MAPPED = false>
 __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     warp_apply_kernel(const KP<Real> p, int *err)
 {
   static_assert(!(HANG && MULTI), "the multi-vector apply has no hanging-node path");
+  static_assert(!(MAPPED && (HANG || MULTI || GEOM != GEOM_GENERAL)), "mapped meshes: general geometry, one vector");
   constexpr int n = P + 1, n2 = n * n, n3 = n2 * n, CPW = WCfg<n>::cpw;
   constexpr int MS = metric_stride(n), VS = velb_stride(n);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -335,6 +339,10 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
         for (int kp = 0; kp < n; ++kp) sacc += T.H[(sz * n + k) * n + kp] * sk[kp];
         A[k] = sacc;
       }
+    } else if (MAPPED) {
+      const int *cmap = p.cmap + (p.cfirst + (long)(act ? cidx : 0)) * n3 + l;
+#pragma unroll
+      for (int k = 0; k < n; ++k) A[k] = act ? p.src[cmap[k * n2]] : Real(0);
     } else {
 #pragma unroll
       for (int k = 0; k < n; ++k) A[k] = act ? p.src[g0 + k * zs] : Real(0);
@@ -362,6 +370,11 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     if (active) colour_cell(cidx, p, ix, iy, iz);
     const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
     const uint4 cm = cmA;
+    // global DoFs of the lane's column
+    long gk[n];
+#pragma unroll
+    for (int k = 0; k < n; ++k)
+      gk[k] = MAPPED ? (active ? (long)p.cmap[(p.cfirst + cidx) * (long)n3 + k * n2 + l] : 0) : g0 + k * zs;
 
     // hanging lane of the fine block: its column is the coarse face's interpolant,
     // its slots are never written (stored 0 by the first cell), its result is staged
@@ -374,7 +387,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       const bool sz = (k == 0 && iz > 0) || (k == P && iz < p.nc[2] - 1);
-      const bool first = !(later_xy || (sz && (iz & 1)));
+      const bool first = !MAPPED && !(later_xy || (sz && (iz & 1)));
       const bool masked = p.masked_write && mask_bit(cm, k);
       first_bits |= (unsigned)first << k;
       mask_bits |= (unsigned)masked << k;
@@ -386,7 +399,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       const bool first = (first_bits >> k) & 1, masked = (mask_bits >> k) & 1;
-      dpre[k] = (active && !first && !masked && !hl) ? dst_v[g0 + k * zs] : Real(0);
+      dpre[k] = (active && !first && !masked && !hl) ? dst_v[gk[k]] : Real(0);
     }
 
     Real u[n];
@@ -491,7 +504,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     if (active) {
 #pragma unroll
       for (int k = 0; k < n; ++k) {
-        const long g = g0 + k * zs;
+        const long g = gk[k];
         if (hl) {
           if ((first_bits >> k) & 1) dst_v[g] = Real(0);
         } else if ((first_bits >> k) & 1) {

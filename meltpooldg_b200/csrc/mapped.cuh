@@ -252,13 +252,17 @@ void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d)
   std::vector<int> cmap((size_t)E * n3);
   std::vector<double> cvert((size_t)E * 24);
   std::vector<uint8_t> flags(E, 0);
+  std::vector<uint32_t> cmask(4 * (size_t)E, 0u);  // Dirichlet local DoFs (bit t), for the warp kernel
   for (long e = 0; e < E; ++e) {
     const long slot = next[colour_of[e]]++;
     uint8_t f = 0;
     for (int t = 0; t < n3; ++t) {
       const long g = d.cell_dofs[e * n3 + t];
       cmap[slot * n3 + t] = (int)g;
-      if (d.dirichlet_mask && d.dirichlet_mask[g]) f |= 1;
+      if (d.dirichlet_mask && d.dirichlet_mask[g]) {
+        f |= 1;
+        cmask[4 * slot + t / 32] |= 1u << (t % 32);
+      }
       if (cons_of[g] >= 0) f |= 2;
     }
     flags[slot] = f;
@@ -266,6 +270,15 @@ void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d)
     if (f & 2) m.ccells.push_back(slot);
   }
   std::sort(m.ccells.begin(), m.ccells.end());
+  // the lattice colours are unused on a mapped mesh; one colour covering all
+  // cells keeps the kernels that decode lattice positions (for fields they do
+  // not read here) within range
+  for (int c = 0; c < 8; ++c) {
+    m.colour[c] = Colour{};
+    m.colour[c].cn[0] = m.colour[c].cn[1] = m.colour[c].cn[2] = 1;
+    m.colour[c].first = (c == 0) ? 0 : E;
+    m.colour[c].count = (c == 0) ? E : 0;
+  }
   size_t &B = m.device_bytes;
   m.d_cmap = upload(cmap, B);
   m.d_cellvert = upload(cvert, B);
@@ -292,7 +305,10 @@ void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d)
     dc[g] = dir[g] || cc[g];
   }
   m.has_dirichlet = any_dir;
-  if (any_dir) m.d_dmask = upload(dir, B);
+  if (any_dir) {
+    m.d_dmask = upload(dir, B);
+    m.d_cell_mask = upload(cmask, B);
+  }
   m.d_tmask_dir = upload(dc, B);
   m.d_tmask_hang = upload(cc, B);
   // geometry: JxW and G per (cell, q) from each cell's corners
@@ -365,8 +381,17 @@ void launch_mapped_apply(Op &op, Real *dst, const Real *src)
   if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
   check_law_fields(op, k);
   MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * N, op.stream));
-  if (kt) dispatch_degree<Real, MODE_LINEAR, true>(op, k);
-  else dispatch_degree<Real, MODE_LINEAR, false>(op, k);
+  if (!kt && !uses_law(op)) {
+    // constant coefficients: the warp kernel on the merged coefficient stream
+    ensure_coef(op, sizeof(Real) == 4);
+    if constexpr (sizeof(Real) == 8) k.metric = op.d_coef64;
+    else k.metric = op.d_coef32;
+    warp_apply_degree<Real, GEOM_GENERAL>(op, k);
+  } else if (kt) {
+    dispatch_degree<Real, MODE_LINEAR, true>(op, k);
+  } else {
+    dispatch_degree<Real, MODE_LINEAR, false>(op, k);
+  }
   mapped_condense<Real>(op, dst);
 }
 

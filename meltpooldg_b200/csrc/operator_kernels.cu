@@ -1562,7 +1562,7 @@ int num_sms()
   return g_num_sms;
 }
 
-template <int P, typename Real, int GEOM, bool HANG, bool MULTI = false>
+template <int P, typename Real, int GEOM, bool HANG, bool MULTI = false, bool MAPPED = false>
 void run_warp_apply(Op &op, KP<Real> k)
 {
   Mesh &m = *op.mesh;
@@ -1579,7 +1579,7 @@ void run_warp_apply(Op &op, KP<Real> k)
     throw Error{MPDG_ERR_ARG, "coefficient stream not 16-byte aligned"};
   if (GEOM == GEOM_GENERAL && (!k.metric || (gvel && !k.velb)))
     throw Error{MPDG_ERR_ARG, "coefficient stream missing"};
-  auto kern = warp_apply_kernel<P, Real, GEOM, HANG, MULTI>;
+  auto kern = warp_apply_kernel<P, Real, GEOM, HANG, MULTI, MAPPED>;
   static int configured_smem = -1, blocks_per_sm = 0;  // per instantiation
   if (configured_smem != (int)smem) {
     MPDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1588,8 +1588,8 @@ void run_warp_apply(Op &op, KP<Real> k)
     configured_smem = (int)smem;
   }
   const long resident = (long)num_sms() * blocks_per_sm;
-  for (int c = 0; c < 8; ++c) {
-    const Colour &C = m.colour[c];
+  for (int c = 0; c < n_colours(m); ++c) {
+    const Colour &C = colours(m)[c];
     if (C.count == 0) continue;
     colour_params(k, C);
     const long groups = (C.count + CPW - 1) / CPW;
@@ -1603,6 +1603,18 @@ template <typename Real, int GEOM>
 void warp_apply_degree(Op &op, const KP<Real> &k)
 {
   const bool hang = k.hsrc != nullptr;
+  if constexpr (GEOM == GEOM_GENERAL) {
+    if (op.mesh->mapped) {
+      switch (op.mesh->degree) {
+        case 1: run_warp_apply<1, Real, GEOM, false, false, true>(op, k); break;
+        case 2: run_warp_apply<2, Real, GEOM, false, false, true>(op, k); break;
+        case 3: run_warp_apply<3, Real, GEOM, false, false, true>(op, k); break;
+        case 4: run_warp_apply<4, Real, GEOM, false, false, true>(op, k); break;
+        default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+      }
+      return;
+    }
+  }
   if (k.nvec > 1) {
     switch (op.mesh->degree) {
       case 1: run_warp_apply<1, Real, GEOM, false, true>(op, k); break;
@@ -2055,7 +2067,7 @@ void launch_apply_multi(Op &op, int nvec, Real *const *dst, const Real *const *s
   const bool heat = D.kind == MPDG_OP_HEAT;
   const bool faces = heat && ((D.robin_faces && D.robin_alpha != 0.0) || (D.rad_faces && D.rad_emissivity != 0.0));
   const bool full = heat && D.full_tangent;
-  const bool fused = !op.fine && !op.d_io && !faces && !supg(op) && !full && !uses_law(op) &&
+  const bool fused = !op.fine && !m.mapped && !op.d_io && !faces && !supg(op) && !full && !uses_law(op) &&
                      (!m.uniform || !uses_kT(op));
   if (!fused) {
     for (int v = 0; v < nvec; ++v) launch_apply<Real>(op, dst[v], src[v]);
