@@ -138,23 +138,23 @@ __device__ __forceinline__ void getY(const Real *t, int a, int b, Real (&v)[n])
 // nodal values u (Z layout) -> values uq and collocation gradients gx, gy, gz
 // at the Gauss points, all in Z layout.  S, Dc: tables in constant memory.
 template <int n, typename Real>
-__device__ __forceinline__ void l_forward(const Real *S, const Real *Dc, Real *t0, Real *t1, bool wr, int a,
-                                          int b, const Real (&u)[n], Real (&uq)[n], Real (&gx)[n],
-                                          Real (&gy)[n], Real (&gz)[n])
+__device__ __forceinline__ void l_forward(const Tables<Real> &T, Real *t0, Real *t1, bool wr, int a, int b,
+                                          const Real (&u)[n], Real (&uq)[n], Real (&gx)[n], Real (&gy)[n],
+                                          Real (&gz)[n])
 {
   Real v[n], w[n];
-  cz<n, Real, false>(S, u, v);  // z: nodes -> Gauss points
+  c1<n, Real, false, false>(T.S, T.eS, u, v);  // z: nodes -> Gauss points
   if (wr) putZ<n>(t0, a, b, v);
   __syncwarp();
   getX<n>(t0, a, b, w);
   __syncwarp();
-  cz<n, Real, false>(S, w, v);  // x
+  c1<n, Real, false, false>(T.S, T.eS, w, v);  // x
   if (wr) putX<n>(t0, a, b, v);
   __syncwarp();
   getY<n>(t0, a, b, w);
   __syncwarp();
-  cz<n, Real, false>(S, w, v);   // y: v = values at the Gauss points (Y layout)
-  cz<n, Real, false>(Dc, v, w);  // d/dy (Y layout)
+  c1<n, Real, false, false>(T.S, T.eS, w, v);    // y: v = values at the Gauss points (Y layout)
+  c1<n, Real, false, true>(T.Dc, T.eDc, v, w);   // d/dy (Y layout)
   if (wr) {
     putY<n>(t0, a, b, v);
     putY<n>(t1, a, b, w);
@@ -164,8 +164,8 @@ __device__ __forceinline__ void l_forward(const Real *S, const Real *Dc, Real *t
   getX<n>(t0, a, b, w);
   getZ<n>(t1, a, b, gy);
   __syncwarp();
-  cz<n, Real, false>(Dc, uq, gz);  // d/dz (Z layout)
-  cz<n, Real, false>(Dc, w, v);    // d/dx (X layout)
+  c1<n, Real, false, true>(T.Dc, T.eDc, uq, gz);  // d/dz (Z layout)
+  c1<n, Real, false, true>(T.Dc, T.eDc, w, v);    // d/dx (X layout)
   if (wr) putX<n>(t0, a, b, v);
   __syncwarp();
   getZ<n>(t0, a, b, gx);
@@ -175,12 +175,12 @@ __device__ __forceinline__ void l_forward(const Real *S, const Real *Dc, Real *t
 // test functions: out = S^T (val + Dc_x^T fx + Dc_y^T fy + Dc_z^T fz) in all
 // three directions; inputs at the Gauss points and output at the nodes, Z layout
 template <int n, typename Real>
-__device__ __forceinline__ void l_backward(const Real *S, const Real *Dc, Real *t0, Real *t1, bool wr, int a,
-                                           int b, const Real (&val)[n], const Real (&fx)[n],
-                                           const Real (&fy)[n], const Real (&fz)[n], Real (&out)[n])
+__device__ __forceinline__ void l_backward(const Tables<Real> &T, Real *t0, Real *t1, bool wr, int a, int b,
+                                           const Real (&val)[n], const Real (&fx)[n], const Real (&fy)[n],
+                                           const Real (&fz)[n], Real (&out)[n])
 {
   Real A[n], B[n], C[n], w[n];
-  cz<n, Real, true>(Dc, fz, A);
+  c1<n, Real, true, true>(T.Dc, T.eDct, fz, A);
 #pragma unroll
   for (int k = 0; k < n; ++k) A[k] += val[k];  // Z layout
   if (wr) {
@@ -191,8 +191,8 @@ __device__ __forceinline__ void l_backward(const Real *S, const Real *Dc, Real *
   getX<n>(t0, a, b, w);
   getY<n>(t1, a, b, C);
   __syncwarp();
-  cz<n, Real, true>(Dc, w, B);  // x part (X layout)
-  cz<n, Real, true>(Dc, C, w);  // y part (Y layout)
+  c1<n, Real, true, true>(T.Dc, T.eDct, w, B);  // x part (X layout)
+  c1<n, Real, true, true>(T.Dc, T.eDct, C, w);  // y part (Y layout)
   if (wr) {
     putZ<n>(t0, a, b, A);
     putX<n>(t1, a, b, B);
@@ -203,17 +203,17 @@ __device__ __forceinline__ void l_backward(const Real *S, const Real *Dc, Real *
   __syncwarp();
 #pragma unroll
   for (int q = 0; q < n; ++q) C[q] = w[q] + A[q] + B[q];  // sum in Y layout
-  cz<n, Real, true>(S, C, w);  // y: Gauss points -> nodes
+  c1<n, Real, true, false>(T.S, T.eSt, C, w);  // y: Gauss points -> nodes
   if (wr) putY<n>(t0, a, b, w);
   __syncwarp();
   getX<n>(t0, a, b, C);
   __syncwarp();
-  cz<n, Real, true>(S, C, w);  // x
+  c1<n, Real, true, false>(T.S, T.eSt, C, w);  // x
   if (wr) putX<n>(t0, a, b, w);
   __syncwarp();
   getZ<n>(t0, a, b, C);
   __syncwarp();
-  cz<n, Real, true>(S, C, out);  // z
+  c1<n, Real, true, false>(T.S, T.eSt, C, out);  // z
 }
 
 // dynamic shared memory per warp, in units of Real, rounded up to a multiple of
@@ -282,7 +282,8 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   const int s_sub = lane_ok ? sub : 0;
   Real *t0 = tiles + s_sub * n3;
   Real *t1 = tiles + (CPW + s_sub) * n3;
-  const long zs = p.NX * p.NY;
+  // DoF offsets are 32-bit: the launcher checks that the lattice has < 2^32 DoFs
+  const unsigned NXu = (unsigned)p.NX, NYu = (unsigned)p.NY, zs = NXu * NYu;
   const int count = (int)p.ccount;
   const int gstride = gridDim.x * kWarpsPerCTA;
   unsigned phase = 0;
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     const bool act = lane_ok && cidx < count;
     int ix = 0, iy = 0, iz = 0;
     if (act) colour_cell(cidx, p, ix, iy, iz);
-    const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
+    const unsigned g0 = ((unsigned)(iz * P) * NYu + (unsigned)(iy * P + j)) * NXu + (unsigned)(ix * P + i);
 #pragma unroll
     for (int k = 0; k < n; ++k) B[k] = act ? src_v[g0 + k * zs] : Real(0);
   };
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     const bool act = lane_ok && grp * CPW < count && cidx < count;
     int ix = 0, iy = 0, iz = 0;
     if (act) colour_cell(cidx, p, ix, iy, iz);
-    const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
+    const unsigned g0 = ((unsigned)(iz * P) * NYu + (unsigned)(iy * P + j)) * NXu + (unsigned)(ix * P + i);
     if (HANG && act && ix == 0 && i == 0) {
       // hanging DoF (0, j, k): the coarse face's interpolant at the fine node,
       // H along y then along z (subface iy % 2, iz % 2 of coarse face (iy/2, iz/2))
@@ -368,13 +369,20 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     const bool active = lane_ok && cidx < count;
     int ix = 0, iy = 0, iz = 0;
     if (active) colour_cell(cidx, p, ix, iy, iz);
-    const long g0 = ((long)(iz * P) * p.NY + (iy * P + j)) * p.NX + (ix * P + i);
-    const uint4 cm = cmA;
+    const unsigned g0 = ((unsigned)(iz * P) * NYu + (unsigned)(iy * P + j)) * NXu + (unsigned)(ix * P + i);
+    // constrained DoFs of the lane's column (bit k: DoF (i, j, k)); skipped as a
+    // whole when no lane's cell has one (the interior of the mesh)
+    unsigned lmask = 0;
+    if (__any_sync(0xffffffffu, (cmA.x | cmA.y | cmA.z | cmA.w) != 0u)) {
+#pragma unroll
+      for (int k = 0; k < n; ++k) lmask |= (unsigned)mask_bit(cmA, k) << k;
+    }
+    const unsigned rmask = p.masked_read ? lmask : 0u;
     // global DoFs of the lane's column
-    long gk[n];
+    unsigned gk[n];
 #pragma unroll
     for (int k = 0; k < n; ++k)
-      gk[k] = MAPPED ? (active ? (long)p.cmap[(p.cfirst + cidx) * (long)n3 + k * n2 + l] : 0) : g0 + k * zs;
+      gk[k] = MAPPED ? (active ? (unsigned)p.cmap[(p.cfirst + cidx) * (long)n3 + k * n2 + l] : 0u) : g0 + k * zs;
 
     // hanging lane of the fine block: its column is the coarse face's interpolant,
     // its slots are never written (stored 0 by the first cell), its result is staged
@@ -388,10 +396,9 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     for (int k = 0; k < n; ++k) {
       const bool sz = (k == 0 && iz > 0) || (k == P && iz < p.nc[2] - 1);
       const bool first = !MAPPED && !(later_xy || (sz && (iz & 1)));
-      const bool masked = p.masked_write && mask_bit(cm, k);
       first_bits |= (unsigned)first << k;
-      mask_bits |= (unsigned)masked << k;
     }
+    mask_bits = p.masked_write ? lmask : 0u;
     const int nv = MULTI ? p.nvec : 1;
     for (int v = 0; v < nv; ++v) {
     Real *dst_v = (MULTI && v > 0) ? p.mdst[v] : p.dst;
@@ -405,17 +412,17 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     Real u[n];
     if (!MULTI || v == 0) {
 #pragma unroll
-      for (int k = 0; k < n; ++k) u[k] = (p.masked_read && mask_bit(cm, k)) ? Real(0) : A[k];
+      for (int k = 0; k < n; ++k) u[k] = ((rmask >> k) & 1u) ? Real(0) : A[k];
       if (has_next) gather(gnext, A, cmA);
     } else {
       Real B[n];
       gather_col(group, p.msrc[v], B);
 #pragma unroll
-      for (int k = 0; k < n; ++k) u[k] = (p.masked_read && mask_bit(cm, k)) ? Real(0) : B[k];
+      for (int k = 0; k < n; ++k) u[k] = ((rmask >> k) & 1u) ? Real(0) : B[k];
     }
 
     Real uq[n], gx[n], gy[n], gz[n];
-    l_forward<n>(T.S, T.Dc, t0, t1, lane_ok, i, j, u, uq, gx, gy, gz);
+    l_forward<n>(T, t0, t1, lane_ok, i, j, u, uq, gx, gy, gz);
 
     if (GEOM == GEOM_GENERAL && v == 0) {
       mbar_wait_bounded(&bars[warp], phase, err);
@@ -470,7 +477,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     }
 
     Real out[n];
-    l_backward<n>(T.S, T.Dc, t0, t1, lane_ok, i, j, val, fx, fy, fz, out);
+    l_backward<n>(T, t0, t1, lane_ok, i, j, val, fx, fy, fz, out);
 
     if (HANG && __any_sync(0xffffffffu, hl)) {
       // transposed interpolation of the hanging results onto the coarse face:
@@ -504,7 +511,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     if (active) {
 #pragma unroll
       for (int k = 0; k < n; ++k) {
-        const long g = gk[k];
+        const unsigned g = gk[k];
         if (hl) {
           if ((first_bits >> k) & 1) dst_v[g] = Real(0);
         } else if ((first_bits >> k) & 1) {

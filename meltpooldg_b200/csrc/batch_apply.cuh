@@ -161,7 +161,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
 #pragma unroll
   for (int k = 0; k < n; ++k) u[k] = uin[k];
   Real uq[n], gx[n], gy[n], gz[n];
-  l_forward<n>(T.S, T.Dc, t0, t1, q.lane_ok, i, j, u, uq, gx, gy, gz);
+  l_forward<n>(T, t0, t1, q.lane_ok, i, j, u, uq, gx, gy, gz);
   Real val[n], fx[n], fy[n], fz[n];
   const Real hvol = (Real)W.hvol, ih = (Real)W.ih, ih2 = (Real)W.ih2;
   const Real c_mass = (Real)W.c_mass, c_vel = (Real)W.c_vel, c_diff = (Real)W.c_diff;
@@ -185,7 +185,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
     fz[k] = kd * gz[k];
   }
   Real out[n];
-  l_backward<n>(T.S, T.Dc, t0, t1, q.lane_ok, i, j, val, fx, fy, fz, out);
+  l_backward<n>(T, t0, t1, q.lane_ok, i, j, val, fx, fy, fz, out);
   if (q.act) {
 #pragma unroll
     for (int k = 0; k < n; ++k) {
