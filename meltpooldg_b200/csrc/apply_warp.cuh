@@ -277,9 +277,14 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   Real *vstage = wsm + (GEOM == GEOM_GENERAL ? CPW * MS : 0);
   Real *tiles = wsm + (GEOM == GEOM_GENERAL ? CPW * (MS + (gvel ? VS : 0)) : 0);
 
-  const int sub = lane / n2, l = lane % n2, i = l % n, j = l / n;
-  const bool lane_ok = sub < CPW;
-  const int s_sub = lane_ok ? sub : 0;
+  // lanes past the last cell (Q2: 5, Q4: 7) copy the position of the lane
+  // 32 - CPW n^2 below them: their unused shared-memory loads then read the
+  // same addresses as active lanes of their own half-warp (a broadcast), which
+  // keeps 64-bit loads at two wavefronts
+  const bool lane_ok = lane < CPW * n2;
+  const int mlane = lane_ok ? lane : lane - (32 - CPW * n2);
+  const int sub = mlane / n2, l = mlane % n2, i = l % n, j = l / n;
+  const int s_sub = sub;
   Real *t0 = tiles + s_sub * n3;
   Real *t1 = tiles + (CPW + s_sub) * n3;
   // DoF offsets are 32-bit: the launcher checks that the lattice has < 2^32 DoFs
@@ -301,22 +306,14 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   // nothing here consumes a load, so the loads stay in flight while the
   // current group is computed
   const bool use_mask = p.cell_mask != nullptr && (p.masked_read || p.masked_write);
-  // column of vector src_v for the lane's cell in group grp (multi-vector apply)
-  auto gather_col = [&](int grp, const Real *src_v, Real (&B)[n]) {
-    const int cidx = grp * CPW + sub;
-    const bool act = lane_ok && cidx < count;
-    int ix = 0, iy = 0, iz = 0;
-    if (act) colour_cell(cidx, p, ix, iy, iz);
-    const unsigned g0 = ((unsigned)(iz * P) * NYu + (unsigned)(iy * P + j)) * NXu + (unsigned)(ix * P + i);
-#pragma unroll
-    for (int k = 0; k < n; ++k) B[k] = act ? src_v[g0 + k * zs] : Real(0);
-  };
-  auto gather = [&](int grp, Real (&A)[n], uint4 &cm) {
+  // the lane's cell (ix, iy, iz) in group grp and the lattice offset g0 of its
+  // DoF (i, j, 0), carried from the gather to the group's compute
+  auto gather = [&](int grp, Real (&A)[n], uint4 &cm, int &ix, int &iy, int &iz, unsigned &g0) {
     const int cidx = grp * CPW + sub;
     const bool act = lane_ok && grp * CPW < count && cidx < count;
-    int ix = 0, iy = 0, iz = 0;
+    ix = 0, iy = 0, iz = 0;
     if (act) colour_cell(cidx, p, ix, iy, iz);
-    const unsigned g0 = ((unsigned)(iz * P) * NYu + (unsigned)(iy * P + j)) * NXu + (unsigned)(ix * P + i);
+    g0 = ((unsigned)(iz * P) * NYu + (unsigned)(iy * P + j)) * NXu + (unsigned)(ix * P + i);
     if (HANG && act && ix == 0 && i == 0) {
       // hanging DoF (0, j, k): the coarse face's interpolant at the fine node,
       // H along y then along z (subface iy % 2, iz % 2 of coarse face (iy/2, iz/2))
@@ -360,20 +357,22 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   if (GEOM == GEOM_GENERAL && lane == 0 && group * CPW < count) issue_stage(group);
   Real A[n];
   uint4 cmA;
-  gather(group, A, cmA);
+  int nix, niy, niz;
+  unsigned ng0;
+  gather(group, A, cmA, nix, niy, niz, ng0);
 
   for (; group * CPW < count; group += gstride) {
     const int gnext = group + gstride;
     const bool has_next = gnext * CPW < count;
     const int cidx = group * CPW + sub;
     const bool active = lane_ok && cidx < count;
-    int ix = 0, iy = 0, iz = 0;
-    if (active) colour_cell(cidx, p, ix, iy, iz);
-    const unsigned g0 = ((unsigned)(iz * P) * NYu + (unsigned)(iy * P + j)) * NXu + (unsigned)(ix * P + i);
+    const int ix = nix, iy = niy, iz = niz;
+    const unsigned g0 = ng0;
     // constrained DoFs of the lane's column (bit k: DoF (i, j, k)); skipped as a
     // whole when no lane's cell has one (the interior of the mesh)
     unsigned lmask = 0;
-    if (__any_sync(0xffffffffu, (cmA.x | cmA.y | cmA.z | cmA.w) != 0u)) {
+    const bool any_mask = __any_sync(0xffffffffu, (cmA.x | cmA.y | cmA.z | cmA.w) != 0u);
+    if (any_mask) {
 #pragma unroll
       for (int k = 0; k < n; ++k) lmask |= (unsigned)mask_bit(cmA, k) << k;
     }
@@ -412,13 +411,16 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     Real u[n];
     if (!MULTI || v == 0) {
 #pragma unroll
-      for (int k = 0; k < n; ++k) u[k] = ((rmask >> k) & 1u) ? Real(0) : A[k];
-      if (has_next) gather(gnext, A, cmA);
+      for (int k = 0; k < n; ++k) u[k] = A[k];
+      if (has_next) gather(gnext, A, cmA, nix, niy, niz, ng0);
     } else {
-      Real B[n];
-      gather_col(group, p.msrc[v], B);
+      const Real *src_v = p.msrc[v];
 #pragma unroll
-      for (int k = 0; k < n; ++k) u[k] = ((rmask >> k) & 1u) ? Real(0) : B[k];
+      for (int k = 0; k < n; ++k) u[k] = active ? src_v[g0 + k * zs] : Real(0);
+    }
+    if (any_mask) {
+#pragma unroll
+      for (int k = 0; k < n; ++k) u[k] = ((rmask >> k) & 1u) ? Real(0) : u[k];
     }
 
     Real uq[n], gx[n], gy[n], gz[n];
@@ -508,7 +510,13 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
       __syncwarp();
     }
 
-    if (active) {
+    if (!HANG && !any_mask) {
+      // no constrained DoF in the warp's cells: dpre is 0 where the cell stores first
+      if (active) {
+#pragma unroll
+        for (int k = 0; k < n; ++k) dst_v[gk[k]] = dpre[k] + out[k];
+      }
+    } else if (active) {
 #pragma unroll
       for (int k = 0; k < n; ++k) {
         const unsigned g = gk[k];

@@ -84,11 +84,13 @@ __device__ __forceinline__ BatchLanePos<P> batch_pos(int colour, int lg, const W
 {
   constexpr int n = P + 1, n2 = n * n, CPW = WCfg<n>::cpw;
   BatchLanePos<P> q;
-  const int sub = lane / n2, l = lane % n2;
+  // idle lanes copy an active lane of their own half-warp (see warp_apply_kernel)
+  q.lane_ok = lane < CPW * n2;
+  const int mlane = q.lane_ok ? lane : lane - (32 - CPW * n2);
+  const int sub = mlane / n2, l = mlane % n2;
   q.i = l % n;
   q.j = l / n;
-  q.lane_ok = sub < CPW;
-  q.s_sub = q.lane_ok ? sub : 0;
+  q.s_sub = sub;
   const int cidx = lg * CPW + sub;
   q.act = q.lane_ok && cidx < W.count;
   q.ix = q.iy = q.iz = 0;

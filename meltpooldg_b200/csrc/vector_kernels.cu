@@ -41,13 +41,31 @@ __device__ __forceinline__ double block_sum(double v)
   return s;
 }
 
+// Grid-stride loops take kU elements per thread per pass (i, i + stride, ...,
+// loaded before any is used), so that each thread keeps kU loads of every
+// operand in flight; the per-thread order of a sum is the plain grid-stride
+// order, so reductions do not depend on kU.
+constexpr int kU = 4;
+
 template <typename A, typename B>
 __global__ void __launch_bounds__(kRedThreads) dot_partial_kernel(const A *a, const B *b, long n,
                                                                   double *partial)
 {
   double s = 0.0;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    s += (double)a[i] * (double)b[i];
+  const long stride = (long)gridDim.x * blockDim.x;
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + (kU - 1) * stride < n; i += kU * stride) {
+    A va[kU];
+    B vb[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      va[u] = a[i + u * stride];
+      vb[u] = b[i + u * stride];
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) s += (double)va[u] * (double)vb[u];
+  }
+  for (; i < n; i += stride) s += (double)a[i] * (double)b[i];
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
@@ -137,8 +155,19 @@ __global__ void combine_kernel(const R *V, long n, int m, const double *y, R *x)
 template <typename R>
 __global__ void axpby_kernel(long n, double a, const R *x, double b, R *y)
 {
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    y[i] = (R)(a * (double)x[i] + b * (double)y[i]);
+  const long stride = (long)gridDim.x * blockDim.x;
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + (kU - 1) * stride < n; i += kU * stride) {
+    R vx[kU], vy[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      vx[u] = x[i + u * stride];
+      vy[u] = y[i + u * stride];
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) y[i + u * stride] = (R)(a * (double)vx[u] + b * (double)vy[u]);
+  }
+  for (; i < n; i += stride) y[i] = (R)(a * (double)x[i] + b * (double)y[i]);
 }
 
 // y = b - y
@@ -180,17 +209,35 @@ __global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long n, const do
   const double alpha = s[kRZ] / s[kPAP];
   const double xa = alpha * xscale;
   double rr = 0.0, rz = 0.0;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    x[i] = (RX)((double)x[i] + xa * (double)p[i]);
-    const R ri = (R)((double)r[i] - alpha * (double)Ap[i]);
+  auto one = [&](long i, RX xi, R pi, R r0, R api, R di) {
+    x[i] = (RX)((double)xi + xa * (double)pi);
+    const R ri = (R)((double)r0 - alpha * (double)api);
     r[i] = ri;
     rr += (double)ri * (double)ri;
     if (invd) {
-      const R zi = invd[i] * ri;
+      const R zi = di * ri;
       z[i] = zi;
       rz += (double)ri * (double)zi;
     }
+  };
+  const long stride = (long)gridDim.x * blockDim.x;
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + (kU - 1) * stride < n; i += kU * stride) {
+    RX vx[kU];
+    R vp[kU], vr[kU], va[kU], vd[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const long j = i + u * stride;
+      vx[u] = x[j];
+      vp[u] = p[j];
+      vr[u] = r[j];
+      va[u] = Ap[j];
+      vd[u] = invd ? invd[j] : R(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) one(i + u * stride, vx[u], vp[u], vr[u], va[u], vd[u]);
   }
+  for (; i < n; i += stride) one(i, x[i], p[i], r[i], Ap[i], invd ? invd[i] : R(0));
   rr = block_sum(rr);
   if (threadIdx.x == 0) partial[blockIdx.x] = rr;
   if (invd) {
@@ -204,8 +251,19 @@ template <typename R>
 __global__ void cg_direction_kernel(long n, double *s, R *p, const R *z)
 {
   const double beta = s[kRZNEW] / s[kRZ];
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    p[i] = (R)((double)z[i] + beta * (double)p[i]);
+  const long stride = (long)gridDim.x * blockDim.x;
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + (kU - 1) * stride < n; i += kU * stride) {
+    R vz[kU], vp[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      vz[u] = z[i + u * stride];
+      vp[u] = p[i + u * stride];
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) p[i + u * stride] = (R)((double)vz[u] + beta * (double)vp[u]);
+  }
+  for (; i < n; i += stride) p[i] = (R)((double)z[i] + beta * (double)p[i]);
 }
 
 __global__ void shift_scalar_kernel(double *s)
@@ -217,7 +275,23 @@ __global__ void shift_scalar_kernel(double *s)
 template <typename R>
 __global__ void cheb_start_kernel(long n, double inv_theta, const R *invd, const R *r, R *d, R *z)
 {
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + (kU - 1) * stride < n; i += kU * stride) {
+    R vi[kU], vr[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      vi[u] = invd[i + u * stride];
+      vr[u] = r[i + u * stride];
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const R v = (R)(inv_theta * (double)(vi[u] * vr[u]));
+      d[i + u * stride] = v;
+      z[i + u * stride] = v;
+    }
+  }
+  for (; i < n; i += stride) {
     const R v = (R)(inv_theta * (double)(invd[i] * r[i]));
     d[i] = v;
     z[i] = v;
@@ -229,7 +303,27 @@ template <typename R>
 __global__ void cheb_step_kernel(long n, double c1, double c2, const R *invd, const R *r, const R *t,
                                  R *d, R *z)
 {
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + (kU - 1) * stride < n; i += kU * stride) {
+    R vi[kU], vr[kU], vt[kU], vd[kU], vz[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const long j = i + u * stride;
+      vi[u] = invd[j];
+      vr[u] = r[j];
+      vt[u] = t[j];
+      vd[u] = d[j];
+      vz[u] = z[j];
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const R v = (R)(c1 * (double)vd[u] + c2 * (double)(vi[u] * (vr[u] - vt[u])));
+      d[i + u * stride] = v;
+      z[i + u * stride] = vz[u] + v;
+    }
+  }
+  for (; i < n; i += stride) {
     const R v = (R)(c1 * (double)d[i] + c2 * (double)(invd[i] * (r[i] - t[i])));
     d[i] = v;
     z[i] += v;
@@ -242,6 +336,15 @@ namespace {
 unsigned vgrid(long n)
 {
   long g = (n + 255) / 256;
+  if (g > 148L * 16) g = 148L * 16;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+// blocks of 256 threads for an unrolled elementwise kernel: one pass of kU
+// elements per thread where n allows, at most 16 blocks per SM
+unsigned vgrid4(long n)
+{
+  long g = (n + 256 * kU - 1) / (256 * kU);
   if (g > 148L * 16) g = 148L * 16;
   if (g < 1) g = 1;
   return (unsigned)g;
@@ -304,7 +407,7 @@ template void dev_combine<float>(const float *, long, int, const double *, float
 template <typename R>
 void dev_axpby(long n, double a, const R *x, double b, R *y, cudaStream_t s)
 {
-  axpby_kernel<R><<<vgrid(n), 256, 0, s>>>(n, a, x, b, y);
+  axpby_kernel<R><<<vgrid4(n), 256, 0, s>>>(n, a, x, b, y);
   MPDG_LAUNCHED();
 }
 template void dev_axpby<double>(long, double, const double *, double, double *, cudaStream_t);
@@ -371,7 +474,7 @@ template void dev_cg_update<float, double>(long, double *, double *, float *, co
 template <typename R>
 void dev_cg_direction(long n, double *s, R *p, const R *z, cudaStream_t st)
 {
-  cg_direction_kernel<R><<<vgrid(n), 256, 0, st>>>(n, s, p, z);
+  cg_direction_kernel<R><<<vgrid4(n), 256, 0, st>>>(n, s, p, z);
   MPDG_LAUNCHED();
   shift_scalar_kernel<<<1, 1, 0, st>>>(s);
   MPDG_LAUNCHED();
@@ -382,7 +485,7 @@ template void dev_cg_direction<float>(long, double *, float *, const float *, cu
 template <typename R>
 void dev_cheb_start(long n, double inv_theta, const R *invd, const R *r, R *d, R *z, cudaStream_t s)
 {
-  cheb_start_kernel<R><<<vgrid(n), 256, 0, s>>>(n, inv_theta, invd, r, d, z);
+  cheb_start_kernel<R><<<vgrid4(n), 256, 0, s>>>(n, inv_theta, invd, r, d, z);
   MPDG_LAUNCHED();
 }
 template void dev_cheb_start<double>(long, double, const double *, const double *, double *,
@@ -394,7 +497,7 @@ template <typename R>
 void dev_cheb_step(long n, double c1, double c2, const R *invd, const R *r, const R *t, R *d, R *z,
                    cudaStream_t s)
 {
-  cheb_step_kernel<R><<<vgrid(n), 256, 0, s>>>(n, c1, c2, invd, r, t, d, z);
+  cheb_step_kernel<R><<<vgrid4(n), 256, 0, s>>>(n, c1, c2, invd, r, t, d, z);
   MPDG_LAUNCHED();
 }
 template void dev_cheb_step<double>(long, double, double, const double *, const double *,
@@ -405,14 +508,22 @@ template void dev_cheb_step<float>(long, double, double, const float *, const fl
 template <typename R>
 __global__ void copy_kernel(long n, const R *x, R *y)
 {
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    y[i] = x[i];
+  const long stride = (long)gridDim.x * blockDim.x;
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + (kU - 1) * stride < n; i += kU * stride) {
+    R v[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) v[u] = x[i + u * stride];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) y[i + u * stride] = v[u];
+  }
+  for (; i < n; i += stride) y[i] = x[i];
 }
 
 template <typename R>
 void dev_copy(long n, const R *x, R *y, cudaStream_t s)
 {
-  copy_kernel<R><<<vgrid(n), 256, 0, s>>>(n, x, y);
+  copy_kernel<R><<<vgrid4(n), 256, 0, s>>>(n, x, y);
   MPDG_LAUNCHED();
 }
 template void dev_copy<double>(long, const double *, double *, cudaStream_t);
