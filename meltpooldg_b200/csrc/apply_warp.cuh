@@ -98,42 +98,49 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t *bar, unsigned phase,
 // cell's shared tile t[k n^2 + j n + i] with n stores and n loads per lane.
 // The former scheme read n^2 tile values per lane for each x or y pass.
 
-template <int n, typename Real>
+template <int n, int S2 = n * n, typename Real>
 __device__ __forceinline__ void putZ(Real *t, int a, int b, const Real (&v)[n])
 {
 #pragma unroll
-  for (int k = 0; k < n; ++k) t[k * n * n + b * n + a] = v[k];
+  for (int k = 0; k < n; ++k) t[k * S2 + b * n + a] = v[k];
 }
-template <int n, typename Real>
+template <int n, int S2 = n * n, typename Real>
 __device__ __forceinline__ void getZ(const Real *t, int a, int b, Real (&v)[n])
 {
 #pragma unroll
-  for (int k = 0; k < n; ++k) v[k] = t[k * n * n + b * n + a];
+  for (int k = 0; k < n; ++k) v[k] = t[k * S2 + b * n + a];
 }
-template <int n, typename Real>
+template <int n, int S2 = n * n, typename Real>
 __device__ __forceinline__ void putX(Real *t, int a, int b, const Real (&v)[n])
 {
 #pragma unroll
-  for (int i = 0; i < n; ++i) t[b * n * n + a * n + i] = v[i];
+  for (int i = 0; i < n; ++i) t[b * S2 + a * n + i] = v[i];
 }
-template <int n, typename Real>
+template <int n, int S2 = n * n, typename Real>
 __device__ __forceinline__ void getX(const Real *t, int a, int b, Real (&v)[n])
 {
 #pragma unroll
-  for (int i = 0; i < n; ++i) v[i] = t[b * n * n + a * n + i];
+  for (int i = 0; i < n; ++i) v[i] = t[b * S2 + a * n + i];
 }
-template <int n, typename Real>
+template <int n, int S2 = n * n, typename Real>
 __device__ __forceinline__ void putY(Real *t, int a, int b, const Real (&v)[n])
 {
 #pragma unroll
-  for (int j = 0; j < n; ++j) t[b * n * n + j * n + a] = v[j];
+  for (int j = 0; j < n; ++j) t[b * S2 + j * n + a] = v[j];
 }
-template <int n, typename Real>
+template <int n, int S2 = n * n, typename Real>
 __device__ __forceinline__ void getY(const Real *t, int a, int b, Real (&v)[n])
 {
 #pragma unroll
-  for (int j = 0; j < n; ++j) v[j] = t[b * n * n + j * n + a];
+  for (int j = 0; j < n; ++j) v[j] = t[b * S2 + j * n + a];
 }
+
+// z-plane stride of the second tile t1.  t1 is only accessed in the Z and Y
+// layouts; for Q4 in FP32 a plane stride of 37 makes both conflict-free (the
+// 25-stride of t0 costs Y accesses a second wavefront).  FP64 keeps 25: its
+// shared-memory traffic was measured slower with the wider tile.
+template <int n, typename Real>
+constexpr int t1s2() { return (n == 5 && sizeof(Real) == 4) ? 37 : n * n; }
 
 // nodal values u (Z layout) -> values uq and collocation gradients gx, gy, gz
 // at the Gauss points, all in Z layout.  S, Dc: tables in constant memory.
@@ -157,12 +164,12 @@ __device__ __forceinline__ void l_forward(const Tables<Real> &T, Real *t0, Real 
   c1<n, Real, false, true>(T.Dc, T.eDc, v, w);   // d/dy (Y layout)
   if (wr) {
     putY<n>(t0, a, b, v);
-    putY<n>(t1, a, b, w);
+    putY<n, t1s2<n, Real>()>(t1, a, b, w);
   }
   __syncwarp();
   getZ<n>(t0, a, b, uq);
   getX<n>(t0, a, b, w);
-  getZ<n>(t1, a, b, gy);
+  getZ<n, t1s2<n, Real>()>(t1, a, b, gy);
   __syncwarp();
   c1<n, Real, false, true>(T.Dc, T.eDc, uq, gz);  // d/dz (Z layout)
   c1<n, Real, false, true>(T.Dc, T.eDc, w, v);    // d/dx (X layout)
@@ -185,21 +192,21 @@ __device__ __forceinline__ void l_backward(const Tables<Real> &T, Real *t0, Real
   for (int k = 0; k < n; ++k) A[k] += val[k];  // Z layout
   if (wr) {
     putZ<n>(t0, a, b, fx);
-    putZ<n>(t1, a, b, fy);
+    putZ<n, t1s2<n, Real>()>(t1, a, b, fy);
   }
   __syncwarp();
   getX<n>(t0, a, b, w);
-  getY<n>(t1, a, b, C);
+  getY<n, t1s2<n, Real>()>(t1, a, b, C);
   __syncwarp();
   c1<n, Real, true, true>(T.Dc, T.eDct, w, B);  // x part (X layout)
   c1<n, Real, true, true>(T.Dc, T.eDct, C, w);  // y part (Y layout)
   if (wr) {
-    putZ<n>(t0, a, b, A);
-    putX<n>(t1, a, b, B);
+    putZ<n, t1s2<n, Real>()>(t1, a, b, A);
+    putX<n>(t0, a, b, B);
   }
   __syncwarp();
-  getY<n>(t0, a, b, A);
-  getY<n>(t1, a, b, B);
+  getY<n, t1s2<n, Real>()>(t1, a, b, A);
+  getY<n>(t0, a, b, B);
   __syncwarp();
 #pragma unroll
   for (int q = 0; q < n; ++q) C[q] = w[q] + A[q] + B[q];  // sum in Y layout
@@ -224,7 +231,7 @@ __host__ __device__ constexpr int warp_smem_elems(bool vel)
 {
   constexpr int n = P + 1, n3 = n * n * n, CPW = WCfg<n>::cpw;
   return (((GEOM == GEOM_GENERAL ? CPW * (metric_stride(n) + (vel ? velb_stride(n) : 0)) : 0) +
-           2 * CPW * n3) + 7) / 8 * 8;
+           2 * CPW * n3 + (t1s2<n, Real>() - n * n) * n) + 7) / 8 * 8;
 }
 constexpr int kSmemAlign = 128;  // the dynamic shared-memory base is aligned by hand
 
@@ -308,9 +315,13 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   const bool use_mask = p.cell_mask != nullptr && (p.masked_read || p.masked_write);
   // the lane's cell (ix, iy, iz) in group grp and the lattice offset g0 of its
   // DoF (i, j, 0), carried from the gather to the group's compute
+  // idle lanes gather their mirror lane's column too: they then compute the
+  // same values and their shared-memory stores repeat the mirror's, so no
+  // store needs a lane predicate (only the global scatter is restricted to
+  // lane_ok lanes)
   auto gather = [&](int grp, Real (&A)[n], uint4 &cm, int &ix, int &iy, int &iz, unsigned &g0) {
     const int cidx = grp * CPW + sub;
-    const bool act = lane_ok && grp * CPW < count && cidx < count;
+    const bool act = grp * CPW < count && cidx < count;
     ix = 0, iy = 0, iz = 0;
     if (act) colour_cell(cidx, p, ix, iy, iz);
     g0 = ((unsigned)(iz * P) * NYu + (unsigned)(iy * P + j)) * NXu + (unsigned)(ix * P + i);
@@ -416,7 +427,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     } else {
       const Real *src_v = p.msrc[v];
 #pragma unroll
-      for (int k = 0; k < n; ++k) u[k] = active ? src_v[g0 + k * zs] : Real(0);
+      for (int k = 0; k < n; ++k) u[k] = (cidx < count) ? src_v[g0 + k * zs] : Real(0);
     }
     if (any_mask) {
 #pragma unroll
@@ -424,7 +435,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     }
 
     Real uq[n], gx[n], gy[n], gz[n];
-    l_forward<n>(T, t0, t1, lane_ok, i, j, u, uq, gx, gy, gz);
+    l_forward<n>(T, t0, t1, true, i, j, u, uq, gx, gy, gz);
 
     if (GEOM == GEOM_GENERAL && v == 0) {
       mbar_wait_bounded(&bars[warp], phase, err);
@@ -479,7 +490,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     }
 
     Real out[n];
-    l_backward<n>(T, t0, t1, lane_ok, i, j, val, fx, fy, fz, out);
+    l_backward<n>(T, t0, t1, true, i, j, val, fx, fy, fz, out);
 
     if (HANG && __any_sync(0xffffffffu, hl)) {
       // transposed interpolation of the hanging results onto the coarse face:

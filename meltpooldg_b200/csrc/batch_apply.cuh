@@ -12,7 +12,7 @@
 // warp_apply_kernel.
 #pragma once
 
-constexpr int kBatchTileElems = 256;   // max over P of 2 * cells_per_warp * (P+1)^3
+constexpr int kBatchTileElems = 320;   // max over P of the two tiles of a warp (t1s2 widens Q4 FP32)
 
 __device__ __forceinline__ int batch_find(const int *__restrict__ prefix, int n, int g)
 {
@@ -74,7 +74,7 @@ __device__ __forceinline__ void load_warp_slot(WarpSlot<Real> &W, int colour, in
 // cell of colour-local group lg and the lane's position in it
 template <int P>
 struct BatchLanePos {
-  bool lane_ok, act, bxy;
+  bool lane_ok, act, gact, bxy;  // gact: gathers (idle lanes copy their mirror lane)
   int i, j, s_sub, ix, iy, iz;
   long NX, g0;
 };
@@ -92,9 +92,10 @@ __device__ __forceinline__ BatchLanePos<P> batch_pos(int colour, int lg, const W
   q.j = l / n;
   q.s_sub = sub;
   const int cidx = lg * CPW + sub;
-  q.act = q.lane_ok && cidx < W.count;
+  q.gact = cidx < W.count;
+  q.act = q.lane_ok && q.gact;
   q.ix = q.iy = q.iz = 0;
-  if (q.act) {
+  if (q.gact) {
     const unsigned x = (unsigned)cidx;
     const unsigned q0 = (unsigned)(((unsigned long long)x * W.m0) >> 40);
     const unsigned q01 = (unsigned)(((unsigned long long)x * W.m01) >> 40);
@@ -124,7 +125,7 @@ __device__ __forceinline__ void batch_gather(int colour, int lg, const WarpSlot<
   for (int k = 0; k < n; ++k) {
     const int Z = q.iz * P + k;
     const bool masked = q.bxy || (dir && (Z == 0 || Z == q.NX - 1));
-    u[k] = (q.act && !masked) ? src[q.g0 + k * zs] : Real(0);
+    u[k] = (q.gact && !masked) ? src[q.g0 + k * zs] : Real(0);
   }
 }
 
@@ -133,7 +134,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
                                            const Real (&uin)[kMaxN], Real *tiles, int lane)
 {
   constexpr int n = P + 1, n3 = n * n * n, CPW = WCfg<n>::cpw;
-  static_assert(2 * CPW * n3 <= kBatchTileElems, "tile area");
+  static_assert(2 * CPW * n3 + (t1s2<n, Real>() - n * n) * n <= kBatchTileElems, "tile area");
   const Tables<Real> &T = tab<Real>(P);
   const BatchLanePos<P> q = batch_pos<P>(colour, local_group, W, lane);
   const int i = q.i, j = q.j, ix = q.ix, iy = q.iy, iz = q.iz;
@@ -163,7 +164,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
 #pragma unroll
   for (int k = 0; k < n; ++k) u[k] = uin[k];
   Real uq[n], gx[n], gy[n], gz[n];
-  l_forward<n>(T, t0, t1, q.lane_ok, i, j, u, uq, gx, gy, gz);
+  l_forward<n>(T, t0, t1, true, i, j, u, uq, gx, gy, gz);
   Real val[n], fx[n], fy[n], fz[n];
   const Real hvol = (Real)W.hvol, ih = (Real)W.ih, ih2 = (Real)W.ih2;
   const Real c_mass = (Real)W.c_mass, c_vel = (Real)W.c_vel, c_diff = (Real)W.c_diff;
@@ -187,7 +188,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
     fz[k] = kd * gz[k];
   }
   Real out[n];
-  l_backward<n>(T, t0, t1, q.lane_ok, i, j, val, fx, fy, fz, out);
+  l_backward<n>(T, t0, t1, true, i, j, val, fx, fy, fz, out);
   if (q.act) {
 #pragma unroll
     for (int k = 0; k < n; ++k) {
