@@ -95,40 +95,54 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t *bar, unsigned phase,
 //   Y: lane (a, b) = (i, k) holds v[j]
 // Every 1D contraction runs in registers on the owned line (tables in
 // constant memory, compile-time indices); the layout changes go through the
-// cell's shared tile t[k n^2 + j n + i] with n stores and n loads per lane.
+// cell's shared tile t[k S2 + j n + i] with n stores and n loads per lane.
 // The former scheme read n^2 tile values per lane for each x or y pass.
+//
+// Tile layout: z-plane stride S2 and offset SC between the cells of a warp,
+// the layouts with the fewest shared-memory wavefronts over the Z, X and Y
+// accesses of a search over all linear layouts (64-bit accesses in two
+// half-warps, 32-bit in one pass; per set of 3n accesses):
+//   Q2 (3 cells per warp): S2 = 34, SC = 9:   64-bit 27 -> 24, 32-bit 15 -> 12
+//   other degrees: the plain layout S2 = n^2, SC = n^3
+template <int n>
+__host__ __device__ constexpr int tile_s2() { return n == 3 ? 34 : n * n; }
+template <int n>
+__host__ __device__ constexpr int tile_sc() { return n == 3 ? 9 : n * n * n; }
+// elements of one tile of a warp with plane stride S2
+template <int n, int S2>
+__host__ __device__ constexpr int tile_elems() { return (WCfg<n>::cpw - 1) * tile_sc<n>() + (n - 1) * S2 + n * n; }
 
-template <int n, int S2 = n * n, typename Real>
+template <int n, int S2 = tile_s2<n>(), typename Real>
 __device__ __forceinline__ void putZ(Real *t, int a, int b, const Real (&v)[n])
 {
 #pragma unroll
   for (int k = 0; k < n; ++k) t[k * S2 + b * n + a] = v[k];
 }
-template <int n, int S2 = n * n, typename Real>
+template <int n, int S2 = tile_s2<n>(), typename Real>
 __device__ __forceinline__ void getZ(const Real *t, int a, int b, Real (&v)[n])
 {
 #pragma unroll
   for (int k = 0; k < n; ++k) v[k] = t[k * S2 + b * n + a];
 }
-template <int n, int S2 = n * n, typename Real>
+template <int n, int S2 = tile_s2<n>(), typename Real>
 __device__ __forceinline__ void putX(Real *t, int a, int b, const Real (&v)[n])
 {
 #pragma unroll
   for (int i = 0; i < n; ++i) t[b * S2 + a * n + i] = v[i];
 }
-template <int n, int S2 = n * n, typename Real>
+template <int n, int S2 = tile_s2<n>(), typename Real>
 __device__ __forceinline__ void getX(const Real *t, int a, int b, Real (&v)[n])
 {
 #pragma unroll
   for (int i = 0; i < n; ++i) v[i] = t[b * S2 + a * n + i];
 }
-template <int n, int S2 = n * n, typename Real>
+template <int n, int S2 = tile_s2<n>(), typename Real>
 __device__ __forceinline__ void putY(Real *t, int a, int b, const Real (&v)[n])
 {
 #pragma unroll
   for (int j = 0; j < n; ++j) t[b * S2 + j * n + a] = v[j];
 }
-template <int n, int S2 = n * n, typename Real>
+template <int n, int S2 = tile_s2<n>(), typename Real>
 __device__ __forceinline__ void getY(const Real *t, int a, int b, Real (&v)[n])
 {
 #pragma unroll
@@ -140,7 +154,13 @@ __device__ __forceinline__ void getY(const Real *t, int a, int b, Real (&v)[n])
 // 25-stride of t0 costs Y accesses a second wavefront).  FP64 keeps 25: its
 // shared-memory traffic was measured slower with the wider tile.
 template <int n, typename Real>
-constexpr int t1s2() { return (n == 5 && sizeof(Real) == 4) ? 37 : n * n; }
+__host__ __device__ constexpr int t1s2() { return (n == 5 && sizeof(Real) == 4) ? 37 : tile_s2<n>(); }
+// both tiles of a warp
+template <int n, typename Real>
+__host__ __device__ constexpr int warp_tile_elems()
+{
+  return tile_elems<n, tile_s2<n>()>() + tile_elems<n, t1s2<n, Real>()>();
+}
 
 // nodal values u (Z layout) -> values uq and collocation gradients gx, gy, gz
 // at the Gauss points, all in Z layout.  S, Dc: tables in constant memory.
@@ -229,9 +249,9 @@ __device__ __forceinline__ void l_backward(const Tables<Real> &T, Real *t0, Real
 template <int P, typename Real, int GEOM>
 __host__ __device__ constexpr int warp_smem_elems(bool vel)
 {
-  constexpr int n = P + 1, n3 = n * n * n, CPW = WCfg<n>::cpw;
+  constexpr int n = P + 1, CPW = WCfg<n>::cpw;
   return (((GEOM == GEOM_GENERAL ? CPW * (metric_stride(n) + (vel ? velb_stride(n) : 0)) : 0) +
-           2 * CPW * n3 + (t1s2<n, Real>() - n * n) * n) + 7) / 8 * 8;
+           warp_tile_elems<n, Real>()) + 7) / 8 * 8;
 }
 constexpr int kSmemAlign = 128;  // the dynamic shared-memory base is aligned by hand
 
@@ -292,8 +312,8 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   const int mlane = lane_ok ? lane : lane - (32 - CPW * n2);
   const int sub = mlane / n2, l = mlane % n2, i = l % n, j = l / n;
   const int s_sub = sub;
-  Real *t0 = tiles + s_sub * n3;
-  Real *t1 = tiles + (CPW + s_sub) * n3;
+  Real *t0 = tiles + s_sub * tile_sc<n>();
+  Real *t1 = tiles + tile_elems<n, tile_s2<n>()>() + s_sub * tile_sc<n>();
   // DoF offsets are 32-bit: the launcher checks that the lattice has < 2^32 DoFs
   const unsigned NXu = (unsigned)p.NX, NYu = (unsigned)p.NY, zs = NXu * NYu;
   const int count = (int)p.ccount;

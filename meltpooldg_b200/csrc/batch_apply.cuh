@@ -12,7 +12,7 @@
 // warp_apply_kernel.
 #pragma once
 
-constexpr int kBatchTileElems = 320;   // max over P of the two tiles of a warp (t1s2 widens Q4 FP32)
+constexpr int kBatchTileElems = 320;   // at least the largest warp_tile_elems over P
 
 __device__ __forceinline__ int batch_find(const int *__restrict__ prefix, int n, int g)
 {
@@ -133,13 +133,13 @@ template <int P, typename Real>
 __device__ __forceinline__ void batch_cell(int colour, int local_group, const WarpSlot<Real> &W,
                                            const Real (&uin)[kMaxN], Real *tiles, int lane)
 {
-  constexpr int n = P + 1, n3 = n * n * n, CPW = WCfg<n>::cpw;
-  static_assert(2 * CPW * n3 + (t1s2<n, Real>() - n * n) * n <= kBatchTileElems, "tile area");
+  constexpr int n = P + 1;
+  static_assert(warp_tile_elems<n, Real>() <= kBatchTileElems, "tile area");
   const Tables<Real> &T = tab<Real>(P);
   const BatchLanePos<P> q = batch_pos<P>(colour, local_group, W, lane);
   const int i = q.i, j = q.j, ix = q.ix, iy = q.iy, iz = q.iz;
-  Real *t0 = tiles + q.s_sub * n3;
-  Real *t1 = tiles + (CPW + q.s_sub) * n3;
+  Real *t0 = tiles + q.s_sub * tile_sc<n>();
+  Real *t1 = tiles + tile_elems<n, tile_s2<n>()>() + q.s_sub * tile_sc<n>();
   const long NX = q.NX, zs = NX * NX, g0 = q.g0;
   Real *dst = W.dst;
   const bool dir = W.dirichlet;
