@@ -102,15 +102,28 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t *bar, unsigned phase,
 // the layouts with the fewest shared-memory wavefronts over the Z, X and Y
 // accesses of a search over all linear layouts (64-bit accesses in two
 // half-warps, 32-bit in one pass; per set of 3n accesses):
-//   Q2 (3 cells per warp): S2 = 34, SC = 9:   64-bit 27 -> 24, 32-bit 15 -> 12
-//   other degrees: the plain layout S2 = n^2, SC = n^3
-template <int n>
-__host__ __device__ constexpr int tile_s2() { return n == 3 ? 34 : n * n; }
-template <int n>
-__host__ __device__ constexpr int tile_sc() { return n == 3 ? 9 : n * n * n; }
+//   Q1 (8 cells per warp): S2 = 5,  SC = 12:  64-bit 24 -> 16, 32-bit 12 -> 8
+//   Q2 (3 cells):          S2 = 34, SC = 9:   27 -> 24, 15 -> 12
+//   Q3 (2 cells):          S2 = 19, SC = 80:  72 -> 32, 40 -> 16
+//   Q4 (1 cell):           S2 = 25 (the plain layout is already the best)
+// (TUNED = false: the plain layout, which the batched apply keeps: it measured
+// faster there)
+template <int n, bool TUNED = true>
+__host__ __device__ constexpr int tile_s2()
+{
+  return !TUNED ? n * n : n == 2 ? 5 : n == 3 ? 34 : n == 4 ? 19 : n * n;
+}
+template <int n, bool TUNED = true>
+__host__ __device__ constexpr int tile_sc()
+{
+  return !TUNED ? n * n * n : n == 2 ? 12 : n == 3 ? 9 : n == 4 ? 80 : n * n * n;
+}
 // elements of one tile of a warp with plane stride S2
-template <int n, int S2>
-__host__ __device__ constexpr int tile_elems() { return (WCfg<n>::cpw - 1) * tile_sc<n>() + (n - 1) * S2 + n * n; }
+template <int n, int S2, bool TUNED = true>
+__host__ __device__ constexpr int tile_elems()
+{
+  return (WCfg<n>::cpw - 1) * tile_sc<n, TUNED>() + (n - 1) * S2 + n * n;
+}
 
 template <int n, int S2 = tile_s2<n>(), typename Real>
 __device__ __forceinline__ void putZ(Real *t, int a, int b, const Real (&v)[n])
@@ -153,55 +166,55 @@ __device__ __forceinline__ void getY(const Real *t, int a, int b, Real (&v)[n])
 // layouts; for Q4 in FP32 a plane stride of 37 makes both conflict-free (the
 // 25-stride of t0 costs Y accesses a second wavefront).  FP64 keeps 25: its
 // shared-memory traffic was measured slower with the wider tile.
-template <int n, typename Real>
-__host__ __device__ constexpr int t1s2() { return (n == 5 && sizeof(Real) == 4) ? 37 : tile_s2<n>(); }
+template <int n, typename Real, bool TUNED = true>
+__host__ __device__ constexpr int t1s2() { return (n == 5 && sizeof(Real) == 4) ? 37 : tile_s2<n, TUNED>(); }
 // both tiles of a warp
-template <int n, typename Real>
+template <int n, typename Real, bool TUNED = true>
 __host__ __device__ constexpr int warp_tile_elems()
 {
-  return tile_elems<n, tile_s2<n>()>() + tile_elems<n, t1s2<n, Real>()>();
+  return tile_elems<n, tile_s2<n, TUNED>(), TUNED>() + tile_elems<n, t1s2<n, Real, TUNED>(), TUNED>();
 }
 
 // nodal values u (Z layout) -> values uq and collocation gradients gx, gy, gz
 // at the Gauss points, all in Z layout.  S, Dc: tables in constant memory.
-template <int n, typename Real>
+template <int n, typename Real, bool TUNED = true>
 __device__ __forceinline__ void l_forward(const Tables<Real> &T, Real *t0, Real *t1, bool wr, int a, int b,
                                           const Real (&u)[n], Real (&uq)[n], Real (&gx)[n], Real (&gy)[n],
                                           Real (&gz)[n])
 {
   Real v[n], w[n];
   c1<n, Real, false, false>(T.S, T.eS, u, v);  // z: nodes -> Gauss points
-  if (wr) putZ<n>(t0, a, b, v);
+  if (wr) putZ<n, tile_s2<n, TUNED>()>(t0, a, b, v);
   __syncwarp();
-  getX<n>(t0, a, b, w);
+  getX<n, tile_s2<n, TUNED>()>(t0, a, b, w);
   __syncwarp();
   c1<n, Real, false, false>(T.S, T.eS, w, v);  // x
-  if (wr) putX<n>(t0, a, b, v);
+  if (wr) putX<n, tile_s2<n, TUNED>()>(t0, a, b, v);
   __syncwarp();
-  getY<n>(t0, a, b, w);
+  getY<n, tile_s2<n, TUNED>()>(t0, a, b, w);
   __syncwarp();
   c1<n, Real, false, false>(T.S, T.eS, w, v);    // y: v = values at the Gauss points (Y layout)
   c1<n, Real, false, true>(T.Dc, T.eDc, v, w);   // d/dy (Y layout)
   if (wr) {
-    putY<n>(t0, a, b, v);
-    putY<n, t1s2<n, Real>()>(t1, a, b, w);
+    putY<n, tile_s2<n, TUNED>()>(t0, a, b, v);
+    putY<n, t1s2<n, Real, TUNED>()>(t1, a, b, w);
   }
   __syncwarp();
-  getZ<n>(t0, a, b, uq);
-  getX<n>(t0, a, b, w);
-  getZ<n, t1s2<n, Real>()>(t1, a, b, gy);
+  getZ<n, tile_s2<n, TUNED>()>(t0, a, b, uq);
+  getX<n, tile_s2<n, TUNED>()>(t0, a, b, w);
+  getZ<n, t1s2<n, Real, TUNED>()>(t1, a, b, gy);
   __syncwarp();
   c1<n, Real, false, true>(T.Dc, T.eDc, uq, gz);  // d/dz (Z layout)
   c1<n, Real, false, true>(T.Dc, T.eDc, w, v);    // d/dx (X layout)
-  if (wr) putX<n>(t0, a, b, v);
+  if (wr) putX<n, tile_s2<n, TUNED>()>(t0, a, b, v);
   __syncwarp();
-  getZ<n>(t0, a, b, gx);
+  getZ<n, tile_s2<n, TUNED>()>(t0, a, b, gx);
   __syncwarp();
 }
 
 // test functions: out = S^T (val + Dc_x^T fx + Dc_y^T fy + Dc_z^T fz) in all
 // three directions; inputs at the Gauss points and output at the nodes, Z layout
-template <int n, typename Real>
+template <int n, typename Real, bool TUNED = true>
 __device__ __forceinline__ void l_backward(const Tables<Real> &T, Real *t0, Real *t1, bool wr, int a, int b,
                                            const Real (&val)[n], const Real (&fx)[n], const Real (&fy)[n],
                                            const Real (&fz)[n], Real (&out)[n])
@@ -211,34 +224,34 @@ __device__ __forceinline__ void l_backward(const Tables<Real> &T, Real *t0, Real
 #pragma unroll
   for (int k = 0; k < n; ++k) A[k] += val[k];  // Z layout
   if (wr) {
-    putZ<n>(t0, a, b, fx);
-    putZ<n, t1s2<n, Real>()>(t1, a, b, fy);
+    putZ<n, tile_s2<n, TUNED>()>(t0, a, b, fx);
+    putZ<n, t1s2<n, Real, TUNED>()>(t1, a, b, fy);
   }
   __syncwarp();
-  getX<n>(t0, a, b, w);
-  getY<n, t1s2<n, Real>()>(t1, a, b, C);
+  getX<n, tile_s2<n, TUNED>()>(t0, a, b, w);
+  getY<n, t1s2<n, Real, TUNED>()>(t1, a, b, C);
   __syncwarp();
   c1<n, Real, true, true>(T.Dc, T.eDct, w, B);  // x part (X layout)
   c1<n, Real, true, true>(T.Dc, T.eDct, C, w);  // y part (Y layout)
   if (wr) {
-    putZ<n, t1s2<n, Real>()>(t1, a, b, A);
-    putX<n>(t0, a, b, B);
+    putZ<n, t1s2<n, Real, TUNED>()>(t1, a, b, A);
+    putX<n, tile_s2<n, TUNED>()>(t0, a, b, B);
   }
   __syncwarp();
-  getY<n, t1s2<n, Real>()>(t1, a, b, A);
-  getY<n>(t0, a, b, B);
+  getY<n, t1s2<n, Real, TUNED>()>(t1, a, b, A);
+  getY<n, tile_s2<n, TUNED>()>(t0, a, b, B);
   __syncwarp();
 #pragma unroll
   for (int q = 0; q < n; ++q) C[q] = w[q] + A[q] + B[q];  // sum in Y layout
   c1<n, Real, true, false>(T.S, T.eSt, C, w);  // y: Gauss points -> nodes
-  if (wr) putY<n>(t0, a, b, w);
+  if (wr) putY<n, tile_s2<n, TUNED>()>(t0, a, b, w);
   __syncwarp();
-  getX<n>(t0, a, b, C);
+  getX<n, tile_s2<n, TUNED>()>(t0, a, b, C);
   __syncwarp();
   c1<n, Real, true, false>(T.S, T.eSt, C, w);  // x
-  if (wr) putX<n>(t0, a, b, w);
+  if (wr) putX<n, tile_s2<n, TUNED>()>(t0, a, b, w);
   __syncwarp();
-  getZ<n>(t0, a, b, C);
+  getZ<n, tile_s2<n, TUNED>()>(t0, a, b, C);
   __syncwarp();
   c1<n, Real, true, false>(T.S, T.eSt, C, out);  // z
 }
