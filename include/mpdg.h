@@ -258,7 +258,12 @@ mpdg_status mpdg_vmult_multi_f32(mpdg_op *op, int n_vectors, float *const *dst, 
  * be NULL) receives how many were used (0: the first image is zero, solution = 0). */
 mpdg_status mpdg_predict_lsq(mpdg_op *op, int n_old, const double *const *old_solutions, const double *rhs,
                              double *solution, int *n_used);
-/* host-buffer form: copies src to the device, applies, copies dst back */
+/* host-buffer form: copies src to the device, applies, copies dst back.  For a
+ * plain warp-kernel operator (no faces, identity rows, hanging nodes, SUPG,
+ * Newton tangent or phase law) on a lattice of >= 4 cell layers the three
+ * steps overlap over up to 8 z-slabs of cell layers (copy-in, apply and
+ * copy-out on separate streams); dst_host is complete when the call returns.
+ * Pinned host buffers let the two copy directions run at once. */
 mpdg_status mpdg_vmult_host(mpdg_op *op, double *dst_host, const double *src_host);
 
 /* OperatorMatrixFree::compute_inverse_diagonal_from_matrixfree, operator_base.hpp:268-272

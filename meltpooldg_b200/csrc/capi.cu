@@ -294,6 +294,15 @@ void free_op_arrays(Op &o)
                   (void *)o.H32, (void *)o.lsq_buf, (void *)o.host_stage,
                   (void *)o.d_io, o.io_tmp})
     if (p) cudaFree(p);
+  if (o.pipe_in) {
+    cudaStreamSynchronize(o.pipe_in);
+    cudaStreamSynchronize(o.pipe_out);
+    cudaStreamDestroy(o.pipe_in);
+    cudaStreamDestroy(o.pipe_out);
+    for (auto &e : o.pipe_ev)
+      if (e) cudaEventDestroy(e);
+    o.pipe_in = o.pipe_out = nullptr;
+  }
 }
 }  // namespace
 
@@ -495,9 +504,58 @@ mpdg_status mpdg_vmult_host(mpdg_op *op, double *dst_host, const double *src_hos
       o.device_bytes += 2 * bytes;
     }
     double *d_src = o.host_stage, *d_dst = o.host_stage + o.mesh->N;
-    MPDG_CUDA(cudaMemcpyAsync(d_src, src_host, bytes, cudaMemcpyHostToDevice, o.stream));
-    launch_apply<double>(o, d_dst, d_src);
-    MPDG_CUDA(cudaMemcpyAsync(dst_host, d_dst, bytes, cudaMemcpyDeviceToHost, o.stream));
+    const Mesh &m = *o.mesh;
+    const int nz = m.nc[2], S = std::min(kPipeSlabs, nz / 2);
+    if (!plain_warp_apply(o) || S < 2) {
+      MPDG_CUDA(cudaMemcpyAsync(d_src, src_host, bytes, cudaMemcpyHostToDevice, o.stream));
+      launch_apply<double>(o, d_dst, d_src);
+      MPDG_CUDA(cudaMemcpyAsync(dst_host, d_dst, bytes, cudaMemcpyDeviceToHost, o.stream));
+      MPDG_CUDA(cudaStreamSynchronize(o.stream));
+      return MPDG_OK;
+    }
+    // z-slab pipeline: the copy-in of slab s+1, the apply of slab s and the
+    // copy-out of slab s-1 overlap (the two copy directions run at once).  A
+    // slab of cell layers [za, zb) reads the DoF planes [za P, zb P] and
+    // completes the planes below zb P; interior slab ends zb are odd, so the
+    // layer below every slab boundary is even and its cells store the shared
+    // plane before the next slab's cells add to it (the first-touch rule)
+    if (!o.pipe_in) {
+      MPDG_CUDA(cudaStreamCreateWithFlags(&o.pipe_in, cudaStreamNonBlocking));
+      MPDG_CUDA(cudaStreamCreateWithFlags(&o.pipe_out, cudaStreamNonBlocking));
+      for (auto &e : o.pipe_ev) MPDG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    const long plane = m.NX * m.NY, P = m.degree, NZ = m.NZ;
+    int bounds[kPipeSlabs + 1];
+    bounds[0] = 0;
+    for (int i = 1; i < S; ++i) {
+      int b = (int)((long)i * nz / S) | 1;
+      bounds[i] = std::min(std::max(b, bounds[i - 1] + 1), nz - 1);
+    }
+    bounds[S] = nz;
+    for (int i = 1; i < S; ++i)
+      if (bounds[i] % 2 == 0 || bounds[i] <= bounds[i - 1])
+        throw Error{MPDG_ERR_ARG, "host apply pipeline: slab bounds"};
+    long in_next = 0, out_next = 0;  // first plane not yet copied in / out
+    for (int sl = 0; sl < S; ++sl) {
+      const int za = bounds[sl], zb = bounds[sl + 1];
+      if (zb <= za) continue;
+      const long in_end = std::min(NZ, (long)zb * P + 1);
+      if (in_end > in_next)
+        MPDG_CUDA(cudaMemcpyAsync(d_src + in_next * plane, src_host + in_next * plane,
+                                  sizeof(double) * (in_end - in_next) * plane, cudaMemcpyHostToDevice, o.pipe_in));
+      in_next = std::max(in_next, in_end);
+      MPDG_CUDA(cudaEventRecord(o.pipe_ev[2 * sl], o.pipe_in));
+      MPDG_CUDA(cudaStreamWaitEvent(o.stream, o.pipe_ev[2 * sl], 0));
+      launch_apply_zrange(o, d_dst, d_src, za, zb);
+      MPDG_CUDA(cudaEventRecord(o.pipe_ev[2 * sl + 1], o.stream));
+      MPDG_CUDA(cudaStreamWaitEvent(o.pipe_out, o.pipe_ev[2 * sl + 1], 0));
+      const long out_end = (zb == nz) ? NZ : (long)zb * P;
+      if (out_end > out_next)
+        MPDG_CUDA(cudaMemcpyAsync(dst_host + out_next * plane, d_dst + out_next * plane,
+                                  sizeof(double) * (out_end - out_next) * plane, cudaMemcpyDeviceToHost, o.pipe_out));
+      out_next = std::max(out_next, out_end);
+    }
+    MPDG_CUDA(cudaStreamSynchronize(o.pipe_out));
     MPDG_CUDA(cudaStreamSynchronize(o.stream));
     return MPDG_OK;
   });

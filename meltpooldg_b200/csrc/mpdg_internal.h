@@ -119,6 +119,8 @@ struct Mesh {
 
 struct Workspace;  // solver vectors (solvers.cu)
 
+constexpr int kPipeSlabs = 8;  // z-slabs of the pipelined host-buffer apply
+
 struct Op {
   Mesh *mesh = nullptr;
   mpdg_op_desc d{};
@@ -159,6 +161,10 @@ struct Op {
   uint8_t *d_io = nullptr;
   // device copies of the host vectors of mpdg_vmult_host (src, dst)
   double *host_stage = nullptr;
+  // z-slab pipeline of the host-buffer apply: copy-in and copy-out streams and
+  // one event per slab and stage (created on first use)
+  cudaStream_t pipe_in = nullptr, pipe_out = nullptr;
+  cudaEvent_t pipe_ev[2 * kPipeSlabs] = {};
   // least-squares predictor: images of the old solutions (lsq_cols vectors of N)
   double *lsq_buf = nullptr;
   int lsq_cols = 0;
@@ -234,6 +240,13 @@ template <typename Real>
 void launch_apply(Op &op, Real *dst, const Real *src);
 template <typename Real>
 void launch_apply_multi(Op &op, int nvec, Real *const *dst, const Real *const *src);
+// the operator's apply is the warp kernel alone (no faces, identity rows,
+// hanging nodes, SUPG, Newton tangent or phase law; a lattice mesh)
+bool plain_warp_apply(const Op &op);
+// the cells of z-layers [z0, z1) of a plain warp apply; dst holds the first
+// stores of their DoFs (layer ranges must be applied in increasing order and
+// end after an even layer, so that every DoF's first toucher runs first)
+void launch_apply_zrange(Op &op, double *dst, const double *src, int z0, int z1);
 constexpr int kMaxLsqVectors = 32;
 // returns the number of old solutions used (predictor.cu)
 int predict_lsq(Op &op, int n_old, const double *const *old, const double *rhs, double *solution);

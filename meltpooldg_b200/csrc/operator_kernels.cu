@@ -245,6 +245,8 @@ struct KP {
   // touch a constrained DoF in the diagonal kernel
   const int *cmap;
   int skip_constrained;
+  // host side only: restrict the colour launches to cell layers [zlo, zhi)
+  int zlo, zhi;
   // multi-vector apply: nvec operands msrc[v] -> mdst[v]
   int nvec;
   const Real *msrc[kMaxMultiVec];
@@ -1685,7 +1687,18 @@ void run_warp_apply(Op &op, KP<Real> k)
     const Colour &C = colours(m)[c];
     if (C.count == 0) continue;
     colour_params(k, C);
-    const long groups = (C.count + CPW - 1) / CPW;
+    if (k.zhi > k.zlo) {
+      // the colour's cells are z-major: layers [zlo, zhi) are a contiguous
+      // run of colour-local indices, and the z parity absorbs the offset
+      const long plane = (long)C.cn[0] * C.cn[1];
+      const long m_lo = (k.zlo - C.par[2] + 1) / 2, m_hi = (k.zhi - C.par[2] + 1) / 2;
+      const long c_lo = std::min((long)C.count, m_lo * plane), c_hi = std::min((long)C.count, m_hi * plane);
+      if (c_hi <= c_lo) continue;
+      k.cfirst = C.first + c_lo;
+      k.ccount = c_hi - c_lo;
+      k.par[2] = C.par[2] + 2 * (int)m_lo;
+    }
+    const long groups = (k.ccount + CPW - 1) / CPW;
     const long blocks = std::min(resident, (groups + kWarpsPerCTA - 1) / kWarpsPerCTA);
     kern<<<(unsigned)blocks, kWarpsPerCTA * 32, smem, op.stream>>>(k, op.d_err);
     MPDG_LAUNCHED();
@@ -2139,6 +2152,36 @@ void launch_cells(Op &op, Real *dst, const Real *src)
 template void launch_apply<double>(Op &, double *, const double *);
 template void launch_apply<float>(Op &, float *, const float *);
 
+bool plain_warp_apply(const Op &op)
+{
+  const Mesh &m = *op.mesh;
+  const mpdg_op_desc &D = op.d;
+  const bool heat = D.kind == MPDG_OP_HEAT;
+  const bool faces = heat && ((D.robin_faces && D.robin_alpha != 0.0) || (D.rad_faces && D.rad_emissivity != 0.0));
+  const bool full = heat && D.full_tangent;
+  return !op.fine && !m.mapped && !op.d_io && !faces && !supg(op) && !full && !uses_law(op) &&
+         (!m.uniform || !uses_kT(op));
+}
+
+void launch_apply_zrange(Op &op, double *dst, const double *src, int z0, int z1)
+{
+  Mesh &m = *op.mesh;
+  if (!plain_warp_apply(op)) throw Error{MPDG_ERR_UNSUPPORTED, "layer-range apply: plain warp operators only"};
+  KP<double> k = base_params<double>(op);
+  if (uses_kT(op) && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
+  k.src = src;
+  k.dst = dst;
+  k.zlo = z0;
+  k.zhi = z1;
+  if (m.uniform) {
+    warp_apply_degree<double, GEOM_UNIFORM>(op, k);
+  } else {
+    ensure_coef(op, false);
+    k.metric = op.d_coef64;
+    warp_apply_degree<double, GEOM_GENERAL>(op, k);
+  }
+}
+
 // dst[v] = A src[v] for nvec vectors.  Operators whose apply is the plain warp
 // kernel (no faces, constraints rows, hanging nodes, SUPG or phase law) take up
 // to kMaxMultiVec vectors per pass, reading each cell's coefficients once;
@@ -2156,17 +2199,11 @@ void launch_apply_multi(Op &op, int nvec, Real *const *dst, const Real *const *s
       if (over_ds || over_dd) throw Error{MPDG_ERR_ARG, "multi-vector apply: destinations overlap a vector"};
     }
   }
-  const mpdg_op_desc &D = op.d;
-  const bool heat = D.kind == MPDG_OP_HEAT;
-  const bool faces = heat && ((D.robin_faces && D.robin_alpha != 0.0) || (D.rad_faces && D.rad_emissivity != 0.0));
-  const bool full = heat && D.full_tangent;
-  const bool fused = !op.fine && !m.mapped && !op.d_io && !faces && !supg(op) && !full && !uses_law(op) &&
-                     (!m.uniform || !uses_kT(op));
-  if (!fused) {
+  if (!plain_warp_apply(op)) {
     for (int v = 0; v < nvec; ++v) launch_apply<Real>(op, dst[v], src[v]);
     return;
   }
-  if (!m.uniform && D.vel_kind != MPDG_VEL_NONE && sizeof(Real) == 4 && !op.d_velb32)
+  if (!m.uniform && op.d.vel_kind != MPDG_VEL_NONE && sizeof(Real) == 4 && !op.d_velb32)
     throw Error{MPDG_ERR_ARG, "the FP32 form was not prepared for this operator (precision_mask)"};
   KP<Real> k = base_params<Real>(op);
   if (uses_kT(op) && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
