@@ -535,16 +535,19 @@ mpdg_status mpdg_vmult_host(mpdg_op *op, double *dst_host, const double *src_hos
     for (int i = 1; i < S; ++i)
       if (bounds[i] % 2 == 0 || bounds[i] <= bounds[i - 1])
         throw Error{MPDG_ERR_ARG, "host apply pipeline: slab bounds"};
+    // all copies in first: they depend on nothing, and the copy-in stream
+    // then never waits for the host to enqueue the applies
     long in_next = 0, out_next = 0;  // first plane not yet copied in / out
     for (int sl = 0; sl < S; ++sl) {
-      const int za = bounds[sl], zb = bounds[sl + 1];
-      if (zb <= za) continue;
-      const long in_end = std::min(NZ, (long)zb * P + 1);
+      const long in_end = std::min(NZ, (long)bounds[sl + 1] * P + 1);
       if (in_end > in_next)
         MPDG_CUDA(cudaMemcpyAsync(d_src + in_next * plane, src_host + in_next * plane,
                                   sizeof(double) * (in_end - in_next) * plane, cudaMemcpyHostToDevice, o.pipe_in));
       in_next = std::max(in_next, in_end);
       MPDG_CUDA(cudaEventRecord(o.pipe_ev[2 * sl], o.pipe_in));
+    }
+    for (int sl = 0; sl < S; ++sl) {
+      const int za = bounds[sl], zb = bounds[sl + 1];
       MPDG_CUDA(cudaStreamWaitEvent(o.stream, o.pipe_ev[2 * sl], 0));
       launch_apply_zrange(o, d_dst, d_src, za, zb);
       MPDG_CUDA(cudaEventRecord(o.pipe_ev[2 * sl + 1], o.stream));
