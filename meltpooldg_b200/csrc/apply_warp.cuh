@@ -106,8 +106,7 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t *bar, unsigned phase,
 //   Q2 (3 cells):          S2 = 34, SC = 9:   27 -> 24, 15 -> 12
 //   Q3 (2 cells):          S2 = 19, SC = 80:  72 -> 32, 40 -> 16
 //   Q4 (1 cell):           S2 = 25 (the plain layout is already the best)
-// (TUNED = false: the plain layout, which the batched apply keeps: it measured
-// faster there)
+// (TUNED = false: the plain layout)
 template <int n, bool TUNED = true>
 __host__ __device__ constexpr int tile_s2()
 {

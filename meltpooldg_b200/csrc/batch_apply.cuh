@@ -134,12 +134,12 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
                                            const Real (&uin)[kMaxN], Real *tiles, int lane)
 {
   constexpr int n = P + 1;
-  static_assert(warp_tile_elems<n, Real, false>() <= kBatchTileElems, "tile area");
+  static_assert(warp_tile_elems<n, Real>() <= kBatchTileElems, "tile area");
   const Tables<Real> &T = tab<Real>(P);
   const BatchLanePos<P> q = batch_pos<P>(colour, local_group, W, lane);
   const int i = q.i, j = q.j, ix = q.ix, iy = q.iy, iz = q.iz;
-  Real *t0 = tiles + q.s_sub * tile_sc<n, false>();
-  Real *t1 = tiles + tile_elems<n, tile_s2<n, false>(), false>() + q.s_sub * tile_sc<n, false>();
+  Real *t0 = tiles + q.s_sub * tile_sc<n>();
+  Real *t1 = tiles + tile_elems<n, tile_s2<n>()>() + q.s_sub * tile_sc<n>();
   const long NX = q.NX, zs = NX * NX, g0 = q.g0;
   Real *dst = W.dst;
   const bool dir = W.dirichlet;
@@ -164,7 +164,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
 #pragma unroll
   for (int k = 0; k < n; ++k) u[k] = uin[k];
   Real uq[n], gx[n], gy[n], gz[n];
-  l_forward<n, Real, false>(T, t0, t1, true, i, j, u, uq, gx, gy, gz);
+  l_forward<n>(T, t0, t1, true, i, j, u, uq, gx, gy, gz);
   Real val[n], fx[n], fy[n], fz[n];
   const Real hvol = (Real)W.hvol, ih = (Real)W.ih, ih2 = (Real)W.ih2;
   const Real c_mass = (Real)W.c_mass, c_vel = (Real)W.c_vel, c_diff = (Real)W.c_diff;
@@ -188,7 +188,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
     fz[k] = kd * gz[k];
   }
   Real out[n];
-  l_backward<n, Real, false>(T, t0, t1, true, i, j, val, fx, fy, fz, out);
+  l_backward<n>(T, t0, t1, true, i, j, val, fx, fy, fz, out);
   if (q.act) {
 #pragma unroll
     for (int k = 0; k < n; ++k) {
