@@ -233,6 +233,12 @@ mpdg_status mpdg_op_set_inflow_outflow(mpdg_op *op, const uint8_t *host_mask);
 /* reads and clears the operator's device error word: nonzero when a bounded
  * device-side wait (bulk-copy completion) expired; synchronises the stream */
 mpdg_status mpdg_op_device_error(mpdg_op *op, int *flag);
+/* test hook: the number of polls after which a bounded device wait of the
+ * apply reports expiry on the current device (polls < 0 restores the default,
+ * 2^26).  An expired wait sets the operator's error word and then waits for
+ * its copy with the full limit, so results are unchanged.  No reference
+ * counterpart (the reference has no device code). */
+mpdg_status mpdg_debug_set_wait_polls(int64_t polls);
 
 /* OperatorMatrixFree::vmult, operator_base.hpp:239-243
  * (heat: source/heat/heat_diffuse_operator.cpp:179-197;
@@ -247,6 +253,34 @@ mpdg_status mpdg_vmult_f32(mpdg_op *op, float *dst, const float *src);
  * the others apply the vectors in turn.  Replaces the n vmult calls of
  * LeastSquaresProjection::vmult (include/meltpooldg/linear_algebra/predictor.hpp:37-46). */
 mpdg_status mpdg_vmult_multi(mpdg_op *op, int n_vectors, double *const *dst, const double *const *src);
+/* Schedule of the resident apply, per precision.  slabs > 1 runs the colour
+ * launches z-slab by z-slab (cell layers split into `slabs` runs with odd
+ * interior ends, each running its 8 colours before the next), so that a slab's
+ * DoF vectors stay in L2 across its colours; l2_evict_first marks the streamed
+ * per-quadrature-point coefficients evict-first in L2; overlap_colours launches
+ * every colour after an apply's first as a programmatic dependent of the one
+ * before, so that its start (coefficient copies, src gathers, the first cells'
+ * arithmetic) overlaps the previous colour's last cells and only its reads of
+ * dst wait for it.  Results are identical for every schedule.  No reference
+ * counterpart: the schedule of deal.II's MatrixFree::cell_loop
+ * (heat_diffuse_operator.cpp:183) is internal to it. */
+typedef struct {
+  int slabs;            /* 1..32 (capped at half the cell layers) */
+  int l2_evict_first;   /* 0 or 1 */
+  int overlap_colours;  /* 0 or 1 */
+} mpdg_schedule;
+mpdg_status mpdg_op_set_schedule(mpdg_op *op, int precision, const mpdg_schedule *schedule);
+mpdg_status mpdg_op_get_schedule(mpdg_op *op, int precision, mpdg_schedule *schedule);
+/* Autotuner of the resident apply: times `reps` applies (after one warm-up) of
+ * each candidate schedule -- slabs 1, 2, 4, 8, 16, each with and without the
+ * evict-first hint where the mesh streams coefficients, each with and without
+ * overlap_colours -- in the given
+ * precision (MPDG_FP64 / MPDG_FP32), keeps the fastest on the operator and
+ * returns it with its time per apply.  candidate_ms (may be NULL) receives up to
+ * n_candidate_ms per-candidate times in that order (-1 past the last).
+ * Allocates two scratch vectors for the duration of the call. */
+mpdg_status mpdg_op_autotune(mpdg_op *op, int precision, int reps, mpdg_schedule *best, double *apply_ms,
+                             double *candidate_ms, int n_candidate_ms);
 /* measured FMA throughput of the current GPU (GFLOP/s, 2 flops per FMA) in
  * FP64 and FP32: the arithmetic ceiling the apply's flop rate is reported against */
 mpdg_status mpdg_fma_peak(double *gflops64, double *gflops32);
@@ -306,9 +340,11 @@ void mpdg_solver_desc_default(mpdg_solver_desc *desc);
  * library holds until exit; problems larger than 262,144 DoFs are rejected
  * with MPDG_ERR_SIZE.  The first call on a device resolves the array's device
  * address (cudaGetSymbolAddress) with that device current: make that first
- * call before any stream capture.  On a general (non-uniform) mesh the
- * operator's coefficient stream must exist already (one mpdg_vmult first),
- * else MPDG_ERR_ARG.  All calls on a device share the array: calls whose work
+ * call before any stream capture.  On a general (non-uniform) mesh, and with
+ * inflow/outflow rows, the operator's coefficient stream and operand copy
+ * must exist already (one mpdg_vmult first), else MPDG_ERR_ARG; operators
+ * whose diagonal needs probe vectors (two-level meshes, SUPG) and mapped
+ * meshes with constraints are rejected with MPDG_ERR_ARG.  All calls on a device share the array: calls whose work
  * overlaps on the GPU race and must be serialised by the caller.  Semantics as
  * mpdg_solve with solver CG and preconditioner Jacobi; x holds the start. */
 mpdg_status mpdg_solve_cg_noalloc(mpdg_op *op, double *x, const double *b, double rel_tolerance,
@@ -321,6 +357,9 @@ mpdg_status mpdg_l2_norm(mpdg_op *op, const double *u, double *norm);
 
 /* number of kernels this library launched since load (its own kernels only) */
 int64_t mpdg_kernel_launches(void);
+/* number of device and pinned-host allocations (cudaMalloc, cudaMallocAsync,
+ * pool and host allocations) this library made since load */
+int64_t mpdg_allocations(void);
 
 /* ------------------------------------------------------- batched solves
  * Many independent problems advanced together on one GPU.  The reference

@@ -86,6 +86,10 @@ class SolveReport(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Schedule(C.Structure):
+    _fields_ = [("slabs", C.c_int), ("l2_evict_first", C.c_int), ("overlap_colours", C.c_int)]
+
+
 class ProblemDesc(C.Structure):
     _fields_ = [("kind", C.c_int), ("degree", C.c_int), ("nc", C.c_int), ("dirichlet", C.c_int),
                 ("vel_kind", C.c_int), ("max_iterations", C.c_int), ("dt", C.c_double),
@@ -114,6 +118,7 @@ def lib():
     vp, dp, fp = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_float)
     L.mpdg_last_error.restype = C.c_char_p
     L.mpdg_kernel_launches.restype = C.c_int64
+    L.mpdg_allocations.restype = C.c_int64
     L.mpdg_mesh_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(vp)]
     L.mpdg_mesh_destroy.argtypes = [vp]
     L.mpdg_mesh_create_two_level.argtypes = [C.POINTER(MeshDesc), C.POINTER(MeshDesc), C.POINTER(vp)]
@@ -131,10 +136,14 @@ def lib():
     L.mpdg_compute_inverse_diagonal_host.argtypes = [vp, dp]
     L.mpdg_create_rhs_host.argtypes = [vp, dp, dp, dp]
     L.mpdg_op_device_error.argtypes = [vp, C.POINTER(C.c_int)]
+    L.mpdg_debug_set_wait_polls.argtypes = [C.c_int64]
     L.mpdg_vmult.argtypes = [vp, vp, vp]
     L.mpdg_vmult_f32.argtypes = [vp, vp, vp]
     L.mpdg_vmult_multi.argtypes = [vp, C.c_int, C.POINTER(vp), C.POINTER(vp)]
     L.mpdg_fma_peak.argtypes = [dp, dp]
+    L.mpdg_op_set_schedule.argtypes = [vp, C.c_int, C.POINTER(Schedule)]
+    L.mpdg_op_get_schedule.argtypes = [vp, C.c_int, C.POINTER(Schedule)]
+    L.mpdg_op_autotune.argtypes = [vp, C.c_int, C.c_int, C.POINTER(Schedule), dp, dp, C.c_int]
     L.mpdg_vmult_multi_f32.argtypes = [vp, C.c_int, C.POINTER(vp), C.POINTER(vp)]
     L.mpdg_predict_lsq.argtypes = [vp, C.c_int, C.POINTER(vp), vp, vp, C.POINTER(C.c_int)]
     L.mpdg_vmult_host.argtypes = [vp, dp, dp]
@@ -178,3 +187,8 @@ def check(status, where):
 
 def kernel_launches():
     return int(lib().mpdg_kernel_launches())
+
+
+def allocations():
+    """Device and pinned-host allocations the library has made since load."""
+    return int(lib().mpdg_allocations())

@@ -57,6 +57,26 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
       : "memory");
 }
 
+// the same copy with an L2 eviction-priority hint: the coefficient stream is
+// read once per apply, so it is marked evict-first and leaves the L2 to the
+// DoF vectors, which the colour launches read again
+__device__ __forceinline__ uint64_t l2_policy_evict_first()
+{
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
+__device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, unsigned bytes, uint64_t *bar,
+                                              uint64_t pol)
+{
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+      "%4;" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+      : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase)
 {
   unsigned ok;
@@ -68,22 +88,36 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase)
   return ok != 0;
 }
 
+// programmatic dependent launch: a colour launch may start while the previous
+// colour's last cells finish; it reads src and its coefficients (which the
+// previous colour does not write) at once and waits for the previous grid only
+// before its first read of dst
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
+// polls of the first phase of a bounded wait before it reports expiry
+// (mpdg_debug_set_wait_polls lowers it to exercise the expiry path; the retry
+// phase always has the full limit, so results do not change)
+__constant__ long long c_wait_first_polls = kMbarSpinLimit;
+
 // bounded wait: on expiry the error word is set and the wait is retried once
-// (also bounded) so that no copy is left targeting this CTA's shared memory
+// with the full limit, so that no copy is left targeting this CTA's shared
+// memory when the kernel goes on
 __device__ __forceinline__ void mbar_wait_bounded(uint64_t *bar, unsigned phase, int *err)
 {
-  long spins = 0;
-  while (!mbar_try_wait(bar, phase)) {
-    if (++spins > kMbarSpinLimit) {
+  const long long first = c_wait_first_polls;
+  for (long long polls = 0;; ++polls) {
+    if (polls >= first) {
       if (err) atomicExch(err, 1);
       long again = 0;
       while (!mbar_try_wait(bar, phase) && ++again < kMbarSpinLimit) {
       }
       return;
     }
+    if (mbar_try_wait(bar, phase)) return;
   }
 }
 
@@ -309,6 +343,11 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   if (lane == 0) mbar_init(&bars[warp], 1);
   fence_mbar_init();
   __syncthreads();
+  // the next colour's CTAs may be scheduled as this grid's CTAs retire
+  if (p.pdl) grid_dep_launch_dependents();
+  // launched as a dependent of the previous colour: dst is read only after
+  // grid_dep_wait, which the first group of each warp does after its compute
+  bool dep_pending = p.pdl != 0;
 
   unsigned char *base = smem_raw + ((kSmemAlign - (smem_u32(smem_raw) & (kSmemAlign - 1))) & (kSmemAlign - 1));
   Real *wsm = reinterpret_cast<Real *>(base) + warp * warp_smem_elems<P, Real, GEOM>(gvel);
@@ -338,8 +377,14 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     const unsigned mb = ncell * MS * sizeof(Real), vb = gvel ? ncell * VS * sizeof(Real) : 0;
     fence_proxy_async();
     mbar_expect_tx(&bars[warp], mb + vb);
-    bulk_g2s(stage, p.metric + (p.cfirst + c0) * (long)MS, mb, &bars[warp]);
-    if (gvel) bulk_g2s(vstage, p.velb + (p.cfirst + c0) * (long)VS, vb, &bars[warp]);
+    if (p.stream_evict_first) {
+      const uint64_t pol = l2_policy_evict_first();
+      bulk_g2s_hint(stage, p.metric + (p.cfirst + c0) * (long)MS, mb, &bars[warp], pol);
+      if (gvel) bulk_g2s_hint(vstage, p.velb + (p.cfirst + c0) * (long)VS, vb, &bars[warp], pol);
+    } else {
+      bulk_g2s(stage, p.metric + (p.cfirst + c0) * (long)MS, mb, &bars[warp]);
+      if (gvel) bulk_g2s(vstage, p.velb + (p.cfirst + c0) * (long)VS, vb, &bars[warp]);
+    }
   };
   // raw src column and constrained-DoF mask of the lane's cell in group grp;
   // nothing here consumes a load, so the loads stay in flight while the
@@ -445,11 +490,15 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     for (int v = 0; v < nv; ++v) {
     Real *dst_v = (MULTI && v > 0) ? p.mdst[v] : p.dst;
     Real dpre[n];
+    const bool late_dst = dep_pending;
+    auto load_dpre = [&]() {
 #pragma unroll
-    for (int k = 0; k < n; ++k) {
-      const bool first = (first_bits >> k) & 1, masked = (mask_bits >> k) & 1;
-      dpre[k] = (active && !first && !masked && !hl) ? dst_v[gk[k]] : Real(0);
-    }
+      for (int k = 0; k < n; ++k) {
+        const bool first = (first_bits >> k) & 1, masked = (mask_bits >> k) & 1;
+        dpre[k] = (active && !first && !masked && !hl) ? dst_v[gk[k]] : Real(0);
+      }
+    };
+    if (!late_dst) load_dpre();
 
     Real u[n];
     if (!MULTI || v == 0) {
@@ -551,6 +600,12 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
         }
       }
       __syncwarp();
+    }
+
+    if (late_dst) {
+      grid_dep_wait();
+      dep_pending = false;
+      load_dpre();
     }
 
     if (!HANG && !any_mask) {

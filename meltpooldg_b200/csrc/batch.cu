@@ -117,7 +117,7 @@ T *balloc(size_t n)
 {
   T *p = nullptr;
   if (n == 0) return nullptr;
-  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  cudaError_t e = tracked_malloc(&p, n * sizeof(T));
   if (e != cudaSuccess) throw Error{MPDG_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
   return p;
 }
@@ -943,12 +943,12 @@ template <typename T>
 T *palloc(Batch &B, size_t n)
 {
   void *p = nullptr;
-  cudaError_t e = cudaMallocFromPoolAsync(&p, n * sizeof(T), B.pool, B.stream);
+  cudaError_t e = tracked_malloc_pool_async(&p, n * sizeof(T), B.pool, B.stream);
   if (e == cudaErrorMemoryAllocation) {
     cudaGetLastError();
     MPDG_CUDA(cudaStreamSynchronize(B.stream));
     MPDG_CUDA(cudaMemPoolTrimTo(B.pool, 0));
-    e = cudaMallocFromPoolAsync(&p, n * sizeof(T), B.pool, B.stream);
+    e = tracked_malloc_pool_async(&p, n * sizeof(T), B.pool, B.stream);
   }
   if (e != cudaSuccess) {
     cudaGetLastError();

@@ -25,10 +25,12 @@ namespace mpdg {
 namespace {
 thread_local std::string g_last_error;
 std::atomic<int64_t> g_launches{0};
+std::atomic<int64_t> g_allocations{0};
 }  // namespace
 
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 void count_launch(int n) { g_launches += n; }
+void count_allocation() { ++g_allocations; }
 
 }  // namespace mpdg
 
@@ -39,6 +41,7 @@ extern "C" {
 const char *mpdg_last_error(void) { return g_last_error.c_str(); }
 int mpdg_version(void) { return 1; }
 int64_t mpdg_kernel_launches(void) { return g_launches.load(); }
+int64_t mpdg_allocations(void) { return g_allocations.load(); }
 
 mpdg_status mpdg_mesh_create(const mpdg_mesh_desc *desc, mpdg_mesh **out)
 {
@@ -154,8 +157,8 @@ mpdg_status mpdg_mesh_create_two_level(const mpdg_mesh_desc *coarse, const mpdg_
       if (fd.dirichlet_mask)
         for (long i = 0; i < Nf; ++i) tdir[Nc + i] = fd.dirichlet_mask[i] ? 1 : 0;
       for (long r = 0; r < NYf * NZf; ++r) tdir[Nc + r * NXf] = thang[Nc + r * NXf] = 1;
-      MPDG_CUDA(cudaMalloc(&m.d_tmask_dir, N));
-      MPDG_CUDA(cudaMalloc(&m.d_tmask_hang, N));
+      MPDG_CUDA(tracked_malloc(&m.d_tmask_dir, N));
+      MPDG_CUDA(tracked_malloc(&m.d_tmask_hang, N));
       MPDG_CUDA(cudaMemcpy(m.d_tmask_dir, tdir.data(), N, cudaMemcpyHostToDevice));
       MPDG_CUDA(cudaMemcpy(m.d_tmask_hang, thang.data(), N, cudaMemcpyHostToDevice));
       m.device_bytes += 2 * N + f->device_bytes;
@@ -271,7 +274,7 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
         build_op_device_data(f);
         const int n = mm.degree + 1;
         const size_t bytes = sizeof(double) * (size_t)mm.fine->nc[1] * mm.fine->nc[2] * n * n;
-        MPDG_CUDA(cudaMalloc(&f.d_stage, bytes));
+        MPDG_CUDA(tracked_malloc(&f.d_stage, bytes));
         MPDG_CUDA(cudaMemset(f.d_stage, 0, bytes));
         f.device_bytes += bytes;
       }
@@ -378,7 +381,7 @@ mpdg_status mpdg_op_set_field_host(mpdg_op *op, int field, const double *values)
     if (o.fine) throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take no fields"};
     const size_t bytes = sizeof(double) * o.mesh->N;
     if (!*own) {
-      MPDG_CUDA(cudaMalloc(own, bytes));
+      MPDG_CUDA(tracked_malloc(own, bytes));
       o.device_bytes += bytes;
     }
     MPDG_CUDA(cudaMemcpyAsync(*own, values, bytes, cudaMemcpyHostToDevice, o.stream));
@@ -417,7 +420,7 @@ mpdg_status mpdg_op_set_inflow_outflow(mpdg_op *op, const uint8_t *host_mask)
     bool any = false;
     for (long i = 0; i < N && !any; ++i) any = host_mask[i] != 0;
     if (!any) return MPDG_OK;
-    MPDG_CUDA(cudaMalloc(&o.d_io, N));
+    MPDG_CUDA(tracked_malloc(&o.d_io, N));
     MPDG_CUDA(cudaMemcpy(o.d_io, host_mask, N, cudaMemcpyHostToDevice));
     return MPDG_OK;
   });
@@ -436,6 +439,63 @@ mpdg_status mpdg_vmult(mpdg_op *op, double *dst, const double *src)
   return guarded([&]() -> int {
     if (!op || !dst || !src) throw Error{MPDG_ERR_ARG, "null argument"};
     launch_apply<double>(op->o, dst, src);
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_debug_set_wait_polls(int64_t polls)
+{
+  return guarded([&]() -> int {
+    set_wait_first_polls((long long)polls);
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_op_set_schedule(mpdg_op *op, int precision, const mpdg_schedule *sched)
+{
+  return guarded([&]() -> int {
+    if (!op || !sched) throw Error{MPDG_ERR_ARG, "null argument"};
+    if (precision != MPDG_FP64 && precision != MPDG_FP32) throw Error{MPDG_ERR_ARG, "precision"};
+    if (sched->slabs < 1 || sched->slabs > kMaxApplySlabs) throw Error{MPDG_ERR_ARG, "slabs must be 1..32"};
+    op->o.sched[precision].slabs = sched->slabs;
+    op->o.sched[precision].evict_first = sched->l2_evict_first ? 1 : 0;
+    op->o.sched[precision].pdl = sched->overlap_colours ? 1 : 0;
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_op_get_schedule(mpdg_op *op, int precision, mpdg_schedule *sched)
+{
+  return guarded([&]() -> int {
+    if (!op || !sched) throw Error{MPDG_ERR_ARG, "null argument"};
+    if (precision != MPDG_FP64 && precision != MPDG_FP32) throw Error{MPDG_ERR_ARG, "precision"};
+    sched->slabs = op->o.sched[precision].slabs;
+    sched->l2_evict_first = op->o.sched[precision].evict_first;
+    sched->overlap_colours = op->o.sched[precision].pdl;
+    return MPDG_OK;
+  });
+}
+
+mpdg_status mpdg_op_autotune(mpdg_op *op, int precision, int reps, mpdg_schedule *best, double *apply_ms,
+                             double *candidate_ms, int n_candidate_ms)
+{
+  return guarded([&]() -> int {
+    if (!op) throw Error{MPDG_ERR_ARG, "null argument"};
+    if (precision != MPDG_FP64 && precision != MPDG_FP32) throw Error{MPDG_ERR_ARG, "precision"};
+    Op &o = op->o;
+    if (precision == MPDG_FP32 && o.T64 && !o.T32) ensure_T32(o);
+    ApplySchedule b;
+    double ms = 0.0;
+    std::vector<double> all;
+    autotune_apply(o, precision, reps, b, ms, &all);
+    if (best) {
+      best->slabs = b.slabs;
+      best->l2_evict_first = b.evict_first;
+      best->overlap_colours = b.pdl;
+    }
+    if (apply_ms) *apply_ms = ms;
+    if (candidate_ms)
+      for (int i = 0; i < n_candidate_ms; ++i) candidate_ms[i] = i < (int)all.size() ? all[i] : -1.0;
     return MPDG_OK;
   });
 }
@@ -500,7 +560,7 @@ mpdg_status mpdg_vmult_host(mpdg_op *op, double *dst_host, const double *src_hos
     // device staging kept by the operator between calls: a vmult from host
     // buffers costs its two PCIe copies and the apply, no allocation
     if (!o.host_stage) {
-      MPDG_CUDA(cudaMalloc(&o.host_stage, 2 * bytes));
+      MPDG_CUDA(tracked_malloc(&o.host_stage, 2 * bytes));
       o.device_bytes += 2 * bytes;
     }
     double *d_src = o.host_stage, *d_dst = o.host_stage + o.mesh->N;
@@ -592,7 +652,7 @@ struct HostStage {
     if (!h) return nullptr;
     double *d = nullptr;
     const size_t bytes = sizeof(double) * o.mesh->N;
-    MPDG_CUDA(cudaMallocAsync(&d, bytes, o.stream));
+    MPDG_CUDA(tracked_malloc_async(&d, bytes, o.stream));
     bufs.push_back(d);
     MPDG_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, o.stream));
     return d;
@@ -690,8 +750,8 @@ mpdg_status mpdg_solve_host(mpdg_op *op, const mpdg_solver_desc *desc, double *x
     Op &o = op->o;
     const size_t bytes = sizeof(double) * o.mesh->N;
     double *d_x = nullptr, *d_b = nullptr;
-    MPDG_CUDA(cudaMalloc(&d_x, bytes));
-    MPDG_CUDA(cudaMalloc(&d_b, bytes));
+    MPDG_CUDA(tracked_malloc(&d_x, bytes));
+    MPDG_CUDA(tracked_malloc(&d_b, bytes));
     MPDG_CUDA(cudaMemcpyAsync(d_x, x_host, bytes, cudaMemcpyHostToDevice, o.stream));
     MPDG_CUDA(cudaMemcpyAsync(d_b, b_host, bytes, cudaMemcpyHostToDevice, o.stream));
     int s = solve(o, *desc, d_x, d_b, local);

@@ -319,7 +319,7 @@ void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d)
     xw[kMaxN + q] = wq[q];
   }
   double *d_xw = nullptr;
-  MPDG_CUDA(cudaMalloc(&d_xw, sizeof(xw)));
+  MPDG_CUDA(tracked_malloc(&d_xw, sizeof(xw)));
   MPDG_CUDA(cudaMemcpy(d_xw, xw, sizeof(xw), cudaMemcpyHostToDevice));
   m.d_metric64 = dev_alloc<double>((size_t)E * metric_stride(n), B);
   MPDG_CUDA(cudaMemset(m.d_metric64, 0, sizeof(double) * E * metric_stride(n)));
@@ -358,7 +358,7 @@ void launch_mapped_apply(Op &op, Real *dst, const Real *src)
       if (op.io_tmp) cudaFree(op.io_tmp);
       op.io_tmp = nullptr;
       op.io_tmp_bytes = 0;
-      MPDG_CUDA(cudaMalloc(&op.io_tmp, bytes));
+      MPDG_CUDA(tracked_malloc(&op.io_tmp, bytes));
       op.io_tmp_bytes = bytes;
     }
     Real *tmp = static_cast<Real *>(op.io_tmp);

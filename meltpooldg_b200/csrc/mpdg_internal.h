@@ -30,6 +30,39 @@ struct Error {
 void set_last_error(const std::string &msg);
 void count_launch(int n = 1);
 
+// Every device and pinned-host allocation of the library goes through these
+// wrappers, which count them (mpdg_allocations): tests use the count to show
+// that an entry point allocated nothing.
+void count_allocation();
+inline cudaError_t tracked_malloc_raw(void **p, size_t bytes)
+{
+  count_allocation();
+  return cudaMalloc(p, bytes);
+}
+template <typename T>
+inline cudaError_t tracked_malloc(T **p, size_t bytes)
+{
+  return tracked_malloc_raw(reinterpret_cast<void **>(p), bytes);
+}
+template <typename T>
+inline cudaError_t tracked_malloc_async(T **p, size_t bytes, cudaStream_t s)
+{
+  count_allocation();
+  return cudaMallocAsync(reinterpret_cast<void **>(p), bytes, s);
+}
+template <typename T>
+inline cudaError_t tracked_malloc_pool_async(T **p, size_t bytes, cudaMemPool_t pool, cudaStream_t s)
+{
+  count_allocation();
+  return cudaMallocFromPoolAsync(reinterpret_cast<void **>(p), bytes, pool, s);
+}
+template <typename T>
+inline cudaError_t tracked_malloc_host(T **p, size_t bytes)
+{
+  count_allocation();
+  return cudaMallocHost(reinterpret_cast<void **>(p), bytes);
+}
+
 // runs the body of an extern "C" entry: internal errors become status codes
 template <typename F>
 int guarded(F &&f)
@@ -119,7 +152,18 @@ struct Mesh {
 
 struct Workspace;  // solver vectors (solvers.cu)
 
-constexpr int kPipeSlabs = 8;  // z-slabs of the pipelined host-buffer apply
+constexpr int kPipeSlabs = 8;       // z-slabs of the pipelined host-buffer apply
+constexpr int kMaxApplySlabs = 32;  // z-slabs of the resident apply
+
+// schedule of the resident warp apply (mpdg_op_set_schedule, mpdg_op_autotune);
+// the defaults are the fastest measured at the benchmark configurations on a
+// B200 (colour overlap: FP64 Q4 64^3 0.519 -> 0.488 ms, FP32 0.327 -> 0.294 ms
+// with the evict-first hint; z-slabs only add launch tails there)
+struct ApplySchedule {
+  int slabs = 1;        // z-slabs of cell layers, each running its 8 colours
+  int evict_first = 0;  // L2 evict-first hint on the coefficient stream
+  int pdl = 1;          // colour launches as programmatic dependents of the previous one
+};
 
 struct Op {
   Mesh *mesh = nullptr;
@@ -170,6 +214,7 @@ struct Op {
   int lsq_cols = 0;
   void *io_tmp = nullptr;
   size_t io_tmp_bytes = 0;
+  ApplySchedule sched[2] = {ApplySchedule{1, 0, 1}, ApplySchedule{1, 1, 1}};  // [MPDG_FP64], [MPDG_FP32]
 };
 
 // ---- batched apply over many solves (batch_apply.cuh / batch.cu)
@@ -247,6 +292,13 @@ bool plain_warp_apply(const Op &op);
 // stores of their DoFs (layer ranges must be applied in increasing order and
 // end after an even layer, so that every DoF's first toucher runs first)
 void launch_apply_zrange(Op &op, double *dst, const double *src, int z0, int z1);
+// bounds[0..S] of S z-slabs of nz cell layers (interior bounds odd); returns S,
+// limited to nz / 2 and kMaxApplySlabs
+int slab_bounds(int nz, int S, int *bounds);
+// times the resident apply of `op` in one precision over the candidate
+// schedules and keeps the fastest (mpdg_op_autotune)
+void autotune_apply(Op &op, int precision, int reps, ApplySchedule &best, double &best_ms,
+                    std::vector<double> *all_ms);
 constexpr int kMaxLsqVectors = 32;
 // returns the number of old solutions used (predictor.cu)
 int predict_lsq(Op &op, int n_old, const double *const *old, const double *rhs, double *solution);
@@ -255,8 +307,11 @@ void launch_diagonal(Op &op, double *diag);
 void launch_invert_diagonal(Op &op, double *diag);
 // inversion with a given threshold (no reduction, no allocation)
 void launch_invert_with_threshold(Op &op, double *diag, double thr);
-// true when an FP64 apply on `op` builds nothing lazily (no device allocation)
-bool apply_ready_without_allocation(const Op &op);
+// polls of a bounded device wait before it reports expiry (< 0: the default)
+void set_wait_first_polls(long long polls);
+// nullptr when an FP64 apply and the diagonal of `op` build nothing lazily (no
+// device allocation); else why not
+const char *noalloc_unready_reason(const Op &op);
 double l2_norm_integrated(Op &op, const double *u);
 
 // ---- vector kernels (vector_kernels.cu)

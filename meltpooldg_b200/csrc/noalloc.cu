@@ -76,9 +76,8 @@ int solve_cg_noalloc(Op &op, double *x, const double *b, double rel_tol, double 
   if (N > kNoAllocMaxDofs)
     throw Error{MPDG_ERR_SIZE, "problem has " + std::to_string(N) + " DoFs; the allocation-free CG "
                 "holds scratch for at most " + std::to_string(kNoAllocMaxDofs)};
-  if (!apply_ready_without_allocation(op))
-    throw Error{MPDG_ERR_ARG, "operator coefficients are not built yet: call mpdg_vmult once "
-                "(outside the allocation-free section) before mpdg_solve_cg_noalloc"};
+  if (const char *why = noalloc_unready_reason(op))
+    throw Error{MPDG_ERR_ARG, std::string("mpdg_solve_cg_noalloc: ") + why};
   double *base = scratch_for_current_device();
   double *r = base, *z = base + N, *p = base + 2 * N, *Ap = base + 3 * N, *invd = base + 4 * N;
   double *partial = base + 5 * kNoAllocMaxDofs;

@@ -247,6 +247,10 @@ struct KP {
   int skip_constrained;
   // host side only: restrict the colour launches to cell layers [zlo, zhi)
   int zlo, zhi;
+  // coefficient stream copies carry an L2 evict-first hint
+  int stream_evict_first;
+  // launched as a programmatic dependent of the previous colour launch
+  int pdl;
   // multi-vector apply: nvec operands msrc[v] -> mdst[v]
   int nvec;
   const Real *msrc[kMaxMultiVec];
@@ -1257,7 +1261,7 @@ T *dev_alloc(size_t count, size_t &bytes)
 {
   T *p = nullptr;
   if (count == 0) return nullptr;
-  cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  cudaError_t e = tracked_malloc(&p, count * sizeof(T));
   if (e != cudaSuccess) throw Error{MPDG_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
   bytes += count * sizeof(T);
   return p;
@@ -1298,7 +1302,7 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
 
   if (!uniform) {
     Colour *d_col = nullptr;
-    MPDG_CUDA(cudaMalloc(&d_col, sizeof(m.colour)));
+    MPDG_CUDA(tracked_malloc(&d_col, sizeof(m.colour)));
     MPDG_CUDA(cudaMemcpy(d_col, m.colour, sizeof(m.colour), cudaMemcpyHostToDevice));
     double *d_xw = nullptr;
     double xw[2 * kMaxN];
@@ -1310,7 +1314,7 @@ void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_genera
         xw[kMaxN + q] = wq[q];
       }
     }
-    MPDG_CUDA(cudaMalloc(&d_xw, sizeof(xw)));
+    MPDG_CUDA(tracked_malloc(&d_xw, sizeof(xw)));
     MPDG_CUDA(cudaMemcpy(d_xw, xw, sizeof(xw), cudaMemcpyHostToDevice));
     m.d_metric64 = dev_alloc<double>((size_t)m.n_cells * metric_stride(n), m.device_bytes);
     MPDG_CUDA(cudaMemset(m.d_metric64, 0, sizeof(double) * m.n_cells * metric_stride(n)));
@@ -1385,9 +1389,9 @@ void build_op_device_data(Op &op)
     double *d_xq = nullptr;
     double xq[kMaxN], wq[kMaxN];
     gauss(n, xq, wq);
-    MPDG_CUDA(cudaMalloc(&d_col, sizeof(m.colour)));
+    MPDG_CUDA(tracked_malloc(&d_col, sizeof(m.colour)));
     MPDG_CUDA(cudaMemcpy(d_col, m.colour, sizeof(m.colour), cudaMemcpyHostToDevice));
-    MPDG_CUDA(cudaMalloc(&d_xq, sizeof(xq)));
+    MPDG_CUDA(tracked_malloc(&d_xq, sizeof(xq)));
     MPDG_CUDA(cudaMemcpy(d_xq, xq, sizeof(xq), cudaMemcpyHostToDevice));
     op.d_tau64 = dev_alloc<double>((size_t)m.n_cells, op.device_bytes);
     if (want32) op.d_tau32 = dev_alloc<float>((size_t)m.n_cells, op.device_bytes);
@@ -1402,7 +1406,7 @@ void build_op_device_data(Op &op)
   if (op.d.vel_kind == MPDG_VEL_NONE) return;
   if (!m.uniform) {
     Colour *d_col = nullptr;
-    MPDG_CUDA(cudaMalloc(&d_col, sizeof(m.colour)));
+    MPDG_CUDA(tracked_malloc(&d_col, sizeof(m.colour)));
     MPDG_CUDA(cudaMemcpy(d_col, m.colour, sizeof(m.colour), cudaMemcpyHostToDevice));
     double xw[2 * kMaxN], xq[kMaxN], wq[kMaxN];
     gauss(n, xq, wq);
@@ -1411,7 +1415,7 @@ void build_op_device_data(Op &op)
       xw[kMaxN + q] = wq[q];
     }
     double *d_xw = nullptr;
-    MPDG_CUDA(cudaMalloc(&d_xw, sizeof(xw)));
+    MPDG_CUDA(tracked_malloc(&d_xw, sizeof(xw)));
     MPDG_CUDA(cudaMemcpy(d_xw, xw, sizeof(xw), cudaMemcpyHostToDevice));
     const long total = m.n_cells * n3;
     op.d_velb64 = dev_alloc<double>((size_t)m.n_cells * velb_stride(n), op.device_bytes);
@@ -1646,6 +1650,16 @@ namespace {
 
 int g_num_sms = 0;
 
+// slabs of the resident apply in one precision: the operator's setting, or 1
+// (one launch per colour over all layers)
+int apply_slabs(const Op &op, int precision)
+{
+  const Mesh &m = *op.mesh;
+  if (m.mapped || op.fine) return 1;
+  const int S = op.sched[precision].slabs > 0 ? op.sched[precision].slabs : 1;
+  return std::max(1, std::min(S, std::min(kMaxApplySlabs, m.nc[2] / 2)));
+}
+
 int num_sms()
 {
   if (g_num_sms == 0) {
@@ -1683,25 +1697,65 @@ void run_warp_apply(Op &op, KP<Real> k)
     configured_smem = (int)smem;
   }
   const long resident = (long)num_sms() * blocks_per_sm;
-  for (int c = 0; c < n_colours(m); ++c) {
-    const Colour &C = colours(m)[c];
-    if (C.count == 0) continue;
-    colour_params(k, C);
-    if (k.zhi > k.zlo) {
-      // the colour's cells are z-major: layers [zlo, zhi) are a contiguous
-      // run of colour-local indices, and the z parity absorbs the offset
-      const long plane = (long)C.cn[0] * C.cn[1];
-      const long m_lo = (k.zlo - C.par[2] + 1) / 2, m_hi = (k.zhi - C.par[2] + 1) / 2;
-      const long c_lo = std::min((long)C.count, m_lo * plane), c_hi = std::min((long)C.count, m_hi * plane);
-      if (c_hi <= c_lo) continue;
-      k.cfirst = C.first + c_lo;
-      k.ccount = c_hi - c_lo;
-      k.par[2] = C.par[2] + 2 * (int)m_lo;
+  constexpr int prec = sizeof(Real) == 4 ? MPDG_FP32 : MPDG_FP64;
+  k.stream_evict_first = op.sched[prec].evict_first;
+  const bool use_pdl = op.sched[prec].pdl != 0 && !HANG;
+  int launched = 0;
+  // the colour launches of cell layers [k.zlo, k.zhi) (all layers when empty)
+  auto colour_launches = [&](KP<Real> k) {
+    for (int c = 0; c < n_colours(m); ++c) {
+      const Colour &C = colours(m)[c];
+      if (C.count == 0) continue;
+      colour_params(k, C);
+      if (k.zhi > k.zlo) {
+        // the colour's cells are z-major: layers [zlo, zhi) are a contiguous
+        // run of colour-local indices, and the z parity absorbs the offset
+        const long plane = (long)C.cn[0] * C.cn[1];
+        const long m_lo = (k.zlo - C.par[2] + 1) / 2, m_hi = (k.zhi - C.par[2] + 1) / 2;
+        const long c_lo = std::min((long)C.count, m_lo * plane), c_hi = std::min((long)C.count, m_hi * plane);
+        if (c_hi <= c_lo) continue;
+        k.cfirst = C.first + c_lo;
+        k.ccount = c_hi - c_lo;
+        k.par[2] = C.par[2] + 2 * (int)m_lo;
+      }
+      const long groups = (k.ccount + CPW - 1) / CPW;
+      const long blocks = std::min(resident, (groups + kWarpsPerCTA - 1) / kWarpsPerCTA);
+      // colours after the first of an apply start as programmatic dependents of
+      // the previous colour: src and the coefficients are not written by it,
+      // and the kernel reads dst only after griddepcontrol.wait.  The first
+      // colour is ordered fully after whatever produced src.
+      const bool pdl = use_pdl && launched > 0;
+      k.pdl = pdl ? 1 : 0;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)blocks);
+      cfg.blockDim = dim3(kWarpsPerCTA * 32);
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = op.stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = pdl ? 1 : 0;
+      MPDG_CUDA(cudaLaunchKernelEx(&cfg, kern, k, op.d_err));
+      MPDG_LAUNCHED();
+      ++launched;
     }
-    const long groups = (k.ccount + CPW - 1) / CPW;
-    const long blocks = std::min(resident, (groups + kWarpsPerCTA - 1) / kWarpsPerCTA);
-    kern<<<(unsigned)blocks, kWarpsPerCTA * 32, smem, op.stream>>>(k, op.d_err);
-    MPDG_LAUNCHED();
+  };
+  // slab order: the 8 colours of one z-slab of cell layers before the next
+  // slab's, so that a slab's DoF vectors stay in L2 across its colours (the
+  // first-touch rule holds across slabs: interior slab ends are odd)
+  const int S = (k.zhi > k.zlo || HANG || MAPPED) ? 1 : apply_slabs(op, prec);
+  if (S <= 1) {
+    colour_launches(k);
+    return;
+  }
+  int bounds[kMaxApplySlabs + 1];
+  const int ns = slab_bounds(m.nc[2], S, bounds);
+  for (int sl = 0; sl < ns; ++sl) {
+    KP<Real> ks = k;
+    ks.zlo = bounds[sl];
+    ks.zhi = bounds[sl + 1];
+    colour_launches(ks);
   }
 }
 
@@ -2085,7 +2139,7 @@ void launch_apply(Op &op, Real *dst, const Real *src)
       if (op.io_tmp) cudaFree(op.io_tmp);
       op.io_tmp = nullptr;
       op.io_tmp_bytes = 0;
-      MPDG_CUDA(cudaMalloc(&op.io_tmp, bytes));
+      MPDG_CUDA(tracked_malloc(&op.io_tmp, bytes));
       op.io_tmp_bytes = bytes;
     }
     io_pre_kernel<Real><<<grid, 256, 0, op.stream>>>((Real *)op.io_tmp, src, op.d_io, N);
@@ -2161,6 +2215,96 @@ bool plain_warp_apply(const Op &op)
   const bool full = heat && D.full_tangent;
   return !op.fine && !m.mapped && !op.d_io && !faces && !supg(op) && !full && !uses_law(op) &&
          (!m.uniform || !uses_kT(op));
+}
+
+void set_wait_first_polls(long long polls)
+{
+  const long long v = polls < 0 ? (long long)kMbarSpinLimit : polls;
+  MPDG_CUDA(cudaMemcpyToSymbol(c_wait_first_polls, &v, sizeof(v)));
+}
+
+int slab_bounds(int nz, int S, int *bounds)
+{
+  S = std::max(1, std::min(S, std::min(kMaxApplySlabs, nz / 2)));
+  bounds[0] = 0;
+  for (int i = 1; i < S; ++i) {
+    const int b = (int)((long)i * nz / S) | 1;
+    bounds[i] = std::min(std::max(b, bounds[i - 1] + 1), nz - 1);
+  }
+  bounds[S] = nz;
+  for (int i = 1; i < S; ++i)
+    if (bounds[i] % 2 == 0 || bounds[i] <= bounds[i - 1] || bounds[i] >= nz)
+      throw Error{MPDG_ERR_ARG, "slab bounds"};
+  return S;
+}
+
+void autotune_apply(Op &op, int precision, int reps, ApplySchedule &best, double &best_ms,
+                    std::vector<double> *all_ms)
+{
+  Mesh &m = *op.mesh;
+  const size_t esz = precision == MPDG_FP32 ? sizeof(float) : sizeof(double);
+  const size_t bytes = esz * (size_t)m.N;
+  reps = std::max(1, reps);
+  // candidates: slabs 1, 2, 4, 8, 16 (as many as the layers allow), each with and
+  // without the evict-first hint where a coefficient stream exists
+  std::vector<ApplySchedule> cand;
+  const bool stream = !m.uniform || m.mapped;
+  for (int S : {1, 2, 4, 8}) {
+    if (S > 1 && (S > m.nc[2] / 2 || m.mapped || op.fine)) continue;
+    for (int h = 0; h <= (stream ? 1 : 0); ++h)
+      for (int d = 0; d <= 1; ++d) {
+        ApplySchedule c;
+        c.slabs = S;
+        c.evict_first = h;
+        c.pdl = d;
+        cand.push_back(c);
+      }
+  }
+  void *x = nullptr, *y = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  const ApplySchedule saved = op.sched[precision];
+  MPDG_CUDA(tracked_malloc(&x, bytes));
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(op.stream);
+    if (x) cudaFree(x);
+    if (y) cudaFree(y);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  try {
+    MPDG_CUDA(tracked_malloc(&y, bytes));
+    MPDG_CUDA(cudaEventCreate(&e0));
+    MPDG_CUDA(cudaEventCreate(&e1));
+    MPDG_CUDA(cudaMemsetAsync(x, 0, bytes, op.stream));
+    best_ms = -1.0;
+    if (all_ms) all_ms->clear();
+    for (const ApplySchedule &c : cand) {
+      op.sched[precision] = c;
+      auto apply = [&]() {
+        if (precision == MPDG_FP32) launch_apply<float>(op, (float *)y, (const float *)x);
+        else launch_apply<double>(op, (double *)y, (const double *)x);
+      };
+      apply();  // warm-up (first use of the schedule)
+      MPDG_CUDA(cudaEventRecord(e0, op.stream));
+      for (int r = 0; r < reps; ++r) apply();
+      MPDG_CUDA(cudaEventRecord(e1, op.stream));
+      MPDG_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      MPDG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      const double per = ms / reps;
+      if (all_ms) all_ms->push_back(per);
+      if (best_ms < 0.0 || per < best_ms) {
+        best_ms = per;
+        best = c;
+      }
+    }
+    op.sched[precision] = best;
+  } catch (...) {
+    op.sched[precision] = saved;
+    cleanup();
+    throw;
+  }
+  cleanup();
 }
 
 void launch_apply_zrange(Op &op, double *dst, const double *src, int z0, int z1)
@@ -2296,8 +2440,8 @@ void launch_composite_diagonal(Op &op, double *diag)
   f.use_dirichlet = op.use_dirichlet;
   launch_block_diagonal(f, diag + m.N_own);
   double *x = nullptr, *y = nullptr;
-  MPDG_CUDA(cudaMalloc(&x, sizeof(double) * m.N));
-  const cudaError_t e = cudaMalloc(&y, sizeof(double) * m.N);
+  MPDG_CUDA(tracked_malloc(&x, sizeof(double) * m.N));
+  const cudaError_t e = tracked_malloc(&y, sizeof(double) * m.N);
   if (e != cudaSuccess) {
     cudaFree(x);
     throw Error{MPDG_ERR_ALLOC, "diagonal probes"};
@@ -2349,8 +2493,8 @@ void launch_probe_diagonal(Op &op, double *diag)
 {
   Mesh &m = *op.mesh;
   double *x = nullptr, *y = nullptr;
-  MPDG_CUDA(cudaMalloc(&x, sizeof(double) * m.N));
-  const cudaError_t e = cudaMalloc(&y, sizeof(double) * m.N);
+  MPDG_CUDA(tracked_malloc(&x, sizeof(double) * m.N));
+  const cudaError_t e = tracked_malloc(&y, sizeof(double) * m.N);
   if (e != cudaSuccess) {
     cudaFree(x);
     throw Error{MPDG_ERR_ALLOC, "diagonal probes"};
@@ -2440,18 +2584,29 @@ void launch_invert_with_threshold(Op &op, double *diag, double thr)
   Mesh &m = *op.mesh;
   invert_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, constraint_mask(op), thr);
   MPDG_LAUNCHED();
+  if (op.d_io) {  // identity rows: inverse diagonal 1 (advection_diffusion_operator.cpp:438-445)
+    set_masked_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, op.d_io, 1.0);
+    MPDG_LAUNCHED();
+  }
 }
 
-bool apply_ready_without_allocation(const Op &op)
+const char *noalloc_unready_reason(const Op &op)
 {
-  if (op.fine && !apply_ready_without_allocation(*op.fine)) return false;
   const Mesh &m = *op.mesh;
   const bool full = op.d.kind == MPDG_OP_HEAT && op.d.full_tangent;
-  if (supg(op)) return false;                    // the diagonal probes allocate
-  if (m.mapped) return m.n_cons == 0;            // constraints: operand copy and element matrices
-  if (uses_law(op)) return true;                 // block kernel on raw geometry
-  if (!full && !m.uniform) return op.coef64_ok;  // merged stream already built
-  return true;                                   // nothing is built lazily on these paths
+  if (op.fine) return "two-level meshes are not supported (their diagonal probes allocate)";
+  if (supg(op)) return "SUPG operators are not supported (their diagonal probes allocate)";
+  if (op.d_io && op.io_tmp_bytes < sizeof(double) * (size_t)m.N)
+    return "the inflow/outflow copy of the operand is not built yet: call mpdg_vmult once first";
+  if (m.mapped) {
+    if (m.n_cons != 0) return "mapped meshes with constraints are not supported (operand copy, element matrices)";
+    if (uses_kT(op) || uses_law(op)) return nullptr;  // block kernel through the map
+    return op.coef64_ok ? nullptr : "the coefficient stream is not built yet: call mpdg_vmult once first";
+  }
+  if (uses_law(op)) return nullptr;  // block kernel on raw geometry
+  if (!full && !m.uniform && !op.coef64_ok)
+    return "the coefficient stream is not built yet: call mpdg_vmult once first";
+  return nullptr;  // nothing is built lazily on the other paths
 }
 
 }  // namespace mpdg
@@ -2531,9 +2686,9 @@ double l2_norm_integrated(Op &op, const double *u)
   const int blocks = 256;
   Colour *d_col = nullptr;
   double *partial = nullptr;
-  MPDG_CUDA(cudaMalloc(&d_col, sizeof(m.colour)));
+  MPDG_CUDA(tracked_malloc(&d_col, sizeof(m.colour)));
   MPDG_CUDA(cudaMemcpy(d_col, m.colour, sizeof(m.colour), cudaMemcpyHostToDevice));
-  MPDG_CUDA(cudaMalloc(&partial, sizeof(double) * blocks));
+  MPDG_CUDA(tracked_malloc(&partial, sizeof(double) * blocks));
   const double *met = m.uniform ? nullptr : m.d_metric64;
   switch (m.degree) {
     case 1: l2_cells_kernel<1><<<blocks, 256, 0, op.stream>>>(u, m.NX, m.NY, m.nc[0], m.nc[1], m.n_cells, d_col, m.d_cmap, met, m.h[0], m.h[1], m.h[2], partial); break;

@@ -36,7 +36,7 @@ double measure(int sms)
 {
   const int threads = 256, blocks = sms * 8, steps = 2048;
   Real *out = nullptr;
-  MPDG_CUDA(cudaMalloc(&out, sizeof(Real) * (size_t)threads * blocks));
+  MPDG_CUDA(tracked_malloc(&out, sizeof(Real) * (size_t)threads * blocks));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);

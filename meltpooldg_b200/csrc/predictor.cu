@@ -55,14 +55,14 @@ int predict_lsq(Op &op, int n_old, const double *const *old, const double *rhs, 
     if (op.lsq_buf) cudaFree(op.lsq_buf);
     op.lsq_buf = nullptr;
     op.lsq_cols = 0;
-    const cudaError_t e = cudaMalloc(&op.lsq_buf, sizeof(double) * (size_t)N * n_old);
+    const cudaError_t e = tracked_malloc(&op.lsq_buf, sizeof(double) * (size_t)N * n_old);
     if (e != cudaSuccess) throw Error{MPDG_ERR_ALLOC, "predictor images"};
     op.lsq_cols = n_old;
     op.device_bytes += sizeof(double) * (size_t)N * n_old;
   }
   DotScratch d;
-  MPDG_CUDA(cudaMalloc(&d.partial, sizeof(double) * kRedBlocks));
-  MPDG_CUDA(cudaMalloc(&d.out, sizeof(double)));
+  MPDG_CUDA(tracked_malloc(&d.partial, sizeof(double) * kRedBlocks));
+  MPDG_CUDA(tracked_malloc(&d.out, sizeof(double)));
   std::vector<double *> w(n_old);
   for (int i = 0; i < n_old; ++i) w[i] = op.lsq_buf + (size_t)i * N;
   // images of every old solution in passes of up to four vectors

@@ -41,7 +41,7 @@ template <typename T>
 T *walloc(Workspace &w, size_t count)
 {
   T *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  cudaError_t e = tracked_malloc(&p, count * sizeof(T));
   if (e != cudaSuccess) throw Error{MPDG_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
   w.bytes += count * sizeof(T);
   return p;
@@ -63,7 +63,7 @@ Workspace &ws64(Op &op)
     w.ct = walloc<double>(w, N);
     w.partial = walloc<double>(w, 64L * kRedBlocks);
     w.scal = walloc<double>(w, kNScalars + 64);
-    MPDG_CUDA(cudaMallocHost(&w.host, sizeof(double) * (kNScalars + 64)));
+    MPDG_CUDA(tracked_malloc_host(&w.host, sizeof(double) * (kNScalars + 64)));
   }
   return w;
 }
@@ -593,7 +593,7 @@ void free_workspace(Op &op)
 double linf(const double *a, long n, cudaStream_t s)
 {
   double *partial = nullptr, *out = nullptr, h = 0.0;
-  MPDG_CUDA(cudaMalloc(&partial, sizeof(double) * (kRedBlocks + 1)));
+  MPDG_CUDA(tracked_malloc(&partial, sizeof(double) * (kRedBlocks + 1)));
   out = partial + kRedBlocks;
   dev_linf(a, n, partial, out, s);
   MPDG_CUDA(cudaMemcpyAsync(&h, out, sizeof(double), cudaMemcpyDeviceToHost, s));

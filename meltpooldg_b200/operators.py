@@ -245,6 +245,34 @@ class _MatrixFreeOperator:
     def compute_diagonal(self, diag):
         A.check(A.lib().mpdg_compute_diagonal(self._h, _dptr(diag)), "compute_diagonal")
 
+    def set_schedule(self, slabs=1, l2_evict_first=False, precision="fp64", overlap_colours=False):
+        """Schedule of the resident apply (mpdg_op_set_schedule): colour launches
+        slab by slab over `slabs` z-slabs of cell layers, the L2 evict-first
+        hint on the coefficient stream, and colour launches that overlap the
+        previous colour's tail (programmatic dependent launch).  Results do not
+        depend on it."""
+        s = A.Schedule(int(slabs), int(bool(l2_evict_first)), int(bool(overlap_colours)))
+        A.check(A.lib().mpdg_op_set_schedule(self._h, A.FP32 if precision == "fp32" else A.FP64, C.byref(s)),
+                "mpdg_op_set_schedule")
+
+    def schedule(self, precision="fp64"):
+        s = A.Schedule()
+        A.check(A.lib().mpdg_op_get_schedule(self._h, A.FP32 if precision == "fp32" else A.FP64, C.byref(s)),
+                "mpdg_op_get_schedule")
+        return {"slabs": s.slabs, "l2_evict_first": bool(s.l2_evict_first),
+                "overlap_colours": bool(s.overlap_colours)}
+
+    def autotune(self, precision="fp64", reps=10):
+        """Times the candidate schedules of the resident apply (mpdg_op_autotune)
+        and keeps the fastest; returns (schedule, ms per apply, candidate times)."""
+        s = A.Schedule()
+        ms = C.c_double()
+        cand = (C.c_double * 32)()
+        A.check(A.lib().mpdg_op_autotune(self._h, A.FP32 if precision == "fp32" else A.FP64, int(reps),
+                                         C.byref(s), C.byref(ms), cand, 32), "mpdg_op_autotune")
+        return ({"slabs": s.slabs, "l2_evict_first": bool(s.l2_evict_first),
+                 "overlap_colours": bool(s.overlap_colours)}, ms.value, [c for c in cand if c >= 0.0])
+
     def device_error(self):
         """Reads and clears the device error word (an expired bounded wait)."""
         f = C.c_int()
