@@ -1,38 +1,35 @@
 """Benchmark of the matrix-free operators.
 
-Default workload (`--workload heat`, config 2):
-Workload (synthetic, seeded): unit cube, 64^3 hexahedra with interior vertices
-displaced by U[-0.1h, 0.1h] (PCG64 seed 2), FE_Q(4) (16,974,593 DoFs), heat
-operator M/dt + div(k(T) grad) with k(T) = k0 (1 + 1e-3 T), k0 = 1, rho c_p = 1,
-dt = 1e-3, T ~ U[300, 3000] (seed 3), Dirichlet T = 0 on all faces.
+Headline workload (config 2, `--workload heat`): unit cube, 64^3 hexahedra with
+interior vertices displaced by U[-0.1h, 0.1h] (PCG64 seed 2), FE_Q(4)
+(16,974,593 DoFs), heat operator M/dt + div(k(T) grad) with
+k(T) = k0 (1 + 1e-3 T), k0 = 1, rho c_p = 1, dt = 1e-3, T ~ U[300, 3000]
+(seed 3), Dirichlet T = 0 on all faces.  A step is one FP64 operator apply
+(vmult) with all data resident in HBM; value = DoFs x steps / time (whole job:
+N GPUs run independent replicas).  After the timed steps the same operator is
+solved with CG + Chebyshev(5)/Jacobi to a relative residual of 1e-10 in the
+plain FP64 form and in the FP32-inner / FP64-defect-correction form (solves/s,
+p50/p99 latency over repeated solves, and each form's true relative residual
+under the oracle's FP64 operator).
 
-A step is one FP64 operator apply (vmult) with all data resident in HBM; value =
-DoFs x steps / time (whole job: N GPUs run independent replicas).  After the
-timed steps the same operator is solved with CG + Chebyshev(5)/Jacobi to a
-relative residual of 1e-10 in the plain FP64 form and in the FP32-inner /
-FP64-defect-correction form (solves/s, iterations, error against the FP64
-solution, p50/p99 latency over repeated solves).
+With no --workload flag (N = 1) the line also carries, as extra keys, the
+other configurations measured in the same run:
+  c1  16^3 Q2 heat (35,937 DoFs): vmult (launch-latency bound), CG + Jacobi;
+  c3  128^3 Q2 advection-diffusion, vortex velocity, theta = 0.5, D = 1e-3:
+      vmult FP64 / FP32, one theta-scheme step of phi0 = tanh(d / 0.01)
+      solved with GMRES(30) + Jacobi in both forms;
+  c4  256 independent heat solves advanced together (batch_problems), against
+      the plain FP64 GPU form of the same problems;
+  c5  the Poisson request stream of serve_requests (20,000 requests at
+      200 req/s) served by the continuous-batching loop, plus a stream below
+      the device's capacity (engine latency without queueing), against the
+      plain FP64 GPU form.
 
-`--workload advdiff` (config 3): unit cube, 128^3 uniform cells, FE_Q(2)
-(16,974,593 DoFs), theta-scheme advection-diffusion (theta = 0.5, D = 1e-3,
-dt = 1e-3) with u = (sin pi x cos pi y, -cos pi x sin pi y, 0) evaluated in the
-kernel; the solve is one time step of phi0 = tanh(d / 0.01),
-d = 0.25 - |x - (0.5, 0.75, 0.5)|, with GMRES(30) + Jacobi to 1e-10 in FP64 and
-in FP32-inner / FP64-defect-correction form.
-
-`--workload c1` (config 1): unit cube, 16^3 uniform cells, FE_Q(2) (35,937
-DoFs), heat operator M/dt + Laplace (k = 1, dt = 1e-3), Dirichlet faces; one
-vmult per step (launch-latency bound), then CG + Jacobi to 1e-10 with
-b = A x*, x* ~ U[-1, 1] (seed 1).
-
-`--workload batch` (config 4): 256 independent heat solves advanced together
-(see `batch_problems`); `--workload serve` (config 5): a Poisson request
-stream served by the library's continuous-batching loop (see
-`serve_requests`), each against the plain FP64 GPU form.
-
-`--impl reference` times the CPU restatement of the reference's operator
-(the reference itself needs deal.II/Trilinos/p4est/MPI, which this image does
-not have) on a bounded sample of the same workload with all host threads.
+`--impl reference` times the tuned CPU port of the reference's operator
+(oracle/cpu_port.cpp: compile-time degree, SIMD over cell batches, OpenMP over
+colour-ordered batches, geometry and k(T_q) precomputed, -march=native): the
+reference itself needs deal.II/Trilinos/p4est/MPI, which this image does not
+have.  Each step is one full apply with all host threads.
 """
 from __future__ import annotations
 
@@ -50,10 +47,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "mat-free DoFs/s & solves/s, FP32+FP64-refined vs FP64 at 1e-10; p50/p99 latency"
-NC, DEGREE = [64, 64, 64], 4
 DT, K0, K_ALPHA = 1e-3, 1.0, 1e-3
-WORKLOAD = {"name": "heat"}
 THETA, DIFFUSIVITY = 0.5, 1e-3
+# the current single-operator workload: name ("heat" = config 2, "advdiff" =
+# config 3, "c1" = config 1), cells per direction and degree
+WL = {"name": "heat", "nc": [64, 64, 64], "degree": 4}
 
 # dram__bytes_read.sum + dram__bytes_write.sum of the FP64 warp apply kernel,
 # per apply (8 colour launches), heat workload at 64^3 cells: the 48^3 capture
@@ -63,14 +61,28 @@ THETA, DIFFUSIVITY = 0.5, 1e-3
 MEASURED_TRAFFIC_BYTES = {("heat", 64): 2.784e9}
 
 
+def set_workload(name, cells=0):
+    WL["name"] = name
+    if name == "advdiff":
+        WL["degree"], WL["nc"] = 2, [cells or 128] * 3
+    elif name == "c1":
+        WL["degree"], WL["nc"] = 2, [cells or 16] * 3
+    else:
+        WL["degree"], WL["nc"] = 4, [cells or 64] * 3
+
+
+def n_dofs_of():
+    return int(np.prod([n * WL["degree"] + 1 for n in WL["nc"]]))
+
+
 def algorithmic_bytes(n_dofs, n_cells, degree, real_bytes):
     """Algorithmic bytes of one apply (the accounting of the hot-path scope
     table): s (N_src + N_dst) + s N_aux + s G + 4 E, with N_aux = N (the
     temperature read for k(T)) and G = 10 geometry values per quadrature point
     (J^-T and JxW) on the perturbed heat mesh, and N_aux = G = 0 on the uniform
-    advection-diffusion mesh; 4 E = one cell index per cell."""
+    meshes; 4 E = one cell index per cell."""
     nq = (degree + 1) ** 3
-    if WORKLOAD["name"] in ("advdiff", "c1"):
+    if WL["name"] in ("advdiff", "c1"):
         return real_bytes * 2 * n_dofs + 4 * n_cells
     return real_bytes * (3 * n_dofs) + real_bytes * 10 * nq * n_cells + 4 * n_cells
 
@@ -81,7 +93,7 @@ def streamed_bytes(n_dofs, n_cells, degree, real_bytes):
     entries of c_diff k(T_q) JxW J^-1 J^-T per quadrature point, which folds the
     temperature and the geometry into 7 values)."""
     nq = (degree + 1) ** 3
-    if WORKLOAD["name"] in ("advdiff", "c1"):
+    if WL["name"] in ("advdiff", "c1"):
         return real_bytes * 2 * n_dofs
     return real_bytes * (2 * n_dofs) + real_bytes * 7 * nq * n_cells
 
@@ -91,7 +103,7 @@ def algorithmic_flops(n_cells, degree):
     roofline): E (24 n^4 + c_q n^3), c_q = 20 on Cartesian heat cells, 45 on
     general geometry (the J^-T transforms), 60 with the analytic velocity."""
     n = degree + 1
-    c_q = {"advdiff": 60, "c1": 20}.get(WORKLOAD["name"], 45)
+    c_q = {"advdiff": 60, "c1": 20}.get(WL["name"], 45)
     return n_cells * (24 * n ** 4 + c_q * n ** 3)
 
 
@@ -119,7 +131,7 @@ class ClockSampler:
     def __init__(self, gpu):
         self.gpu = gpu
         self.proc = None
-        self.path = os.path.join("/tmp", f"mpdg_clocks_{os.getpid()}.csv")
+        self.path = os.path.join("/tmp", f"mpdg_clocks_{os.getpid()}_{id(self)}.csv")
 
     def __enter__(self):
         try:
@@ -185,135 +197,162 @@ def replica_throughput(units_per_rank, world, t_job):
     return units_per_rank * world / t_job
 
 
-def build_problem():
-    import meltpooldg_b200 as M
-    if WORKLOAD["name"] == "advdiff":
-        V = M.box_vertices(NC)
-        mesh = M.Mesh(V, NC, DEGREE, None)
-        return M, V, None, mesh, None
-    if WORKLOAD["name"] == "c1":
-        V = M.box_vertices(NC)
-        mask = M.boundary_mask(NC, DEGREE)
-        return M, V, mask, M.Mesh(V, NC, DEGREE, mask), None
-    V = M.box_vertices(NC, perturb=0.1, seed=2)
-    mask = M.boundary_mask(NC, DEGREE)
-    mesh = M.Mesh(V, NC, DEGREE, mask)
-    T = np.random.Generator(np.random.PCG64(3)).uniform(300.0, 3000.0, mesh.n_dofs)
-    return M, V, mask, mesh, T
+def percentiles(lat_s):
+    lat = np.sort(np.asarray(lat_s, dtype=np.float64))
+    return {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "max_ms": 1e3 * float(lat[-1]), "samples": int(lat.size)}
+
+
+# ------------------------------------------------------------ problem set-up
+def mesh_inputs():
+    """(vertices, Dirichlet mask or None, temperature or None) of the workload."""
+    from meltpooldg_b200.operators import box_vertices, boundary_mask
+    nc, p = WL["nc"], WL["degree"]
+    if WL["name"] == "advdiff":
+        return box_vertices(nc), None, None
+    if WL["name"] == "c1":
+        return box_vertices(nc), boundary_mask(nc, p), None
+    V = box_vertices(nc, perturb=0.1, seed=2)
+    T = np.random.Generator(np.random.PCG64(3)).uniform(300.0, 3000.0, n_dofs_of())
+    return V, boundary_mask(nc, p), T
 
 
 def make_operator(M, mesh, T):
     import torch
-    if WORKLOAD["name"] == "advdiff":
+    if WL["name"] == "advdiff":
         return M.AdvectionDiffusionOperator(mesh, DT, theta=THETA, diffusivity=DIFFUSIVITY,
                                             velocity="vortex", precisions=("fp64", "fp32")), None
-    if WORKLOAD["name"] == "c1":
+    if WL["name"] == "c1":
         return M.HeatDiffuseOperator(mesh, DT, rho_cp=1.0, k0=1.0, precisions=("fp64", "fp32")), None
-    op = M.HeatDiffuseOperator(mesh, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA,
-                               precisions=("fp64", "fp32"))
+    op = M.HeatDiffuseOperator(mesh, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA, precisions=("fp64", "fp32"))
     Td = torch.tensor(T, device="cuda")
     op.set_temperature(Td)
     return op, Td
 
 
-def oracle_operator(O, T, mask):
-    if WORKLOAD["name"] == "advdiff":
-        return O.Operator(O.ADVDIFF, DT, theta=THETA, diffusivity=DIFFUSIVITY, vel_kind=O.VEL_VORTEX)
-    if WORKLOAD["name"] == "c1":
-        return O.Operator(O.HEAT, DT, rho_cp=1.0, k0=1.0, dirichlet=mask)
-    return O.Operator(O.HEAT, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA, temperature=T, dirichlet=mask)
+def workload_config():
+    N, E = n_dofs_of(), int(np.prod(WL["nc"]))
+    name = {"advdiff": "advection-diffusion operator apply, Q2, 128^3 uniform hex cells, vortex velocity, "
+                       "theta=0.5, D=1e-3",
+            "c1": "heat operator apply, Q2, 16^3 uniform hex cells, k=1, dt=1e-3, Dirichlet faces",
+            }.get(WL["name"], "heat operator apply, Q4, 64^3 perturbed hex cells, k(T)=k0(1+1e-3T)")
+    return {"workload": name, "n_dofs": N, "cells": E, "degree": WL["degree"]}
 
 
-def workload_config(N, E):
-    if WORKLOAD["name"] == "advdiff":
-        return {"workload": "advection-diffusion operator apply, Q2, 128^3 uniform hex cells, "
-                            "vortex velocity, theta=0.5, D=1e-3",
-                "n_dofs": N, "cells": E, "degree": DEGREE}
-    if WORKLOAD["name"] == "c1":
-        return {"workload": "heat operator apply, Q2, 16^3 uniform hex cells, k=1, dt=1e-3, Dirichlet faces",
-                "n_dofs": N, "cells": E, "degree": DEGREE}
-    return {"workload": "heat operator apply, Q4, 64^3 perturbed hex cells, k(T)=k0(1+1e-3T)",
-            "n_dofs": N, "cells": E, "degree": DEGREE}
+# ------------------------------------------------------------ CPU legs (port and oracle)
+def port_operator():
+    """The tuned CPU port of the workload's operator (oracle/cpu_port.cpp)."""
+    from oracle import cpu_port as P
+    V, mask, T = mesh_inputs()
+    nc, p = WL["nc"], WL["degree"]
+    if WL["name"] == "advdiff":
+        return P.PortOperator(V, nc, p, None, uniform=True, kind=1, dt=DT, theta=THETA, diffusivity=DIFFUSIVITY,
+                              velocity="vortex")
+    if WL["name"] == "c1":
+        return P.PortOperator(V, nc, p, mask, uniform=True, kind=0, dt=DT, rho_cp=1.0, k0=1.0)
+    return P.PortOperator(V, nc, p, mask, uniform=False, kind=0, dt=DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA,
+                          temperature=T)
 
 
-def cpu_reference_rate(V, T, mask, n_dofs, target_seconds=10.0, cell_fraction=None):
-    """Oracle apply over a contiguous block of cells; returns (DoFs/s, sample text, threads)."""
+def cpu_apply_rate(seconds=5.0, port=None):
+    """The port's full applies on all host threads for about `seconds` (after 3
+    warm-up applies); returns the cpu_baseline dict."""
+    from oracle import cpu_port as P
+    own = port is None
+    port = port or port_operator()
+    N = port.n_dofs
+    src = np.random.Generator(np.random.PCG64(0)).uniform(-1.0, 1.0, N)
+    dst = np.zeros(N)
+    for _ in range(3):
+        port.vmult(dst, src)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        port.vmult(dst, src)
+        reps += 1
+        dt = time.perf_counter() - t0
+        if dt > seconds:
+            break
+    if own:
+        port.close()
+    return {"value": N * reps / dt, "unit": "DoFs/s", "cores": P.threads(), "kind": "port",
+            "sample": f"{reps} full applies of the workload in {dt:.2f} s (after 3 untimed), "
+                      "tuned C++ port (oracle/cpu_port.cpp, -O3 -march=native, OpenMP)"}
+
+
+def oracle_true_residual(b_host, x_host):
+    """|b - A x| / |b| with A the oracle's FP64 operator of the workload: the
+    error of a device solve stated against the oracle."""
     from oracle import oracle as O
-    om = O.Mesh(3, DEGREE, NC, V)
-    op = oracle_operator(O, T, mask)
-    src = np.random.Generator(np.random.PCG64(0)).uniform(-1.0, 1.0, n_dofs)
-    n_cells = int(np.prod(NC))
-    # calibrate on a small block, then time a block of ~target_seconds
-    c = 256
-    t0 = time.perf_counter()
-    O.vmult_cells(om, op, src, 0, c)
-    dt = time.perf_counter() - t0
-    if cell_fraction is None:
-        c = int(min(n_cells, max(256, c * target_seconds / max(dt, 1e-6))))
+    V, mask, T = mesh_inputs()
+    om = O.Mesh(3, WL["degree"], WL["nc"], V)
+    if WL["name"] == "advdiff":
+        oop = O.Operator(O.ADVDIFF, DT, theta=THETA, diffusivity=DIFFUSIVITY, vel_kind=O.VEL_VORTEX)
+    elif WL["name"] == "c1":
+        oop = O.Operator(O.HEAT, DT, rho_cp=1.0, k0=1.0, dirichlet=mask)
     else:
-        c = max(1, int(n_cells * cell_fraction))
-    t0 = time.perf_counter()
-    O.vmult_cells(om, op, src, 0, c)
-    dt = time.perf_counter() - t0
-    rate = n_dofs * (c / n_cells) / dt
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return rate, f"{c} of {n_cells} cells of one apply ({dt:.2f} s)", threads, dt
+        oop = O.Operator(O.HEAT, DT, rho_cp=1.0, k0=K0, k_alpha=K_ALPHA, temperature=T, dirichlet=mask)
+    r = b_host - O.vmult(om, oop, x_host)
+    return float(np.linalg.norm(r) / np.linalg.norm(b_host))
 
 
+# ------------------------------------------------------------ reference arm
 def run_reference(args, rank, world):
+    """The reference's CPU path, restated as the tuned port, on the headline
+    workload: each step one full apply with all host threads."""
     if rank != 0:
         return
-    from meltpooldg_b200.operators import box_vertices, boundary_mask
-    n_dofs = int(np.prod([n * DEGREE + 1 for n in NC]))
-    if WORKLOAD["name"] == "advdiff":
-        V, mask, T = box_vertices(NC), None, None
-    elif WORKLOAD["name"] == "c1":
-        V, mask, T = box_vertices(NC), boundary_mask(NC, DEGREE), None
-    else:
-        V = box_vertices(NC, perturb=0.1, seed=2)
-        mask = boundary_mask(NC, DEGREE)
-        T = np.random.Generator(np.random.PCG64(3)).uniform(300.0, 3000.0, n_dofs)
-    # each step: a fixed sample of cells, sized so the whole run takes ~2.5 minutes
-    per_step = max(0.05, min(4.0, 150.0 / (args.steps + args.warmup)))
-    _, _, _, _ = cpu_reference_rate(V, T, mask, n_dofs, target_seconds=0.5)
-    rate0, sample, threads, dt0 = cpu_reference_rate(V, T, mask, n_dofs, target_seconds=per_step)
-    frac = float(sample.split(" of ")[0]) / np.prod(NC)
-    for _ in range(args.warmup):
-        cpu_reference_rate(V, T, mask, n_dofs, cell_fraction=frac)
+    from oracle import cpu_port as P
+    port = port_operator()
+    N = port.n_dofs
+    src = np.random.Generator(np.random.PCG64(0)).uniform(-1.0, 1.0, N)
+    dst = np.zeros(N)
+    for _ in range(max(args.warmup, 3)):
+        port.vmult(dst, src)
     times = []
     for _ in range(args.steps):
-        r, _, _, dt = cpu_reference_rate(V, T, mask, n_dofs, cell_fraction=frac)
-        times.append(dt)
+        t0 = time.perf_counter()
+        port.vmult(dst, src)
+        times.append(time.perf_counter() - t0)
+    port.close()
     tot = sum(times)
-    value = n_dofs * frac * args.steps / tot
+    value = N * args.steps / tot
+    cores = P.threads()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "DoFs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": dict(workload_config(n_dofs, int(np.prod(NC))),
-                       sample=f"{frac:.5f} of the cells per step"),
-        "cpu_baseline": {"value": value, "unit": "DoFs/s", "cores": threads, "kind": "port",
-                         "sample": f"{frac * np.prod(NC):.0f} cells of one apply per step"},
+        "data": "synthetic", "config": dict(workload_config(), parallelism=f"OpenMP x{cores}"),
+        "cpu_baseline": {"value": value, "unit": "DoFs/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} full applies of the workload (one per step)"},
         "e2e": {"value": value, "unit": "DoFs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "CPU restatement of the reference's operator (oracle/); the reference needs "
-                "deal.II + Trilinos + p4est + MPI, absent from this image",
+        "note": "tuned C++ port of the reference's operator (oracle/cpu_port.cpp: compile-time degree, "
+                "SIMD batches of 8 cells, OpenMP over colour-ordered batches, geometry and k(T_q) "
+                "precomputed, -O3 -march=native); the reference needs deal.II + Trilinos + p4est + MPI, "
+                "absent from this image",
     }
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, rank, world):
+# ------------------------------------------------------------ single-operator workloads
+def run_operator_workload(args, rank, world, headline):
+    """One apply workload (config 2, 3 or 1): timed FP64 applies, FP32 applies,
+    the multi-vector pass, the host-buffer e2e apply, the solves, the CPU
+    baseline.  Returns the line's dict (printed by the caller)."""
     import torch
     import torch.distributed as dist
+    import meltpooldg_b200 as M
     local = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(local)
-    M, V, mask, mesh, T = build_problem()
+    V, mask, T = mesh_inputs()
+    nc, p = WL["nc"], WL["degree"]
+    mesh = M.Mesh(V, nc, p, mask)
     N = mesh.n_dofs
     op, Td = make_operator(M, mesh, T)
     rng = np.random.Generator(np.random.PCG64(0))
     src = torch.tensor(rng.uniform(-1.0, 1.0, N), device="cuda")
     dst = torch.empty_like(src)
     src32, dst32 = src.float(), torch.empty(N, dtype=torch.float32, device="cuda")
+    steps = args.steps if headline else max(20, min(args.steps, 200))
 
     def barrier():
         if world > 1:
@@ -329,7 +368,7 @@ def run_ours(args, rank, world):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             op.vmult(dst, src)
         e1.record(stream)
         torch.cuda.synchronize()
@@ -337,35 +376,37 @@ def run_ours(args, rank, world):
     barrier()
     t = e0.elapsed_time(e1) / 1e3
     t_max = job_seconds(t, world)
-    value = replica_throughput(N * args.steps, world, t_max)
-    apply_s = t / args.steps
+    value = replica_throughput(N * steps, world, t_max)
+    apply_s = t / steps
 
     # FP32 apply
     for _ in range(3):
         op.vmult(dst32, src32)
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         op.vmult(dst32, src32)
     e1.record(stream)
     torch.cuda.synchronize()
-    apply32_s = e0.elapsed_time(e1) / 1e3 / args.steps
+    apply32_s = e0.elapsed_time(e1) / 1e3 / steps
 
-    # multi-vector apply: 4 operands per pass share one read of the coefficients
-    # (the images of the least-squares predictor, mpdg_vmult_multi)
-    srcs = [src] + [torch.roll(src, 7 * v) for v in range(1, 4)]
-    dsts = [dst] + [torch.empty_like(src) for _ in range(3)]
-    for _ in range(3):
-        op.vmult_multi(dsts, srcs)
-    multi_steps = max(3, args.steps // 4)
-    e0.record(stream)
-    for _ in range(multi_steps):
-        op.vmult_multi(dsts, srcs)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    multi_s = e0.elapsed_time(e1) / 1e3 / multi_steps
-    multi = {"vectors": 4, "ms_per_pass": 1e3 * multi_s, "value": 4 * N / multi_s, "unit": "DoFs/s",
-             "speedup_vs_4_single_applies": 4 * apply_s / multi_s}
-    del srcs, dsts
+    multi = None
+    if headline:
+        # multi-vector apply: 4 operands per pass share one read of the
+        # coefficients (the images of the least-squares predictor, mpdg_vmult_multi)
+        srcs = [src] + [torch.roll(src, 7 * v) for v in range(1, 4)]
+        dsts = [dst] + [torch.empty_like(src) for _ in range(3)]
+        for _ in range(3):
+            op.vmult_multi(dsts, srcs)
+        multi_steps = max(3, steps // 4)
+        e0.record(stream)
+        for _ in range(multi_steps):
+            op.vmult_multi(dsts, srcs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        multi_s = e0.elapsed_time(e1) / 1e3 / multi_steps
+        multi = {"vectors": 4, "ms_per_pass": 1e3 * multi_s, "value": 4 * N / multi_s, "unit": "DoFs/s",
+                 "speedup_vs_4_single_applies": 4 * apply_s / multi_s}
+        del srcs, dsts
 
     # end to end through the host-buffer C-ABI call (pinned host buffers)
     e2e_s = float("nan")
@@ -375,32 +416,27 @@ def run_ours(args, rank, world):
         hsrc.copy_(src.cpu())
         hs, hd = hsrc.numpy(), hdst.numpy()
         op.vmult_host(hd, hs)
-        e2e_steps = max(3, min(50, args.steps // 2))
+        e2e_steps = max(3, min(50, steps // 2))
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             op.vmult_host(hd, hs)
         e2e_s = (time.perf_counter() - t0) / e2e_steps
 
     peak, peak_kind = load_peaks()
-    E = int(np.prod(NC))
+    E = int(np.prod(nc))
     f64_peak, f32_peak = fma_peaks(M)
-    flops = algorithmic_flops(E, DEGREE)
-    geom = "UNIFORM" if WORKLOAD["name"] in ("advdiff", "c1") else "GENERAL"
-    kernel_name = f"warp_apply_kernel<{DEGREE},double,{geom}> x 8 colour launches"
-    b64 = algorithmic_bytes(N, E, DEGREE, 8)
-    b32 = algorithmic_bytes(N, E, DEGREE, 4)
-    st64 = streamed_bytes(N, E, DEGREE, 8)
-    st32 = streamed_bytes(N, E, DEGREE, 4)
-    traffic = MEASURED_TRAFFIC_BYTES.get((WORKLOAD["name"], NC[0]))
+    flops = algorithmic_flops(E, p)
+    geom = "UNIFORM" if WL["name"] in ("advdiff", "c1") else "GENERAL"
+    b64, b32 = algorithmic_bytes(N, E, p, 8), algorithmic_bytes(N, E, p, 4)
+    st64, st32 = streamed_bytes(N, E, p, 8), streamed_bytes(N, E, p, 4)
+    traffic = MEASURED_TRAFFIC_BYTES.get((WL["name"], nc[0]))
     roof = {"bound": "hbm", "achieved": b64 / apply_s / 1e9, "peak": peak, "unit": "GB/s",
-            "frac": b64 / apply_s / 1e9 / peak,
-            "traffic": traffic,
+            "frac": b64 / apply_s / 1e9 / peak, "traffic": traffic,
             "traffic_note": None if traffic is None else
             "ncu dram read+write per apply (8 launches), 48^3 capture scaled by cells",
-            "algorithmic_bytes": b64, "kernel": kernel_name,
+            "algorithmic_bytes": b64, "kernel": f"warp_apply_kernel<{p},double,{geom}> x 8 colour launches",
             "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
-            "streamed": {"bytes": st64, "achieved": st64 / apply_s / 1e9,
-                         "frac": st64 / apply_s / 1e9 / peak},
+            "streamed": {"bytes": st64, "achieved": st64 / apply_s / 1e9, "frac": st64 / apply_s / 1e9 / peak},
             "fp32": {"achieved": b32 / apply32_s / 1e9, "frac": b32 / apply32_s / 1e9 / peak,
                      "algorithmic_bytes": b32, "streamed_bytes": st32,
                      "streamed_frac": st32 / apply32_s / 1e9 / peak},
@@ -411,12 +447,12 @@ def run_ours(args, rank, world):
                                "frac": flops / apply32_s / 1e9 / f32_peak},
                       "peak_source": "mpdg_fma_peak: FMA chains measured on this GPU (8 per thread, 8 CTAs per SM)"}}
 
-    # solves: CG + Chebyshev(5)/Jacobi to 1e-10, FP64 and FP32-inner/FP64-refined
-    solves = None
+    # solves to 1e-10 in the plain FP64 form and the FP32-inner / FP64-refined form
+    solves, solve_io = None, None
     if not args.no_solve:
-        if WORKLOAD["name"] == "advdiff":
+        if WL["name"] == "advdiff":
             # one theta-scheme step of the tanh level set
-            X = [np.linspace(0.0, 1.0, n * DEGREE + 1) for n in NC]  # Q2 Gauss-Lobatto nodes are uniform
+            X = [np.linspace(0.0, 1.0, n * p + 1) for n in nc]  # Q2 Gauss-Lobatto nodes are uniform
             Z, Y, Xg = np.meshgrid(X[2], X[1], X[0], indexing="ij")
             d = 0.25 - np.sqrt((Xg - 0.5) ** 2 + (Y - 0.75) ** 2 + (Z - 0.5) ** 2)
             phi0 = torch.tensor(np.tanh(d / 0.01).reshape(-1), device="cuda")
@@ -425,69 +461,79 @@ def run_ours(args, rank, world):
             xs = None
             solver_type, prec = "GMRES", "Diagonal"
         else:
-            seed = 1 if WORKLOAD["name"] == "c1" else 5
+            seed = 1 if WL["name"] == "c1" else 5
             xs = torch.tensor(np.random.Generator(np.random.PCG64(seed)).uniform(-1, 1, N), device="cuda")
             xs[torch.tensor(mask.astype(bool), device="cuda")] = 0.0
             b = torch.empty_like(xs)
             op.vmult(b, xs)
-            solver_type, prec = ("CG", "Diagonal") if WORKLOAD["name"] == "c1" else ("CG", "Chebyshev")
-        solves = {"solver": f"{solver_type} + {prec}"}
+            solver_type, prec = ("CG", "Diagonal") if WL["name"] == "c1" else ("CG", "Chebyshev")
+        solves = {"solver": f"{solver_type} + {prec}",
+                  "timing": f"wall clock per solve, {args.solve_reps} solves after one untimed warm-up solve"}
+        solve_io = {"b": b.cpu().numpy(), "x": {}}
         ref_x = None
         for form, mixed in (("fp64", False), ("fp32_refined", True)):
             data = M.LinearSolverData(solver_type=solver_type, preconditioner_type=prec,
                                       rel_tolerance=1e-10, abs_tolerance=1e-20, mixed_precision=mixed)
             lat = []
             rep = None
-            for r in range(args.solve_reps):
+            for r in range(args.solve_reps + 1):
                 x = torch.zeros_like(b)
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
                 M.LinearSolver.solve(op, x, b, data)
                 torch.cuda.synchronize()
-                lat.append(time.perf_counter() - t0)
+                if r > 0:
+                    lat.append(time.perf_counter() - t0)
                 rep = dict(M.LinearSolver.last_report)
             if ref_x is None:
                 ref_x = x.clone()
+            solve_io["x"][form] = x.cpu().numpy()
             err = float((x - ref_x).abs().max() / ref_x.abs().max())
-            lat.sort()
-            solves[form] = {
-                "solves_per_s": world / statistics.median(lat),
-                "p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
-                "iterations": rep["iterations"], "outer_iterations": rep["outer_iterations"],
-                "operator_applies": rep["operator_applies"],
-                "relative_residual": rep["final_residual"] / rep["initial_residual"],
-                "max_rel_error_vs_fp64_solution": err,
-                "max_rel_error_vs_exact": None if xs is None else float((x - xs).abs().max() / xs.abs().max()),
-            }
+            solves[form] = dict(
+                percentiles(lat), solves_per_s=world / statistics.median(lat),
+                iterations=rep["iterations"], outer_iterations=rep["outer_iterations"],
+                operator_applies=rep["operator_applies"],
+                relative_residual=rep["final_residual"] / rep["initial_residual"],
+                lambda_max=rep["lambda_max"] or None,
+                max_rel_error_vs_fp64_solution=err,
+                max_rel_error_vs_exact=None if xs is None else float((x - xs).abs().max() / xs.abs().max()))
         solves["speedup_fp32_refined_vs_fp64"] = (solves["fp32_refined"]["solves_per_s"] /
                                                   solves["fp64"]["solves_per_s"])
+    sched64, sched32 = op.schedule("fp64"), op.schedule("fp32")
+    op.close()
+    mesh.close()
+    del src, dst, src32, dst32, Td
+    torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        rate, sample, threads, _ = cpu_reference_rate(V, T, mask, N, target_seconds=args.cpu_seconds)
-        cpu = {"value": rate, "unit": "DoFs/s", "cores": threads, "kind": "port", "sample": sample}
+        cpu = cpu_apply_rate(args.cpu_seconds)
+        if solve_io is not None:
+            # the CPU checker's view of every device solve: the true relative
+            # residual under the oracle's FP64 operator
+            for form, xh in solve_io["x"].items():
+                solves[form]["true_relative_residual_vs_oracle"] = oracle_true_residual(solve_io["b"], xh)
 
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "DoFs/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(workload_config(N, E), parallelism=f"replicas x{world}",
-                           l2={"advdiff": "inputs larger than L2: src/dst 2 x 136 MB",
-                               "c1": "inputs smaller than L2 (0.6 MB): launch-latency bound, L2 not flushed",
-                               }.get(WORKLOAD["name"], "inputs larger than L2: coefficient stream 1.8 GB per apply")),
-            "roofline": roof,
-            "cpu_baseline": cpu,
-            "e2e": None if args.no_e2e else {
-                "value": N / e2e_s, "unit": "DoFs/s", "h2d_bytes_per_step": 8 * N,
-                "d2h_bytes_per_step": 8 * N, "call": "mpdg_vmult_host (pinned host buffers)"},
-            "fp32_apply": {"value": N / apply32_s, "unit": "DoFs/s"},
-            "multi_apply": multi,
-            "solves": solves,
-            "gpu_launches": launches,
-            "clocks": clk.summary(),
-        }
-        print(json.dumps(line), flush=True)
+    return {
+        "metric": METRIC, "value": value, "unit": "DoFs/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_max / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(workload_config(), parallelism=f"replicas x{world}",
+                       l2={"advdiff": "inputs larger than L2: src/dst 2 x 136 MB",
+                           "c1": "inputs smaller than L2 (0.6 MB): launch-latency bound, L2 not flushed",
+                           }.get(WL["name"], "inputs larger than L2: coefficient stream 1.8 GB per apply"),
+                       schedule={"fp64": sched64, "fp32": sched32}),
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": None if args.no_e2e else {
+            "value": N / e2e_s, "unit": "DoFs/s", "h2d_bytes_per_step": 8 * N,
+            "d2h_bytes_per_step": 8 * N, "call": "mpdg_vmult_host (pinned host buffers)"},
+        "fp32_apply": {"value": N / apply32_s, "unit": "DoFs/s", "ms_per_apply": 1e3 * apply32_s},
+        "multi_apply": multi,
+        "solves": solves,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
 
 
 # ----------------------------------------------------------------- batched solves
@@ -510,13 +556,13 @@ def batch_problems(n=BATCH_SIZE):
     return out
 
 
-def serve_requests(n_req, rate=200.0):
+def serve_requests(n_req, rate=200.0, seed=7):
     """Poisson arrivals (mean rate req/s, PCG64 seed 7): cells n^3 with
     n = min(96, round(LogNormal(ln 24, 0.5))), degree ~ U{2,3,4}, half heat
     (k0 = 1, rho c_p = 1) and half advection-diffusion (vortex velocity,
     theta = 0.5, D = 1e-3), dt = 1e-3, tolerance 1e-10, seeds 1000 + i."""
     from meltpooldg_b200 import batch as B
-    rng = np.random.Generator(np.random.PCG64(7))
+    rng = np.random.Generator(np.random.PCG64(seed))
     arr = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
     out = []
     for i in range(n_req):
@@ -564,6 +610,7 @@ def run_batch(args, rank, world):
     n_dofs = [p.n_dofs for p in probs]
     N_total = int(sum(n_dofs))
     budget = 150 * 10**9
+    steps = args.batch_steps
 
     def one_batch(e2e=False, tune=False, keep=False):
         rhs = [p.rhs() for p in probs] if e2e else None
@@ -572,10 +619,10 @@ def run_batch(args, rank, world):
         with B.Batch(budget, capacity=len(probs)) as bt:
             ts = [bt.submit(p, rhs=rhs[i] if e2e else None) for i, p in enumerate(probs)]
             tune_res = bt.autotune() if tune else None
-            steps, _ = bt.run(poll_steps=16)
+            gsteps, _ = bt.run(poll_steps=16)
             res = [bt.take(t, p.n_dofs if (e2e or keep) else None) for t, p in zip(ts, probs)]
         t1 = time.perf_counter()
-        return t1 - t0, steps, res, tune_res
+        return t1 - t0, gsteps, res, tune_res
 
     # warm-up (also the autotuner's pass over this membership)
     _, _, _, tune_res = one_batch(tune=True)
@@ -585,7 +632,7 @@ def run_batch(args, rank, world):
     launches0 = M.kernel_launches()
     times, graph_steps = [], []
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             dt, st, res, _ = one_batch()
             times.append(dt)
             graph_steps.append(st)
@@ -618,64 +665,62 @@ def run_batch(args, rank, world):
     cpu = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_batch_rate(probs, its64, args.cpu_seconds)
-    if rank == 0:
-        iters = [r["iterations"] for r in reps]
-        line = {
-            "metric": "batched heat solves/s at 1e-10 (FP32 apply, FP64 residuals)", "value": value,
-            "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 apply / f64 residuals", "data": "synthetic",
-            "config": {"workload": f"{len(probs)} heat solves, n^3 cells n~U{{8..48}}, Q2/Q3/Q4, k0 log-uniform [1,100], "
-                                   "dt=1e-3, seeded rhs, CG + Jacobi to 1e-10",
-                       "n_dofs_total": N_total, "problems": len(probs),
-                       "l2": f"inputs larger than L2: {N_total * 44 / 1e9:.1f} GB resident",
-                       "timing": "host clock around synchronous batch calls (admission to release)"},
-            "roofline": roof, "cpu_baseline": cpu,
-            "e2e": {"value": len(probs) / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": 8 * N_total,
-                    "d2h_bytes_per_step": 8 * N_total,
-                    "call": "mpdg_batch_submit (host rhs) / mpdg_batch_run / mpdg_batch_take (host x)"},
-            "fp64_plain": {"solves_per_s": len(probs) / t64, "seconds": t64,
-                           "iterations_mean": float(np.mean(its64)),
-                           "speedup_batched_vs_fp64": value / (len(probs) / t64)},
-            "batched": {"graph_steps": graph_steps[-1], "iterations_mean": float(np.mean(iters)),
-                        "iterations_max": int(max(iters)),
-            "all_converged": all(r["status"] == 0 for r in reps),
-                        "max_rel_residual": max(r["final_residual"] / r["initial_residual"] for r in reps),
-                        "max_rel_error_vs_fp64_solution": max(errs),
-                        "iteration_diff_vs_fp64_max": int(max(abs(a - b) for a, b in zip(iters, its64)))},
-            "gpu_launches": launches,
-            "clocks": clk.summary(),
-        }
-        print(json.dumps(line), flush=True)
+    iters = [r["iterations"] for r in reps]
+    return {
+        "metric": "batched heat solves/s at 1e-10 (FP32 apply, FP64 residuals)", "value": value,
+        "unit": "solves/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 apply / f64 residuals", "data": "synthetic",
+        "config": {"workload": f"{len(probs)} heat solves, n^3 cells n~U{{8..48}}, Q2/Q3/Q4, k0 log-uniform [1,100], "
+                               "dt=1e-3, seeded rhs, CG + Jacobi to 1e-10",
+                   "n_dofs_total": N_total, "problems": len(probs),
+                   "l2": f"inputs larger than L2: {N_total * 44 / 1e9:.1f} GB resident",
+                   "timing": "host clock around synchronous batch calls (admission to release)"},
+        "roofline": roof, "cpu_baseline": cpu,
+        "e2e": {"value": len(probs) / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": 8 * N_total,
+                "d2h_bytes_per_step": 8 * N_total,
+                "call": "mpdg_batch_submit (host rhs) / mpdg_batch_run / mpdg_batch_take (host x)"},
+        "fp64_plain": {"solves_per_s": len(probs) / t64, "seconds": t64,
+                       "iterations_mean": float(np.mean(its64)),
+                       "speedup_batched_vs_fp64": value / (len(probs) / t64)},
+        "batched": {"graph_steps": graph_steps[-1], "iterations_mean": float(np.mean(iters)),
+                    "iterations_max": int(max(iters)),
+                    "all_converged": all(r["status"] == 0 for r in reps),
+                    "max_rel_residual": max(r["final_residual"] / r["initial_residual"] for r in reps),
+                    "max_rel_error_vs_fp64_solution": max(errs),
+                    "iteration_diff_vs_fp64_max": int(max(abs(a - b) for a, b in zip(iters, its64)))},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
 
 
 def cpu_batch_rate(probs, its64, seconds):
-    """Oracle FP64 CG + Jacobi solves of the smallest problems of the batch
-    until about `seconds` of CPU time; the rate per DoF-iteration scales to the
-    whole batch (sum of n_dofs x FP64 iterations)."""
-    from oracle import oracle as O
-    from meltpooldg_b200 import box_vertices
+    """The tuned CPU port's FP64 CG + Jacobi solves (diagonal by unit vectors
+    per cell, as deal.II's compute_diagonal) of the smallest problems of the
+    batch until about `seconds`; the rate per DoF-iteration scales to the whole
+    batch (sum of n_dofs x FP64 iterations)."""
+    from oracle import cpu_port as P
+    from meltpooldg_b200 import box_vertices, boundary_mask
     order = np.argsort([p.n_dofs for p in probs])
     spent, work, done = 0.0, 0.0, 0
     for i in order:
         p = probs[i]
         nc = (p.nc,) * 3
-        om = O.Mesh(3, p.degree, nc, box_vertices(nc))
-        op = O.Operator(O.HEAT, p.dt, rho_cp=p.rho_cp, k0=p.k0, dirichlet=om.boundary_face_mask())
+        port = P.PortOperator(box_vertices(nc), nc, p.degree, boundary_mask(nc, p.degree), uniform=True, kind=0,
+                              dt=p.dt, rho_cp=p.rho_cp, k0=p.k0)
         b = p.rhs()
         t0 = time.perf_counter()
-        inv = O.inverse_diagonal(om, op)
-        _, it, _, ok = O.cg(om, op, b, inv_diag=inv, rel_tol=1e-10, abs_tol=0.0)
+        _, it, _ = port.cg_jacobi(b, rel_tol=1e-10, abs_tol=0.0)
         spent += time.perf_counter() - t0
+        port.close()
         work += p.n_dofs * max(it, 1)
         done += 1
         if spent > seconds:
             break
     total_work = float(sum(p.n_dofs * max(it, 1) for p, it in zip(probs, its64)))
     rate = len(probs) / (spent * total_work / work)
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": rate, "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": f"oracle CG+Jacobi of the {done} smallest problems ({spent:.1f} s), scaled by "
+    return {"value": rate, "unit": "solves/s", "cores": P.threads(), "kind": "port",
+            "sample": f"port CG+Jacobi of the {done} smallest problems ({spent:.1f} s), scaled by "
                       f"n_dofs x iterations to all {len(probs)}"}
 
 
@@ -698,7 +743,9 @@ def serve_work(probs, reps, wall):
 def run_serve(args, rank, world):
     """Config 5: Poisson stream of heat / advection-diffusion requests served by
     the library's loop (continuous batching, 150 GB admission budget), against
-    the plain FP64 GPU form serving the same stream one request at a time."""
+    the plain FP64 GPU form serving the same stream one request at a time; and
+    the same kind of stream below the device's capacity, whose latencies are the
+    engine's own rather than queueing."""
     import torch
     import meltpooldg_b200 as M
     from meltpooldg_b200 import batch as B
@@ -717,9 +764,18 @@ def run_serve(args, rank, world):
         with B.Batch(budget, capacity=4096) as bt:
             out = bt.serve(probs, arr, poll_steps=args.poll_steps, keep_solutions=keep)
     launches = M.kernel_launches() - launches0
-    lat = np.sort(out["latency_s"])
     reps = out["reports"]
     value = n_req / out["wall_s"]
+
+    # below capacity: the same distribution of requests at a lower arrival rate
+    low = None
+    if args.low_rate > 0 and args.low_requests > 0:
+        lp, la = serve_requests(args.low_requests, rate=args.low_rate, seed=8)
+        with B.Batch(budget, capacity=4096) as bt:
+            lo = bt.serve(lp, la, poll_steps=args.poll_steps)
+        low = dict(percentiles(lo["latency_s"]), requests=args.low_requests, rate_req_per_s=args.low_rate,
+                   solves_per_s=args.low_requests / lo["wall_s"],
+                   all_converged=all(r["status"] == 0 for r in lo["reports"]))
 
     # plain FP64 GPU form on the same stream: one request at a time, FIFO
     fp64 = None
@@ -737,37 +793,46 @@ def run_serve(args, rank, world):
                 xb = out["solutions"][i]
                 errs.append(float(np.linalg.norm(xb - x64) / max(np.linalg.norm(x64), 1e-300)))
         wall64 = time.perf_counter() - t0
-        lat64 = np.sort(np.asarray(lat64))
-        fp64 = {"requests": n64, "solves_per_s": n64 / wall64,
-                "p50_ms": 1e3 * float(np.percentile(lat64, 50)), "p99_ms": 1e3 * float(np.percentile(lat64, 99)),
-                "max_rel_error_batched_vs_fp64": max(errs) if errs else None,
-                "compared_solutions": len(errs)}
-    if rank == 0:
-        n_dofs = np.array([p.n_dofs for p in probs])
-        line = {
-            "metric": "served solves/s at 1e-10 with p50/p99 latency (continuous batching)",
-            "value": value, "unit": "solves/s", "n_gpus": world, "steps": 1, "warmup": args.warmup,
-            "ms_per_step": 1e3 * out["wall_s"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 apply / f64 residuals", "data": "synthetic",
-            "config": {"workload": f"Poisson stream, 200 req/s, {n_req} requests, n=min(96, LogNormal(ln 24, 0.5)), "
-                                   "Q2/Q3/Q4, 50% heat (CG) / 50% advection-diffusion (BiCGStab), 150 GB budget",
-                       "n_dofs_mean": float(n_dofs.mean()), "n_dofs_max": int(n_dofs.max()),
-                       "poll_steps": args.poll_steps,
-                       "timing": "host clock (request arrival to solution on the host)"},
-            "latency": {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
-                        "max_ms": 1e3 * float(lat[-1])},
-            "loop": out["stats"],
-            "work": serve_work(probs, reps, out["wall_s"]),
-            "all_converged": all(r["status"] == 0 for r in reps),
-            "max_rel_residual": max(r["final_residual"] / max(r["initial_residual"], 1e-300) for r in reps),
-            "fp64_plain": fp64,
-            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": int(8 * n_dofs.sum()),
-                    "call": "mpdg_serve (device right-hand sides, solutions copied to the host)"},
-            "gpu_launches": launches,
-            "clocks": clk.summary(),
-        }
-        print(json.dumps(line), flush=True)
+        fp64 = dict(percentiles(lat64), requests=n64, solves_per_s=n64 / wall64,
+                    max_rel_error_batched_vs_fp64=max(errs) if errs else None, compared_solutions=len(errs))
+    n_dofs = np.array([p.n_dofs for p in probs])
+    return {
+        "metric": "served solves/s at 1e-10 with p50/p99 latency (continuous batching)",
+        "value": value, "unit": "solves/s", "n_gpus": world, "steps": 1, "warmup": args.warmup,
+        "ms_per_step": 1e3 * out["wall_s"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 apply / f64 residuals", "data": "synthetic",
+        "config": {"workload": f"Poisson stream, 200 req/s, {n_req} requests, n=min(96, LogNormal(ln 24, 0.5)), "
+                               "Q2/Q3/Q4, 50% heat (CG) / 50% advection-diffusion (BiCGStab in the batch; "
+                               "the reference and the single-problem path use GMRES), 150 GB budget",
+                   "n_dofs_mean": float(n_dofs.mean()), "n_dofs_max": int(n_dofs.max()),
+                   "poll_steps": args.poll_steps,
+                   "timing": "host clock (request arrival to solution on the host)"},
+        "latency": percentiles(out["latency_s"]),
+        "below_capacity": low,
+        "loop": out["stats"],
+        "work": serve_work(probs, reps, out["wall_s"]),
+        "all_converged": all(r["status"] == 0 for r in reps),
+        "max_rel_residual": max(r["final_residual"] / max(r["initial_residual"], 1e-300) for r in reps),
+        "fp64_plain": fp64,
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(8 * n_dofs.sum()),
+                "call": "mpdg_serve (device right-hand sides, solutions copied to the host)"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+
+
+def run_extras(args, rank, world):
+    """The other configurations, measured in the same run as the headline."""
+    extras = {}
+    for name in ("c1", "advdiff"):
+        set_workload(name)
+        line = run_operator_workload(args, rank, world, headline=False)
+        extras["c3" if name == "advdiff" else "c1"] = line
+    set_workload("heat")
+    extras["c4"] = run_batch(args, rank, world)
+    extras["c5"] = run_serve(args, rank, world)
+    return extras
 
 
 def main():
@@ -776,34 +841,28 @@ def main():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--solve-reps", type=int, default=3)
+    ap.add_argument("--solve-reps", type=int, default=20, help="timed solves per form (after one warm-up solve)")
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--cpu-seconds", type=float, default=5.0)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="headline workload only")
     ap.add_argument("--cells", type=int, default=0,
                     help="cells per direction (default: the workload's; smaller sizes for profiling)")
-    ap.add_argument("--workload", default="heat", choices=["heat", "advdiff", "c1", "batch", "serve"])
+    ap.add_argument("--workload", default=None, choices=["heat", "advdiff", "c1", "batch", "serve"],
+                    help="one workload only (default: the headline plus the others as extra keys)")
     ap.add_argument("--problems", type=int, default=BATCH_SIZE,
                     help="batch: problems in the batch (the first of the seeded sequence)")
+    ap.add_argument("--batch-steps", type=int, default=2, help="batch: timed whole batches")
     ap.add_argument("--requests", type=int, default=20000, help="serve: requests in the stream")
     ap.add_argument("--poll-steps", type=int, default=4, help="serve: graph steps between checks")
+    ap.add_argument("--low-rate", type=float, default=40.0, help="serve: arrival rate of the below-capacity stream")
+    ap.add_argument("--low-requests", type=int, default=1000, help="serve: requests of the below-capacity stream")
     ap.add_argument("--no-fp64-arm", action="store_true", help="serve: skip the plain FP64 arm")
-    ap.add_argument("--fp64-requests", type=int, default=2000,
+    ap.add_argument("--fp64-requests", type=int, default=500,
                     help="serve: requests of the stream the plain FP64 arm serves")
     args = ap.parse_args()
-    if args.workload in ("batch", "serve") and args.steps == 400:
-        args.steps = 2 if args.workload == "batch" else 1
-    WORKLOAD["name"] = args.workload
-    global DEGREE
-    if args.workload == "advdiff":
-        DEGREE = 2
-        NC[:] = [args.cells or 128] * 3
-    elif args.workload == "c1":
-        DEGREE = 2
-        NC[:] = [args.cells or 16] * 3
-    else:
-        NC[:] = [args.cells or 64] * 3
+    set_workload(args.workload if args.workload in ("heat", "advdiff", "c1") else "heat", args.cells)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if world > 1 and args.impl == "ours":
@@ -815,11 +874,19 @@ def main():
         if args.impl == "reference":
             run_reference(args, rank, world)
         elif args.workload == "batch":
-            run_batch(args, rank, world)
+            line = run_batch(args, rank, world)
+            if rank == 0:
+                print(json.dumps(line), flush=True)
         elif args.workload == "serve":
-            run_serve(args, rank, world)
+            line = run_serve(args, rank, world)
+            if rank == 0:
+                print(json.dumps(line), flush=True)
         else:
-            run_ours(args, rank, world)
+            line = run_operator_workload(args, rank, world, headline=True)
+            if args.workload is None and not args.no_extras and world == 1:
+                line["extra"] = run_extras(args, rank, world)
+            if rank == 0:
+                print(json.dumps(line), flush=True)
     finally:
         if world > 1 and args.impl == "ours":
             import torch.distributed as dist
