@@ -261,13 +261,17 @@ mpdg_status mpdg_vmult_multi(mpdg_op *op, int n_vectors, double *const *dst, con
  * every colour after an apply's first as a programmatic dependent of the one
  * before, so that its start (coefficient copies, src gathers, the first cells'
  * arithmetic) overlaps the previous colour's last cells and only its reads of
- * dst wait for it.  Results are identical for every schedule.  No reference
+ * dst wait for it; cta_cell_groups lets the four warps of a CTA share their
+ * cells (5 Q4 cells or 14 Q2 cells per 128 threads instead of 4 or 12, so
+ * fewer lanes idle; the tile exchanges become CTA barriers), for degrees 2
+ * and 4 on lattice meshes.  Results are identical for every schedule.  No reference
  * counterpart: the schedule of deal.II's MatrixFree::cell_loop
  * (heat_diffuse_operator.cpp:183) is internal to it. */
 typedef struct {
   int slabs;            /* 1..32 (capped at half the cell layers) */
   int l2_evict_first;   /* 0 or 1 */
   int overlap_colours;  /* 0 or 1 */
+  int cta_cell_groups;  /* 0 or 1 */
 } mpdg_schedule;
 mpdg_status mpdg_op_set_schedule(mpdg_op *op, int precision, const mpdg_schedule *schedule);
 mpdg_status mpdg_op_get_schedule(mpdg_op *op, int precision, mpdg_schedule *schedule);

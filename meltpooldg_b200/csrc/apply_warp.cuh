@@ -208,46 +208,82 @@ __host__ __device__ constexpr int warp_tile_elems()
   return tile_elems<n, tile_s2<n, TUNED>(), TUNED>() + tile_elems<n, t1s2<n, Real, TUNED>(), TUNED>();
 }
 
+// Tiles of one cell group of GROUP threads: plane strides s0, s1 and cell
+// offsets sc0, sc1 of t0 and t1.  GROUP = 32 is the warp-per-group apply (the
+// layouts above).  GROUP = 128 lets the CTA's four warps share the cells: a
+// Q4 cell has 25 lines and a Q2 cell 9, so a warp leaves 7 (Q4) or 5 (Q2) lanes
+// idle, a CTA only 3 or 2 (5 Q4 cells, or 14 Q2 cells, per 128 threads).
+// Their layouts come from the same wavefront search over the CTA's four
+// warps (32-bit accesses in one pass, 64-bit in two half-warps): t0 over the Z,
+// X and Y accesses, t1 (only Z and Y) on its own --
+//   Q4 FP32: t0 25 / 125, t1 25 / 153: 100 + 60 wavefronts per 5 cells
+//   Q4 FP64: t0 25 / 125, t1 27 / 137: 180 + 115
+//   Q2 FP32: t0 9 / 27,   t1 11 / 41:  60 + 36 per 14 cells
+//   Q2 FP64: t0 9 / 27,   t1 19 / 57:  117 + 48
+// per cell the same as the warp layouts; Q1 and Q3 fill a warp exactly and
+// keep their warp layouts (cell c at c sc).
+template <int n, typename Real, int GROUP>
+struct TileLayout {
+  static constexpr bool cta = GROUP == 128 && (n == 5 || n == 3);
+  static constexpr bool f64 = sizeof(Real) == 8;
+  static constexpr int cells = GROUP / (n * n);
+  static constexpr int s0 = cta ? n * n : tile_s2<n>();
+  static constexpr int sc0 = cta ? n * n * n : tile_sc<n>();
+  static constexpr int s1 = cta ? (n == 5 ? (f64 ? 27 : 25) : (f64 ? 19 : 11)) : t1s2<n, Real>();
+  static constexpr int sc1 = cta ? (n == 5 ? (f64 ? 137 : 153) : (f64 ? 57 : 41)) : tile_sc<n>();
+  static constexpr int t0_elems = (cells - 1) * sc0 + (n - 1) * s0 + n * n;
+  static constexpr int t1_elems = (cells - 1) * sc1 + (n - 1) * s1 + n * n;
+  static constexpr int elems = t0_elems + t1_elems;
+};
+
+// the tiles of a cell group are shared by a warp (GROUP 32) or the whole CTA
+template <bool CTA>
+__device__ __forceinline__ void group_sync()
+{
+  if constexpr (CTA) __syncthreads();
+  else __syncwarp();
+}
+
 // nodal values u (Z layout) -> values uq and collocation gradients gx, gy, gz
 // at the Gauss points, all in Z layout.  S, Dc: tables in constant memory.
-template <int n, typename Real, bool TUNED = true>
+template <int n, typename Real, class L = TileLayout<n, Real, 32>, bool CTA = false>
 __device__ __forceinline__ void l_forward(const Tables<Real> &T, Real *t0, Real *t1, bool wr, int a, int b,
                                           const Real (&u)[n], Real (&uq)[n], Real (&gx)[n], Real (&gy)[n],
                                           Real (&gz)[n])
 {
   Real v[n], w[n];
   c1<n, Real, false, false>(T.S, T.eS, u, v);  // z: nodes -> Gauss points
-  if (wr) putZ<n, tile_s2<n, TUNED>()>(t0, a, b, v);
-  __syncwarp();
-  getX<n, tile_s2<n, TUNED>()>(t0, a, b, w);
-  __syncwarp();
+  if (wr) putZ<n, L::s0>(t0, a, b, v);
+  group_sync<CTA>();
+  getX<n, L::s0>(t0, a, b, w);
+  group_sync<CTA>();
   c1<n, Real, false, false>(T.S, T.eS, w, v);  // x
-  if (wr) putX<n, tile_s2<n, TUNED>()>(t0, a, b, v);
-  __syncwarp();
-  getY<n, tile_s2<n, TUNED>()>(t0, a, b, w);
-  __syncwarp();
+  if (wr) putX<n, L::s0>(t0, a, b, v);
+  group_sync<CTA>();
+  getY<n, L::s0>(t0, a, b, w);
+  group_sync<CTA>();
   c1<n, Real, false, false>(T.S, T.eS, w, v);    // y: v = values at the Gauss points (Y layout)
   c1<n, Real, false, true>(T.Dc, T.eDc, v, w);   // d/dy (Y layout)
   if (wr) {
-    putY<n, tile_s2<n, TUNED>()>(t0, a, b, v);
-    putY<n, t1s2<n, Real, TUNED>()>(t1, a, b, w);
+    putY<n, L::s0>(t0, a, b, v);
+    putY<n, L::s1>(t1, a, b, w);
   }
-  __syncwarp();
-  getZ<n, tile_s2<n, TUNED>()>(t0, a, b, uq);
-  getX<n, tile_s2<n, TUNED>()>(t0, a, b, w);
-  getZ<n, t1s2<n, Real, TUNED>()>(t1, a, b, gy);
-  __syncwarp();
+  group_sync<CTA>();
+  getZ<n, L::s0>(t0, a, b, uq);
+  getX<n, L::s0>(t0, a, b, w);
+  getZ<n, L::s1>(t1, a, b, gy);
+  group_sync<CTA>();
   c1<n, Real, false, true>(T.Dc, T.eDc, uq, gz);  // d/dz (Z layout)
   c1<n, Real, false, true>(T.Dc, T.eDc, w, v);    // d/dx (X layout)
-  if (wr) putX<n, tile_s2<n, TUNED>()>(t0, a, b, v);
-  __syncwarp();
-  getZ<n, tile_s2<n, TUNED>()>(t0, a, b, gx);
-  __syncwarp();
+  if (wr) putX<n, L::s0>(t0, a, b, v);
+  group_sync<CTA>();
+  getZ<n, L::s0>(t0, a, b, gx);
+  group_sync<CTA>();
 }
 
 // test functions: out = S^T (val + Dc_x^T fx + Dc_y^T fy + Dc_z^T fz) in all
 // three directions; inputs at the Gauss points and output at the nodes, Z layout
-template <int n, typename Real, bool TUNED = true>
+template <int n, typename Real, class L = TileLayout<n, Real, 32>, bool CTA = false>
 __device__ __forceinline__ void l_backward(const Tables<Real> &T, Real *t0, Real *t1, bool wr, int a, int b,
                                            const Real (&val)[n], const Real (&fx)[n], const Real (&fy)[n],
                                            const Real (&fz)[n], Real (&out)[n])
@@ -257,47 +293,47 @@ __device__ __forceinline__ void l_backward(const Tables<Real> &T, Real *t0, Real
 #pragma unroll
   for (int k = 0; k < n; ++k) A[k] += val[k];  // Z layout
   if (wr) {
-    putZ<n, tile_s2<n, TUNED>()>(t0, a, b, fx);
-    putZ<n, t1s2<n, Real, TUNED>()>(t1, a, b, fy);
+    putZ<n, L::s0>(t0, a, b, fx);
+    putZ<n, L::s1>(t1, a, b, fy);
   }
-  __syncwarp();
-  getX<n, tile_s2<n, TUNED>()>(t0, a, b, w);
-  getY<n, t1s2<n, Real, TUNED>()>(t1, a, b, C);
-  __syncwarp();
+  group_sync<CTA>();
+  getX<n, L::s0>(t0, a, b, w);
+  getY<n, L::s1>(t1, a, b, C);
+  group_sync<CTA>();
   c1<n, Real, true, true>(T.Dc, T.eDct, w, B);  // x part (X layout)
   c1<n, Real, true, true>(T.Dc, T.eDct, C, w);  // y part (Y layout)
   if (wr) {
-    putZ<n, t1s2<n, Real, TUNED>()>(t1, a, b, A);
-    putX<n, tile_s2<n, TUNED>()>(t0, a, b, B);
+    putZ<n, L::s1>(t1, a, b, A);
+    putX<n, L::s0>(t0, a, b, B);
   }
-  __syncwarp();
-  getY<n, t1s2<n, Real, TUNED>()>(t1, a, b, A);
-  getY<n, tile_s2<n, TUNED>()>(t0, a, b, B);
-  __syncwarp();
+  group_sync<CTA>();
+  getY<n, L::s1>(t1, a, b, A);
+  getY<n, L::s0>(t0, a, b, B);
+  group_sync<CTA>();
 #pragma unroll
   for (int q = 0; q < n; ++q) C[q] = w[q] + A[q] + B[q];  // sum in Y layout
   c1<n, Real, true, false>(T.S, T.eSt, C, w);  // y: Gauss points -> nodes
-  if (wr) putY<n, tile_s2<n, TUNED>()>(t0, a, b, w);
-  __syncwarp();
-  getX<n, tile_s2<n, TUNED>()>(t0, a, b, C);
-  __syncwarp();
+  if (wr) putY<n, L::s0>(t0, a, b, w);
+  group_sync<CTA>();
+  getX<n, L::s0>(t0, a, b, C);
+  group_sync<CTA>();
   c1<n, Real, true, false>(T.S, T.eSt, C, w);  // x
-  if (wr) putX<n, tile_s2<n, TUNED>()>(t0, a, b, w);
-  __syncwarp();
-  getZ<n, tile_s2<n, TUNED>()>(t0, a, b, C);
-  __syncwarp();
+  if (wr) putX<n, L::s0>(t0, a, b, w);
+  group_sync<CTA>();
+  getZ<n, L::s0>(t0, a, b, C);
+  group_sync<CTA>();
   c1<n, Real, true, false>(T.S, T.eSt, C, out);  // z
 }
 
-// dynamic shared memory per warp, in units of Real, rounded up to a multiple of
-// 8 elements so that every warp's stage starts on a 32-byte boundary (bulk
-// copies need 16-byte aligned shared-memory destinations)
-template <int P, typename Real, int GEOM>
+// dynamic shared memory per cell group, in units of Real, rounded up to a
+// multiple of 8 elements so that every group's stage starts on a 32-byte
+// boundary (bulk copies need 16-byte aligned shared-memory destinations)
+template <int P, typename Real, int GEOM, int GROUP = 32>
 __host__ __device__ constexpr int warp_smem_elems(bool vel)
 {
-  constexpr int n = P + 1, CPW = WCfg<n>::cpw;
+  constexpr int n = P + 1, CPW = GROUP / (n * n);
   return (((GEOM == GEOM_GENERAL ? CPW * (metric_stride(n) + (vel ? velb_stride(n) : 0)) : 0) +
-           warp_tile_elems<n, Real>()) + 7) / 8 * 8;
+           TileLayout<n, Real, GROUP>::elems) + 7) / 8 * 8;
 }
 constexpr int kSmemAlign = 128;  // the dynamic shared-memory base is aligned by hand
 
@@ -325,18 +361,27 @@ struct WOcc {
 // MAPPED: a mapped mesh's cells, gathered and scattered through the
 // cell->DoF map p.cmap; dst is cleared before the colours and every cell adds
 // (the mesh's greedy colouring keeps the cells of a launch apart)
-template <int P, typename Real, int GEOM, bool HANG = false, bool MULTI = false, bool MAPPED = false>
+// GROUP: threads that share a group of cells -- 32 (a warp per group, four
+// groups per CTA) or 128 (the whole CTA per group, fewer idle lanes for Q2/Q4;
+// every tile exchange is then a CTA barrier)
+template <int P, typename Real, int GEOM, bool HANG = false, bool MULTI = false, bool MAPPED = false,
+          int GROUP = 32>
 __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     warp_apply_kernel(const KP<Real> p, int *err)
 {
   static_assert(!(HANG && MULTI), "the multi-vector apply has no hanging-node path");
   static_assert(!(MAPPED && (HANG || MULTI || GEOM != GEOM_GENERAL)), "mapped meshes: general geometry, one vector");
-  constexpr int n = P + 1, n2 = n * n, n3 = n2 * n, CPW = WCfg<n>::cpw;
+  static_assert(GROUP == 32 || (GROUP == kWarpsPerCTA * 32 && !HANG && !MULTI && !MAPPED),
+                "CTA-wide cell groups: plain applies only");
+  constexpr bool CTA = GROUP != 32;
+  using L = TileLayout<P + 1, Real, GROUP>;
+  constexpr int n = P + 1, n2 = n * n, n3 = n2 * n, CPW = GROUP / n2;
+  constexpr int GPC = kWarpsPerCTA * 32 / GROUP;  // cell groups per CTA
   constexpr int MS = metric_stride(n), VS = velb_stride(n);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bars[kWarpsPerCTA];
+  __shared__ __align__(8) uint64_t bars[GPC];
   const Tables<Real> &T = tab<Real>(P);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = CTA ? 0 : threadIdx.x >> 5, lane = CTA ? threadIdx.x : threadIdx.x & 31;
   const bool has_vel = p.vel_kind != MPDG_VEL_NONE;
   const bool gvel = GEOM == GEOM_GENERAL && has_vel;
 
@@ -350,25 +395,25 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
   bool dep_pending = p.pdl != 0;
 
   unsigned char *base = smem_raw + ((kSmemAlign - (smem_u32(smem_raw) & (kSmemAlign - 1))) & (kSmemAlign - 1));
-  Real *wsm = reinterpret_cast<Real *>(base) + warp * warp_smem_elems<P, Real, GEOM>(gvel);
+  Real *wsm = reinterpret_cast<Real *>(base) + warp * warp_smem_elems<P, Real, GEOM, GROUP>(gvel);
   Real *stage = wsm;
   Real *vstage = wsm + (GEOM == GEOM_GENERAL ? CPW * MS : 0);
   Real *tiles = wsm + (GEOM == GEOM_GENERAL ? CPW * (MS + (gvel ? VS : 0)) : 0);
 
-  // lanes past the last cell (Q2: 5, Q4: 7) copy the position of the lane
-  // 32 - CPW n^2 below them: their unused shared-memory loads then read the
-  // same addresses as active lanes of their own half-warp (a broadcast), which
-  // keeps 64-bit loads at two wavefronts
+  // lanes past the last cell (warp groups: Q2 5, Q4 7; CTA groups: Q2 2, Q4
+  // 3) copy the position of the lane GROUP - CPW n^2 below them: their unused
+  // shared-memory loads then read the same addresses as active lanes of their
+  // own half-warp (a broadcast), which keeps 64-bit loads at two wavefronts
   const bool lane_ok = lane < CPW * n2;
-  const int mlane = lane_ok ? lane : lane - (32 - CPW * n2);
+  const int mlane = lane_ok ? lane : lane - (GROUP - CPW * n2);
   const int sub = mlane / n2, l = mlane % n2, i = l % n, j = l / n;
   const int s_sub = sub;
-  Real *t0 = tiles + s_sub * tile_sc<n>();
-  Real *t1 = tiles + tile_elems<n, tile_s2<n>()>() + s_sub * tile_sc<n>();
+  Real *t0 = tiles + s_sub * L::sc0;
+  Real *t1 = tiles + L::t0_elems + s_sub * L::sc1;
   // DoF offsets are 32-bit: the launcher checks that the lattice has < 2^32 DoFs
   const unsigned NXu = (unsigned)p.NX, NYu = (unsigned)p.NY, zs = NXu * NYu;
   const int count = (int)p.ccount;
-  const int gstride = gridDim.x * kWarpsPerCTA;
+  const int gstride = gridDim.x * GPC;
   unsigned phase = 0;
 
   auto issue_stage = [&](int grp) {
@@ -441,7 +486,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     return (w >> (b & 31)) & 1u;
   };
 
-  int group = blockIdx.x * kWarpsPerCTA + warp;
+  int group = blockIdx.x * GPC + warp;
   if (GEOM == GEOM_GENERAL && lane == 0 && group * CPW < count) issue_stage(group);
   Real A[n];
   uint4 cmA;
@@ -459,7 +504,10 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     // constrained DoFs of the lane's column (bit k: DoF (i, j, k)); skipped as a
     // whole when no lane's cell has one (the interior of the mesh)
     unsigned lmask = 0;
-    const bool any_mask = __any_sync(0xffffffffu, (cmA.x | cmA.y | cmA.z | cmA.w) != 0u);
+    const bool cell_has_mask = (cmA.x | cmA.y | cmA.z | cmA.w) != 0u;
+    bool any_mask;
+    if constexpr (CTA) any_mask = __syncthreads_or(cell_has_mask) != 0;
+    else any_mask = __any_sync(0xffffffffu, cell_has_mask);
     if (any_mask) {
 #pragma unroll
       for (int k = 0; k < n; ++k) lmask |= (unsigned)mask_bit(cmA, k) << k;
@@ -516,7 +564,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     }
 
     Real uq[n], gx[n], gy[n], gz[n];
-    l_forward<n>(T, t0, t1, true, i, j, u, uq, gx, gy, gz);
+    l_forward<n, Real, L, CTA>(T, t0, t1, true, i, j, u, uq, gx, gy, gz);
 
     if (GEOM == GEOM_GENERAL && v == 0) {
       mbar_wait_bounded(&bars[warp], phase, err);
@@ -566,12 +614,12 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     }
     if (GEOM == GEOM_GENERAL && v == nv - 1) {
       // the stage is consumed by every vector: start the next group's copy now
-      __syncwarp();
+      group_sync<CTA>();
       if (lane == 0 && has_next) issue_stage(gnext);
     }
 
     Real out[n];
-    l_backward<n>(T, t0, t1, true, i, j, val, fx, fy, fz, out);
+    l_backward<n, Real, L, CTA>(T, t0, t1, true, i, j, val, fx, fy, fz, out);
 
     if (HANG && __any_sync(0xffffffffu, hl)) {
       // transposed interpolation of the hanging results onto the coarse face:

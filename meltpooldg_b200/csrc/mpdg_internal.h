@@ -163,6 +163,7 @@ struct ApplySchedule {
   int slabs = 1;        // z-slabs of cell layers, each running its 8 colours
   int evict_first = 0;  // L2 evict-first hint on the coefficient stream
   int pdl = 1;          // colour launches as programmatic dependents of the previous one
+  int cta = 0;          // cell groups of a whole CTA (Q2, Q4) instead of a warp
 };
 
 struct Op {
@@ -214,7 +215,7 @@ struct Op {
   int lsq_cols = 0;
   void *io_tmp = nullptr;
   size_t io_tmp_bytes = 0;
-  ApplySchedule sched[2] = {ApplySchedule{1, 0, 1}, ApplySchedule{1, 1, 1}};  // [MPDG_FP64], [MPDG_FP32]
+  ApplySchedule sched[2] = {ApplySchedule{1, 0, 1, 0}, ApplySchedule{1, 1, 1, 0}};  // [MPDG_FP64], [MPDG_FP32]
 };
 
 // ---- batched apply over many solves (batch_apply.cuh / batch.cu)

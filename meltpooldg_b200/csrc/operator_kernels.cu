@@ -1670,14 +1670,14 @@ int num_sms()
   return g_num_sms;
 }
 
-template <int P, typename Real, int GEOM, bool HANG, bool MULTI = false, bool MAPPED = false>
+template <int P, typename Real, int GEOM, bool HANG, bool MULTI = false, bool MAPPED = false, int GROUP = 32>
 void run_warp_apply(Op &op, KP<Real> k)
 {
   Mesh &m = *op.mesh;
-  constexpr int n = P + 1, CPW = WCfg<n>::cpw;
+  constexpr int n = P + 1, CPW = GROUP / (n * n), GPC = kWarpsPerCTA * 32 / GROUP;
   const bool gvel = GEOM == GEOM_GENERAL && op.d.vel_kind != MPDG_VEL_NONE;
-  const size_t per_warp = sizeof(Real) * warp_smem_elems<P, Real, GEOM>(gvel);
-  const size_t smem = per_warp * kWarpsPerCTA + kSmemAlign;
+  const size_t per_warp = sizeof(Real) * warp_smem_elems<P, Real, GEOM, GROUP>(gvel);
+  const size_t smem = per_warp * GPC + kSmemAlign;
   // bulk-copy alignment contract, checked before any launch: 16-byte aligned
   // shared destinations, global sources and sizes
   static_assert((metric_stride(n) * sizeof(Real)) % 16 == 0, "metric stride");
@@ -1688,7 +1688,7 @@ void run_warp_apply(Op &op, KP<Real> k)
   if (GEOM == GEOM_GENERAL && (!k.metric || (gvel && !k.velb)))
     throw Error{MPDG_ERR_ARG, "coefficient stream missing"};
   if (m.N >= (1L << 32)) throw Error{MPDG_ERR_UNSUPPORTED, "the warp apply indexes DoFs with 32 bits"};
-  auto kern = warp_apply_kernel<P, Real, GEOM, HANG, MULTI, MAPPED>;
+  auto kern = warp_apply_kernel<P, Real, GEOM, HANG, MULTI, MAPPED, GROUP>;
   static int configured_smem = -1, blocks_per_sm = 0;  // per instantiation
   if (configured_smem != (int)smem) {
     MPDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1719,7 +1719,7 @@ void run_warp_apply(Op &op, KP<Real> k)
         k.par[2] = C.par[2] + 2 * (int)m_lo;
       }
       const long groups = (k.ccount + CPW - 1) / CPW;
-      const long blocks = std::min(resident, (groups + kWarpsPerCTA - 1) / kWarpsPerCTA);
+      const long blocks = std::min(resident, (groups + GPC - 1) / GPC);
       // colours after the first of an apply start as programmatic dependents of
       // the previous colour: src and the coefficients are not written by it,
       // and the kernel reads dst only after griddepcontrol.wait.  The first
@@ -1785,11 +1785,22 @@ void warp_apply_degree(Op &op, const KP<Real> &k)
     }
     return;
   }
+  // CTA-wide cell groups (fewer idle lanes) where the schedule asks for them;
+  // they only differ from warp groups for Q2 and Q4
+  const bool cta = op.sched[sizeof(Real) == 4 ? MPDG_FP32 : MPDG_FP64].cta && !hang;
   switch (op.mesh->degree) {
     case 1: hang ? run_warp_apply<1, Real, GEOM, true>(op, k) : run_warp_apply<1, Real, GEOM, false>(op, k); break;
-    case 2: hang ? run_warp_apply<2, Real, GEOM, true>(op, k) : run_warp_apply<2, Real, GEOM, false>(op, k); break;
+    case 2:
+      if (cta) run_warp_apply<2, Real, GEOM, false, false, false, 128>(op, k);
+      else if (hang) run_warp_apply<2, Real, GEOM, true>(op, k);
+      else run_warp_apply<2, Real, GEOM, false>(op, k);
+      break;
     case 3: hang ? run_warp_apply<3, Real, GEOM, true>(op, k) : run_warp_apply<3, Real, GEOM, false>(op, k); break;
-    case 4: hang ? run_warp_apply<4, Real, GEOM, true>(op, k) : run_warp_apply<4, Real, GEOM, false>(op, k); break;
+    case 4:
+      if (cta) run_warp_apply<4, Real, GEOM, false, false, false, 128>(op, k);
+      else if (hang) run_warp_apply<4, Real, GEOM, true>(op, k);
+      else run_warp_apply<4, Real, GEOM, false>(op, k);
+      break;
     default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
   }
 }
@@ -2249,16 +2260,19 @@ void autotune_apply(Op &op, int precision, int reps, ApplySchedule &best, double
   // without the evict-first hint where a coefficient stream exists
   std::vector<ApplySchedule> cand;
   const bool stream = !m.uniform || m.mapped;
-  for (int S : {1, 2, 4, 8}) {
+  const bool cta_differs = (m.degree == 2 || m.degree == 4) && !m.mapped && !op.fine;
+  for (int S : {1, 2}) {
     if (S > 1 && (S > m.nc[2] / 2 || m.mapped || op.fine)) continue;
     for (int h = 0; h <= (stream ? 1 : 0); ++h)
-      for (int d = 0; d <= 1; ++d) {
-        ApplySchedule c;
-        c.slabs = S;
-        c.evict_first = h;
-        c.pdl = d;
-        cand.push_back(c);
-      }
+      for (int d = 0; d <= 1; ++d)
+        for (int g = 0; g <= (cta_differs ? 1 : 0); ++g) {
+          ApplySchedule c;
+          c.slabs = S;
+          c.evict_first = h;
+          c.pdl = d;
+          c.cta = g;
+          cand.push_back(c);
+        }
   }
   void *x = nullptr, *y = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -245,13 +245,14 @@ class _MatrixFreeOperator:
     def compute_diagonal(self, diag):
         A.check(A.lib().mpdg_compute_diagonal(self._h, _dptr(diag)), "compute_diagonal")
 
-    def set_schedule(self, slabs=1, l2_evict_first=False, precision="fp64", overlap_colours=False):
+    def set_schedule(self, slabs=1, l2_evict_first=False, precision="fp64", overlap_colours=False,
+                     cta_cell_groups=False):
         """Schedule of the resident apply (mpdg_op_set_schedule): colour launches
         slab by slab over `slabs` z-slabs of cell layers, the L2 evict-first
-        hint on the coefficient stream, and colour launches that overlap the
-        previous colour's tail (programmatic dependent launch).  Results do not
-        depend on it."""
-        s = A.Schedule(int(slabs), int(bool(l2_evict_first)), int(bool(overlap_colours)))
+        hint on the coefficient stream, colour launches that overlap the
+        previous colour's tail (programmatic dependent launch), and cell groups
+        shared by a whole CTA (degrees 2 and 4).  Results do not depend on it."""
+        s = A.Schedule(int(slabs), int(bool(l2_evict_first)), int(bool(overlap_colours)), int(bool(cta_cell_groups)))
         A.check(A.lib().mpdg_op_set_schedule(self._h, A.FP32 if precision == "fp32" else A.FP64, C.byref(s)),
                 "mpdg_op_set_schedule")
 
@@ -260,7 +261,7 @@ class _MatrixFreeOperator:
         A.check(A.lib().mpdg_op_get_schedule(self._h, A.FP32 if precision == "fp32" else A.FP64, C.byref(s)),
                 "mpdg_op_get_schedule")
         return {"slabs": s.slabs, "l2_evict_first": bool(s.l2_evict_first),
-                "overlap_colours": bool(s.overlap_colours)}
+                "overlap_colours": bool(s.overlap_colours), "cta_cell_groups": bool(s.cta_cell_groups)}
 
     def autotune(self, precision="fp64", reps=10):
         """Times the candidate schedules of the resident apply (mpdg_op_autotune)
@@ -271,7 +272,8 @@ class _MatrixFreeOperator:
         A.check(A.lib().mpdg_op_autotune(self._h, A.FP32 if precision == "fp32" else A.FP64, int(reps),
                                          C.byref(s), C.byref(ms), cand, 32), "mpdg_op_autotune")
         return ({"slabs": s.slabs, "l2_evict_first": bool(s.l2_evict_first),
-                 "overlap_colours": bool(s.overlap_colours)}, ms.value, [c for c in cand if c >= 0.0])
+                 "overlap_colours": bool(s.overlap_colours), "cta_cell_groups": bool(s.cta_cell_groups)},
+                ms.value, [c for c in cand if c >= 0.0])
 
     def device_error(self):
         """Reads and clears the device error word (an expired bounded wait)."""

@@ -8,8 +8,8 @@
 * Config 3 at full size: 128^3 uniform cells, FE_Q(2), advection-diffusion
   with the vortex velocity, theta = 0.5, D = 1e-3, dt = 1e-3
   (advection_diffusion_operator.cpp:238-272, 450-495).
-* Every schedule of the resident apply (z-slabs, L2 hint) returns the same
-  bits as the one-launch-per-colour apply.
+* Every schedule of the resident apply (z-slabs, L2 hint, colour overlap, CTA
+  cell groups) returns the same bits as the one-launch-per-colour apply.
 * CG + Chebyshev(5)/Jacobi at 32^3 Q4 (perturbed, k(T)): the device's Lanczos
   estimate of lambda_max equals the oracle's own estimate from the same start
   vector to 1e-10, and CG with the oracle's own Chebyshev interval takes as
@@ -47,11 +47,12 @@ def _schedules_bit_identical(op, src, dtype):
     ref = torch.empty_like(src)
     op.set_schedule(1, False, prec, overlap_colours=False)
     op.vmult(ref, src)
-    for slabs, hint, overlap in [(1, False, True), (2, False, False), (8, True, True), (16, False, True)]:
-        op.set_schedule(slabs, hint, prec, overlap_colours=overlap)
+    for slabs, hint, overlap, cta in [(1, False, True, False), (2, False, False, False), (8, True, True, True),
+                                      (16, False, True, False), (1, True, True, True)]:
+        op.set_schedule(slabs, hint, prec, overlap_colours=overlap, cta_cell_groups=cta)
         out = torch.empty_like(src)
         op.vmult(out, src)
-        assert torch.equal(out, ref), (slabs, hint, overlap)
+        assert torch.equal(out, ref), (slabs, hint, overlap, cta)
     op.set_schedule(1, False, prec, overlap_colours=False)
     return ref
 
