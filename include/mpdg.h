@@ -44,12 +44,19 @@ enum {
   MPDG_VEL_NONE = 0,
   MPDG_VEL_ROTATION = 1, /* u = s (z, 0, -x): advection_diffusion_vortex.hpp:93-115 (dim 3) */
   MPDG_VEL_VORTEX = 2,   /* u = (sin pi x cos pi y, -cos pi x sin pi y, 0) */
-  MPDG_VEL_CONST = 3     /* u = vel_param */
+  MPDG_VEL_CONST = 3,    /* u = vel_param */
+  /* u given as a DoF vector (MPDG_FIELD_VELOCITY): the velocity field the
+   * reference operators read with read_dof_values_plain
+   * (heat_diffuse_operator.cpp:975-980, advection_diffusion_operator.cpp:461-465) */
+  MPDG_VEL_NODAL = 4
 };
 enum { MPDG_GEOM_AUTO = 0, MPDG_GEOM_GENERAL = 1 };
 enum { MPDG_SOLVER_CG = 0, MPDG_SOLVER_GMRES = 1 };
 enum { MPDG_PREC_IDENTITY = 0, MPDG_PREC_JACOBI = 1, MPDG_PREC_CHEBYSHEV = 2 };
-enum { MPDG_FIELD_TEMPERATURE = 0, MPDG_FIELD_TEMPERATURE_OLD = 1, MPDG_FIELD_HEAVISIDE = 2 };
+/* MPDG_FIELD_VELOCITY: 3 n_dofs values, component-major (u_x of every DoF,
+ * then u_y, then u_z), for operators with vel_kind MPDG_VEL_NODAL */
+enum { MPDG_FIELD_TEMPERATURE = 0, MPDG_FIELD_TEMPERATURE_OLD = 1, MPDG_FIELD_HEAVISIDE = 2,
+       MPDG_FIELD_VELOCITY = 3 };
 /* heat material laws (MaterialTypes; Material::compute_parameters_internal,
  * include/meltpooldg/core/material.templates.hpp:213-760).  LINEAR: rho_cp and
  * k(T) = k0 (1 + k_alpha T).  The phase laws interpolate the gas / liquid / solid
@@ -218,7 +225,9 @@ mpdg_status mpdg_op_use_dirichlet(mpdg_op *op, int use_dirichlet);
  * operator folds k(T) into its per-quadrature-point coefficients when this is
  * called: a caller that changes the field's values in place calls it again
  * before the next vmult (the reference re-reads T in every vmult,
- * heat_diffuse_operator.cpp:1000-1012). */
+ * heat_diffuse_operator.cpp:1000-1012).  MPDG_FIELD_VELOCITY (3 n_dofs values)
+ * is interpolated to the quadrature points when set, into the stream
+ * JxW J^-1 u the apply reads (and tau_K with SUPG); the same rule applies. */
 mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *device_values);
 /* the same with host values, copied into operator-owned device memory */
 mpdg_status mpdg_op_set_field_host(mpdg_op *op, int field, const double *host_values);

@@ -18,11 +18,11 @@ OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_NOT_CONVERGED, ERR_BREAKDOWN, ERR_NAN, ERR
     ERR_BUDGET, ERR_SIZE = 0, -1, -2, -3, -4, -5, -6, -7, -8, -9
 OP_HEAT, OP_ADVDIFF = 0, 1
 FP64, FP32 = 0, 1
-VEL_NONE, VEL_ROTATION, VEL_VORTEX, VEL_CONST = 0, 1, 2, 3
+VEL_NONE, VEL_ROTATION, VEL_VORTEX, VEL_CONST, VEL_NODAL = 0, 1, 2, 3, 4
 GEOM_AUTO, GEOM_GENERAL = 0, 1
 SOLVER_CG, SOLVER_GMRES = 0, 1
 PREC_IDENTITY, PREC_JACOBI, PREC_CHEBYSHEV = 0, 1, 2
-FIELD_TEMPERATURE, FIELD_TEMPERATURE_OLD, FIELD_HEAVISIDE = 0, 1, 2
+FIELD_TEMPERATURE, FIELD_TEMPERATURE_OLD, FIELD_HEAVISIDE, FIELD_VELOCITY = 0, 1, 2, 3
 MAT_LINEAR, MAT_GAS_LIQUID, MAT_LIQUID_SOLID, MAT_GAS_LIQUID_SOLID = 0, 1, 2, 3
 
 _STATUS_NAMES = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_ALLOC", -4: "ERR_NOT_CONVERGED",

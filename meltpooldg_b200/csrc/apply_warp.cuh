@@ -573,8 +573,12 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
 
     // velocity parts that do not vary along the lane's z column (uniform mesh)
     Real uv0[3] = {0, 0, 0};
-    if (GEOM != GEOM_GENERAL && has_vel && p.vel_kind != MPDG_VEL_ROTATION)
+    const bool nodal_vel = GEOM != GEOM_GENERAL && p.vel_kind == MPDG_VEL_NODAL;
+    if (GEOM != GEOM_GENERAL && has_vel && p.vel_kind != MPDG_VEL_ROTATION && !nodal_vel)
       uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, 0, uv0);
+    // velocity given as a DoF vector on a uniform mesh: the stream JxW J^-1 u,
+    // read from global memory (lanes of a cell read consecutive values)
+    const Real *vq = nodal_vel ? p.velb + (p.cfirst + (cidx < count ? cidx : 0)) * (long)VS + j * n + i : nullptr;
 
     Real val[n], fx[n], fy[n], fz[n];
     const Real *ms = stage + s_sub * MS + j * n + i;
@@ -597,7 +601,11 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
         fz[k] = G02 * gx[k] + G12 * gy[k] + G22 * gz[k];
       } else {
         const Real JxW = p.hvol * T.w[i] * T.w[j] * T.w[k];
-        if (has_vel) {
+        if (nodal_vel) {
+          b0 = p.c_vel * vq[k * n2];
+          b1 = p.c_vel * vq[k * n2 + n3];
+          b2 = p.c_vel * vq[k * n2 + 2 * n3];
+        } else if (has_vel) {
           Real uv[3] = {uv0[0], uv0[1], uv0[2]};
           if (p.vel_kind == MPDG_VEL_ROTATION) uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, k, uv);
           const Real cj = p.c_vel * JxW;

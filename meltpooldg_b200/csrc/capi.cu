@@ -230,7 +230,7 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     if (!mesh || !desc || !out) throw Error{MPDG_ERR_ARG, "null argument"};
     if (desc->kind != MPDG_OP_HEAT && desc->kind != MPDG_OP_ADVDIFF) throw Error{MPDG_ERR_ARG, "unknown operator kind"};
     if (!(desc->dt > 0.0)) throw Error{MPDG_ERR_ARG, "time increment must be positive"};
-    if (desc->vel_kind < MPDG_VEL_NONE || desc->vel_kind > MPDG_VEL_CONST) throw Error{MPDG_ERR_ARG, "unknown velocity kind"};
+    if (desc->vel_kind < MPDG_VEL_NONE || desc->vel_kind > MPDG_VEL_NODAL) throw Error{MPDG_ERR_ARG, "unknown velocity kind"};
     Mesh &mm = mesh->m;
     if (mm.fine && (desc->k_alpha != 0.0 || desc->full_tangent || (desc->robin_faces && desc->robin_alpha != 0.0)))
       throw Error{MPDG_ERR_UNSUPPORTED,
@@ -246,6 +246,10 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     if (desc->supg && desc->kind != MPDG_OP_ADVDIFF)
       throw Error{MPDG_ERR_ARG, "SUPG stabilisation applies to the advection-diffusion operator"};
     if (desc->supg && mm.fine) throw Error{MPDG_ERR_UNSUPPORTED, "SUPG on two-level meshes"};
+    if (desc->vel_kind == MPDG_VEL_NODAL && mm.fine)
+      throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take no fields (velocity as a DoF vector)"};
+    if (desc->vel_kind == MPDG_VEL_NODAL && desc->supg && mm.mapped)
+      throw Error{MPDG_ERR_UNSUPPORTED, "SUPG on mapped meshes"};
     if (mm.mapped && (desc->supg || (desc->robin_faces && desc->robin_alpha != 0.0) ||
                       (desc->rad_faces && desc->rad_emissivity != 0.0)))
       throw Error{MPDG_ERR_UNSUPPORTED, "mapped meshes take no boundary faces or SUPG"};
@@ -300,7 +304,7 @@ void free_op_arrays(Op &o)
                   (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32, (void *)o.d_trig64, o.d_stage,
                   (void *)o.d_tau64, (void *)o.d_tau32, (void *)o.Told_own, (void *)o.H_own, (void *)o.Told32,
                   (void *)o.H32, (void *)o.lsq_buf, (void *)o.host_stage,
-                  (void *)o.d_io, o.io_tmp})
+                  (void *)o.d_io, o.io_tmp, (void *)o.U_own})
     if (p) cudaFree(p);
   if (o.pipe_in) {
     cudaStreamSynchronize(o.pipe_in);
@@ -355,8 +359,28 @@ void field_slots(Op &o, int field, const double **&slot, double **&own)
     case MPDG_FIELD_TEMPERATURE: slot = &o.T64; own = &o.T_own; return;
     case MPDG_FIELD_TEMPERATURE_OLD: slot = &o.Told64; own = &o.Told_own; return;
     case MPDG_FIELD_HEAVISIDE: slot = &o.H64; own = &o.H_own; return;
+    case MPDG_FIELD_VELOCITY:
+      if (o.d.vel_kind != MPDG_VEL_NODAL)
+        throw Error{MPDG_ERR_ARG, "MPDG_FIELD_VELOCITY needs an operator created with vel_kind MPDG_VEL_NODAL"};
+      slot = &o.U64;
+      own = &o.U_own;
+      return;
     default: throw Error{MPDG_ERR_ARG, "unknown field"};
   }
+}
+
+// values of a field: n_dofs, or 3 n_dofs for the velocity
+size_t field_count(const Op &o, int field) { return (field == MPDG_FIELD_VELOCITY ? 3 : 1) * (size_t)o.mesh->N; }
+
+// what setting a field rebuilds
+void field_changed(Op &o, int field)
+{
+  if (field == MPDG_FIELD_VELOCITY) {
+    build_nodal_velocity(o);
+    return;
+  }
+  invalidate_coef(o);
+  if (o.d.precision_mask & (1 << MPDG_FP32)) ensure_T32(o);
 }
 }  // namespace
 
@@ -369,8 +393,7 @@ mpdg_status mpdg_op_set_field(mpdg_op *op, int field, const double *values)
     field_slots(op->o, field, slot, own);
     if (op->o.fine) throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take no fields"};
     *slot = values;
-    invalidate_coef(op->o);
-    if (values && (op->o.d.precision_mask & (1 << MPDG_FP32))) ensure_T32(op->o);
+    if (values || field != MPDG_FIELD_VELOCITY) field_changed(op->o, field);
     return MPDG_OK;
   });
 }
@@ -384,7 +407,7 @@ mpdg_status mpdg_op_set_field_host(mpdg_op *op, int field, const double *values)
     double **own = nullptr;
     field_slots(o, field, slot, own);
     if (o.fine) throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take no fields"};
-    const size_t bytes = sizeof(double) * o.mesh->N;
+    const size_t bytes = sizeof(double) * field_count(o, field);
     if (!*own) {
       MPDG_CUDA(tracked_malloc(own, bytes));
       o.device_bytes += bytes;
@@ -392,8 +415,7 @@ mpdg_status mpdg_op_set_field_host(mpdg_op *op, int field, const double *values)
     MPDG_CUDA(cudaMemcpyAsync(*own, values, bytes, cudaMemcpyHostToDevice, o.stream));
     MPDG_CUDA(cudaStreamSynchronize(o.stream));
     *slot = *own;
-    invalidate_coef(o);
-    if (o.d.precision_mask & (1 << MPDG_FP32)) ensure_T32(o);
+    field_changed(o, field);
     return MPDG_OK;
   });
 }

@@ -179,7 +179,11 @@ struct Op {
   const double *Told64 = nullptr, *H64 = nullptr;
   double *Told_own = nullptr, *H_own = nullptr;
   float *Told32 = nullptr, *H32 = nullptr;  // FP32: T - T_old and the heaviside
-  double *d_velb64 = nullptr;          // general geometry + velocity: [cell][3][n^3]
+  // velocity as a DoF vector (MPDG_VEL_NODAL): component-major [3][N],
+  // caller-owned or set from host values
+  const double *U64 = nullptr;
+  double *U_own = nullptr;
+  double *d_velb64 = nullptr;          // general geometry or nodal velocity: [cell][3][n^3]
   float *d_velb32 = nullptr;
   float *d_trig32 = nullptr;           // uniform vortex velocity: sin/cos tables
   double *d_tau64 = nullptr;           // SUPG: tau_K per colour-major cell
@@ -274,6 +278,9 @@ void shape_1d(int p, double *S, double *D, double *w, double *x);
 void build_mesh_device_data(Mesh &m, const uint8_t *host_mask, bool force_general);
 void ensure_metric32(Mesh &m, cudaStream_t s);
 void build_op_device_data(Op &op);
+// interpolates the nodal velocity field op.U64 to the quadrature points: the
+// stream JxW J^-1 u of the apply (both precisions) and, with SUPG, tau_K
+void build_nodal_velocity(Op &op);
 void ensure_T32(Op &op);
 void fma_peak(double &gflops64, double &gflops32);
 void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d);

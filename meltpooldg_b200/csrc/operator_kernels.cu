@@ -679,7 +679,14 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
       G11 = JxW / (p.h[1] * p.h[1]);
       G22 = JxW / (p.h[2] * p.h[2]);
       G01 = G02 = G12 = 0;
-      if (p.vel_kind != MPDG_VEL_NONE) {
+      if (p.vel_kind == MPDG_VEL_NODAL) {
+        if (active) {  // the stream JxW J^-1 u of the velocity field
+          const Real *vb = p.velb + cell * velb_stride(n) + k * n2 + j * n + i;
+          b0 = vb[0];
+          b1 = vb[n3];
+          b2 = vb[2 * n3];
+        }
+      } else if (p.vel_kind != MPDG_VEL_NONE) {
         Real uv[3];
         uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, k, uv);
         b0 = JxW * uv[0] / p.h[0];
@@ -875,7 +882,14 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
       G11 = JxW / (p.h[1] * p.h[1]);
       G22 = JxW / (p.h[2] * p.h[2]);
       G01 = G02 = G12 = 0;
-      if (p.vel_kind != MPDG_VEL_NONE) {
+      if (p.vel_kind == MPDG_VEL_NODAL) {
+        if (active) {  // the stream JxW J^-1 u of the velocity field
+          const Real *vb = p.velb + cell * velb_stride(n) + k * n2 + j * n + i;
+          b0 = vb[0];
+          b1 = vb[n3];
+          b2 = vb[2 * n3];
+        }
+      } else if (p.vel_kind != MPDG_VEL_NONE) {
         Real uv[3];
         uniform_velocity<Real, n>(p, T, ix, iy, iz, i, j, k, uv);
         b0 = JxW * uv[0] / p.h[0];
@@ -1127,6 +1141,81 @@ __global__ void velb_kernel(const double *vert, int nc0, int nc1, long n_cells, 
   }
 }
 
+// per (cell, qp) of a colour-major cell: the nodal velocity field U
+// (component-major [3][N], the vector the reference operators read with
+// read_dof_values_plain, heat_diffuse_operator.cpp:975-980,
+// advection_diffusion_operator.cpp:461-465) interpolated to the Gauss point
+// with the Gauss-Lobatto basis, u_q = sum_{a,b,c} S(q_x,a) S(q_y,b) S(q_z,c)
+// U(dof(a,b,c)); then the apply's stream value w adj(J) u_q = JxW J^-1 u_q (as
+// velb_kernel) and, for tau_K, |u_q|.  Lattice cells find their DoFs from their
+// position, mapped cells through the cell->DoF map.
+__global__ void nodal_velb_kernel(const double *vert, int nc0, int nc1, long NX, long NY, long N, long n_cells,
+                                  int P, const Colour *colours, const double *cellvert, const int *cmap,
+                                  const double *U, double *velb, float *velb32, double *umag)
+{
+  const int n = P + 1, n3 = n * n * n;
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= n_cells * n3) return;
+  const long cell = gid / n3;
+  const int q = (int)(gid % n3);
+  const Tables<double> &T = tab<double>(P);
+  const int qi = q % n, qj = (q / n) % n, qk = q / (n * n);
+  long base = 0;
+  if (!cmap) {
+    int c = 0;
+    while (c < 7 && cell >= colours[c + 1].first) ++c;
+    const Colour &C = colours[c];
+    const long cidx = cell - C.first;
+    const long ix = 2 * (cidx % C.cn[0]) + C.par[0];
+    const long iy = 2 * ((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
+    const long iz = 2 * (cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
+    base = (iz * P * NY + iy * P) * NX + ix * P;
+  }
+  double u[3] = {0, 0, 0};
+  for (int c = 0; c < n; ++c) {
+    const double sc = T.S[qk * n + c];
+    for (int b = 0; b < n; ++b) {
+      const double sbc = sc * T.S[qj * n + b];
+      for (int a = 0; a < n; ++a) {
+        const double wgt = sbc * T.S[qi * n + a];
+        const long g = cmap ? (long)cmap[cell * n3 + (c * n + b) * n + a] : base + ((long)c * NY + b) * NX + a;
+        u[0] += wgt * U[g];
+        u[1] += wgt * U[N + g];
+        u[2] += wgt * U[2 * N + g];
+      }
+    }
+  }
+  double V[8][3];
+  cell_corners(vert, nc0, nc1, colours, cellvert, cell, V);
+  const double xi[3] = {T.x[qi], T.x[qj], T.x[qk]};
+  const double w = T.w[qi] * T.w[qj] * T.w[qk];
+  double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int v = 0; v < 8; ++v) {
+    const int bx = v & 1, by = (v >> 1) & 1, bz = (v >> 2) & 1;
+    const double f[3] = {bx ? xi[0] : 1 - xi[0], by ? xi[1] : 1 - xi[1], bz ? xi[2] : 1 - xi[2]};
+    const double df[3] = {bx ? 1.0 : -1.0, by ? 1.0 : -1.0, bz ? 1.0 : -1.0};
+    const double dB[3] = {df[0] * f[1] * f[2], f[0] * df[1] * f[2], f[0] * f[1] * df[2]};
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) J[a][b] += V[v][a] * dB[b];
+  }
+  double A[3][3];
+  A[0][0] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  A[0][1] = J[0][2] * J[2][1] - J[0][1] * J[2][2];
+  A[0][2] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+  A[1][0] = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  A[1][1] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+  A[1][2] = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+  A[2][0] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  A[2][1] = J[0][1] * J[2][0] - J[0][0] * J[2][1];
+  A[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+  for (int a = 0; a < 3; ++a) {
+    const double b = w * (A[a][0] * u[0] + A[a][1] * u[1] + A[a][2] * u[2]);
+    velb[cell * velb_stride(n) + a * n3 + q] = b;
+    if (velb32) velb32[cell * velb_stride(n) + a * n3 + q] = (float)b;
+  }
+  if (umag) umag[gid] = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+}
+
 // per colour-major cell: the SUPG parameter tau_K (compute_stabilization_parameter,
 // advection_diffusion_operator.cpp:499-533): coefficient h_K, or, for a negative
 // coefficient, h_K / max_q |u(x_q)| (0 when that maximum is below 1e-6), with the
@@ -1134,7 +1223,7 @@ __global__ void velb_kernel(const double *vert, int nc0, int nc1, long n_cells, 
 // a hexahedron is its longest main diagonal
 __global__ void tau_kernel(const double *vert, int nc0, int nc1, int nc2, int P, const Colour *colours,
                            int vel_kind, double s0, double s1, double s2, double coef, const double *xq_all,
-                           double *tau64, float *tau32)
+                           double *tau64, float *tau32, const double *umag)
 {
   const int n = P + 1;
   const long cell = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1165,6 +1254,10 @@ __global__ void tau_kernel(const double *vert, int nc0, int nc1, int nc2, int P,
   } else {
     double umax = 0.0;
     for (int q = 0; q < n * n * n; ++q) {
+      if (umag) {  // velocity given as a DoF vector: |u| at the Gauss points
+        umax = fmax(umax, umag[cell * n * n * n + q]);
+        continue;
+      }
       const double xi[3] = {xq_all[q % n], xq_all[(q / n) % n], xq_all[q / (n * n)]};
       double x[3] = {0, 0, 0};
       for (int v = 0; v < 8; ++v) {
@@ -1395,15 +1488,22 @@ void build_op_device_data(Op &op)
     MPDG_CUDA(cudaMemcpy(d_xq, xq, sizeof(xq), cudaMemcpyHostToDevice));
     op.d_tau64 = dev_alloc<double>((size_t)m.n_cells, op.device_bytes);
     if (want32) op.d_tau32 = dev_alloc<float>((size_t)m.n_cells, op.device_bytes);
-    tau_kernel<<<grid_for(m.n_cells, 128), 128>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col, op.d.vel_kind,
-                                                  op.d.vel_param[0], op.d.vel_param[1], op.d.vel_param[2],
-                                                  op.d.supg_coefficient, d_xq, op.d_tau64, op.d_tau32);
-    MPDG_LAUNCHED();
+    if (op.d.vel_kind == MPDG_VEL_NODAL && op.d.supg_coefficient < 0.0) {
+      // tau_K = h_K / max |u| follows the velocity field (build_nodal_velocity)
+      MPDG_CUDA(cudaMemset(op.d_tau64, 0, sizeof(double) * m.n_cells));
+      if (op.d_tau32) MPDG_CUDA(cudaMemset(op.d_tau32, 0, sizeof(float) * m.n_cells));
+    } else {
+      tau_kernel<<<grid_for(m.n_cells, 128), 128>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col,
+                                                    op.d.vel_kind, op.d.vel_param[0], op.d.vel_param[1],
+                                                    op.d.vel_param[2], op.d.supg_coefficient, d_xq, op.d_tau64,
+                                                    op.d_tau32, nullptr);
+      MPDG_LAUNCHED();
+    }
     MPDG_CUDA(cudaDeviceSynchronize());
     cudaFree(d_col);
     cudaFree(d_xq);
   }
-  if (op.d.vel_kind == MPDG_VEL_NONE) return;
+  if (op.d.vel_kind == MPDG_VEL_NONE || op.d.vel_kind == MPDG_VEL_NODAL) return;  // nodal: at set_field
   if (!m.uniform) {
     Colour *d_col = nullptr;
     MPDG_CUDA(tracked_malloc(&d_col, sizeof(m.colour)));
@@ -1458,6 +1558,59 @@ void build_op_device_data(Op &op)
   }
 }
 
+void build_nodal_velocity(Op &op)
+{
+  Mesh &m = *op.mesh;
+  if (op.d.vel_kind != MPDG_VEL_NODAL)
+    throw Error{MPDG_ERR_ARG, "MPDG_FIELD_VELOCITY needs an operator created with vel_kind MPDG_VEL_NODAL"};
+  if (!op.U64) return;
+  const int p = m.degree, n = p + 1, n3 = n * n * n;
+  const bool want32 = (op.d.precision_mask & (1 << MPDG_FP32)) != 0;
+  const size_t count = (size_t)m.n_cells * velb_stride(n);
+  if (!op.d_velb64) {
+    op.d_velb64 = dev_alloc<double>(count, op.device_bytes);
+    MPDG_CUDA(cudaMemsetAsync(op.d_velb64, 0, sizeof(double) * count, op.stream));
+  }
+  if (want32 && !op.d_velb32) {
+    op.d_velb32 = dev_alloc<float>(count, op.device_bytes);
+    MPDG_CUDA(cudaMemsetAsync(op.d_velb32, 0, sizeof(float) * count, op.stream));
+  }
+  const bool with_tau = op.d.kind == MPDG_OP_ADVDIFF && op.d.supg && op.d.supg_coefficient < 0.0;
+  Colour *d_col = nullptr;
+  double *umag = nullptr, *d_xq = nullptr;
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(op.stream);
+    if (d_col) cudaFree(d_col);
+    if (umag) cudaFree(umag);
+    if (d_xq) cudaFree(d_xq);
+  };
+  try {
+    MPDG_CUDA(tracked_malloc(&d_col, sizeof(m.colour)));
+    MPDG_CUDA(cudaMemcpyAsync(d_col, m.colour, sizeof(m.colour), cudaMemcpyHostToDevice, op.stream));
+    if (with_tau) MPDG_CUDA(tracked_malloc(&umag, sizeof(double) * (size_t)m.n_cells * n3));
+    const long total = m.n_cells * n3;
+    nodal_velb_kernel<<<grid_for(total, 256), 256, 0, op.stream>>>(
+        m.d_vert, m.nc[0], m.nc[1], m.NX, m.NY, m.N, m.n_cells, p, d_col, m.d_cellvert, m.d_cmap, op.U64,
+        op.d_velb64, want32 ? op.d_velb32 : nullptr, umag);
+    MPDG_LAUNCHED();
+    if (with_tau) {
+      double xq[kMaxN], wq[kMaxN];
+      gauss(n, xq, wq);
+      MPDG_CUDA(tracked_malloc(&d_xq, sizeof(xq)));
+      MPDG_CUDA(cudaMemcpyAsync(d_xq, xq, sizeof(xq), cudaMemcpyHostToDevice, op.stream));
+      tau_kernel<<<grid_for(m.n_cells, 128), 128, 0, op.stream>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col,
+                                                                 op.d.vel_kind, 0.0, 0.0, 0.0,
+                                                                 op.d.supg_coefficient, d_xq, op.d_tau64,
+                                                                 op.d_tau32, umag);
+      MPDG_LAUNCHED();
+    }
+  } catch (...) {
+    cleanup();
+    throw;
+  }
+  cleanup();
+}
+
 __global__ void diff_cast_kernel(const double *a, const double *b, float *c, long n)
 {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1507,6 +1660,10 @@ KP<Real> base_params(Op &op)
     k.vel_param[d] = (Real)op.d.vel_param[d];
   }
   k.vel_kind = op.d.vel_kind;
+  if (op.d.vel_kind == MPDG_VEL_NODAL && !op.d_velb64)
+    throw Error{MPDG_ERR_ARG, "the operator needs the velocity field (MPDG_FIELD_VELOCITY)"};
+  if (op.d.vel_kind == MPDG_VEL_NODAL && sizeof(Real) == 4 && !op.d_velb32)
+    throw Error{MPDG_ERR_ARG, "the FP32 form was not prepared for this operator (precision_mask)"};
   for (int d = 0; d < 3; ++d) {
     k.ih[d] = (Real)(1.0 / m.h[d]);
     k.ih2[d] = (Real)(1.0 / (m.h[d] * m.h[d]));

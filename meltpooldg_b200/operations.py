@@ -32,10 +32,15 @@ class AdvectionDiffusionOperation:
 
     def __init__(self, mesh, dt, theta=0.5, diffusivity=0.0, velocity=None, dirichlet_values=None,
                  linear_solver: LinearSolverData = None, device="cuda", inflow_outflow=None, supg=False,
-                 supg_coefficient=-1.0):
+                 supg_coefficient=-1.0, velocity_field=None):
         self.mesh = mesh
         self.op = AdvectionDiffusionOperator(mesh, dt, theta=theta, diffusivity=diffusivity,
-                                             velocity=velocity, supg=supg, supg_coefficient=supg_coefficient)
+                                             velocity="nodal" if velocity_field is not None else velocity,
+                                             supg=supg, supg_coefficient=supg_coefficient)
+        if velocity_field is not None:
+            # the velocity as a DoF vector (3 n_dofs, component-major), e.g. the flow solver's
+            self.velocity = torch.tensor(np.asarray(velocity_field, np.float64).reshape(-1), device=device)
+            self.op.set_velocity(self.velocity)
         self.io = None
         if inflow_outflow is not None:
             io_mask, io_vals = inflow_outflow
@@ -103,13 +108,18 @@ class HeatDiffuseOperation:
                  linear_solver: LinearSolverData = None, residual_tolerance=1e-9,
                  field_correction_tolerance=1e-10, max_nonlinear_iterations=10, device="cuda",
                  robin_alpha=0.0, robin_t_inf=0.0, robin_faces=(), rad_emissivity=0.0, rad_t_inf=0.0,
-                 rad_faces=(), velocity=None, material=None, heaviside=None):
+                 rad_faces=(), velocity=None, material=None, heaviside=None, velocity_field=None):
         self.mesh = mesh
         self.op = HeatDiffuseOperator(mesh, dt, rho_cp=rho_cp, k0=k0, k_alpha=k_alpha,
                                       full_tangent=full_tangent, robin_alpha=robin_alpha,
                                       robin_t_inf=robin_t_inf, robin_faces=robin_faces,
                                       rad_emissivity=rad_emissivity, rad_t_inf=rad_t_inf, rad_faces=rad_faces,
-                                      velocity=velocity, material=material)
+                                      velocity="nodal" if velocity_field is not None else velocity,
+                                      material=material)
+        if velocity_field is not None:
+            # the velocity as a DoF vector (3 n_dofs, component-major), e.g. the flow solver's
+            self.velocity = torch.tensor(np.asarray(velocity_field, np.float64).reshape(-1), device=device)
+            self.op.set_velocity(self.velocity)
         self.dt = dt
         self.time = 0.0
         self.heaviside = heaviside

@@ -245,6 +245,16 @@ class _MatrixFreeOperator:
     def compute_diagonal(self, diag):
         A.check(A.lib().mpdg_compute_diagonal(self._h, _dptr(diag)), "compute_diagonal")
 
+    def set_velocity(self, U):
+        """The velocity as a DoF vector (operators created with velocity="nodal"):
+        a contiguous CUDA float64 tensor of 3 n_dofs values, component-major
+        (shape (3, n_dofs) or (3 n_dofs,)) -- the vector the reference operators
+        read with read_dof_values_plain (heat_diffuse_operator.cpp:975-980,
+        advection_diffusion_operator.cpp:461-465).  Call again after changing
+        its values."""
+        self._fields["U"] = U
+        A.check(A.lib().mpdg_op_set_field(self._h, A.FIELD_VELOCITY, _dptr(U)), "set_field")
+
     def set_schedule(self, slabs=1, l2_evict_first=False, precision="fp64", overlap_colours=False,
                      cta_cell_groups=False):
         """Schedule of the resident apply (mpdg_op_set_schedule): colour launches
@@ -402,6 +412,8 @@ def _velocity(v):
     if isinstance(v, str):
         if v == "vortex":
             return A.VEL_VORTEX, (0.0, 0.0, 0.0)
+        if v == "nodal":
+            return A.VEL_NODAL, (0.0, 0.0, 0.0)
         raise ValueError(v)
     if isinstance(v, tuple) and v and v[0] == "rotation":
         return A.VEL_ROTATION, (float(v[1]), 0.0, 0.0)

@@ -2,7 +2,7 @@
 into reference_outputs.json.  Run once in a container where the reference
 sources are mounted (read as text only); the JSON is the committed fixture:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference checkout>
 """
 import json
 import os
@@ -80,4 +80,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the reference checkout>")
+    main(sys.argv[1])

@@ -150,3 +150,21 @@ def test_cg_and_gmres_reach_tolerance():
     x3, it3, hist3, ok3 = O.cg(m, op, b, inv_diag=inv, rel_tol=1e-10,
                                chebyshev={"degree": 5, "lambda_min": lam / 30, "lambda_max": 1.2 * lam})
     assert ok3 and it3 < it and np.abs(x3 - xs).max() < 1e-8
+
+
+def test_oracle_nodal_velocity_of_a_constant_field_equals_the_constant_velocity():
+    """The oracle's velocity-as-a-DoF-vector path (ORC_VEL_NODAL, the field
+    interpolated to the quadrature points) against its prescribed constant
+    velocity on perturbed cells: the two operators agree to rounding."""
+    import numpy as np
+    from oracle import oracle as O
+    nc, p = (3, 4, 2), 3
+    V = O.box_vertices(3, nc, (0, 0, 0), (1, 1, 1), 0.1, 5)
+    om = O.Mesh(3, p, nc, V)
+    vel = (0.3, -0.2, 0.7)
+    U = np.concatenate([np.full(om.n_dofs, v) for v in vel])
+    src = np.random.Generator(np.random.PCG64(1)).uniform(-1, 1, om.n_dofs)
+    for kind in (O.HEAT, O.ADVDIFF):
+        a = O.vmult(om, O.Operator(kind, 1e-2, theta=0.5, diffusivity=1e-2, vel_kind=O.VEL_CONST, vel_param=vel), src)
+        b = O.vmult(om, O.Operator(kind, 1e-2, theta=0.5, diffusivity=1e-2, vel_kind=O.VEL_NODAL, vel_nodal=U), src)
+        assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max()
