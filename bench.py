@@ -622,7 +622,7 @@ def run_batch(args, rank, world):
         t0 = time.perf_counter()
         with B.Batch(budget, capacity=len(probs)) as bt:
             ts = [bt.submit(p, rhs=rhs[i] if e2e else None) for i, p in enumerate(probs)]
-            tune_res = bt.autotune() if tune else None
+            tune_res = (bt.autotune(), bt.shape()) if tune else None
             gsteps, _ = bt.run(poll_steps=16)
             res = [bt.take(t, p.n_dofs if (e2e or keep) else None) for t, p in zip(ts, probs)]
         t1 = time.perf_counter()
@@ -630,7 +630,7 @@ def run_batch(args, rank, world):
 
     # warm-up (also the autotuner's pass over this membership)
     _, _, _, tune_res = one_batch(tune=True)
-    cap, apply_ms = tune_res
+    (cap, apply_ms), shape = tune_res
     for _ in range(max(0, args.warmup - 1)):
         one_batch()
     launches0 = M.kernel_launches()
@@ -664,7 +664,7 @@ def run_batch(args, rank, world):
             "frac": b_apply / (apply_ms * 1e-3) / 1e9 / peak, "traffic": None,
             "algorithmic_bytes": b_apply,
             "kernel": f"batch_apply_kernel<float> x 8 colour launches over all {len(probs)} problems",
-            "apply_ms": apply_ms, "autotuned_ctas_per_sm": cap,
+            "apply_ms": apply_ms, "autotuned_shape": shape,
             "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
     cpu = None
     if rank == 0 and not args.no_cpu:

@@ -428,9 +428,17 @@ mpdg_status mpdg_batch_poll(mpdg_batch *batch, int64_t ticket, mpdg_solve_report
 /* copies a finished problem's solution to the host (x_host may be NULL), fills
  * the report and releases the problem's slot and memory */
 mpdg_status mpdg_batch_take(mpdg_batch *batch, int64_t ticket, double *x_host, mpdg_solve_report *report);
-/* picks the resident CTAs per SM of the batched apply by timing the current
- * membership (call once problems are admitted); returns the choice and its time */
+/* the batch's autotuner: times the batched FP32 apply of the current
+ * membership (call once problems are admitted) over its block and tile shapes
+ * -- 2, 4 or 8 warps per CTA, the conflict-minimal or the plain tile layout,
+ * and 1, 2, 3, 4, 6, 8 or the occupancy maximum of resident CTAs per SM --
+ * and keeps the fastest; returns its CTAs per SM and time (mpdg_batch_shape
+ * reads the whole shape).  No reference counterpart (the reference has no
+ * batched solves). */
 mpdg_status mpdg_batch_autotune(mpdg_batch *batch, int *ctas_per_sm, double *apply_ms);
+/* the shape the batched apply runs with: warps per CTA, tile layout (1: the
+ * conflict-minimal one) and resident CTAs per SM (0: occupancy maximum) */
+mpdg_status mpdg_batch_shape(mpdg_batch *batch, int *warps_per_cta, int *tuned_tiles, int *ctas_per_sm);
 /* device bytes admitted now */
 mpdg_status mpdg_batch_used_bytes(mpdg_batch *batch, int64_t *bytes);
 /* counters of the last mpdg_serve call (n <= 9 values): host seconds spent in

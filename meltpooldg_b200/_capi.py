@@ -170,6 +170,7 @@ def lib():
     L.mpdg_batch_poll.argtypes = [vp, C.c_int64, C.POINTER(SolveReport)]
     L.mpdg_batch_take.argtypes = [vp, C.c_int64, dp, C.POINTER(SolveReport)]
     L.mpdg_batch_autotune.argtypes = [vp, ip, dp]
+    L.mpdg_batch_shape.argtypes = [vp, ip, ip, ip]
     L.mpdg_batch_used_bytes.argtypes = [vp, i64p]
     L.mpdg_batch_stats.argtypes = [vp, dp, C.c_int]
     L.mpdg_serve.argtypes = [vp, pd, dp, C.c_int, C.c_int, C.POINTER(dp), dp, dp,

@@ -144,10 +144,18 @@ class Batch:
         return x, rep.as_dict()
 
     def autotune(self):
-        """(resident CTAs per SM chosen for the batched apply, its time in ms)."""
+        """Picks the batched apply's block and tile shape by timing the current
+        membership; returns (resident CTAs per SM, its time in ms)."""
         cap, ms = C.c_int(), C.c_double()
         check(lib().mpdg_batch_autotune(self._h, C.byref(cap), C.byref(ms)), "mpdg_batch_autotune")
         return int(cap.value), float(ms.value)
+
+    def shape(self):
+        """The batched apply's shape: warps per CTA, tile layout, CTAs per SM."""
+        w, t, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().mpdg_batch_shape(self._h, C.byref(w), C.byref(t), C.byref(c)), "mpdg_batch_shape")
+        return {"warps_per_cta": w.value, "tile_layout": "conflict-minimal" if t.value else "plain",
+                "ctas_per_sm": c.value}
 
     @property
     def used_bytes(self) -> int:

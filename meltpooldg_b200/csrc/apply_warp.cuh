@@ -236,6 +236,17 @@ struct TileLayout {
   static constexpr int elems = t0_elems + t1_elems;
 };
 
+// the plain tile layout of a warp group (z-plane stride n^2, cell offset n^3):
+// one of the layouts the batched apply's autotuner tries
+template <int n, typename Real>
+struct PlainTileLayout {
+  static constexpr int cells = 32 / (n * n);
+  static constexpr int s0 = n * n, sc0 = n * n * n, s1 = n * n, sc1 = n * n * n;
+  static constexpr int t0_elems = (cells - 1) * sc0 + (n - 1) * s0 + n * n;
+  static constexpr int t1_elems = t0_elems;
+  static constexpr int elems = t0_elems + t1_elems;
+};
+
 // the tiles of a cell group are shared by a warp (GROUP 32) or the whole CTA
 template <bool CTA>
 __device__ __forceinline__ void group_sync()

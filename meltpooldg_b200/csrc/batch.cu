@@ -100,7 +100,7 @@ struct Batch {
   BatchSchedule sched[3];    // heat slots, advection-diffusion slots, defect slots
   cudaGraphExec_t graph = nullptr;
   int64_t step_kernels = 0;  // kernels of one graph step
-  int tuned_cap = 0;         // resident CTAs per SM of the batched apply (0 = occupancy maximum)
+  BatchShape shape;          // block and tile shape of the batched FP32 apply (autotuned)
   double tuned_ms = 0;
   double *d_norms = nullptr;  // |x|^2 of finished slots (serving)
   double *h_norms = nullptr;  // pinned
@@ -1020,8 +1020,9 @@ void drop_graph(Batch &B)
 }
 
 // one Krylov step of every running slot (the body of the graph)
-void enqueue_step(Batch &B, int cap)
+void enqueue_step(Batch &B, const BatchShape &shape)
 {
+  const BatchShape shape64;  // the FP64 defect applies (a few per solve) keep the default shape
   cudaStream_t st = B.stream;
   const int S = B.capacity;
   const unsigned gs = (unsigned)((S + 255) / 256), gc = kChunkBlocks;
@@ -1037,18 +1038,18 @@ void enqueue_step(Batch &B, int cap)
   bk_schedule<<<9, kSchedThreads, 0, st>>>(B.d_active, MPDG_OP_ADVDIFF, T.info, S, SA);
   MPDG_LAUNCHED();
   // CG on the heat problems: Ap = A p (FP32), alpha, x/r/z update
-  launch_batch_apply<float>(SH, T.info, B.d_params, T.p, T.Ap, B.d_active, cap, st);
+  launch_batch_apply<float>(SH, T.info, B.d_params, T.p, T.Ap, B.d_active, shape, st);
   BK(bk_dot_pap, gc, SH, T, B.d_active);
   BK(bk_finish_pap, gs, B.d_sc, B.d_active, T, S);
   BK(bk_cg_update, gc, SH, T, B.d_active, B.d_sc);
   BK(bk_cg_decide, gs, B.d_sc, B.d_active, B.d_defect, T, S, B.delta);
   // BiCGStab on the advection-diffusion problems: v = A M p, alpha, s, t = A M s, omega, update
   BK(bk_bicg_precond_p, gc, SA, T, B.d_active, B.d_sc);
-  launch_batch_apply<float>(SA, T.info, B.d_params, T.z, T.v, B.d_active, cap, st);
+  launch_batch_apply<float>(SA, T.info, B.d_params, T.z, T.v, B.d_active, shape, st);
   BK(bk_bicg_alpha_partials, gc, SA, T, B.d_active, B.d_sc);
   BK(bk_bicg_alpha, gs, B.d_sc, B.d_active, T, S);
   BK(bk_bicg_s, gc, SA, T, B.d_active, B.d_sc);
-  launch_batch_apply<float>(SA, T.info, B.d_params, T.z, T.t, B.d_active, cap, st);
+  launch_batch_apply<float>(SA, T.info, B.d_params, T.z, T.t, B.d_active, shape, st);
   BK(bk_bicg_omega_partials, gc, SA, T, B.d_active, B.d_sc);
   BK(bk_bicg_omega, gs, B.d_sc, B.d_active, T, S);
   BK(bk_bicg_update, gc, SA, T, B.d_active, B.d_sc);
@@ -1056,7 +1057,7 @@ void enqueue_step(Batch &B, int cap)
   // FP64 defects b - A x of the slots whose FP32 residual dropped by delta (or that look converged)
   bk_schedule<<<9, kSchedThreads, 0, st>>>(B.d_defect, -1, T.info, S, SD);
   MPDG_LAUNCHED();
-  launch_batch_apply<double>(SD, T.info, B.d_params, T.x, T.r64, B.d_defect, cap, st);
+  launch_batch_apply<double>(SD, T.info, B.d_params, T.x, T.r64, B.d_defect, shape64, st);
   BK(bk_defect, gc, SD, T, B.d_defect);
   BK(bk_defect_decide, gs, B.d_sc, B.d_active, B.d_defect, T, S);
   BK(bk_cg_replace, gc, SD, T, B.d_defect, B.d_sc);
@@ -1082,7 +1083,7 @@ void ensure_graph(Batch &B)
   cudaGraph_t g = nullptr;
   MPDG_CUDA(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
   try {
-    enqueue_step(B, B.tuned_cap);
+    enqueue_step(B, B.shape);
   } catch (...) {
     cudaStreamEndCapture(B.stream, &g);
     if (g) cudaGraphDestroy(g);
@@ -1599,7 +1600,7 @@ mpdg_status mpdg_batch_autotune(mpdg_batch *batch, int *ctas_per_sm, double *app
     for (int s = 0; s < B.capacity; ++s) ones[s] = B.slots[s].used ? 1 : 0;
     int *d_all = balloc<int>(B.capacity);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    int best_cap = 0;
+    BatchShape best_shape;
     double best = 1e30;
     const BatchSchedule &SD = B.sched[2];  // scratch schedule outside the graph steps
     try {
@@ -1609,22 +1610,30 @@ mpdg_status mpdg_batch_autotune(mpdg_batch *batch, int *ctas_per_sm, double *app
       MPDG_LAUNCHED();
       MPDG_CUDA(cudaEventCreate(&e0));
       MPDG_CUDA(cudaEventCreate(&e1));
-      for (int cap : {1, 2, 3, 4, 6, 8, 0}) {
-        launch_batch_apply<float>(SD, B.tab.info, B.d_params, B.tab.p, B.tab.Ap, d_all, cap, B.stream);
-        MPDG_CUDA(cudaEventRecord(e0, B.stream));
-        const int reps = 5;
-        for (int r = 0; r < reps; ++r)
-          launch_batch_apply<float>(SD, B.tab.info, B.d_params, B.tab.p, B.tab.Ap, d_all, cap, B.stream);
-        MPDG_CUDA(cudaEventRecord(e1, B.stream));
-        MPDG_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        MPDG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        const double t = ms / reps;
-        if (t < best * 0.98) {  // prefer the smaller cap unless clearly faster
-          best = t;
-          best_cap = cap;
-        }
-      }
+      // block shape (warps per CTA), tile layout and resident CTAs per SM of the
+      // batched FP32 apply over the current membership
+      for (int wpc : {4, 2, 8})
+        for (int tuned = 1; tuned >= 0; --tuned)
+          for (int cap : {1, 2, 3, 4, 6, 8, 0}) {
+            BatchShape sh;
+            sh.warps_per_cta = wpc;
+            sh.tuned_tiles = tuned != 0;
+            sh.ctas_per_sm = cap;
+            launch_batch_apply<float>(SD, B.tab.info, B.d_params, B.tab.p, B.tab.Ap, d_all, sh, B.stream);
+            MPDG_CUDA(cudaEventRecord(e0, B.stream));
+            const int reps = 5;
+            for (int r = 0; r < reps; ++r)
+              launch_batch_apply<float>(SD, B.tab.info, B.d_params, B.tab.p, B.tab.Ap, d_all, sh, B.stream);
+            MPDG_CUDA(cudaEventRecord(e1, B.stream));
+            MPDG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            MPDG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            const double t = ms / reps;
+            if (t < best * 0.98) {  // keep the earlier (default-like) shape unless clearly faster
+              best = t;
+              best_shape = sh;
+            }
+          }
     } catch (...) {
       cudaStreamSynchronize(B.stream);
       cudaFree(d_all);
@@ -1636,13 +1645,23 @@ mpdg_status mpdg_batch_autotune(mpdg_batch *batch, int *ctas_per_sm, double *app
     cudaFree(d_all);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    B.tuned_cap = best_cap;
+    B.shape = best_shape;
     B.tuned_ms = best;
     drop_graph(B);
-    if (ctas_per_sm) *ctas_per_sm = best_cap;
+    if (ctas_per_sm) *ctas_per_sm = best_shape.ctas_per_sm;
     if (apply_ms) *apply_ms = best;
     return MPDG_OK;
   });
+}
+
+mpdg_status mpdg_batch_shape(mpdg_batch *batch, int *warps_per_cta, int *tuned_tiles, int *ctas_per_sm)
+{
+  if (!batch) return MPDG_ERR_ARG;
+  const BatchShape &sh = batch->b.shape;
+  if (warps_per_cta) *warps_per_cta = sh.warps_per_cta;
+  if (tuned_tiles) *tuned_tiles = sh.tuned_tiles ? 1 : 0;
+  if (ctas_per_sm) *ctas_per_sm = sh.ctas_per_sm;
+  return MPDG_OK;
 }
 
 mpdg_status mpdg_batch_used_bytes(mpdg_batch *batch, int64_t *bytes)

@@ -12,6 +12,8 @@
 // warp_apply_kernel.
 #pragma once
 
+#include <type_traits>
+
 constexpr int kBatchTileElems = 320;   // at least the largest warp_tile_elems over P
 
 __device__ __forceinline__ int batch_find(const int *__restrict__ prefix, int n, int g)
@@ -129,17 +131,19 @@ __device__ __forceinline__ void batch_gather(int colour, int lg, const WarpSlot<
   }
 }
 
-template <int P, typename Real>
+// TUNED: the conflict-minimal tile layouts of the warp apply, else the plain one
+template <int P, typename Real, bool TUNED>
 __device__ __forceinline__ void batch_cell(int colour, int local_group, const WarpSlot<Real> &W,
                                            const Real (&uin)[kMaxN], Real *tiles, int lane)
 {
   constexpr int n = P + 1;
-  static_assert(warp_tile_elems<n, Real>() <= kBatchTileElems, "tile area");
+  using L = typename std::conditional<TUNED, TileLayout<n, Real, 32>, PlainTileLayout<n, Real>>::type;
+  static_assert(L::elems <= kBatchTileElems, "tile area");
   const Tables<Real> &T = tab<Real>(P);
   const BatchLanePos<P> q = batch_pos<P>(colour, local_group, W, lane);
   const int i = q.i, j = q.j, ix = q.ix, iy = q.iy, iz = q.iz;
-  Real *t0 = tiles + q.s_sub * tile_sc<n>();
-  Real *t1 = tiles + tile_elems<n, tile_s2<n>()>() + q.s_sub * tile_sc<n>();
+  Real *t0 = tiles + q.s_sub * L::sc0;
+  Real *t1 = tiles + L::t0_elems + q.s_sub * L::sc1;
   const long NX = q.NX, zs = NX * NX, g0 = q.g0;
   Real *dst = W.dst;
   const bool dir = W.dirichlet;
@@ -164,7 +168,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
 #pragma unroll
   for (int k = 0; k < n; ++k) u[k] = uin[k];
   Real uq[n], gx[n], gy[n], gz[n];
-  l_forward<n>(T, t0, t1, true, i, j, u, uq, gx, gy, gz);
+  l_forward<n, Real, L, false>(T, t0, t1, true, i, j, u, uq, gx, gy, gz);
   Real val[n], fx[n], fy[n], fz[n];
   const Real hvol = (Real)W.hvol, ih = (Real)W.ih, ih2 = (Real)W.ih2;
   const Real c_mass = (Real)W.c_mass, c_vel = (Real)W.c_vel, c_diff = (Real)W.c_diff;
@@ -188,7 +192,7 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
     fz[k] = kd * gz[k];
   }
   Real out[n];
-  l_backward<n>(T, t0, t1, true, i, j, val, fx, fy, fz, out);
+  l_backward<n, Real, L, false>(T, t0, t1, true, i, j, val, fx, fy, fz, out);
   if (q.act) {
 #pragma unroll
     for (int k = 0; k < n; ++k) {
@@ -199,16 +203,24 @@ __device__ __forceinline__ void batch_cell(int colour, int local_group, const Wa
   }
 }
 
-template <typename Real>
-__global__ void __launch_bounds__(kWarpsPerCTA * 32, sizeof(Real) == 8 ? 3 : 4)
+template <typename Real, int WPC>
+struct BatchOcc {  // register budget: 16 (FP32) or 12 (FP64) resident warps per SM
+  static constexpr int warps = sizeof(Real) == 8 ? 12 : 16;
+  static constexpr int min_blocks = warps / WPC > 0 ? warps / WPC : 1;
+};
+
+// WPC warps per CTA and the tile layout (TUNED) are the block and tile shapes
+// the batch's autotuner picks from (mpdg_batch_autotune)
+template <typename Real, int WPC, bool TUNED>
+__global__ void __launch_bounds__(WPC * 32, BatchOcc<Real, WPC>::min_blocks)
     batch_apply_kernel(int colour, const BatchScheduleHeader *__restrict__ hdr,
                        const int *__restrict__ seg_slot, const int *__restrict__ seg_prefix,
                        const SlotInfo *__restrict__ info, const BatchSlotParams *__restrict__ params,
                        Real *const *__restrict__ src_ptrs, Real *const *__restrict__ dst_ptrs,
                        const int *__restrict__ mask)
 {
-  __shared__ Real tiles_all[kWarpsPerCTA][kBatchTileElems];
-  __shared__ WarpSlot<Real> wslot[kWarpsPerCTA][2];
+  __shared__ Real tiles_all[WPC][kBatchTileElems];
+  __shared__ WarpSlot<Real> wslot[WPC][2];
   const int total = hdr->total_groups[colour], nseg = hdr->n_seg[colour];
   if (total == 0) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -216,7 +228,7 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, sizeof(Real) == 8 ? 3 : 4)
   // each warp walks a contiguous range of groups: one binary search per launch,
   // then the segment index only advances (neighbouring groups are neighbouring
   // cells of the same solve)
-  const int nwarps = gridDim.x * kWarpsPerCTA, wid = blockIdx.x * kWarpsPerCTA + warp;
+  const int nwarps = gridDim.x * WPC, wid = blockIdx.x * WPC + warp;
   const int per = (total + nwarps - 1) / nwarps;
   const int gbeg = min(total, wid * per), gend = min(total, gbeg + per);
   if (gbeg >= gend) return;
@@ -254,10 +266,10 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, sizeof(Real) == 8 ? 3 : 4)
     const WarpSlot<Real> &W = wslot[warp][buf];
     if (W.ok) {
       switch (W.degree) {
-        case 1: batch_cell<1, Real>(colour, lg, W, u, tiles, lane); break;
-        case 2: batch_cell<2, Real>(colour, lg, W, u, tiles, lane); break;
-        case 3: batch_cell<3, Real>(colour, lg, W, u, tiles, lane); break;
-        default: batch_cell<4, Real>(colour, lg, W, u, tiles, lane); break;
+        case 1: batch_cell<1, Real, TUNED>(colour, lg, W, u, tiles, lane); break;
+        case 2: batch_cell<2, Real, TUNED>(colour, lg, W, u, tiles, lane); break;
+        case 3: batch_cell<3, Real, TUNED>(colour, lg, W, u, tiles, lane); break;
+        default: batch_cell<4, Real, TUNED>(colour, lg, W, u, tiles, lane); break;
       }
     }
     __syncwarp();  // the slot buffer of this group may be reloaded for the group after next

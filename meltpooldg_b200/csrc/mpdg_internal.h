@@ -264,11 +264,20 @@ struct BatchSchedule {
 int cells_per_warp(int degree);
 // one-time set-up of the batched apply (tables, occupancy): before any graph capture
 void batch_apply_setup();
+// block and tile shape of the batched apply (picked by mpdg_batch_autotune):
+// warps per CTA (2, 4, 8), the conflict-minimal or the plain tile layout, and
+// the resident CTAs per SM of its persistent grid (0: the occupancy maximum)
+struct BatchShape {
+  int warps_per_cta = 4;
+  bool tuned_tiles = true;
+  int ctas_per_sm = 0;
+};
 // one launch per colour over the scheduled slots whose mask entry is set; persistent
-// grid of SMs x min(cap, occupancy) CTAs (cap 0: the occupancy maximum)
+// grid of SMs x min(ctas_per_sm, occupancy) CTAs
 template <typename Real>
 void launch_batch_apply(const BatchSchedule &sched, const SlotInfo *info, const BatchSlotParams *params,
-                        Real *const *src, Real *const *dst, const int *mask, int cap, cudaStream_t s);
+                        Real *const *src, Real *const *dst, const int *mask, const BatchShape &shape,
+                        cudaStream_t s);
 
 // ---- operator kernels (operator_kernels.cu)
 // 1D tables of degree p on [0,1]: GLL Lagrange basis values S[q*(p+1)+i] and

@@ -2895,42 +2895,72 @@ int cells_per_warp(int degree)
 }
 
 namespace {
-template <typename Real>
+template <typename Real, int WPC, bool TUNED>
 int batch_occupancy()
 {
   static int blocks_per_sm = 0;
   if (!blocks_per_sm) {
     upload_tables();
-    MPDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, batch_apply_kernel<Real>,
-                                                            kWarpsPerCTA * 32, 0));
+    MPDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, batch_apply_kernel<Real, WPC, TUNED>,
+                                                            WPC * 32, 0));
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   return blocks_per_sm;
 }
-}  // namespace
 
-void batch_apply_setup()
-{
-  batch_occupancy<float>();
-  batch_occupancy<double>();
-}
-
-template <typename Real>
-void launch_batch_apply(const BatchSchedule &sched, const SlotInfo *info, const BatchSlotParams *params,
+template <typename Real, int WPC, bool TUNED>
+void launch_batch_shape(const BatchSchedule &sched, const SlotInfo *info, const BatchSlotParams *params,
                         Real *const *src, Real *const *dst, const int *mask, int cap, cudaStream_t s)
 {
-  const int occ = batch_occupancy<Real>();  // tables uploaded before any launch (and before graph capture)
+  const int occ = batch_occupancy<Real, WPC, TUNED>();  // tables uploaded before any launch (and capture)
   const int blocks = num_sms() * ((cap > 0) ? std::min(cap, occ) : occ);
   for (int c = 0; c < 8; ++c) {
-    batch_apply_kernel<Real><<<(unsigned)blocks, kWarpsPerCTA * 32, 0, s>>>(
+    batch_apply_kernel<Real, WPC, TUNED><<<(unsigned)blocks, WPC * 32, 0, s>>>(
         c, sched.hdr, sched.seg_slot + (size_t)c * sched.cap, sched.seg_prefix + (size_t)c * sched.cap, info,
         params, src, dst, mask);
     MPDG_LAUNCHED();
   }
 }
+
+template <typename Real>
+void batch_setup_all()
+{
+  batch_occupancy<Real, 2, true>();
+  batch_occupancy<Real, 4, true>();
+  batch_occupancy<Real, 8, true>();
+  batch_occupancy<Real, 2, false>();
+  batch_occupancy<Real, 4, false>();
+  batch_occupancy<Real, 8, false>();
+}
+}  // namespace
+
+void batch_apply_setup()
+{
+  batch_setup_all<float>();
+  batch_setup_all<double>();
+}
+
+template <typename Real>
+void launch_batch_apply(const BatchSchedule &sched, const SlotInfo *info, const BatchSlotParams *params,
+                        Real *const *src, Real *const *dst, const int *mask, const BatchShape &shape,
+                        cudaStream_t s)
+{
+  const int cap = shape.ctas_per_sm;
+  switch (shape.warps_per_cta * 2 + (shape.tuned_tiles ? 1 : 0)) {
+    case 4: launch_batch_shape<Real, 2, false>(sched, info, params, src, dst, mask, cap, s); break;
+    case 5: launch_batch_shape<Real, 2, true>(sched, info, params, src, dst, mask, cap, s); break;
+    case 8: launch_batch_shape<Real, 4, false>(sched, info, params, src, dst, mask, cap, s); break;
+    case 9: launch_batch_shape<Real, 4, true>(sched, info, params, src, dst, mask, cap, s); break;
+    case 16: launch_batch_shape<Real, 8, false>(sched, info, params, src, dst, mask, cap, s); break;
+    case 17: launch_batch_shape<Real, 8, true>(sched, info, params, src, dst, mask, cap, s); break;
+    default: throw Error{MPDG_ERR_ARG, "batched apply: warps per CTA must be 2, 4 or 8"};
+  }
+}
 template void launch_batch_apply<double>(const BatchSchedule &, const SlotInfo *, const BatchSlotParams *,
-                                         double *const *, double *const *, const int *, int, cudaStream_t);
+                                         double *const *, double *const *, const int *, const BatchShape &,
+                                         cudaStream_t);
 template void launch_batch_apply<float>(const BatchSchedule &, const SlotInfo *, const BatchSlotParams *,
-                                        float *const *, float *const *, const int *, int, cudaStream_t);
+                                        float *const *, float *const *, const int *, const BatchShape &,
+                                        cudaStream_t);
 
 }  // namespace mpdg

@@ -163,6 +163,9 @@ def test_autotune_keeps_results():
         ts = [bt.submit(p) for p in ps]
         cap, ms = bt.autotune()
         assert cap in (0, 1, 2, 3, 4, 6, 8) and ms > 0
+        shape = bt.shape()
+        assert shape["warps_per_cta"] in (2, 4, 8) and shape["ctas_per_sm"] == cap
+        assert shape["tile_layout"] in ("conflict-minimal", "plain")
         bt.run()
         got = [bt.take(t, p.n_dofs)[0] for t, p in zip(ts, ps)]
     for a, b in zip(ref, got):
