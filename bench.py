@@ -348,8 +348,9 @@ def run_operator_workload(args, rank, world, headline):
     mesh = M.Mesh(V, nc, p, mask)
     N = mesh.n_dofs
     op, Td = make_operator(M, mesh, T)
-    # the library's autotuner picks the apply schedule per precision (untimed)
-    tuned = {prec: op.autotune(prec, reps=10)[:2] for prec in ("fp64", "fp32")}
+    # the library's autotuner picks the apply schedule per precision (untimed);
+    # --no-autotune keeps the operator's default schedule (profiling runs)
+    tuned = {} if args.no_autotune else {prec: op.autotune(prec, reps=10)[:2] for prec in ("fp64", "fp32")}
     rng = np.random.Generator(np.random.PCG64(0))
     src = torch.tensor(rng.uniform(-1.0, 1.0, N), device="cuda")
     dst = torch.empty_like(src)
@@ -526,7 +527,8 @@ def run_operator_workload(args, rank, world, headline):
                            }.get(WL["name"], "inputs larger than L2: coefficient stream 1.8 GB per apply"),
                        schedule={"fp64": sched64, "fp32": sched32,
                                  "autotuned_ms": {k: v[1] for k, v in tuned.items()},
-                                 "picked_by": "mpdg_op_autotune (10 applies per candidate)"}),
+                                 "picked_by": "default schedule" if args.no_autotune else
+                                 "mpdg_op_autotune (10 applies per candidate)"}),
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": None if args.no_e2e else {
@@ -851,6 +853,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=5.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="headline workload only")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default apply schedule")
     ap.add_argument("--cells", type=int, default=0,
                     help="cells per direction (default: the workload's; smaller sizes for profiling)")
     ap.add_argument("--workload", default=None, choices=["heat", "advdiff", "c1", "batch", "serve"],
