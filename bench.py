@@ -53,12 +53,14 @@ THETA, DIFFUSIVITY = 0.5, 1e-3
 # config 3, "c1" = config 1), cells per direction and degree
 WL = {"name": "heat", "nc": [64, 64, 64], "degree": 4}
 
-# dram__bytes_read.sum + dram__bytes_write.sum of the FP64 warp apply kernel,
-# per apply (8 colour launches), heat workload at 64^3 cells: the 48^3 capture
-# of profiles/warp_apply_q4_general_48c.md (288.8 MB over two colour launches,
-# 1155 MB per apply of 110,592 cells) scaled by the cells of an apply
-# (262,144 / 110,592); traffic grows with the cells processed.
-MEASURED_TRAFFIC_BYTES = {("heat", 64): 2.784e9}
+# dram__bytes_read.sum + dram__bytes_write.sum of the FP64 warp apply kernel
+# (default schedule: CTA cell groups), per apply (8 colour launches): the heat
+# workload's 48^3 capture of profiles/warp_apply_q4_general_48c.md (286.9 MB
+# over two colour launches, 1,147.6 MB per apply of 110,592 cells) scaled by
+# the cells of a 64^3 apply (262,144 / 110,592), as traffic grows with the
+# cells processed; the level-set workload's capture is at full size
+# (profiles/warp_apply_q2_uniform_128c.md: 381.4 MB over two launches).
+MEASURED_TRAFFIC_BYTES = {("heat", 64): 2.720e9, ("advdiff", 128): 1.526e9}
 
 
 def set_workload(name, cells=0):
@@ -436,7 +438,8 @@ def run_operator_workload(args, rank, world, headline):
     roof = {"bound": "hbm", "achieved": b64 / apply_s / 1e9, "peak": peak, "unit": "GB/s",
             "frac": b64 / apply_s / 1e9 / peak, "traffic": traffic,
             "traffic_note": None if traffic is None else
-            "ncu dram read+write per apply (8 launches), 48^3 capture scaled by cells",
+            ("ncu dram read+write per apply (8 launches), 48^3 capture scaled by cells" if WL["name"] == "heat"
+             else "ncu dram read+write per apply (8 launches), full-size capture"),
             "algorithmic_bytes": b64, "kernel": f"warp_apply_kernel<{p},double,{geom}> x 8 colour launches",
             "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
             "streamed": {"bytes": st64, "achieved": st64 / apply_s / 1e9, "frac": st64 / apply_s / 1e9 / peak},
