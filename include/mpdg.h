@@ -273,7 +273,13 @@ mpdg_status mpdg_vmult_multi(mpdg_op *op, int n_vectors, double *const *dst, con
  * dst wait for it; cta_cell_groups lets the four warps of a CTA share their
  * cells (5 Q4 cells or 14 Q2 cells per 128 threads instead of 4 or 12, so
  * fewer lanes idle; the tile exchanges become CTA barriers), for degrees 2
- * and 4 on lattice meshes.  Results are identical for every schedule.  No reference
+ * and 4 on lattice meshes.  lane_cells (uniform lattices of degree 1 or 2,
+ * constant coefficients, one operand, velocities other than MPDG_VEL_NODAL)
+ * gives every cell one thread that keeps its whole sum factorisation in
+ * registers; 32 lanes own a row segment of cells and add their shared x-faces
+ * by warp shuffles, so these launches colour by segment parity in x.  Results
+ * are identical for every schedule without lane_cells, and agree with them to
+ * rounding with it.  No reference
  * counterpart: the schedule of deal.II's MatrixFree::cell_loop
  * (heat_diffuse_operator.cpp:183) is internal to it. */
 typedef struct {
@@ -281,6 +287,7 @@ typedef struct {
   int l2_evict_first;   /* 0 or 1 */
   int overlap_colours;  /* 0 or 1 */
   int cta_cell_groups;  /* 0 or 1 */
+  int lane_cells;       /* 0: warp apply; 1, 2: lane apply, 2 with more registers per thread */
 } mpdg_schedule;
 mpdg_status mpdg_op_set_schedule(mpdg_op *op, int precision, const mpdg_schedule *schedule);
 mpdg_status mpdg_op_get_schedule(mpdg_op *op, int precision, mpdg_schedule *schedule);

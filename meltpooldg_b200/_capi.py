@@ -88,7 +88,7 @@ class SolveReport(C.Structure):
 
 class Schedule(C.Structure):
     _fields_ = [("slabs", C.c_int), ("l2_evict_first", C.c_int), ("overlap_colours", C.c_int),
-                ("cta_cell_groups", C.c_int)]
+                ("cta_cell_groups", C.c_int), ("lane_cells", C.c_int)]
 
 
 class ProblemDesc(C.Structure):

@@ -488,6 +488,8 @@ mpdg_status mpdg_op_set_schedule(mpdg_op *op, int precision, const mpdg_schedule
     op->o.sched[precision].evict_first = sched->l2_evict_first ? 1 : 0;
     op->o.sched[precision].pdl = sched->overlap_colours ? 1 : 0;
     op->o.sched[precision].cta = sched->cta_cell_groups ? 1 : 0;
+    if (sched->lane_cells < 0 || sched->lane_cells > 2) throw Error{MPDG_ERR_ARG, "lane_cells must be 0, 1 or 2"};
+    op->o.sched[precision].lane = sched->lane_cells;
     return MPDG_OK;
   });
 }
@@ -501,6 +503,7 @@ mpdg_status mpdg_op_get_schedule(mpdg_op *op, int precision, mpdg_schedule *sche
     sched->l2_evict_first = op->o.sched[precision].evict_first;
     sched->overlap_colours = op->o.sched[precision].pdl;
     sched->cta_cell_groups = op->o.sched[precision].cta;
+    sched->lane_cells = op->o.sched[precision].lane;
     return MPDG_OK;
   });
 }
@@ -522,6 +525,7 @@ mpdg_status mpdg_op_autotune(mpdg_op *op, int precision, int reps, mpdg_schedule
       best->l2_evict_first = b.evict_first;
       best->overlap_colours = b.pdl;
       best->cta_cell_groups = b.cta;
+      best->lane_cells = b.lane;
     }
     if (apply_ms) *apply_ms = ms;
     if (candidate_ms)

@@ -164,6 +164,7 @@ struct ApplySchedule {
   int evict_first = 0;  // L2 evict-first hint on the coefficient stream
   int pdl = 1;          // colour launches as programmatic dependents of the previous one
   int cta = 0;          // cell groups of a whole CTA (Q2, Q4) instead of a warp
+  int lane = 0;         // one thread per cell (Q1, Q2 on uniform lattices, constant coefficients)
 };
 
 struct Op {

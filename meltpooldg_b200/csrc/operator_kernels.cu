@@ -539,6 +539,7 @@ __device__ __forceinline__ void law_eval(const KP<Real> &p, Real T, Real H, Real
 }
 
 #include "apply_warp.cuh"
+#include "apply_lane.cuh"
 #include "batch_apply.cuh"
 
 // ------------------------------------------------------------ the cell kernel
@@ -1916,9 +1917,96 @@ void run_warp_apply(Op &op, KP<Real> k)
   }
 }
 
+// the lane apply serves uniform lattices of degree 1 or 2 with one operand, no
+// hanging DoFs and a velocity it evaluates in-kernel
+template <typename Real>
+bool lane_apply_eligible(const Op &op, const KP<Real> &k)
+{
+  const Mesh &m = *op.mesh;
+  return m.uniform && !m.mapped && (m.degree == 1 || m.degree == 2) && k.hsrc == nullptr && k.nvec <= 1 &&
+         k.vel_kind != MPDG_VEL_NODAL;
+}
+
+template <int P, typename Real, int VK, int WIDE>
+void run_lane_apply(Op &op, KP<Real> k)
+{
+  Mesh &m = *op.mesh;
+  if (m.N >= (1L << 32)) throw Error{MPDG_ERR_UNSUPPORTED, "the lane apply indexes DoFs with 32 bits"};
+  constexpr int prec = sizeof(Real) == 4 ? MPDG_FP32 : MPDG_FP64;
+  const bool use_pdl = op.sched[prec].pdl != 0;
+  LaneColour lc{};
+  for (int c = 0; c < 8; ++c) {
+    lc.pfirst[c] = m.colour[c].first;
+    lc.pcn0[c] = m.colour[c].cn[0];
+    lc.pcn1[c] = m.colour[c].cn[1];
+  }
+  const int nseg = (m.nc[0] + kLaneSeg - 1) / kLaneSeg;
+  int launched = 0;
+  // the colour launches of cell layers [zlo, zhi) (all layers when empty), in
+  // the order x-segment parity, then y, then z parity
+  auto colour_launches = [&](int zlo, int zhi) {
+    for (int c = 0; c < 8; ++c) {
+      lc.sx = c & 1;
+      lc.py = (c >> 1) & 1;
+      lc.pz = (c >> 2) & 1;
+      lc.nsx = (nseg - lc.sx + 1) / 2;
+      lc.cny = (m.nc[1] - lc.py + 1) / 2;
+      const int zi0 = (zlo - lc.pz + 1) / 2, zi1 = (zhi - lc.pz + 1) / 2;
+      lc.zi0 = zi0;
+      lc.nwarps = (long)lc.nsx * lc.cny * std::max(0, zi1 - zi0);
+      if (lc.nwarps == 0) continue;
+      const bool pdl = use_pdl && launched > 0;
+      k.pdl = pdl ? 1 : 0;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)((lc.nwarps + 3) / 4));
+      cfg.blockDim = dim3(128);
+      cfg.dynamicSmemBytes = 0;
+      cfg.stream = op.stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = pdl ? 1 : 0;
+      MPDG_CUDA(cudaLaunchKernelEx(&cfg, lane_apply_kernel<P, Real, VK, WIDE>, k, lc));
+      MPDG_LAUNCHED();
+      ++launched;
+    }
+  };
+  if (k.zhi > k.zlo) {
+    colour_launches(k.zlo, k.zhi);
+    return;
+  }
+  // z-slabs with odd interior ends keep the first-touch rule across slabs
+  int bounds[kMaxApplySlabs + 1];
+  const int ns = slab_bounds(m.nc[2], apply_slabs(op, prec), bounds);
+  for (int sl = 0; sl < ns; ++sl) colour_launches(bounds[sl], bounds[sl + 1]);
+}
+
+template <int P, typename Real, int WIDE>
+void lane_apply_velocity(Op &op, const KP<Real> &k)
+{
+  switch (k.vel_kind) {
+    case MPDG_VEL_NONE: run_lane_apply<P, Real, LANE_VEL_NONE, WIDE>(op, k); break;
+    case MPDG_VEL_CONST: run_lane_apply<P, Real, LANE_VEL_CONST, WIDE>(op, k); break;
+    case MPDG_VEL_VORTEX: run_lane_apply<P, Real, LANE_VEL_VORTEX, WIDE>(op, k); break;
+    case MPDG_VEL_ROTATION: run_lane_apply<P, Real, LANE_VEL_ROTATION, WIDE>(op, k); break;
+    default: throw Error{MPDG_ERR_UNSUPPORTED, "velocity kind not evaluated by the lane apply"};
+  }
+}
+
 template <typename Real, int GEOM>
 void warp_apply_degree(Op &op, const KP<Real> &k)
 {
+  if constexpr (GEOM == GEOM_UNIFORM) {
+    const int lane = op.sched[sizeof(Real) == 4 ? MPDG_FP32 : MPDG_FP64].lane;
+    if (lane && lane_apply_eligible(op, k)) {
+      // Q1 fits either bound without spilling: one variant
+      if (op.mesh->degree == 1) lane_apply_velocity<1, Real, 0>(op, k);
+      else if (lane == 2) lane_apply_velocity<2, Real, 1>(op, k);
+      else lane_apply_velocity<2, Real, 0>(op, k);
+      return;
+    }
+  }
   const bool hang = k.hsrc != nullptr;
   if constexpr (GEOM == GEOM_GENERAL) {
     if (op.mesh->mapped) {
@@ -2418,10 +2506,15 @@ void autotune_apply(Op &op, int precision, int reps, ApplySchedule &best, double
   std::vector<ApplySchedule> cand;
   const bool stream = !m.uniform || m.mapped;
   const bool cta_differs = (m.degree == 2 || m.degree == 4) && !m.mapped && !op.fine;
+  // the lane apply: uniform lattices of degree 1 or 2 whose vmult takes the
+  // constant-coefficient path with an in-kernel velocity
+  const bool lane_ok = m.uniform && !m.mapped && !op.fine && (m.degree == 1 || m.degree == 2) &&
+                       plain_warp_apply(op) && !uses_kT(op) && op.d.vel_kind != MPDG_VEL_NODAL;
+  const int lane_max = lane_ok ? (m.degree == 2 ? 2 : 1) : 0;
   for (int S : {1, 2}) {
     if (S > 1 && (S > m.nc[2] / 2 || m.mapped || op.fine)) continue;
     for (int h = 0; h <= (stream ? 1 : 0); ++h)
-      for (int d = 0; d <= 1; ++d)
+      for (int d = 0; d <= 1; ++d) {
         for (int g = 0; g <= (cta_differs ? 1 : 0); ++g) {
           ApplySchedule c;
           c.slabs = S;
@@ -2430,6 +2523,15 @@ void autotune_apply(Op &op, int precision, int reps, ApplySchedule &best, double
           c.cta = g;
           cand.push_back(c);
         }
+        for (int l = 1; l <= lane_max; ++l) {
+          ApplySchedule c;
+          c.slabs = S;
+          c.evict_first = h;
+          c.pdl = d;
+          c.lane = l;
+          cand.push_back(c);
+        }
+      }
   }
   void *x = nullptr, *y = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -256,13 +256,16 @@ class _MatrixFreeOperator:
         A.check(A.lib().mpdg_op_set_field(self._h, A.FIELD_VELOCITY, _dptr(U)), "set_field")
 
     def set_schedule(self, slabs=1, l2_evict_first=False, precision="fp64", overlap_colours=False,
-                     cta_cell_groups=False):
+                     cta_cell_groups=False, lane_cells=0):
         """Schedule of the resident apply (mpdg_op_set_schedule): colour launches
         slab by slab over `slabs` z-slabs of cell layers, the L2 evict-first
         hint on the coefficient stream, colour launches that overlap the
-        previous colour's tail (programmatic dependent launch), and cell groups
-        shared by a whole CTA (degrees 2 and 4).  Results do not depend on it."""
-        s = A.Schedule(int(slabs), int(bool(l2_evict_first)), int(bool(overlap_colours)), int(bool(cta_cell_groups)))
+        previous colour's tail (programmatic dependent launch), cell groups
+        shared by a whole CTA (degrees 2 and 4), and one thread per cell
+        (lane_cells 1 or 2: uniform lattices of degree 1 or 2).  Results do not
+        depend on it, except for rounding with lane_cells."""
+        s = A.Schedule(int(slabs), int(bool(l2_evict_first)), int(bool(overlap_colours)), int(bool(cta_cell_groups)),
+                       int(lane_cells))
         A.check(A.lib().mpdg_op_set_schedule(self._h, A.FP32 if precision == "fp32" else A.FP64, C.byref(s)),
                 "mpdg_op_set_schedule")
 
@@ -271,18 +274,20 @@ class _MatrixFreeOperator:
         A.check(A.lib().mpdg_op_get_schedule(self._h, A.FP32 if precision == "fp32" else A.FP64, C.byref(s)),
                 "mpdg_op_get_schedule")
         return {"slabs": s.slabs, "l2_evict_first": bool(s.l2_evict_first),
-                "overlap_colours": bool(s.overlap_colours), "cta_cell_groups": bool(s.cta_cell_groups)}
+                "overlap_colours": bool(s.overlap_colours), "cta_cell_groups": bool(s.cta_cell_groups),
+                 "lane_cells": s.lane_cells}
 
     def autotune(self, precision="fp64", reps=10):
         """Times the candidate schedules of the resident apply (mpdg_op_autotune)
         and keeps the fastest; returns (schedule, ms per apply, candidate times)."""
         s = A.Schedule()
         ms = C.c_double()
-        cand = (C.c_double * 32)()
+        cand = (C.c_double * 64)()
         A.check(A.lib().mpdg_op_autotune(self._h, A.FP32 if precision == "fp32" else A.FP64, int(reps),
-                                         C.byref(s), C.byref(ms), cand, 32), "mpdg_op_autotune")
+                                         C.byref(s), C.byref(ms), cand, 64), "mpdg_op_autotune")
         return ({"slabs": s.slabs, "l2_evict_first": bool(s.l2_evict_first),
-                 "overlap_colours": bool(s.overlap_colours), "cta_cell_groups": bool(s.cta_cell_groups)},
+                 "overlap_colours": bool(s.overlap_colours), "cta_cell_groups": bool(s.cta_cell_groups),
+                 "lane_cells": s.lane_cells},
                 ms.value, [c for c in cand if c >= 0.0])
 
     def device_error(self):

@@ -12,10 +12,10 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-SCHEDULES = [dict(slabs=1, l2_evict_first=False, overlap_colours=True, cta_cell_groups=False),
-             dict(slabs=1, l2_evict_first=False, overlap_colours=True, cta_cell_groups=True),
-             dict(slabs=1, l2_evict_first=True, overlap_colours=False, cta_cell_groups=True),
-             dict(slabs=2, l2_evict_first=True, overlap_colours=True, cta_cell_groups=True)]
+SCHEDULES = [dict(slabs=1, l2_evict_first=False, overlap_colours=True, cta_cell_groups=False, lane_cells=0),
+             dict(slabs=1, l2_evict_first=False, overlap_colours=True, cta_cell_groups=True, lane_cells=0),
+             dict(slabs=1, l2_evict_first=True, overlap_colours=False, cta_cell_groups=True, lane_cells=0),
+             dict(slabs=2, l2_evict_first=True, overlap_colours=True, cta_cell_groups=True, lane_cells=0)]
 
 
 @pytest.mark.parametrize("p", [1, 2, 3, 4])
