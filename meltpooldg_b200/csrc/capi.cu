@@ -270,6 +270,13 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     // 64^3 Q4 FP64 0.490 -> 0.485 ms; Q4 FP32 0.294 -> 0.299 ms, kept on warps)
     o.sched[MPDG_FP64].cta = (mm.degree == 2 || mm.degree == 4) ? 1 : 0;
     o.sched[MPDG_FP32].cta = mm.degree == 2 ? 1 : 0;
+    // the lane apply (uniform lattices, constant coefficients; other operators
+    // keep the warp apply) measured faster for Q2 on a B200: 128^3 advection-
+    // diffusion 0.664 -> 0.372 ms FP64, 0.431 -> 0.216 ms FP32; 64^3 heat
+    // 0.092 -> 0.052 ms FP64.  Below ~20^3 cells the warp apply is a little
+    // faster (16^3: 19.6 vs 20.5 us); the autotuner decides there.
+    o.sched[MPDG_FP64].lane = mm.degree == 2 ? 2 : 0;
+    o.sched[MPDG_FP32].lane = mm.degree == 2 ? 2 : 0;
     try {
       build_op_device_data(o);
       if (mm.fine) {

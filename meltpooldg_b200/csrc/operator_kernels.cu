@@ -1923,7 +1923,7 @@ template <typename Real>
 bool lane_apply_eligible(const Op &op, const KP<Real> &k)
 {
   const Mesh &m = *op.mesh;
-  return m.uniform && !m.mapped && (m.degree == 1 || m.degree == 2) && k.hsrc == nullptr && k.nvec <= 1 &&
+  return m.uniform && !m.mapped && (m.degree == 1 || m.degree == 2) && k.hsrc == nullptr &&
          k.vel_kind != MPDG_VEL_NODAL;
 }
 
@@ -2000,10 +2000,19 @@ void warp_apply_degree(Op &op, const KP<Real> &k)
   if constexpr (GEOM == GEOM_UNIFORM) {
     const int lane = op.sched[sizeof(Real) == 4 ? MPDG_FP32 : MPDG_FP64].lane;
     if (lane && lane_apply_eligible(op, k)) {
-      // Q1 fits either bound without spilling: one variant
-      if (op.mesh->degree == 1) lane_apply_velocity<1, Real, 0>(op, k);
-      else if (lane == 2) lane_apply_velocity<2, Real, 1>(op, k);
-      else lane_apply_velocity<2, Real, 0>(op, k);
+      // a uniform lattice streams no coefficients, so a multi-vector apply
+      // loses nothing by applying its vectors in turn (and then returns the
+      // bits of the single applies)
+      for (int v = 0; v < std::max(1, k.nvec); ++v) {
+        KP<Real> kv = k;
+        kv.src = k.nvec > 1 ? k.msrc[v] : k.src;
+        kv.dst = k.nvec > 1 ? k.mdst[v] : k.dst;
+        kv.nvec = 1;
+        // Q1 fits either bound without spilling: one variant
+        if (op.mesh->degree == 1) lane_apply_velocity<1, Real, 0>(op, kv);
+        else if (lane == 2) lane_apply_velocity<2, Real, 1>(op, kv);
+        else lane_apply_velocity<2, Real, 0>(op, kv);
+      }
       return;
     }
   }

@@ -9,7 +9,8 @@
   with the vortex velocity, theta = 0.5, D = 1e-3, dt = 1e-3
   (advection_diffusion_operator.cpp:238-272, 450-495).
 * Every schedule of the resident apply (z-slabs, L2 hint, colour overlap, CTA
-  cell groups) returns the same bits as the one-launch-per-colour apply.
+  cell groups) returns the same bits as the one-launch-per-colour apply; the
+  lane apply of config 3 (one thread per cell) matches the oracle likewise.
 * CG + Chebyshev(5)/Jacobi at 32^3 Q4 (perturbed, k(T)): the device's Lanczos
   estimate of lambda_max equals the oracle's own estimate from the same start
   vector to 1e-10, and CG with the oracle's own Chebyshev interval takes as
@@ -84,6 +85,16 @@ def test_config3_full_size_vmult_parity(cuda):
     assert relerr(d64.cpu().numpy(), ref) < TOL64
     d32 = _schedules_bit_identical(op, dev(src, torch.float32), torch.float32)
     assert relerr(d32.double().cpu().numpy(), ref) < TOL32
+    # the lane apply (one thread per cell; 4 x-segments per row of cells), in
+    # both register variants, one launch per colour and in z-slabs
+    for prec, dtype, tol in (("fp64", torch.float64, TOL64), ("fp32", torch.float32, TOL32)):
+        s = dev(src, dtype)
+        for lane, slabs in ((1, 1), (2, 1), (2, 4)):
+            op.set_schedule(slabs, False, prec, overlap_colours=True, lane_cells=lane)
+            out = torch.full_like(s, float("nan"))
+            op.vmult(out, s)
+            assert relerr(out.double().cpu().numpy(), ref) < tol, (prec, lane, slabs)
+    assert op.device_error() == 0
 
 
 def lanczos_start(n, mask, seed=4):
