@@ -287,7 +287,7 @@ typedef struct {
   int l2_evict_first;   /* 0 or 1 */
   int overlap_colours;  /* 0 or 1 */
   int cta_cell_groups;  /* 0 or 1 */
-  int lane_cells;       /* 0: warp apply; 1, 2: lane apply, 2 with more registers per thread */
+  int lane_cells;       /* 0: warp apply; 1, 2: lane apply, 2 with more resident CTAs per SM */
 } mpdg_schedule;
 mpdg_status mpdg_op_set_schedule(mpdg_op *op, int precision, const mpdg_schedule *schedule);
 mpdg_status mpdg_op_get_schedule(mpdg_op *op, int precision, mpdg_schedule *schedule);

@@ -29,6 +29,7 @@
 //    of dst wait for it (griddepcontrol.wait).
 
 constexpr int kLaneSeg = 32;  // cells of an x-segment: the lanes of a warp
+constexpr int kLaneN2 = 9, kLaneN3 = 27;  // tables sized for Q2
 
 // one colour launch of the lane apply
 struct LaneColour {
@@ -46,20 +47,34 @@ struct LaneColour {
 enum { LANE_VEL_NONE = 0, LANE_VEL_CONST = 1, LANE_VEL_VORTEX = 2, LANE_VEL_ROTATION = 3 };
 
 // resident CTAs of 128 threads per SM the register allocation is bounded for:
-// WIDE = 0 favours occupancy (Q2 FP64 spills a few hundred bytes), WIDE = 1
-// gives a Q2 cell's sum factorisation registers enough not to spill
-template <int P, typename Real, int WIDE>
+// OCC = 0 gives a Q2 cell's sum factorisation registers enough not to spill
+// (FP64 166, FP32 96 registers); OCC = 1 trades a few spilled values for one
+// more resident CTA per SM (FP64 128, FP32 80 registers)
+template <int P, typename Real, int OCC>
 struct LaneOcc {
   static constexpr int min_blocks =
-      (sizeof(Real) == 8) ? (P == 2 ? (WIDE ? 2 : 3) : 6) : (P == 2 ? (WIDE ? 4 : 5) : 8);
+      (sizeof(Real) == 8) ? (P == 2 ? (OCC ? 4 : 3) : 6) : (P == 2 ? (OCC ? 6 : 5) : 8);
 };
 
-template <int P, typename Real, int VK, int WIDE>
-__global__ void __launch_bounds__(128, LaneOcc<P, Real, WIDE>::min_blocks)
-    lane_apply_kernel(const KP<Real> p, const LaneColour lc)
+// per-quadrature-point coefficients of a uniform lattice, the same for every
+// cell (JxW = hvol w_x w_y w_z, J^-1 = diag(1/h)), kernel parameters so that
+// every product reads a constant-bank operand
+template <typename Real>
+struct LaneCoef {
+  Real mass[kLaneN3];     // c_mass JxW
+  Real diff[3][kLaneN3];  // c_diff JxW / h_d^2
+  Real adv[3][kLaneN3];   // c_vel JxW / h_d times the constant factor of u_d
+  Real line[3][kLaneN2];  // c_diff hvol / h_d^2 times the weights off the line
+  Real K[kLaneN2];        // Dc^T diag(w) Dc
+};
+
+template <int P, typename Real, int VK, int OCC>
+__global__ void __launch_bounds__(128, LaneOcc<P, Real, OCC>::min_blocks)
+    lane_apply_kernel(const KP<Real> p, const LaneColour lc, const LaneCoef<Real> c)
 {
   constexpr int n = P + 1, n2 = n * n, n3 = n2 * n;
   static_assert(n3 <= 32, "the lane apply keeps one 32-bit Dirichlet mask word per cell");
+  static_assert(n3 <= kLaneN3, "coefficient tables sized for Q2");
   const Tables<Real> &T = tab<Real>(P);
   if (p.pdl) grid_dep_launch_dependents();
   const long w = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -132,14 +147,10 @@ __global__ void __launch_bounds__(128, LaneOcc<P, Real, WIDE>::min_blocks)
       for (int j = 0; j < n; ++j) u[(k * n + j) * n + i] = b[j];
     }
 
-  // per-cell constants: JxW = hvol w_x w_y w_z, J^-1 = diag(1/h)
-  const Real cmass = p.c_mass * p.hvol;
-  const Real cd[3] = {p.c_diff * p.hvol * p.ih2[0], p.c_diff * p.hvol * p.ih2[1], p.c_diff * p.hvol * p.ih2[2]};
-  const Real cv[3] = {p.c_vel * p.hvol * p.ih[0], p.c_vel * p.hvol * p.ih[1], p.c_vel * p.hvol * p.ih[2]};
   // velocity factors at the Gauss coordinates of the cell: vx0, vx1 along x,
   // vy0, vy1 along y, vz along z.  Vortex: u = (sin(pi x) cos(pi y),
   // -cos(pi x) sin(pi y), 0) from the trigonometric table; rotation:
-  // u = (w z, 0, -w x)
+  // u = (w z, 0, -w x) (w folded into the advection table)
   Real vx0[n], vx1[n], vy0[n], vy1[n], vz[n];
 #pragma unroll
   for (int q = 0; q < n; ++q) {
@@ -154,22 +165,21 @@ __global__ void __launch_bounds__(128, LaneOcc<P, Real, WIDE>::min_blocks)
       vz[q] = p.origin[2] + (iz + T.x[q]) * p.h[2];
     }
   }
+  // velocity component d at Gauss point (qx, qy, qz), without the factors the
+  // advection table holds (a constant velocity, the rotation rate and sign)
   auto vel = [&](int d, int qx, int qy, int qz) -> Real {
-    if constexpr (VK == LANE_VEL_CONST) return p.vel_param[d];
-    else if constexpr (VK == LANE_VEL_VORTEX) return d == 0 ? vx0[qx] * vy1[qy] : d == 1 ? -vx1[qx] * vy0[qy] : Real(0);
-    else if constexpr (VK == LANE_VEL_ROTATION) return d == 0 ? p.vel_param[0] * vz[qz] : d == 1 ? Real(0) : -p.vel_param[0] * vx0[qx];
-    else return Real(0);
+    if constexpr (VK == LANE_VEL_VORTEX) return d == 0 ? vx0[qx] * vy1[qy] : vx1[qx] * vy0[qy];
+    else if constexpr (VK == LANE_VEL_ROTATION) return d == 0 ? vz[qz] : vx0[qx];
+    else return Real(1);
   };
 
   // residual at the Gauss points: mass term, then per direction the
   // advection term b_d g_d and the transposed collocation derivative of the
-  // diffusion flux, line by line
+  // diffusion flux, line by line.  Directions without advection apply the
+  // line stiffness K = Dc^T diag(w) Dc to the values at once.
   Real R[n3];
 #pragma unroll
-  for (int q = 0; q < n3; ++q) {
-    const int qx = q % n, qy = (q / n) % n, qz = q / n2;
-    R[q] = cmass * (T.w[qx] * T.w[qy] * T.w[qz]) * u[q];
-  }
+  for (int q = 0; q < n3; ++q) R[q] = c.mass[q] * u[q];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     // directions in which the velocity vanishes identically carry no advection term
@@ -183,21 +193,27 @@ __global__ void __launch_bounds__(128, LaneOcc<P, Real, WIDE>::min_blocks)
 #pragma unroll
         for (int t = 0; t < n; ++t)
           idx[t] = d == 0 ? (b * n + a) * n + t : d == 1 ? (b * n + t) * n + a : (t * n + b) * n + a;
-        Real line[n], g[n], f[n], back[n];
+        Real line[n], back[n];
 #pragma unroll
         for (int t = 0; t < n; ++t) line[t] = u[idx[t]];
-        cz<n, Real, false>(T.Dc, line, g);
+        if (adv) {
+          Real g[n], f[n];
+          cz<n, Real, false>(T.Dc, line, g);
 #pragma unroll
-        for (int t = 0; t < n; ++t) {
-          const int q = idx[t];
-          const int qx = q % n, qy = (q / n) % n, qz = q / n2;
-          const Real W = T.w[qx] * T.w[qy] * T.w[qz];
-          f[t] = cd[d] * W * g[t];
-          if (adv) R[q] += cv[d] * W * vel(d, qx, qy, qz) * g[t];
+          for (int t = 0; t < n; ++t) {
+            const int q = idx[t];
+            const int qx = q % n, qy = (q / n) % n, qz = q / n2;
+            f[t] = c.diff[d][q] * g[t];
+            R[q] += (c.adv[d][q] * vel(d, qx, qy, qz)) * g[t];
+          }
+          cz<n, Real, true>(T.Dc, f, back);
+#pragma unroll
+          for (int t = 0; t < n; ++t) R[idx[t]] += back[t];
+        } else {
+          cz<n, Real, false>(c.K, line, back);
+#pragma unroll
+          for (int t = 0; t < n; ++t) R[idx[t]] += c.line[d][b * n + a] * back[t];
         }
-        cz<n, Real, true>(T.Dc, f, back);
-#pragma unroll
-        for (int t = 0; t < n; ++t) R[idx[t]] += back[t];
       }
   }
 

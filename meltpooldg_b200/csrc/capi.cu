@@ -274,9 +274,11 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     // keep the warp apply) measured faster for Q2 on a B200: 128^3 advection-
     // diffusion 0.664 -> 0.372 ms FP64, 0.431 -> 0.216 ms FP32; 64^3 heat
     // 0.092 -> 0.052 ms FP64.  Below ~20^3 cells the warp apply is a little
-    // faster (16^3: 19.6 vs 20.5 us); the autotuner decides there.
-    o.sched[MPDG_FP64].lane = mm.degree == 2 ? 2 : 0;
-    o.sched[MPDG_FP32].lane = mm.degree == 2 ? 2 : 0;
+    // faster (16^3: 19.6 vs 20.5 us), so the default starts at 32^3 cells;
+    // the autotuner decides case by case.
+    const int lane_default = (mm.degree == 2 && mm.n_cells >= 32768) ? 1 : 0;
+    o.sched[MPDG_FP64].lane = lane_default;
+    o.sched[MPDG_FP32].lane = lane_default;
     try {
       build_op_device_data(o);
       if (mm.fine) {

@@ -1927,9 +1927,50 @@ bool lane_apply_eligible(const Op &op, const KP<Real> &k)
          k.vel_kind != MPDG_VEL_NODAL;
 }
 
-template <int P, typename Real, int VK, int WIDE>
+// the per-quadrature-point coefficient tables of the lane apply (degree P,
+// velocity kind VK) for the operator's constants
+template <int P, typename Real, int VK>
+LaneCoef<Real> lane_coef(const KP<Real> &k)
+{
+  constexpr int n = P + 1, n2 = n * n, n3 = n2 * n;
+  double xq[kMaxN], wq[kMaxN], Dc[kMaxN * kMaxN];
+  gauss(n, xq, wq);
+  for (int q = 0; q < n; ++q)
+    for (int r = 0; r < n; ++r) {
+      double v, d;
+      lagrange(n, xq, r, xq[q], v, d);
+      Dc[q * n + r] = d;
+    }
+  const double hvol = (double)k.hvol;
+  double vf[3] = {1.0, 1.0, 1.0};  // the velocity factor the kernel does not evaluate
+  if (VK == LANE_VEL_CONST) for (int d = 0; d < 3; ++d) vf[d] = (double)k.vel_param[d];
+  if (VK == LANE_VEL_VORTEX) vf[1] = -1.0;
+  if (VK == LANE_VEL_ROTATION) vf[0] = (double)k.vel_param[0], vf[2] = -(double)k.vel_param[0];
+  LaneCoef<Real> c{};
+  for (int q = 0; q < n3; ++q) {
+    const double W = wq[q % n] * wq[(q / n) % n] * wq[q / n2];
+    c.mass[q] = (Real)((double)k.c_mass * hvol * W);
+    for (int d = 0; d < 3; ++d) {
+      c.diff[d][q] = (Real)((double)k.c_diff * hvol * (double)k.ih2[d] * W);
+      c.adv[d][q] = (Real)((double)k.c_vel * hvol * (double)k.ih[d] * W * vf[d]);
+    }
+  }
+  for (int d = 0; d < 3; ++d)
+    for (int b = 0; b < n; ++b)
+      for (int a = 0; a < n; ++a) c.line[d][b * n + a] = (Real)((double)k.c_diff * hvol * (double)k.ih2[d] * wq[a] * wq[b]);
+  for (int r = 0; r < n; ++r)
+    for (int s = 0; s < n; ++s) {
+      double acc = 0.0;
+      for (int t = 0; t < n; ++t) acc += Dc[t * n + r] * wq[t] * Dc[t * n + s];
+      c.K[r * n + s] = (Real)acc;
+    }
+  return c;
+}
+
+template <int P, typename Real, int VK, int OCC>
 void run_lane_apply(Op &op, KP<Real> k)
 {
+  const LaneCoef<Real> coef = lane_coef<P, Real, VK>(k);
   Mesh &m = *op.mesh;
   if (m.N >= (1L << 32)) throw Error{MPDG_ERR_UNSUPPORTED, "the lane apply indexes DoFs with 32 bits"};
   constexpr int prec = sizeof(Real) == 4 ? MPDG_FP32 : MPDG_FP64;
@@ -1967,7 +2008,7 @@ void run_lane_apply(Op &op, KP<Real> k)
       attr[0].val.programmaticStreamSerializationAllowed = 1;
       cfg.attrs = attr;
       cfg.numAttrs = pdl ? 1 : 0;
-      MPDG_CUDA(cudaLaunchKernelEx(&cfg, lane_apply_kernel<P, Real, VK, WIDE>, k, lc));
+      MPDG_CUDA(cudaLaunchKernelEx(&cfg, lane_apply_kernel<P, Real, VK, OCC>, k, lc, coef));
       MPDG_LAUNCHED();
       ++launched;
     }
@@ -1982,14 +2023,14 @@ void run_lane_apply(Op &op, KP<Real> k)
   for (int sl = 0; sl < ns; ++sl) colour_launches(bounds[sl], bounds[sl + 1]);
 }
 
-template <int P, typename Real, int WIDE>
+template <int P, typename Real, int OCC>
 void lane_apply_velocity(Op &op, const KP<Real> &k)
 {
   switch (k.vel_kind) {
-    case MPDG_VEL_NONE: run_lane_apply<P, Real, LANE_VEL_NONE, WIDE>(op, k); break;
-    case MPDG_VEL_CONST: run_lane_apply<P, Real, LANE_VEL_CONST, WIDE>(op, k); break;
-    case MPDG_VEL_VORTEX: run_lane_apply<P, Real, LANE_VEL_VORTEX, WIDE>(op, k); break;
-    case MPDG_VEL_ROTATION: run_lane_apply<P, Real, LANE_VEL_ROTATION, WIDE>(op, k); break;
+    case MPDG_VEL_NONE: run_lane_apply<P, Real, LANE_VEL_NONE, OCC>(op, k); break;
+    case MPDG_VEL_CONST: run_lane_apply<P, Real, LANE_VEL_CONST, OCC>(op, k); break;
+    case MPDG_VEL_VORTEX: run_lane_apply<P, Real, LANE_VEL_VORTEX, OCC>(op, k); break;
+    case MPDG_VEL_ROTATION: run_lane_apply<P, Real, LANE_VEL_ROTATION, OCC>(op, k); break;
     default: throw Error{MPDG_ERR_UNSUPPORTED, "velocity kind not evaluated by the lane apply"};
   }
 }
@@ -2008,7 +2049,8 @@ void warp_apply_degree(Op &op, const KP<Real> &k)
         kv.src = k.nvec > 1 ? k.msrc[v] : k.src;
         kv.dst = k.nvec > 1 ? k.mdst[v] : k.dst;
         kv.nvec = 1;
-        // Q1 fits either bound without spilling: one variant
+        // Q1 fits either bound without spilling: one variant; lane 2 is the
+        // variant with more resident CTAs per SM
         if (op.mesh->degree == 1) lane_apply_velocity<1, Real, 0>(op, kv);
         else if (lane == 2) lane_apply_velocity<2, Real, 1>(op, kv);
         else lane_apply_velocity<2, Real, 0>(op, kv);
