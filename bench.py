@@ -59,8 +59,13 @@ WL = {"name": "heat", "nc": [64, 64, 64], "degree": 4}
 # over two colour launches, 1,147.6 MB per apply of 110,592 cells) scaled by
 # the cells of a 64^3 apply (262,144 / 110,592), as traffic grows with the
 # cells processed; the level-set workload's capture is at full size
-# (profiles/warp_apply_q2_uniform_128c.md: 381.4 MB over two launches).
-MEASURED_TRAFFIC_BYTES = {("heat", 64): 2.720e9, ("advdiff", 128): 1.526e9}
+# (profiles/warp_apply_q2_uniform_128c.md: 381.4 MB over two launches).  The
+# lane apply (one thread per Q2 cell, the level-set workload's default) was
+# captured at full size over all 8 colour launches of an apply with the cache
+# left warm between launches (profiles/lane_apply_q2_uniform_128c.md: 481.8 MB
+# read, 298.4 MB written).
+MEASURED_TRAFFIC_BYTES = {("heat", 64, "warp"): 2.720e9, ("advdiff", 128, "warp"): 1.526e9,
+                         ("advdiff", 128, "lane"): 0.780e9}
 
 
 def set_workload(name, cells=0):
@@ -107,6 +112,14 @@ def algorithmic_flops(n_cells, degree):
     n = degree + 1
     c_q = {"advdiff": 60, "c1": 20}.get(WL["name"], 45)
     return n_cells * (24 * n ** 4 + c_q * n ** 3)
+
+
+def apply_kernel_name(op, p, geom):
+    """The FP64 apply kernel the operator's schedule runs."""
+    sc = op.schedule("fp64")
+    if sc["lane_cells"] and geom == "UNIFORM" and p <= 2:
+        return f"lane_apply_kernel<{p},double> x {4 if WL['nc'][0] <= 32 else 8} colour launches"
+    return f"warp_apply_kernel<{p},double,{geom}> x 8 colour launches"
 
 
 def fma_peaks(M):
@@ -434,13 +447,14 @@ def run_operator_workload(args, rank, world, headline):
     geom = "UNIFORM" if WL["name"] in ("advdiff", "c1") else "GENERAL"
     b64, b32 = algorithmic_bytes(N, E, p, 8), algorithmic_bytes(N, E, p, 4)
     st64, st32 = streamed_bytes(N, E, p, 8), streamed_bytes(N, E, p, 4)
-    traffic = MEASURED_TRAFFIC_BYTES.get((WL["name"], nc[0]))
+    kernel_kind = "lane" if apply_kernel_name(op, p, geom).startswith("lane") else "warp"
+    traffic = MEASURED_TRAFFIC_BYTES.get((WL["name"], nc[0], kernel_kind))
     roof = {"bound": "hbm", "achieved": b64 / apply_s / 1e9, "peak": peak, "unit": "GB/s",
             "frac": b64 / apply_s / 1e9 / peak, "traffic": traffic,
             "traffic_note": None if traffic is None else
             ("ncu dram read+write per apply (8 launches), 48^3 capture scaled by cells" if WL["name"] == "heat"
-             else "ncu dram read+write per apply (8 launches), full-size capture"),
-            "algorithmic_bytes": b64, "kernel": f"warp_apply_kernel<{p},double,{geom}> x 8 colour launches",
+             else f"ncu dram read+write per apply (8 {kernel_kind} apply launches), full-size capture"),
+            "algorithmic_bytes": b64, "kernel": apply_kernel_name(op, p, geom),
             "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
             "streamed": {"bytes": st64, "achieved": st64 / apply_s / 1e9, "frac": st64 / apply_s / 1e9 / peak},
             "fp32": {"achieved": b32 / apply32_s / 1e9, "frac": b32 / apply32_s / 1e9 / peak,
