@@ -107,8 +107,10 @@ typedef struct {
    * tau_K u (u/dt + theta u.grad u - theta D lap u) (right-hand side:
    * tau_K u (phi/dt - (1-theta) u.grad phi + (1-theta) D lap phi)), with
    * tau_K = supg_coefficient h_K, or h_K / max_q |u| when supg_coefficient < 0,
-   * h_K = cell diameter / sqrt(3).  With diffusion the cells must be axis-aligned
-   * boxes.  The diagonal is built by probing (n^3 applies). */
+   * h_K = cell diameter / sqrt(3).  lap u is the physical Laplacian on every
+   * cell shape, the trilinear map's curvature included (get_laplacian,
+   * advection_diffusion_operator.cpp:483-486).  The diagonal is built by
+   * probing (n^3 applies). */
   int supg;
   double supg_coefficient;
   /* heat: radiative faces (heat_diffuse_operator.cpp:766-772, 1122-1124): tangent

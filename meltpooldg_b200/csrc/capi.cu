@@ -183,18 +183,6 @@ void free_mesh_arrays(Mesh &m)
     if (p) cudaFree(p);
 }
 
-// every vertex is (X[a], Y[b], Z[c]): all cells are axis-aligned boxes
-bool axis_aligned_lattice(const Mesh &m)
-{
-  const long V0 = m.nc[0] + 1, V1 = m.nc[1] + 1, V2 = m.nc[2] + 1;
-  const auto at = [&](long a, long b, long c, int d) { return m.vertices[(size_t)(((c * V1 + b) * V0 + a) * 3 + d)]; };
-  for (long c = 0; c < V2; ++c)
-    for (long b = 0; b < V1; ++b)
-      for (long a = 0; a < V0; ++a)
-        if (at(a, b, c, 0) != at(a, 0, 0, 0) || at(a, b, c, 1) != at(0, b, 0, 1) || at(a, b, c, 2) != at(0, 0, c, 2))
-          return false;
-  return true;
-}
 }  // namespace
 
 mpdg_status mpdg_mesh_destroy(mpdg_mesh *mesh)
@@ -257,9 +245,6 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
         (desc->k_alpha != 0.0 || desc->full_tangent || desc->material != MPDG_MAT_LINEAR))
       throw Error{MPDG_ERR_UNSUPPORTED,
                   "mapped meshes with constraints take constant coefficients (no k(T), phase law or full tangent)"};
-    if (desc->supg && desc->diffusivity != 0.0 && !mm.uniform && !axis_aligned_lattice(mm))
-      throw Error{MPDG_ERR_UNSUPPORTED,
-                  "SUPG with diffusion needs axis-aligned cells (its Laplacian drops the Jacobian derivatives)"};
     auto *h = new mpdg_op();
     Op &o = h->o;
     o.mesh = &mm;
@@ -311,7 +296,7 @@ void free_op_arrays(Op &o)
   free_workspace(o);
   for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32,
                   (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32, (void *)o.d_trig64, o.d_stage,
-                  (void *)o.d_tau64, (void *)o.d_tau32, (void *)o.Told_own, (void *)o.H_own, (void *)o.Told32,
+                  (void *)o.d_tau64, (void *)o.d_tau32, (void *)o.d_lam64, (void *)o.d_lam32, (void *)o.Told_own, (void *)o.H_own, (void *)o.Told32,
                   (void *)o.H32, (void *)o.lsq_buf, (void *)o.host_stage,
                   (void *)o.d_io, o.io_tmp, (void *)o.U_own})
     if (p) cudaFree(p);

@@ -188,6 +188,8 @@ struct Op {
   float *d_velb32 = nullptr;
   float *d_trig32 = nullptr;           // uniform vortex velocity: sin/cos tables
   double *d_tau64 = nullptr;           // SUPG: tau_K per colour-major cell
+  double *d_lam64 = nullptr;           // SUPG with diffusion on general cells: Laplacian curvature term
+  float *d_lam32 = nullptr;
   float *d_tau32 = nullptr;
   double *d_trig64 = nullptr;
   Workspace *ws = nullptr;

@@ -256,7 +256,8 @@ struct KP {
   const Real *msrc[kMaxMultiVec];
   Real *mdst[kMaxMultiVec];
   const Real *Hs;         // level-set heaviside (two-phase laws)
-  int supg_lap;           // SUPG with diffusion: the Laplacian term (axis-aligned cells)
+  int supg_lap;           // SUPG with diffusion: the Laplacian term
+  const Real *lam;        // SUPG with diffusion, general cells: [cell][3][n^3] curvature term (lam_kernel)
   const uint8_t *dmask;
   const uint8_t *cell_flags;
   const uint4 *cell_mask;
@@ -638,7 +639,9 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
 
   // SUPG with diffusion: second reference derivatives d2/dxi_d^2 at the Gauss
   // points, by collocation differentiation of the gradient along its own axis
-  Real gxx[n], gyy[n], gzz[n];
+  // and, on general cells, the mixed ones (d/dy of the x-gradient, d/dz of the
+  // x- and y-gradients)
+  Real gxx[n], gyy[n], gzz[n], gxy[n], gxz[n], gyz[n];
   if (MODE == MODE_SUPG && p.supg_lap) {
     put<n>(t0, i, j, gx);
     put<n>(t1, i, j, gy);
@@ -646,6 +649,11 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
     cx<n, Real, false>(sDc, t0, i, j, gxx);
     cy<n, Real, false>(sDc, t1, i, j, gyy);
     cz<n, Real, false>(sDc, gz, gzz);
+    if (GEOM == GEOM_GENERAL) {
+      cy<n, Real, false>(sDc, t0, i, j, gxy);
+      cz<n, Real, false>(sDc, gx, gxz);
+      cz<n, Real, false>(sDc, gy, gyz);
+    }
     __syncthreads();
   }
 
@@ -721,14 +729,23 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
       fz[k] = kq * f2;
       if (MODE == MODE_SUPG) {
         // tau_K u r tested with grad N: reference flux tau_K r JxW J^-1 u = tau_K r b,
-        // with u.grad u = adv / JxW and, on axis-aligned cells,
-        // lap u = sum_d (J^-1)_dd^2 d2u/dxi_d^2 = sum_d G_dd / JxW d2u/dxi_d^2
+        // with u.grad u = adv / JxW and lap u = G : H_xi / JxW - lam . grad_xi u
+        // (G = JxW J^-1 J^-T, lam from lam_kernel; lam = 0 and G diagonal on
+        // axis-aligned cells)
         const Real tau = active ? p.tau[cell] : Real(0);
         Real r = p.c_mass * uq[k] + p.c_vel * adv / JxW;
         if (p.supg_lap) {
-          const Real lap = (GEOM == GEOM_GENERAL)
-                               ? (G00 * gxx[k] + G11 * gyy[k] + G22 * gzz[k]) / JxW
-                               : p.ih2[0] * gxx[k] + p.ih2[1] * gyy[k] + p.ih2[2] * gzz[k];
+          Real lap;
+          if (GEOM == GEOM_GENERAL) {
+            lap = (G00 * gxx[k] + G11 * gyy[k] + G22 * gzz[k] +
+                   Real(2) * (G01 * gxy[k] + G02 * gxz[k] + G12 * gyz[k])) / JxW;
+            if (active) {
+              const Real *lm = p.lam + cell * 3 * n3 + k * n2 + j * n + i;
+              lap -= lm[0] * gx[k] + lm[n3] * gy[k] + lm[2 * n3] * gz[k];
+            }
+          } else {
+            lap = p.ih2[0] * gxx[k] + p.ih2[1] * gyy[k] + p.ih2[2] * gzz[k];
+          }
           r -= p.c_diff * lap;
         }
         const Real tr = tau * r;
@@ -1081,6 +1098,71 @@ __global__ void metric_kernel(const double *vert, int nc0, int nc1, long n_cells
     float *m32 = metric32 + cell * metric_stride(n) + q;
     m32[0] = (float)JxW;
     for (int e = 0; e < 6; ++e) m32[(e + 1) * n3] = (float)G[e];
+  }
+}
+
+// per (cell, qp): the curvature term lam of the physical Laplacian on a
+// trilinear cell, lap u = sum_ab Gt_ab d2u/dxi_a dxi_b - lam . grad_xi u with
+// Gt = J^-1 J^-T, K_j[a][b] = d2 x_j / dxi_a dxi_b (mixed only) and
+// lam_a = sum_j (J^-1)_aj sum_bc Gt_bc K_j[b][c]: the chain rule through
+// d(J^-1)/dxi_c = -J^-1 (dJ/dxi_c) J^-1.  It is the Laplacian
+// FEEvaluation::get_laplacian returns on non-affine cells (SUPG with
+// diffusion, advection_diffusion_operator.cpp:483-486).  Layout [cell][3][n^3].
+__global__ void lam_kernel(const double *vert, int nc0, int nc1, long n_cells, int P, const Colour *colours,
+                           const double *cellvert, const double *xq_all, double *lam, float *lam32)
+{
+  const int n = P + 1, n3 = n * n * n;
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= n_cells * n3) return;
+  const long cell = gid / n3;
+  const int q = (int)(gid % n3);
+  double V[8][3];
+  cell_corners(vert, nc0, nc1, colours, cellvert, cell, V);
+  const double xi[3] = {xq_all[q % n], xq_all[(q / n) % n], xq_all[q / (n * n)]};
+  double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, K[3][3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      for (int c = 0; c < 3; ++c) K[a][b][c] = 0.0;
+  for (int v = 0; v < 8; ++v) {
+    double f[3], df[3];
+    for (int d = 0; d < 3; ++d) {
+      const int bit = (v >> d) & 1;
+      f[d] = bit ? xi[d] : 1.0 - xi[d];
+      df[d] = bit ? 1.0 : -1.0;
+    }
+    const double dB[3] = {df[0] * f[1] * f[2], f[0] * df[1] * f[2], f[0] * f[1] * df[2]};
+    // mixed second derivatives: (xy) f_z, (xz) f_y, (yz) f_x
+    const double d2[3] = {df[0] * df[1] * f[2], df[0] * f[1] * df[2], f[0] * df[1] * df[2]};
+    for (int a = 0; a < 3; ++a) {
+      for (int b = 0; b < 3; ++b) J[a][b] += V[v][a] * dB[b];
+      K[a][0][1] += V[v][a] * d2[0];
+      K[a][0][2] += V[v][a] * d2[1];
+      K[a][1][2] += V[v][a] * d2[2];
+    }
+  }
+  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                     J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  const double id = 1.0 / det;
+  double Ji[3][3];
+  Ji[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) * id;
+  Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+  Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+  Ji[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) * id;
+  Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+  Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+  Ji[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) * id;
+  Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+  Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  double Gt[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) Gt[a][b] = Ji[a][0] * Ji[b][0] + Ji[a][1] * Ji[b][1] + Ji[a][2] * Ji[b][2];
+  double kap[3];
+  for (int j = 0; j < 3; ++j) kap[j] = 2.0 * (Gt[0][1] * K[j][0][1] + Gt[0][2] * K[j][0][2] + Gt[1][2] * K[j][1][2]);
+  for (int a = 0; a < 3; ++a) {
+    const double l = Ji[a][0] * kap[0] + Ji[a][1] * kap[1] + Ji[a][2] * kap[2];
+    lam[(cell * 3 + a) * n3 + q] = l;
+    if (lam32) lam32[(cell * 3 + a) * n3 + q] = (float)l;
   }
 }
 
@@ -1500,6 +1582,16 @@ void build_op_device_data(Op &op)
                                                     op.d_tau32, nullptr);
       MPDG_LAUNCHED();
     }
+    if (op.d.diffusivity != 0.0 && !m.uniform) {
+      // the Laplacian of the SUPG residual on general cells needs the
+      // curvature of the map at every quadrature point
+      const size_t cnt = (size_t)m.n_cells * 3 * n3;
+      op.d_lam64 = dev_alloc<double>(cnt, op.device_bytes);
+      if (want32) op.d_lam32 = dev_alloc<float>(cnt, op.device_bytes);
+      lam_kernel<<<grid_for(m.n_cells * n3, 256), 256>>>(m.d_vert, m.nc[0], m.nc[1], m.n_cells, p, d_col,
+                                                         m.d_cellvert, d_xq, op.d_lam64, op.d_lam32);
+      MPDG_LAUNCHED();
+    }
     MPDG_CUDA(cudaDeviceSynchronize());
     cudaFree(d_col);
     cudaFree(d_xq);
@@ -1676,12 +1768,14 @@ KP<Real> base_params(Op &op)
     k.trig = op.d_trig64;
     k.T = op.T64;
     k.tau = op.d_tau64;
+    k.lam = op.d_lam64;
   } else {
     k.metric = m.d_metric32;
     k.velb = op.d_velb32;
     k.trig = op.d_trig32;
     k.T = op.T32;
     k.tau = op.d_tau32;
+    k.lam = op.d_lam32;
   }
   k.supg_lap = op.d.kind == MPDG_OP_ADVDIFF && op.d.supg && op.d.diffusivity != 0.0;
   k.cmap = m.d_cmap;

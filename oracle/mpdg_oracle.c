@@ -225,6 +225,56 @@ static double inverse3(double J[3][3], double Ji[3][3])
   return det;
 }
 
+/* Curvature term of the physical Laplacian at reference point xi of the
+ * (bi/tri)linear map of corners vc.  With K_j[a][b] = d2 x_j / dxi_a dxi_b
+ * (only mixed derivatives are nonzero for this map) and Gt = J^-1 J^-T,
+ *   lap u = sum_ab Gt_ab d2u/dxi_a dxi_b - sum_a lam_a du/dxi_a,
+ *   lam_a = sum_j (J^-1)_aj sum_bc Gt_bc K_j[b][c],
+ * which follows from d(J^-1)/dxi_c = -J^-1 (dJ/dxi_c) J^-1.  This is the
+ * Laplacian FEEvaluation::get_laplacian returns on non-affine cells
+ * (advection_diffusion_operator.cpp:483-486, with jacobian gradients). */
+static void map_second(const geo_t *g, double vc[8][3], const double xi[3], double K[3][3][3])
+{
+  const int dim = g->dim, nv = 1 << dim;
+  memset(K, 0, sizeof(double) * 27);
+  for (int c = 0; c < nv; ++c)
+    for (int a = 0; a < dim; ++a)
+      for (int b = a + 1; b < dim; ++b) {
+        double d2 = 1.0;
+        for (int d = 0; d < dim; ++d) {
+          const int bit = (c >> d) & 1;
+          d2 *= (d == a || d == b) ? (bit ? 1.0 : -1.0) : (bit ? xi[d] : 1.0 - xi[d]);
+        }
+        for (int j = 0; j < dim; ++j) {
+          K[j][a][b] += vc[c][j] * d2;
+          K[j][b][a] += vc[c][j] * d2;
+        }
+      }
+}
+
+static void map_lambda(const geo_t *g, double vc[8][3], const double xi[3], double Ji[3][3], double lam[3])
+{
+  const int dim = g->dim;
+  double K[3][3][3];
+  map_second(g, vc, xi, K);
+  double Gt[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double t = 0.0;
+      for (int i = 0; i < dim; ++i) t += Ji[a][i] * Ji[b][i];
+      Gt[a][b] = t;
+    }
+  double kap[3] = {0.0, 0.0, 0.0};
+  for (int j = 0; j < dim; ++j)
+    for (int a = 0; a < dim; ++a)
+      for (int b = 0; b < dim; ++b) kap[j] += Gt[a][b] * K[j][a][b];
+  for (int a = 0; a < 3; ++a) {
+    double t = 0.0;
+    for (int j = 0; j < dim; ++j) t += Ji[a][j] * kap[j];
+    lam[a] = (a < dim) ? t : 0.0;
+  }
+}
+
 static void cell_dofs(const geo_t *g, int ix, int iy, int iz, long *idx)
 {
   const int n = g->n, nz = (g->dim == 3) ? n : 1;
@@ -354,6 +404,7 @@ static void integrate(const geo_t *g, const double *val, double grad[3][MAXN3], 
 /* per-cell quadrature-point data shared by the tangent, the residual and the diagonal */
 typedef struct {
   double JxW, Ji[3][3], x[3], vel[3];
+  double lam[3]; /* curvature term of the physical Laplacian (map_lambda) */
   double T, gradT[3]; /* physical */
   double Told, H;     /* T_old and the heaviside at the point */
 } qdata_t;
@@ -464,6 +515,7 @@ static void cell_qdata(const orc_mesh *m, const orc_op *op, const geo_t *g, int 
         map_point(g, vc, xi, qd[q].x, J);
         double det = inverse3(J, qd[q].Ji);
         qd[q].JxW = det * w;
+        map_lambda(g, vc, xi, qd[q].Ji, qd[q].lam);
         if (op->vel_kind == ORC_VEL_NODAL) {
           for (int d = 0; d < 3; ++d) qd[q].vel[d] = (d < dim) ? Vv[d][q] : 0.0;
         } else {
@@ -537,24 +589,26 @@ static double cell_tau(const orc_mesh *m, const orc_op *op, const geo_t *g, int 
   return (umax >= 1e-6) ? h / umax : 0.0;
 }
 
-/* physical Laplacian at the quadrature points from the reference gradients
- * (axis-aligned cells: J^-1 diagonal) */
+/* physical Laplacian at the quadrature points from the reference gradients:
+ * sum_ab Gt_ab d2u/dxi_a dxi_b - lam . grad_ref u (map_lambda), the second
+ * reference derivatives by collocation differentiation of the gradients */
 static void laplacian_qp(const geo_t *g, double ug[3][MAXN3], const qdata_t *qd, double *lap)
 {
   const int dim = g->dim, nqt = g->n * g->n * ((dim == 3) ? g->n : 1);
   double t[MAXN3];
-  for (int q = 0; q < nqt; ++q) lap[q] = 0.0;
-  for (int d = 0; d < dim; ++d) {
-    contract(g, g->Dc, 0, d, ug[d], t);
-    for (int q = 0; q < nqt; ++q) {
-      for (int e = 0; e < dim; ++e)
-        if (e != d && (fabs(qd[q].Ji[d][e]) > 1e-12 * fabs(qd[q].Ji[d][d]))) {
-          fprintf(stderr, "orc: SUPG with diffusion needs axis-aligned cells\n");
-          abort();
-        }
-      lap[q] += qd[q].Ji[d][d] * qd[q].Ji[d][d] * t[q];
-    }
+  for (int q = 0; q < nqt; ++q) {
+    lap[q] = 0.0;
+    for (int a = 0; a < dim; ++a) lap[q] -= qd[q].lam[a] * ug[a][q];
   }
+  for (int a = 0; a < dim; ++a)
+    for (int b = a; b < dim; ++b) {
+      contract(g, g->Dc, 0, b, ug[a], t); /* d/dxi_b of du/dxi_a */
+      for (int q = 0; q < nqt; ++q) {
+        double gab = 0.0;
+        for (int i = 0; i < dim; ++i) gab += qd[q].Ji[a][i] * qd[q].Ji[b][i];
+        lap[q] += ((a == b) ? 1.0 : 2.0) * gab * t[q];
+      }
+    }
 }
 
 /* one cell of the sum-factorised tangent; adds into dst (caller guarantees no race) */
@@ -789,6 +843,8 @@ static void element_matrix_vc(const orc_op *op, const geo_t *g, double vc[8][3],
         map_point(g, vc, xi, qd.x, J);
         double det = inverse3(J, qd.Ji);
         qd.JxW = det * w;
+        double Kq[3][3][3];
+        map_second(g, vc, xi, Kq);
         /* shape values and physical gradients by direct products */
         for (int t = 0; t < nqt; ++t) {
           int c[3] = {t % n, (t / n) % n, t / (n * n)};
@@ -831,15 +887,33 @@ static void element_matrix_vc(const orc_op *op, const geo_t *g, double vc[8][3],
           double v, fl[3];
           tangent_qp(op, dim, &qd, phi[j], gphi[j], &v, fl);
           if (op->supg && op->kind == ORC_ADVDIFF) {
-            /* Laplacian of basis j (axis-aligned cells) */
+            /* Laplacian of basis j: the physical Hessian
+             * J^-T (Hhat - sum_i (grad phi)_i K_i) J^-1 (chain rule of the map),
+             * traced; Hhat from products of the 1D value, derivative and
+             * second-derivative tables */
             int c[3] = {j % n, (j / n) % n, j / (n * n)};
+            double Hh[3][3];
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b) {
+                if (a >= dim || b >= dim) {
+                  Hh[a][b] = 0.0;
+                  continue;
+                }
+                double pr = 1.0;
+                for (int e = 0; e < dim; ++e) {
+                  const int k = (e == a) + (e == b);
+                  const double *tab1 = (k == 0) ? g->S : (k == 1) ? g->D : g->D2;
+                  pr *= tab1[qq[e] * n + c[e]];
+                }
+                Hh[a][b] = pr;
+              }
+            for (int i = 0; i < dim; ++i)
+              for (int a = 0; a < dim; ++a)
+                for (int b = 0; b < dim; ++b) Hh[a][b] -= gphi[j][i] * Kq[i][a][b];
             double lapj = 0.0;
-            for (int d = 0; d < dim; ++d) {
-              double pr = qd.Ji[d][d] * qd.Ji[d][d] * g->D2[qq[d] * n + c[d]];
-              for (int e = 0; e < dim; ++e)
-                if (e != d) pr *= g->S[qq[e] * n + c[e]];
-              lapj += pr;
-            }
+            for (int i = 0; i < dim; ++i)
+              for (int a = 0; a < dim; ++a)
+                for (int b = 0; b < dim; ++b) lapj += qd.Ji[a][i] * Hh[a][b] * qd.Ji[b][i];
             const double r = v - op->theta * op->diffusivity * lapj;
             for (int a = 0; a < dim; ++a) fl[a] += tau * qd.vel[a] * r;
           }
