@@ -69,6 +69,9 @@ enum { MPDG_FIELD_TEMPERATURE = 0, MPDG_FIELD_TEMPERATURE_OLD = 1, MPDG_FIELD_HE
  * dk/dT grad T du (heat_diffuse_operator.cpp:1040-1062) and read
  * MPDG_FIELD_TEMPERATURE_OLD.  Latent heat (apparent capacity) is not offered. */
 enum { MPDG_MAT_LINEAR = 0, MPDG_MAT_GAS_LIQUID = 1, MPDG_MAT_LIQUID_SOLID = 2, MPDG_MAT_GAS_LIQUID_SOLID = 3 };
+/* apparent heat capacity profiles of the latent heat of fusion
+ * (ApparentCapacityType, include/meltpooldg/core/material_data.hpp:43-113) */
+enum { MPDG_AC_POLY4_BELL = 0, MPDG_AC_CONSTANT = 1, MPDG_AC_QLQ = 2 };
 
 typedef struct mpdg_mesh mpdg_mesh;
 typedef struct mpdg_op mpdg_op;
@@ -123,6 +126,13 @@ typedef struct {
   double mat_rho[3], mat_cp[3], mat_k[3];
   double solidus, liquidus;
   int two_phase_sharp, solid_liquid_sharp, volume_specific;
+  /* heat, laws with a solid phase: latent heat of fusion (> 0 adds the
+   * apparent capacity of profile MPDG_AC_* to c_p in the mushy zone, and its
+   * T derivative to the Newton terms: Material, material.templates.hpp:566-616;
+   * ApparentCapacity, source/heat/apparent_capacity.cpp).  Not defined with
+   * volume_specific, as in the reference. */
+  double latent_heat;
+  int apparent_capacity;
 } mpdg_op_desc;
 
 typedef struct {

@@ -24,6 +24,7 @@ SOLVER_CG, SOLVER_GMRES = 0, 1
 PREC_IDENTITY, PREC_JACOBI, PREC_CHEBYSHEV = 0, 1, 2
 FIELD_TEMPERATURE, FIELD_TEMPERATURE_OLD, FIELD_HEAVISIDE, FIELD_VELOCITY = 0, 1, 2, 3
 MAT_LINEAR, MAT_GAS_LIQUID, MAT_LIQUID_SOLID, MAT_GAS_LIQUID_SOLID = 0, 1, 2, 3
+AC_POLY4_BELL, AC_CONSTANT, AC_QLQ = 0, 1, 2
 
 _STATUS_NAMES = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_ALLOC", -4: "ERR_NOT_CONVERGED",
                  -5: "ERR_BREAKDOWN", -6: "ERR_NAN", -7: "ERR_UNSUPPORTED", -8: "ERR_BUDGET",
@@ -64,7 +65,8 @@ class OpDesc(C.Structure):
                 ("rad_t_inf", C.c_double), ("rad_faces", C.c_int), ("material", C.c_int),
                 ("mat_rho", C.c_double * 3), ("mat_cp", C.c_double * 3), ("mat_k", C.c_double * 3),
                 ("solidus", C.c_double), ("liquidus", C.c_double), ("two_phase_sharp", C.c_int),
-                ("solid_liquid_sharp", C.c_int), ("volume_specific", C.c_int)]
+                ("solid_liquid_sharp", C.c_int), ("volume_specific", C.c_int),
+                ("latent_heat", C.c_double), ("apparent_capacity", C.c_int)]
 
 
 class SolverDesc(C.Structure):

@@ -229,6 +229,17 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
       throw Error{MPDG_ERR_ARG, "material laws apply to the heat operator"};
     if (law_has_solid(desc->material) && !desc->solid_liquid_sharp && !(desc->liquidus > desc->solidus))
       throw Error{MPDG_ERR_ARG, "the mushy zone needs liquidus > solidus"};
+    if (!(desc->latent_heat >= 0.0)) throw Error{MPDG_ERR_ARG, "latent heat of fusion must be >= 0"};
+    if (desc->apparent_capacity < MPDG_AC_POLY4_BELL || desc->apparent_capacity > MPDG_AC_QLQ)
+      throw Error{MPDG_ERR_ARG, "unknown apparent capacity profile"};
+    if (desc->latent_heat > 0.0 && law_has_solid(desc->material)) {
+      // ApparentCapacity asserts liquidus > solidus (apparent_capacity.cpp:160-165) and
+      // Material refuses it with the volume-specific capacity (material.templates.hpp:322-328)
+      if (!(desc->liquidus > desc->solidus))
+        throw Error{MPDG_ERR_ARG, "the apparent capacity needs liquidus > solidus"};
+      if (desc->volume_specific)
+        throw Error{MPDG_ERR_UNSUPPORTED, "the apparent capacity is not defined for the volume-specific heat capacity"};
+    }
     if (mm.fine && (desc->material != MPDG_MAT_LINEAR || (desc->rad_faces && desc->rad_emissivity != 0.0)))
       throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take constant coefficients: no material law or radiation"};
     if (desc->supg && desc->kind != MPDG_OP_ADVDIFF)

@@ -239,6 +239,8 @@ struct KP {
   // heat material law (MPDG_MAT_*); LINEAR uses c_mass, c_vel, c_diff, k_alpha
   int mat, two_phase_sharp, solid_sharp, vol_specific;
   Real mrho[3], mcp[3], mk[3], solidus, liquidus, inv_mushy, dt_inv;
+  Real latent;  // latent heat of fusion (0: no apparent capacity)
+  int ac_type;  // its apparent-capacity profile (MPDG_AC_*)
   const Real *Told;       // T_old (laws with a solid phase), or T - T_old when told_inc
   int told_inc;
   // mapped mesh: cell->DoF map [colour-major cell][n^3]; skip the cells that
@@ -496,6 +498,49 @@ __device__ __forceinline__ Real ls_deriv(Real fs, Real inv_mushy, Real vl, Real 
   return -inv_mushy * (vs - vl) * (Real(-6) * fs * fs + Real(6) * fs);
 }
 
+// apparent heat capacity of the latent heat of fusion L over the mushy zone
+// [Ts, Tl] as a function of the solid fraction fs, and its T derivative
+// (ApparentCapacity::evaluate / compute_temperature_derivative,
+// source/heat/apparent_capacity.cpp); 0 outside 0 < fs < 1.  constant: L/(Tl-Ts);
+// poly4_bell: L r b(xi), r = 2/(Tl-Ts), xi = 1 - 2 fs, b(x) = 15/16 (x^2-1)^2;
+// qlq: at T = Tl - fs (Tl-Ts) two ramps 0 -> 2L/(Tl-Ts) -> 0 over the halves of
+// the zone, each quadratic with zero end slope over (Tl-Ts)/6 and linear between
+template <typename Real>
+__device__ __forceinline__ void qlq_ramp(Real x, Real x1, Real x2, Real y1, Real y2, Real delta, Real &f, Real &df)
+{
+  const Real s = (y2 - y1) / (x2 - x1 - delta);
+  if (x < x1 + delta) {
+    f = y1 + Real(0.5) * s / delta * (x - x1) * (x - x1);
+    df = s * (x - x1) / delta;
+  } else if (x > x2 - delta) {
+    f = y2 - Real(0.5) * s / delta * (x2 - x) * (x2 - x);
+    df = s * (x2 - x) / delta;
+  } else {
+    f = y1 + Real(0.5) * s * delta + s * (x - x1 - delta);
+    df = s;
+  }
+}
+
+template <typename Real>
+__device__ __forceinline__ void apparent_capacity(const KP<Real> &p, Real fs, Real &c, Real &dc)
+{
+  c = dc = Real(0);
+  if (!(p.latent > Real(0)) || fs <= Real(0) || fs >= Real(1)) return;
+  const Real dT = p.liquidus - p.solidus;
+  if (p.ac_type == MPDG_AC_CONSTANT) {
+    c = p.latent / dT;
+  } else if (p.ac_type == MPDG_AC_POLY4_BELL) {
+    const Real r = Real(2) / dT, xi = Real(1) - Real(2) * fs, x2 = xi * xi;
+    c = p.latent * r * (Real(15.0 / 16.0) * x2 * x2 - Real(15.0 / 8.0) * x2 + Real(15.0 / 16.0));
+    dc = p.latent * r * r * (Real(15.0 / 4.0) * x2 * xi - Real(15.0 / 4.0) * xi);
+  } else {
+    const Real T = p.liquidus - fs * dT, Tp = Real(0.5) * (p.solidus + p.liquidus), Cp = Real(2) * p.latent / dT,
+               delta = dT / Real(6);
+    if (T <= Tp) qlq_ramp<Real>(T, p.solidus, Tp, Real(0), Cp, delta, c, dc);
+    else qlq_ramp<Real>(T, Tp, p.liquidus, Cp, Real(0), delta, c, dc);
+  }
+}
+
 template <typename Real>
 __device__ __forceinline__ void law_eval(const KP<Real> &p, Real T, Real H, Real &cm, Real &cv, Real &kq,
                                          Real &dcm, Real &dcv, Real &dk)
@@ -524,6 +569,14 @@ __device__ __forceinline__ void law_eval(const KP<Real> &p, Real T, Real H, Real
     const Real vg = (e == 0) ? p.mrho[0] : (e == 1) ? p.mcp[0] : (e == 2) ? p.mk[0] : p.mrho[0] * p.mcp[0];
     v[e] = sol ? ls_value(fs, vl, vs) : vl;
     dv[e] = sol ? ls_deriv(fs, p.inv_mushy, vl, vs) : Real(0);
+    if (sol && e == 1) {
+      // latent heat: the solid/liquid c_p gains the apparent capacity
+      // (material.templates.hpp:566-578, 604-616), before the gas weighting
+      Real c, dc;
+      apparent_capacity<Real>(p, fs, c, dc);
+      v[1] += c;
+      dv[1] += dc;
+    }
     if (gas) {
       v[e] = (Real(1) - w) * vg + w * v[e];
       dv[e] = w * dv[e];
@@ -1805,6 +1858,8 @@ KP<Real> base_params(Op &op)
   k.solidus = (Real)op.d.solidus;
   k.liquidus = (Real)op.d.liquidus;
   k.inv_mushy = law_T ? (Real)(1.0 / (op.d.liquidus - op.d.solidus)) : Real(0);
+  k.latent = law_T ? (Real)op.d.latent_heat : Real(0);
+  k.ac_type = op.d.apparent_capacity;
   k.dt_inv = (Real)(1.0 / op.d.dt);
   if (law_T) k.full_tangent = 1;  // heat_diffuse_operator.cpp:1040-1055 (do_solidification)
   if constexpr (sizeof(Real) == 8) {

@@ -325,12 +325,15 @@ class HeatDiffuseOperator(_MatrixFreeOperator):
     `material` selects a phase law (Material, material.templates.hpp:213-760):
     a dict with `kind` ("gas_liquid", "liquid_solid", "gas_liquid_solid"),
     `rho`, `cp`, `k` as (gas, liquid, solid) and `solidus`, `liquidus`,
-    `two_phase_sharp`, `solid_liquid_sharp`, `volume_specific`; the laws read
-    the heaviside (`set_heaviside`) and, with a solid phase, T_old
-    (`set_temperature_old`)."""
+    `two_phase_sharp`, `solid_liquid_sharp`, `volume_specific`, and for laws
+    with a solid phase the latent heat of fusion `latent_heat` with its
+    `apparent_capacity` profile ("qlq" by default, "poly4_bell", "constant");
+    the laws read the heaviside (`set_heaviside`) and, with a solid phase,
+    T_old (`set_temperature_old`)."""
 
     MATERIALS = {"gas_liquid": A.MAT_GAS_LIQUID, "liquid_solid": A.MAT_LIQUID_SOLID,
                  "gas_liquid_solid": A.MAT_GAS_LIQUID_SOLID}
+    APPARENT_CAPACITY = {"poly4_bell": A.AC_POLY4_BELL, "constant": A.AC_CONSTANT, "qlq": A.AC_QLQ}
 
     def __init__(self, mesh, dt, rho_cp=1.0, k0=1.0, k_alpha=0.0, full_tangent=False,
                  velocity=None, precisions=("fp64",), robin_alpha=0.0, robin_t_inf=0.0,
@@ -354,6 +357,9 @@ class HeatDiffuseOperator(_MatrixFreeOperator):
             d.two_phase_sharp = int(bool(material.get("two_phase_sharp", False)))
             d.solid_liquid_sharp = int(bool(material.get("solid_liquid_sharp", False)))
             d.volume_specific = int(bool(material.get("volume_specific", False)))
+            d.latent_heat = float(material.get("latent_heat", 0.0))
+            ac = material.get("apparent_capacity", "qlq")
+            d.apparent_capacity = self.APPARENT_CAPACITY[ac] if isinstance(ac, str) else int(ac)
         super().__init__(mesh, d, precisions)
 
     def set_temperature(self, T):

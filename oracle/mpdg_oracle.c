@@ -434,6 +434,58 @@ static int mat_has_T(const orc_op *op)
   return op->material == ORC_MAT_LIQUID_SOLID || op->material == ORC_MAT_GAS_LIQUID_SOLID;
 }
 
+/* Apparent heat capacity of the latent heat of fusion L over the mushy zone
+ * [Ts, Tl] (ApparentCapacity::evaluate / compute_temperature_derivative,
+ * source/heat/apparent_capacity.cpp), as a function of the solid fraction fs
+ * and its T derivative; 0 outside 0 < fs < 1.  Profiles:
+ *   constant:   L / (Tl - Ts);
+ *   poly4_bell: L r b(xi), r = 2 / (Tl - Ts), xi = 1 - 2 fs,
+ *               b(x) = 15/16 x^4 - 15/8 x^2 + 15/16 (unit integral on [-1, 1]);
+ *   qlq:        at T = Tl - fs (Tl - Ts), two ramps 0 -> C_peak -> 0 over
+ *               [Ts, T_peak] and [T_peak, Tl] (T_peak the midpoint, C_peak =
+ *               2 L / (Tl - Ts)), each quadratic with zero slope over delta =
+ *               (Tl - Ts) / 6 at both ends and linear in between. */
+static void qlq_ramp(double x, double x1, double x2, double y1, double y2, double delta, double *f, double *df)
+{
+  /* slope s of the linear part: the two quadratic ends y1 + s/(2 delta) (x-x1)^2
+   * and y2 - s/(2 delta) (x2-x)^2 meet it with continuous value and slope */
+  const double s = (y2 - y1) / (x2 - x1 - delta);
+  if (x < x1 + delta) {
+    *f = y1 + 0.5 * s / delta * (x - x1) * (x - x1);
+    *df = s * (x - x1) / delta;
+  } else if (x > x2 - delta) {
+    *f = y2 - 0.5 * s / delta * (x2 - x) * (x2 - x);
+    *df = s * (x2 - x) / delta;
+  } else {
+    *f = y1 + 0.5 * s * delta + s * (x - x1 - delta);
+    *df = s;
+  }
+}
+
+static void apparent_capacity_fs(const orc_op *op, double fs, double *c, double *dc)
+{
+  *c = *dc = 0.0;
+  if (!(op->latent_heat > 0.0) || fs <= 0.0 || fs >= 1.0) return;
+  const double L = op->latent_heat, Ts = op->solidus, Tl = op->liquidus, dT = Tl - Ts;
+  if (op->apparent_capacity == ORC_AC_CONSTANT) {
+    *c = L / dT;
+  } else if (op->apparent_capacity == ORC_AC_POLY4_BELL) {
+    const double r = 2.0 / dT, xi = 1.0 - 2.0 * fs, x2 = xi * xi;
+    *c = L * r * (15.0 / 16.0 * x2 * x2 - 15.0 / 8.0 * x2 + 15.0 / 16.0);
+    *dc = L * r * r * (15.0 / 4.0 * x2 * xi - 15.0 / 4.0 * xi);
+  } else {
+    const double T = Tl - fs * dT, Tp = 0.5 * (Ts + Tl), Cp = 2.0 * L / dT, delta = dT / 6.0;
+    if (T <= Tp) qlq_ramp(T, Ts, Tp, 0.0, Cp, delta, c, dc);
+    else qlq_ramp(T, Tp, Tl, Cp, 0.0, delta, c, dc);
+  }
+}
+
+void orc_apparent_capacity(const orc_op *op, double T, double *c, double *dc)
+{
+  const double fs = fmin(fmax((op->liquidus - T) / (op->liquidus - op->solidus), 0.0), 1.0);
+  apparent_capacity_fs(op, fs, c, dc);
+}
+
 static void mat_eval(const orc_op *op, double T, double H, double *rc, double *k, double *drc, double *dk)
 {
   if (op->material == ORC_MAT_LINEAR) {
@@ -458,6 +510,14 @@ static void mat_eval(const orc_op *op, double T, double H, double *rc, double *k
   for (int e = 0; e < 4; ++e) {
     v[e] = sol ? ls_value(fs, vl[e], vs[e]) : vl[e];
     dv[e] = sol ? ls_deriv(fs, inv_mushy, vl[e], vs[e]) : 0.0;
+    if (sol && e == 1) {
+      /* latent heat: c_p of the solid/liquid mix gains the apparent capacity
+       * (material.templates.hpp:566-578, 604-616), before the gas weighting */
+      double c, dc;
+      apparent_capacity_fs(op, fs, &c, &dc);
+      v[1] += c;
+      dv[1] += dc;
+    }
     if (gas) {
       v[e] = (1.0 - w) * vg[e] + w * v[e];
       dv[e] = w * dv[e];
@@ -466,6 +526,10 @@ static void mat_eval(const orc_op *op, double T, double H, double *rc, double *k
   *k = v[2];
   *dk = dv[2];
   if (op->volume_specific) {
+    if (op->latent_heat > 0.0 && sol) {
+      fprintf(stderr, "orc: the apparent capacity is not defined for the volume-specific heat capacity\n");
+      abort();
+    }
     *rc = v[3];
     *drc = dv[3];
   } else {

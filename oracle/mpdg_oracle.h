@@ -46,6 +46,8 @@ enum { ORC_PREC_IDENTITY = 0, ORC_PREC_JACOBI = 1, ORC_PREC_CHEBYSHEV = 2 };
  * k(T) = k0 (1 + k_alpha T); the phase laws interpolate gas / liquid / solid
  * properties by the level-set heaviside H and the solid fraction f_s(T) */
 enum { ORC_MAT_LINEAR = 0, ORC_MAT_GAS_LIQUID = 1, ORC_MAT_LIQUID_SOLID = 2, ORC_MAT_GAS_LIQUID_SOLID = 3 };
+/* apparent heat capacity profiles of the latent heat of fusion (ApparentCapacityType) */
+enum { ORC_AC_POLY4_BELL = 0, ORC_AC_CONSTANT = 1, ORC_AC_QLQ = 2 };
 #define ORC_STEFAN_BOLTZMANN 5.670374419e-8
 
 typedef struct {
@@ -92,6 +94,10 @@ typedef struct {
   int volume_specific;      /* interpolate rho*c_p itself instead of rho and c_p */
   const double *temperature_old; /* T_old: solidification terms of the tangent */
   const double *heaviside;       /* level set as heaviside, nodal (two-phase laws) */
+  /* latent heat of fusion (> 0: the apparent capacity of profile ORC_AC_* is
+   * added to c_p in the mushy zone of laws with a solid phase) */
+  double latent_heat;
+  int apparent_capacity;
 } orc_op;
 
 typedef struct {
@@ -174,6 +180,9 @@ typedef struct {
 } orc_mapped;
 
 void orcm_vmult(const orc_mapped *m, const orc_op *op, double *dst, const double *src);
+/* apparent capacity of op's latent heat at temperature T and its T derivative
+ * (solid fraction from op's solidus/liquidus, clamped to [0, 1]) */
+void orc_apparent_capacity(const orc_op *op, double T, double *c, double *dc);
 void orcm_diagonal(const orc_mapped *m, const orc_op *op, double *diag);
 
 #ifdef __cplusplus

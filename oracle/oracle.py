@@ -20,6 +20,7 @@ HEAT, ADVDIFF = 0, 1
 VEL_NONE, VEL_ROTATION, VEL_VORTEX, VEL_CONST, VEL_NODAL = 0, 1, 2, 3, 4
 PREC_IDENTITY, PREC_JACOBI, PREC_CHEBYSHEV = 0, 1, 2
 MAT_LINEAR, MAT_GAS_LIQUID, MAT_LIQUID_SOLID, MAT_GAS_LIQUID_SOLID = 0, 1, 2, 3
+AC_POLY4_BELL, AC_CONSTANT, AC_QLQ = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)
@@ -44,6 +45,7 @@ class _Op(C.Structure):
         ("mat_k", C.c_double * 3), ("solidus", C.c_double), ("liquidus", C.c_double),
         ("two_phase_sharp", C.c_int), ("solid_liquid_sharp", C.c_int), ("volume_specific", C.c_int),
         ("temperature_old", _dp), ("heaviside", _dp),
+        ("latent_heat", C.c_double), ("apparent_capacity", C.c_int),
     ]
 
 
@@ -111,6 +113,7 @@ def lib():
         P_mm = C.POINTER(_Mapped)
         L.orcm_vmult.argtypes = [P_mm, P_o, _dp, _dp]
         L.orcm_diagonal.argtypes = [P_mm, P_o, _dp]
+        L.orc_apparent_capacity.argtypes = [P_o, C.c_double, _dp, _dp]
         _lib = L
     return _lib
 
@@ -189,7 +192,9 @@ class Operator:
     `material` selects a phase law of the heat operator: a dict with `kind`
     (MAT_GAS_LIQUID, MAT_LIQUID_SOLID, MAT_GAS_LIQUID_SOLID), `rho`, `cp`, `k`
     (each (gas, liquid, solid)), `solidus`, `liquidus` and the flags
-    `two_phase_sharp`, `solid_liquid_sharp`, `volume_specific`; None keeps
+    `two_phase_sharp`, `solid_liquid_sharp`, `volume_specific`, and the latent
+    heat of fusion `latent_heat` with its `apparent_capacity` profile (AC_*,
+    default AC_QLQ as in MaterialData); None keeps
     rho_cp and k(T) = k0 (1 + k_alpha T).  `temperature_old` and `heaviside` are
     the nodal fields those laws read."""
 
@@ -217,7 +222,8 @@ class Operator:
                       float(mat.get("liquidus", 0.0)), int(bool(mat.get("two_phase_sharp", False))),
                       int(bool(mat.get("solid_liquid_sharp", False))),
                       int(bool(mat.get("volume_specific", False))),
-                      _ptr(self.temperature_old), _ptr(self.heaviside))
+                      _ptr(self.temperature_old), _ptr(self.heaviside),
+                      float(mat.get("latent_heat", 0.0)), int(mat.get("apparent_capacity", AC_QLQ)))
         self.params = dict(kind=kind, dt=dt, rho_cp=rho_cp, k0=k0, k_alpha=k_alpha,
                            full_tangent=full_tangent, robin_alpha=robin_alpha,
                            robin_t_inf=robin_t_inf, robin_faces=robin_faces, theta=theta,
@@ -290,6 +296,14 @@ def rhs_advdiff(mesh, op, phi_old, scatter_mask=None, dst=None):
     lib().orc_rhs_advdiff(C.byref(mesh._c), C.byref(op._c), _ptr(dst), _ptr(phi_old),
                           _ptr(sm, _u8p))
     return dst
+
+
+def apparent_capacity(op, T):
+    """(apparent capacity, its T derivative) of the operator's latent heat at
+    temperature T (ApparentCapacity, source/heat/apparent_capacity.cpp)."""
+    c, dc = C.c_double(), C.c_double()
+    lib().orc_apparent_capacity(C.byref(op._c), float(T), C.byref(c), C.byref(dc))
+    return c.value, dc.value
 
 
 def l2_norm(mesh, u):

@@ -3,7 +3,9 @@ the gas/liquid, liquid/solid and gas/liquid/solid laws with their Newton terms
 (T_old and heaviside fields), convective plus radiative faces and velocity
 (vmult and create_rhs FP64 to 1e-12, FP32 to 2e-5; the diagonal to 1e-12), and
 the reference's unidirectional heat-transfer goldens with radiation, velocity,
-two phases and solidification through the CUDA path."""
+two phases and solidification through the CUDA path.  The laws with a solid
+phase also run with the latent heat of fusion (apparent capacity: qlq,
+constant and poly4_bell profiles)."""
 import json
 import os
 
@@ -29,6 +31,13 @@ LAWS = {
     "liquid_solid": (dict(PHASES, kind="liquid_solid"), O.MAT_LIQUID_SOLID),
     "liquid_solid_sharp": (dict(PHASES, kind="liquid_solid", solid_liquid_sharp=True), O.MAT_LIQUID_SOLID),
     "gas_liquid_solid": (dict(PHASES, kind="gas_liquid_solid"), O.MAT_GAS_LIQUID_SOLID),
+    # latent heat of fusion through the apparent capacity, each profile
+    "liquid_solid_latent_qlq": (dict(PHASES, kind="liquid_solid", latent_heat=2.7e5, apparent_capacity=O.AC_QLQ),
+                                O.MAT_LIQUID_SOLID),
+    "liquid_solid_latent_const": (dict(PHASES, kind="liquid_solid", latent_heat=2.7e5,
+                                       apparent_capacity=O.AC_CONSTANT), O.MAT_LIQUID_SOLID),
+    "gas_liquid_solid_latent_bell": (dict(PHASES, kind="gas_liquid_solid", latent_heat=2.7e5,
+                                          apparent_capacity=O.AC_POLY4_BELL), O.MAT_GAS_LIQUID_SOLID),
 }
 
 
@@ -171,3 +180,17 @@ def test_unidirectional_heat_golden_on_gpu(cuda, name):
     for printed in GOLDEN[name]["printed"]:
         opn.solve()
         assert cases.printed_match(opn.l2_norm(), printed), (opn.l2_norm(), printed)
+
+
+def test_latent_heat_refusals(cuda):
+    import meltpooldg_b200 as M
+    nc = (2, 2, 2)
+    gm, _ = meshes(nc, 2, 0.0)
+    with pytest.raises(Exception, match="volume-specific"):
+        M.HeatDiffuseOperator(gm, 1e-3, material=dict(PHASES, kind="liquid_solid", volume_specific=True,
+                                                       latent_heat=1e5))
+    with pytest.raises(Exception, match="latent heat"):
+        M.HeatDiffuseOperator(gm, 1e-3, material=dict(PHASES, kind="liquid_solid", latent_heat=-1.0))
+    with pytest.raises(Exception, match="apparent capacity profile"):
+        M.HeatDiffuseOperator(gm, 1e-3, material=dict(PHASES, kind="liquid_solid", latent_heat=1e5,
+                                                       apparent_capacity=7))
