@@ -305,7 +305,7 @@ namespace {
 void free_op_arrays(Op &o)
 {
   free_workspace(o);
-  for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32,
+  for (void *p : {(void *)o.T_own, (void *)o.d_err, (void *)o.d_coef64, (void *)o.d_coef32, (void *)o.T32, (void *)o.Ts32,
                   (void *)o.d_velb64, (void *)o.d_velb32, (void *)o.d_trig32, (void *)o.d_trig64, o.d_stage,
                   (void *)o.d_tau64, (void *)o.d_tau32, (void *)o.d_lam64, (void *)o.d_lam32, (void *)o.Told_own, (void *)o.H_own, (void *)o.Told32,
                   (void *)o.H32, (void *)o.lsq_buf, (void *)o.host_stage,

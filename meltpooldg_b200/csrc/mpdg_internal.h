@@ -180,6 +180,7 @@ struct Op {
   const double *Told64 = nullptr, *H64 = nullptr;
   double *Told_own = nullptr, *H_own = nullptr;
   float *Told32 = nullptr, *H32 = nullptr;  // FP32: T - T_old and the heaviside
+  float *Ts32 = nullptr;                    // FP32, laws with a solid phase: T - solidus
   // velocity as a DoF vector (MPDG_VEL_NODAL): component-major [3][N],
   // caller-owned or set from host values
   const double *U64 = nullptr;

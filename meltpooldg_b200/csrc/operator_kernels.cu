@@ -1763,6 +1763,12 @@ __global__ void diff_cast_kernel(const double *a, const double *b, float *c, lon
   if (i < n) c[i] = (float)(a[i] - b[i]);
 }
 
+__global__ void shift_cast_kernel(const double *a, double shift, float *c, long n)
+{
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) c[i] = (float)(a[i] - shift);
+}
+
 // FP32 copies of the fields the FP32 form reads: T, the heaviside, and the
 // increment T - T_old (formed in FP64: the float copies of T and T_old would
 // lose its digits to cancellation)
@@ -1780,6 +1786,14 @@ void ensure_T32(Op &op)
   if (op.T64 && op.Told64) {
     if (!op.Told32) op.Told32 = dev_alloc<float>(N, op.device_bytes);
     diff_cast_kernel<<<grid_for(N, 256), 256, 0, op.stream>>>(op.T64, op.Told64, op.Told32, N);
+    MPDG_LAUNCHED();
+  }
+  // laws with a solid phase read T - solidus: within the mushy zone the
+  // solid fraction and the apparent capacity vary on the scale of
+  // liquidus - solidus, far finer than a float's resolution of T itself
+  if (op.T64 && op.d.kind == MPDG_OP_HEAT && law_has_solid(op.d.material)) {
+    if (!op.Ts32) op.Ts32 = dev_alloc<float>(N, op.device_bytes);
+    shift_cast_kernel<<<grid_for(N, 256), 256, 0, op.stream>>>(op.T64, op.d.solidus, op.Ts32, N);
     MPDG_LAUNCHED();
   }
 }
@@ -1869,6 +1883,13 @@ KP<Real> base_params(Op &op)
     k.Told = law_T ? op.Told32 : nullptr;  // T - T_old
     k.told_inc = 1;
     k.Hs = law_H ? op.H32 : nullptr;
+    if (law_T) {
+      // T - solidus against the shifted zone [0, liquidus - solidus] (ensure_T32)
+      if (!op.Ts32) throw Error{MPDG_ERR_ARG, "the FP32 form was not prepared for this operator (precision_mask)"};
+      k.T = op.Ts32;
+      k.solidus = Real(0);
+      k.liquidus = (Real)(op.d.liquidus - op.d.solidus);
+    }
   }
   const bool mask = op.use_dirichlet && m.has_dirichlet;
   k.masked_read = mask;
