@@ -441,7 +441,6 @@ mpdg_status mpdg_op_set_inflow_outflow(mpdg_op *op, const uint8_t *host_mask)
   return guarded([&]() -> int {
     if (!op) throw Error{MPDG_ERR_ARG, "null operator"};
     Op &o = op->o;
-    if (o.mesh->mapped && host_mask) throw Error{MPDG_ERR_UNSUPPORTED, "inflow/outflow rows on mapped meshes"};
     if (o.d_io) {
       MPDG_CUDA(cudaStreamSynchronize(o.stream));
       cudaFree(o.d_io);

@@ -2601,10 +2601,6 @@ __global__ void io_post_kernel(Real *dst, const Real *src, const uint8_t *io, lo
 template <typename Real>
 void launch_apply(Op &op, Real *dst, const Real *src)
 {
-  if (op.mesh->mapped) {
-    launch_mapped_apply<Real>(op, dst, src);
-    return;
-  }
   const Real *in = src;
   const long N = op.mesh->N;
   const unsigned grid = (unsigned)std::min(grid_for(N, 256), (unsigned)(148 * 16));
@@ -2623,9 +2619,13 @@ void launch_apply(Op &op, Real *dst, const Real *src)
     MPDG_LAUNCHED();
     in = (const Real *)op.io_tmp;
   }
-  launch_cells<Real>(op, dst, in);
-  launch_robin<Real>(op, dst, in, ROBIN_APPLY);
-  if (op.fine) launch_fine_block<Real>(op, dst, in);
+  if (op.mesh->mapped) {
+    launch_mapped_apply<Real>(op, dst, in);
+  } else {
+    launch_cells<Real>(op, dst, in);
+    launch_robin<Real>(op, dst, in, ROBIN_APPLY);
+    if (op.fine) launch_fine_block<Real>(op, dst, in);
+  }
   if (op.d_io) {
     // do_post_vmult: identity rows
     io_post_kernel<Real><<<grid, 256, 0, op.stream>>>(dst, src, op.d_io, N);

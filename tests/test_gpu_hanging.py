@@ -133,3 +133,28 @@ def test_two_level_cg_iterations_match_oracle(cuda, p):
                                                             mixed_precision=True))
     r = b - O.vmult2(om, oop, x2.cpu().numpy())
     assert np.linalg.norm(r) <= 1.01e-10 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_two_level_inflow_outflow_identity_rows(cuda, p):
+    """Identity rows (advection_diffusion_operator.cpp:537-578) across both
+    blocks of a two-level mesh: src read as 0 at the flagged DoFs, the result
+    there equal to src (hanging DoFs never flagged: they are not unknowns)."""
+    import torch
+    gm, om, mask = two_level(p, perturb=0.1, seed=30 + p, dirichlet=False)
+    op, oop = _ops(gm, "advdiff", mask)
+    R = np.random.default_rng(40 + p)
+    hm = om.hanging_mask().astype(bool)
+    io = (R.uniform(size=gm.n_dofs) < 0.2).astype(np.uint8)
+    io[hm] = 0
+    src = R.uniform(-1, 1, gm.n_dofs)
+    src[hm] = 0.0
+    ref = O.vmult2(om, oop, np.where(io == 1, 0.0, src))
+    ref[io == 1] = src[io == 1]
+    op.set_inflow_outflow(io)
+    dst = torch.empty(gm.n_dofs, dtype=torch.float64, device="cuda")
+    op.vmult(dst, dev(src))
+    assert relerr(dst.cpu().numpy(), ref) < TOL64
+    d32 = torch.empty(gm.n_dofs, dtype=torch.float32, device="cuda")
+    op.vmult(d32, dev(src, torch.float32))
+    assert relerr(d32.double().cpu().numpy(), ref) < TOL32

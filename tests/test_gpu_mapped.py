@@ -295,3 +295,43 @@ def test_locally_refined_mesh(cuda, p, kind):
     d = torch.empty_like(y)
     op.compute_diagonal(d)
     assert relerr(d.cpu().numpy(), O.mapped_diagonal(mm, oop)) < TOL64
+
+
+def test_mapped_inflow_outflow_identity_rows(cuda):
+    """Identity rows (do_pre_vmult / do_post_vmult,
+    advection_diffusion_operator.cpp:537-578) on a mapped mesh with a random
+    DoF numbering and hanging-node constraints: src read as 0 at the flagged
+    DoFs, the result there equal to src, the inverse diagonal 1 there."""
+    import torch
+    import meltpooldg_b200 as M
+    from meltpooldg_b200.refine import refine_box
+    p = 2
+    V = O.box_vertices(3, (3, 3, 3), [-1.0] * 3, [1.0] * 3, 0.1, 12)
+    r = refine_box((3, 3, 3), p, [13, 4], vertices=V)
+    mm = O.MappedMesh(p, r["cell_vertices"], r["cell_dofs"], r["n_dofs"], r["constraints"])
+    gm = device_mesh(mm, None)
+    R = rng(88)
+    io = (R.uniform(size=mm.n_dofs) < 0.2).astype(np.uint8)
+    io[mm.constrained_mask().astype(bool)] = 0
+    op, oop = _ops(gm, "advdiff", None)
+    src = R.uniform(-1, 1, mm.n_dofs)
+    ref = O.mapped_vmult(mm, oop, np.where(io == 1, 0.0, src))
+    ref[io == 1] = src[io == 1]
+    op.set_inflow_outflow(io)
+    d_src = dev(src)
+    dst = torch.empty_like(d_src)
+    op.vmult(dst, d_src)
+    assert relerr(dst.cpu().numpy(), ref) < TOL64
+    assert torch.equal(d_src, dev(src))
+    d32 = torch.empty(mm.n_dofs, dtype=torch.float32, device="cuda")
+    op.vmult(d32, dev(src, torch.float32))
+    assert relerr(d32.double().cpu().numpy(), ref) < TOL32
+    inv = torch.empty_like(d_src)
+    op.compute_inverse_diagonal_from_matrixfree(inv)
+    d = O.mapped_diagonal(mm, oop)
+    thr = 1e-14 * max(1.0, np.abs(d).max())
+    want = np.where(np.abs(d) > thr, 1.0 / np.where(d == 0, 1.0, d), 1.0)
+    want[io == 1] = 1.0
+    got = inv.cpu().numpy()
+    free = mm.constrained_mask() == 0
+    assert relerr(got[free], want[free]) < TOL64
