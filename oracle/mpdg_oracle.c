@@ -653,6 +653,46 @@ static double cell_tau(const orc_mesh *m, const orc_op *op, const geo_t *g, int 
   return (umax >= 1e-6) ? h / umax : 0.0;
 }
 
+/* SUPG parameter of a cell given by its corners vc and DoFs idx (mapped
+ * meshes): as cell_tau, with the velocity at the mapped Gauss points (the
+ * nodal field interpolated through idx) */
+static double tau_vc(const orc_op *op, const geo_t *g, double vc[8][3], const long *idx)
+{
+  if (!op->supg || op->kind != ORC_ADVDIFF) return 0.0;
+  const int dim = g->dim, n = g->n, nz = (dim == 3) ? n : 1, nqt = n * n * nz;
+  const int pairs3[4][2] = {{0, 7}, {1, 6}, {2, 5}, {3, 4}}, pairs2[2][2] = {{0, 3}, {1, 2}};
+  double diam = 0.0;
+  for (int k = 0; k < ((dim == 3) ? 4 : 2); ++k) {
+    const int a = (dim == 3) ? pairs3[k][0] : pairs2[k][0], b = (dim == 3) ? pairs3[k][1] : pairs2[k][1];
+    double d2 = 0.0;
+    for (int c = 0; c < dim; ++c) d2 += (vc[a][c] - vc[b][c]) * (vc[a][c] - vc[b][c]);
+    diam = fmax(diam, sqrt(d2));
+  }
+  const double h = diam / sqrt((double)dim);
+  if (op->supg_coefficient >= 0.0) return op->supg_coefficient * h;
+  double umax = 0.0;
+  for (int q = 0; q < nqt; ++q) {
+    const int qq[3] = {q % n, (q / n) % n, q / (n * n)};
+    const double xi[3] = {g->xq[qq[0]], g->xq[qq[1]], (dim == 3) ? g->xq[qq[2]] : 0.0};
+    double x[3], J[3][3], u[3] = {0.0, 0.0, 0.0};
+    map_point(g, vc, xi, x, J);
+    if (op->vel_kind == ORC_VEL_NODAL) {
+      for (int t = 0; t < nqt; ++t) {
+        const int c[3] = {t % n, (t / n) % n, t / (n * n)};
+        double phi = 1.0;
+        for (int d = 0; d < dim; ++d) phi *= g->S[qq[d] * n + c[d]];
+        for (int d = 0; d < dim; ++d) u[d] += op->vel_nodal[(long)d * g->N + idx[t]] * phi;
+      }
+    } else {
+      velocity_at(op, dim, x, u);
+    }
+    double s2 = 0.0;
+    for (int a = 0; a < dim; ++a) s2 += u[a] * u[a];
+    umax = fmax(umax, sqrt(s2));
+  }
+  return (umax >= 1e-6) ? h / umax : 0.0;
+}
+
 /* physical Laplacian at the quadrature points from the reference gradients:
  * sum_ab Gt_ab d2u/dxi_a dxi_b - lam . grad_ref u (map_lambda), the second
  * reference derivatives by collocation differentiation of the gradients */
@@ -1705,6 +1745,7 @@ static void mapped_geo(const orc_mapped *m, geo_t *g)
 {
   orc_mesh dummy = {3, m->degree, {1, 1, 1}, NULL};
   geo_init(&dummy, g);
+  g->N = m->n_dofs; /* component stride of a nodal velocity field */
 }
 
 static void mapped_cell(const orc_mapped *m, long K, double vc[8][3], long *idx, int nqt)
@@ -1725,7 +1766,7 @@ void orcm_vmult(const orc_mapped *m, const orc_op *op, double *dst, const double
     double vc[8][3], ul[MAXN3];
     long idx[MAXN3];
     mapped_cell(m, K, vc, idx, nqt);
-    element_matrix_vc(op, &g, vc, idx, 0.0, A);
+    element_matrix_vc(op, &g, vc, idx, tau_vc(op, &g, vc, idx), A);
     for (int t = 0; t < nqt; ++t) {
       long cnt, own;
       double one, v = 0.0;
@@ -1764,7 +1805,7 @@ void orcm_diagonal(const orc_mapped *m, const orc_op *op, double *diag)
     double vc[8][3];
     long idx[MAXN3];
     mapped_cell(m, K, vc, idx, nqt);
-    element_matrix_vc(op, &g, vc, idx, 0.0, A);
+    element_matrix_vc(op, &g, vc, idx, tau_vc(op, &g, vc, idx), A);
     /* distinct targets of the cell and their weights per local DoF */
     long tg[4 * MAXN3];
     int nt = 0;

@@ -44,3 +44,45 @@ def test_mapped_hanging_constraints_equal_two_level(p, kind):
     assert np.abs(O.mapped_vmult(mm, op, x) - a).max() <= 1e-14 * np.abs(a).max()
     d = O.diagonal2(m2, op)
     assert np.abs(O.mapped_diagonal(mm, op) - d).max() <= 1e-13 * np.abs(d).max()
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+@pytest.mark.parametrize("coef", [-1.0, 0.7])
+def test_mapped_supg_equals_structured(p, coef):
+    """SUPG with diffusion (the Laplacian with the map's curvature) through the
+    mapped path, with tau_K from the mapped cell's corners and Gauss points,
+    equals the structured oracle on the same perturbed mesh, renumbered."""
+    m = O.Mesh.box(3, p, [3, 2, 3], perturb=0.15, seed=4)
+    mask = m.boundary_face_mask([(1, 0)])
+    op = O.Operator(O.ADVDIFF, 1e-2, theta=0.5, diffusivity=0.05, vel_kind=O.VEL_VORTEX, dirichlet=mask,
+                    supg=True, supg_coefficient=coef)
+    x = np.random.default_rng(p).uniform(-1, 1, m.n_dofs)
+    a = O.vmult(m, op, x)
+    R = np.random.default_rng(20 + p)
+    perm = R.permutation(m.n_dofs)
+    mp = O.mapped_from_mesh(m, perm=perm, cell_order=R.permutation(m.n_cells))
+    opp = op.with_dirichlet(mask[np.argsort(perm)])
+    xp = np.empty_like(x)
+    xp[perm] = x
+    assert np.abs(O.mapped_vmult(mp, opp, xp)[perm] - a).max() <= 1e-13 * np.abs(a).max()
+    d = O.diagonal(m, op)
+    assert np.abs(O.mapped_diagonal(mp, opp)[perm] - d).max() <= 1e-13 * np.abs(d).max()
+
+
+def test_mapped_nodal_velocity_equals_structured():
+    """A velocity DoF vector read through the cell->DoF map of a renumbered mesh
+    (component stride = the mapped mesh's DoF count)."""
+    m = O.Mesh.box(3, 2, [3, 2, 2], perturb=0.1, seed=6)
+    R = np.random.default_rng(7)
+    U = R.uniform(-1, 1, (3, m.n_dofs))
+    op = O.Operator(O.HEAT, 1e-2, rho_cp=2.0, k0=1.5, vel_kind=O.VEL_NODAL, vel_nodal=U.reshape(-1))
+    x = R.uniform(-1, 1, m.n_dofs)
+    a = O.vmult(m, op, x)
+    perm = R.permutation(m.n_dofs)
+    mp = O.mapped_from_mesh(m, perm=perm)
+    Up = np.empty_like(U)
+    Up[:, perm] = U
+    opp = O.Operator(O.HEAT, 1e-2, rho_cp=2.0, k0=1.5, vel_kind=O.VEL_NODAL, vel_nodal=Up.reshape(-1))
+    xp = np.empty_like(x)
+    xp[perm] = x
+    assert np.abs(O.mapped_vmult(mp, opp, xp)[perm] - a).max() <= 1e-13 * np.abs(a).max()
