@@ -247,11 +247,9 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     if (desc->supg && mm.fine) throw Error{MPDG_ERR_UNSUPPORTED, "SUPG on two-level meshes"};
     if (desc->vel_kind == MPDG_VEL_NODAL && mm.fine)
       throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take no fields (velocity as a DoF vector)"};
-    if (desc->vel_kind == MPDG_VEL_NODAL && desc->supg && mm.mapped)
-      throw Error{MPDG_ERR_UNSUPPORTED, "SUPG on mapped meshes"};
-    if (mm.mapped && (desc->supg || (desc->robin_faces && desc->robin_alpha != 0.0) ||
+    if (mm.mapped && ((desc->robin_faces && desc->robin_alpha != 0.0) ||
                       (desc->rad_faces && desc->rad_emissivity != 0.0)))
-      throw Error{MPDG_ERR_UNSUPPORTED, "mapped meshes take no boundary faces or SUPG"};
+      throw Error{MPDG_ERR_UNSUPPORTED, "mapped meshes take no boundary faces"};
     if (mm.mapped && mm.n_cons > 0 &&
         (desc->k_alpha != 0.0 || desc->full_tangent || desc->material != MPDG_MAT_LINEAR))
       throw Error{MPDG_ERR_UNSUPPORTED,

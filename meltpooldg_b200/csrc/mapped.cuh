@@ -97,6 +97,72 @@ __global__ void elem_matrix_kernel(const KP<double> p, const long *ccells, doubl
   }
 }
 
+// element matrices of the listed cells with the SUPG terms of the
+// advection-diffusion tangent (advection_diffusion_operator.cpp:471-493): the
+// matrix above plus tau_K (b.grad phi_t) (c_mass phi_u + c_vel b.grad phi_u / JxW
+// - c_diff lap phi_u), lap phi_u = G : H_xi(phi_u) / JxW - lam . grad_xi phi_u
+// (second reference derivatives of the basis: D2 = Dc D, the collocation
+// derivative of its derivative at the Gauss points, as the cell kernel takes them)
+template <int P>
+__global__ void elem_matrix_supg_kernel(const KP<double> p, const long *cells, double *A)
+{
+  constexpr int n = P + 1, n2 = n * n, n3 = n2 * n;
+  const Tables<double> &T = tab<double>(P);
+  __shared__ double D2[n * n];
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int q = e / n, i = e % n;
+    double s = 0.0;
+    for (int r = 0; r < n; ++r) s += T.Dc[q * n + r] * T.D[r * n + i];
+    D2[e] = s;
+  }
+  __syncthreads();
+  const long cell = cells[blockIdx.x];
+  const double *m = p.metric + cell * metric_stride(n);
+  const double *vb = p.velb + cell * velb_stride(n);
+  const double *lm = p.lam ? p.lam + cell * 3 * n3 : nullptr;
+  const double tau = p.tau[cell];
+  double *Ac = A + (long)blockIdx.x * n3 * n3;
+  for (int e = threadIdx.x; e < n3 * n3; e += blockDim.x) {
+    const int t = e / n3, u = e % n3;
+    const int tc[3] = {t % n, (t / n) % n, t / n2}, uc[3] = {u % n, (u / n) % n, u / n2};
+    double s = 0.0;
+    for (int q = 0; q < n3; ++q) {
+      const int qc[3] = {q % n, (q / n) % n, q / n2};
+      double st[3], dt[3], su[3], du[3], d2u[3];
+      for (int d = 0; d < 3; ++d) {
+        st[d] = T.S[qc[d] * n + tc[d]];
+        dt[d] = T.D[qc[d] * n + tc[d]];
+        su[d] = T.S[qc[d] * n + uc[d]];
+        du[d] = T.D[qc[d] * n + uc[d]];
+        d2u[d] = D2[qc[d] * n + uc[d]];
+      }
+      const double pt = st[0] * st[1] * st[2], pu = su[0] * su[1] * su[2];
+      const double gt[3] = {dt[0] * st[1] * st[2], st[0] * dt[1] * st[2], st[0] * st[1] * dt[2]};
+      const double gu[3] = {du[0] * su[1] * su[2], su[0] * du[1] * su[2], su[0] * su[1] * du[2]};
+      const double JxW = m[q], G00 = m[n3 + q], G01 = m[2 * n3 + q], G02 = m[3 * n3 + q],
+                   G11 = m[4 * n3 + q], G12 = m[5 * n3 + q], G22 = m[6 * n3 + q];
+      const double b0 = vb[q], b1 = vb[n3 + q], b2 = vb[2 * n3 + q];
+      const double adv_u = b0 * gu[0] + b1 * gu[1] + b2 * gu[2], adv_t = b0 * gt[0] + b1 * gt[1] + b2 * gt[2];
+      double v = p.c_mass * JxW * pt * pu + pt * p.c_vel * adv_u;
+      const double f0 = G00 * gu[0] + G01 * gu[1] + G02 * gu[2];
+      const double f1 = G01 * gu[0] + G11 * gu[1] + G12 * gu[2];
+      const double f2 = G02 * gu[0] + G12 * gu[1] + G22 * gu[2];
+      v += p.c_diff * (gt[0] * f0 + gt[1] * f1 + gt[2] * f2);
+      double r = p.c_mass * pu + p.c_vel * adv_u / JxW;
+      if (p.supg_lap) {
+        const double hxx = d2u[0] * su[1] * su[2], hyy = su[0] * d2u[1] * su[2], hzz = su[0] * su[1] * d2u[2];
+        const double hxy = du[0] * du[1] * su[2], hxz = du[0] * su[1] * du[2], hyz = su[0] * du[1] * du[2];
+        double lap = (G00 * hxx + G11 * hyy + G22 * hzz + 2.0 * (G01 * hxy + G02 * hxz + G12 * hyz)) / JxW;
+        if (lm) lap -= lm[q] * gu[0] + lm[n3 + q] * gu[1] + lm[2 * n3 + q] * gu[2];
+        r -= p.c_diff * lap;
+      }
+      v += tau * adv_t * r;
+      s += v;
+    }
+    Ac[e] = s;
+  }
+}
+
 // one warp per task (constrained-cell slot, target DoF): w^T A w, with w_t the
 // weight of the target in local DoF t's entries (itself, or its constraint)
 template <int P>
@@ -381,7 +447,13 @@ void launch_mapped_apply(Op &op, Real *dst, const Real *src)
   if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
   check_law_fields(op, k);
   MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * N, op.stream));
-  if (!kt && !uses_law(op)) {
+  if (supg(op)) {
+    // SUPG: the block kernel with the stabilisation flux through the map
+    if constexpr (sizeof(Real) == 4) {
+      if (!op.d_tau32) throw Error{MPDG_ERR_ARG, "the FP32 form was not prepared for this operator (precision_mask)"};
+    }
+    dispatch_degree<Real, MODE_SUPG, false>(op, k);
+  } else if (!kt && !uses_law(op)) {
     // constant coefficients: the warp kernel on the merged coefficient stream
     ensure_coef(op, sizeof(Real) == 4);
     if constexpr (sizeof(Real) == 8) k.metric = op.d_coef64;
@@ -396,12 +468,15 @@ void launch_mapped_apply(Op &op, Real *dst, const Real *src)
 }
 
 namespace {
+// diagonal contributions w^T A_K w of the cells `cells` (device copy d_cells)
+// through their element matrices: the constrained cells of a mapped mesh, or
+// with `supg` every cell (SUPG element matrices)
 template <int P>
-void mapped_constrained_diagonal(Op &op, double *diag)
+void mapped_element_diagonal(Op &op, double *diag, const std::vector<long> &cells, const long *d_cells, bool supg)
 {
   Mesh &m = *op.mesh;
   constexpr int n = P + 1, n3 = n * n * n;
-  const long ncc = (long)m.ccells.size();
+  const long ncc = (long)cells.size();
   if (ncc == 0) return;
   // tasks: every DoF (target) of every constrained cell, sorted by target
   std::vector<int> hmap((size_t)ncc * n3);
@@ -409,7 +484,7 @@ void mapped_constrained_diagonal(Op &op, double *diag)
     std::vector<int> all((size_t)m.n_cells * n3);
     MPDG_CUDA(cudaMemcpy(all.data(), m.d_cmap, sizeof(int) * all.size(), cudaMemcpyDeviceToHost));
     for (long c = 0; c < ncc; ++c)
-      for (int t = 0; t < n3; ++t) hmap[(size_t)c * n3 + t] = all[(size_t)m.ccells[c] * n3 + t];
+      for (int t = 0; t < n3; ++t) hmap[(size_t)c * n3 + t] = all[(size_t)cells[c] * n3 + t];
   }
   std::vector<int> cons_of(m.N);
   MPDG_CUDA(cudaMemcpy(cons_of.data(), m.d_cons_of, sizeof(int) * m.N, cudaMemcpyDeviceToHost));
@@ -458,11 +533,12 @@ void mapped_constrained_diagonal(Op &op, double *diag)
     d_tgt = upload(tgt, scratch);
     d_tptr = upload(tptr, scratch);
     KP<double> k = base_params<double>(op);
-    elem_matrix_kernel<P><<<(unsigned)ncc, 256, 0, op.stream>>>(k, m.d_ccells, A);
+    if (supg) elem_matrix_supg_kernel<P><<<(unsigned)ncc, 256, 0, op.stream>>>(k, d_cells, A);
+    else elem_matrix_kernel<P><<<(unsigned)ncc, 256, 0, op.stream>>>(k, d_cells, A);
     MPDG_LAUNCHED();
     const long nt = (long)tasks.size();
     cell_task_kernel<P><<<(unsigned)((nt + 3) / 4), 128, 0, op.stream>>>(
-        nt, d_task_cc, d_task_tgt, m.d_ccells, m.d_cmap, m.d_cons_of, m.d_cons_ptr, m.d_cons_mast, m.d_cons_w, A,
+        nt, d_task_cc, d_task_tgt, d_cells, m.d_cmap, m.d_cons_of, m.d_cons_ptr, m.d_cons_mast, m.d_cons_w, A,
         val);
     MPDG_LAUNCHED();
     task_fold_kernel<<<grid_for((long)tgt.size(), 256), 256, 0, op.stream>>>((long)tgt.size(), d_tgt, d_tptr, val,
@@ -493,12 +569,52 @@ void launch_mapped_diagonal(Op &op, double *diag)
   if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
   check_law_fields(op, k);
   MPDG_CUDA(cudaMemsetAsync(diag, 0, sizeof(double) * m.N, op.stream));
-  switch (m.degree) {
-    case 1: kt ? run_diag<1, true>(op, k) : run_diag<1, false>(op, k); mapped_constrained_diagonal<1>(op, diag); break;
-    case 2: kt ? run_diag<2, true>(op, k) : run_diag<2, false>(op, k); mapped_constrained_diagonal<2>(op, diag); break;
-    case 3: kt ? run_diag<3, true>(op, k) : run_diag<3, false>(op, k); mapped_constrained_diagonal<3>(op, diag); break;
-    case 4: kt ? run_diag<4, true>(op, k) : run_diag<4, false>(op, k); mapped_constrained_diagonal<4>(op, diag); break;
-    default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+  if (supg(op)) {
+    // SUPG: the element matrices of every cell, in chunks of cells that bound
+    // the scratch (the diagonal is built once per operator)
+    if (!op.d_velb64 || !op.d_tau64) throw Error{MPDG_ERR_ARG, "SUPG diagonal: velocity stream or tau missing"};
+    const long chunk = 16384;
+    for (long c0 = 0; c0 < m.n_cells; c0 += chunk) {
+      std::vector<long> cells;
+      for (long c = c0; c < std::min(m.n_cells, c0 + chunk); ++c) cells.push_back(c);
+      size_t scratch = 0;
+      long *d_cells = upload(cells, scratch);
+      try {
+        switch (m.degree) {
+          case 1: mapped_element_diagonal<1>(op, diag, cells, d_cells, true); break;
+          case 2: mapped_element_diagonal<2>(op, diag, cells, d_cells, true); break;
+          case 3: mapped_element_diagonal<3>(op, diag, cells, d_cells, true); break;
+          case 4: mapped_element_diagonal<4>(op, diag, cells, d_cells, true); break;
+          default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+        }
+      } catch (...) {
+        cudaStreamSynchronize(op.stream);
+        cudaFree(d_cells);
+        throw;
+      }
+      MPDG_CUDA(cudaStreamSynchronize(op.stream));
+      cudaFree(d_cells);
+    }
+  } else {
+    switch (m.degree) {
+      case 1:
+        kt ? run_diag<1, true>(op, k) : run_diag<1, false>(op, k);
+        mapped_element_diagonal<1>(op, diag, m.ccells, m.d_ccells, false);
+        break;
+      case 2:
+        kt ? run_diag<2, true>(op, k) : run_diag<2, false>(op, k);
+        mapped_element_diagonal<2>(op, diag, m.ccells, m.d_ccells, false);
+        break;
+      case 3:
+        kt ? run_diag<3, true>(op, k) : run_diag<3, false>(op, k);
+        mapped_element_diagonal<3>(op, diag, m.ccells, m.d_ccells, false);
+        break;
+      case 4:
+        kt ? run_diag<4, true>(op, k) : run_diag<4, false>(op, k);
+        mapped_element_diagonal<4>(op, diag, m.ccells, m.d_ccells, false);
+        break;
+      default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
+    }
   }
   const uint8_t *tm = op.use_dirichlet ? m.d_tmask_dir : m.d_tmask_hang;
   set_masked_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, tm, 1.0);

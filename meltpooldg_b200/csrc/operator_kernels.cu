@@ -1357,26 +1357,15 @@ __global__ void nodal_velb_kernel(const double *vert, int nc0, int nc1, long NX,
 // coefficient, h_K / max_q |u(x_q)| (0 when that maximum is below 1e-6), with the
 // cell size h_K = diameter / sqrt(3) (scratch_data.cpp:249-266); the diameter of
 // a hexahedron is its longest main diagonal
-__global__ void tau_kernel(const double *vert, int nc0, int nc1, int nc2, int P, const Colour *colours,
-                           int vel_kind, double s0, double s1, double s2, double coef, const double *xq_all,
-                           double *tau64, float *tau32, const double *umag)
+__global__ void tau_kernel(const double *vert, int nc0, int nc1, long n_cells, int P, const Colour *colours,
+                           const double *cellvert, int vel_kind, double s0, double s1, double s2, double coef,
+                           const double *xq_all, double *tau64, float *tau32, const double *umag)
 {
   const int n = P + 1;
   const long cell = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long n_cells = (long)nc0 * nc1 * nc2;
   if (cell >= n_cells) return;
-  int c = 0;
-  while (c < 7 && cell >= colours[c + 1].first) ++c;
-  const Colour &C = colours[c];
-  const long cidx = cell - C.first;
-  const int ix = 2 * (int)(cidx % C.cn[0]) + C.par[0];
-  const int iy = 2 * (int)((cidx / C.cn[0]) % C.cn[1]) + C.par[1];
-  const int iz = 2 * (int)(cidx / ((long)C.cn[0] * C.cn[1])) + C.par[2];
   double V[8][3];
-  for (int v = 0; v < 8; ++v) {
-    const long vid = ((long)(iz + ((v >> 2) & 1)) * (nc1 + 1) + (iy + ((v >> 1) & 1))) * (nc0 + 1) + (ix + (v & 1));
-    for (int a = 0; a < 3; ++a) V[v][a] = vert[vid * 3 + a];
-  }
+  cell_corners(vert, nc0, nc1, colours, cellvert, cell, V);
   double diam = 0.0;
   for (int d = 0; d < 4; ++d) {
     double s = 0.0;
@@ -1629,8 +1618,8 @@ void build_op_device_data(Op &op)
       MPDG_CUDA(cudaMemset(op.d_tau64, 0, sizeof(double) * m.n_cells));
       if (op.d_tau32) MPDG_CUDA(cudaMemset(op.d_tau32, 0, sizeof(float) * m.n_cells));
     } else {
-      tau_kernel<<<grid_for(m.n_cells, 128), 128>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col,
-                                                    op.d.vel_kind, op.d.vel_param[0], op.d.vel_param[1],
+      tau_kernel<<<grid_for(m.n_cells, 128), 128>>>(m.d_vert, m.nc[0], m.nc[1], m.n_cells, p, d_col,
+                                                    m.d_cellvert, op.d.vel_kind, op.d.vel_param[0], op.d.vel_param[1],
                                                     op.d.vel_param[2], op.d.supg_coefficient, d_xq, op.d_tau64,
                                                     op.d_tau32, nullptr);
       MPDG_LAUNCHED();
@@ -1744,8 +1733,8 @@ void build_nodal_velocity(Op &op)
       gauss(n, xq, wq);
       MPDG_CUDA(tracked_malloc(&d_xq, sizeof(xq)));
       MPDG_CUDA(cudaMemcpyAsync(d_xq, xq, sizeof(xq), cudaMemcpyHostToDevice, op.stream));
-      tau_kernel<<<grid_for(m.n_cells, 128), 128, 0, op.stream>>>(m.d_vert, m.nc[0], m.nc[1], m.nc[2], p, d_col,
-                                                                 op.d.vel_kind, 0.0, 0.0, 0.0,
+      tau_kernel<<<grid_for(m.n_cells, 128), 128, 0, op.stream>>>(m.d_vert, m.nc[0], m.nc[1], m.n_cells, p, d_col,
+                                                                 m.d_cellvert, op.d.vel_kind, 0.0, 0.0, 0.0,
                                                                  op.d.supg_coefficient, d_xq, op.d_tau64,
                                                                  op.d_tau32, umag);
       MPDG_LAUNCHED();

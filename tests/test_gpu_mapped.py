@@ -335,3 +335,77 @@ def test_mapped_inflow_outflow_identity_rows(cuda):
     got = inv.cpu().numpy()
     free = mm.constrained_mask() == 0
     assert relerr(got[free], want[free]) < TOL64
+
+
+def _supg_ops(gm, mask, coef):
+    import meltpooldg_b200 as M
+    return (M.AdvectionDiffusionOperator(gm, 1e-2, theta=0.5, diffusivity=0.05, velocity="vortex",
+                                         precisions=("fp64", "fp32"), supg=True, supg_coefficient=coef),
+            O.Operator(O.ADVDIFF, 1e-2, theta=0.5, diffusivity=0.05, vel_kind=O.VEL_VORTEX, dirichlet=mask,
+                       supg=True, supg_coefficient=coef))
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+@pytest.mark.parametrize("coef", [-1.0, 0.7])
+def test_mapped_supg_renumbered(cuda, p, coef):
+    """SUPG with diffusion (tau_K from the cell's corners, the Laplacian with
+    the map's curvature) through a mapped mesh with a random numbering: vmult
+    (FP64, FP32) and the element-matrix diagonal against the oracle's mapped
+    operator; create_rhs as the structured device path's."""
+    import torch
+    import meltpooldg_b200 as M
+    nc = (3, 2, 3)
+    mask_s = M.boundary_mask(nc, p, faces=[(1, 0)])
+    gs, om = meshes(nc, p, 0.15, seed=30 + p, mask=mask_s, lo=(-1, -1, -1), hi=(1, 1, 1))
+    R = rng(60 + p)
+    perm = R.permutation(om.n_dofs)
+    mm = O.mapped_from_mesh(om, perm=perm, cell_order=R.permutation(om.n_cells))
+    mask = np.empty_like(mask_s)
+    mask[perm] = mask_s
+    gm = device_mesh(mm, mask)
+    op, oop = _supg_ops(gm, mask, coef)
+    x = R.uniform(-1, 1, om.n_dofs)
+    ref = O.mapped_vmult(mm, oop, x)
+    y = torch.empty(om.n_dofs, dtype=torch.float64, device="cuda")
+    op.vmult(y, dev(x))
+    assert relerr(y.cpu().numpy(), ref) < TOL64
+    y32 = torch.empty(om.n_dofs, dtype=torch.float32, device="cuda")
+    op.vmult(y32, dev(x, torch.float32))
+    assert relerr(y32.double().cpu().numpy(), ref) < TOL32
+    d = torch.empty_like(y)
+    op.compute_diagonal(d)
+    assert relerr(d.cpu().numpy(), O.mapped_diagonal(mm, oop)) < TOL64
+    # create_rhs: as the structured path on the same mesh
+    ops, _ = _supg_ops(gs, mask_s, coef)
+    phi = R.uniform(-1, 1, om.n_dofs)
+    rs = torch.zeros(om.n_dofs, dtype=torch.float64, device="cuda")
+    ops.create_rhs(rs, dev(phi))
+    phim = np.empty_like(phi)
+    phim[perm] = phi
+    rm = torch.zeros_like(rs)
+    op.create_rhs(rm, dev(phim))
+    assert relerr(rm.cpu().numpy()[perm], rs.cpu().numpy()) < TOL64
+    assert op.device_error() == 0
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_mapped_supg_with_hanging_constraints(cuda, p):
+    """SUPG on a locally refined mesh (face and edge hanging nodes, perturbed
+    vertices): vmult and the diagonal of the condensed operator against the
+    oracle's mapped operator."""
+    import torch
+    from meltpooldg_b200.refine import refine_box
+    V = O.box_vertices(3, (3, 3, 3), [-1.0] * 3, [1.0] * 3, 0.1, 17)
+    r = refine_box((3, 3, 3), p, [13, 4], vertices=V)
+    mm = O.MappedMesh(p, r["cell_vertices"], r["cell_dofs"], r["n_dofs"], r["constraints"])
+    mask = r["boundary"]
+    gm = device_mesh(mm, mask)
+    op, oop = _supg_ops(gm, mask, -1.0)
+    x = rng(70 + p).uniform(-1, 1, mm.n_dofs)
+    ref = O.mapped_vmult(mm, oop, x)
+    y = torch.empty(mm.n_dofs, dtype=torch.float64, device="cuda")
+    op.vmult(y, dev(x))
+    assert relerr(y.cpu().numpy(), ref) < TOL64
+    d = torch.empty_like(y)
+    op.compute_diagonal(d)
+    assert relerr(d.cpu().numpy(), O.mapped_diagonal(mm, oop)) < TOL64
