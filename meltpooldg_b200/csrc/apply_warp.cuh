@@ -370,8 +370,9 @@ struct WOcc {
 // mdst[v] (msrc[0] = src, mdst[0] = dst) in one pass: each group's coefficient
 // block is staged once and serves every vector
 // MAPPED: a mapped mesh's cells, gathered and scattered through the
-// cell->DoF map p.cmap; dst is cleared before the colours and every cell adds
-// (the mesh's greedy colouring keeps the cells of a launch apart)
+// cell->DoF map p.cmap; the mesh's greedy colouring keeps the cells of a
+// launch apart, and the per-cell mask p.cell_first names the DoFs a cell
+// touches first in colour order: it stores them, later colours add
 // GROUP: threads that share a group of cells -- 32 (a warp per group, four
 // groups per CTA) or 128 (the whole CTA per group, fewer idle lanes for Q2/Q4;
 // every tile exchange is then a CTA barrier)
@@ -538,10 +539,16 @@ __global__ void __launch_bounds__(kWarpsPerCTA * 32, WOcc<P, Real>::min_blocks)
     const bool sy = (j == 0 && iy > 0) || (j == P && iy < p.nc[1] - 1);
     const bool later_xy = (sx && (ix & 1)) || (sy && (iy & 1));
     unsigned first_bits = 0, mask_bits = 0;
+    // mapped meshes: the cell's first-touch DoFs (lowest colour among their
+    // cells) from the per-cell mask; none when the mesh has no masks (dst cleared)
+    uint4 cfm = make_uint4(0u, 0u, 0u, 0u);
+    if constexpr (MAPPED) {
+      if (p.cell_first && active) cfm = p.cell_first[p.cfirst + cidx];
+    }
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       const bool sz = (k == 0 && iz > 0) || (k == P && iz < p.nc[2] - 1);
-      const bool first = !MAPPED && !(later_xy || (sz && (iz & 1)));
+      const bool first = MAPPED ? mask_bit(cfm, k) : !(later_xy || (sz && (iz & 1)));
       first_bits |= (unsigned)first << k;
     }
     mask_bits = p.masked_write ? lmask : 0u;

@@ -177,7 +177,7 @@ void free_mesh_arrays(Mesh &m)
 {
   for (void *p : {(void *)m.d_vert, (void *)m.d_metric64, (void *)m.d_metric32, (void *)m.d_dmask,
                   (void *)m.d_cell_flags, (void *)m.d_cell_mask, (void *)m.d_tmask_dir, (void *)m.d_tmask_hang,
-                  (void *)m.d_cmap, (void *)m.d_cellvert, (void *)m.d_cons_dof, (void *)m.d_cons_ptr,
+                  (void *)m.d_cmap, (void *)m.d_cell_first, (void *)m.d_cellvert, (void *)m.d_cons_dof, (void *)m.d_cons_ptr,
                   (void *)m.d_cons_mast, (void *)m.d_cons_w, (void *)m.d_mast_dof, (void *)m.d_mast_ptr,
                   (void *)m.d_mast_cons, (void *)m.d_mast_w, (void *)m.d_cons_of, (void *)m.d_ccells})
     if (p) cudaFree(p);

@@ -118,7 +118,7 @@ __global__ void elem_matrix_supg_kernel(const KP<double> p, const long *cells, d
   __syncthreads();
   const long cell = cells[blockIdx.x];
   const double *m = p.metric + cell * metric_stride(n);
-  const double *vb = p.velb + cell * velb_stride(n);
+  const double *vb = p.velb ? p.velb + cell * velb_stride(n) : nullptr;  // null: no velocity
   const double *lm = p.lam ? p.lam + cell * 3 * n3 : nullptr;
   const double tau = p.tau[cell];
   double *Ac = A + (long)blockIdx.x * n3 * n3;
@@ -141,7 +141,7 @@ __global__ void elem_matrix_supg_kernel(const KP<double> p, const long *cells, d
       const double gu[3] = {du[0] * su[1] * su[2], su[0] * du[1] * su[2], su[0] * su[1] * du[2]};
       const double JxW = m[q], G00 = m[n3 + q], G01 = m[2 * n3 + q], G02 = m[3 * n3 + q],
                    G11 = m[4 * n3 + q], G12 = m[5 * n3 + q], G22 = m[6 * n3 + q];
-      const double b0 = vb[q], b1 = vb[n3 + q], b2 = vb[2 * n3 + q];
+      const double b0 = vb ? vb[q] : 0.0, b1 = vb ? vb[n3 + q] : 0.0, b2 = vb ? vb[2 * n3 + q] : 0.0;
       const double adv_u = b0 * gu[0] + b1 * gu[1] + b2 * gu[2], adv_t = b0 * gt[0] + b1 * gt[1] + b2 * gt[2];
       double v = p.c_mass * JxW * pt * pu + pt * p.c_vel * adv_u;
       const double f0 = G00 * gu[0] + G01 * gu[1] + G02 * gu[2];
@@ -319,12 +319,16 @@ void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d)
   std::vector<double> cvert((size_t)E * 24);
   std::vector<uint8_t> flags(E, 0);
   std::vector<uint32_t> cmask(4 * (size_t)E, 0u);  // Dirichlet local DoFs (bit t), for the warp kernel
+  // first touch: the cell of the lowest colour among a DoF's cells stores it
+  // (colours launch in order and no two cells of a colour share a DoF)
+  std::vector<uint32_t> cfirst(4 * (size_t)E, 0u);
   for (long e = 0; e < E; ++e) {
     const long slot = next[colour_of[e]]++;
     uint8_t f = 0;
     for (int t = 0; t < n3; ++t) {
       const long g = d.cell_dofs[e * n3 + t];
       cmap[slot * n3 + t] = (int)g;
+      if (colour_of[e] == __builtin_ctzll(used[g])) cfirst[4 * slot + t / 32] |= 1u << (t % 32);
       if (d.dirichlet_mask && d.dirichlet_mask[g]) {
         f |= 1;
         cmask[4 * slot + t / 32] |= 1u << (t % 32);
@@ -347,6 +351,8 @@ void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d)
   }
   size_t &B = m.device_bytes;
   m.d_cmap = upload(cmap, B);
+  m.d_cell_first = upload(cfirst, B);
+  m.all_dofs_touched = std::all_of(used.begin(), used.end(), [](uint64_t u) { return u != 0; });
   m.d_cellvert = upload(cvert, B);
   m.d_cell_flags = upload(flags, B);
   m.d_ccells = upload(m.ccells, B);
@@ -446,7 +452,11 @@ void launch_mapped_apply(Op &op, Real *dst, const Real *src)
   const bool kt = uses_kT(op);
   if (kt && !k.T) throw Error{MPDG_ERR_ARG, "k(T) operator needs the temperature field"};
   check_law_fields(op, k);
-  MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * N, op.stream));
+  // the block kernels add into dst; the warp kernel stores each DoF's first
+  // touch, so dst needs clearing only where no cell touches a DoF
+  const bool warp_path = !supg(op) && !kt && !uses_law(op);
+  if (!warp_path || !m.all_dofs_touched || !m.d_cell_first)
+    MPDG_CUDA(cudaMemsetAsync(dst, 0, sizeof(Real) * N, op.stream));
   if (supg(op)) {
     // SUPG: the block kernel with the stabilisation flux through the map
     if constexpr (sizeof(Real) == 4) {
@@ -572,7 +582,7 @@ void launch_mapped_diagonal(Op &op, double *diag)
   if (supg(op)) {
     // SUPG: the element matrices of every cell, in chunks of cells that bound
     // the scratch (the diagonal is built once per operator)
-    if (!op.d_velb64 || !op.d_tau64) throw Error{MPDG_ERR_ARG, "SUPG diagonal: velocity stream or tau missing"};
+    if (!op.d_tau64) throw Error{MPDG_ERR_ARG, "SUPG diagonal: tau missing"};
     const long chunk = 16384;
     for (long c0 = 0; c0 < m.n_cells; c0 += chunk) {
       std::vector<long> cells;

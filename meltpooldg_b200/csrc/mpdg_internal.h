@@ -120,6 +120,10 @@ struct Mesh {
   uint8_t *d_cell_flags = nullptr;     // per colour-major cell: bit0 touches a constrained DoF
   uint32_t *d_cell_mask = nullptr;     // per colour-major cell: 128-bit mask of its constrained
                                        // local DoFs (bit k*n*n + j*n + i)
+  // mapped meshes: per colour-major cell, 128-bit mask of the local DoFs it
+  // touches first in colour order (it stores them; later colours add)
+  uint32_t *d_cell_first = nullptr;
+  bool all_dofs_touched = false;       // mapped meshes: every DoF lies in some cell
   bool has_dirichlet = false;
   size_t device_bytes = 0;
   bool metric32_ready = false;

@@ -263,6 +263,7 @@ struct KP {
   const uint8_t *dmask;
   const uint8_t *cell_flags;
   const uint4 *cell_mask;
+  const uint4 *cell_first;  // mapped meshes: first-touch local DoFs per cell (null: every cell adds)
   long NX, NY;
   int nc[3];
   int trig_stride;
@@ -1840,6 +1841,7 @@ KP<Real> base_params(Op &op)
   k.dmask = m.d_dmask;
   k.cell_flags = m.d_cell_flags;
   k.cell_mask = reinterpret_cast<const uint4 *>(m.d_cell_mask);
+  k.cell_first = reinterpret_cast<const uint4 *>(m.d_cell_first);
   const bool heat = op.d.kind == MPDG_OP_HEAT;
   k.c_mass = (Real)(heat ? op.d.rho_cp / op.d.dt : 1.0 / op.d.dt);
   k.c_vel = (Real)(heat ? op.d.rho_cp : op.d.theta);
