@@ -765,6 +765,13 @@ static void apply_cell(const orc_mesh *m, const orc_op *op, const geo_t *g, int 
  * dofs only). */
 enum { ROB_TANGENT = 0, ROB_RESIDUAL = 1 };
 
+static void face_terms_id(const orc_op *op, int id, int *conv, int *rad)
+{
+  const int bit = 1 << id;
+  *conv = op->kind == ORC_HEAT && (op->robin_faces & bit) && op->robin_alpha != 0.0;
+  *rad = op->kind == ORC_HEAT && (op->rad_faces & bit) && op->rad_emissivity != 0.0;
+}
+
 static void face_terms(const orc_op *op, int d, int s, int *conv, int *rad)
 {
   const int bit = 1 << (2 * d + s);
@@ -782,17 +789,17 @@ static int has_face_terms(const orc_op *op)
   return 0;
 }
 
-static void robin_face_apply(const orc_mesh *m, const orc_op *op, const geo_t *g, int ix, int iy, int iz,
-                             int d, int s, int mode, const long *idx, const double *ul_cell, double *out_cell,
-                             double *diag_cell)
+/* face terms of local face (d, s) of the cell with corners vc, selected by
+ * boundary id `id` (bit of robin_faces / rad_faces) */
+static void robin_face_apply_vc(const orc_op *op, const geo_t *g, double vc[8][3], int d, int s, int id,
+                                int mode, const long *idx, const double *ul_cell, double *out_cell,
+                                double *diag_cell)
 {
   const int n = g->n, dim = g->dim;
   int conv, rad;
-  face_terms(op, d, s, &conv, &rad);
+  face_terms_id(op, id, &conv, &rad);
   if (!conv && !rad) return;
   const double es = op->rad_emissivity * ORC_STEFAN_BOLTZMANN;
-  double vc[8][3];
-  cell_vertices(m, g, ix, iy, iz, vc);
   int t0 = (d == 0) ? 1 : 0;           /* tangential directions */
   int t1 = (dim == 3) ? ((d == 2) ? 1 : 2) : -1;
   const int nq1 = (dim == 3) ? n : 1, nb = (dim == 3) ? n : 1;
@@ -845,6 +852,36 @@ static void robin_face_apply(const orc_mesh *m, const orc_op *op, const geo_t *g
           if (out_cell) out_cell[li] += val * phi * JxW;
         }
     }
+}
+
+static void robin_face_apply(const orc_mesh *m, const orc_op *op, const geo_t *g, int ix, int iy, int iz,
+                             int d, int s, int mode, const long *idx, const double *ul_cell, double *out_cell,
+                             double *diag_cell)
+{
+  double vc[8][3];
+  cell_vertices(m, g, ix, iy, iz, vc);
+  robin_face_apply_vc(op, g, vc, d, s, 2 * d + s, mode, idx, ul_cell, out_cell, diag_cell);
+}
+
+/* adds the face matrices of a mapped cell's boundary faces to its element
+ * matrix A (columns by unit local vectors through robin_face_apply_vc) */
+static void add_face_matrices(const orc_mapped *m, const orc_op *op, const geo_t *g, long K, double vc[8][3],
+                              const long *idx, double *A)
+{
+  if (!m->face_ids) return;
+  const int n = g->n, nqt = n * n * n;
+  double e[MAXN3], col[MAXN3];
+  for (int f = 0; f < 6; ++f) {
+    const int id = m->face_ids[K * 6 + f];
+    if (id < 0) continue;
+    for (int u = 0; u < nqt; ++u) {
+      memset(e, 0, sizeof(double) * nqt);
+      memset(col, 0, sizeof(double) * nqt);
+      e[u] = 1.0;
+      robin_face_apply_vc(op, g, vc, f / 2, f % 2, id, ROB_TANGENT, idx, e, col, NULL);
+      for (int t = 0; t < nqt; ++t) A[t * nqt + u] += col[t];
+    }
+  }
 }
 
 static int cell_on_face(const geo_t *g, int ix, int iy, int iz, int d, int s)
@@ -1767,6 +1804,7 @@ void orcm_vmult(const orc_mapped *m, const orc_op *op, double *dst, const double
     long idx[MAXN3];
     mapped_cell(m, K, vc, idx, nqt);
     element_matrix_vc(op, &g, vc, idx, tau_vc(op, &g, vc, idx), A);
+    add_face_matrices(m, op, &g, K, vc, idx, A);
     for (int t = 0; t < nqt; ++t) {
       long cnt, own;
       double one, v = 0.0;
@@ -1806,6 +1844,7 @@ void orcm_diagonal(const orc_mapped *m, const orc_op *op, double *diag)
     long idx[MAXN3];
     mapped_cell(m, K, vc, idx, nqt);
     element_matrix_vc(op, &g, vc, idx, tau_vc(op, &g, vc, idx), A);
+    add_face_matrices(m, op, &g, K, vc, idx, A);
     /* distinct targets of the cell and their weights per local DoF */
     long tg[4 * MAXN3];
     int nt = 0;

@@ -177,6 +177,9 @@ typedef struct {
   const long *cons_ptr;
   const long *cons_idx;
   const double *cons_w;
+  /* boundary id of each cell's local face 2 d + s ([n_cells][6]; -1 interior,
+   * 0..5 the bit of robin_faces / rad_faces that selects it), or NULL */
+  const signed char *face_ids;
 } orc_mapped;
 
 void orcm_vmult(const orc_mapped *m, const orc_op *op, double *dst, const double *src);

@@ -58,7 +58,8 @@ _lp = C.POINTER(C.c_long)
 
 class _Mapped(C.Structure):
     _fields_ = [("degree", C.c_int), ("n_cells", C.c_long), ("n_dofs", C.c_long), ("cell_vertices", _dp),
-                ("cell_dofs", _lp), ("cons_ptr", _lp), ("cons_idx", _lp), ("cons_w", _dp)]
+                ("cell_dofs", _lp), ("cons_ptr", _lp), ("cons_idx", _lp), ("cons_w", _dp),
+                ("face_ids", C.POINTER(C.c_int8))]
 
 
 class _Prec(C.Structure):
@@ -488,9 +489,12 @@ def _cell_corners(vert, nc, ix, iy, iz):
 class MappedMesh:
     """Unstructured hexahedral mesh in the ingestion form (orc_mapped): each
     cell's 8 corners (x fastest), its n^3 global DoFs (lexicographic within the
-    cell), and homogeneous constraints {dof: [(master, weight), ...]}."""
+    cell), homogeneous constraints {dof: [(master, weight), ...]}, and optionally
+    the boundary id of each cell's local face 2 d + s (`face_ids`, shape
+    (n_cells, 6), -1 interior; id b is selected by bit b of robin_faces /
+    rad_faces)."""
 
-    def __init__(self, degree, cell_vertices, cell_dofs, n_dofs, constraints=None):
+    def __init__(self, degree, cell_vertices, cell_dofs, n_dofs, constraints=None, face_ids=None):
         self.degree = int(degree)
         n = degree + 1
         self.cell_vertices = np.ascontiguousarray(cell_vertices, np.float64).reshape(-1, 8, 3)
@@ -508,9 +512,11 @@ class MappedMesh:
         self.cons_ptr = ptr
         self.cons_idx = np.ascontiguousarray(idx if idx else [0], np.int64)
         self.cons_w = np.ascontiguousarray(w if w else [0.0], np.float64)
+        self.face_ids = None if face_ids is None else np.ascontiguousarray(face_ids, np.int8).reshape(-1, 6)
         self._c = _Mapped(self.degree, self.n_cells, self.n_dofs, _ptr(self.cell_vertices),
                           self.cell_dofs.ctypes.data_as(_lp), ptr.ctypes.data_as(_lp),
-                          self.cons_idx.ctypes.data_as(_lp), _ptr(self.cons_w))
+                          self.cons_idx.ctypes.data_as(_lp), _ptr(self.cons_w),
+                          None if self.face_ids is None else self.face_ids.ctypes.data_as(C.POINTER(C.c_int8)))
 
     def constrained_mask(self):
         m = np.zeros(self.n_dofs, np.uint8)
@@ -520,20 +526,23 @@ class MappedMesh:
 
 def mapped_from_mesh(mesh, perm=None, cell_order=None):
     """The structured 3D mesh `mesh` in the ingestion form; `perm[g]` renumbers
-    DoF g, `cell_order` lists the cells (lexicographic index) in the order given."""
+    DoF g, `cell_order` lists the cells (lexicographic index) in the order given;
+    the box faces carry boundary ids 2 d + s (as the lattice's robin_faces bits)."""
     p, nc = mesh.degree, mesh.nc
     n = p + 1
     NX, NY = mesh.shape[0], mesh.shape[1]
     cells = list(cell_order) if cell_order is not None else range(nc[0] * nc[1] * nc[2])
-    verts, dofs = [], []
+    verts, dofs, fids = [], [], []
     for c in cells:
         ix, iy, iz = c % nc[0], (c // nc[0]) % nc[1], c // (nc[0] * nc[1])
         verts.append(_cell_corners(mesh.vert, nc, ix, iy, iz))
+        ic = (ix, iy, iz)
+        fids.append([2 * d + s if ic[d] == (nc[d] - 1 if s else 0) else -1 for d in range(3) for s in range(2)])
         k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
         g = ((iz * p + k) * NY + (iy * p + j)) * NX + (ix * p + i)
         g = g.reshape(-1)
         dofs.append(g if perm is None else np.asarray(perm)[g])
-    return MappedMesh(p, np.array(verts), np.array(dofs), mesh.n_dofs)
+    return MappedMesh(p, np.array(verts), np.array(dofs), mesh.n_dofs, face_ids=np.array(fids, np.int8))
 
 
 def mapped_from_mesh2(m2):

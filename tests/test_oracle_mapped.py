@@ -86,3 +86,28 @@ def test_mapped_nodal_velocity_equals_structured():
     xp = np.empty_like(x)
     xp[perm] = x
     assert np.abs(O.mapped_vmult(mp, opp, xp)[perm] - a).max() <= 1e-13 * np.abs(a).max()
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_mapped_boundary_faces_equal_structured(p):
+    """Convective and radiative faces selected by the cells' boundary ids equal
+    the structured oracle's box faces on the same mesh, renumbered (apply and
+    the diagonal)."""
+    m = O.Mesh.box(3, p, [2, 3, 2], perturb=0.1, seed=8)
+    T = 300.0 + 50.0 * np.random.default_rng(1).uniform(size=m.n_dofs)
+    op = O.Operator(O.HEAT, 1e-2, rho_cp=2.0, k0=1.5, temperature=T, robin_alpha=25.0, robin_t_inf=300.0,
+                    robin_faces=(1 << 1) | (1 << 2), rad_emissivity=0.8, rad_t_inf=350.0,
+                    rad_faces=(1 << 1) | (1 << 5))
+    x = np.random.default_rng(p).uniform(-1, 1, m.n_dofs)
+    a = O.vmult(m, op, x)
+    R = np.random.default_rng(30 + p)
+    perm = R.permutation(m.n_dofs)
+    mp = O.mapped_from_mesh(m, perm=perm, cell_order=R.permutation(m.n_cells))
+    Tp = np.empty_like(T)
+    Tp[perm] = T
+    opp = op.with_temperature(Tp)
+    xp = np.empty_like(x)
+    xp[perm] = x
+    assert np.abs(O.mapped_vmult(mp, opp, xp)[perm] - a).max() <= 1e-13 * np.abs(a).max()
+    d = O.diagonal(m, op)
+    assert np.abs(O.mapped_diagonal(mp, opp)[perm] - d).max() <= 1e-13 * np.abs(d).max()
