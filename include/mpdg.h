@@ -198,9 +198,10 @@ mpdg_status mpdg_mesh_create_two_level(const mpdg_mesh_desc *coarse, const mpdg_
  * coloured greedily (no two cells of a colour share a DoF; at most 64 colours),
  * so the scatter is atomic-free and deterministic.  Operators on it: the heat
  * operator (k(T) and the phase laws only without constraints) and the
- * advection-diffusion operator (prescribed velocity), without boundary faces
- * or SUPG; vmult, the diagonal, create_rhs, the solvers and the integrated L2
- * norm. */
+ * advection-diffusion operator (prescribed velocity or a velocity vector,
+ * SUPG, inflow/outflow rows), convective and radiative faces selected by the
+ * cells' face_ids (not through constrained DoFs); vmult, the diagonal,
+ * create_rhs, the solvers and the integrated L2 norm. */
 typedef struct {
   int degree;                        /* 1..4 */
   int64_t n_cells, n_dofs;
@@ -212,6 +213,10 @@ typedef struct {
   const int64_t *constraint_offsets; /* n_constraints + 1 */
   const int64_t *constraint_masters;
   const double *constraint_weights;
+  /* host, n_cells x 6 or NULL: boundary id of each cell's local face 2 d + s
+   * (-1 interior; 0..5 selects the face by bit id of mpdg_op_desc.robin_faces
+   * and rad_faces, as the box faces of a lattice do) */
+  const int8_t *face_ids;
 } mpdg_mapped_mesh_desc;
 mpdg_status mpdg_mesh_create_mapped(const mpdg_mapped_mesh_desc *desc, mpdg_mesh **mesh);
 mpdg_status mpdg_mesh_destroy(mpdg_mesh *mesh);

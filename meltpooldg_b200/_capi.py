@@ -52,7 +52,8 @@ class MappedMeshDesc(C.Structure):
                 ("cell_vertices", C.POINTER(C.c_double)), ("cell_dofs", C.POINTER(C.c_int64)),
                 ("dirichlet_mask", C.POINTER(C.c_uint8)), ("n_constraints", C.c_int64),
                 ("constrained_dofs", C.POINTER(C.c_int64)), ("constraint_offsets", C.POINTER(C.c_int64)),
-                ("constraint_masters", C.POINTER(C.c_int64)), ("constraint_weights", C.POINTER(C.c_double))]
+                ("constraint_masters", C.POINTER(C.c_int64)), ("constraint_weights", C.POINTER(C.c_double)),
+                ("face_ids", C.POINTER(C.c_int8))]
 
 
 class OpDesc(C.Structure):

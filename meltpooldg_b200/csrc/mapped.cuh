@@ -352,6 +352,62 @@ void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d)
   size_t &B = m.device_bytes;
   m.d_cmap = upload(cmap, B);
   m.d_cell_first = upload(cfirst, B);
+  // boundary faces: greedy face colours (no two faces of a colour share a DoF)
+  if (d.face_ids) {
+    std::vector<uint64_t> fused(N, 0);
+    std::vector<std::vector<std::array<int, 3>>> by_colour;  // (slot, local face, id)
+    std::vector<long> slot_of(E);
+    {
+      std::vector<long> nxt(n_col);
+      for (int c = 0; c < n_col; ++c) nxt[c] = m.mcol[c].first;
+      for (long e = 0; e < E; ++e) slot_of[e] = nxt[colour_of[e]]++;
+    }
+    const int P = d.degree;
+    for (long e = 0; e < E; ++e)
+      for (int f = 0; f < 6; ++f) {
+        const int id = d.face_ids[e * 6 + f];
+        if (id < 0) continue;
+        if (id > 5) throw Error{MPDG_ERR_ARG, "face ids are -1 or 0..5"};
+        const int fd = f >> 1, fs = f & 1, t0 = (fd == 0) ? 1 : 0, t1 = (fd == 2) ? 1 : 2;
+        std::vector<long> fg;
+        bool touches_cons = false;
+        for (int b = 0; b < n; ++b)
+          for (int a = 0; a < n; ++a) {
+            int loc[3];
+            loc[fd] = fs ? P : 0;
+            loc[t0] = a;
+            loc[t1] = b;
+            const long g = d.cell_dofs[e * n3 + (loc[2] * n + loc[1]) * n + loc[0]];
+            fg.push_back(g);
+            touches_cons = touches_cons || cons_of[g] >= 0;
+          }
+        uint64_t forbidden = 0;
+        for (long g : fg) forbidden |= fused[g];
+        if (~forbidden == 0) throw Error{MPDG_ERR_UNSUPPORTED, "mapped mesh needs more than 64 face colours"};
+        int c = 0;
+        while ((forbidden >> c) & 1u) ++c;
+        for (long g : fg) fused[g] |= (uint64_t)1 << c;
+        if ((int)by_colour.size() <= c) by_colour.resize(c + 1);
+        by_colour[c].push_back({(int)slot_of[e], f, id});
+        if (touches_cons) m.mface_cons_ids |= 1 << id;
+      }
+    std::vector<int> fcell;
+    std::vector<int8_t> ff, fid;
+    m.mface_first.assign(1, 0);
+    for (auto &lst : by_colour) {
+      for (auto &x : lst) {
+        fcell.push_back(x[0]);
+        ff.push_back((int8_t)x[1]);
+        fid.push_back((int8_t)x[2]);
+      }
+      m.mface_first.push_back((long)fcell.size());
+    }
+    if (!fcell.empty()) {
+      m.d_mface_cell = upload(fcell, B);
+      m.d_mface_f = upload(ff, B);
+      m.d_mface_id = upload(fid, B);
+    }
+  }
   m.all_dofs_touched = std::all_of(used.begin(), used.end(), [](uint64_t u) { return u != 0; });
   m.d_cellvert = upload(cvert, B);
   m.d_cell_flags = upload(flags, B);
@@ -474,6 +530,7 @@ void launch_mapped_apply(Op &op, Real *dst, const Real *src)
   } else {
     dispatch_degree<Real, MODE_LINEAR, false>(op, k);
   }
+  launch_robin<Real>(op, dst, in, ROBIN_APPLY);  // boundary faces selected by the cells' ids
   mapped_condense<Real>(op, dst);
 }
 
@@ -626,6 +683,7 @@ void launch_mapped_diagonal(Op &op, double *diag)
       default: throw Error{MPDG_ERR_UNSUPPORTED, "degree must be 1..4"};
     }
   }
+  launch_robin<double>(op, diag, nullptr, ROBIN_DIAGONAL);
   const uint8_t *tm = op.use_dirichlet ? m.d_tmask_dir : m.d_tmask_hang;
   set_masked_kernel<<<grid_for(m.N, 256), 256, 0, op.stream>>>(diag, m.N, tm, 1.0);
   MPDG_LAUNCHED();

@@ -124,6 +124,12 @@ struct Mesh {
   // touches first in colour order (it stores them; later colours add)
   uint32_t *d_cell_first = nullptr;
   bool all_dofs_touched = false;       // mapped meshes: every DoF lies in some cell
+  // mapped meshes: cells' local faces with a boundary id, grouped by face
+  // colour (faces of a colour share no DoF), colour c at [mface_first[c], [c+1])
+  int *d_mface_cell = nullptr;
+  int8_t *d_mface_f = nullptr, *d_mface_id = nullptr;
+  std::vector<long> mface_first;
+  int mface_cons_ids = 0;              // ids whose faces touch a constrained DoF
   bool has_dirichlet = false;
   size_t device_bytes = 0;
   bool metric32_ready = false;

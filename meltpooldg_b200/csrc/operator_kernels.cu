@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -2316,35 +2317,17 @@ void ensure_coef(Op &op, bool want32)
 // parity colours, so the scatter adds without atomics.
 enum { ROBIN_APPLY = 0, ROBIN_RESIDUAL = 1, ROBIN_DIAGONAL = 2 };
 
+// the terms of one boundary face (local face (d, s) of the cell with corners
+// V) for the warp that owns it: lane (a, b) < n^2 (on) holds face DoF g
 template <int P, typename Real>
-__global__ void __launch_bounds__(128) robin_kernel(const double *vert, int nc0, int nc1, int nc2, int d, int s,
-                                                    int colour, long NX, long NY, int conv, double alpha,
-                                                    double t_inf, int rad, double es, double t_rad, int mode,
-                                                    const Real *src, const Real *Tf, Real *dst,
-                                                    const uint8_t *rmask, const uint8_t *wmask)
+__device__ __forceinline__ void robin_face(const double (&V)[8][3], int d, int s, long g, bool on, int a, int b,
+                                           Real *t, int conv, double alpha, double t_inf, int rad, double es,
+                                           double t_rad, int mode, const Real *src, const Real *Tf, Real *dst,
+                                           const uint8_t *rmask, const uint8_t *wmask)
 {
-  constexpr int n = P + 1, n2 = n * n;
-  __shared__ Real tile[4][n2];
+  constexpr int n = P + 1;
   const Tables<Real> &T = tab<Real>(P);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nc[3] = {nc0, nc1, nc2};
   const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
-  const int pa = colour & 1, pb = (colour >> 1) & 1;
-  const int ca = (nc[t0] - pa + 1) / 2, cb = (nc[t1] - pb + 1) / 2;
-  const long f = (long)blockIdx.x * 4 + warp;
-  if (f >= (long)ca * cb) return;  // warp-uniform
-  const int fa = 2 * (int)(f % ca) + pa, fb = 2 * (int)(f / ca) + pb;
-  int cell[3];
-  cell[d] = s ? nc[d] - 1 : 0;
-  cell[t0] = fa;
-  cell[t1] = fb;
-  const bool on = lane < n2;
-  const int a = on ? lane % n : 0, b = on ? lane / n : 0;
-  int loc[3];
-  loc[d] = s ? P : 0;
-  loc[t0] = a;
-  loc[t1] = b;
-  const long g = ((long)(cell[2] * P + loc[2]) * NY + (cell[1] * P + loc[1])) * NX + (cell[0] * P + loc[0]);
   // surface element at the lane's face quadrature point
   double xi[3];
   xi[d] = s ? 1.0 : 0.0;
@@ -2353,7 +2336,6 @@ __global__ void __launch_bounds__(128) robin_kernel(const double *vert, int nc0,
   double Ja[3] = {0, 0, 0}, Jb[3] = {0, 0, 0};
   for (int v = 0; v < 8; ++v) {
     const int bv[3] = {v & 1, (v >> 1) & 1, (v >> 2) & 1};
-    const long vid = ((long)(cell[2] + bv[2]) * (nc1 + 1) + (cell[1] + bv[1])) * (nc0 + 1) + (cell[0] + bv[0]);
     double fv[3], dfv[3];
     for (int e = 0; e < 3; ++e) {
       fv[e] = bv[e] ? xi[e] : 1.0 - xi[e];
@@ -2365,14 +2347,13 @@ __global__ void __launch_bounds__(128) robin_kernel(const double *vert, int nc0,
     for (int e = 0; e < 3; ++e)
       if (e != t1) db *= fv[e];
     for (int e = 0; e < 3; ++e) {
-      Ja[e] += vert[vid * 3 + e] * da;
-      Jb[e] += vert[vid * 3 + e] * db;
+      Ja[e] += V[v][e] * da;
+      Jb[e] += V[v][e] * db;
     }
   }
   const double cr[3] = {Ja[1] * Jb[2] - Ja[2] * Jb[1], Ja[2] * Jb[0] - Ja[0] * Jb[2],
                         Ja[0] * Jb[1] - Ja[1] * Jb[0]};
   const double jxw = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) * (double)T.w[a] * (double)T.w[b];
-  Real *t = tile[warp];
   // face interpolation: lane (a, b) holds a nodal value and receives the value
   // at face quadrature point (a, b), along t0 then t1
   const auto interp = [&](Real v) -> Real {
@@ -2429,6 +2410,81 @@ __global__ void __launch_bounds__(128) robin_kernel(const double *vert, int nc0,
   if (on && !(wmask && wmask[g])) dst[g] += out;
 }
 
+template <int P, typename Real>
+__global__ void __launch_bounds__(128) robin_kernel(const double *vert, int nc0, int nc1, int nc2, int d, int s,
+                                                    int colour, long NX, long NY, int conv, double alpha,
+                                                    double t_inf, int rad, double es, double t_rad, int mode,
+                                                    const Real *src, const Real *Tf, Real *dst,
+                                                    const uint8_t *rmask, const uint8_t *wmask)
+{
+  constexpr int n = P + 1, n2 = n * n;
+  __shared__ Real tile[4][n2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nc[3] = {nc0, nc1, nc2};
+  const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
+  const int pa = colour & 1, pb = (colour >> 1) & 1;
+  const int ca = (nc[t0] - pa + 1) / 2, cb = (nc[t1] - pb + 1) / 2;
+  const long f = (long)blockIdx.x * 4 + warp;
+  if (f >= (long)ca * cb) return;  // warp-uniform
+  const int fa = 2 * (int)(f % ca) + pa, fb = 2 * (int)(f / ca) + pb;
+  int cell[3];
+  cell[d] = s ? nc[d] - 1 : 0;
+  cell[t0] = fa;
+  cell[t1] = fb;
+  const bool on = lane < n2;
+  const int a = on ? lane % n : 0, b = on ? lane / n : 0;
+  int loc[3];
+  loc[d] = s ? P : 0;
+  loc[t0] = a;
+  loc[t1] = b;
+  const long g = ((long)(cell[2] * P + loc[2]) * NY + (cell[1] * P + loc[1])) * NX + (cell[0] * P + loc[0]);
+  double V[8][3];
+  for (int v = 0; v < 8; ++v) {
+    const long vid = ((long)(cell[2] + ((v >> 2) & 1)) * (nc1 + 1) + (cell[1] + ((v >> 1) & 1))) * (nc0 + 1) +
+                     (cell[0] + (v & 1));
+    for (int e = 0; e < 3; ++e) V[v][e] = vert[vid * 3 + e];
+  }
+  robin_face<P, Real>(V, d, s, g, on, a, b, tile[warp], conv, alpha, t_inf, rad, es, t_rad, mode, src, Tf, dst,
+                      rmask, wmask);
+}
+
+// boundary faces of a mapped mesh (cells' local faces with a boundary id
+// whose bit conv_bits / rad_bits selects), one warp per face of one face
+// colour: the faces of a colour share no DoF, so the scatter adds without atomics
+template <int P, typename Real>
+__global__ void __launch_bounds__(128) mapped_face_kernel(const int *fcell, const int8_t *fface, const int8_t *fid,
+                                                          long first, long count, const int *cmap,
+                                                          const double *cellvert, int conv_bits, double alpha,
+                                                          double t_inf, int rad_bits, double es, double t_rad,
+                                                          int mode, const Real *src, const Real *Tf, Real *dst,
+                                                          const uint8_t *rmask, const uint8_t *wmask)
+{
+  constexpr int n = P + 1, n2 = n * n, n3 = n2 * n;
+  __shared__ Real tile[4][n2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long f = (long)blockIdx.x * 4 + warp;
+  if (f >= count) return;  // warp-uniform
+  const long e = first + f;
+  const long slot = fcell[e];
+  const int face = fface[e], id = fid[e];
+  const int conv = (conv_bits >> id) & 1, rad = (rad_bits >> id) & 1;
+  if (!conv && !rad) return;  // warp-uniform
+  const int d = face >> 1, s = face & 1;
+  const int t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
+  const bool on = lane < n2;
+  const int a = on ? lane % n : 0, b = on ? lane / n : 0;
+  int loc[3];
+  loc[d] = s ? P : 0;
+  loc[t0] = a;
+  loc[t1] = b;
+  const long g = cmap[slot * n3 + (loc[2] * n + loc[1]) * n + loc[0]];
+  double V[8][3];
+  for (int v = 0; v < 8; ++v)
+    for (int c = 0; c < 3; ++c) V[v][c] = cellvert[(slot * 8 + v) * 3 + c];
+  robin_face<P, Real>(V, d, s, g, on, a, b, tile[warp], conv, alpha, t_inf, rad, es, t_rad, mode, src, Tf, dst,
+                      rmask, wmask);
+}
+
 template <typename Real>
 void launch_robin(Op &op, Real *dst, const Real *src, int mode)
 {
@@ -2446,6 +2502,29 @@ void launch_robin(Op &op, Real *dst, const Real *src, int mode)
   const bool mask = op.use_dirichlet && m.has_dirichlet;
   const uint8_t *rmask = (mode == ROBIN_APPLY && mask) ? m.d_dmask : nullptr;
   const uint8_t *wmask = mask ? m.d_dmask : nullptr;
+  if (m.mapped) {
+    // the cells' faces with a selected boundary id, colour by colour
+    const int conv_bits = any_conv ? D.robin_faces : 0, rad_bits = any_rad ? D.rad_faces : 0;
+    for (size_t c = 0; c + 1 < m.mface_first.size(); ++c) {
+      const long first = m.mface_first[c], count = m.mface_first[c + 1] - first;
+      if (count == 0) continue;
+      const unsigned grid = (unsigned)((count + 3) / 4);
+#define MPDG_MFACE(PP)                                                                                            \
+  mapped_face_kernel<PP, Real><<<grid, 128, 0, op.stream>>>(m.d_mface_cell, m.d_mface_f, m.d_mface_id, first, count, \
+                                                            m.d_cmap, m.d_cellvert, conv_bits, D.robin_alpha,        \
+                                                            D.robin_t_inf, rad_bits, es, D.rad_t_inf, mode, src, Tf, \
+                                                            dst, rmask, wmask)
+      switch (m.degree) {
+        case 1: MPDG_MFACE(1); break;
+        case 2: MPDG_MFACE(2); break;
+        case 3: MPDG_MFACE(3); break;
+        default: MPDG_MFACE(4); break;
+      }
+#undef MPDG_MFACE
+      MPDG_LAUNCHED();
+    }
+    return;
+  }
   for (int d = 0; d < 3; ++d)
     for (int s = 0; s < 2; ++s) {
       const int bit = 1 << (2 * d + s);

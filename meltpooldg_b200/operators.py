@@ -129,9 +129,12 @@ class MappedMesh(Mesh):
     (degree+1)^3 global DoFs (lexicographic within the cell), a Dirichlet mask,
     and homogeneous constraints {dof: [(master, weight), ...]} (hanging nodes;
     masters unconstrained).  Vectors use the caller's DoF numbering; the
-    constrained DoFs stay 0 in results, like Dirichlet DoFs."""
+    constrained DoFs stay 0 in results, like Dirichlet DoFs.  `face_ids`
+    (n_cells x 6, -1 interior) gives each cell's local face 2 d + s a boundary
+    id 0..5, which the heat operator's robin_faces / rad_faces bits select."""
 
-    def __init__(self, cell_vertices, cell_dofs, n_dofs, degree, dirichlet_mask=None, constraints=None):
+    def __init__(self, cell_vertices, cell_dofs, n_dofs, degree, dirichlet_mask=None, constraints=None,
+                 face_ids=None):
         L = A.lib()
         self.degree = int(degree)
         n3 = (self.degree + 1) ** 3
@@ -147,13 +150,15 @@ class MappedMesh(Mesh):
         self._coff = off
         self._cmast = np.ascontiguousarray([m for _, ent in cons for m, _ in ent] or [0], np.int64)
         self._cw = np.ascontiguousarray([w for _, ent in cons for _, w in ent] or [0.0], np.float64)
+        self.face_ids = None if face_ids is None else np.ascontiguousarray(face_ids, np.int8).reshape(-1, 6)
         i64 = C.POINTER(C.c_int64)
         d = A.MappedMeshDesc(self.degree, self.cell_dofs.shape[0], self.n_dofs,
                              self.cell_vertices.ctypes.data_as(C.POINTER(C.c_double)),
                              self.cell_dofs.ctypes.data_as(i64),
                              None if self.mask is None else self.mask.ctypes.data_as(C.POINTER(C.c_uint8)),
                              len(cons), self._cdofs.ctypes.data_as(i64), self._coff.ctypes.data_as(i64),
-                             self._cmast.ctypes.data_as(i64), self._cw.ctypes.data_as(C.POINTER(C.c_double)))
+                             self._cmast.ctypes.data_as(i64), self._cw.ctypes.data_as(C.POINTER(C.c_double)),
+                             None if self.face_ids is None else self.face_ids.ctypes.data_as(C.POINTER(C.c_int8)))
         h = C.c_void_p()
         A.check(L.mpdg_mesh_create_mapped(C.byref(d), C.byref(h)), "mpdg_mesh_create_mapped")
         self._h = h

@@ -409,3 +409,90 @@ def test_mapped_supg_with_hanging_constraints(cuda, p):
     d = torch.empty_like(y)
     op.compute_diagonal(d)
     assert relerr(d.cpu().numpy(), O.mapped_diagonal(mm, oop)) < TOL64
+
+
+# local corners (x fastest) of face 2 d + s of a hexahedron
+_FACE_CORNERS = {2 * d + s: [v for v in range(8) if ((v >> d) & 1) == s] for d in range(3) for s in range(2)}
+
+
+def box_face_ids(cell_vertices, lo=(-1.0, -1.0, -1.0), hi=(1.0, 1.0, 1.0)):
+    """Boundary id 2 d + s of every cell face that lies on the box face (d, s)."""
+    cv = np.asarray(cell_vertices).reshape(-1, 8, 3)
+    ids = -np.ones((cv.shape[0], 6), np.int8)
+    for f, corners in _FACE_CORNERS.items():
+        d, s = f // 2, f % 2
+        plane = hi[d] if s else lo[d]
+        on = np.all(np.abs(cv[:, corners, d] - plane) < 1e-12, axis=1)
+        ids[on, f] = f
+    return ids
+
+
+def _face_ops(gm, T, mask):
+    import meltpooldg_b200 as M
+    kw = dict(robin_alpha=25.0, robin_t_inf=300.0, rad_emissivity=0.8, rad_t_inf=350.0)
+    op = M.HeatDiffuseOperator(gm, 1e-2, rho_cp=2.0, k0=1.5, precisions=("fp64", "fp32"),
+                               robin_faces=[(0, 1), (1, 0)], rad_faces=[(0, 1), (2, 1)], **kw)
+    oop = O.Operator(O.HEAT, 1e-2, rho_cp=2.0, k0=1.5, temperature=T, dirichlet=mask,
+                     robin_faces=(1 << 1) | (1 << 2), rad_faces=(1 << 1) | (1 << 5), **kw)
+    return op, oop
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_mapped_boundary_faces(cuda, p):
+    """Convective and radiative faces selected by the cells' boundary ids on a
+    renumbered perturbed mesh: vmult (FP64, FP32) and the diagonal against the
+    oracle's mapped operator, create_rhs as the structured device path's."""
+    import torch
+    import meltpooldg_b200 as M
+    nc = (3, 2, 3)
+    mask_s = M.boundary_mask(nc, p, faces=[(2, 0)])
+    gs, om = meshes(nc, p, 0.1, seed=40 + p, mask=mask_s, lo=(-1, -1, -1), hi=(1, 1, 1))
+    R = rng(90 + p)
+    perm = R.permutation(om.n_dofs)
+    mm = O.mapped_from_mesh(om, perm=perm, cell_order=R.permutation(om.n_cells))
+    mask = np.empty_like(mask_s)
+    mask[perm] = mask_s
+    gm = M.MappedMesh(mm.cell_vertices, mm.cell_dofs, mm.n_dofs, p, dirichlet_mask=mask, face_ids=mm.face_ids)
+    T = 300.0 + 50.0 * R.uniform(size=om.n_dofs)
+    Tp = np.empty_like(T)
+    Tp[perm] = T
+    op, oop = _face_ops(gm, Tp, mask)
+    Td = dev(Tp)
+    op.set_temperature(Td)
+    x = R.uniform(-1, 1, om.n_dofs)
+    ref = O.mapped_vmult(mm, oop, x)
+    y = torch.empty(om.n_dofs, dtype=torch.float64, device="cuda")
+    op.vmult(y, dev(x))
+    assert relerr(y.cpu().numpy(), ref) < TOL64
+    y32 = torch.empty(om.n_dofs, dtype=torch.float32, device="cuda")
+    op.vmult(y32, dev(x, torch.float32))
+    assert relerr(y32.double().cpu().numpy(), ref) < TOL32
+    d = torch.empty_like(y)
+    op.compute_diagonal(d)
+    assert relerr(d.cpu().numpy(), O.mapped_diagonal(mm, oop)) < TOL64
+    # the Newton residual with its face terms: as the structured path's
+    ops, _ = _face_ops(gs, T, mask_s)
+    Ts = dev(T)
+    ops.set_temperature(Ts)
+    t_old = R.uniform(290.0, 310.0, om.n_dofs)
+    rs = torch.zeros(om.n_dofs, dtype=torch.float64, device="cuda")
+    ops.create_rhs(rs, dev(t_old))
+    t_oldp = np.empty_like(t_old)
+    t_oldp[perm] = t_old
+    rm = torch.zeros_like(rs)
+    op.create_rhs(rm, dev(t_oldp))
+    assert relerr(rm.cpu().numpy()[perm], rs.cpu().numpy()) < TOL64
+
+
+def test_mapped_boundary_faces_through_hanging_nodes_are_refused(cuda):
+    import meltpooldg_b200 as M
+    from meltpooldg_b200.refine import refine_box
+    V = O.box_vertices(3, (3, 3, 3), [-1.0] * 3, [1.0] * 3, 0.0, 1)
+    r = refine_box((3, 3, 3), 2, [4], vertices=V)  # cell 4 touches the face z = -1
+    ids = box_face_ids(r["cell_vertices"])
+    gm = M.MappedMesh(r["cell_vertices"], r["cell_dofs"], r["n_dofs"], 2, constraints=r["constraints"],
+                      face_ids=ids)
+    with pytest.raises(Exception, match="constrained"):
+        M.HeatDiffuseOperator(gm, 1e-2, robin_alpha=10.0, robin_faces=[(0, 0), (0, 1), (1, 0), (1, 1), (2, 0)])
+    # faces away from the hanging nodes are served
+    M.HeatDiffuseOperator(gm, 1e-2, robin_alpha=10.0, robin_faces=[(2, 1)])
