@@ -255,10 +255,6 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
       if (desc->kind == MPDG_OP_HEAT && (sel & mm.mface_cons_ids))
         throw Error{MPDG_ERR_UNSUPPORTED, "boundary faces through constrained (hanging) DoFs of a mapped mesh"};
     }
-    if (mm.mapped && mm.n_cons > 0 &&
-        (desc->k_alpha != 0.0 || desc->full_tangent || desc->material != MPDG_MAT_LINEAR))
-      throw Error{MPDG_ERR_UNSUPPORTED,
-                  "mapped meshes with constraints take constant coefficients (no k(T), phase law or full tangent)"};
     auto *h = new mpdg_op();
     Op &o = h->o;
     o.mesh = &mm;

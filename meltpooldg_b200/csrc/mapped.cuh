@@ -97,6 +97,96 @@ __global__ void elem_matrix_kernel(const KP<double> p, const long *ccells, doubl
   }
 }
 
+// element matrices of the listed cells of a heat operator whose coefficients
+// follow the fields (k(T), the phase laws, the full Newton tangent;
+// heat_diffuse_operator.cpp:1029-1078): the fields (read plain through the
+// map, as read_dof_values_plain does) are interpolated to the Gauss points
+// and the law evaluated there once per cell, then
+// A(t,u) = sum_q phi_t [c_m JxW phi_u + c_v b.grad phi_u
+//                       + (d c_m/dT (T - T_old) JxW + d c_v/dT b.grad T) phi_u]
+//          + grad phi_t . [k G grad phi_u + dk/dT phi_u G grad T]
+// (the bracketed Newton terms with the full tangent; reference gradients,
+// G = JxW J^-1 J^-T, b = JxW J^-1 u)
+template <int P>
+__global__ void elem_matrix_field_kernel(const KP<double> p, const long *cells, double *A)
+{
+  constexpr int n = P + 1, n2 = n * n, n3 = n2 * n;
+  const Tables<double> &T = tab<double>(P);
+  __shared__ double sT[n3], sg[3][n3], sc[6][n3];  // T, reference grad T, (cm, cv, k, dcm, dcv, dk)
+  const long cell = cells[blockIdx.x];
+  const int *cmap = p.cmap + cell * n3;
+  for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+    const int qc[3] = {q % n, (q / n) % n, q / n2};
+    double tq = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, oq = 0.0, hq = 0.0;
+    for (int t = 0; t < n3; ++t) {
+      const int tc[3] = {t % n, (t / n) % n, t / n2};
+      const double s0 = T.S[qc[0] * n + tc[0]], s1 = T.S[qc[1] * n + tc[1]], s2 = T.S[qc[2] * n + tc[2]];
+      const double d0 = T.D[qc[0] * n + tc[0]], d1 = T.D[qc[1] * n + tc[1]], d2 = T.D[qc[2] * n + tc[2]];
+      const long g = cmap[t];
+      const double Tv = p.T[g];
+      tq += s0 * s1 * s2 * Tv;
+      g0 += d0 * s1 * s2 * Tv;
+      g1 += s0 * d1 * s2 * Tv;
+      g2 += s0 * s1 * d2 * Tv;
+      if (p.Told) oq += s0 * s1 * s2 * p.Told[g];
+      if (p.Hs) hq += s0 * s1 * s2 * p.Hs[g];
+    }
+    double cm, cv, kq, dcm, dcv, dk;
+    law_eval<double>(p, tq, hq, cm, cv, kq, dcm, dcv, dk);
+    sT[q] = tq - oq;  // T - T_old (the Newton term's increment)
+    sg[0][q] = g0;
+    sg[1][q] = g1;
+    sg[2][q] = g2;
+    sc[0][q] = cm;
+    sc[1][q] = cv;
+    sc[2][q] = kq;
+    sc[3][q] = dcm;
+    sc[4][q] = dcv;
+    sc[5][q] = dk;
+  }
+  __syncthreads();
+  const double *m = p.metric + cell * metric_stride(n);
+  const double *vb = p.velb ? p.velb + cell * velb_stride(n) : nullptr;
+  const bool newton = p.full_tangent != 0, incr = p.Told != nullptr;
+  double *Ac = A + (long)blockIdx.x * n3 * n3;
+  for (int e = threadIdx.x; e < n3 * n3; e += blockDim.x) {
+    const int t = e / n3, u = e % n3;
+    const int tc[3] = {t % n, (t / n) % n, t / n2}, uc[3] = {u % n, (u / n) % n, u / n2};
+    double s = 0.0;
+    for (int q = 0; q < n3; ++q) {
+      const int qc[3] = {q % n, (q / n) % n, q / n2};
+      double st[3], dt[3], su[3], du[3];
+      for (int d = 0; d < 3; ++d) {
+        st[d] = T.S[qc[d] * n + tc[d]];
+        dt[d] = T.D[qc[d] * n + tc[d]];
+        su[d] = T.S[qc[d] * n + uc[d]];
+        du[d] = T.D[qc[d] * n + uc[d]];
+      }
+      const double pt = st[0] * st[1] * st[2], pu = su[0] * su[1] * su[2];
+      const double gt[3] = {dt[0] * st[1] * st[2], st[0] * dt[1] * st[2], st[0] * st[1] * dt[2]};
+      const double gu[3] = {du[0] * su[1] * su[2], su[0] * du[1] * su[2], su[0] * su[1] * du[2]};
+      const double JxW = m[q], G00 = m[n3 + q], G01 = m[2 * n3 + q], G02 = m[3 * n3 + q],
+                   G11 = m[4 * n3 + q], G12 = m[5 * n3 + q], G22 = m[6 * n3 + q];
+      const double b0 = vb ? vb[q] : 0.0, b1 = vb ? vb[n3 + q] : 0.0, b2 = vb ? vb[2 * n3 + q] : 0.0;
+      double fu0 = G00 * gu[0] + G01 * gu[1] + G02 * gu[2];
+      double fu1 = G01 * gu[0] + G11 * gu[1] + G12 * gu[2];
+      double fu2 = G02 * gu[0] + G12 * gu[1] + G22 * gu[2];
+      double v = sc[0][q] * JxW * pu + sc[1][q] * (b0 * gu[0] + b1 * gu[1] + b2 * gu[2]);
+      double f0 = sc[2][q] * fu0, f1 = sc[2][q] * fu1, f2 = sc[2][q] * fu2;
+      if (newton) {
+        const double du_ = sc[5][q] * pu;
+        f0 += du_ * (G00 * sg[0][q] + G01 * sg[1][q] + G02 * sg[2][q]);
+        f1 += du_ * (G01 * sg[0][q] + G11 * sg[1][q] + G12 * sg[2][q]);
+        f2 += du_ * (G02 * sg[0][q] + G12 * sg[1][q] + G22 * sg[2][q]);
+        if (incr)
+          v += (sc[3][q] * sT[q] * JxW + sc[4][q] * (b0 * sg[0][q] + b1 * sg[1][q] + b2 * sg[2][q])) * pu;
+      }
+      s += pt * v + gt[0] * f0 + gt[1] * f1 + gt[2] * f2;
+    }
+    Ac[e] = s;
+  }
+}
+
 // element matrices of the listed cells with the SUPG terms of the
 // advection-diffusion tangent (advection_diffusion_operator.cpp:471-493): the
 // matrix above plus tau_K (b.grad phi_t) (c_mass phi_u + c_vel b.grad phi_u / JxW
@@ -601,6 +691,7 @@ void mapped_element_diagonal(Op &op, double *diag, const std::vector<long> &cell
     d_tptr = upload(tptr, scratch);
     KP<double> k = base_params<double>(op);
     if (supg) elem_matrix_supg_kernel<P><<<(unsigned)ncc, 256, 0, op.stream>>>(k, d_cells, A);
+    else if (uses_kT(op)) elem_matrix_field_kernel<P><<<(unsigned)ncc, 256, 0, op.stream>>>(k, d_cells, A);
     else elem_matrix_kernel<P><<<(unsigned)ncc, 256, 0, op.stream>>>(k, d_cells, A);
     MPDG_LAUNCHED();
     const long nt = (long)tasks.size();

@@ -496,3 +496,50 @@ def test_mapped_boundary_faces_through_hanging_nodes_are_refused(cuda):
         M.HeatDiffuseOperator(gm, 1e-2, robin_alpha=10.0, robin_faces=[(0, 0), (0, 1), (1, 0), (1, 1), (2, 0)])
     # faces away from the hanging nodes are served
     M.HeatDiffuseOperator(gm, 1e-2, robin_alpha=10.0, robin_faces=[(2, 1)])
+
+
+@pytest.mark.parametrize("p", [1, 2])
+@pytest.mark.parametrize("law", ["kT_full", "liquid_solid_latent"])
+def test_mapped_hanging_constraints_with_field_coefficients(cuda, p, law):
+    """k(T) with its full tangent, and the liquid/solid law with latent heat,
+    on a locally refined mesh (hanging constraints, perturbed vertices): vmult
+    (FP64, FP32) and the diagonal (element matrices with the fields at the
+    Gauss points for the constrained cells) against the oracle's mapped operator."""
+    import torch
+    import meltpooldg_b200 as M
+    from meltpooldg_b200.refine import refine_box
+    V = O.box_vertices(3, (3, 3, 3), [-1.0] * 3, [1.0] * 3, 0.1, 23)
+    r = refine_box((3, 3, 3), p, [13, 22], vertices=V)
+    mm = O.MappedMesh(p, r["cell_vertices"], r["cell_dofs"], r["n_dofs"], r["constraints"])
+    mask = r["boundary"]
+    gm = device_mesh(mm, mask)
+    N = mm.n_dofs
+    R = rng(110 + p)
+    T = 1970.0 + 4.0 * R.uniform(-1, 1, N)
+    T_old = T + R.uniform(-0.5, 0.5, N)
+    if law == "kT_full":
+        op = M.HeatDiffuseOperator(gm, 1e-2, rho_cp=2.0, k0=1.5, k_alpha=1e-3, full_tangent=True,
+                                   velocity=(0.3, -0.2, 0.1), precisions=("fp64", "fp32"))
+        oop = O.Operator(O.HEAT, 1e-2, rho_cp=2.0, k0=1.5, k_alpha=1e-3, full_tangent=True, temperature=T,
+                         dirichlet=mask, vel_kind=O.VEL_CONST, vel_param=(0.3, -0.2, 0.1))
+    else:
+        mat = dict(rho=(1.0, 7850.0, 7000.0), cp=(1.0, 460.0, 700.0), k=(1.0, 55.0, 17.0), solidus=1966.0,
+                   liquidus=1974.0, latent_heat=2.7e5)
+        op = M.HeatDiffuseOperator(gm, 1e-2, material=dict(mat, kind="liquid_solid"), precisions=("fp64", "fp32"))
+        oop = O.Operator(O.HEAT, 1e-2, material=dict(mat, kind=O.MAT_LIQUID_SOLID), temperature=T,
+                         temperature_old=T_old, dirichlet=mask)
+    Td, Od = dev(T), dev(T_old)
+    op.set_temperature(Td)
+    if law != "kT_full":
+        op.set_temperature_old(Od)
+    x = R.uniform(-1, 1, N)
+    ref = O.mapped_vmult(mm, oop, x)
+    y = torch.empty(N, dtype=torch.float64, device="cuda")
+    op.vmult(y, dev(x))
+    assert relerr(y.cpu().numpy(), ref) < TOL64
+    y32 = torch.empty(N, dtype=torch.float32, device="cuda")
+    op.vmult(y32, dev(x, torch.float32))
+    assert relerr(y32.double().cpu().numpy(), ref) < TOL32
+    d = torch.empty_like(y)
+    op.compute_diagonal(d)
+    assert relerr(d.cpu().numpy(), O.mapped_diagonal(mm, oop)) < TOL64

@@ -111,3 +111,56 @@ def test_mapped_boundary_faces_equal_structured(p):
     assert np.abs(O.mapped_vmult(mp, opp, xp)[perm] - a).max() <= 1e-13 * np.abs(a).max()
     d = O.diagonal(m, op)
     assert np.abs(O.mapped_diagonal(mp, opp)[perm] - d).max() <= 1e-13 * np.abs(d).max()
+
+
+@pytest.mark.parametrize("p", [1, 2])
+@pytest.mark.parametrize("law", ["kT_full", "liquid_solid"])
+def test_mapped_hanging_constraints_with_field_coefficients(p, law):
+    """k(T) with its full tangent, and the liquid/solid law with latent heat,
+    through the hanging-node constraints of a mapped mesh: the operator is
+    C^T A C with A the same cells without constraints (the fields read plain),
+    and its diagonal is (C e_g)^T A (C e_g)."""
+    m2 = O.Mesh2(p, (2, 2, 2), 2, perturb=0.1, seed=5)
+    x2 = m2.dof_coordinates()
+    R = np.random.default_rng(9 + p)
+    N = m2.n_dofs
+    T = 1970.0 + 4.0 * np.sin(3.0 * x2[:, 0]) * np.cos(2.0 * x2[:, 1]) + R.uniform(-0.3, 0.3, N)
+    T_old = T + R.uniform(-0.5, 0.5, N)
+    if law == "kT_full":
+        op = O.Operator(O.HEAT, 1e-2, rho_cp=2.0, k0=1.5, k_alpha=1e-3, full_tangent=True, temperature=T,
+                        vel_kind=O.VEL_CONST, vel_param=(0.3, -0.2, 0.1))
+    else:
+        mat = dict(kind=O.MAT_LIQUID_SOLID, rho=(1.0, 7850.0, 7000.0), cp=(1.0, 460.0, 700.0),
+                   k=(1.0, 55.0, 17.0), solidus=1966.0, liquidus=1974.0, latent_heat=2.7e5)
+        op = O.Operator(O.HEAT, 1e-2, material=mat, temperature=T, temperature_old=T_old)
+    mm = O.mapped_from_mesh2(m2)
+    free = O.MappedMesh(p, mm.cell_vertices, mm.cell_dofs, N)
+    cons = mm.constraints
+
+    def C(x):  # constrained entries from their masters
+        y = x.copy()
+        for c, ent in cons.items():
+            y[c] = sum(w * x[mst] for mst, w in ent)
+        return y
+
+    def Ct(y):  # transpose: constrained rows to their masters, then 0
+        z = y.copy()
+        for c, ent in cons.items():
+            for mst, w in ent:
+                z[mst] += w * y[c]
+            z[c] = 0.0
+        return z
+
+    x = R.uniform(-1, 1, N)
+    want = Ct(O.mapped_vmult(free, op, C(x)))
+    got = O.mapped_vmult(mm, op, x)
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    d = O.mapped_diagonal(mm, op)
+    masters = sorted({mst for ent in cons.values() for mst, _ in ent})
+    for g in masters[:: max(1, len(masters) // 8)] + [0, N // 2]:
+        if g in cons:
+            continue
+        e = np.zeros(N)
+        e[g] = 1.0
+        ce = C(e)
+        assert abs(ce @ O.mapped_vmult(free, op, ce) - d[g]) <= 1e-12 * abs(d[g])
