@@ -197,7 +197,7 @@ mpdg_status mpdg_mesh_create_two_level(const mpdg_mesh_desc *coarse, const mpdg_
  * constraint, written to their masters and stay 0; diagonal 1 there.  Cells are
  * coloured greedily (no two cells of a colour share a DoF; at most 64 colours),
  * so the scatter is atomic-free and deterministic.  Operators on it: the heat
- * operator (k(T) and the phase laws only without constraints) and the
+ * operator (k(T), the phase laws and the full tangent; fields read plain) and the
  * advection-diffusion operator (prescribed velocity or a velocity vector,
  * SUPG, inflow/outflow rows), convective and radiative faces selected by the
  * cells' face_ids (not through constrained DoFs); vmult, the diagonal,
