@@ -200,7 +200,7 @@ mpdg_status mpdg_mesh_create_two_level(const mpdg_mesh_desc *coarse, const mpdg_
  * operator (k(T), the phase laws and the full tangent; fields read plain) and the
  * advection-diffusion operator (prescribed velocity or a velocity vector,
  * SUPG, inflow/outflow rows), convective and radiative faces selected by the
- * cells' face_ids (not through constrained DoFs); vmult, the diagonal,
+ * cells' face_ids; vmult, the diagonal,
  * create_rhs, the solvers and the integrated L2 norm. */
 typedef struct {
   int degree;                        /* 1..4 */

@@ -177,7 +177,7 @@ void free_mesh_arrays(Mesh &m)
 {
   for (void *p : {(void *)m.d_vert, (void *)m.d_metric64, (void *)m.d_metric32, (void *)m.d_dmask,
                   (void *)m.d_cell_flags, (void *)m.d_cell_mask, (void *)m.d_tmask_dir, (void *)m.d_tmask_hang,
-                  (void *)m.d_cmap, (void *)m.d_cell_first, (void *)m.d_mface_cell, (void *)m.d_mface_f, (void *)m.d_mface_id, (void *)m.d_cellvert, (void *)m.d_cons_dof, (void *)m.d_cons_ptr,
+                  (void *)m.d_cmap, (void *)m.d_cell_first, (void *)m.d_mface_cell, (void *)m.d_mface_f, (void *)m.d_mface_id, (void *)m.d_cell_fids, (void *)m.d_cellvert, (void *)m.d_cons_dof, (void *)m.d_cons_ptr,
                   (void *)m.d_cons_mast, (void *)m.d_cons_w, (void *)m.d_mast_dof, (void *)m.d_mast_ptr,
                   (void *)m.d_mast_cons, (void *)m.d_mast_w, (void *)m.d_cons_of, (void *)m.d_ccells})
     if (p) cudaFree(p);
@@ -247,14 +247,6 @@ mpdg_status mpdg_op_create(mpdg_mesh *mesh, const mpdg_op_desc *desc, mpdg_op **
     if (desc->supg && mm.fine) throw Error{MPDG_ERR_UNSUPPORTED, "SUPG on two-level meshes"};
     if (desc->vel_kind == MPDG_VEL_NODAL && mm.fine)
       throw Error{MPDG_ERR_UNSUPPORTED, "two-level meshes take no fields (velocity as a DoF vector)"};
-    if (mm.mapped) {
-      // boundary faces through constrained DoFs would need the faces' matrices in
-      // the constrained cells' element matrices (the diagonal)
-      const int sel = ((desc->robin_alpha != 0.0) ? desc->robin_faces : 0) |
-                      ((desc->rad_emissivity != 0.0) ? desc->rad_faces : 0);
-      if (desc->kind == MPDG_OP_HEAT && (sel & mm.mface_cons_ids))
-        throw Error{MPDG_ERR_UNSUPPORTED, "boundary faces through constrained (hanging) DoFs of a mapped mesh"};
-    }
     auto *h = new mpdg_op();
     Op &o = h->o;
     o.mesh = &mm;

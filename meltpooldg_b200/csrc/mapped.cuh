@@ -187,6 +187,82 @@ __global__ void elem_matrix_field_kernel(const KP<double> p, const long *cells, 
   }
 }
 
+// adds to the element matrices of the listed cells their boundary faces'
+// matrices: sum over the face's Gauss points of (alpha + 4 eps sigma T^3) ds
+// phi_t phi_u for the faces whose boundary id conv_bits / rad_bits selects
+// (heat_diffuse_operator.cpp:1088-1129; T read plain at the face DoFs)
+template <int P>
+__global__ void elem_face_matrix_kernel(const KP<double> p, const long *cells, const int8_t *cell_fids,
+                                        const double *cellvert, int conv_bits, double alpha, int rad_bits,
+                                        double es, double *A)
+{
+  constexpr int n = P + 1, n2 = n * n, n3 = n2 * n;
+  const Tables<double> &T = tab<double>(P);
+  __shared__ double cq[n2];
+  const long cell = cells[blockIdx.x];
+  double *Ac = A + (long)blockIdx.x * n3 * n3;
+  for (int f = 0; f < 6; ++f) {
+    const int id = cell_fids[cell * 6 + f];
+    if (id < 0) continue;  // block-uniform
+    const int conv = (conv_bits >> id) & 1, rad = (rad_bits >> id) & 1;
+    if (!conv && !rad) continue;
+    const int d = f >> 1, s = f & 1, t0 = (d == 0) ? 1 : 0, t1 = (d == 2) ? 1 : 2;
+    auto local = [&](int a, int b) {
+      int loc[3];
+      loc[d] = s ? P : 0;
+      loc[t0] = a;
+      loc[t1] = b;
+      return (loc[2] * n + loc[1]) * n + loc[0];
+    };
+    __syncthreads();
+    for (int q = threadIdx.x; q < n2; q += blockDim.x) {
+      const int qa = q % n, qb = q / n;
+      double xi[3];
+      xi[d] = s ? 1.0 : 0.0;
+      xi[t0] = T.x[qa];
+      xi[t1] = T.x[qb];
+      double Ja[3] = {0, 0, 0}, Jb[3] = {0, 0, 0};
+      for (int v = 0; v < 8; ++v) {
+        const int bv[3] = {v & 1, (v >> 1) & 1, (v >> 2) & 1};
+        double fv[3], dfv[3];
+        for (int c = 0; c < 3; ++c) {
+          fv[c] = bv[c] ? xi[c] : 1.0 - xi[c];
+          dfv[c] = bv[c] ? 1.0 : -1.0;
+        }
+        double da = dfv[t0], db = dfv[t1];
+        for (int c = 0; c < 3; ++c)
+          if (c != t0) da *= fv[c];
+        for (int c = 0; c < 3; ++c)
+          if (c != t1) db *= fv[c];
+        for (int c = 0; c < 3; ++c) {
+          const double x = cellvert[(cell * 8 + v) * 3 + c];
+          Ja[c] += x * da;
+          Jb[c] += x * db;
+        }
+      }
+      const double cr[3] = {Ja[1] * Jb[2] - Ja[2] * Jb[1], Ja[2] * Jb[0] - Ja[0] * Jb[2],
+                            Ja[0] * Jb[1] - Ja[1] * Jb[0]};
+      const double ds = sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]) * T.w[qa] * T.w[qb];
+      double Tq = 0.0;
+      if (rad)
+        for (int b = 0; b < n; ++b)
+          for (int a = 0; a < n; ++a) Tq += T.S[qa * n + a] * T.S[qb * n + b] * p.T[p.cmap[cell * n3 + local(a, b)]];
+      cq[q] = ((conv ? alpha : 0.0) + (rad ? 4.0 * es * Tq * Tq * Tq : 0.0)) * ds;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < n2 * n2; e += blockDim.x) {
+      const int tf = e / n2, uf = e % n2;
+      const int ta = tf % n, tb = tf / n, ua = uf % n, ub = uf / n;
+      double sum = 0.0;
+      for (int q = 0; q < n2; ++q) {
+        const int qa = q % n, qb = q / n;
+        sum += cq[q] * T.S[qa * n + ta] * T.S[qb * n + tb] * T.S[qa * n + ua] * T.S[qb * n + ub];
+      }
+      Ac[local(ta, tb) * n3 + local(ua, ub)] += sum;
+    }
+  }
+}
+
 // element matrices of the listed cells with the SUPG terms of the
 // advection-diffusion tangent (advection_diffusion_operator.cpp:471-493): the
 // matrix above plus tau_K (b.grad phi_t) (c_mass phi_u + c_vel b.grad phi_u / JxW
@@ -460,7 +536,6 @@ void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d)
         if (id > 5) throw Error{MPDG_ERR_ARG, "face ids are -1 or 0..5"};
         const int fd = f >> 1, fs = f & 1, t0 = (fd == 0) ? 1 : 0, t1 = (fd == 2) ? 1 : 2;
         std::vector<long> fg;
-        bool touches_cons = false;
         for (int b = 0; b < n; ++b)
           for (int a = 0; a < n; ++a) {
             int loc[3];
@@ -469,7 +544,6 @@ void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d)
             loc[t1] = b;
             const long g = d.cell_dofs[e * n3 + (loc[2] * n + loc[1]) * n + loc[0]];
             fg.push_back(g);
-            touches_cons = touches_cons || cons_of[g] >= 0;
           }
         uint64_t forbidden = 0;
         for (long g : fg) forbidden |= fused[g];
@@ -479,8 +553,11 @@ void build_mapped_mesh(Mesh &m, const mpdg_mapped_mesh_desc &d)
         for (long g : fg) fused[g] |= (uint64_t)1 << c;
         if ((int)by_colour.size() <= c) by_colour.resize(c + 1);
         by_colour[c].push_back({(int)slot_of[e], f, id});
-        if (touches_cons) m.mface_cons_ids |= 1 << id;
       }
+    std::vector<int8_t> slot_fids((size_t)E * 6);
+    for (long e = 0; e < E; ++e)
+      for (int f = 0; f < 6; ++f) slot_fids[(size_t)slot_of[e] * 6 + f] = d.face_ids[e * 6 + f];
+    m.d_cell_fids = upload(slot_fids, B);
     std::vector<int> fcell;
     std::vector<int8_t> ff, fid;
     m.mface_first.assign(1, 0);
@@ -694,6 +771,16 @@ void mapped_element_diagonal(Op &op, double *diag, const std::vector<long> &cell
     else if (uses_kT(op)) elem_matrix_field_kernel<P><<<(unsigned)ncc, 256, 0, op.stream>>>(k, d_cells, A);
     else elem_matrix_kernel<P><<<(unsigned)ncc, 256, 0, op.stream>>>(k, d_cells, A);
     MPDG_LAUNCHED();
+    const mpdg_op_desc &D = op.d;
+    const int conv_bits = (D.kind == MPDG_OP_HEAT && D.robin_alpha != 0.0) ? D.robin_faces : 0;
+    const int rad_bits = (D.kind == MPDG_OP_HEAT && D.rad_emissivity != 0.0) ? D.rad_faces : 0;
+    if (!supg && m.d_cell_fids && (conv_bits || rad_bits)) {
+      if (rad_bits && !op.T64) throw Error{MPDG_ERR_ARG, "radiative faces need the temperature field"};
+      elem_face_matrix_kernel<P><<<(unsigned)ncc, 128, 0, op.stream>>>(
+          k, d_cells, m.d_cell_fids, m.d_cellvert, conv_bits, D.robin_alpha, rad_bits,
+          D.rad_emissivity * 5.670374419e-8, A);
+      MPDG_LAUNCHED();
+    }
     const long nt = (long)tasks.size();
     cell_task_kernel<P><<<(unsigned)((nt + 3) / 4), 128, 0, op.stream>>>(
         nt, d_task_cc, d_task_tgt, d_cells, m.d_cmap, m.d_cons_of, m.d_cons_ptr, m.d_cons_mast, m.d_cons_w, A,

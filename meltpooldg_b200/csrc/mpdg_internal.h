@@ -128,8 +128,8 @@ struct Mesh {
   // colour (faces of a colour share no DoF), colour c at [mface_first[c], [c+1])
   int *d_mface_cell = nullptr;
   int8_t *d_mface_f = nullptr, *d_mface_id = nullptr;
+  int8_t *d_cell_fids = nullptr;       // per colour-major cell: its 6 faces' boundary ids
   std::vector<long> mface_first;
-  int mface_cons_ids = 0;              // ids whose faces touch a constrained DoF
   bool has_dirichlet = false;
   size_t device_bytes = 0;
   bool metric32_ready = false;

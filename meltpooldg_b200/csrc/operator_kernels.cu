@@ -2457,7 +2457,8 @@ __global__ void __launch_bounds__(128) mapped_face_kernel(const int *fcell, cons
                                                           const double *cellvert, int conv_bits, double alpha,
                                                           double t_inf, int rad_bits, double es, double t_rad,
                                                           int mode, const Real *src, const Real *Tf, Real *dst,
-                                                          const uint8_t *rmask, const uint8_t *wmask)
+                                                          const uint8_t *rmask, const uint8_t *wmask,
+                                                          const uint8_t *cell_flags)
 {
   constexpr int n = P + 1, n2 = n * n, n3 = n2 * n;
   __shared__ Real tile[4][n2];
@@ -2466,6 +2467,9 @@ __global__ void __launch_bounds__(128) mapped_face_kernel(const int *fcell, cons
   if (f >= count) return;  // warp-uniform
   const long e = first + f;
   const long slot = fcell[e];
+  // the diagonal of a cell with constrained DoFs comes from its element
+  // matrix, face matrices included
+  if (mode == ROBIN_DIAGONAL && cell_flags && (cell_flags[slot] & 2)) return;  // warp-uniform
   const int face = fface[e], id = fid[e];
   const int conv = (conv_bits >> id) & 1, rad = (rad_bits >> id) & 1;
   if (!conv && !rad) return;  // warp-uniform
@@ -2513,7 +2517,7 @@ void launch_robin(Op &op, Real *dst, const Real *src, int mode)
   mapped_face_kernel<PP, Real><<<grid, 128, 0, op.stream>>>(m.d_mface_cell, m.d_mface_f, m.d_mface_id, first, count, \
                                                             m.d_cmap, m.d_cellvert, conv_bits, D.robin_alpha,        \
                                                             D.robin_t_inf, rad_bits, es, D.rad_t_inf, mode, src, Tf, \
-                                                            dst, rmask, wmask)
+                                                            dst, rmask, wmask, m.d_cell_flags)
       switch (m.degree) {
         case 1: MPDG_MFACE(1); break;
         case 2: MPDG_MFACE(2); break;

@@ -484,18 +484,41 @@ def test_mapped_boundary_faces(cuda, p):
     assert relerr(rm.cpu().numpy()[perm], rs.cpu().numpy()) < TOL64
 
 
-def test_mapped_boundary_faces_through_hanging_nodes_are_refused(cuda):
+def test_mapped_boundary_faces_through_hanging_nodes(cuda):
+    """Convective and radiative faces on a locally refined mesh whose refined
+    cell touches the boundary (hanging DoFs on the selected faces): vmult and
+    the diagonal (face matrices inside the constrained cells' element
+    matrices) against the oracle's mapped operator."""
+    import torch
     import meltpooldg_b200 as M
     from meltpooldg_b200.refine import refine_box
-    V = O.box_vertices(3, (3, 3, 3), [-1.0] * 3, [1.0] * 3, 0.0, 1)
-    r = refine_box((3, 3, 3), 2, [4], vertices=V)  # cell 4 touches the face z = -1
+    p = 2
+    V = O.box_vertices(3, (3, 3, 3), [-1.0] * 3, [1.0] * 3, 0.1, 1)
+    r = refine_box((3, 3, 3), p, [4], vertices=V)  # cell 4 touches the face z = -1
     ids = box_face_ids(r["cell_vertices"])
-    gm = M.MappedMesh(r["cell_vertices"], r["cell_dofs"], r["n_dofs"], 2, constraints=r["constraints"],
+    mm = O.MappedMesh(p, r["cell_vertices"], r["cell_dofs"], r["n_dofs"], r["constraints"], face_ids=ids)
+    gm = M.MappedMesh(r["cell_vertices"], r["cell_dofs"], r["n_dofs"], p, constraints=r["constraints"],
                       face_ids=ids)
-    with pytest.raises(Exception, match="constrained"):
-        M.HeatDiffuseOperator(gm, 1e-2, robin_alpha=10.0, robin_faces=[(0, 0), (0, 1), (1, 0), (1, 1), (2, 0)])
-    # faces away from the hanging nodes are served
-    M.HeatDiffuseOperator(gm, 1e-2, robin_alpha=10.0, robin_faces=[(2, 1)])
+    N = mm.n_dofs
+    T = 300.0 + 50.0 * rng(5).uniform(size=N)
+    kw = dict(robin_alpha=25.0, robin_t_inf=300.0, rad_emissivity=0.8, rad_t_inf=350.0)
+    op = M.HeatDiffuseOperator(gm, 1e-2, rho_cp=2.0, k0=1.5, precisions=("fp64", "fp32"),
+                               robin_faces=[(2, 0), (0, 1)], rad_faces=[(2, 0), (1, 1)], **kw)
+    oop = O.Operator(O.HEAT, 1e-2, rho_cp=2.0, k0=1.5, temperature=T, robin_faces=(1 << 4) | (1 << 1),
+                     rad_faces=(1 << 4) | (1 << 3), **kw)
+    Td = dev(T)
+    op.set_temperature(Td)
+    x = rng(6).uniform(-1, 1, N)
+    ref = O.mapped_vmult(mm, oop, x)
+    y = torch.empty(N, dtype=torch.float64, device="cuda")
+    op.vmult(y, dev(x))
+    assert relerr(y.cpu().numpy(), ref) < TOL64
+    y32 = torch.empty(N, dtype=torch.float32, device="cuda")
+    op.vmult(y32, dev(x, torch.float32))
+    assert relerr(y32.double().cpu().numpy(), ref) < TOL32
+    d = torch.empty_like(y)
+    op.compute_diagonal(d)
+    assert relerr(d.cpu().numpy(), O.mapped_diagonal(mm, oop)) < TOL64
 
 
 @pytest.mark.parametrize("p", [1, 2])

@@ -164,3 +164,53 @@ def test_mapped_hanging_constraints_with_field_coefficients(p, law):
         e[g] = 1.0
         ce = C(e)
         assert abs(ce @ O.mapped_vmult(free, op, ce) - d[g]) <= 1e-12 * abs(d[g])
+
+
+def test_mapped_faces_through_hanging_nodes_are_CtAC():
+    """Convective and radiative faces through hanging DoFs of a locally refined
+    mesh: the operator is C^T A C with A the same cells and faces without
+    constraints, and its diagonal (C e_g)^T A (C e_g)."""
+    from meltpooldg_b200.refine import refine_box
+    p = 2
+    V = O.box_vertices(3, (3, 3, 3), [-1.0] * 3, [1.0] * 3, 0.1, 1)
+    r = refine_box((3, 3, 3), p, [4], vertices=V)
+    cv = np.asarray(r["cell_vertices"]).reshape(-1, 8, 3)
+    ids = -np.ones((cv.shape[0], 6), np.int8)
+    for d in range(3):
+        for s in range(2):
+            corners = [v for v in range(8) if ((v >> d) & 1) == s]
+            on = np.all(np.abs(cv[:, corners, d] - (1.0 if s else -1.0)) < 1e-12, axis=1)
+            ids[on, 2 * d + s] = 2 * d + s
+    N = r["n_dofs"]
+    mm = O.MappedMesh(p, r["cell_vertices"], r["cell_dofs"], N, r["constraints"], face_ids=ids)
+    free = O.MappedMesh(p, r["cell_vertices"], r["cell_dofs"], N, face_ids=ids)
+    cons = mm.constraints
+    assert (ids[:, 4] >= 0).any()
+    T = 300.0 + 50.0 * np.random.default_rng(2).uniform(size=N)
+    op = O.Operator(O.HEAT, 1e-2, rho_cp=2.0, k0=1.5, temperature=T, robin_alpha=25.0, robin_t_inf=300.0,
+                    robin_faces=1 << 4, rad_emissivity=0.8, rad_t_inf=350.0, rad_faces=1 << 4)
+
+    def C(x):
+        y = x.copy()
+        for c, ent in cons.items():
+            y[c] = sum(w * x[mst] for mst, w in ent)
+        return y
+
+    def Ct(y):
+        z = y.copy()
+        for c, ent in cons.items():
+            for mst, w in ent:
+                z[mst] += w * y[c]
+            z[c] = 0.0
+        return z
+
+    x = np.random.default_rng(3).uniform(-1, 1, N)
+    want = Ct(O.mapped_vmult(free, op, C(x)))
+    assert np.abs(O.mapped_vmult(mm, op, x) - want).max() <= 1e-12 * np.abs(want).max()
+    d = O.mapped_diagonal(mm, op)
+    masters = sorted({mst for ent in cons.values() for mst, _ in ent})
+    for g in masters[:: max(1, len(masters) // 10)]:
+        e = np.zeros(N)
+        e[g] = 1.0
+        ce = C(e)
+        assert abs(ce @ O.mapped_vmult(free, op, ce) - d[g]) <= 1e-12 * abs(d[g])
