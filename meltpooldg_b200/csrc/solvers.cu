@@ -169,21 +169,53 @@ int pcg(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero, d
   dot_into(v.r, v.z, sc + kRZ);
   dev_copy<R>(N, v.z, v.p, s);
   const bool fused_jacobi = P.kind == MPDG_PREC_JACOBI;
+  // The test |r| <= tol runs on the device after every iteration
+  // (dev_cg_check); the host reads its verdict every K iterations.  On small
+  // problems the round trip costs more than the iterations launched past
+  // convergence, whose updates are skipped (x, r, p stay those of the
+  // converged iteration: the result, the iteration count and the residual are
+  // the per-iteration test's).
+  const int K = (N <= (4L << 20)) ? 4 : 1;
+  dev_cg_check_init(sc, tol, s);
+  const int applies0 = applies;
+  int prec_count = 0, launched = 0;
+  auto report = [&](int it) {
+    iters = it;
+    applies = applies0 + it + (it > 0 ? (it - 1) * prec_count : 0);
+  };
   while (true) {
-    launch_apply<R>(op, v.Ap, v.p);
-    ++applies;
-    dot_into(v.p, v.Ap, sc + kPAP);
-    dev_cg_update<R, R>(N, sc, x, v.r, v.p, v.Ap, fused_jacobi ? v.invd : nullptr, v.z, w.partial, s);
-    ++iters;
-    res = std::sqrt(fetch(op, w, sc + kRR));
-    if (!std::isfinite(res)) return MPDG_ERR_NAN;
-    if (res <= tol) return MPDG_OK;
-    if (iters >= max_it) return MPDG_ERR_NOT_CONVERGED;
-    if (!fused_jacobi) {
-      prec_apply<R>(op, P, v, v.r, v.z, applies);
-      dot_into(v.r, v.z, sc + kRZNEW);
+    const int batch = std::min(K, max_it - launched);
+    for (int bi = 0; bi < batch; ++bi) {
+      launch_apply<R>(op, v.Ap, v.p);
+      dot_into(v.p, v.Ap, sc + kPAP);
+      dev_cg_update_lagged<R, R>(N, sc, x, v.r, v.p, v.Ap, fused_jacobi ? v.invd : nullptr, v.z, w.partial, s);
+      ++launched;
+      dev_cg_check(sc, launched, s);
+      if (!fused_jacobi) {
+        int pa = 0;
+        prec_apply<R>(op, P, v, v.r, v.z, pa);
+        prec_count = pa;
+        dot_into(v.r, v.z, sc + kRZNEW);
+      }
+      dev_cg_direction_lagged<R>(N, sc, v.p, v.z, s);
     }
-    dev_cg_direction<R>(N, sc, v.p, v.z, s);
+    fetch(op, w, sc + kDONE, 3);
+    const double done = w.host[0], conv = w.host[1], rr = w.host[2];
+    if (done == 1.0) {
+      report((int)conv);
+      res = std::sqrt(rr);
+      return MPDG_OK;
+    }
+    if (done != 0.0) {
+      report((int)conv);
+      res = std::sqrt(rr);
+      return MPDG_ERR_NAN;
+    }
+    if (launched >= max_it) {
+      report(launched);
+      res = std::sqrt(fetch(op, w, sc + kRR));
+      return MPDG_ERR_NOT_CONVERGED;
+    }
   }
 }
 

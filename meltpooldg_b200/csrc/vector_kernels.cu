@@ -200,12 +200,13 @@ __global__ void mul_kernel(long n, const R *d, const R *x, R *y)
 
 // CG step part 1: alpha = s[RZ] / s[PAP]; x += alpha p; r -= alpha Ap;
 // with jacobi: z = invd r; partials of r.r (slot 0) and r.z (slot 1)
-template <typename R, typename RX>
+template <typename R, typename RX, bool LAG = false>
 __global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long n, const double *s, RX *x,
                                                                 R *r, const R *p, const R *Ap,
                                                                 const R *invd, R *z,
                                                                 double *partial, double xscale)
 {
+  if (LAG && s[kDONE] != 0.0) return;  // grid-uniform: the solve stopped
   const double alpha = s[kRZ] / s[kPAP];
   const double xa = alpha * xscale;
   double rr = 0.0, rz = 0.0;
@@ -247,9 +248,10 @@ __global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long n, const do
 }
 
 // CG step part 2: beta = s[RZNEW] / s[RZ]; p = z + beta p; s[RZ] <- s[RZNEW] (block 0)
-template <typename R>
+template <typename R, bool LAG = false>
 __global__ void cg_direction_kernel(long n, double *s, R *p, const R *z)
 {
+  if (LAG && s[kDONE] != 0.0) return;
   const double beta = s[kRZNEW] / s[kRZ];
   const long stride = (long)gridDim.x * blockDim.x;
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -269,6 +271,29 @@ __global__ void cg_direction_kernel(long n, double *s, R *p, const R *z)
 __global__ void shift_scalar_kernel(double *s)
 {
   s[kRZ] = s[kRZNEW];
+}
+
+__global__ void shift_scalar_lagged_kernel(double *s)
+{
+  if (s[kDONE] == 0.0) s[kRZ] = s[kRZNEW];
+}
+
+// after iteration `iter`: the host loop's test |r| <= tol (sqrt correctly
+// rounded, so the decision is the host's) and the non-finite check, recorded
+// once; r.r is kept, since later (skipped) iterations reuse the partials
+__global__ void cg_check_kernel(double *s, int iter)
+{
+  if (s[kDONE] != 0.0) return;
+  const double rr = s[kRR], res = sqrt(rr);
+  if (!isfinite(res)) {
+    s[kDONE] = 2.0;
+  } else if (res <= s[kTOL]) {
+    s[kDONE] = 1.0;
+  } else {
+    return;
+  }
+  s[kCONV] = (double)iter;
+  s[kRRCONV] = rr;
 }
 
 // Chebyshev start: d = invd r / theta; z = d
@@ -481,6 +506,57 @@ void dev_cg_direction(long n, double *s, R *p, const R *z, cudaStream_t st)
 }
 template void dev_cg_direction<double>(long, double *, double *, const double *, cudaStream_t);
 template void dev_cg_direction<float>(long, double *, float *, const float *, cudaStream_t);
+
+template <typename R, typename RX>
+void dev_cg_update_lagged(long n, double *s, RX *x, R *r, const R *p, const R *Ap, const R *invd, R *z,
+                          double *partial, cudaStream_t st)
+{
+  cg_update_kernel<R, RX, true><<<kRedBlocks, kRedThreads, 0, st>>>(n, s, x, r, p, Ap, invd, z, partial, 1.0);
+  MPDG_LAUNCHED();
+  finish_kernel<<<1, kRedThreads, 0, st>>>(partial, 1, s + kRR, 0);
+  MPDG_LAUNCHED();
+  if (invd) {
+    finish_kernel<<<1, kRedThreads, 0, st>>>(partial + kRedBlocks, 1, s + kRZNEW, 0);
+    MPDG_LAUNCHED();
+  }
+}
+template void dev_cg_update_lagged<double, double>(long, double *, double *, double *, const double *,
+                                                   const double *, const double *, double *, double *,
+                                                   cudaStream_t);
+template void dev_cg_update_lagged<float, float>(long, double *, float *, float *, const float *,
+                                                 const float *, const float *, float *, double *,
+                                                 cudaStream_t);
+
+template <typename R>
+void dev_cg_direction_lagged(long n, double *s, R *p, const R *z, cudaStream_t st)
+{
+  cg_direction_kernel<R, true><<<vgrid4(n), 256, 0, st>>>(n, s, p, z);
+  MPDG_LAUNCHED();
+  shift_scalar_lagged_kernel<<<1, 1, 0, st>>>(s);
+  MPDG_LAUNCHED();
+}
+template void dev_cg_direction_lagged<double>(long, double *, double *, const double *, cudaStream_t);
+template void dev_cg_direction_lagged<float>(long, double *, float *, const float *, cudaStream_t);
+
+__global__ void cg_check_init_kernel(double *s, double tol)
+{
+  s[kDONE] = 0.0;
+  s[kCONV] = 0.0;
+  s[kRRCONV] = 0.0;
+  s[kTOL] = tol;
+}
+
+void dev_cg_check_init(double *s, double tol, cudaStream_t st)
+{
+  cg_check_init_kernel<<<1, 1, 0, st>>>(s, tol);
+  MPDG_LAUNCHED();
+}
+
+void dev_cg_check(double *s, int iter, cudaStream_t st)
+{
+  cg_check_kernel<<<1, 1, 0, st>>>(s, iter);
+  MPDG_LAUNCHED();
+}
 
 template <typename R>
 void dev_cheb_start(long n, double inv_theta, const R *invd, const R *r, R *d, R *z, cudaStream_t s)

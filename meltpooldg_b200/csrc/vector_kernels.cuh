@@ -10,6 +10,10 @@ constexpr int kRedBlocks = 592;   // 4 blocks per SM on 148 SMs: fixed, so sums 
 
 // slots of the device scalar array used by the CG kernels
 enum { kRZ = 0, kRZNEW = 1, kPAP = 2, kRR = 3, kNScalars = 8 };
+// CG with the convergence test on the device (dev_cg_check): the solve's state
+// (0 running, 1 converged, 2 not finite), the iteration it stopped at, r.r
+// there, and the tolerance on |r|
+enum { kDONE = 4, kCONV = 5, kRRCONV = 6, kTOL = 7 };
 
 void dev_dot(const double *a, const double *b, long n, double *partial, double *out, cudaStream_t s);
 void dev_dot_f(const float *a, const float *b, long n, double *partial, double *out, cudaStream_t s);
@@ -34,6 +38,16 @@ void dev_cg_update(long n, double *s, RX *x, R *r, const R *p, const R *Ap, cons
                    double *partial, cudaStream_t st, double xscale = 1.0);
 template <typename R>
 void dev_cg_direction(long n, double *s, R *p, const R *z, cudaStream_t st);
+// the same two steps, skipped once s[kDONE] is set, and the device-side test
+// that sets it after iteration `iter` (|r| <= s[kTOL], or r.r not finite)
+template <typename R, typename RX>
+void dev_cg_update_lagged(long n, double *s, RX *x, R *r, const R *p, const R *Ap, const R *invd, R *z,
+                          double *partial, cudaStream_t st);
+template <typename R>
+void dev_cg_direction_lagged(long n, double *s, R *p, const R *z, cudaStream_t st);
+void dev_cg_check(double *s, int iter, cudaStream_t st);
+// resets the state slots and sets the tolerance
+void dev_cg_check_init(double *s, double tol, cudaStream_t st);
 template <typename R>
 void dev_cheb_start(long n, double inv_theta, const R *invd, const R *r, R *d, R *z, cudaStream_t s);
 template <typename R>
