@@ -66,6 +66,12 @@ double read_scalar(const double *dev, cudaStream_t s)
   return h;
 }
 
+void read_scalars(const double *dev, double *h, int count, cudaStream_t s)
+{
+  MPDG_CUDA(cudaMemcpyAsync(h, dev, sizeof(double) * count, cudaMemcpyDeviceToHost, s));
+  MPDG_CUDA(cudaStreamSynchronize(s));
+}
+
 }  // namespace
 
 int solve_cg_noalloc(Op &op, double *x, const double *b, double rel_tol, double abs_tol, int max_it,
@@ -110,24 +116,38 @@ int solve_cg_noalloc(Op &op, double *x, const double *b, double rel_tol, double 
     dev_mul<double>(N, invd, r, z, s);
     dev_dot(r, z, N, partial, sc + kRZ, s);
     dev_copy<double>(N, z, p, s);
+    // the convergence test on the device after every iteration, read every 4
+    // iterations (updates past convergence are skipped: results and counts
+    // are the per-iteration test's)
+    constexpr int K = 4;
+    dev_cg_check_init(sc, tol, s);
+    int launched = 0;
     while (true) {
-      launch_apply<double>(op, Ap, p);
-      ++applies;
-      dev_dot(p, Ap, N, partial, sc + kPAP, s);
-      dev_cg_update<double, double>(N, sc, x, r, p, Ap, invd, z, partial, s);
-      ++it;
-      res = std::sqrt(read_scalar(sc + kRR, s));
-      if (!std::isfinite(res)) {
-        status = MPDG_ERR_NAN;
+      const int batch = std::min(K, max_it - launched);
+      for (int bi = 0; bi < batch; ++bi) {
+        launch_apply<double>(op, Ap, p);
+        dev_dot(p, Ap, N, partial, sc + kPAP, s);
+        dev_cg_update_lagged<double, double>(N, sc, x, r, p, Ap, invd, z, partial, s);
+        ++launched;
+        dev_cg_check(sc, launched, s);
+        dev_cg_direction_lagged<double>(N, sc, p, z, s);
+      }
+      double h[3];
+      read_scalars(sc + kDONE, h, 3, s);
+      if (h[0] != 0.0) {
+        it = (int)h[1];
+        res = std::sqrt(h[2]);
+        if (h[0] != 1.0) status = MPDG_ERR_NAN;
         break;
       }
-      if (res <= tol) break;
-      if (it >= max_it) {
+      if (launched >= max_it) {
+        it = launched;
+        res = std::sqrt(read_scalar(sc + kRR, s));
         status = MPDG_ERR_NOT_CONVERGED;
         break;
       }
-      dev_cg_direction<double>(N, sc, p, z, s);
     }
+    applies += it;
   }
   MPDG_CUDA(cudaStreamSynchronize(s));
   rep = mpdg_solve_report{};
