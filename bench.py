@@ -349,6 +349,52 @@ def run_reference(args, rank, world):
 
 
 # ------------------------------------------------------------ single-operator workloads
+def solve_inputs(op, mask, N):
+    """The workload's linear system: (b, exact solution or None, solver, preconditioner)."""
+    import torch
+    nc, p = WL["nc"], WL["degree"]
+    if WL["name"] == "advdiff":
+        # one theta-scheme step of the tanh level set
+        X = [np.linspace(0.0, 1.0, n * p + 1) for n in nc]  # Q2 Gauss-Lobatto nodes are uniform
+        Z, Y, Xg = np.meshgrid(X[2], X[1], X[0], indexing="ij")
+        d = 0.25 - np.sqrt((Xg - 0.5) ** 2 + (Y - 0.75) ** 2 + (Z - 0.5) ** 2)
+        phi0 = torch.tensor(np.tanh(d / 0.01).reshape(-1), device="cuda")
+        b = torch.zeros_like(phi0)
+        op.create_rhs(b, phi0)
+        return b, None, "GMRES", "Diagonal"
+    seed = 1 if WL["name"] == "c1" else 5
+    xs = torch.tensor(np.random.Generator(np.random.PCG64(seed)).uniform(-1, 1, N), device="cuda")
+    xs[torch.tensor(mask.astype(bool), device="cuda")] = 0.0
+    b = torch.empty_like(xs)
+    op.vmult(b, xs)
+    return b, xs, "CG", ("Diagonal" if WL["name"] == "c1" else "Chebyshev")
+
+
+def run_profile_solve(args):
+    """One solve of the workload's system in the given form after an untimed
+    warm-up solve, inside a cudaProfilerStart/Stop range (for
+    `ncu --profile-from-start off`); prints the solve's report."""
+    import torch
+    import meltpooldg_b200 as M
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    V, mask, T = mesh_inputs()
+    mesh = M.Mesh(V, WL["nc"], WL["degree"], mask)
+    op, Td = make_operator(M, mesh, T)
+    b, _, solver_type, prec = solve_inputs(op, mask, mesh.n_dofs)
+    data = M.LinearSolverData(solver_type=solver_type, preconditioner_type=prec, rel_tolerance=1e-10,
+                              abs_tolerance=1e-20, mixed_precision=args.profile_solve == "fp32_refined")
+    x = torch.zeros_like(b)
+    M.LinearSolver.solve(op, x, b, data)
+    torch.cuda.synchronize()
+    x.zero_()
+    torch.cuda.cudart().cudaProfilerStart()
+    M.LinearSolver.solve(op, x, b, data)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
+    print(json.dumps({"profile_solve": args.profile_solve, "workload": WL["name"],
+                      "report": dict(M.LinearSolver.last_report)}), flush=True)
+
+
 def run_operator_workload(args, rank, world, headline):
     """One apply workload (config 2, 3 or 1): timed FP64 applies, FP32 applies,
     the multi-vector pass, the host-buffer e2e apply, the solves, the CPU
@@ -470,23 +516,7 @@ def run_operator_workload(args, rank, world, headline):
     # solves to 1e-10 in the plain FP64 form and the FP32-inner / FP64-refined form
     solves, solve_io = None, None
     if not args.no_solve:
-        if WL["name"] == "advdiff":
-            # one theta-scheme step of the tanh level set
-            X = [np.linspace(0.0, 1.0, n * p + 1) for n in nc]  # Q2 Gauss-Lobatto nodes are uniform
-            Z, Y, Xg = np.meshgrid(X[2], X[1], X[0], indexing="ij")
-            d = 0.25 - np.sqrt((Xg - 0.5) ** 2 + (Y - 0.75) ** 2 + (Z - 0.5) ** 2)
-            phi0 = torch.tensor(np.tanh(d / 0.01).reshape(-1), device="cuda")
-            b = torch.zeros_like(phi0)
-            op.create_rhs(b, phi0)
-            xs = None
-            solver_type, prec = "GMRES", "Diagonal"
-        else:
-            seed = 1 if WL["name"] == "c1" else 5
-            xs = torch.tensor(np.random.Generator(np.random.PCG64(seed)).uniform(-1, 1, N), device="cuda")
-            xs[torch.tensor(mask.astype(bool), device="cuda")] = 0.0
-            b = torch.empty_like(xs)
-            op.vmult(b, xs)
-            solver_type, prec = ("CG", "Diagonal") if WL["name"] == "c1" else ("CG", "Chebyshev")
+        b, xs, solver_type, prec = solve_inputs(op, mask, N)
         solves = {"solver": f"{solver_type} + {prec}",
                   "timing": f"wall clock per solve, {args.solve_reps} solves after one untimed warm-up solve"}
         solve_io = {"b": b.cpu().numpy(), "x": {}}
@@ -883,6 +913,8 @@ def main():
     ap.add_argument("--low-rate", type=float, default=40.0, help="serve: arrival rate of the below-capacity stream")
     ap.add_argument("--low-requests", type=int, default=1000, help="serve: requests of the below-capacity stream")
     ap.add_argument("--no-fp64-arm", action="store_true", help="serve: skip the plain FP64 arm")
+    ap.add_argument("--profile-solve", default=None, choices=["fp64", "fp32_refined"],
+                    help="one solve of the workload's system inside a profiler range (ncu --profile-from-start off)")
     ap.add_argument("--fp64-requests", type=int, default=500,
                     help="serve: requests of the stream the plain FP64 arm serves")
     args = ap.parse_args()
@@ -895,7 +927,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        if args.impl == "reference":
+        if args.profile_solve:
+            run_profile_solve(args)
+        elif args.impl == "reference":
             run_reference(args, rank, world)
         elif args.workload == "batch":
             line = run_batch(args, rank, world)
