@@ -129,7 +129,7 @@ int solve_cg_noalloc(Op &op, double *x, const double *b, double rel_tol, double 
         dev_dot(p, Ap, N, partial, sc + kPAP, s);
         dev_cg_update_lagged<double, double>(N, sc, x, r, p, Ap, invd, z, partial, s);
         ++launched;
-        dev_cg_check(sc, launched, s);
+        dev_cg_check(sc, s);
         dev_cg_direction_lagged<double>(N, sc, p, z, s);
       }
       double h[3];

@@ -183,14 +183,12 @@ int pcg(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero, d
     iters = it;
     applies = applies0 + it + (it > 0 ? (it - 1) * prec_count : 0);
   };
-  while (true) {
-    const int batch = std::min(K, max_it - launched);
+  auto run_batch = [&](int batch) {
     for (int bi = 0; bi < batch; ++bi) {
       launch_apply<R>(op, v.Ap, v.p);
       dot_into(v.p, v.Ap, sc + kPAP);
       dev_cg_update_lagged<R, R>(N, sc, x, v.r, v.p, v.Ap, fused_jacobi ? v.invd : nullptr, v.z, w.partial, s);
-      ++launched;
-      dev_cg_check(sc, launched, s);
+      dev_cg_check(sc, s);
       if (!fused_jacobi) {
         int pa = 0;
         prec_apply<R>(op, P, v, v.r, v.z, pa);
@@ -199,6 +197,66 @@ int pcg(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero, d
       }
       dev_cg_direction_lagged<R>(N, sc, v.p, v.z, s);
     }
+  };
+  // Batches after the first replay one CUDA graph of K iterations (the launch
+  // sequence is the same every time: pointers fixed, scalars and the
+  // iteration count on the device), which removes the per-kernel launch cost
+  // that dominates small solves.  Captured on a stream of its own; if the
+  // capture fails, the batches run launch by launch.
+  cudaGraphExec_t gexec = nullptr;
+  int64_t graph_kernels = 0;
+  bool graph_tried = false;
+  struct GraphGuard {
+    cudaGraphExec_t &g;
+    ~GraphGuard()
+    {
+      if (g) cudaGraphExecDestroy(g);
+    }
+  } guard{gexec};
+  auto capture = [&]() {
+    graph_tried = true;
+    cudaStream_t cap = nullptr;
+    if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    const cudaStream_t saved = op.stream;
+    const int64_t k0 = mpdg_kernel_launches();
+    cudaGraph_t g = nullptr;
+    bool ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      op.stream = cap;
+      s = cap;
+      try {
+        run_batch(K);
+      } catch (...) {
+        ok = false;
+      }
+      op.stream = saved;
+      s = saved;
+      ok = (cudaStreamEndCapture(cap, &g) == cudaSuccess) && ok && g != nullptr;
+      if (ok) ok = cudaGraphInstantiate(&gexec, g, 0) == cudaSuccess;
+      if (g) cudaGraphDestroy(g);
+    }
+    cudaStreamDestroy(cap);
+    cudaGetLastError();  // a failed capture leaves no sticky error
+    graph_kernels = mpdg_kernel_launches() - k0;
+    count_launch((int)-graph_kernels);  // captured, not run: counted at each replay
+    if (!ok && gexec) {
+      cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+    }
+  };
+  while (true) {
+    const int batch = std::min(K, max_it - launched);
+    if (K > 1 && batch == K && launched > 0 && !graph_tried) capture();
+    if (gexec && batch == K) {
+      MPDG_CUDA(cudaGraphLaunch(gexec, op.stream));
+      count_launch((int)graph_kernels);
+    } else {
+      run_batch(batch);
+    }
+    launched += batch;
     fetch(op, w, sc + kDONE, 3);
     const double done = w.host[0], conv = w.host[1], rr = w.host[2];
     if (done == 1.0) {

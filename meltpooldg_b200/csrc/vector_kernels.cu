@@ -322,12 +322,15 @@ __global__ void shift_scalar_lagged_kernel(double *s)
   if (s[kDONE] == 0.0) s[kRZ] = s[kRZNEW];
 }
 
-// after iteration `iter`: the host loop's test |r| <= tol (sqrt correctly
-// rounded, so the decision is the host's) and the non-finite check, recorded
-// once; r.r is kept, since later (skipped) iterations reuse the partials
-__global__ void cg_check_kernel(double *s, int iter)
+// after each iteration: counts it (s[kCONV]) and runs the host loop's test
+// |r| <= tol (sqrt correctly rounded, so the decision is the host's) and the
+// non-finite check, once; r.r is kept, since later (skipped) iterations reuse
+// the partials.  The iteration number lives on the device, so a batch of
+// iterations is the same launch sequence every time (a graph replays it).
+__global__ void cg_check_kernel(double *s)
 {
   if (s[kDONE] != 0.0) return;
+  s[kCONV] += 1.0;
   const double rr = s[kRR], res = sqrt(rr);
   if (!isfinite(res)) {
     s[kDONE] = 2.0;
@@ -336,7 +339,6 @@ __global__ void cg_check_kernel(double *s, int iter)
   } else {
     return;
   }
-  s[kCONV] = (double)iter;
   s[kRRCONV] = rr;
 }
 
@@ -612,9 +614,9 @@ void dev_cg_check_init(double *s, double tol, cudaStream_t st)
   MPDG_LAUNCHED();
 }
 
-void dev_cg_check(double *s, int iter, cudaStream_t st)
+void dev_cg_check(double *s, cudaStream_t st)
 {
-  cg_check_kernel<<<1, 1, 0, st>>>(s, iter);
+  cg_check_kernel<<<1, 1, 0, st>>>(s);
   MPDG_LAUNCHED();
 }
 

@@ -43,13 +43,14 @@ void dev_cg_update(long n, double *s, RX *x, R *r, const R *p, const R *Ap, cons
 template <typename R>
 void dev_cg_direction(long n, double *s, R *p, const R *z, cudaStream_t st);
 // the same two steps, skipped once s[kDONE] is set, and the device-side test
-// that sets it after iteration `iter` (|r| <= s[kTOL], or r.r not finite)
+// that counts the iteration in s[kCONV] and sets s[kDONE] (|r| <= s[kTOL], or
+// r.r not finite)
 template <typename R, typename RX>
 void dev_cg_update_lagged(long n, double *s, RX *x, R *r, const R *p, const R *Ap, const R *invd, R *z,
                           double *partial, cudaStream_t st);
 template <typename R>
 void dev_cg_direction_lagged(long n, double *s, R *p, const R *z, cudaStream_t st);
-void dev_cg_check(double *s, int iter, cudaStream_t st);
+void dev_cg_check(double *s, cudaStream_t st);
 // resets the state slots and sets the tolerance
 void dev_cg_check_init(double *s, double tol, cudaStream_t st);
 template <typename R>
