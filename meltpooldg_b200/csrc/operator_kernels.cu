@@ -2640,6 +2640,7 @@ void launch_fine_block(Op &op, Real *dst, const Real *src)
   Mesh &m = *op.mesh;
   const bool mask = op.use_dirichlet && m.has_dirichlet;
   f.use_dirichlet = op.use_dirichlet;
+  f.stream = op.stream;  // the fine block runs in the apply's stream (or its capture)
   f.hang_src = src;
   f.hang_mask = mask ? m.d_dmask : nullptr;
   try {

@@ -423,23 +423,16 @@ int gmres(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero,
       prec_apply<R>(op, P, v, vj, v.z, applies);
       launch_apply<R>(op, vn, v.z);
       ++applies;
-      // two passes of classical Gram-Schmidt; the first pass's update and the
-      // second pass's dots share one sweep over the basis where it fits
+      // two passes of classical Gram-Schmidt
       for (int k = 0; k <= j; ++k) h[k] = 0.0;
-      auto take_h = [&]() {
+      for (int pass = 0; pass < 2; ++pass) {
+        dev_mdot<R>(VB, N, j + 1, vn, w.partial, w.scal + kNScalars, s);
         MPDG_CUDA(cudaMemcpyAsync(w.host, w.scal + kNScalars, sizeof(double) * (j + 1),
                                   cudaMemcpyDeviceToHost, s));
         MPDG_CUDA(cudaStreamSynchronize(s));
         for (int k = 0; k <= j; ++k) h[k] += w.host[k];
-      };
-      dev_mdot<R>(VB, N, j + 1, vn, w.partial, w.scal + kNScalars, s);
-      take_h();
-      if (!dev_mgs_update_mdot<R>(VB, N, j + 1, w.scal + kNScalars, vn, w.partial, w.scal + kNScalars, s)) {
         dev_mgs_update<R>(VB, N, j + 1, w.scal + kNScalars, vn, s);
-        dev_mdot<R>(VB, N, j + 1, vn, w.partial, w.scal + kNScalars, s);
       }
-      take_h();
-      dev_mgs_update<R>(VB, N, j + 1, w.scal + kNScalars, vn, s);
       dot_any<R>(vn, vn, N, w.partial, w.scal + kRR, s);
       const double hn = std::sqrt(fetch(op, w, w.scal + kRR));
       dev_axpby<R>(N, 0.0, vn, hn > 0 ? 1.0 / hn : 0.0, vn, s);

@@ -142,38 +142,6 @@ __global__ void __launch_bounds__(kRedThreads) mdot_partial_kernel(const R *V, l
   }
 }
 
-// w -= sum_k h[k] V_k (as mgs_update_kernel) and the partial dots V_k . w of
-// the updated w (as mdot_partial_kernel): the two halves of consecutive
-// Gram-Schmidt passes in one sweep over the basis (m <= kFusedMdot); the
-// second read of V_k[i] comes from L1
-constexpr int kFusedMdot = 32;
-template <typename R>
-__global__ void __launch_bounds__(kRedThreads) mgs_update_mdot_kernel(const R *V, long n, int m, const double *h,
-                                                                      R *w, double *partial)
-{
-  double acc[kFusedMdot];
-#pragma unroll
-  for (int u = 0; u < kFusedMdot; ++u) acc[u] = 0.0;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    double s = (double)w[i];
-#pragma unroll
-    for (int u = 0; u < kFusedMdot; ++u)
-      if (u < m) s -= h[u] * (double)V[(long)u * n + i];
-    const R wr = (R)s;
-    w[i] = wr;
-    const double wd = (double)wr;
-#pragma unroll
-    for (int u = 0; u < kFusedMdot; ++u)
-      if (u < m) acc[u] += (double)V[(long)u * n + i] * wd;
-  }
-#pragma unroll
-  for (int u = 0; u < kFusedMdot; ++u)
-    if (u < m) {  // block-uniform
-      const double t = block_sum(acc[u]);
-      if (threadIdx.x == 0) partial[(long)u * kRedBlocks + blockIdx.x] = t;
-    }
-}
-
 // w -= sum_k h[k] V_k
 template <typename R>
 __global__ void mgs_update_kernel(const R *V, long n, int m, const double *h, R *w)
@@ -456,22 +424,6 @@ void dev_mdot(const R *V, long n, int m, const R *w, double *partial, double *ou
 }
 template void dev_mdot<double>(const double *, long, int, const double *, double *, double *, cudaStream_t);
 template void dev_mdot<float>(const float *, long, int, const float *, double *, double *, cudaStream_t);
-
-template <typename R>
-bool dev_mgs_update_mdot(const R *V, long n, int m, const double *h, R *w, double *partial, double *out,
-                         cudaStream_t s)
-{
-  if (m > kFusedMdot) return false;
-  mgs_update_mdot_kernel<R><<<kRedBlocks, kRedThreads, 0, s>>>(V, n, m, h, w, partial);
-  MPDG_LAUNCHED();
-  finish_kernel<<<m, kRedThreads, 0, s>>>(partial, m, out, 0);
-  MPDG_LAUNCHED();
-  return true;
-}
-template bool dev_mgs_update_mdot<double>(const double *, long, int, const double *, double *, double *, double *,
-                                          cudaStream_t);
-template bool dev_mgs_update_mdot<float>(const float *, long, int, const double *, float *, double *, double *,
-                                         cudaStream_t);
 
 template <typename R>
 void dev_mgs_update(const R *V, long n, int m, const double *h, R *w, cudaStream_t s)

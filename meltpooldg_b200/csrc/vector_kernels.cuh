@@ -22,10 +22,7 @@ template <typename R>
 void dev_mdot(const R *V, long n, int m, const R *w, double *partial, double *out, cudaStream_t s);
 template <typename R>
 void dev_mgs_update(const R *V, long n, int m, const double *h, R *w, cudaStream_t s);
-// w -= V h, then out = V^T w, in one sweep over V (false: m too large, nothing done)
-template <typename R>
-bool dev_mgs_update_mdot(const R *V, long n, int m, const double *h, R *w, double *partial, double *out,
-                         cudaStream_t s);
+
 template <typename R>
 void dev_combine(const R *V, long n, int m, const double *y, R *x, cudaStream_t s);
 template <typename R>
