@@ -2640,16 +2640,21 @@ void launch_fine_block(Op &op, Real *dst, const Real *src)
   Mesh &m = *op.mesh;
   const bool mask = op.use_dirichlet && m.has_dirichlet;
   f.use_dirichlet = op.use_dirichlet;
-  f.stream = op.stream;  // the fine block runs in the apply's stream (or its capture)
+  // the fine block runs in the apply's stream, which may be a capture stream
+  // that is destroyed after the capture: the fine op's own stream comes back
+  const cudaStream_t fine_stream = f.stream;
+  f.stream = op.stream;
   f.hang_src = src;
   f.hang_mask = mask ? m.d_dmask : nullptr;
   try {
     launch_cells<Real>(f, dst + m.N_own, src + m.N_own);
   } catch (...) {
     f.hang_src = nullptr;
+    f.stream = fine_stream;
     throw;
   }
   f.hang_src = nullptr;
+  f.stream = fine_stream;
   const Mesh &fm = *f.mesh;
   const long cnt = m.NY * m.NZ;
   hang_fold_kernel<Real><<<grid_for(cnt, 256), 256, 0, op.stream>>>(

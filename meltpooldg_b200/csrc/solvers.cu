@@ -367,8 +367,8 @@ void dot_any(const R *a, const R *b, long n, double *partial, double *out, cudaS
   else dev_dot_f(a, b, n, partial, out, s);
 }
 
-// right-preconditioned restarted GMRES (classical Gram-Schmidt applied twice),
-// vectors in R, Hessenberg and dot products in FP64
+// right-preconditioned restarted GMRES (classical Gram-Schmidt, a second pass
+// only when the first cancelled more than half of |w|^2), vectors in R, Hessenberg and dot products in FP64
 template <typename R>
 int gmres(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero, double rel_tol,
           double abs_tol, int max_it, int restart, int &iters, double &res0, double &res,
@@ -423,15 +423,27 @@ int gmres(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero,
       prec_apply<R>(op, P, v, vj, v.z, applies);
       launch_apply<R>(op, vn, v.z);
       ++applies;
-      // two passes of classical Gram-Schmidt
+      // classical Gram-Schmidt, repeated once when the projection removed
+      // more than half of |w|^2 (the Daniel-Gragg-Kaufman-Stewart test with
+      // eta = 1/sqrt(2)): the first pass's dots include w.w (basis column
+      // j+1 is w), and |w - V h|^2 = w.w - h.h for an orthonormal V
       for (int k = 0; k <= j; ++k) h[k] = 0.0;
       for (int pass = 0; pass < 2; ++pass) {
-        dev_mdot<R>(VB, N, j + 1, vn, w.partial, w.scal + kNScalars, s);
-        MPDG_CUDA(cudaMemcpyAsync(w.host, w.scal + kNScalars, sizeof(double) * (j + 1),
+        const int cnt = pass == 0 ? j + 2 : j + 1;
+        dev_mdot<R>(VB, N, cnt, vn, w.partial, w.scal + kNScalars, s);
+        MPDG_CUDA(cudaMemcpyAsync(w.host, w.scal + kNScalars, sizeof(double) * cnt,
                                   cudaMemcpyDeviceToHost, s));
         MPDG_CUDA(cudaStreamSynchronize(s));
-        for (int k = 0; k <= j; ++k) h[k] += w.host[k];
+        double hh = 0.0;
+        for (int k = 0; k <= j; ++k) {
+          h[k] += w.host[k];
+          hh += w.host[k] * w.host[k];
+        }
         dev_mgs_update<R>(VB, N, j + 1, w.scal + kNScalars, vn, s);
+        if (pass == 0) {
+          const double ww = w.host[j + 1];
+          if (std::isfinite(ww) && ww - hh > 0.5 * ww) break;
+        }
       }
       dot_any<R>(vn, vn, N, w.partial, w.scal + kRR, s);
       const double hn = std::sqrt(fetch(op, w, w.scal + kRR));
