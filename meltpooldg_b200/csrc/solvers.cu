@@ -28,8 +28,8 @@ struct Workspace {
   int V_cols = 0;
   float *V32 = nullptr;  // GMRES basis (FP32 inner solves)
   int V32_cols = 0;
-  double *partial = nullptr;  // reduction partials: 64 groups of kRedBlocks
-  double *scal = nullptr;     // device scalars (kNScalars) + GMRES h (64)
+  double *partial = nullptr;  // reduction partials: 128 groups of kRedBlocks
+  double *scal = nullptr;     // device scalars (kNScalars) + GMRES dots (128)
   double *host = nullptr;     // pinned host mirror
   bool invd_valid = false;
   size_t bytes = 0;
@@ -61,9 +61,9 @@ Workspace &ws64(Op &op)
     w.invd = walloc<double>(w, N);
     w.cd = walloc<double>(w, N);
     w.ct = walloc<double>(w, N);
-    w.partial = walloc<double>(w, 64L * kRedBlocks);
-    w.scal = walloc<double>(w, kNScalars + 64);
-    MPDG_CUDA(tracked_malloc_host(&w.host, sizeof(double) * (kNScalars + 64)));
+    w.partial = walloc<double>(w, 128L * kRedBlocks);
+    w.scal = walloc<double>(w, kNScalars + 128);
+    MPDG_CUDA(tracked_malloc_host(&w.host, sizeof(double) * (kNScalars + 128)));
   }
   return w;
 }
@@ -367,8 +367,24 @@ void dot_any(const R *a, const R *b, long n, double *partial, double *out, cudaS
   else dev_dot_f(a, b, n, partial, out, s);
 }
 
-// right-preconditioned restarted GMRES (classical Gram-Schmidt, a second pass
-// only when the first cancelled more than half of |w|^2), vectors in R, Hessenberg and dot products in FP64
+// Right-preconditioned restarted GMRES, vectors in R, Hessenberg and dot
+// products in FP64.  The Arnoldi basis is orthogonalised by delayed classical
+// Gram-Schmidt with re-orthogonalisation (DCGS2: Swirydowicz, Langou,
+// Ananthan, Yang and Thomas, "Low synchronization Gram-Schmidt and generalized
+// minimal residual algorithms", Numer. Linear Algebra Appl. 28, 2021).  Step j
+// holds q_0..q_{j-1} final and u_j, the once-projected candidate for q_j:
+//   w = B u_j                               (B = A M^-1; one apply)
+//   s = Q_{j-1}^T u_j, t = u_j.u_j, z = Q_{j-1}^T w, y = u_j.w   (one pass)
+//   alpha = |u_j - Q_{j-1} s| = sqrt(t - s.s)
+//   column j-1 of H gets + s and alpha below the diagonal: its Givens
+//   rotation gives the residual estimate of step j-1
+//   c = Q_j^T w / alpha (q_j.w = (y - s.z) / alpha)
+//   H[:, j] = c - H_{j-1} s / alpha   (B Q_{j-1} = Q_j H_{j-1})
+//   q_j = (u_j - Q_{j-1} s) / alpha, u_{j+1} = w / alpha - Q_j c   (one sweep)
+// which is two passes of classical Gram-Schmidt with the second pass of each
+// vector made in the next step: one read of the basis for the dots and one for
+// the update per iteration, and one host round trip.  The residual estimate
+// lags by one apply, so each cycle applies B once more than it iterates.
 template <typename R>
 int gmres(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero, double rel_tol,
           double abs_tol, int max_it, int restart, int &iters, double &res0, double &res,
@@ -385,7 +401,10 @@ int gmres(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero,
     VB = walloc<R>(w, (size_t)N * (m + 1));
     *cols = m + 1;
   }
-  std::vector<double> H((m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), y(m), h(m + 1);
+  // H: the Arnoldi Hessenberg; Hr: its Givens-rotated copy (least squares)
+  std::vector<double> H((m + 1) * m, 0.0), Hr((m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), y(m);
+  DcgsCoef cf;
+  double *dsc = w.scal + kNScalars;
   iters = 0;
   double tol = -1.0;
   int status = MPDG_ERR_NOT_CONVERGED;
@@ -415,72 +434,91 @@ int gmres(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero,
     if (iters >= max_it) break;
     dev_axpby<R>(N, 0.0, VB, 1.0 / beta, VB, s);
     std::fill(g.begin(), g.end(), 0.0);
+    std::fill(H.begin(), H.end(), 0.0);
     g[0] = beta;
-    int j = 0;
+    const int it0 = iters;
+    int k = 0;  // final columns of this cycle
     bool done = false;
-    for (; j < m && iters < max_it; ++j) {
-      R *vj = VB + (long)j * N, *vn = VB + (long)(j + 1) * N;
-      prec_apply<R>(op, P, v, vj, v.z, applies);
-      launch_apply<R>(op, vn, v.z);
-      ++applies;
-      // classical Gram-Schmidt, repeated once when the projection removed
-      // more than half of |w|^2 (the Daniel-Gragg-Kaufman-Stewart test with
-      // eta = 1/sqrt(2)): the first pass's dots include w.w (basis column
-      // j+1 is w), and |w - V h|^2 = w.w - h.h for an orthonormal V
-      for (int k = 0; k <= j; ++k) h[k] = 0.0;
-      for (int pass = 0; pass < 2; ++pass) {
-        const int cnt = pass == 0 ? j + 2 : j + 1;
-        dev_mdot<R>(VB, N, cnt, vn, w.partial, w.scal + kNScalars, s);
-        MPDG_CUDA(cudaMemcpyAsync(w.host, w.scal + kNScalars, sizeof(double) * cnt,
-                                  cudaMemcpyDeviceToHost, s));
-        MPDG_CUDA(cudaStreamSynchronize(s));
-        double hh = 0.0;
-        for (int k = 0; k <= j; ++k) {
-          h[k] += w.host[k];
-          hh += w.host[k] * w.host[k];
+    for (int j = 0;; ++j) {
+      R *uj = VB + (long)j * N, *wn = VB + (long)(j + 1) * N;
+      // no further apply once the cycle or the iteration budget is full: the
+      // step only completes column j-1
+      const bool last = j == m || it0 + j >= max_it;
+      if (!last) {
+        prec_apply<R>(op, P, v, uj, v.z, applies);
+        launch_apply<R>(op, wn, v.z);
+        ++applies;
+      }
+      dev_mdot2<R>(VB, N, j + 1, uj, last ? nullptr : wn, w.partial, dsc, s);
+      const int cnt = last ? j + 1 : 2 * (j + 1);
+      MPDG_CUDA(cudaMemcpyAsync(w.host, dsc, sizeof(double) * cnt, cudaMemcpyDeviceToHost, s));
+      MPDG_CUDA(cudaStreamSynchronize(s));
+      const double *hs = w.host, *hz = w.host + (j + 1);
+      double ss = 0.0, sz = 0.0;
+      for (int i = 0; i < j; ++i) {
+        ss += hs[i] * hs[i];
+        if (!last) sz += hs[i] * hz[i];
+      }
+      const double t = hs[j], a2 = t - ss;
+      if (!std::isfinite(t) || !std::isfinite(a2) || !std::isfinite(sz)) return MPDG_ERR_NAN;
+      const double alpha = a2 > 1e-28 * t ? std::sqrt(a2) : 0.0;
+      if (j > 0) {
+        // column j-1 is final: + s, alpha below the diagonal; its rotation
+        const int jc = j - 1;
+        for (int i = 0; i < j; ++i) H[i * m + jc] += hs[i];
+        H[j * m + jc] = alpha;
+        for (int i = 0; i <= j; ++i) Hr[i * m + jc] = H[i * m + jc];
+        for (int i = 0; i < jc; ++i) {
+          const double a = Hr[i * m + jc], c = Hr[(i + 1) * m + jc];
+          Hr[i * m + jc] = cs[i] * a + sn[i] * c;
+          Hr[(i + 1) * m + jc] = -sn[i] * a + cs[i] * c;
         }
-        dev_mgs_update<R>(VB, N, j + 1, w.scal + kNScalars, vn, s);
-        if (pass == 0) {
-          const double ww = w.host[j + 1];
-          if (std::isfinite(ww) && ww - hh > 0.5 * ww) break;
+        const double a = Hr[jc * m + jc], c = Hr[j * m + jc], rr = std::sqrt(a * a + c * c);
+        cs[jc] = a / rr;
+        sn[jc] = c / rr;
+        Hr[jc * m + jc] = rr;
+        Hr[j * m + jc] = 0.0;
+        g[j] = -sn[jc] * g[jc];
+        g[jc] = cs[jc] * g[jc];
+        ++iters;
+        res = std::fabs(g[j]);
+        if (!std::isfinite(res)) return MPDG_ERR_NAN;
+        if (res <= tol) {
+          k = j;
+          done = true;
+          break;
         }
       }
-      dot_any<R>(vn, vn, N, w.partial, w.scal + kRR, s);
-      const double hn = std::sqrt(fetch(op, w, w.scal + kRR));
-      dev_axpby<R>(N, 0.0, vn, hn > 0 ? 1.0 / hn : 0.0, vn, s);
-      for (int k = 0; k <= j; ++k) H[k * m + j] = h[k];
-      H[(j + 1) * m + j] = hn;
-      for (int k = 0; k < j; ++k) {
-        const double t = cs[k] * H[k * m + j] + sn[k] * H[(k + 1) * m + j];
-        H[(k + 1) * m + j] = -sn[k] * H[k * m + j] + cs[k] * H[(k + 1) * m + j];
-        H[k * m + j] = t;
-      }
-      const double a = H[j * m + j], c = H[(j + 1) * m + j], rr = std::sqrt(a * a + c * c);
-      cs[j] = a / rr;
-      sn[j] = c / rr;
-      H[j * m + j] = rr;
-      H[(j + 1) * m + j] = 0.0;
-      g[j + 1] = -sn[j] * g[j];
-      g[j] = cs[j] * g[j];
-      ++iters;
-      res = std::fabs(g[j + 1]);
-      if (!std::isfinite(res)) return MPDG_ERR_NAN;
-      if (res <= tol) {
-        ++j;
-        done = true;
+      if (last || alpha == 0.0) {
+        k = j;
         break;
       }
+      // column j from the first pass; the sweep makes q_j and u_{j+1}
+      const double ia = 1.0 / alpha;
+      for (int i = 0; i < j; ++i) {
+        cf.s[i] = hs[i];
+        cf.c[i] = hz[i] * ia;
+      }
+      cf.c[j] = (hz[j] - sz) * ia * ia;
+      for (int i = 0; i <= j; ++i) {
+        double hsum = 0.0;
+        for (int l = std::max(0, i - 1); l < j; ++l) hsum += H[i * m + l] * hs[l];
+        H[i * m + j] = cf.c[i] - hsum * ia;
+      }
+      dev_dcgs2_sweep<R>(VB, N, j, ia, cf, s);
     }
-    for (int k = j - 1; k >= 0; --k) {
-      double t = g[k];
-      for (int l = k + 1; l < j; ++l) t -= H[k * m + l] * y[l];
-      y[k] = t / H[k * m + k];
+    if (k > 0) {
+      for (int i = k - 1; i >= 0; --i) {
+        double t = g[i];
+        for (int l = i + 1; l < k; ++l) t -= Hr[i * m + l] * y[l];
+        y[i] = t / Hr[i * m + i];
+      }
+      MPDG_CUDA(cudaMemcpyAsync(dsc, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+      dev_combine<R>(VB, N, k, dsc, v.ct, s);
+      prec_apply<R>(op, P, v, v.ct, v.z, applies);
+      dev_axpby<R>(N, 1.0, v.z, 1.0, x, s);
+      MPDG_CUDA(cudaStreamSynchronize(s));  // y is read from pageable memory
     }
-    MPDG_CUDA(cudaMemcpyAsync(w.scal + kNScalars, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, s));
-    dev_combine<R>(VB, N, j, w.scal + kNScalars, v.ct, s);
-    prec_apply<R>(op, P, v, v.ct, v.z, applies);
-    dev_axpby<R>(N, 1.0, v.z, 1.0, x, s);
-    MPDG_CUDA(cudaStreamSynchronize(s));  // y is read from pageable memory
     if (done) {
       status = MPDG_OK;
       break;

@@ -115,41 +115,77 @@ __global__ void __launch_bounds__(kRedThreads) finish_kernel(const double *parti
   }
 }
 
-// multi-dot: partial[k][block] = V_k . w for k < m  (V rows of stride n), FP64 accumulation
-template <typename R>
-__global__ void __launch_bounds__(kRedThreads) mdot_partial_kernel(const R *V, long n, int m,
-                                                                   const R *w, double *partial)
+// V_k . u and (HAS_W) V_k . w for k0 <= k < k0 + CNT: partial groups k and
+// m + k.  CNT is a compile-time width, so every load of an element's row is
+// issued before the first product that uses one.
+template <typename R, bool HAS_W, int CNT>
+__device__ __forceinline__ void mdot2_chunk(const R *V, long n, int m, int k0, const R *u, const R *w,
+                                            double *partial)
 {
-  // 8 vectors per pass over w (each thread's per-vector sum runs over its
-  // elements in grid-stride order, as one vector at a time would)
-  for (int k0 = 0; k0 < m; k0 += 8) {
-    const int cnt = min(8, m - k0);
-    double s[8];
+  double su[CNT], sw[CNT];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) s[u] = 0.0;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-      const double wi = (double)w[i];
+  for (int c = 0; c < CNT; ++c) su[c] = sw[c] = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double ui = (double)u[i];
+    const double wi = HAS_W ? (double)w[i] : 0.0;
+    double vk[CNT];
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-        if (u < cnt) s[u] += (double)V[(long)(k0 + u) * n + i] * wi;
+    for (int c = 0; c < CNT; ++c) vk[c] = (double)V[(long)(k0 + c) * n + i];
+#pragma unroll
+    for (int c = 0; c < CNT; ++c) {
+      su[c] += vk[c] * ui;
+      if (HAS_W) sw[c] += vk[c] * wi;
     }
+  }
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (u < cnt) {  // block-uniform
-        const double t = block_sum(s[u]);
-        if (threadIdx.x == 0) partial[(long)(k0 + u) * kRedBlocks + blockIdx.x] = t;
-      }
+  for (int c = 0; c < CNT; ++c) {
+    const double t = block_sum(su[c]);
+    if (threadIdx.x == 0) partial[(long)(k0 + c) * kRedBlocks + blockIdx.x] = t;
+    if (HAS_W) {
+      const double t2 = block_sum(sw[c]);
+      if (threadIdx.x == 0) partial[(long)(m + k0 + c) * kRedBlocks + blockIdx.x] = t2;
+    }
   }
 }
 
-// w -= sum_k h[k] V_k
-template <typename R>
-__global__ void mgs_update_kernel(const R *V, long n, int m, const double *h, R *w)
+// V_k . u and (HAS_W) V_k . w for k < m in one pass, 8 basis vectors at a
+// time (u and w are read once per 8)
+template <typename R, bool HAS_W>
+__global__ void __launch_bounds__(kRedThreads, 4) mdot2_partial_kernel(const R *V, long n, int m, const R *u,
+                                                                    const R *w, double *partial)
 {
+  for (int k0 = 0; k0 < m; k0 += 8) {
+    switch (min(8, m - k0)) {
+      case 8: mdot2_chunk<R, HAS_W, 8>(V, n, m, k0, u, w, partial); break;
+      case 7: mdot2_chunk<R, HAS_W, 7>(V, n, m, k0, u, w, partial); break;
+      case 6: mdot2_chunk<R, HAS_W, 6>(V, n, m, k0, u, w, partial); break;
+      case 5: mdot2_chunk<R, HAS_W, 5>(V, n, m, k0, u, w, partial); break;
+      case 4: mdot2_chunk<R, HAS_W, 4>(V, n, m, k0, u, w, partial); break;
+      case 3: mdot2_chunk<R, HAS_W, 3>(V, n, m, k0, u, w, partial); break;
+      case 2: mdot2_chunk<R, HAS_W, 2>(V, n, m, k0, u, w, partial); break;
+      default: mdot2_chunk<R, HAS_W, 1>(V, n, m, k0, u, w, partial); break;
+    }
+  }
+}
+
+// One sweep of delayed classical Gram-Schmidt over the basis columns 0..j+1:
+//   q_j     = (V_j - sum_{k<j} s_k V_k) / alpha          (written over V_j)
+//   u_{j+1} = V_{j+1} / alpha - sum_{k<j} c_k V_k - c_j q_j   (over V_{j+1})
+// V_{j+1} holds w = B u_j on entry; s and c come as kernel parameters.
+template <typename R>
+__global__ void dcgs2_sweep_kernel(R *V, long n, int j, double inv_alpha, const DcgsCoef cf)
+{
+  R *vj = V + (long)j * n, *vn = V + (long)(j + 1) * n;
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    double s = (double)w[i];
-    for (int k = 0; k < m; ++k) s -= h[k] * (double)V[(long)k * n + i];
-    w[i] = (R)s;
+    double q = (double)vj[i], u = (double)vn[i] * inv_alpha;
+    for (int k = 0; k < j; ++k) {
+      const double vk = (double)V[(long)k * n + i];
+      q -= cf.s[k] * vk;
+      u -= cf.c[k] * vk;
+    }
+    const R qr = (R)(q * inv_alpha);
+    vj[i] = qr;
+    vn[i] = (R)(u - cf.c[j] * (double)qr);
   }
 }
 
@@ -415,24 +451,30 @@ void dev_linf(const double *a, long n, double *partial, double *out, cudaStream_
 }
 
 template <typename R>
-void dev_mdot(const R *V, long n, int m, const R *w, double *partial, double *out, cudaStream_t s)
+void dev_mdot2(const R *V, long n, int m, const R *u, const R *w, double *partial, double *out, cudaStream_t s)
 {
-  mdot_partial_kernel<R><<<kRedBlocks, kRedThreads, 0, s>>>(V, n, m, w, partial);
+  if (w)
+    mdot2_partial_kernel<R, true><<<kRedBlocks, kRedThreads, 0, s>>>(V, n, m, u, w, partial);
+  else
+    mdot2_partial_kernel<R, false><<<kRedBlocks, kRedThreads, 0, s>>>(V, n, m, u, w, partial);
   MPDG_LAUNCHED();
-  finish_kernel<<<m, kRedThreads, 0, s>>>(partial, m, out, 0);
+  const int groups = w ? 2 * m : m;
+  finish_kernel<<<groups, kRedThreads, 0, s>>>(partial, groups, out, 0);
   MPDG_LAUNCHED();
 }
-template void dev_mdot<double>(const double *, long, int, const double *, double *, double *, cudaStream_t);
-template void dev_mdot<float>(const float *, long, int, const float *, double *, double *, cudaStream_t);
+template void dev_mdot2<double>(const double *, long, int, const double *, const double *, double *, double *,
+                                cudaStream_t);
+template void dev_mdot2<float>(const float *, long, int, const float *, const float *, double *, double *,
+                               cudaStream_t);
 
 template <typename R>
-void dev_mgs_update(const R *V, long n, int m, const double *h, R *w, cudaStream_t s)
+void dev_dcgs2_sweep(R *V, long n, int j, double inv_alpha, const DcgsCoef &cf, cudaStream_t s)
 {
-  mgs_update_kernel<R><<<vgrid(n), 256, 0, s>>>(V, n, m, h, w);
+  dcgs2_sweep_kernel<R><<<vgrid(n), 256, 0, s>>>(V, n, j, inv_alpha, cf);
   MPDG_LAUNCHED();
 }
-template void dev_mgs_update<double>(const double *, long, int, const double *, double *, cudaStream_t);
-template void dev_mgs_update<float>(const float *, long, int, const double *, float *, cudaStream_t);
+template void dev_dcgs2_sweep<double>(double *, long, int, double, const DcgsCoef &, cudaStream_t);
+template void dev_dcgs2_sweep<float>(float *, long, int, double, const DcgsCoef &, cudaStream_t);
 
 template <typename R>
 void dev_combine(const R *V, long n, int m, const double *y, R *x, cudaStream_t s)

@@ -18,10 +18,18 @@ enum { kDONE = 4, kCONV = 5, kRRCONV = 6, kTOL = 7 };
 void dev_dot(const double *a, const double *b, long n, double *partial, double *out, cudaStream_t s);
 void dev_dot_f(const float *a, const float *b, long n, double *partial, double *out, cudaStream_t s);
 void dev_linf(const double *a, long n, double *partial, double *out, cudaStream_t s);
+// delayed classical Gram-Schmidt (GMRES): the dots V_k.u and, when w is given,
+// V_k.w for k < m (out[k], out[m + k]), one pass over the basis
 template <typename R>
-void dev_mdot(const R *V, long n, int m, const R *w, double *partial, double *out, cudaStream_t s);
+void dev_mdot2(const R *V, long n, int m, const R *u, const R *w, double *partial, double *out, cudaStream_t s);
+// coefficients of one sweep, passed by value (restart length <= 60)
+struct DcgsCoef {
+  double s[64];
+  double c[64];
+};
+// q_j = (V_j - V s) / alpha over V_j; V_{j+1} = V_{j+1} / alpha - V c - c_j q_j
 template <typename R>
-void dev_mgs_update(const R *V, long n, int m, const double *h, R *w, cudaStream_t s);
+void dev_dcgs2_sweep(R *V, long n, int j, double inv_alpha, const DcgsCoef &cf, cudaStream_t s);
 
 template <typename R>
 void dev_combine(const R *V, long n, int m, const double *y, R *x, cudaStream_t s);
