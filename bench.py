@@ -715,6 +715,16 @@ def run_batch(args, rank, world):
             "kernel": f"batch_apply_kernel<float> x 8 colour launches over all {len(probs)} problems",
             "apply_ms": apply_ms, "autotuned_shape": shape,
             "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
+    # box cells move ~8 bytes per DoF: the apply is bound by its arithmetic
+    # (Cartesian heat cells: E (24 n^4 + 20 n^3) per problem), as the
+    # single-problem applies of the same degrees are
+    _, f32_peak = fma_peaks(M)
+    f_apply = float(sum(p.nc ** 3 * (24 * (p.degree + 1) ** 4 + 20 * (p.degree + 1) ** 3) for p in probs))
+    roof["flops"] = {"per_apply": f_apply, "unit": "GFLOP/s",
+                     "fp32": {"achieved": f_apply / (apply_ms * 1e-3) / 1e9, "peak": f32_peak,
+                              "frac": f_apply / (apply_ms * 1e-3) / 1e9 / f32_peak},
+                     "dofs_per_s": N_total / (apply_ms * 1e-3),
+                     "peak_source": "mpdg_fma_peak: FMA chains measured on this GPU (8 per thread, 8 CTAs per SM)"}
     cpu = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_batch_rate(probs, its64, args.cpu_seconds)
