@@ -848,31 +848,12 @@ __global__ void __launch_bounds__(128) cell_kernel(const KP<Real> p)
 // components), each a product of squared/mixed 1D tables: the same entries
 // MatrixFreeTools::compute_diagonal extracts by unit-vector sweeps.
 
-template <int n, typename Real>
-__device__ __forceinline__ void diag_term(Real *t, int i, int j, const Real (&F)[n],
-                                          const Real *Ax, const Real *Ay, const Real *Az,
-                                          Real (&acc)[n])
-{
-  Real a[n], b[n];
-  cz<n, Real, true>(Az, F, a);
-  put<n>(t, i, j, a);
-  __syncthreads();
-  cy<n, Real, true>(Ay, t, i, j, b);
-  __syncthreads();
-  put<n>(t, i, j, b);
-  __syncthreads();
-  cx<n, Real, true>(Ax, t, i, j, a);
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < n; ++k) acc[k] += a[k];
-}
-
 template <int P, int GEOM, bool KT>
 __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
 {
   using Real = double;
   constexpr int n = P + 1, n2 = n * n, n3 = n2 * n, CPB = Cfg<n>::cpb;
-  __shared__ Real sm[CPB][n3];
+  __shared__ Real sm[6][CPB][n3];  // one tile per term group of the y sweep
   __shared__ Real tb[5][n2];  // S^2, D^2, S*D, S, Dc
   const Tables<Real> &T = tab<Real>(P);
   const int tid = threadIdx.x, slot = threadIdx.y;
@@ -907,7 +888,7 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
   // cells of a mapped mesh that touch a constrained DoF get their diagonal share
   // from their element matrices (skip_constrained)
   const bool wr = active && !(p.skip_constrained && p.cell_flags && (p.cell_flags[cell] & 2));
-  Real *t = sm[slot];
+  Real *t = sm[0][slot];
 
   Real Tq[n], Tgx[n], Tgy[n], Tgz[n];
   if (KT) {
@@ -993,20 +974,71 @@ __global__ void __launch_bounds__(128) diag_kernel(const KP<double> p)
     Fb1[k] = e1;
     Fb2[k] = e2;
   }
-  Real acc[n];
+  // The terms grouped by their (x, y) tables: a group's z contractions are
+  // summed in registers, and the y contractions of the groups that share an x
+  // table are summed before the one x contraction of each x table.  Groups:
+  // 0 (S2,S2): mass, F22, b2   1 (D2,S2): F00   2 (S2,D2): F11
+  // 3 (SD,S2): b0, F02         4 (S2,SD): b1, F12   5 (SD,SD): F01
+  constexpr int NG = GEOM == GEOM_GENERAL ? 6 : 5;
+  {
+    Real g[NG][n], a[n];
+    cz<n, Real, true>(SS, Fm, g[0]);
+    cz<n, Real, true>(DD, F22, a);
 #pragma unroll
-  for (int k = 0; k < n; ++k) acc[k] = 0;
-  diag_term<n>(t, i, j, Fm, SS, SS, SS, acc);
-  diag_term<n>(t, i, j, F00, DD, SS, SS, acc);
-  diag_term<n>(t, i, j, F11, SS, DD, SS, acc);
-  diag_term<n>(t, i, j, F22, SS, SS, DD, acc);
-  diag_term<n>(t, i, j, Fb0, SD, SS, SS, acc);
-  diag_term<n>(t, i, j, Fb1, SS, SD, SS, acc);
-  diag_term<n>(t, i, j, Fb2, SS, SS, SD, acc);
-  if (GEOM == GEOM_GENERAL) {
-    diag_term<n>(t, i, j, F01, SD, SD, SS, acc);
-    diag_term<n>(t, i, j, F02, SD, SS, SD, acc);
-    diag_term<n>(t, i, j, F12, SS, SD, SD, acc);
+    for (int k = 0; k < n; ++k) g[0][k] += a[k];
+    cz<n, Real, true>(SD, Fb2, a);
+#pragma unroll
+    for (int k = 0; k < n; ++k) g[0][k] += a[k];
+    cz<n, Real, true>(SS, F00, g[1]);
+    cz<n, Real, true>(SS, F11, g[2]);
+    cz<n, Real, true>(SS, Fb0, g[3]);
+    cz<n, Real, true>(SS, Fb1, g[4]);
+    if constexpr (GEOM == GEOM_GENERAL) {
+      cz<n, Real, true>(SD, F02, a);
+#pragma unroll
+      for (int k = 0; k < n; ++k) g[3][k] += a[k];
+      cz<n, Real, true>(SD, F12, a);
+#pragma unroll
+      for (int k = 0; k < n; ++k) g[4][k] += a[k];
+      cz<n, Real, true>(SS, F01, g[NG - 1]);
+    }
+    __syncthreads();  // the tiles of the quadrature-point interpolations are free
+#pragma unroll
+    for (int gi = 0; gi < NG; ++gi) put<n>(sm[gi][slot], i, j, g[gi]);
+  }
+  __syncthreads();
+  Real xs[3][n];  // by x table: S2, D2, SD
+  {
+    Real b[n];
+    cy<n, Real, true>(SS, sm[0][slot], i, j, xs[0]);
+    cy<n, Real, true>(DD, sm[2][slot], i, j, b);
+#pragma unroll
+    for (int k = 0; k < n; ++k) xs[0][k] += b[k];
+    cy<n, Real, true>(SD, sm[4][slot], i, j, b);
+#pragma unroll
+    for (int k = 0; k < n; ++k) xs[0][k] += b[k];
+    cy<n, Real, true>(SS, sm[1][slot], i, j, xs[1]);
+    cy<n, Real, true>(SS, sm[3][slot], i, j, xs[2]);
+    if constexpr (GEOM == GEOM_GENERAL) {
+      cy<n, Real, true>(SD, sm[NG - 1][slot], i, j, b);
+#pragma unroll
+      for (int k = 0; k < n; ++k) xs[2][k] += b[k];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int gi = 0; gi < 3; ++gi) put<n>(sm[gi][slot], i, j, xs[gi]);
+  __syncthreads();
+  Real acc[n];
+  {
+    Real b[n];
+    cx<n, Real, true>(SS, sm[0][slot], i, j, acc);
+    cx<n, Real, true>(DD, sm[1][slot], i, j, b);
+#pragma unroll
+    for (int k = 0; k < n; ++k) acc[k] += b[k];
+    cx<n, Real, true>(SD, sm[2][slot], i, j, b);
+#pragma unroll
+    for (int k = 0; k < n; ++k) acc[k] += b[k];
   }
   if (wr) {
 #pragma unroll
