@@ -514,8 +514,9 @@ int gmres(Op &op, Workspace &w, const Prec &P, const R *b, R *x, bool x_is_zero,
         y[i] = t / Hr[i * m + i];
       }
       MPDG_CUDA(cudaMemcpyAsync(dsc, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
-      dev_combine<R>(VB, N, k, dsc, v.ct, s);
-      prec_apply<R>(op, P, v, v.ct, v.z, applies);
+      // V y into p: the Chebyshev smoother keeps its A z in ct
+      dev_combine<R>(VB, N, k, dsc, v.p, s);
+      prec_apply<R>(op, P, v, v.p, v.z, applies);
       dev_axpby<R>(N, 1.0, v.z, 1.0, x, s);
       MPDG_CUDA(cudaStreamSynchronize(s));  // y is read from pageable memory
     }
@@ -680,12 +681,13 @@ int solve(Op &op, const mpdg_solver_desc &d, double *x, const double *b, mpdg_so
         break;
       }
       // unit-norm FP32 defect, FP32 correction, FP64 update
-      dev_scale_copy<float>(N, 1.0 / res, w.r, w32.z32, s);
+      dev_scale_copy<float>(N, 1.0 / res, w.r, w32.r32, s);
       MPDG_CUDA(cudaMemsetAsync(w32.x32, 0, sizeof(float) * N, s));
       int it = 0;
       double r0i = 0, ri = 0;
-      // the inner CG reads its rhs from z32 (copied into r32 by pcg)
-      int st = gmres<float>(op, w32, P, w32.z32, w32.x32, true, inner, 0.0,
+      // the inner GMRES reads its rhs from r32, which it uses for nothing else
+      // (z32 holds the preconditioner's output)
+      int st = gmres<float>(op, w32, P, w32.r32, w32.x32, true, inner, 0.0,
                             std::max(1, max_it - total), d.gmres_restart > 0 ? d.gmres_restart : 30,
                             it, r0i, ri, applies);
       total += it;

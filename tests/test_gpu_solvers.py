@@ -53,6 +53,60 @@ def test_gmres_advdiff_matches_oracle(cuda):
     assert abs(it - it_o) <= 2
 
 
+def _advdiff_system(nc=(6, 6, 6), p=2):
+    import meltpooldg_b200 as M
+    mask = M.boundary_mask(nc, p, faces=[(0, 0)])
+    gm, om = meshes(nc, p, 0.1, seed=9, mask=mask, lo=(-1, -1, -1), hi=(1, 1, 1))
+    b = rng(2).uniform(-1, 1, gm.n_dofs)
+    b[mask == 1] = 0.0
+    oop = O.Operator(O.ADVDIFF, 1e-2, theta=0.5, diffusivity=1e-2, vel_kind=O.VEL_VORTEX, dirichlet=mask)
+    return gm, om, b, oop
+
+
+@pytest.mark.parametrize("restart", [2, 5])
+@pytest.mark.parametrize("mixed", [False, True])
+def test_gmres_restarted_matches_oracle(cuda, restart, mixed):
+    """Restart cycles: each ends with the step that only completes the last
+    Hessenberg column (no apply), then a fresh residual."""
+    import torch
+    import meltpooldg_b200 as M
+    gm, om, b, oop = _advdiff_system()
+    inv = O.inverse_diagonal(om, oop)
+    xo, it_o, _, ok = O.gmres(om, oop, b, inv_diag=inv, rel_tol=1e-10, restart=restart)
+    assert ok
+    op = M.AdvectionDiffusionOperator(gm, 1e-2, theta=0.5, diffusivity=1e-2, velocity="vortex",
+                                      precisions=("fp64", "fp32") if mixed else ("fp64",))
+    x = torch.zeros(gm.n_dofs, dtype=torch.float64, device="cuda")
+    it = M.LinearSolver.solve(op, x, dev(b), M.LinearSolverData(rel_tolerance=1e-10, gmres_restart=restart,
+                                                                mixed_precision=mixed))
+    rep = M.LinearSolver.last_report
+    assert rep["final_residual"] <= 1e-10 * rep["initial_residual"]
+    assert relerr(x.cpu().numpy(), xo) < (1e-7 if mixed else 1e-8)
+    if not mixed:
+        assert abs(it - it_o) <= 2, (it, it_o)
+    # the true residual under the oracle's operator
+    r = b - O.vmult(om, oop, x.cpu().numpy())
+    assert np.linalg.norm(r) <= 2e-10 * np.linalg.norm(b)
+
+
+def test_gmres_iteration_limit_inside_a_cycle(cuda):
+    """max_iterations that ends a restart cycle early: NOT_CONVERGED after
+    exactly that many iterations, with the solution updated from them."""
+    import torch
+    import meltpooldg_b200 as M
+    from meltpooldg_b200._capi import NoConvergence
+    gm, om, b, oop = _advdiff_system()
+    op = M.AdvectionDiffusionOperator(gm, 1e-2, theta=0.5, diffusivity=1e-2, velocity="vortex")
+    x = torch.zeros(gm.n_dofs, dtype=torch.float64, device="cuda")
+    with pytest.raises(NoConvergence):
+        M.LinearSolver.solve(op, x, dev(b), M.LinearSolverData(rel_tolerance=1e-14, gmres_restart=3,
+                                                               max_iterations=7))
+    rep = M.LinearSolver.last_report
+    assert rep["iterations"] == 7
+    r = b - O.vmult(om, oop, x.cpu().numpy())
+    assert np.linalg.norm(r) < np.linalg.norm(b)
+
+
 def _c2_like(nc, p):
     """Config 2 shape at a small size: perturbed vertices (10% h, seed 2),
     T ~ U[300,3000] (seed 3), k = k0 (1 + 1e-3 T), Dirichlet on all faces."""
@@ -93,6 +147,28 @@ def test_chebyshev_cg_and_mixed_precision(cuda):
     x3 = torch.zeros_like(x64)
     M.LinearSolver.solve(op, x3, dev(b), data2)
     assert relerr(x3.cpu().numpy(), x64.cpu().numpy()) < 1e-8
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_gmres_chebyshev_restarted(cuda, mixed):
+    """GMRES with the Chebyshev smoother as its right preconditioner, over
+    several restart cycles: each cycle's correction V y goes through the
+    smoother, whose own scratch vectors must not hold it."""
+    import torch
+    import meltpooldg_b200 as M
+    gm, om, mask, T, xs, oop, b = _c2_like((6, 6, 6), 3)
+    op = M.HeatDiffuseOperator(gm, 1e-3, k0=1.0, k_alpha=1e-3, precisions=("fp64", "fp32"))
+    op.set_temperature(dev(T))
+    data = M.LinearSolverData(solver_type="GMRES", preconditioner_type="Chebyshev", rel_tolerance=1e-10,
+                              abs_tolerance=1e-20, gmres_restart=3, mixed_precision=mixed)
+    x = torch.zeros(gm.n_dofs, dtype=torch.float64, device="cuda")
+    it = M.LinearSolver.solve(op, x, dev(b), data)
+    rep = M.LinearSolver.last_report
+    assert rep["final_residual"] <= 1e-10 * rep["initial_residual"], rep
+    assert it > 3  # more than one cycle
+    r = b - O.vmult(om, oop, x.cpu().numpy())
+    assert np.linalg.norm(r) <= 2e-10 * np.linalg.norm(b)
+    assert relerr(x.cpu().numpy(), xs) < 1e-7
 
 
 def test_solver_failure_modes_are_reported(cuda):
