@@ -149,6 +149,44 @@ def test_chebyshev_cg_and_mixed_precision(cuda):
     assert relerr(x3.cpu().numpy(), x64.cpu().numpy()) < 1e-8
 
 
+@pytest.mark.parametrize("solver", ["CG", "GMRES"])
+@pytest.mark.parametrize("mixed", [False, True])
+def test_solves_from_a_nonzero_initial_guess(cuda, solver, mixed):
+    """The Newton loop starts each solve from the previous increment: the
+    relative tolerance is taken against the residual of that start (deal.II
+    ReductionControl), as in the oracle started from the same vector."""
+    import torch
+    import meltpooldg_b200 as M
+    if solver == "CG":
+        gm, om, mask, T, xs, oop, b = _c2_like((6, 6, 6), 2)
+        op = M.HeatDiffuseOperator(gm, 1e-3, k0=1.0, k_alpha=1e-3, precisions=("fp64", "fp32"))
+        op.set_temperature(dev(T))
+    else:
+        gm, om, b, oop = _advdiff_system()
+        mask = M.boundary_mask((6, 6, 6), 2, faces=[(0, 0)])
+        op = M.AdvectionDiffusionOperator(gm, 1e-2, theta=0.5, diffusivity=1e-2, velocity="vortex",
+                                          precisions=("fp64", "fp32"))
+    x0 = rng(21).uniform(-1, 1, gm.n_dofs)
+    x0[np.asarray(mask) == 1] = 0.0
+    inv = O.inverse_diagonal(om, oop)
+    if solver == "CG":
+        xo, it_o, _, ok = O.cg(om, oop, b, x0=x0, inv_diag=inv, rel_tol=1e-10, abs_tol=1e-20)
+    else:
+        xo, it_o, _, ok = O.gmres(om, oop, b, x0=x0, inv_diag=inv, rel_tol=1e-10, restart=5)
+    assert ok
+    x = dev(x0.copy())
+    it = M.LinearSolver.solve(op, x, dev(b), M.LinearSolverData(solver_type=solver, rel_tolerance=1e-10,
+                                                                abs_tolerance=1e-20, gmres_restart=5,
+                                                                mixed_precision=mixed))
+    rep = M.LinearSolver.last_report
+    r0 = np.linalg.norm(b - O.vmult(om, oop, x0))
+    assert abs(rep["initial_residual"] - r0) <= 1e-12 * r0
+    assert rep["final_residual"] <= 1e-10 * rep["initial_residual"]
+    assert relerr(x.cpu().numpy(), xo) < (1e-7 if mixed else 1e-8)
+    if not mixed:
+        assert abs(it - it_o) <= (0 if solver == "CG" else 2), (it, it_o)
+
+
 @pytest.mark.parametrize("mixed", [False, True])
 def test_gmres_chebyshev_restarted(cuda, mixed):
     """GMRES with the Chebyshev smoother as its right preconditioner, over
