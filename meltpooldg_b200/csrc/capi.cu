@@ -778,16 +778,25 @@ mpdg_status mpdg_solve_host(mpdg_op *op, const mpdg_solver_desc *desc, double *x
     if (!op || !desc || !x_host || !b_host) throw Error{MPDG_ERR_ARG, "null argument"};
     Op &o = op->o;
     const size_t bytes = sizeof(double) * o.mesh->N;
-    double *d_x = nullptr, *d_b = nullptr;
-    MPDG_CUDA(tracked_malloc(&d_x, bytes));
-    MPDG_CUDA(tracked_malloc(&d_b, bytes));
-    MPDG_CUDA(cudaMemcpyAsync(d_x, x_host, bytes, cudaMemcpyHostToDevice, o.stream));
-    MPDG_CUDA(cudaMemcpyAsync(d_b, b_host, bytes, cudaMemcpyHostToDevice, o.stream));
-    int s = solve(o, *desc, d_x, d_b, local);
-    MPDG_CUDA(cudaMemcpyAsync(x_host, d_x, bytes, cudaMemcpyDeviceToHost, o.stream));
+    // device copies of x and b, freed on every exit (a failed solve throws)
+    struct Buffers {
+      double *x = nullptr, *b = nullptr;
+      cudaStream_t st = nullptr;
+      ~Buffers()
+      {
+        if (st) cudaStreamSynchronize(st);
+        if (x) cudaFree(x);
+        if (b) cudaFree(b);
+      }
+    } d;
+    d.st = o.stream;
+    MPDG_CUDA(tracked_malloc(&d.x, bytes));
+    MPDG_CUDA(tracked_malloc(&d.b, bytes));
+    MPDG_CUDA(cudaMemcpyAsync(d.x, x_host, bytes, cudaMemcpyHostToDevice, o.stream));
+    MPDG_CUDA(cudaMemcpyAsync(d.b, b_host, bytes, cudaMemcpyHostToDevice, o.stream));
+    int s = solve(o, *desc, d.x, d.b, local);
+    MPDG_CUDA(cudaMemcpyAsync(x_host, d.x, bytes, cudaMemcpyDeviceToHost, o.stream));
     MPDG_CUDA(cudaStreamSynchronize(o.stream));
-    cudaFree(d_x);
-    cudaFree(d_b);
     return s;
   });
   local.status = st;

@@ -225,3 +225,33 @@ def test_solver_failure_modes_are_reported(cuda):
     with pytest.raises(M.MpdgError) as e:
         M.LinearSolver.solve(op, x, dev(bad), M.LinearSolverData(solver_type="CG"))
     assert e.value.status == -6
+
+
+@pytest.mark.parametrize("solver", ["CG", "GMRES"])
+def test_solve_with_host_buffers_equals_device_solve(cuda, solver):
+    """mpdg_solve_host (host x and b, device copies inside the call) runs the
+    same loop as mpdg_solve: the same iterates, bit for bit; a failing solve
+    reports its error and leaves the operator usable."""
+    import torch
+    import meltpooldg_b200 as M
+    if solver == "CG":
+        gm, om, mask, T, xs, oop, b = _c2_like((5, 5, 5), 2)
+        op = M.HeatDiffuseOperator(gm, 1e-3, k0=1.0, k_alpha=1e-3)
+        op.set_temperature(dev(T))
+    else:
+        gm, om, b, oop = _advdiff_system()
+        op = M.AdvectionDiffusionOperator(gm, 1e-2, theta=0.5, diffusivity=1e-2, velocity="vortex")
+    data = M.LinearSolverData(solver_type=solver, rel_tolerance=1e-10, abs_tolerance=1e-20)
+    x = torch.zeros(gm.n_dofs, dtype=torch.float64, device="cuda")
+    it = M.LinearSolver.solve(op, x, dev(b), data)
+    xh = np.zeros(gm.n_dofs)
+    it_h = M.LinearSolver.solve_host(op, xh, np.ascontiguousarray(b), data)
+    assert it_h == it
+    assert np.array_equal(xh, x.cpu().numpy())
+    bad = b.copy()
+    bad[len(bad) // 2] = np.nan
+    with pytest.raises(M.MpdgError):
+        M.LinearSolver.solve_host(op, np.zeros(gm.n_dofs), bad, data)
+    xh2 = np.zeros(gm.n_dofs)
+    assert M.LinearSolver.solve_host(op, xh2, np.ascontiguousarray(b), data) == it
+    assert np.array_equal(xh2, xh)
