@@ -357,7 +357,14 @@ mpdg_status mpdg_create_rhs_host(mpdg_op *op, double *dst_host, const double *sr
 
 /* LinearSolver::solve, include/meltpooldg/linear_algebra/linear_solver.hpp:26-134,
  * with the Jacobi preconditioner of preconditioner_jacobi.hpp:29-88 (or the
- * Chebyshev smoother on top of it).  x holds the initial guess on entry. */
+ * Chebyshev smoother on top of it).  x holds the initial guess on entry.
+ * GMRES is right-preconditioned with restart gmres_restart (default 30, at
+ * most 60); its Arnoldi basis is orthogonalised by delayed classical
+ * Gram-Schmidt with re-orthogonalisation, which builds the Krylov basis and
+ * residual estimates of modified Gram-Schmidt in exact arithmetic, and applies
+ * the operator once more than it iterates in each cycle that converges.  CG
+ * tests convergence on the device after every iteration; the report counts
+ * the iterations up to the one that converged. */
 mpdg_status mpdg_solve(mpdg_op *op, const mpdg_solver_desc *desc, double *x, const double *b,
                        mpdg_solve_report *report);
 /* host-buffer form of mpdg_solve (x_host in/out, b_host in) */
