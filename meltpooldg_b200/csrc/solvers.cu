@@ -31,7 +31,6 @@ struct Workspace {
   double *partial = nullptr;  // reduction partials: 128 groups of kRedBlocks
   double *scal = nullptr;     // device scalars (kNScalars) + GMRES dots (128)
   double *host = nullptr;     // pinned host mirror
-  bool invd_valid = false;
   size_t bytes = 0;
 };
 
